@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 hot path (the driver's bench contract).
+
+One step = one pass of ORCTM's nonhydrostatic hot path (OCUAD, OCVAD, OCWAD,
+OCADPO for T, S and a passive tracer, OCTDIFF, OCVISC, OCVTOT_NH with its
+Poisson solve to a 1e-10 relative residual), orctm.f90:1454-1562, on a seeded
+synthetic instance of the 1024 x 1024 x 80 configuration (c3) resident on one
+GPU.  Multi-GPU runs are independent replicas (one instance per rank, weak
+scaling, no collective on the data path); timing is the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes per interior cell per launch of each launcher group
+# (each distinct array the math needs read once, each output written once;
+# thickness/mask geometry is compressed to 2D and counts 0 B).
+BYTES_PER_CELL_F64 = {
+    "ocuad": 40, "ocvad": 40, "ocwad": 40, "ocadpo": 40,
+    "ocvisc": 56, "nh_rhs": 56, "nh_post": 56,
+    "pcg_spmv": 32, "pcg_col": 56, "resid": 24,
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group(backend="gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def workload(args, rank):
+    from orctm_b200 import configs
+
+    over = {}
+    if args.size:
+        nx, ny, nz = (int(v) for v in args.size.split("x"))
+        over = {"nx": nx, "ny": ny, "nz": nz}
+    t = time.time()
+    inst = configs.make_instance(args.config, index=rank, **over)
+    log(f"[bench] rank {rank}: instance {args.config} {inst['nx']}x{inst['ny']}x{inst['nz']} "
+        f"generated in {time.time() - t:.1f}s")
+    return inst
+
+
+def cpu_sample(args, solver_rtol=1e-10):
+    """The CPU restatement (oracle) timed on the host cores on a bounded sample
+    of the same workload: one hot-path step of a sub-domain generated with the
+    same generators (same dx, dz, dt, bathymetry statistics)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    from orctm_b200 import configs
+
+    nx, ny, nz = args.cpu_sample
+    inst = configs.make_instance(args.config, builder=O.build_grid, nx=nx, ny=ny, nz=nz)
+    orc = O.Oracle(inst)
+    st = configs.copy_state(inst)
+    orc.step_hotpath(st, solver="fgmres", rtol=solver_rtol)  # warm-up (and warm start)
+    t0 = time.perf_counter()
+    steps = 0
+    solve_s = 0.0
+    while True:
+        info = orc.step_hotpath(st, solver="fgmres", rtol=solver_rtol)
+        steps += 1
+        if time.perf_counter() - t0 > args.cpu_seconds or steps >= 50:
+            break
+    dt_ = time.perf_counter() - t0
+    cells = nx * ny * nz
+    return {"value": cells * steps / dt_, "unit": "cell-steps/s",
+            "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+            "sample": f"{steps} hot-path steps of a {nx}x{ny}x{nz} sub-domain with the "
+                      f"{args.config} generators (C restatement, OpenMP, FGMRES(30)+line "
+                      f"preconditioner to {solver_rtol:g})",
+            "ms_per_step": 1e3 * dt_ / steps, "last_krylov_its": int(info["its"])}
+
+
+def run_reference(args, ws, rank, pg):
+    if rank != 0:
+        return 0
+    cb = cpu_sample(args)
+    line = {"impl": "reference", "metric": "cell-steps/s", "value": cb["value"],
+            "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic (seeded PCG64, base seed 20261203)",
+            "config": {"workload": f"{args.config} hot path, CPU sample"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def timed_steps(gpu, k, pg):
+    from orctm_b200.api import Instance
+
+    barrier(pg)
+    gpu.synchronize()
+    n0 = Instance.kernel_launches()
+    gpu.timer_start()
+    stats = [gpu.step_hotpath() for _ in range(k)]
+    ms = gpu.timer_stop()
+    launches = Instance.kernel_launches() - n0
+    barrier(pg)
+    return ms, stats, launches
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c3")
+    ap.add_argument("--size", default=None, help="override nx x ny x nz (e.g. 256x256x60)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-sample", type=lambda s: tuple(int(v) for v in s.split("x")),
+                    default=(128, 128, 80))
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank, pg)
+
+    from orctm_b200 import configs
+    from orctm_b200.api import Instance
+
+    inst = workload(args, rank)
+    cells = inst["nx"] * inst["ny"] * inst["nz"]
+    gpu = Instance(inst, device=local)
+    gpu.upload_state(configs.copy_state(inst))
+    gpu.set_solver("fp64", rtol=1e-10, maxit=5000)
+    for _ in range(args.warmup):
+        gpu.step_hotpath()
+
+    # ---- FP64 drop-in path (headline) ------------------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    gpu.set_profiling(True)
+    ms, stats, launches = timed_steps(gpu, args.steps, pg)
+    prof = gpu.profile()
+    gpu.set_profiling(False)
+    ck = clocks.stop()
+    # the same steps without event brackets: the timed number
+    ms, stats2, launches = timed_steps(gpu, args.steps, pg)
+    ms_max = max_over_ranks(pg, ms)
+    value = ws * cells * args.steps / (ms_max / 1e3)
+    poisson_ms = statistics.mean(s["solve_ms"] for s in stats2)
+    iters = statistics.mean(s["iterations"] for s in stats2)
+    relres = max(s["relres"] for s in stats2)
+
+    # ---- FP32-refined solver form ------------------------------------------
+    gpu.set_solver("fp32_refined", rtol=1e-10, maxit=5000)
+    for _ in range(2):
+        gpu.step_hotpath()
+    ms_m, stats_m, _ = timed_steps(gpu, args.steps, pg)
+    ms_m = max_over_ranks(pg, ms_m)
+    mixed = {"value": ws * cells * args.steps / (ms_m / 1e3), "unit": "cell-steps/s",
+             "ms_per_step": ms_m / args.steps,
+             "poisson_ms": statistics.mean(s["solve_ms"] for s in stats_m),
+             "poisson_iterations": statistics.mean(s["iterations"] for s in stats_m),
+             "outer_iterations": statistics.mean(s["outer_iterations"] for s in stats_m),
+             "relres_max": max(s["relres"] for s in stats_m)}
+    mixed["speedup_vs_fp64"] = mixed["value"] / value
+    gpu.set_solver("fp64", rtol=1e-10, maxit=5000)
+
+    # ---- roofline of the dominant kernel --------------------------------
+    hbm, peak_kind = peaks()
+    top = max((k for k in prof if prof[k]["launches"] > 0), key=lambda k: prof[k]["ms"])
+    per_launch_ms = prof[top]["ms"] / prof[top]["launches"]
+    bpl = BYTES_PER_CELL_F64.get(top, 0) * cells
+    achieved = bpl / (per_launch_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        if top in tj:
+            traffic = tj[top]["dram_bytes_per_cell"] * cells
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind ==
+                "measured" else "fallback 6.65 TB/s",
+                "bytes_per_launch": bpl, "avg_launch_ms": per_launch_ms,
+                "breakdown_ms_per_step": {k: round(v["ms"] / args.steps, 3) for k, v in prof.items()},
+                "algorithmic_bytes_per_cell": BYTES_PER_CELL_F64}
+
+    # ---- end to end through the public API with host buffers ---------------
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(gpu, inst, cells, args, ws, pg)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_sample(args)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"error": repr(ex)}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-steps/s (hot path incl. Poisson solve @1e-10 rel. residual)",
+            "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64, base seed 20261203; generators of BASELINE configs)",
+            "config": {"workload": f"{args.config} {inst['nx']}x{inst['ny']}x{inst['nz']} "
+                                   f"dt={inst['dt']:g}s, one instance per GPU",
+                       "cells_per_gpu": cells, "tracers": inst["ntracers"],
+                       "l2": "inputs larger than L2 (each 3D field "
+                             f"{8 * cells / 1e9:.2f} GB vs 126 MB L2)",
+                       "solver": "FP64 PCG (line preconditioner, scaled operator) in "
+                                 "double-double-residual refinement"},
+            "poisson_ms": poisson_ms, "poisson_iterations": iters, "relres_max": relres,
+            "mixed": mixed, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": ck,
+        }
+        print(json.dumps(line), flush=True)
+    gpu.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def run_e2e(gpu, inst, cells, args, ws, pg):
+    """Each step: inputs copied from pinned host memory (the fields the
+    hydrostatic part of the reference step produces), the hot path, the
+    outputs read back (the fields the rest of the model consumes)."""
+    import torch
+
+    from orctm_b200 import configs
+
+    st = configs.copy_state(inst)
+    ins = ["uoo", "voe", "wno", "uko", "vke", "wo"]
+    outs = ["uoo", "voe", "wno", "pnh"]
+    pinned = {}
+
+    def pin(a):
+        t = torch.empty(a.shape[::-1], dtype=torch.float64, pin_memory=True)
+        v = t.numpy().T  # Fortran-ordered view
+        v[...] = a
+        return t, v
+
+    for k in ins:
+        pinned["in_" + k] = pin(st[k])
+    for n, tr in enumerate(st["tracers"]):
+        pinned[f"in_tracer{n}"] = pin(tr)
+    for k in outs:
+        pinned["out_" + k] = pin(np.zeros(gpu.shape(k)))
+    for n in range(gpu.ntr):
+        pinned[f"out_tracer{n}"] = pin(np.zeros(gpu.shape("pnh")))
+    h2d = sum(pinned[k][1].nbytes for k in pinned if k.startswith("in_"))
+    d2h = sum(pinned[k][1].nbytes for k in pinned if k.startswith("out_"))
+    k_steps = max(2, min(args.steps, 5))
+
+    def one():
+        for k in ins:
+            gpu.upload(k, pinned["in_" + k][1])
+        for n in range(gpu.ntr):
+            gpu.upload(f"tracer{n}", pinned[f"in_tracer{n}"][1])
+        s = gpu.step_hotpath()
+        for k in outs:
+            gpu.download(k, pinned["out_" + k][1])
+        for n in range(gpu.ntr):
+            gpu.download(f"tracer{n}", pinned[f"out_tracer{n}"][1])
+        return s
+
+    one()
+    barrier(pg)
+    gpu.timer_start()
+    for _ in range(k_steps):
+        one()
+    ms = gpu.timer_stop()
+    ms = max_over_ranks(pg, ms)
+    return {"value": ws * cells * k_steps / (ms / 1e3), "unit": "cell-steps/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "steps": k_steps, "ms_per_step": ms / k_steps}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,183 @@
+/*
+ * orctm_gpu.h -- C ABI of the B200 (sm_100a) implementation of ORCTM's
+ * nonhydrostatic time-step hot path.
+ *
+ * The entry points replace the bodies of the reference's Fortran subroutines
+ * (paths relative to the reference project, ORCTM/src_orctm/):
+ *
+ *   orctm_create        petsc_start          mo_petsc.f90:41-128 (operator set up
+ *                                            once, like KSPSetComputeOperators)
+ *   orctm_destroy       petsc_end            mo_petsc.f90:131-143
+ *   orctm_ocuad         SUBROUTINE OCUAD     ocuad.f90:1-271
+ *   orctm_ocvad         SUBROUTINE OCVAD     ocvad.f90:1-271
+ *   orctm_ocwad         SUBROUTINE OCWAD     ocwad.f90:1-238
+ *   orctm_ocadpo        SUBROUTINE OCADPO    ocadpo.f90:1-368
+ *   orctm_octdiff       OCTDIFF_BASE + OCTDIFF_TS  octdiff_base.f90:1-229,
+ *                                            octdiff_ts.f90:1-430
+ *   orctm_octimf        SUBROUTINE OCTIMF    octimf.f90:1-22
+ *   orctm_ocvisc        SUBROUTINE OCVISC    ocvisc.f90:1-772 (FREESLIP)
+ *   orctm_ocvtot_nh     SUBROUTINE OCVTOT_NH ocvtot_nh.f90:1-259, including
+ *                       petsc_solve_3D / ComputeRHS / compute_matrix
+ *                                            mo_petsc.f90:211-397, 543-782
+ *   orctm_step_hotpath  the driver's call sequence orctm.f90:1454-1562
+ *   orctm_upload / orctm_download   the module arrays of MO_COMMO1
+ *                                   (mo_commo1.f90:32-146) that the path reads
+ *                                   and writes, moved between host and device
+ *   orctm_build_grid    BELEG + BODEN geometry (beleg.f90:48-139,
+ *                       boden.f90:38-286), a set-up helper for callers that
+ *                       have no Fortran host
+ *
+ * Conventions
+ *  - Every function returns an int status: ORCTM_OK (0) or a negative error
+ *    class.  The library never aborts; a Fortran caller maps a nonzero status
+ *    to ABSTURZ (absturz.f90:10-11) as the reference's fatal path does.
+ *  - Host arrays are the reference's Fortran arrays on a single-rank domain
+ *    (I_start = J_start = 0), column-major, halos included:
+ *        p-points  X(1:IE, 1:JE, 1:KE)     IE*JE*KE values
+ *        u-points  X(0:IE, 1:JE, 1:KE)     (IE+1)*JE*KE
+ *        v-points  X(1:IE, 0:JE, 1:KE)     IE*(JE+1)*KE
+ *        w-points  X(1:IE, 1:JE, 1:KE+1)   IE*JE*(KE+1)
+ *        2D arrays analogous (IE*JE, (IE+1)*JE, IE*(JE+1)).
+ *  - All arithmetic of the default path is IEEE binary64.
+ *  - A handle is used by one host thread at a time.  The model state lives
+ *    on the device between calls (resident mode); only orctm_upload and
+ *    orctm_download move it.  Both return after the copy has completed.
+ *  - All entry points are asynchronous with respect to the host except the
+ *    copies, orctm_synchronize and the solve statistics of orctm_ocvtot_nh.
+ */
+#ifndef ORCTM_GPU_H
+#define ORCTM_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORCTM_ABI_VERSION 1
+
+/* status codes */
+#define ORCTM_OK 0
+#define ORCTM_E_ARG (-1)           /* bad argument or size */
+#define ORCTM_E_CUDA (-2)          /* CUDA runtime error */
+#define ORCTM_E_NOMEM (-3)         /* device allocation failed */
+#define ORCTM_E_NOT_CONVERGED (-4) /* Poisson solve hit maxit (state still updated) */
+#define ORCTM_E_GEOMETRY (-5)      /* masks/thicknesses not of the BODEN form */
+#define ORCTM_E_UNSUPPORTED (-6)   /* option outside the restated path */
+#define ORCTM_E_NODEVICE (-7)      /* no usable CUDA device */
+
+/* field ids for orctm_upload / orctm_download (MO_COMMO1 array names) */
+enum {
+  ORCTM_F_UOO = 0,   /* u-points */
+  ORCTM_F_VOE = 1,   /* v-points */
+  ORCTM_F_WNO = 2,   /* w-points */
+  ORCTM_F_UKO = 3,   /* u-points */
+  ORCTM_F_VKE = 4,   /* v-points */
+  ORCTM_F_WO = 5,    /* w-points */
+  ORCTM_F_UOO_1 = 6, /* u-points */
+  ORCTM_F_VOE_1 = 7, /* v-points */
+  ORCTM_F_WNO_1 = 8, /* w-points */
+  ORCTM_F_PNH = 9,   /* p-points */
+  ORCTM_F_ZO = 10,   /* 2D p-points */
+  ORCTM_F_DVO = 11,  /* w-points (IE,JE,KEP) */
+  ORCTM_F_AVO = 12,  /* w-points (IE,JE,KEP) */
+  ORCTM_F_THO = 13,  /* tracer 0; tracer n is ORCTM_F_THO + n (SAO = tracer 1) */
+  ORCTM_F_SAO = 14
+};
+
+/* solver modes (orctm_set_solver) */
+#define ORCTM_SOLVER_FP64 0        /* FP64 PCG, column-tridiagonal preconditioner */
+#define ORCTM_SOLVER_FP32_REFINED 1 /* FP32 inner PCG inside FP64 iterative refinement */
+
+typedef struct orctm_desc {
+  int ie, je, ke;          /* IE, JE, KE including the 1-cell halo */
+  int i_start, j_start;    /* must be 0: single-rank domain (mo_parallel.f90:197-206) */
+  int ntracers;            /* >= 2: THO, SAO, then passive tracers (max 8) */
+  int ob_west, ob_east, ob_north, ob_south; /* open-boundary switches (mo_obcs.f90:9-20) */
+  double dt;               /* DT */
+  double almzer;           /* ALMZER (orctm.f90:240) */
+  double aulapts, aulapuv; /* biharmonic coefficients (orctm.f90:500-501) */
+  double ah00;             /* harmonic tracer diffusion; must be <= almzer */
+  const double* dzw;       /* DZW(KE) */
+  const double* di;        /* DI(KE+1) */
+  const double *dlxp, *dlyp, *dtdxpo, *dtdyo; /* 2D p-points */
+  const double *dlxu, *dlyu, *dtdxuo;         /* 2D u-points */
+  const double *dlxv, *dlyv, *dpye;           /* 2D v-points */
+  const double *ddpo, *weto;                  /* 3D p-points */
+  const double *dduo, *amsuo;                 /* 3D u-points */
+  const double *ddue, *amsue;                 /* 3D v-points */
+  int device;              /* CUDA device ordinal */
+} orctm_desc;
+
+typedef struct orctm_solve_stats {
+  int iterations;       /* Krylov iterations (inner iterations for the refined solver) */
+  int outer_iterations; /* refinement sweeps (1 for the FP64 solver) */
+  int converged;        /* 1 if ||b - A x||_2 <= rtol ||b||_2 */
+  double relres;        /* final ||b - A x||_2 / ||b||_2, computed in FP64 */
+  double relres_initial;/* the same for the warm start */
+  double solve_ms;      /* device time of the solve */
+} orctm_solve_stats;
+
+typedef struct orctm_handle orctm_handle;
+
+int orctm_abi_version(void);
+const char* orctm_status_string(int status);
+/* last error message of a handle (or of the thread's last failed create) */
+const char* orctm_last_error(const orctm_handle* h);
+
+int orctm_create(const orctm_desc* desc, orctm_handle** out);
+int orctm_destroy(orctm_handle* h);
+
+/* number of doubles of a field in the host layout */
+int orctm_field_size(const orctm_handle* h, int field, size_t* n);
+int orctm_upload(orctm_handle* h, int field, const double* host, size_t n);
+int orctm_download(orctm_handle* h, int field, double* host, size_t n);
+
+int orctm_ocuad(orctm_handle* h);
+int orctm_ocvad(orctm_handle* h);
+int orctm_ocwad(orctm_handle* h);
+int orctm_ocadpo(orctm_handle* h, int tracer);
+int orctm_octdiff(orctm_handle* h);
+int orctm_octimf(orctm_handle* h);
+int orctm_ocvisc(orctm_handle* h);
+int orctm_ocvtot_nh(orctm_handle* h, orctm_solve_stats* stats);
+int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* stats);
+
+/* solver mode and relative-residual target (default FP64, 1e-10, 5000) */
+int orctm_set_solver(orctm_handle* h, int mode, double rtol, int maxit);
+int orctm_synchronize(orctm_handle* h);
+
+/* Device-time measurement on the handle's stream (CUDA events). */
+int orctm_timer_start(orctm_handle* h);
+int orctm_timer_stop(orctm_handle* h, double* ms);
+
+/* Optional per-launcher device timing: when on, every launcher group of the
+ * kinds below is bracketed by CUDA events; orctm_profile_get returns the
+ * number of bracketed launches and their summed device time since the last
+ * orctm_set_profiling call. */
+enum {
+  ORCTM_PROF_OCUAD = 0, ORCTM_PROF_OCVAD, ORCTM_PROF_OCWAD, ORCTM_PROF_OCADPO,
+  ORCTM_PROF_OCTDIFF, ORCTM_PROF_OCVISC, ORCTM_PROF_NH_RHS, ORCTM_PROF_PCG_SPMV,
+  ORCTM_PROF_PCG_COL, ORCTM_PROF_RESID, ORCTM_PROF_NH_POST, ORCTM_PROF_KINDS
+};
+int orctm_set_profiling(orctm_handle* h, int on);
+int orctm_profile_get(orctm_handle* h, int kind, long long* launches, double* total_ms);
+
+/* Number of CUDA kernels this library has launched in the calling process. */
+unsigned long long orctm_kernel_launches(void);
+
+/* BELEG + BODEN restated on the host.  depto (IE*JE) is adjusted in place as
+ * BODEN does (ISTART == 0).  Output arrays are caller-allocated in the host
+ * layouts above; tiestu, tiestw, dz and di hold KE+1 values. */
+int orctm_build_grid(int ie, int je, int ke, double dt, const double* dzw, double* depto,
+                     const double* dlxp, const double* dlyp, const double* dlxu,
+                     const double* dlyu, const double* dlxv, const double* dlyv,
+                     double* tiestu, double* tiestw, double* dz, double* di, double* dtdxpo,
+                     double* dtdyo, double* dtdxuo, double* dpyo, double* dtdxue, double* dpye,
+                     double* ddpo, double* weto, double* dduo, double* amsuo, double* ddue,
+                     double* amsue);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORCTM_GPU_H */

@@ -1,0 +1,209 @@
+"""ctypes front end of the CPU restatement (oracle) of ORCTM's NH hot path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, and only as the checker or the timed CPU
+baseline.  PARITY UNPINNED: the reference (Fortran/PETSc) cannot run here and
+ships no golden outputs; see orctm_oracle.c.
+
+Arrays are numpy float64 in Fortran order with the reference's shapes
+(single-rank domain, I_start = J_start = 0):
+    p-points (IE, JE, KE)      u-points (IE+1, JE, KE)
+    v-points (IE, JE+1, KE)    w-points (IE, JE, KE+1)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "liborctm_oracle.so")
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+def build(force: bool = False) -> str:
+    """Compiles liborctm_oracle.so with the Makefile next to this file."""
+    if force or not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(
+        os.path.join(_HERE, "orctm_oracle.c")
+    ):
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "all"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _SO
+
+
+class _Grid(C.Structure):
+    _fields_ = [
+        ("ie", C.c_int), ("je", C.c_int), ("ke", C.c_int),
+        ("ob_west", C.c_int), ("ob_east", C.c_int), ("ob_north", C.c_int), ("ob_south", C.c_int),
+        ("dt", C.c_double), ("almzer", C.c_double), ("aulapts", C.c_double),
+        ("aulapuv", C.c_double), ("ah00", C.c_double),
+        ("dzw", _D), ("di", _D), ("dz", _D), ("tiestu", _D), ("tiestw", _D),
+        ("dlxp", _D), ("dlyp", _D), ("dtdxpo", _D), ("dtdyo", _D),
+        ("dlxu", _D), ("dlyu", _D), ("dtdxuo", _D), ("dpyo", _D),
+        ("dlxv", _D), ("dlyv", _D), ("dtdxue", _D), ("dpye", _D),
+        ("ddpo", _D), ("weto", _D), ("dduo", _D), ("amsuo", _D), ("ddue", _D), ("amsue", _D),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        _lib.og_matrix_nnz.restype = C.c_size_t
+        _lib.og_solve.restype = C.c_int
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim == 1), a.flags
+    return a.ctypes.data_as(_D)
+
+
+GEOM_KEYS = ("tiestu", "tiestw", "dz", "di", "dtdxpo", "dtdyo", "dtdxuo", "dpyo", "dtdxue",
+             "dpye", "ddpo", "weto", "dduo", "amsuo", "ddue", "amsue")
+
+
+def build_grid(ie, je, ke, dt, dzw, depto, dlxp, dlyp, dlxu, dlyu, dlxv, dlyv):
+    """BELEG + BODEN restated: returns (depto_adjusted, geometry dict)."""
+    f = lambda s: np.zeros(s, dtype=np.float64, order="F")
+    depto = np.array(depto, dtype=np.float64, order="F", copy=True)
+    g = {
+        "tiestu": f(ke + 1), "tiestw": f(ke + 1), "dz": f(ke + 1), "di": f(ke + 1),
+        "dtdxpo": f((ie, je)), "dtdyo": f((ie, je)), "dtdxuo": f((ie + 1, je)),
+        "dpyo": f((ie + 1, je)), "dtdxue": f((ie, je + 1)), "dpye": f((ie, je + 1)),
+        "ddpo": f((ie, je, ke)), "weto": f((ie, je, ke)), "dduo": f((ie + 1, je, ke)),
+        "amsuo": f((ie + 1, je, ke)), "ddue": f((ie, je + 1, ke)), "amsue": f((ie, je + 1, ke)),
+    }
+    dzw = np.ascontiguousarray(dzw, dtype=np.float64)
+    args = [np.asfortranarray(a, dtype=np.float64) for a in (dlxp, dlyp, dlxu, dlyu, dlxv, dlyv)]
+    lib().og_build_grid(ie, je, ke, C.c_double(dt), _p(dzw), _p(depto), *[_p(a) for a in args],
+                        *[_p(g[k]) for k in GEOM_KEYS])
+    return depto, g
+
+
+class Oracle:
+    """Holds one instance's geometry and exposes the restated routines."""
+
+    def __init__(self, inst: dict):
+        self.inst = inst
+        self.ie, self.je, self.ke = inst["ie"], inst["je"], inst["ke"]
+        self._keep = {}
+        gr = _Grid()
+        gr.ie, gr.je, gr.ke = self.ie, self.je, self.ke
+        ob = inst["ob"]
+        gr.ob_west, gr.ob_east, gr.ob_north, gr.ob_south = (int(ob[k]) for k in ("west", "east", "north", "south"))
+        gr.dt = inst["dt"]
+        gr.almzer = inst["almzer"]
+        gr.aulapts = inst["aulapts"]
+        gr.aulapuv = inst["aulapuv"]
+        gr.ah00 = inst["ah00"]
+        for k in ("dzw", "di", "dz", "tiestu", "tiestw", "dlxp", "dlyp", "dtdxpo", "dtdyo", "dlxu",
+                  "dlyu", "dtdxuo", "dpyo", "dlxv", "dlyv", "dtdxue", "dpye", "ddpo", "weto",
+                  "dduo", "amsuo", "ddue", "amsue"):
+            a = np.asfortranarray(inst[k], dtype=np.float64)
+            self._keep[k] = a
+            setattr(gr, k, _p(a))
+        self.g = gr
+
+    # -- stencils ---------------------------------------------------------
+    def ocadpo(self, trf, uko, vke, wo, zo):
+        lib().og_ocadpo(C.byref(self.g), _p(trf), _p(uko), _p(vke), _p(wo), _p(zo))
+
+    def ocuad(self, uoo, uko, vke, wo):
+        lib().og_ocuad(C.byref(self.g), _p(uoo), _p(uko), _p(vke), _p(wo))
+
+    def ocvad(self, voe, uko, vke, wo):
+        lib().og_ocvad(C.byref(self.g), _p(voe), _p(uko), _p(vke), _p(wo))
+
+    def ocwad(self, wno, uko, vke, wo, zo):
+        lib().og_ocwad(C.byref(self.g), _p(wno), _p(uko), _p(vke), _p(wo), _p(zo))
+
+    def octdiff(self, tracers, dvo, zo):
+        arr = (_D * len(tracers))(*[_p(t) for t in tracers])
+        lib().og_octdiff(C.byref(self.g), len(tracers), arr, _p(dvo), _p(zo))
+
+    def ocvisc(self, uoo, voe, wno, uko, vke, avo):
+        lib().og_ocvisc(C.byref(self.g), _p(uoo), _p(voe), _p(wno), _p(uko), _p(vke), _p(avo))
+
+    def octimf(self, uoo, voe, uko, vke):
+        lib().og_octimf(C.byref(self.g), _p(uoo), _p(voe), _p(uko), _p(vke))
+
+    # -- OCVTOT_NH ----------------------------------------------------------
+    @property
+    def nunk(self):
+        return (self.ie - 2) * (self.je - 2) * self.ke
+
+    def nh_rhs(self, uoo, uoo1, voe, voe1, wno, wno1, zo):
+        b = np.zeros(self.nunk)
+        lib().og_nh_rhs(C.byref(self.g), _p(uoo), _p(uoo1), _p(voe), _p(voe1), _p(wno), _p(wno1),
+                        _p(zo), _p(b))
+        return b
+
+    def matrix(self):
+        """compute_matrix as a scipy CSR matrix (DMDA natural order)."""
+        import scipy.sparse as sp
+
+        nnz = lib().og_matrix_nnz(C.byref(self.g))
+        rp = np.zeros(self.nunk + 1, dtype=np.int32)
+        ci = np.zeros(nnz, dtype=np.int32)
+        v = np.zeros(nnz)
+        lib().og_matrix_csr(C.byref(self.g), rp.ctypes.data_as(_I), ci.ctypes.data_as(_I), _p(v))
+        return sp.csr_matrix((v, ci, rp), shape=(self.nunk, self.nunk))
+
+    def solve(self, A, b, x0=None, rtol=1e-13, maxit=5000):
+        """FGMRES + column preconditioner (CPU).  Returns (x, its, relres)."""
+        x = np.zeros(self.nunk) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        rp = np.ascontiguousarray(A.indptr, dtype=np.int32)
+        ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+        v = np.ascontiguousarray(A.data, dtype=np.float64)
+        rel = C.c_double(0.0)
+        its = lib().og_solve(C.byref(self.g), rp.ctypes.data_as(_I), ci.ctypes.data_as(_I), _p(v),
+                             _p(np.ascontiguousarray(b)), _p(x), C.c_double(rtol), maxit,
+                             C.byref(rel))
+        return x, its, rel.value
+
+    @staticmethod
+    def direct_solve(A, b):
+        """Sparse LU solve (SuperLU): the stand-in for PETSc's FGMRES + one-level
+        PCMG, whose single level is a direct factorisation."""
+        import scipy.sparse.linalg as spl
+
+        return spl.spsolve(A.tocsc(), b)
+
+    def nh_post(self, x, pnh, uoo, voe, wno, uoo1, voe1, wno1, wo):
+        lib().og_nh_post(C.byref(self.g), _p(np.ascontiguousarray(x)), _p(pnh), _p(uoo), _p(voe),
+                         _p(wno), _p(uoo1), _p(voe1), _p(wno1), _p(wo))
+
+    def ocvtot_nh(self, st, solver="direct", rtol=1e-13):
+        """Whole OCVTOT_NH on a state dict (in place).  Returns solve info."""
+        b = self.nh_rhs(st["uoo"], st["uoo1"], st["voe"], st["voe1"], st["wno"], st["wno1"], st["zo"])
+        A = self.matrix()
+        x0 = st["pnh"][1:-1, 1:-1, :].reshape(-1, order="F").copy()
+        if solver == "direct":
+            x = self.direct_solve(A, b)
+            its, rel = 1, float(np.linalg.norm(b - A @ x) / max(np.linalg.norm(b), 1e-300))
+        else:
+            x, its, rel = self.solve(A, b, x0=x0, rtol=rtol)
+        self.nh_post(x, st["pnh"], st["uoo"], st["voe"], st["wno"], st["uoo1"], st["voe1"],
+                     st["wno1"], st["wo"])
+        return {"its": its, "relres": rel, "b": b, "x": x}
+
+    def step_hotpath(self, st, solver="direct", rtol=1e-13):
+        """One pass of the hot path in the driver's order (orctm.f90:1454-1562)."""
+        self.ocuad(st["uoo"], st["uko"], st["vke"], st["wo"])
+        self.ocvad(st["voe"], st["uko"], st["vke"], st["wo"])
+        self.ocwad(st["wno"], st["uko"], st["vke"], st["wo"], st["zo"])
+        for t in st["tracers"]:
+            self.ocadpo(t, st["uko"], st["vke"], st["wo"], st["zo"])
+        self.octdiff(st["tracers"], st["dvo"], st["zo"])
+        self.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
+        self.ocvisc(st["uoo"], st["voe"], st["wno"], st["uko"], st["vke"], st["avo"])
+        info = self.ocvtot_nh(st, solver=solver, rtol=rtol)
+        self.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
+        return info

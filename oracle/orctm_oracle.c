@@ -1,0 +1,1665 @@
+/*
+ * CPU restatement (oracle) of ORCTM's nonhydrostatic hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py load this library, and
+ * only as the checker or the timed CPU baseline; the CUDA product never calls
+ * it.  PARITY UNPINNED: the reference (Fortran 90 + PETSc 3.10.2) cannot be
+ * built here and ships no golden outputs (see orctm_oracle.h).
+ *
+ * Every routine follows the reference loop by loop; the file:line cited in
+ * front of each block is the reference code it restates
+ * (ORCTM/src_orctm/...).  Build flags: -O2 -ffp-contract=off -fopenmp.
+ * OpenMP only splits loops whose iterations are independent, so results do
+ * not depend on the thread count (the Krylov solve's dot products excepted).
+ */
+#include "orctm_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* Fortran-layout accessors (see orctm_oracle.h). */
+#define P3(a, i, j, k) (a)[((size_t)((k)-1) * JE + (size_t)((j)-1)) * IE + (size_t)((i)-1)]
+#define U3(a, i, j, k) (a)[((size_t)((k)-1) * JE + (size_t)((j)-1)) * (IE + 1) + (size_t)(i)]
+#define V3(a, i, j, k) (a)[((size_t)((k)-1) * (JE + 1) + (size_t)(j)) * IE + (size_t)((i)-1)]
+/* levels 0..KE (TRM/WTM in the reference are dimensioned 0:KE) */
+#define M3(a, i, j, k) (a)[((size_t)(k) * JE + (size_t)((j)-1)) * IE + (size_t)((i)-1)]
+#define MU3(a, i, j, k) (a)[((size_t)(k) * JE + (size_t)((j)-1)) * (IE + 1) + (size_t)(i)]
+#define MV3(a, i, j, k) (a)[((size_t)(k) * (JE + 1) + (size_t)(j)) * IE + (size_t)((i)-1)]
+#define P2(a, i, j) (a)[(size_t)((j)-1) * IE + (size_t)((i)-1)]
+#define U2(a, i, j) (a)[(size_t)((j)-1) * (IE + 1) + (size_t)(i)]
+#define V2(a, i, j) (a)[(size_t)(j) * IE + (size_t)((i)-1)]
+#define K1(a, k) (a)[(k)-1]
+
+#define DIMS                      \
+  const int IE = g->ie;           \
+  const int JE = g->je;           \
+  const int KE = g->ke;           \
+  const int KEP = KE + 1;         \
+  const int IE1 = IE - 1;         \
+  const int JE1 = JE - 1;         \
+  (void)KEP; (void)IE1; (void)JE1
+
+/* Fortran MAX(a,b) / MIN(a,b) for non-NaN operands. */
+static inline double fmx(double a, double b) { return a > b ? a : b; }
+static inline double fmn(double a, double b) { return b < a ? b : a; }
+
+static double *zalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+
+/* ------------------------------------------------------------------------ */
+/* BELEG (beleg.f90:48-139) + BODEN (boden.f90:38-213)                      */
+/* ------------------------------------------------------------------------ */
+void og_build_grid(int ie, int je, int ke, double dt, const double *dzw,
+                   double *depto, const double *dlxp, const double *dlyp,
+                   const double *dlxu, const double *dlyu, const double *dlxv,
+                   const double *dlyv, double *tiestu, double *tiestw,
+                   double *dz, double *di, double *dtdxpo, double *dtdyo,
+                   double *dtdxuo, double *dpyo, double *dtdxue, double *dpye,
+                   double *ddpo, double *weto, double *dduo, double *amsuo,
+                   double *ddue, double *amsue) {
+  const int IE = ie, JE = je, KE = ke, KEP = ke + 1, IE1 = ie - 1, JE1 = je - 1;
+  /* beleg.f90:42-76 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      P2(dtdxpo, i, j) = dt / P2(dlxp, i, j);
+      P2(dtdyo, i, j) = dt / P2(dlyp, i, j);
+    }
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i) {
+      U2(dtdxuo, i, j) = dt / U2(dlxu, i, j);
+      U2(dpyo, i, j) = dt / U2(dlyu, i, j);
+    }
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      V2(dtdxue, i, j) = dt / V2(dlxv, i, j);
+      V2(dpye, i, j) = dt / V2(dlyv, i, j);
+    }
+  /* beleg.f90:87-105, 125-139 */
+  K1(tiestu, 1) = 0.5 * K1(dzw, 1);
+  K1(tiestw, 1) = 0.0;
+  for (int k = 1; k <= KE; ++k) K1(tiestw, k + 1) = K1(tiestw, k) + K1(dzw, k);
+  for (int k = 2; k <= KE; ++k) K1(tiestu, k) = 0.5 * (K1(tiestw, k + 1) + K1(tiestw, k));
+  K1(tiestu, KEP) = 9000.;
+  K1(dz, 1) = K1(tiestu, 1);
+  for (int k = 2; k <= KEP; ++k) K1(dz, k) = K1(tiestu, k) - K1(tiestu, k - 1);
+  for (int k = 1; k <= KE; ++k) K1(di, k) = 1. / K1(dz, k);
+  K1(di, KEP) = 1. / K1(dz, KE);
+
+  /* boden.f90:38-62 (ISTART == 0) */
+  const double minvalue = fmn(1.0, K1(dzw, 1) / 10.0);
+  const double depmin = K1(dzw, 1) + K1(dzw, 2) + minvalue;
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      if (P2(depto, i, j) <= minvalue) P2(depto, i, j) = 0.;
+      if (P2(depto, i, j) > minvalue && P2(depto, i, j) < depmin) P2(depto, i, j) = depmin;
+    }
+  /* boden.f90:101-107 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i)
+      for (int k = 1; k <= KE; ++k)
+        if (fabs(P2(depto, i, j) - K1(tiestu, k)) < minvalue / 2)
+          P2(depto, i, j) = K1(tiestu, k) + minvalue;
+  /* boden.f90:116-130: DEUTO (u-points, 0:IE) and DEUTE (v-points, 0:JE) */
+  double *deuto = zalloc((size_t)(IE + 1) * JE);
+  double *deute = zalloc((size_t)IE * (JE + 1));
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE1; ++i) U2(deuto, i, j) = fmn(P2(depto, i, j), P2(depto, i + 1, j));
+  for (int j = 1; j <= JE; ++j) {
+    U2(deuto, 0, j) = U2(deuto, 1, j);
+    U2(deuto, IE, j) = U2(deuto, IE1, j);
+  }
+  for (int j = 1; j <= JE1; ++j)
+    for (int i = 1; i <= IE; ++i) V2(deute, i, j) = fmn(P2(depto, i, j), P2(depto, i, j + 1));
+  for (int i = 1; i <= IE; ++i) {
+    V2(deute, i, 0) = V2(deute, i, 1);
+    V2(deute, i, JE) = V2(deute, i, JE1);
+  }
+  /* boden.f90:182-213 (arrays start at zero, BELEG_ZERO) */
+  memset(ddpo, 0, sizeof(double) * (size_t)IE * JE * KE);
+  memset(weto, 0, sizeof(double) * (size_t)IE * JE * KE);
+  memset(dduo, 0, sizeof(double) * (size_t)(IE + 1) * JE * KE);
+  memset(amsuo, 0, sizeof(double) * (size_t)(IE + 1) * JE * KE);
+  memset(ddue, 0, sizeof(double) * (size_t)IE * (JE + 1) * KE);
+  memset(amsue, 0, sizeof(double) * (size_t)IE * (JE + 1) * KE);
+  for (int k = 1; k <= KE; ++k) {
+    const double tu = K1(tiestu, k), tu1 = K1(tiestu, k + 1), tw = K1(tiestw, k);
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        const double d = P2(depto, i, j);
+        if (tu < d) P3(weto, i, j, k) = 1.;
+        if (tu1 < d) P3(ddpo, i, j, k) = K1(dzw, k);
+        if (tu < d && tu1 >= d) P3(ddpo, i, j, k) = d - tw;
+      }
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        const double d = U2(deuto, i, j);
+        if (tu1 < d) U3(dduo, i, j, k) = K1(dzw, k);
+        if (tu < d && tu1 >= d) U3(dduo, i, j, k) = d - tw;
+        if (U3(dduo, i, j, k) > 0.) U3(amsuo, i, j, k) = 1.;
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        const double d = V2(deute, i, j);
+        if (tu1 < d) V3(ddue, i, j, k) = K1(dzw, k);
+        if (tu < d && tu1 >= d) V3(ddue, i, j, k) = d - tw;
+        if (V3(ddue, i, j, k) > 0.) V3(amsue, i, j, k) = 1.;
+      }
+  }
+  free(deuto);
+  free(deute);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCADPO (ocadpo.f90:94-348), options ADPO on, SMOADV/SMOADH and           */
+/* SLOPECON_ADPO off (Makefile:42-51).  Sea-ice terms SICTHO/SICSNO are     */
+/* zero: the ice model is not called (octher.f90:51).                      */
+/* ------------------------------------------------------------------------ */
+void og_ocadpo(const og_grid *g, double *trf, const double *uko, const double *vke,
+               const double *wo, const double *zo) {
+  DIMS;
+  const double DT = g->dt;
+  const size_t n3 = (size_t)IE * JE * KE, n0 = (size_t)IE * JE * (KE + 1);
+  double *s1o = zalloc(n3), *t1o = zalloc(n3);
+  double *trp = zalloc(n0), *wtp = zalloc(n0); /* 1..KEP */
+  double *trm = zalloc(n0), *wtm = zalloc(n0); /* 0..KE  */
+  /* ocadpo.f90:94-116 */
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        P3(s1o, i, j, k) = P3(g->weto, i, j, k) * P2(g->dlxp, i, j) * P2(g->dlyp, i, j) *
+                           P3(g->ddpo, i, j, k);
+        P3(t1o, i, j, k) = P3(trf, i, j, k);
+      }
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i)
+      P3(s1o, i, j, 1) = P3(s1o, i, j, 1) + P2(g->dlxp, i, j) * P2(g->dlyp, i, j) *
+                                                P3(g->weto, i, j, 1) *
+                                                (P2(zo, i, j) - P3(wo, i, j, 1) * DT);
+  /* vertical transports, ocadpo.f90:120-143 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    const int klo = k + 1 < KE ? k + 1 : KE;
+    const int kup = k - 1 > 1 ? k - 1 : 1;
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = P3(trf, i, j, k), tu = P3(trf, i, j, kup), tl = P3(trf, i, j, klo);
+        const double abl = fabs(tu - tl);
+        const double zwabl = fabs(tu + tl - 2. * t);
+        const double w0 = P3(wo, i, j, k), w1 = P3(wo, i, j, k + 1);
+        const double up = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (w0 + fabs(w0));
+        const double um = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (fabs(w1) - w1);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+        double sch = fmn(P3(g->weto, i, j, klo), scha * P3(s1o, i, j, k) / (up + um + 1.E-20));
+        if (k == 1 || k == KE) sch = 0.;
+        const double schi = 1. - sch;
+        P3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tu));
+        M3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tl));
+        P3(wtp, i, j, k) = up;
+        M3(wtm, i, j, k) = um;
+      }
+  }
+  /* ocadpo.f90:158-173 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (P3(g->weto, i, j, k) > 0.5) {
+          const double rn = P3(s1o, i, j, k) + P3(wtp, i, j, k + 1) - P3(wtp, i, j, k) -
+                            M3(wtm, i, j, k) + M3(wtm, i, j, k - 1);
+          P3(t1o, i, j, k) = (P3(trf, i, j, k) * P3(s1o, i, j, k) + P3(trp, i, j, k + 1) -
+                              P3(trp, i, j, k) - M3(trm, i, j, k) + M3(trm, i, j, k - 1)) /
+                             rn;
+          P3(s1o, i, j, k) = rn;
+        }
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) P3(trf, i, j, k) = P3(t1o, i, j, k);
+
+  /* x-direction, ocadpo.f90:181-258 */
+  memset(trp, 0, sizeof(double) * n0);
+  memset(trm, 0, sizeof(double) * n0);
+  memset(wtp, 0, sizeof(double) * n0);
+  memset(wtm, 0, sizeof(double) * n0);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = P3(trf, i, j, k), te = P3(trf, i + 1, j, k), tw = P3(trf, i - 1, j, k);
+        const double abl = fabs(te - tw);
+        const double zwabl = fabs(te + tw - 2. * t);
+        const double u0 = U3(uko, i, j, k), um1 = U3(uko, i - 1, j, k);
+        const double up = 0.5 * DT * U3(g->dduo, i, j, k) * U2(g->dlyu, i, j) * (u0 + fabs(u0));
+        const double um = 0.5 * DT * U3(g->dduo, i - 1, j, k) * (fabs(um1) - um1) *
+                          U2(g->dlyu, i - 1, j);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * P3(g->weto, i, j, k) *
+                            P3(g->weto, i + 1, j, k) * P3(g->weto, i - 1, j, k);
+        const double sch = fmn(1., scha * P3(s1o, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        P3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + te));
+        M3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tw));
+        P3(wtp, i, j, k) = up;
+        M3(wtm, i, j, k) = um;
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (P3(g->weto, i, j, k) > 0.5) {
+          const double rn = P3(s1o, i, j, k) + P3(wtp, i - 1, j, k) - P3(wtp, i, j, k) -
+                            M3(wtm, i, j, k) + M3(wtm, i + 1, j, k);
+          P3(t1o, i, j, k) = (P3(trf, i, j, k) * P3(s1o, i, j, k) + P3(trp, i - 1, j, k) -
+                              P3(trp, i, j, k) - M3(trm, i, j, k) + M3(trm, i + 1, j, k)) /
+                             rn;
+          P3(s1o, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) P3(trf, i, j, k) = P3(t1o, i, j, k);
+  }
+
+  /* y-direction, ocadpo.f90:266-345 */
+  memset(trp, 0, sizeof(double) * n0);
+  memset(trm, 0, sizeof(double) * n0);
+  memset(wtp, 0, sizeof(double) * n0);
+  memset(wtm, 0, sizeof(double) * n0);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = P3(trf, i, j, k), tn = P3(trf, i, j - 1, k), ts = P3(trf, i, j + 1, k);
+        const double abl = fabs(tn - ts);
+        const double zwabl = fabs(tn + ts - 2. * t);
+        const double vn = V3(vke, i, j - 1, k), vs = V3(vke, i, j, k);
+        const double up = 0.5 * DT * V3(g->ddue, i, j - 1, k) * V2(g->dlxv, i, j - 1) * (vn + fabs(vn));
+        const double um = 0.5 * DT * V3(g->ddue, i, j, k) * V2(g->dlxv, i, j) * (fabs(vs) - vs);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * P3(g->weto, i, j, k) *
+                            P3(g->weto, i, j - 1, k) * P3(g->weto, i, j + 1, k);
+        const double sch = fmn(1., scha * P3(s1o, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        P3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tn));
+        M3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + ts));
+        P3(wtp, i, j, k) = up;
+        M3(wtm, i, j, k) = um;
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (P3(g->weto, i, j, k) > 0.5) {
+          const double rn = P3(s1o, i, j, k) + P3(wtp, i, j + 1, k) - P3(wtp, i, j, k) -
+                            M3(wtm, i, j, k) + M3(wtm, i, j - 1, k);
+          P3(t1o, i, j, k) = (P3(trf, i, j, k) * P3(s1o, i, j, k) + P3(trp, i, j + 1, k) -
+                              P3(trp, i, j, k) - M3(trm, i, j, k) + M3(trm, i, j - 1, k)) /
+                             rn;
+          P3(s1o, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) P3(trf, i, j, k) = P3(t1o, i, j, k);
+  }
+  free(s1o); free(t1o); free(trp); free(wtp); free(trm); free(wtm);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCUAD (ocuad.f90:1-271): u-points, TRF(I_start:IE,JE,KE), I_start = 0.   */
+/* ------------------------------------------------------------------------ */
+void og_ocuad(const og_grid *g, double *trf, const double *uko, const double *vke,
+              const double *wo) {
+  DIMS;
+  const double DT = g->dt;
+  const size_t n3 = (size_t)(IE + 1) * JE * KE, n0 = (size_t)(IE + 1) * JE * (KE + 1);
+  double *trvol = zalloc(n3), *tr1 = zalloc(n3);
+  double *trp = zalloc(n0), *wtp = zalloc(n0), *trm = zalloc(n0), *wtm = zalloc(n0);
+  /* ocuad.f90:20-32 */
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        U3(trvol, i, j, k) = U3(g->amsuo, i, j, k) * U2(g->dlxu, i, j) * U2(g->dlyu, i, j) *
+                             U3(g->dduo, i, j, k);
+        U3(tr1, i, j, k) = U3(trf, i, j, k);
+      }
+  /* vertical, ocuad.f90:35-55 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    const int klo = k + 1 < KE ? k + 1 : KE;
+    const int kup = k - 1 > 1 ? k - 1 : 1;
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) {
+        const double t = U3(trf, i, j, k), tu = U3(trf, i, j, kup), tl = U3(trf, i, j, klo);
+        const double abl = fabs(tu - tl);
+        const double zwabl = fabs(tu + tl - 2. * t);
+        const double wup = 0.5 * (P3(wo, i, j, k) + P3(wo, i + 1, j, k));
+        const double wlo = 0.5 * (P3(wo, i, j, k + 1) + P3(wo, i + 1, j, k + 1));
+        const double up = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (wup + fabs(wup));
+        const double um = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (fabs(wlo) - wlo);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+        const double sch = fmn(1., scha * U3(trvol, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        U3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tu));
+        MU3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tl));
+        U3(wtp, i, j, k) = up;
+        MU3(wtm, i, j, k) = um;
+      }
+  }
+  /* ocuad.f90:71-86 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i)
+        if (U3(g->amsuo, i, j, k) > 0.5) {
+          const double rn = U3(trvol, i, j, k) + U3(wtp, i, j, k + 1) - U3(wtp, i, j, k) -
+                            MU3(wtm, i, j, k) + MU3(wtm, i, j, k - 1);
+          U3(tr1, i, j, k) = (U3(trf, i, j, k) * U3(trvol, i, j, k) + U3(trp, i, j, k + 1) -
+                              U3(trp, i, j, k) - MU3(trm, i, j, k) + MU3(trm, i, j, k - 1)) /
+                             rn;
+          U3(trvol, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) U3(trf, i, j, k) = U3(tr1, i, j, k);
+  }
+  memset(trp, 0, sizeof(double) * n0); memset(trm, 0, sizeof(double) * n0);
+  memset(wtp, 0, sizeof(double) * n0); memset(wtm, 0, sizeof(double) * n0);
+  /* x-direction, ocuad.f90:99-148 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) {
+        const double t = U3(trf, i, j, k), te = U3(trf, i + 1, j, k), tw = U3(trf, i - 1, j, k);
+        const double abl = fabs(te - tw);
+        const double zwabl = fabs(te + tw - 2. * t);
+        const double uos = 0.5 * (U3(uko, i, j, k) * U3(g->dduo, i, j, k) +
+                                  U3(uko, i + 1, j, k) * U3(g->dduo, i + 1, j, k));
+        const double uwe = 0.5 * (U3(uko, i - 1, j, k) * U3(g->dduo, i - 1, j, k) +
+                                  U3(uko, i, j, k) * U3(g->dduo, i, j, k));
+        const double up = 0.5 * DT * P2(g->dlyp, i + 1, j) * (uos + fabs(uos));
+        const double um = 0.5 * DT * (fabs(uwe) - uwe) * P2(g->dlyp, i, j);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+        const double sch = fmn(1., scha * U3(trvol, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        U3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + te));
+        MU3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tw));
+        U3(wtp, i, j, k) = up;
+        MU3(wtm, i, j, k) = um;
+      }
+    for (int j = 2; j <= JE1; ++j) { /* have_g_is, I = 0 */
+      const int i = 0;
+      const double uos = 0.5 * (U3(uko, i, j, k) * U3(g->dduo, i, j, k) +
+                                U3(uko, i + 1, j, k) * U3(g->dduo, i + 1, j, k));
+      const double uwe = U3(uko, i, j, k) * U3(g->dduo, i, j, k);
+      const double up = 0.5 * DT * P2(g->dlyp, i + 1, j) * (uos + fabs(uos));
+      const double um = 0.5 * DT * (fabs(uwe) - uwe) * U2(g->dlyu, i, j);
+      U3(trp, i, j, k) = up * U3(trf, i, j, k);
+      MU3(trm, i, j, k) = um * U3(trf, i, j, k);
+      U3(wtp, i, j, k) = up;
+      MU3(wtm, i, j, k) = um;
+    }
+    for (int j = 2; j <= JE1; ++j) { /* have_g_ie, I = IE */
+      const int i = IE;
+      const double uos = U3(uko, i, j, k) * U3(g->dduo, i, j, k);
+      const double uwe = 0.5 * (U3(uko, i - 1, j, k) * U3(g->dduo, i - 1, j, k) +
+                                U3(uko, i, j, k) * U3(g->dduo, i, j, k));
+      const double up = 0.5 * DT * P2(g->dlyp, i, j) * (uos + fabs(uos));
+      const double um = 0.5 * DT * (fabs(uwe) - uwe) * U2(g->dlyu, i, j);
+      U3(trp, i, j, k) = up * U3(trf, i, j, k);
+      MU3(trm, i, j, k) = um * U3(trf, i, j, k);
+      U3(wtp, i, j, k) = up;
+      MU3(wtm, i, j, k) = um;
+    }
+  }
+  /* ocuad.f90:157-172 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i)
+        if (U3(g->amsuo, i, j, k) > 0.5) {
+          const double rn = U3(trvol, i, j, k) + U3(wtp, i - 1, j, k) - U3(wtp, i, j, k) -
+                            MU3(wtm, i, j, k) + MU3(wtm, i + 1, j, k);
+          U3(tr1, i, j, k) = (U3(trf, i, j, k) * U3(trvol, i, j, k) + U3(trp, i - 1, j, k) -
+                              U3(trp, i, j, k) - MU3(trm, i, j, k) + MU3(trm, i + 1, j, k)) /
+                             rn;
+          U3(trvol, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) U3(trf, i, j, k) = U3(tr1, i, j, k);
+  }
+  memset(trp, 0, sizeof(double) * n0); memset(trm, 0, sizeof(double) * n0);
+  memset(wtp, 0, sizeof(double) * n0); memset(wtm, 0, sizeof(double) * n0);
+  /* y-direction, ocuad.f90:184-233 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) {
+        const double t = U3(trf, i, j, k), tn = U3(trf, i, j - 1, k), ts = U3(trf, i, j + 1, k);
+        const double abl = fabs(tn - ts);
+        const double zwabl = fabs(tn + ts - 2. * t);
+        const double vsu = 0.5 * (V3(vke, i, j, k) * V3(g->ddue, i, j, k) +
+                                  V3(vke, i + 1, j, k) * V3(g->ddue, i + 1, j, k));
+        const double vno = 0.5 * (V3(vke, i, j - 1, k) * V3(g->ddue, i, j - 1, k) +
+                                  V3(vke, i + 1, j - 1, k) * V3(g->ddue, i + 1, j - 1, k));
+        const double up = 0.5 * DT * (0.5 * (V2(g->dlxv, i, j - 1) + V2(g->dlxv, i + 1, j - 1))) *
+                          (vno + fabs(vno));
+        const double um = 0.5 * DT * (0.5 * (V2(g->dlxv, i, j) + V2(g->dlxv, i + 1, j))) *
+                          (fabs(vsu) - vsu);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+        const double sch = fmn(1., scha * U3(trvol, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        U3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tn));
+        MU3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + ts));
+        U3(wtp, i, j, k) = up;
+        MU3(wtm, i, j, k) = um;
+      }
+    for (int e = 0; e < 2; ++e) { /* have_g_js (J = 1) and have_g_je (J = JE) */
+      const int j = e == 0 ? 1 : JE;
+      for (int i = 1; i <= IE1; ++i) {
+        const double vsu = 0.5 * (V3(vke, i, j, k) * V3(g->ddue, i, j, k) +
+                                  V3(vke, i + 1, j, k) * V3(g->ddue, i + 1, j, k));
+        const double vno = 0.5 * (V3(vke, i, j - 1, k) * V3(g->ddue, i, j - 1, k) +
+                                  V3(vke, i + 1, j - 1, k) * V3(g->ddue, i + 1, j - 1, k));
+        const double up = 0.5 * DT * (0.5 * (V2(g->dlxv, i, j - 1) + V2(g->dlxv, i + 1, j - 1))) *
+                          (vno + fabs(vno));
+        const double um = 0.5 * DT * (0.5 * (V2(g->dlxv, i, j) + V2(g->dlxv, i + 1, j))) *
+                          (fabs(vsu) - vsu);
+        U3(trp, i, j, k) = up * U3(trf, i, j, k);
+        MU3(trm, i, j, k) = um * U3(trf, i, j, k);
+        U3(wtp, i, j, k) = up;
+        MU3(wtm, i, j, k) = um;
+      }
+    }
+  }
+  /* ocuad.f90:242-257 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i)
+        if (U3(g->amsuo, i, j, k) > 0.5) {
+          const double rn = U3(trvol, i, j, k) + U3(wtp, i, j + 1, k) - U3(wtp, i, j, k) -
+                            MU3(wtm, i, j, k) + MU3(wtm, i, j - 1, k);
+          U3(tr1, i, j, k) = (U3(trf, i, j, k) * U3(trvol, i, j, k) + U3(trp, i, j + 1, k) -
+                              U3(trp, i, j, k) - MU3(trm, i, j, k) + MU3(trm, i, j - 1, k)) /
+                             rn;
+          U3(trvol, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) U3(trf, i, j, k) = U3(tr1, i, j, k);
+  }
+  free(trvol); free(tr1); free(trp); free(wtp); free(trm); free(wtm);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCVAD (ocvad.f90:1-271): v-points, TRF(IE,J_start:JE,KE), J_start = 0.   */
+/* The J = 0 edge flux reads DLXU(I,0) (ocvad.f90:211), an element outside  */
+/* DLXU's bounds (J from 1): the restatement reads DLXV(I,0), the zonal     */
+/* width at that v-point, in its place.                                    */
+/* ------------------------------------------------------------------------ */
+void og_ocvad(const og_grid *g, double *trf, const double *uko, const double *vke,
+              const double *wo) {
+  DIMS;
+  const double DT = g->dt;
+  const size_t n3 = (size_t)IE * (JE + 1) * KE, n0 = (size_t)IE * (JE + 1) * (KE + 1);
+  double *trvol = zalloc(n3), *tr1 = zalloc(n3);
+  double *trp = zalloc(n0), *wtp = zalloc(n0), *trm = zalloc(n0), *wtm = zalloc(n0);
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        V3(trvol, i, j, k) = V3(g->amsue, i, j, k) * V2(g->dlxv, i, j) * V2(g->dlyv, i, j) *
+                             V3(g->ddue, i, j, k);
+        V3(tr1, i, j, k) = V3(trf, i, j, k);
+      }
+  /* vertical, ocvad.f90:35-55 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    const int klo = k + 1 < KE ? k + 1 : KE;
+    const int kup = k - 1 > 1 ? k - 1 : 1;
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = V3(trf, i, j, k), tu = V3(trf, i, j, kup), tl = V3(trf, i, j, klo);
+        const double abl = fabs(tu - tl);
+        const double zwabl = fabs(tu + tl - 2. * t);
+        const double wup = 0.5 * (P3(wo, i, j, k) + P3(wo, i, j + 1, k));
+        const double wlo = 0.5 * (P3(wo, i, j, k + 1) + P3(wo, i, j + 1, k + 1));
+        const double up = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (wup + fabs(wup));
+        const double um = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (fabs(wlo) - wlo);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+        const double sch = fmn(1., scha * V3(trvol, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        V3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tu));
+        MV3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tl));
+        V3(wtp, i, j, k) = up;
+        MV3(wtm, i, j, k) = um;
+      }
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (V3(g->amsue, i, j, k) > 0.5) {
+          const double rn = V3(trvol, i, j, k) + V3(wtp, i, j, k + 1) - V3(wtp, i, j, k) -
+                            MV3(wtm, i, j, k) + MV3(wtm, i, j, k - 1);
+          V3(tr1, i, j, k) = (V3(trf, i, j, k) * V3(trvol, i, j, k) + V3(trp, i, j, k + 1) -
+                              V3(trp, i, j, k) - MV3(trm, i, j, k) + MV3(trm, i, j, k - 1)) /
+                             rn;
+          V3(trvol, i, j, k) = rn;
+        }
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) V3(trf, i, j, k) = V3(tr1, i, j, k);
+  }
+  memset(trp, 0, sizeof(double) * n0); memset(trm, 0, sizeof(double) * n0);
+  memset(wtp, 0, sizeof(double) * n0); memset(wtm, 0, sizeof(double) * n0);
+  /* x-direction, ocvad.f90:99-148 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        const int edge = (i == 1 || i == IE);
+        const double t = V3(trf, i, j, k);
+        const double uos = 0.5 * (U3(uko, i, j, k) * U3(g->dduo, i, j, k) +
+                                  U3(uko, i, j + 1, k) * U3(g->dduo, i, j + 1, k));
+        const double uwe = 0.5 * (U3(uko, i - 1, j, k) * U3(g->dduo, i - 1, j, k) +
+                                  U3(uko, i - 1, j + 1, k) * U3(g->dduo, i - 1, j + 1, k));
+        const double up = 0.5 * DT * (0.5 * (U2(g->dlyu, i, j) + U2(g->dlyu, i, j + 1))) *
+                          (uos + fabs(uos));
+        const double um = 0.5 * DT * (fabs(uwe) - uwe) *
+                          (0.5 * (U2(g->dlyu, i - 1, j) + U2(g->dlyu, i - 1, j + 1)));
+        if (edge) { /* have_g_is / have_g_ie rows, ocvad.f90:120-148 */
+          V3(trp, i, j, k) = up * t;
+          MV3(trm, i, j, k) = um * t;
+        } else {
+          const double te = V3(trf, i + 1, j, k), tw = V3(trf, i - 1, j, k);
+          const double abl = fabs(te - tw);
+          const double zwabl = fabs(te + tw - 2. * t);
+          const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+          const double sch = fmn(1., scha * V3(trvol, i, j, k) / (up + um + 1.E-20));
+          const double schi = 1. - sch;
+          V3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + te));
+          MV3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tw));
+        }
+        V3(wtp, i, j, k) = up;
+        MV3(wtm, i, j, k) = um;
+      }
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (V3(g->amsue, i, j, k) > 0.5) {
+          const double rn = V3(trvol, i, j, k) + V3(wtp, i - 1, j, k) - V3(wtp, i, j, k) -
+                            MV3(wtm, i, j, k) + MV3(wtm, i + 1, j, k);
+          V3(tr1, i, j, k) = (V3(trf, i, j, k) * V3(trvol, i, j, k) + V3(trp, i - 1, j, k) -
+                              V3(trp, i, j, k) - MV3(trm, i, j, k) + MV3(trm, i + 1, j, k)) /
+                             rn;
+          V3(trvol, i, j, k) = rn;
+        }
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) V3(trf, i, j, k) = V3(tr1, i, j, k);
+  }
+  memset(trp, 0, sizeof(double) * n0); memset(trm, 0, sizeof(double) * n0);
+  memset(wtp, 0, sizeof(double) * n0); memset(wtm, 0, sizeof(double) * n0);
+  /* y-direction, ocvad.f90:184-233 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = V3(trf, i, j, k), tn = V3(trf, i, j - 1, k), ts = V3(trf, i, j + 1, k);
+        const double abl = fabs(tn - ts);
+        const double zwabl = fabs(tn + ts - 2. * t);
+        const double vno = 0.5 * (V3(vke, i, j, k) * V3(g->ddue, i, j, k) +
+                                  V3(vke, i, j - 1, k) * V3(g->ddue, i, j - 1, k));
+        const double vsu = 0.5 * (V3(vke, i, j, k) * V3(g->ddue, i, j, k) +
+                                  V3(vke, i, j + 1, k) * V3(g->ddue, i, j + 1, k));
+        const double up = 0.5 * DT * P2(g->dlxp, i, j) * (vno + fabs(vno));
+        const double um = 0.5 * DT * P2(g->dlxp, i, j + 1) * (fabs(vsu) - vsu);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+        const double sch = fmn(1., scha * V3(trvol, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        V3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tn));
+        MV3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + ts));
+        V3(wtp, i, j, k) = up;
+        MV3(wtm, i, j, k) = um;
+      }
+    for (int i = 2; i <= IE1; ++i) { /* have_g_js, J = 0 */
+      const int j = 0;
+      const double vno = V3(vke, i, j, k) * V3(g->ddue, i, j, k);
+      const double vsu = 0.5 * (V3(vke, i, j, k) * V3(g->ddue, i, j, k) +
+                                V3(vke, i, j + 1, k) * V3(g->ddue, i, j + 1, k));
+      const double up = 0.5 * DT * V2(g->dlxv, i, j) * (vno + fabs(vno)); /* DLXU(I,0) in ref */
+      const double um = 0.5 * DT * P2(g->dlxp, i, j + 1) * (fabs(vsu) - vsu);
+      V3(trp, i, j, k) = up * V3(trf, i, j, k);
+      MV3(trm, i, j, k) = um * V3(trf, i, j, k);
+      V3(wtp, i, j, k) = up;
+      MV3(wtm, i, j, k) = um;
+    }
+    for (int i = 2; i <= IE1; ++i) { /* have_g_je, J = JE */
+      const int j = JE;
+      const double vno = 0.5 * (V3(vke, i, j, k) * V3(g->ddue, i, j, k) +
+                                V3(vke, i, j - 1, k) * V3(g->ddue, i, j - 1, k));
+      const double vsu = V3(vke, i, j, k) * V3(g->ddue, i, j, k);
+      const double up = 0.5 * DT * P2(g->dlxp, i, j) * (vno + fabs(vno));
+      const double um = 0.5 * DT * U2(g->dlxu, i, j) * (fabs(vsu) - vsu);
+      V3(trp, i, j, k) = up * V3(trf, i, j, k);
+      MV3(trm, i, j, k) = um * V3(trf, i, j, k);
+      V3(wtp, i, j, k) = up;
+      MV3(wtm, i, j, k) = um;
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (V3(g->amsue, i, j, k) > 0.5) {
+          const double rn = V3(trvol, i, j, k) + V3(wtp, i, j + 1, k) - V3(wtp, i, j, k) -
+                            MV3(wtm, i, j, k) + MV3(wtm, i, j - 1, k);
+          V3(tr1, i, j, k) = (V3(trf, i, j, k) * V3(trvol, i, j, k) + V3(trp, i, j + 1, k) -
+                              V3(trp, i, j, k) - MV3(trm, i, j, k) + MV3(trm, i, j - 1, k)) /
+                             rn;
+          V3(trvol, i, j, k) = rn;
+        }
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) V3(trf, i, j, k) = V3(tr1, i, j, k);
+  }
+  free(trvol); free(tr1); free(trp); free(wtp); free(trm); free(wtm);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCWAD (ocwad.f90:1-238): w-points, TRF(IE,JE,KEP).  At K = KE the        */
+/* vertical limiter reads WETO(I,J,KEP) (ocwad.f90:63), one level past      */
+/* WETO's last level: the restatement takes it as 0 (no water below the    */
+/* deepest level), which makes that interface first-order upwind.          */
+/* ------------------------------------------------------------------------ */
+void og_ocwad(const og_grid *g, double *trf, const double *uko, const double *vke,
+              const double *wo, const double *zo) {
+  DIMS;
+  const double DT = g->dt;
+  const size_t n3 = (size_t)IE * JE * KE, n0 = (size_t)IE * JE * (KE + 1);
+  double *s1o = zalloc(n3), *t1o = zalloc(n3);
+  double *trp = zalloc(n0), *wtp = zalloc(n0), *trm = zalloc(n0), *wtm = zalloc(n0);
+  /* ocwad.f90:14-37 */
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        P3(t1o, i, j, k) = P3(trf, i, j, k);
+        const double a = P3(g->weto, i, j, k) * P2(g->dlxp, i, j) * P2(g->dlyp, i, j);
+        if (k == 1)
+          P3(s1o, i, j, k) = a * (P3(g->ddpo, i, j, k) + P2(zo, i, j)) / 2.0;
+        else if (k == 2)
+          P3(s1o, i, j, k) = a * (P3(g->ddpo, i, j, k - 1) + P3(g->ddpo, i, j, k) + P2(zo, i, j)) / 2.0;
+        else
+          P3(s1o, i, j, k) = a * (P3(g->ddpo, i, j, k - 1) + P3(g->ddpo, i, j, k)) / 2.0;
+      }
+  /* vertical, ocwad.f90:50-69 */
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= KE; ++k) {
+    const int klo = k + 1, kup = k - 1;
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = P3(trf, i, j, k), tu = P3(trf, i, j, kup), tl = P3(trf, i, j, klo);
+        const double abl = fabs(tu - tl);
+        const double zwabl = fabs(tu + tl - 2. * t);
+        const double wup = 0.5 * (P3(wo, i, j, k) + P3(wo, i, j, kup));
+        const double wum = 0.5 * (P3(wo, i, j, k) + P3(wo, i, j, klo));
+        const double up = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (wup + fabs(wup));
+        const double um = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (fabs(wum) - wum);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+        const double wklo = klo <= KE ? P3(g->weto, i, j, klo) : 0.0;
+        const double sch = fmn(wklo, scha * P3(s1o, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        P3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tu));
+        M3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tl));
+        P3(wtp, i, j, k) = up;
+        M3(wtm, i, j, k) = um;
+      }
+  }
+  /* ocwad.f90:72-83 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      const double wup = 0.5 * (P3(wo, i, j, KEP) + P3(wo, i, j, KE));
+      const double up = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (wup + fabs(wup));
+      P3(trp, i, j, KEP) = up * (0.5 * (P3(trf, i, j, KE) + P3(trf, i, j, KEP)));
+      P3(wtp, i, j, KEP) = up;
+      const double wum = 0.5 * (P3(wo, i, j, 1) + P3(wo, i, j, 2));
+      const double um = 0.5 * DT * P2(g->dlyp, i, j) * P2(g->dlxp, i, j) * (fabs(wum) - wum);
+      M3(trm, i, j, 1) = um * (0.5 * (P3(trf, i, j, 1) + P3(trf, i, j, 2)));
+      M3(wtm, i, j, 1) = um;
+    }
+  /* ocwad.f90:88-102 */
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (P3(g->weto, i, j, k) > 0.5) {
+          const double rn = P3(s1o, i, j, k) + P3(wtp, i, j, k + 1) - P3(wtp, i, j, k) -
+                            M3(wtm, i, j, k) + M3(wtm, i, j, k - 1);
+          P3(t1o, i, j, k) = (P3(trf, i, j, k) * P3(s1o, i, j, k) + P3(trp, i, j, k + 1) -
+                              P3(trp, i, j, k) - M3(trm, i, j, k) + M3(trm, i, j, k - 1)) /
+                             rn;
+          P3(s1o, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) P3(trf, i, j, k) = P3(t1o, i, j, k);
+  }
+  /* x-direction, ocwad.f90:110-165 (TRP etc. keep their vertical values
+   * elsewhere; only zero entries at the halo columns are read) */
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = P3(trf, i, j, k), te = P3(trf, i + 1, j, k), tw = P3(trf, i - 1, j, k);
+        const double abl = fabs(te - tw);
+        const double zwabl = fabs(te + tw - 2. * t);
+        const double uos = 0.5 * (U3(uko, i, j, k) * U3(g->dduo, i, j, k) +
+                                  U3(uko, i, j, k - 1) * U3(g->dduo, i, j, k - 1));
+        const double uwe = 0.5 * (U3(uko, i - 1, j, k) * U3(g->dduo, i - 1, j, k) +
+                                  U3(uko, i - 1, j, k - 1) * U3(g->dduo, i - 1, j, k - 1));
+        const double up = 0.5 * DT * U2(g->dlyu, i, j) * (uos + fabs(uos));
+        const double um = 0.5 * DT * U2(g->dlyu, i - 1, j) * (fabs(uwe) - uwe);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * P3(g->weto, i, j, k) *
+                            P3(g->weto, i + 1, j, k) * P3(g->weto, i - 1, j, k);
+        const double sch = fmn(1., scha * P3(s1o, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        P3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + te));
+        M3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + tw));
+        P3(wtp, i, j, k) = up;
+        M3(wtm, i, j, k) = um;
+      }
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (P3(g->weto, i, j, k) > 0.5) {
+          const double rn = P3(s1o, i, j, k) + P3(wtp, i - 1, j, k) - P3(wtp, i, j, k) -
+                            M3(wtm, i, j, k) + M3(wtm, i + 1, j, k);
+          P3(t1o, i, j, k) = (P3(trf, i, j, k) * P3(s1o, i, j, k) + P3(trp, i - 1, j, k) -
+                              P3(trp, i, j, k) - M3(trm, i, j, k) + M3(trm, i + 1, j, k)) /
+                             rn;
+          P3(s1o, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) P3(trf, i, j, k) = P3(t1o, i, j, k);
+  }
+  /* y-direction, ocwad.f90:173-228 */
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double t = P3(trf, i, j, k), tn = P3(trf, i, j - 1, k), ts = P3(trf, i, j + 1, k);
+        const double abl = fabs(tn - ts);
+        const double zwabl = fabs(tn + ts - 2. * t);
+        const double vsu = 0.5 * (V3(vke, i, j, k) * V3(g->ddue, i, j, k) +
+                                  V3(vke, i, j, k - 1) * V3(g->ddue, i, j, k - 1));
+        const double vno = 0.5 * (V3(vke, i, j - 1, k) * V3(g->ddue, i, j - 1, k) +
+                                  V3(vke, i, j - 1, k - 1) * V3(g->ddue, i, j - 1, k - 1));
+        const double up = 0.5 * DT * V2(g->dlxv, i, j - 1) * (vno + fabs(vno));
+        const double um = 0.5 * DT * V2(g->dlxv, i, j) * (fabs(vsu) - vsu);
+        const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * P3(g->weto, i, j, k) *
+                            P3(g->weto, i, j - 1, k) * P3(g->weto, i, j + 1, k);
+        const double sch = fmn(1., scha * P3(s1o, i, j, k) / (up + um + 1.E-20));
+        const double schi = 1. - sch;
+        P3(trp, i, j, k) = up * (schi * t + sch * 0.5 * (t + tn));
+        M3(trm, i, j, k) = um * (schi * t + sch * 0.5 * (t + ts));
+        P3(wtp, i, j, k) = up;
+        M3(wtm, i, j, k) = um;
+      }
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        if (P3(g->weto, i, j, k) > 0.5) {
+          const double rn = P3(s1o, i, j, k) + P3(wtp, i, j + 1, k) - P3(wtp, i, j, k) -
+                            M3(wtm, i, j, k) + M3(wtm, i, j - 1, k);
+          P3(t1o, i, j, k) = (P3(trf, i, j, k) * P3(s1o, i, j, k) + P3(trp, i, j + 1, k) -
+                              P3(trp, i, j, k) - M3(trm, i, j, k) + M3(trm, i, j - 1, k)) /
+                             rn;
+          P3(s1o, i, j, k) = rn;
+        }
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) P3(trf, i, j, k) = P3(t1o, i, j, k);
+  }
+  free(s1o); free(t1o); free(trp); free(wtp); free(trm); free(wtm);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCTDIFF_BASE (octdiff_base.f90:182-221) + OCTDIFF_TS                     */
+/* (octdiff_ts.f90:51-59, 282-407) generalised from (THO,SAO) to ntr        */
+/* tracers, each treated exactly as THO.  Harmonic/isopycnal diffusion      */
+/* (AH00 > ALMZER) is not restated: the caller must pass AH00 = 0, as all   */
+/* verification runs do (OCECTL CAH00 = 0).  VOL_TERM is only assigned      */
+/* under AH00 > ALMZER, so it is taken as 0 here and T1O at the halo cells, */
+/* which the biharmonic second pass reads, is 0.  I3DREST = 0.             */
+/* ------------------------------------------------------------------------ */
+void og_octdiff(const og_grid *g, int ntr, double *const *tr, const double *dvo,
+                const double *zo) {
+  DIMS;
+  const double DT = g->dt, ALMZER = g->almzer;
+  const size_t n3 = (size_t)IE * JE * KE;
+  double *t1o = zalloc(n3);
+  /* vertical implicit diffusion, octdiff_base.f90:182-204 + octdiff_ts.f90:294-324 */
+#pragma omp parallel
+  {
+    double *t1 = (double *)malloc(sizeof(double) * (size_t)KE * 3 + 8);
+    double *t2 = t1 + KE, *t3 = t2 + KE;
+    double *col = (double *)malloc(sizeof(double) * (size_t)KE + 8);
+#pragma omp for schedule(static)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        for (int k = 1; k <= KE; ++k) {
+          const double zzsurf = k == 1 ? 1. : 0.;
+          const double den = P3(g->ddpo, i, j, k) + zzsurf * (P2(zo, i, j)) + ALMZER;
+          t1[k - 1] = -DT * P3(dvo, i, j, k) * P3(g->weto, i, j, k) * K1(g->di, k) / den;
+          t3[k - 1] = -DT * P3(dvo, i, j, k + 1) * K1(g->di, k + 1) / den;
+          t2[k - 1] = 1. - t1[k - 1] - t3[k - 1];
+        }
+        for (int k = 2; k <= KE; ++k) {
+          const double a = t1[k - 1];
+          t1[k - 2] = a / t2[k - 2];
+          t2[k - 1] = t2[k - 1] - t3[k - 2] * a / t2[k - 2];
+        }
+        for (int n = 0; n < ntr; ++n) {
+          double *T = tr[n];
+          for (int k = 1; k <= KE; ++k) col[k - 1] = P3(T, i, j, k);
+          for (int k = 2; k <= KE; ++k) col[k - 1] = col[k - 1] - t1[k - 2] * col[k - 2];
+          P3(T, i, j, KE) = col[KE - 1] / t2[KE - 1];
+          for (int k = 1; k <= KE - 1; ++k) {
+            const int l = KE - k;
+            P3(T, i, j, l) = (col[l - 1] - t3[l - 1] * P3(T, i, j, l + 1)) / t2[l - 1];
+          }
+        }
+      }
+    free(t1);
+    free(col);
+  }
+  /* biharmonic, octdiff_base.f90:208-221 + octdiff_ts.f90:344-407 */
+  if (g->aulapts > ALMZER) {
+    double *aulx = zalloc((size_t)IE * JE), *auly = zalloc((size_t)IE * JE);
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        const double x = U2(g->dlxu, i, j), y = V2(g->dlyv, i, j);
+        P2(aulx, i, j) = g->aulapts * ((x * x) * (x * x));
+        P2(auly, i, j) = g->aulapts * ((y * y) * (y * y));
+      }
+    for (int n = 0; n < ntr; ++n) {
+      double *T = tr[n];
+      memset(t1o, 0, sizeof(double) * n3);
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= KE; ++k)
+        for (int j = 2; j <= JE1; ++j)
+          for (int i = 2; i <= IE1; ++i) {
+            const double c = P3(T, i, j, k);
+            P3(t1o, i, j, k) =
+                P3(g->weto, i, j, k) *
+                ((P3(g->weto, i - 1, j, k) * (P3(T, i - 1, j, k) - c) / U2(g->dlxu, i - 1, j) +
+                  P3(g->weto, i + 1, j, k) * (P3(T, i + 1, j, k) - c) / U2(g->dlxu, i, j)) /
+                     P2(g->dlxp, i, j) +
+                 (P3(g->weto, i, j - 1, k) * (P3(T, i, j - 1, k) - c) / V2(g->dlyv, i, j - 1) +
+                  P3(g->weto, i, j + 1, k) * (P3(T, i, j + 1, k) - c) / V2(g->dlyv, i, j)) /
+                     P2(g->dlyp, i, j));
+          }
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= KE; ++k) {
+        const double zzsurf = k == 1 ? 1. : 0.;
+        for (int j = 2; j <= JE1; ++j)
+          for (int i = 2; i <= IE1; ++i) {
+            const double c = P3(t1o, i, j, k);
+            const double den = (P3(g->ddpo, i, j, k) + ALMZER + zzsurf * (P2(zo, i, j))) *
+                               P2(g->dlxp, i, j) * P2(g->dlyp, i, j);
+            P3(T, i, j, k) =
+                P3(T, i, j, k) -
+                (P3(g->weto, i, j, k) / den) * K1(g->dzw, k) *
+                    (P3(g->weto, i - 1, j, k) * P2(aulx, i - 1, j) * U2(g->dlyu, i - 1, j) *
+                         (P3(t1o, i - 1, j, k) - c) / U2(g->dlxu, i - 1, j) +
+                     P3(g->weto, i + 1, j, k) * P2(aulx, i, j) * U2(g->dlyu, i, j) *
+                         (P3(t1o, i + 1, j, k) - c) / U2(g->dlxu, i, j) +
+                     P3(g->weto, i, j - 1, k) * P2(auly, i, j - 1) * V2(g->dlxv, i, j - 1) *
+                         (P3(t1o, i, j - 1, k) - c) / V2(g->dlyv, i, j - 1) +
+                     P3(g->weto, i, j + 1, k) * P2(auly, i, j) * V2(g->dlxv, i, j) *
+                         (P3(t1o, i, j + 1, k) - c) / V2(g->dlyv, i, j));
+          }
+      }
+    }
+    free(aulx);
+    free(auly);
+  }
+  free(t1o);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCVISC (ocvisc.f90:37-478, 615-688), FREESLIP branch (Makefile:47),      */
+/* AULREDUV off; x**4 is evaluated as (x*x)*(x*x).  Ends with OCTIMF.       */
+/* ------------------------------------------------------------------------ */
+void og_ocvisc(const og_grid *g, double *uoo, double *voe, double *wno,
+               double *uko, double *vke, const double *avo) {
+  DIMS;
+  const double DT = g->dt, ALMZER = g->almzer, AULAPUV = g->aulapuv;
+  const double minvalue = fmn(1.0, K1(g->dzw, 1) / 10.0);
+  const double BOFRIC = 3.E-3, RAYFRIC = 3.E-3;
+  double *speedu = zalloc((size_t)IE * JE), *speedv = zalloc((size_t)IE * JE);
+  /* ocvisc.f90:53-104 */
+  for (int j = 2; j <= JE1; ++j) {
+    for (int k = 1; k <= KE - 1; ++k)
+      for (int i = 1; i <= IE1; ++i)
+        if (U3(g->amsuo, i, j, k) - U3(g->amsuo, i, j, k + 1) > 0.5) {
+          const double a = 0.25 * (V3(voe, i, j, k) + V3(voe, i + 1, j, k) + V3(voe, i, j - 1, k) +
+                                   V3(voe, i + 1, j - 1, k));
+          const double u = U3(uoo, i, j, k);
+          P2(speedu, i, j) = fmx(sqrt(u * u + a * a), 1.E-3);
+        }
+    for (int i = 1; i <= IE1; ++i)
+      if (U3(g->amsuo, i, j, KE) > 0.5) {
+        const int k = KE;
+        const double a = 0.25 * (V3(voe, i, j, k) + V3(voe, i + 1, j, k) + V3(voe, i, j - 1, k) +
+                                 V3(voe, i + 1, j - 1, k));
+        const double u = U3(uoo, i, j, k);
+        P2(speedu, i, j) = fmx(sqrt(u * u + a * a), 1.E-3);
+      }
+  }
+  for (int j = 1; j <= JE1; ++j) {
+    for (int k = 1; k <= KE - 1; ++k)
+      for (int i = 2; i <= IE1; ++i)
+        if (V3(g->amsue, i, j, k) - V3(g->amsue, i, j, k + 1) > 0.5) {
+          const double a = 0.25 * (U3(uoo, i, j, k) + U3(uoo, i - 1, j, k) + U3(uoo, i, j + 1, k) +
+                                   U3(uoo, i - 1, j + 1, k));
+          const double v = V3(voe, i, j, k);
+          P2(speedv, i, j) = fmx(sqrt(v * v + a * a), 1.E-3);
+        }
+    for (int i = 2; i <= IE1; ++i)
+      if (V3(g->amsue, i, j, KE) > 0.5) {
+        const int k = KE;
+        const double a = 0.25 * (U3(uoo, i, j, k) + U3(uoo, i - 1, j, k) + U3(uoo, i, j + 1, k) +
+                                 U3(uoo, i - 1, j + 1, k));
+        const double v = V3(voe, i, j, k);
+        P2(speedv, i, j) = fmx(sqrt(v * v + a * a), 1.E-3);
+      }
+  }
+  /* vertical diffusion of v, ocvisc.f90:114-165 */
+#pragma omp parallel
+  {
+    double *t1 = (double *)malloc(sizeof(double) * (size_t)(KE + 1) * 3 + 8);
+    double *t2 = t1 + (KE + 1), *t3 = t2 + (KE + 1);
+    double *x1 = (double *)malloc(sizeof(double) * (size_t)(KE + 1) + 8);
+#define TR1(k) t1[(k)-1]
+#define TR2(k) t2[(k)-1]
+#define TR3(k) t3[(k)-1]
+#pragma omp for schedule(static)
+    for (int i = 2; i <= IE1; ++i)
+      for (int j = 1; j <= JE1; ++j) {
+        for (int k = 1; k <= KE - 1; ++k) {
+          const double avup = 0.5 * (P3(avo, i, j, k) + P3(avo, i, j + 1, k)) * V3(g->amsue, i, j, k);
+          const double avlo = 0.5 * (P3(avo, i, j, k + 1) + P3(avo, i, j + 1, k + 1)) *
+                                  V3(g->amsue, i, j, k + 1) +
+                              (BOFRIC + RAYFRIC * V3(g->ddue, i, j, k) * P2(speedv, i, j)) *
+                                  (V3(g->amsue, i, j, k) - V3(g->amsue, i, j, k + 1));
+          TR1(k) = -DT * avup * V3(g->amsue, i, j, k) * K1(g->di, k) / (ALMZER + V3(g->ddue, i, j, k));
+          TR3(k) = -DT * avlo * V3(g->amsue, i, j, k) * K1(g->di, k + 1) / (ALMZER + V3(g->ddue, i, j, k));
+          TR2(k) = 1. - TR1(k) - TR3(k);
+          TR3(k) = TR3(k) * V3(g->amsue, i, j, k + 1);
+        }
+        {
+          const int k = KE;
+          const double avup = 0.5 * (P3(avo, i, j, k) + P3(avo, i, j + 1, k)) * V3(g->amsue, i, j, k);
+          const double avlo = (BOFRIC + RAYFRIC * V3(g->ddue, i, j, k) * P2(speedv, i, j)) *
+                              V3(g->amsue, i, j, k);
+          TR1(k) = -DT * avup * V3(g->amsue, i, j, k) * K1(g->di, k) / (ALMZER + V3(g->ddue, i, j, k));
+          TR3(k) = -DT * avlo * V3(g->amsue, i, j, k) * K1(g->di, k + 1) / (ALMZER + V3(g->ddue, i, j, k));
+          TR2(k) = 1. - TR1(k) - TR3(k);
+          TR3(k) = 0.;
+        }
+        for (int k = 2; k <= KE; ++k) {
+          const double a = TR1(k);
+          TR1(k - 1) = a / TR2(k - 1);
+          TR2(k) = TR2(k) - TR3(k - 1) * a / TR2(k - 1);
+        }
+        for (int k = 1; k <= KE; ++k) x1[k] = V3(voe, i, j, k);
+        for (int k = 2; k <= KE; ++k) x1[k] = x1[k] - TR1(k - 1) * x1[k - 1];
+        V3(vke, i, j, KE) = V3(g->amsue, i, j, KE) * x1[KE] / TR2(KE);
+        for (int k = 1; k <= KE - 1; ++k) {
+          const int l = KE - k;
+          V3(vke, i, j, l) = (x1[l] - TR3(l) * V3(vke, i, j, l + 1)) * V3(g->amsue, i, j, l) / TR2(l);
+        }
+      }
+    /* vertical diffusion of u, ocvisc.f90:168-218 */
+#pragma omp for schedule(static)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) {
+        for (int k = 1; k <= KE - 1; ++k) {
+          const double avup = 0.5 * (P3(avo, i, j, k) + P3(avo, i + 1, j, k)) * U3(g->amsuo, i, j, k);
+          const double avlo = 0.5 * (P3(avo, i, j, k + 1) + P3(avo, i + 1, j, k + 1)) *
+                                  U3(g->amsuo, i, j, k + 1) +
+                              (BOFRIC + RAYFRIC * U3(g->dduo, i, j, k) * P2(speedu, i, j)) *
+                                  (U3(g->amsuo, i, j, k) - U3(g->amsuo, i, j, k + 1));
+          TR1(k) = -DT * avup * U3(g->amsuo, i, j, k) * K1(g->di, k) / (ALMZER + U3(g->dduo, i, j, k));
+          TR3(k) = -DT * avlo * U3(g->amsuo, i, j, k) * K1(g->di, k + 1) / (ALMZER + U3(g->dduo, i, j, k));
+          TR2(k) = 1. - TR1(k) - TR3(k);
+          TR3(k) = TR3(k) * U3(g->amsuo, i, j, k + 1);
+        }
+        {
+          const int k = KE;
+          const double avup = 0.5 * (P3(avo, i, j, k) + P3(avo, i + 1, j, k)) * U3(g->amsuo, i, j, k);
+          const double avlo = (BOFRIC + RAYFRIC * U3(g->dduo, i, j, k) * P2(speedu, i, j)) *
+                              U3(g->amsuo, i, j, k);
+          TR1(k) = -DT * avup * U3(g->amsuo, i, j, k) * K1(g->di, k) / (ALMZER + U3(g->dduo, i, j, k));
+          TR3(k) = -DT * avlo * U3(g->amsuo, i, j, k) * K1(g->di, k + 1) / (ALMZER + U3(g->dduo, i, j, k));
+          TR2(k) = 1. - TR1(k) - TR3(k);
+          TR3(k) = 0.;
+        }
+        for (int k = 2; k <= KE; ++k) {
+          const double a = TR1(k);
+          TR1(k - 1) = a / TR2(k - 1);
+          TR2(k) = TR2(k) - TR3(k - 1) * a / TR2(k - 1);
+        }
+        for (int k = 1; k <= KE; ++k) x1[k] = U3(uoo, i, j, k);
+        for (int k = 2; k <= KE; ++k) x1[k] = x1[k] - TR1(k - 1) * x1[k - 1];
+        U3(uko, i, j, KE) = U3(g->amsuo, i, j, KE) * x1[KE] / TR2(KE);
+        for (int k = 1; k <= KE - 1; ++k) {
+          const int l = KE - k;
+          U3(uko, i, j, l) = (x1[l] - TR3(l) * U3(uko, i, j, l + 1)) * U3(g->amsuo, i, j, l) / TR2(l);
+        }
+      }
+    /* vertical diffusion of w, ocvisc.f90:225-270 */
+#pragma omp for schedule(static)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        for (int k = 2; k <= KE - 1; ++k) {
+          const double avup = 0.5 * (P3(avo, i, j, k - 1) + P3(avo, i, j, k)) * P3(g->weto, i, j, k - 1);
+          const double avlo = 0.5 * (P3(avo, i, j, k + 1) + P3(avo, i, j, k)) * P3(g->weto, i, j, k);
+          const double den = 2.0 * ALMZER + P3(g->ddpo, i, j, k - 1) + P3(g->ddpo, i, j, k);
+          TR1(k) = -2.0 * DT * avup * P3(g->weto, i, j, k) * K1(g->di, k - 1) / den;
+          TR3(k) = -2.0 * DT * avlo * P3(g->weto, i, j, k) * K1(g->di, k) / den;
+          TR2(k) = 1. - TR1(k) - TR3(k);
+        }
+        {
+          const int k = KE;
+          const double avup = 0.5 * (P3(avo, i, j, k - 1) + P3(avo, i, j, k)) * P3(g->weto, i, j, k - 1);
+          const double avlo = 0.0;
+          const double den = 2.0 * ALMZER + P3(g->ddpo, i, j, k - 1) + P3(g->ddpo, i, j, k);
+          TR1(k) = -2.0 * DT * avup * P3(g->weto, i, j, k) * K1(g->di, k - 1) / den;
+          TR3(k) = -2.0 * DT * avlo * P3(g->weto, i, j, k) * K1(g->di, k) / den;
+          TR2(k) = 1. - TR1(k) - TR3(k);
+          TR3(k) = 0.;
+        }
+        for (int k = 3; k <= KE; ++k) {
+          const double a = TR1(k);
+          TR1(k - 1) = a / TR2(k - 1);
+          TR2(k) = TR2(k) - TR3(k - 1) * a / TR2(k - 1);
+        }
+        for (int k = 2; k <= KE; ++k) x1[k] = P3(wno, i, j, k);
+        for (int k = 3; k <= KE; ++k) x1[k] = x1[k] - TR1(k - 1) * x1[k - 1];
+        P3(wno, i, j, KE) = P3(g->weto, i, j, KE) * x1[KE] / TR2(KE);
+        for (int k = KE - 1; k >= 2; --k)
+          P3(wno, i, j, k) = (x1[k] - TR3(k) * P3(wno, i, j, k + 1)) * P3(g->weto, i, j, k) / TR2(k);
+      }
+#undef TR1
+#undef TR2
+#undef TR3
+    free(t1);
+    free(x1);
+  }
+  /* biharmonic coefficients, ocvisc.f90:286-340 */
+  double *dlypsi = zalloc((size_t)(IE + 1) * JE); /* U2 layout (I_start:IE, JE) */
+  double *dlxpsi = zalloc((size_t)IE * (JE + 1)); /* V2 layout (IE, J_start:JE) */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE1; ++i) U2(dlypsi, i, j) = 0.5 * (V2(g->dlyv, i, j) + V2(g->dlyv, i + 1, j));
+  for (int j = 1; j <= JE; ++j) {
+    U2(dlypsi, 0, j) = V2(g->dlyv, 1, j);
+    U2(dlypsi, IE, j) = V2(g->dlyv, IE, j);
+  }
+  for (int i = 1; i <= IE; ++i)
+    for (int j = 1; j <= JE1; ++j) V2(dlxpsi, i, j) = 0.5 * (U2(g->dlxu, i, j) + U2(g->dlxu, i, j + 1));
+  for (int i = 1; i <= IE; ++i) {
+    V2(dlxpsi, i, 0) = U2(g->dlxu, i, 1);
+    V2(dlxpsi, i, JE) = U2(g->dlxu, i, JE);
+  }
+  const size_t n2 = (size_t)IE * JE;
+  double *aulux = zalloc(n2), *auluy = zalloc(n2), *aulvx = zalloc(n2), *aulvy = zalloc(n2);
+  double *aulwx = zalloc(n2), *aulwy = zalloc(n2);
+#define POW4(x) (((x) * (x)) * ((x) * (x)))
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      double m;
+      m = fmx(P2(g->dlxp, i, j), minvalue); P2(aulux, i, j) = AULAPUV * POW4(m);
+      m = fmx(minvalue, U2(dlypsi, i, j)); P2(auluy, i, j) = AULAPUV * POW4(m);
+      m = fmx(minvalue, P2(g->dlyp, i, j)); P2(aulvy, i, j) = AULAPUV * POW4(m);
+      m = fmx(V2(dlxpsi, i, j), minvalue); P2(aulvx, i, j) = AULAPUV * POW4(m);
+      m = fmx(U2(g->dlxu, i, j), minvalue); P2(aulwx, i, j) = AULAPUV * POW4(m);
+      m = fmx(V2(g->dlyv, i, j), minvalue); P2(aulwy, i, j) = AULAPUV * POW4(m);
+    }
+#undef POW4
+  const size_t nu = (size_t)(IE + 1) * JE * KE, nv = (size_t)IE * (JE + 1) * KE, np = (size_t)IE * JE * KE;
+  double *uk1o = zalloc(nu), *vk1e = zalloc(nv), *wn1o = zalloc(np);
+  /* first Laplacian, ocvisc.f90:350-438 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+#define AO(i, j) U3(g->amsuo, i, j, k)
+#define UK(i, j) U3(uko, i, j, k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i)
+        U3(uk1o, i, j, k) = AO(i, j) *
+            ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / P2(g->dlxp, i + 1, j) -
+              AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / P2(g->dlxp, i, j)) / U2(g->dlxu, i, j) +
+             (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / U2(dlypsi, i, j - 1) -
+              AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / U2(dlypsi, i, j)) / U2(g->dlyu, i, j));
+#define AE(i, j) V3(g->amsue, i, j, k)
+#define VK(i, j) V3(vke, i, j, k)
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        V3(vk1e, i, j, k) = AE(i, j) *
+            ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / V2(dlxpsi, i, j) -
+              AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / V2(dlxpsi, i - 1, j)) / V2(g->dlxv, i, j) +
+             (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / P2(g->dlyp, i, j) -
+              AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / P2(g->dlyp, i, j + 1)) / V2(g->dlyv, i, j));
+    /* have_g_is */
+    for (int j = 2; j <= JE1; ++j) {
+      const int i = 0;
+      U3(uk1o, i, j, k) = AO(i, j) *
+          ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / P2(g->dlxp, i + 1, j)) / U2(g->dlxu, i, j) +
+           (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / U2(dlypsi, i, j - 1) -
+            AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / U2(dlypsi, i, j)) / U2(g->dlyu, i, j));
+    }
+    for (int j = 1; j <= JE1; ++j) {
+      const int i = 1;
+      V3(vk1e, i, j, k) = AE(i, j) *
+          ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / V2(dlxpsi, i, j)) / V2(g->dlxv, i, j) +
+           (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / P2(g->dlyp, i, j) -
+            AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / P2(g->dlyp, i, j + 1)) / V2(g->dlyv, i, j));
+    }
+    /* have_g_ie */
+    for (int j = 2; j <= JE1; ++j) {
+      const int i = IE;
+      U3(uk1o, i, j, k) = AO(i, j) *
+          ((-AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / P2(g->dlxp, i, j)) / U2(g->dlxu, i, j) +
+           (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / U2(dlypsi, i, j - 1) -
+            AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / U2(dlypsi, i, j)) / U2(g->dlyu, i, j));
+    }
+    for (int j = 1; j <= JE1; ++j) {
+      const int i = IE;
+      V3(vk1e, i, j, k) = AE(i, j) *
+          ((-AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / V2(dlxpsi, i - 1, j)) / V2(g->dlxv, i, j) +
+           (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / P2(g->dlyp, i, j) -
+            AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / P2(g->dlyp, i, j + 1)) / V2(g->dlyv, i, j));
+    }
+    /* have_g_js */
+    for (int i = 1; i <= IE1; ++i) {
+      const int j = 1;
+      U3(uk1o, i, j, k) = AO(i, j) *
+          ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / P2(g->dlxp, i + 1, j) -
+            AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / P2(g->dlxp, i, j)) / U2(g->dlxu, i, j) +
+           (-AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / U2(dlypsi, i, j)) / U2(g->dlyu, i, j));
+    }
+    for (int i = 2; i <= IE1; ++i) {
+      const int j = 0;
+      V3(vk1e, i, j, k) = AE(i, j) *
+          ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / V2(dlxpsi, i, j) -
+            AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / V2(dlxpsi, i - 1, j)) / V2(g->dlxv, i, j) +
+           (-AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / P2(g->dlyp, i, j + 1)) / V2(g->dlyv, i, j));
+    }
+    /* have_g_je */
+    for (int i = 1; i <= IE1; ++i) {
+      const int j = JE;
+      U3(uk1o, i, j, k) = AO(i, j) *
+          ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / P2(g->dlxp, i + 1, j) -
+            AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / P2(g->dlxp, i, j)) / U2(g->dlxu, i, j) +
+           (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / U2(dlypsi, i, j - 1)) / U2(g->dlyu, i, j));
+    }
+    for (int i = 2; i <= IE1; ++i) {
+      const int j = JE;
+      V3(vk1e, i, j, k) = AE(i, j) *
+          ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / V2(dlxpsi, i, j) -
+            AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / V2(dlxpsi, i - 1, j)) / V2(g->dlxv, i, j) +
+           (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / P2(g->dlyp, i, j)) / V2(g->dlyv, i, j));
+    }
+  }
+  /* second pass, ocvisc.f90:445-477 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+#define U1(i, j) U3(uk1o, i, j, k)
+#define V1(i, j) V3(vk1e, i, j, k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i) {
+        const double a = U2(g->dlxu, i, j) * U2(g->dlyu, i, j);
+        U3(uoo, i, j, k) = (AO(i, j) / (U2(g->dlxu, i, j) * U2(g->dlyu, i, j))) *
+            (U2(g->dlxu, i, j) * U2(g->dlyu, i, j) * UK(i, j) -
+             (P2(aulux, i + 1, j) * P2(g->dlyp, i + 1, j) * AO(i + 1, j) * (U1(i + 1, j) - U1(i, j)) / P2(g->dlxp, i + 1, j) -
+              P2(aulux, i, j) * P2(g->dlyp, i, j) * AO(i - 1, j) * (U1(i, j) - U1(i - 1, j)) / P2(g->dlxp, i, j) +
+              P2(auluy, i, j - 1) * V2(dlxpsi, i, j - 1) * AO(i, j - 1) * (U1(i, j - 1) - U1(i, j)) / U2(dlypsi, i, j - 1) -
+              P2(auluy, i, j) * V2(dlxpsi, i, j) * AO(i, j + 1) * (U1(i, j) - U1(i, j + 1)) / U2(dlypsi, i, j)));
+        (void)a;
+      }
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        V3(voe, i, j, k) = (AE(i, j) / (V2(g->dlxv, i, j) * V2(g->dlyv, i, j))) *
+            (V2(g->dlxv, i, j) * V2(g->dlyv, i, j) * VK(i, j) -
+             (P2(aulvx, i, j) * U2(dlypsi, i, j) * AE(i + 1, j) * (V1(i + 1, j) - V1(i, j)) / V2(dlxpsi, i, j) -
+              P2(aulvx, i - 1, j) * U2(dlypsi, i - 1, j) * AE(i - 1, j) * (V1(i, j) - V1(i - 1, j)) / V2(dlxpsi, i - 1, j) +
+              P2(aulvy, i, j) * P2(g->dlxp, i, j) * AE(i, j - 1) * (V1(i, j - 1) - V1(i, j)) / P2(g->dlyp, i, j) -
+              P2(aulvy, i, j + 1) * P2(g->dlxp, i, j + 1) * AE(i, j + 1) * (V1(i, j) - V1(i, j + 1)) / P2(g->dlyp, i, j + 1)));
+#undef U1
+#undef V1
+  }
+#undef AO
+#undef UK
+#undef AE
+#undef VK
+  /* w biharmonic, ocvisc.f90:617-688 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+#define WE(i, j) P3(g->weto, i, j, k)
+#define WN(i, j) P3(wno, i, j, k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        P3(wn1o, i, j, k) = WE(i, j) *
+            ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / U2(g->dlxu, i, j) -
+              WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / U2(g->dlxu, i - 1, j)) / P2(g->dlxp, i, j) +
+             (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / V2(g->dlyv, i, j - 1) -
+              WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / V2(g->dlyv, i, j)) / P2(g->dlyp, i, j));
+    for (int j = 2; j <= JE1; ++j) {
+      const int i = 1;
+      P3(wn1o, i, j, k) = WE(i, j) *
+          ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / U2(g->dlxu, i, j)) / P2(g->dlxp, i, j) +
+           (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / V2(g->dlyv, i, j - 1) -
+            WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / V2(g->dlyv, i, j)) / P2(g->dlyp, i, j));
+    }
+    for (int j = 2; j <= JE1; ++j) {
+      const int i = IE;
+      P3(wn1o, i, j, k) = WE(i, j) *
+          ((-WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / U2(g->dlxu, i - 1, j)) / P2(g->dlxp, i, j) +
+           (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / V2(g->dlyv, i, j - 1) -
+            WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / V2(g->dlyv, i, j)) / P2(g->dlyp, i, j));
+    }
+    for (int i = 2; i <= IE1; ++i) {
+      const int j = 1;
+      P3(wn1o, i, j, k) = WE(i, j) *
+          ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / U2(g->dlxu, i, j) -
+            WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / U2(g->dlxu, i - 1, j)) / P2(g->dlxp, i, j) +
+           (-WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / V2(g->dlyv, i, j)) / P2(g->dlyp, i, j));
+    }
+    for (int i = 2; i <= IE1; ++i) {
+      const int j = JE;
+      P3(wn1o, i, j, k) = WE(i, j) *
+          ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / U2(g->dlxu, i, j) -
+            WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / U2(g->dlxu, i - 1, j)) / P2(g->dlxp, i, j) +
+           (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / V2(g->dlyv, i, j - 1)) / P2(g->dlyp, i, j));
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+#define W1(i, j) P3(wn1o, i, j, k)
+#define DZU(i, j) fmx(U3(g->dduo, i, j, k), minvalue)
+#define DZV(i, j) fmx(V3(g->ddue, i, j, k), minvalue)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double dzp = fmx(P3(g->ddpo, i, j, k), minvalue);
+        P3(wno, i, j, k) = (WE(i, j) / (P2(g->dlxp, i, j) * P2(g->dlyp, i, j) * dzp)) *
+            (P2(g->dlxp, i, j) * P2(g->dlyp, i, j) * dzp * WN(i, j) -
+             (+P2(aulwx, i, j) * U2(g->dlyu, i, j) * DZU(i, j) * WE(i + 1, j) * (W1(i + 1, j) - W1(i, j)) / U2(g->dlxu, i, j) -
+              P2(aulwx, i - 1, j) * U2(g->dlyu, i - 1, j) * DZU(i - 1, j) * WE(i - 1, j) * (W1(i, j) - W1(i - 1, j)) / U2(g->dlxu, i - 1, j) +
+              P2(aulwy, i, j - 1) * V2(g->dlxv, i, j - 1) * DZV(i, j - 1) * WE(i, j - 1) * (W1(i, j - 1) - W1(i, j)) / V2(g->dlyv, i, j - 1) -
+              P2(aulwy, i, j) * V2(g->dlxv, i, j) * DZV(i, j) * WE(i, j + 1) * (W1(i, j) - W1(i, j + 1)) / V2(g->dlyv, i, j)));
+      }
+#undef W1
+#undef DZU
+#undef DZV
+#undef WE
+#undef WN
+  }
+  og_octimf(g, uoo, voe, uko, vke);
+  free(speedu); free(speedv); free(dlypsi); free(dlxpsi);
+  free(aulux); free(auluy); free(aulvx); free(aulvy); free(aulwx); free(aulwy);
+  free(uk1o); free(vk1e); free(wn1o);
+}
+
+void og_octimf(const og_grid *g, const double *uoo, const double *voe, double *uko,
+               double *vke) {
+  DIMS;
+  memcpy(uko, uoo, sizeof(double) * (size_t)(IE + 1) * JE * KE);
+  memcpy(vke, voe, sizeof(double) * (size_t)IE * (JE + 1) * KE);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCVTOT_NH right-hand side: ocvtot_nh.f90:11-62 and ComputeRHS            */
+/* (mo_petsc.f90:298-376, CG2D4NONHY off: rhs = DIVG*WETO).                 */
+/* ------------------------------------------------------------------------ */
+void og_nh_rhs(const og_grid *g, const double *uoo, const double *uoo1,
+               const double *voe, const double *voe1, const double *wno,
+               const double *wno1, const double *zo, double *b) {
+  DIMS;
+  const double DT = g->dt;
+  const int nx = IE - 2, ny = JE - 2;
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        const double gu0 = (U3(uoo, i, j, k) - U3(uoo1, i, j, k)) / DT;
+        const double gum = (U3(uoo, i - 1, j, k) - U3(uoo1, i - 1, j, k)) / DT;
+        const double divgu = (gu0 - gum) / P2(g->dlxp, i, j);
+        const double gvm = (V3(voe, i, j - 1, k) - V3(voe1, i, j - 1, k)) / DT;
+        const double gv0 = (V3(voe, i, j, k) - V3(voe1, i, j, k)) / DT;
+        const double divgv = (gvm - gv0) / P2(g->dlyp, i, j);
+        const double gw0 = (P3(wno, i, j, k) - P3(wno1, i, j, k)) / DT;
+        const double gw1 = (P3(wno, i, j, k + 1) - P3(wno1, i, j, k + 1)) / DT;
+        double divgw;
+        if (k >= 2)
+          divgw = (gw0 - gw1) / fmx(P3(g->ddpo, i, j, k), 1.E-3);
+        else
+          divgw = (gw0 - gw1) / (fmx(P3(g->ddpo, i, j, 1), 1.E-3) + P2(zo, i, j));
+        const double divg = divgu + divgv + divgw;
+        b[(size_t)(i - 2) + (size_t)nx * ((size_t)(j - 2) + (size_t)ny * (size_t)(k - 1))] =
+            divg * P3(g->weto, i, j, k);
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* compute_matrix (mo_petsc.f90:543-782), single rank (xs = ys = zs = 0),   */
+/* CYCLICWE/CYCLICNS off, Neumann = .FALSE.                                */
+/* ------------------------------------------------------------------------ */
+typedef struct { double zw[2]; double zp; } og_zz;
+
+/* ZW(K) for the matrix copy, mo_petsc.f90:557-583 */
+static double og_zw(const og_grid *g, int i, int j, int k) {
+  DIMS;
+  double dd;
+  if (k == 1) {
+    dd = P3(g->ddpo, i, j, 1) == 0 ? K1(g->dzw, 1) / 2.0 : P3(g->ddpo, i, j, 1) / 2.0;
+  } else if (k == KEP) {
+    dd = P3(g->ddpo, i, j, KE) == 0 ? K1(g->dzw, KE) : P3(g->ddpo, i, j, KE);
+  } else {
+    if (P3(g->ddpo, i, j, k - 1) == 0)
+      dd = (K1(g->dzw, k) + K1(g->dzw, k - 1)) / 2.0;
+    else if (P3(g->ddpo, i, j, k) == 0)
+      dd = P3(g->ddpo, i, j, k - 1);
+    else
+      dd = (P3(g->ddpo, i, j, k - 1) + P3(g->ddpo, i, j, k)) / 2.0;
+  }
+  return 1.0 / dd;
+}
+
+typedef struct { int col[7]; double val[7]; int n; } og_row;
+
+static void og_matrix_row(const og_grid *g, int i, int j, int k, og_row *r) {
+  DIMS;
+  const int nx = IE - 2, ny = JE - 2;
+  const long row = (long)(i - 2) + (long)nx * ((long)(j - 2) + (long)ny * (long)(k - 1));
+  const double xu_w = 1.0 / U2(g->dlxu, i - 1, j), xu_e = 1.0 / U2(g->dlxu, i, j);
+  const double xp = 1.0 / P2(g->dlxp, i, j);
+  const double yv_n = 1.0 / V2(g->dlyv, i, j - 1), yv_s = 1.0 / V2(g->dlyv, i, j);
+  const double yp = 1.0 / P2(g->dlyp, i, j);
+  const double zw0 = og_zw(g, i, j, k), zw1 = og_zw(g, i, j, k + 1);
+  const double zp = 1.0 / ((1.0 / zw0 + 1.0 / zw1) / 2.0);
+  double X_W = xu_w * xp, X_C = (xu_w + xu_e) * xp, X_E = xu_e * xp;
+  double Y_N = yv_n * yp, Y_C = (yv_n + yv_s) * yp, Y_S = yv_s * yp;
+  double Z_U = zw0 * zp, Z_C = (zw0 + zw1) * zp, Z_D = zw1 * zp;
+  r->n = 0;
+#define WET(ii, jj, kk) P3(g->weto, ii, jj, kk)
+  if (WET(i, j, k) == 0) {
+    r->col[0] = (int)row;
+    r->val[0] = -(X_C + Y_C + Z_C);
+    r->n = 1;
+    return;
+  }
+  if (WET(i - 1, j, k) == 0 && WET(i + 1, j, k) == 1) {
+    X_W = 0.0; X_C = xu_e * xp;
+  } else if (WET(i - 1, j, k) == 1 && WET(i + 1, j, k) == 0) {
+    X_E = 0.0; X_C = xu_w * xp;
+  } else if (WET(i - 1, j, k) == 0 && WET(i + 1, j, k) == 0) {
+    X_W = 0.0; X_E = 0.0; X_C = 0.0;
+  }
+  if (WET(i, j - 1, k) == 0 && WET(i, j + 1, k) == 1) {
+    Y_N = 0.0; Y_C = yv_s * yp;
+  } else if (WET(i, j - 1, k) == 1 && WET(i, j + 1, k) == 0) {
+    Y_S = 0.0; Y_C = yv_n * yp;
+  } else if (WET(i, j - 1, k) == 0 && WET(i, j + 1, k) == 0) {
+    Y_N = 0.0; Y_S = 0.0; Y_C = 0.0;
+  }
+  if (k == 1) {
+    Z_U = 0.0;
+  } else if (k == KE) {
+    Z_D = 0.0; Z_C = zw0 * zp;
+  } else if (WET(i, j, k + 1) == 0) {
+    Z_D = 0.0; Z_C = zw0 * zp;
+  }
+  if (g->ob_west && i == 2) X_W = 0.0;
+  if (g->ob_east && i == IE1) X_E = 0.0;
+  if (g->ob_north && j == 2) Y_N = 0.0;
+  if (g->ob_south && j == JE1) Y_S = 0.0;
+  /* entries in increasing column order: up, north, west, centre, east, south, down */
+  if (k != 1) { r->col[r->n] = (int)(row - (long)nx * ny); r->val[r->n++] = Z_U; }
+  if (WET(i, j - 1, k) == 1 && j - 2 != 0) { r->col[r->n] = (int)(row - nx); r->val[r->n++] = Y_N; }
+  if (WET(i - 1, j, k) == 1 && i - 2 != 0) { r->col[r->n] = (int)(row - 1); r->val[r->n++] = X_W; }
+  r->col[r->n] = (int)row; r->val[r->n++] = -(X_C + Y_C + Z_C);
+  if (WET(i + 1, j, k) == 1 && i - 2 != nx - 1) { r->col[r->n] = (int)(row + 1); r->val[r->n++] = X_E; }
+  if (WET(i, j + 1, k) == 1 && j - 2 != ny - 1) { r->col[r->n] = (int)(row + nx); r->val[r->n++] = Y_S; }
+  if (k != KE && WET(i, j, k + 1) == 1) { r->col[r->n] = (int)(row + (long)nx * ny); r->val[r->n++] = Z_D; }
+#undef WET
+}
+
+size_t og_matrix_nnz(const og_grid *g) {
+  DIMS;
+  size_t nnz = 0;
+  og_row r;
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        og_matrix_row(g, i, j, k, &r);
+        nnz += (size_t)r.n;
+      }
+  return nnz;
+}
+
+void og_matrix_csr(const og_grid *g, int *rowptr, int *colind, double *val) {
+  DIMS;
+  size_t p = 0, row = 0;
+  og_row r;
+  rowptr[0] = 0;
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i) {
+        og_matrix_row(g, i, j, k, &r);
+        for (int e = 0; e < r.n; ++e) { colind[p] = r.col[e]; val[p] = r.val[e]; ++p; }
+        rowptr[++row] = (int)p;
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCVTOT_NH after the solve: ocvtot_nh.f90:150-255, petsc_solve_3D         */
+/* (mo_petsc.f90:222-229).                                                  */
+/* ------------------------------------------------------------------------ */
+void og_nh_post(const og_grid *g, const double *x, double *pnh, double *uoo,
+                double *voe, double *wno, double *uoo1, double *voe1,
+                double *wno1, double *wo) {
+  DIMS;
+  const double DT = g->dt, DTI = 1. / DT;
+  const int nx = IE - 2, ny = JE - 2;
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        P3(pnh, i, j, k) = x[(size_t)(i - 2) + (size_t)nx * ((size_t)(j - 2) + (size_t)ny * (size_t)(k - 1))];
+  if (g->ob_west)
+    for (int j = 2; j <= JE1; ++j)
+      for (int k = 1; k <= KE; ++k) P3(pnh, 1, j, k) = P3(pnh, 2, j, k);
+  if (g->ob_east)
+    for (int j = 2; j <= JE1; ++j)
+      for (int k = 1; k <= KE; ++k) P3(pnh, IE, j, k) = P3(pnh, IE1, j, k);
+  if (g->ob_north)
+    for (int i = 1; i <= IE; ++i)
+      for (int k = 1; k <= KE; ++k) P3(pnh, i, 1, k) = P3(pnh, i, 2, k);
+  if (g->ob_south)
+    for (int i = 1; i <= IE; ++i)
+      for (int k = 1; k <= KE; ++k) P3(pnh, i, JE, k) = P3(pnh, i, JE1, k);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 2; j <= JE1; ++j)
+      for (int i = 1; i <= IE1; ++i)
+        U3(uoo, i, j, k) = U3(uoo, i, j, k) + U3(g->amsuo, i, j, k) * U2(g->dtdxuo, i, j) *
+                                                  (P3(pnh, i, j, k) - P3(pnh, i + 1, j, k));
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 2; i <= IE1; ++i)
+        V3(voe, i, j, k) = V3(voe, i, j, k) + V3(g->amsue, i, j, k) * V2(g->dpye, i, j) *
+                                                  (P3(pnh, i, j + 1, k) - P3(pnh, i, j, k));
+  }
+  memset(wno, 0, sizeof(double) * (size_t)IE * JE * KEP);
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= JE; ++j)
+    for (int k = KE; k >= 1; --k)
+      for (int i = 1; i <= IE; ++i)
+        P3(wno, i, j, k) =
+            P3(wno, i, j, k + 1) +
+            DTI * P3(g->weto, i, j, k) *
+                (P2(g->dtdxpo, i, j) *
+                 (U3(uoo, i - 1, j, k) * U3(g->dduo, i - 1, j, k) * U2(g->dlyu, i - 1, j) -
+                  U3(uoo, i, j, k) * U3(g->dduo, i, j, k) * U2(g->dlyu, i, j)) /
+                 P2(g->dlyp, i, j)) +
+            DTI * P3(g->weto, i, j, k) *
+                (+P2(g->dtdyo, i, j) *
+                 (V3(voe, i, j, k) * V3(g->ddue, i, j, k) * V2(g->dlxv, i, j) -
+                  V3(voe, i, j - 1, k) * V3(g->ddue, i, j - 1, k) * V2(g->dlxv, i, j - 1)) /
+                 P2(g->dlxp, i, j));
+  memcpy(uoo1, uoo, sizeof(double) * (size_t)(IE + 1) * JE * KE);
+  memcpy(voe1, voe, sizeof(double) * (size_t)IE * (JE + 1) * KE);
+  memcpy(wno1, wno, sizeof(double) * (size_t)IE * JE * KEP);
+  memcpy(wo, wno, sizeof(double) * (size_t)IE * JE * KEP);
+}
+
+/* ------------------------------------------------------------------------ */
+/* CPU Krylov solve: right-preconditioned FGMRES(30) with a column          */
+/* tridiagonal (line Jacobi in z) preconditioner.  Stands in for PETSc's    */
+/* -ksp_type fgmres -pc_type mg -pc_mg_levels 1 (whose single level is a    */
+/* direct solve); the operator and right-hand side are the reference's.     */
+/* ------------------------------------------------------------------------ */
+typedef struct { int nx, ny, nz; double *a, *d, *c; } og_linepc;
+
+static void og_pc_setup(const og_grid *g, const int *rp, const int *ci, const double *v,
+                        og_linepc *pc) {
+  DIMS;
+  pc->nx = IE - 2; pc->ny = JE - 2; pc->nz = KE;
+  const size_t n = (size_t)pc->nx * pc->ny * pc->nz, plane = (size_t)pc->nx * pc->ny;
+  pc->a = zalloc(n); pc->d = zalloc(n); pc->c = zalloc(n);
+#pragma omp parallel for schedule(static)
+  for (long r = 0; r < (long)n; ++r)
+    for (int e = rp[r]; e < rp[r + 1]; ++e) {
+      const long cc = ci[e];
+      if (cc == r) pc->d[r] = v[e];
+      else if (cc == r - (long)plane) pc->a[r] = v[e];
+      else if (cc == r + (long)plane) pc->c[r] = v[e];
+    }
+}
+
+static void og_pc_apply(const og_linepc *pc, const double *r, double *z) {
+  const size_t plane = (size_t)pc->nx * pc->ny;
+#pragma omp parallel
+  {
+    double *cp = (double *)malloc(sizeof(double) * (size_t)pc->nz + 8);
+#pragma omp for schedule(static)
+    for (long q = 0; q < (long)plane; ++q) {
+      /* Thomas algorithm down the column */
+      double den = pc->d[q];
+      cp[0] = pc->c[q] / den;
+      z[q] = r[q] / den;
+      for (int k = 1; k < pc->nz; ++k) {
+        const size_t ix = (size_t)q + plane * (size_t)k;
+        den = pc->d[ix] - pc->a[ix] * cp[k - 1];
+        cp[k] = pc->c[ix] / den;
+        z[ix] = (r[ix] - pc->a[ix] * z[ix - plane]) / den;
+      }
+      for (int k = pc->nz - 2; k >= 0; --k) {
+        const size_t ix = (size_t)q + plane * (size_t)k;
+        z[ix] = z[ix] - cp[k] * z[ix + plane];
+      }
+    }
+    free(cp);
+  }
+}
+
+static void og_spmv(long n, const int *rp, const int *ci, const double *v, const double *x,
+                    double *y) {
+#pragma omp parallel for schedule(static)
+  for (long r = 0; r < n; ++r) {
+    double s = 0.0;
+    for (int e = rp[r]; e < rp[r + 1]; ++e) s += v[e] * x[ci[e]];
+    y[r] = s;
+  }
+}
+
+static double og_dot(long n, const double *a, const double *b) {
+  double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+  for (long i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+int og_solve(const og_grid *g, const int *rp, const int *ci, const double *val,
+             const double *b, double *x, double rtol, int maxit, double *relres) {
+  DIMS;
+  const long n = (long)(IE - 2) * (JE - 2) * KE;
+  const int m = 30;
+  og_linepc pc;
+  og_pc_setup(g, rp, ci, val, &pc);
+  double *V = zalloc((size_t)n * (m + 1)), *Z = zalloc((size_t)n * m);
+  double *H = zalloc((size_t)(m + 1) * m), *cs = zalloc(m), *sn = zalloc(m), *s = zalloc(m + 1);
+  double *r = zalloc(n), *w = zalloc(n);
+  const double bnorm = sqrt(og_dot(n, b, b));
+  int it = 0, converged = 0;
+  double rel = 0.0;
+  if (bnorm == 0.0) {
+    memset(x, 0, sizeof(double) * (size_t)n);
+    converged = 1;
+  }
+  while (!converged && it < maxit) {
+    og_spmv(n, rp, ci, val, x, r);
+    for (long i = 0; i < n; ++i) r[i] = b[i] - r[i];
+    double beta = sqrt(og_dot(n, r, r));
+    rel = beta / bnorm;
+    if (rel <= rtol) { converged = 1; break; }
+    for (long i = 0; i < n; ++i) V[i] = r[i] / beta;
+    memset(s, 0, sizeof(double) * (m + 1));
+    s[0] = beta;
+    int j;
+    for (j = 0; j < m && it < maxit; ++j, ++it) {
+      og_pc_apply(&pc, V + (size_t)n * j, Z + (size_t)n * j);
+      og_spmv(n, rp, ci, val, Z + (size_t)n * j, w);
+      for (int q = 0; q <= j; ++q) { /* modified Gram-Schmidt */
+        const double h = og_dot(n, w, V + (size_t)n * q);
+        H[q * m + j] = h;
+        const double *vq = V + (size_t)n * q;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; ++i) w[i] -= h * vq[i];
+      }
+      const double hn = sqrt(og_dot(n, w, w));
+      H[(j + 1) * m + j] = hn;
+      if (hn != 0.0)
+        for (long i = 0; i < n; ++i) V[(size_t)n * (j + 1) + i] = w[i] / hn;
+      for (int q = 0; q < j; ++q) {
+        const double t = cs[q] * H[q * m + j] + sn[q] * H[(q + 1) * m + j];
+        H[(q + 1) * m + j] = -sn[q] * H[q * m + j] + cs[q] * H[(q + 1) * m + j];
+        H[q * m + j] = t;
+      }
+      const double den = sqrt(H[j * m + j] * H[j * m + j] + hn * hn);
+      cs[j] = H[j * m + j] / den;
+      sn[j] = hn / den;
+      H[j * m + j] = den;
+      H[(j + 1) * m + j] = 0.0;
+      s[j + 1] = -sn[j] * s[j];
+      s[j] = cs[j] * s[j];
+      if (fabs(s[j + 1]) / bnorm <= rtol * 0.5) { ++j; ++it; break; }
+    }
+    /* back substitution and x += Z y */
+    double *y = zalloc(m);
+    for (int q = j - 1; q >= 0; --q) {
+      double t = s[q];
+      for (int p = q + 1; p < j; ++p) t -= H[q * m + p] * y[p];
+      y[q] = t / H[q * m + q];
+    }
+    for (int q = 0; q < j; ++q) {
+      const double *zq = Z + (size_t)n * q;
+      const double yq = y[q];
+#pragma omp parallel for schedule(static)
+      for (long i = 0; i < n; ++i) x[i] += yq * zq[i];
+    }
+    free(y);
+  }
+  if (!converged) {
+    og_spmv(n, rp, ci, val, x, r);
+    for (long i = 0; i < n; ++i) r[i] = b[i] - r[i];
+    rel = bnorm == 0.0 ? 0.0 : sqrt(og_dot(n, r, r)) / bnorm;
+    converged = rel <= rtol;
+  }
+  if (relres) *relres = rel;
+  free(V); free(Z); free(H); free(cs); free(sn); free(s); free(r); free(w);
+  free(pc.a); free(pc.d); free(pc.c);
+  return converged ? it : -it - 1;
+}

@@ -1,0 +1,103 @@
+/*
+ * CPU restatement (oracle) of ORCTM's nonhydrostatic hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: this library is the checker that the CUDA path is
+ * compared against, and the CPU baseline that bench.py times.  Nothing in the
+ * product (orctm_b200/, include/) links or calls it.
+ *
+ * PARITY UNPINNED: the reference (Fortran 90 + PETSc 3.10.2 + MPI) cannot be
+ * compiled here and ships no golden outputs or tests, so this restatement is
+ * checked only against itself (golden fixtures it generated, an independent
+ * numpy restatement of selected routines, and property tests).
+ *
+ * Arrays use the reference's Fortran layout (column-major, i fastest) with its
+ * halos and index origins on a single-rank domain (I_start = J_start = 0):
+ *   p-points  X(1:IE, 1:JE, 1:KE)      u-points X(0:IE, 1:JE, 1:KE)
+ *   v-points  X(1:IE, 0:JE, 1:KE)      w-points X(1:IE, 1:JE, 1:KE+1)
+ *   2D arrays analogous (p: IE*JE, u: (IE+1)*JE, v: IE*(JE+1)).
+ * All arithmetic is IEEE binary64, evaluated in the textual (left-to-right)
+ * order of the Fortran source; compile with -ffp-contract=off.
+ */
+#ifndef ORCTM_ORACLE_H
+#define ORCTM_ORACLE_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct og_grid {
+  int ie, je, ke;              /* IE, JE, KE including the 1-cell halo */
+  int ob_west, ob_east, ob_north, ob_south; /* open-boundary switches (mo_obcs.f90:9-20) */
+  double dt, almzer, aulapts, aulapuv, ah00;
+  /* 1D vertical grid, 1-based in the comments: DZW(KE), DI(KEP), DZ(KEP), TIESTU(KEP), TIESTW(KEP) */
+  const double *dzw, *di, *dz, *tiestu, *tiestw;
+  /* 2D metrics */
+  const double *dlxp, *dlyp, *dtdxpo, *dtdyo;        /* p: IE*JE */
+  const double *dlxu, *dlyu, *dtdxuo, *dpyo;         /* u: (IE+1)*JE */
+  const double *dlxv, *dlyv, *dtdxue, *dpye;         /* v: IE*(JE+1) */
+  /* 3D geometry (BODEN) */
+  const double *ddpo, *weto;                         /* p: IE*JE*KE */
+  const double *dduo, *amsuo;                        /* u: (IE+1)*JE*KE */
+  const double *ddue, *amsue;                        /* v: IE*(JE+1)*KE */
+} og_grid;
+
+/* BELEG (beleg.f90:48-139) + BODEN (boden.f90:38-286) restated.  depto is
+ * modified in place exactly as BODEN does (ISTART == 0 branch).  Outputs are
+ * caller-allocated in the layouts above; tiestu/tiestw/dz/di have KE+1
+ * entries, dwi KE. */
+void og_build_grid(int ie, int je, int ke, double dt, const double *dzw,
+                   double *depto,
+                   const double *dlxp, const double *dlyp,
+                   const double *dlxu, const double *dlyu,
+                   const double *dlxv, const double *dlyv,
+                   double *tiestu, double *tiestw, double *dz, double *di,
+                   double *dtdxpo, double *dtdyo, double *dtdxuo, double *dpyo,
+                   double *dtdxue, double *dpye,
+                   double *ddpo, double *weto, double *dduo, double *amsuo,
+                   double *ddue, double *amsue);
+
+/* Hot-path routines (in/out arrays in reference layout). */
+void og_ocadpo(const og_grid *g, double *trf, const double *uko, const double *vke,
+               const double *wo, const double *zo);
+void og_ocuad(const og_grid *g, double *uoo, const double *uko, const double *vke,
+              const double *wo);
+void og_ocvad(const og_grid *g, double *voe, const double *uko, const double *vke,
+              const double *wo);
+void og_ocwad(const og_grid *g, double *wno, const double *uko, const double *vke,
+              const double *wo, const double *zo);
+void og_octdiff(const og_grid *g, int ntr, double *const *tr, const double *dvo,
+                const double *zo);
+void og_ocvisc(const og_grid *g, double *uoo, double *voe, double *wno,
+               double *uko, double *vke, const double *avo);
+
+/* OCVTOT_NH, split around the solve.  b has (IE-2)*(JE-2)*KE entries in PETSc
+ * DMDA natural order (x fastest). */
+void og_nh_rhs(const og_grid *g, const double *uoo, const double *uoo1,
+               const double *voe, const double *voe1, const double *wno,
+               const double *wno1, const double *zo, double *b);
+/* Number of stored entries of the compute_matrix operator. */
+size_t og_matrix_nnz(const og_grid *g);
+/* compute_matrix (mo_petsc.f90:543-782) as CSR over the DMDA natural order. */
+void og_matrix_csr(const og_grid *g, int *rowptr, int *colind, double *val);
+/* Writes the solve's x into PNH interior, fills the open-boundary halo,
+ * corrects u/v, re-diagnoses WNO and rotates the _1 copies (ocvtot_nh.f90:150-255). */
+void og_nh_post(const og_grid *g, const double *x, double *pnh, double *uoo,
+                double *voe, double *wno, double *uoo1, double *voe1,
+                double *wno1, double *wo);
+
+/* CPU Krylov solve of the assembled operator: right-preconditioned restarted
+ * FGMRES with the column (line) tridiagonal preconditioner.  x holds the
+ * initial guess on entry.  Returns the iteration count (negative if not
+ * converged); *relres = ||b - A x||_2 / ||b||_2 on exit. */
+int og_solve(const og_grid *g, const int *rowptr, const int *colind,
+             const double *val, const double *b, double *x, double rtol,
+             int maxit, double *relres);
+
+/* Applies OCTIMF (octimf.f90:1-22): uko <- uoo, vke <- voe. */
+void og_octimf(const og_grid *g, const double *uoo, const double *voe,
+               double *uko, double *vke);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,110 @@
+"""ctypes binding of liborctm_gpu.so (the C ABI declared in include/orctm_gpu.h).
+
+The shared library is built in-tree (orctm_b200/build.py).  There is no
+fallback: if the library is missing or cannot be loaded, load() raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(_HERE, "liborctm_gpu.so")
+_D = C.POINTER(C.c_double)
+
+ORCTM_OK = 0
+ORCTM_E_NOT_CONVERGED = -4
+
+F_UOO, F_VOE, F_WNO, F_UKO, F_VKE, F_WO, F_UOO_1, F_VOE_1, F_WNO_1, F_PNH, F_ZO, F_DVO, F_AVO, \
+    F_THO, F_SAO = range(15)
+SOLVER_FP64, SOLVER_FP32_REFINED = 0, 1
+
+
+class Desc(C.Structure):
+    _fields_ = [
+        ("ie", C.c_int), ("je", C.c_int), ("ke", C.c_int),
+        ("i_start", C.c_int), ("j_start", C.c_int), ("ntracers", C.c_int),
+        ("ob_west", C.c_int), ("ob_east", C.c_int), ("ob_north", C.c_int), ("ob_south", C.c_int),
+        ("dt", C.c_double), ("almzer", C.c_double), ("aulapts", C.c_double),
+        ("aulapuv", C.c_double), ("ah00", C.c_double),
+        ("dzw", _D), ("di", _D),
+        ("dlxp", _D), ("dlyp", _D), ("dtdxpo", _D), ("dtdyo", _D),
+        ("dlxu", _D), ("dlyu", _D), ("dtdxuo", _D),
+        ("dlxv", _D), ("dlyv", _D), ("dpye", _D),
+        ("ddpo", _D), ("weto", _D), ("dduo", _D), ("amsuo", _D), ("ddue", _D), ("amsue", _D),
+        ("device", C.c_int),
+    ]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("outer_iterations", C.c_int), ("converged", C.c_int),
+                ("relres", C.c_double), ("relres_initial", C.c_double), ("solve_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+EXPORTS = (
+    "orctm_abi_version", "orctm_status_string", "orctm_last_error", "orctm_create",
+    "orctm_destroy", "orctm_field_size", "orctm_upload", "orctm_download", "orctm_ocuad",
+    "orctm_ocvad", "orctm_ocwad", "orctm_ocadpo", "orctm_octdiff", "orctm_octimf",
+    "orctm_ocvisc", "orctm_ocvtot_nh", "orctm_step_hotpath", "orctm_set_solver",
+    "orctm_synchronize", "orctm_build_grid", "orctm_timer_start", "orctm_timer_stop",
+    "orctm_set_profiling", "orctm_profile_get", "orctm_kernel_launches",
+)
+
+PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
+              "pcg_col", "resid", "nh_post")
+
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    """Loads the CUDA library (building it with nvcc first if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(SO):
+        if not build_if_missing:
+            raise RuntimeError(f"{SO} is missing; run orctm_b200/build.py")
+        from . import build as _build
+
+        _build.build()
+    lib = C.CDLL(SO)
+    lib.orctm_status_string.restype = C.c_char_p
+    lib.orctm_last_error.restype = C.c_char_p
+    lib.orctm_last_error.argtypes = [C.c_void_p]
+    lib.orctm_create.argtypes = [C.POINTER(Desc), C.POINTER(C.c_void_p)]
+    for name in ("orctm_destroy", "orctm_ocuad", "orctm_ocvad", "orctm_ocwad", "orctm_octdiff",
+                 "orctm_octimf", "orctm_ocvisc", "orctm_synchronize"):
+        getattr(lib, name).argtypes = [C.c_void_p]
+    lib.orctm_ocadpo.argtypes = [C.c_void_p, C.c_int]
+    lib.orctm_ocvtot_nh.argtypes = [C.c_void_p, C.POINTER(SolveStats)]
+    lib.orctm_step_hotpath.argtypes = [C.c_void_p, C.POINTER(SolveStats)]
+    lib.orctm_set_solver.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
+    lib.orctm_field_size.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)]
+    lib.orctm_upload.argtypes = [C.c_void_p, C.c_int, _D, C.c_size_t]
+    lib.orctm_download.argtypes = [C.c_void_p, C.c_int, _D, C.c_size_t]
+    lib.orctm_timer_start.argtypes = [C.c_void_p]
+    lib.orctm_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.orctm_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    lib.orctm_profile_get.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
+                                      C.POINTER(C.c_double)]
+    lib.orctm_kernel_launches.restype = C.c_ulonglong
+    lib.orctm_kernel_launches.argtypes = []
+    _lib = lib
+    return lib
+
+
+class OrctmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"ORCTM status {status}: {msg}")
+        self.status = status
+
+
+def check(status: int, handle=None, allow=()):
+    if status == ORCTM_OK or status in allow:
+        return status
+    lib = load()
+    detail = lib.orctm_last_error(handle).decode()
+    raise OrctmError(status, f"{lib.orctm_status_string(status).decode()} {detail}".strip())

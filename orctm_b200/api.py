@@ -1,0 +1,178 @@
+"""Host-side mirror of the reference's hot-path interface.
+
+``Instance`` owns one device-resident regional domain and exposes the
+reference's subroutine names (OCUAD, OCVAD, OCWAD, OCADPO, OCTDIFF_BASE +
+OCTDIFF_TS, OCTIMF, OCVISC, OCVTOT_NH) as methods that call the C ABI of
+liborctm_gpu.so.  Arrays are numpy float64 in the reference's Fortran layouts
+(see orctm_b200.configs).  Every call goes to the CUDA library; there is no
+host fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (F_AVO, F_DVO, F_PNH, F_THO, F_UKO, F_UOO, F_UOO_1, F_VKE, F_VOE, F_VOE_1,
+                   F_WNO, F_WNO_1, F_WO, F_ZO, SOLVER_FP32_REFINED, SOLVER_FP64, SolveStats)
+
+_D = C.POINTER(C.c_double)
+
+FIELDS = {"uoo": F_UOO, "voe": F_VOE, "wno": F_WNO, "uko": F_UKO, "vke": F_VKE, "wo": F_WO,
+          "uoo1": F_UOO_1, "voe1": F_VOE_1, "wno1": F_WNO_1, "pnh": F_PNH, "zo": F_ZO,
+          "dvo": F_DVO, "avo": F_AVO}
+SHAPES = {"uoo": "u", "voe": "v", "wno": "w", "uko": "u", "vke": "v", "wo": "w", "uoo1": "u",
+          "voe1": "v", "wno1": "w", "pnh": "p", "zo": "2", "dvo": "w", "avo": "w"}
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+class Instance:
+    """One regional domain resident on a GPU (an orctm_handle)."""
+
+    def __init__(self, inst: dict, device: int = 0):
+        self.lib = _lib.load()
+        self.ie, self.je, self.ke = inst["ie"], inst["je"], inst["ke"]
+        self.ntr = int(inst.get("ntracers", len(inst.get("tracers", [])) or 2))
+        self._keep = []
+        d = _lib.Desc()
+        d.ie, d.je, d.ke = self.ie, self.je, self.ke
+        d.i_start = d.j_start = 0
+        d.ntracers = self.ntr
+        ob = inst["ob"]
+        d.ob_west, d.ob_east, d.ob_north, d.ob_south = (int(ob[k]) for k in
+                                                        ("west", "east", "north", "south"))
+        d.dt, d.almzer, d.aulapts, d.aulapuv, d.ah00 = (inst["dt"], inst["almzer"], inst["aulapts"],
+                                                        inst["aulapuv"], inst["ah00"])
+        for k in ("dzw", "di", "dlxp", "dlyp", "dtdxpo", "dtdyo", "dlxu", "dlyu", "dtdxuo", "dlxv",
+                  "dlyv", "dpye", "ddpo", "weto", "dduo", "amsuo", "ddue", "amsue"):
+            a = np.asfortranarray(inst[k], dtype=np.float64)
+            self._keep.append(a)
+            setattr(d, k, _p(a))
+        d.device = device
+        h = C.c_void_p()
+        st = self.lib.orctm_create(C.byref(d), C.byref(h))
+        _lib.check(st, None)
+        self.h = h
+        self._keep = []
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.orctm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- data movement ------------------------------------------------------
+    def shape(self, name: str):
+        ie, je, ke = self.ie, self.je, self.ke
+        return {"p": (ie, je, ke), "u": (ie + 1, je, ke), "v": (ie, je + 1, ke),
+                "w": (ie, je, ke + 1), "2": (ie, je)}[SHAPES.get(name, "p")]
+
+    def _fid(self, name):
+        if isinstance(name, int):
+            return name
+        if name.startswith("tracer"):
+            return F_THO + int(name[6:])
+        return FIELDS[name]
+
+    def upload(self, name, arr: np.ndarray):
+        a = np.asfortranarray(arr, dtype=np.float64)
+        _lib.check(self.lib.orctm_upload(self.h, self._fid(name), _p(a), a.size), self.h)
+
+    def download(self, name, out: np.ndarray | None = None) -> np.ndarray:
+        shp = self.shape(name if isinstance(name, str) and not name.startswith("tracer") else "pnh")
+        a = np.zeros(shp, dtype=np.float64, order="F") if out is None else out
+        _lib.check(self.lib.orctm_download(self.h, self._fid(name), _p(a), a.size), self.h)
+        return a
+
+    def upload_state(self, st: dict):
+        for k in FIELDS:
+            if k in st:
+                self.upload(k, st[k])
+        for n, t in enumerate(st.get("tracers", [])):
+            self.upload(f"tracer{n}", t)
+
+    def download_state(self) -> dict:
+        out = {k: self.download(k) for k in FIELDS}
+        out["tracers"] = [self.download(f"tracer{n}") for n in range(self.ntr)]
+        return out
+
+    # -- the reference's routines -----------------------------------------
+    def ocuad(self):
+        _lib.check(self.lib.orctm_ocuad(self.h), self.h)
+
+    def ocvad(self):
+        _lib.check(self.lib.orctm_ocvad(self.h), self.h)
+
+    def ocwad(self):
+        _lib.check(self.lib.orctm_ocwad(self.h), self.h)
+
+    def ocadpo(self, tracer: int):
+        _lib.check(self.lib.orctm_ocadpo(self.h, tracer), self.h)
+
+    def octdiff(self):
+        _lib.check(self.lib.orctm_octdiff(self.h), self.h)
+
+    def octimf(self):
+        _lib.check(self.lib.orctm_octimf(self.h), self.h)
+
+    def ocvisc(self):
+        _lib.check(self.lib.orctm_ocvisc(self.h), self.h)
+
+    def ocvtot_nh(self) -> dict:
+        s = SolveStats()
+        _lib.check(self.lib.orctm_ocvtot_nh(self.h, C.byref(s)), self.h,
+                   allow=(_lib.ORCTM_E_NOT_CONVERGED,))
+        return s.as_dict()
+
+    def step_hotpath(self) -> dict:
+        s = SolveStats()
+        _lib.check(self.lib.orctm_step_hotpath(self.h, C.byref(s)), self.h,
+                   allow=(_lib.ORCTM_E_NOT_CONVERGED,))
+        return s.as_dict()
+
+    def set_solver(self, mode: str | int = "fp64", rtol: float = 1e-10, maxit: int = 5000):
+        m = {"fp64": SOLVER_FP64, "fp32_refined": SOLVER_FP32_REFINED}.get(mode, mode)
+        _lib.check(self.lib.orctm_set_solver(self.h, int(m), float(rtol), int(maxit)), self.h)
+
+    def synchronize(self):
+        _lib.check(self.lib.orctm_synchronize(self.h), self.h)
+
+    # -- device timing -------------------------------------------------------
+    def timer_start(self):
+        _lib.check(self.lib.orctm_timer_start(self.h), self.h)
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        _lib.check(self.lib.orctm_timer_stop(self.h, C.byref(ms)), self.h)
+        return ms.value
+
+    def set_profiling(self, on: bool):
+        _lib.check(self.lib.orctm_set_profiling(self.h, int(bool(on))), self.h)
+
+    def profile(self) -> dict:
+        out = {}
+        for k, name in enumerate(_lib.PROF_KINDS):
+            n, ms = C.c_longlong(), C.c_double()
+            _lib.check(self.lib.orctm_profile_get(self.h, k, C.byref(n), C.byref(ms)), self.h)
+            out[name] = {"launches": n.value, "ms": ms.value}
+        return out
+
+    @staticmethod
+    def kernel_launches() -> int:
+        return int(_lib.load().orctm_kernel_launches())

@@ -1,0 +1,678 @@
+// Mass-conserving limited advection (Maier-Reimer scheme) of tracers and of
+// the u, v, w momenta: OCADPO (ocadpo.f90:94-348), OCUAD (ocuad.f90:1-271),
+// OCVAD (ocvad.f90:1-271) and OCWAD (ocwad.f90:1-238).
+//
+// Each routine is three direction-split sweeps z -> x -> y.  Per sweep a cell
+// volume V and the field T are updated from face transports
+//     RN = V + WTP(-) - WTP(0) - WTM(0) + WTM(+)
+//     T' = (T*V + TRP(-) - TRP(0) - TRM(0) + TRM(+)) / RN
+// The z sweep runs one thread per column marching down the column with the
+// transports of the level below carried in registers; the x and y sweeps run
+// one thread per cell.  Every sweep writes a fresh buffer (never in place), so
+// neighbouring columns always read the previous sweep's values.  Arithmetic is
+// IEEE binary64 in the reference's operation order (built with --fmad=false),
+// so results match the CPU restatement bit for bit.
+#include "common.cuh"
+#include "ops.h"
+
+namespace orctm {
+
+namespace {
+
+struct Fl { double trp, trm, wtp, wtm; };
+
+#define AT(a, i, j, K) (a)[G.L.at((i), (j), (K)-1)]
+#define A2(a, i, j) (a)[G.L.at2((i), (j))]
+
+// one face transport pair with the curvature limiter
+__device__ __forceinline__ Fl limited(double up, double um, double t, double tprev, double tnext,
+                                      double vol, double cap, double mask) {
+  const double abl = fabs(tprev - tnext);
+  const double zwabl = fabs(tprev + tnext - 2. * t);
+  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * mask;
+  const double sch = fmn(cap, scha * vol / (up + um + 1.E-20));
+  const double schi = 1. - sch;
+  Fl f;
+  f.trp = up * (schi * t + sch * 0.5 * (t + tprev));
+  f.trm = um * (schi * t + sch * 0.5 * (t + tnext));
+  f.wtp = up;
+  f.wtm = um;
+  return f;
+}
+
+// the same without a mask factor (OCUAD/OCVAD forms: SCHA has no WETO product)
+__device__ __forceinline__ Fl limited_nm(double up, double um, double t, double tprev, double tnext,
+                                         double vol, double cap) {
+  const double abl = fabs(tprev - tnext);
+  const double zwabl = fabs(tprev + tnext - 2. * t);
+  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+  const double sch = fmn(cap, scha * vol / (up + um + 1.E-20));
+  const double schi = 1. - sch;
+  Fl f;
+  f.trp = up * (schi * t + sch * 0.5 * (t + tprev));
+  f.trm = um * (schi * t + sch * 0.5 * (t + tnext));
+  f.wtp = up;
+  f.wtm = um;
+  return f;
+}
+
+__device__ __forceinline__ Fl upwind(double up, double um, double t) {
+  Fl f;
+  f.trp = up * t;
+  f.trm = um * t;
+  f.wtp = up;
+  f.wtm = um;
+  return f;
+}
+
+__device__ __forceinline__ Fl zero_fl() { return Fl{0., 0., 0., 0.}; }
+
+// update from the transports of the previous (m) / own (c) / next (p) faces
+__device__ __forceinline__ void apply(double t, double v, const Fl& m, const Fl& c, const Fl& p,
+                                      double& tn, double& vn) {
+  const double rn = v + m.wtp - c.wtp - c.wtm + p.wtm;
+  tn = (t * v + m.trp - c.trp - c.trm + p.trm) / rn;
+  vn = rn;
+}
+
+// vertical update: RN = V + WTP(K+1) - WTP(K) - WTM(K) + WTM(K-1)
+__device__ __forceinline__ void apply_z(double t, double v, const Fl& fm, const Fl& fc,
+                                        const Fl& fp, double& tn, double& vn) {
+  const double rn = v + fp.wtp - fc.wtp - fc.wtm + fm.wtm;
+  tn = (t * v + fp.trp - fc.trp - fc.trm + fm.trm) / rn;
+  vn = rn;
+}
+
+// ---------------------------------------------------------------- OCADPO ---
+// vertical sweep, ocadpo.f90:94-173; one thread per p-column
+__global__ void k_adpo_z(Geo G, const double* __restrict__ T, const double* __restrict__ wo,
+                         const double* __restrict__ zo, double* __restrict__ To,
+                         double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const long long ij = G.L.at2(i, j);
+  const double dlxp = G.dlxp[ij], dlyp = G.dlyp[ij];
+  auto v0 = [&](int K) {
+    double s = wet(G.gp, ij, K) * dlxp * dlyp * thick(G.gp, G.dzw, ij, K);
+    if (K == 1) s = s + dlxp * dlyp * wet(G.gp, ij, 1) * (zo[ij] - AT(wo, i, j, 1) * G.dt);
+    return s;
+  };
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1;
+  if (!interior) {
+    for (int K = 1; K <= KE; ++K) {
+      AT(To, i, j, K) = AT(T, i, j, K);
+      AT(Vo, i, j, K) = v0(K);
+    }
+    return;
+  }
+  const double cdt = 0.5 * G.dt * dlyp * dlxp;
+  auto flux = [&](int K, double vol) {
+    const int klo = K + 1 < KE ? K + 1 : KE;
+    const int kup = K - 1 > 1 ? K - 1 : 1;
+    const double t = AT(T, i, j, K), tu = AT(T, i, j, kup), tl = AT(T, i, j, klo);
+    const double w0 = AT(wo, i, j, K), w1 = AT(wo, i, j, K + 1);
+    const double up = cdt * (w0 + fabs(w0));
+    const double um = cdt * (fabs(w1) - w1);
+    const double abl = fabs(tu - tl);
+    const double zwabl = fabs(tu + tl - 2. * t);
+    const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
+    double sch = fmn(wet(G.gp, ij, klo), scha * vol / (up + um + 1.E-20));
+    if (K == 1 || K == KE) sch = 0.;
+    const double schi = 1. - sch;
+    Fl f;
+    f.trp = up * (schi * t + sch * 0.5 * (t + tu));
+    f.trm = um * (schi * t + sch * 0.5 * (t + tl));
+    f.wtp = up;
+    f.wtm = um;
+    return f;
+  };
+  Fl fm = zero_fl();               // transports of level K-1 (TRM/WTM(0) = 0)
+  double vk = v0(1);
+  Fl fc = flux(1, vk);
+  for (int K = 1; K <= KE; ++K) {
+    double vn = 0.;
+    Fl fp = zero_fl();             // TRP/WTP(KEP) = 0
+    if (K < KE) {
+      vn = v0(K + 1);
+      fp = flux(K + 1, vn);
+    }
+    const double t = AT(T, i, j, K);
+    double tn = t, vv = vk;
+    if (wetb(G.gp, ij, K)) apply_z(t, vk, fm, fc, fp, tn, vv);
+    AT(To, i, j, K) = tn;
+    AT(Vo, i, j, K) = vv;
+    fm = fc;
+    fc = fp;
+    vk = vn;
+  }
+}
+
+// x-direction transports at p-column q of row j (ocadpo.f90:203-232)
+__device__ __forceinline__ Fl adpo_xflux(const Geo& G, const double* T, const double* V,
+                                         const double* uko, int q, int j, int K) {
+  if (q < 2 || q > G.L.ie - 1) return zero_fl();
+  const double u0 = AT(uko, q, j, K), um1 = AT(uko, q - 1, j, K);
+  const long long ij = G.L.at2(q, j), ijm = G.L.at2(q - 1, j);
+  const double up = 0.5 * G.dt * thick(G.gu, G.dzw, ij, K) * G.dlyu[ij] * (u0 + fabs(u0));
+  const double um = 0.5 * G.dt * thick(G.gu, G.dzw, ijm, K) * (fabs(um1) - um1) * G.dlyu[ijm];
+  // SCHA = MAX(...)*WETO(I)*WETO(I+1)*WETO(I-1), factors applied in that order
+  const double t = AT(T, q, j, K), te = AT(T, q + 1, j, K), tw = AT(T, q - 1, j, K);
+  const double abl = fabs(te - tw);
+  const double zwabl = fabs(te + tw - 2. * t);
+  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, ij, K) *
+                      wet(G.gp, G.L.at2(q + 1, j), K) * wet(G.gp, G.L.at2(q - 1, j), K);
+  const double sch = fmn(1., scha * AT(V, q, j, K) / (up + um + 1.E-20));
+  const double schi = 1. - sch;
+  Fl f;
+  f.trp = up * (schi * t + sch * 0.5 * (t + te));
+  f.trm = um * (schi * t + sch * 0.5 * (t + tw));
+  f.wtp = up;
+  f.wtm = um;
+  return f;
+}
+
+__device__ __forceinline__ Fl adpo_yflux(const Geo& G, const double* T, const double* V,
+                                         const double* vke, int i, int q, int K) {
+  if (q < 2 || q > G.L.je - 1) return zero_fl();
+  const long long ijn = G.L.at2(i, q - 1), ij = G.L.at2(i, q);
+  const double vn = AT(vke, i, q - 1, K), vs = AT(vke, i, q, K);
+  const double up = 0.5 * G.dt * thick(G.gv, G.dzw, ijn, K) * G.dlxv[ijn] * (vn + fabs(vn));
+  const double um = 0.5 * G.dt * thick(G.gv, G.dzw, ij, K) * G.dlxv[ij] * (fabs(vs) - vs);
+  const double t = AT(T, i, q, K), tn = AT(T, i, q - 1, K), ts = AT(T, i, q + 1, K);
+  const double abl = fabs(tn - ts);
+  const double zwabl = fabs(tn + ts - 2. * t);
+  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, ij, K) *
+                      wet(G.gp, G.L.at2(i, q - 1), K) * wet(G.gp, G.L.at2(i, q + 1), K);
+  const double sch = fmn(1., scha * AT(V, i, q, K) / (up + um + 1.E-20));
+  const double schi = 1. - sch;
+  Fl f;
+  f.trp = up * (schi * t + sch * 0.5 * (t + tn));
+  f.trm = um * (schi * t + sch * 0.5 * (t + ts));
+  f.wtp = up;
+  f.wtm = um;
+  return f;
+}
+
+template <int DIR>  // 0: x (ocadpo.f90:181-258), 1: y (ocadpo.f90:266-345)
+__global__ void k_adpo_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
+                         const double* __restrict__ vel, double* __restrict__ To,
+                         double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  const double t = AT(T, i, j, K), v = AT(V, i, j, K);
+  double tn = t, vn = v;
+  if (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1 && wetb(G.gp, G.L.at2(i, j), K)) {
+    if (DIR == 0) {
+      const Fl m = adpo_xflux(G, T, V, vel, i - 1, j, K);
+      const Fl c = adpo_xflux(G, T, V, vel, i, j, K);
+      const Fl p = adpo_xflux(G, T, V, vel, i + 1, j, K);
+      apply(t, v, m, c, p, tn, vn);
+    } else {
+      const Fl m = adpo_yflux(G, T, V, vel, i, j + 1, K);  // RN uses WTP(J+1), WTM(J-1)
+      const Fl c = adpo_yflux(G, T, V, vel, i, j, K);
+      const Fl p = adpo_yflux(G, T, V, vel, i, j - 1, K);
+      apply(t, v, m, c, p, tn, vn);
+    }
+  }
+  AT(To, i, j, K) = tn;
+  if (Vo) AT(Vo, i, j, K) = vn;
+}
+
+// ----------------------------------------------------------------- OCUAD ---
+// vertical sweep, ocuad.f90:20-86; u-columns i in [0, IE]
+__global__ void k_uad_z(Geo G, const double* __restrict__ T, const double* __restrict__ wo,
+                        double* __restrict__ To, double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const long long ij = G.L.at2(i, j);
+  auto v0 = [&](int K) {
+    return wet(G.gu, ij, K) * G.dlxu[ij] * G.dlyu[ij] * thick(G.gu, G.dzw, ij, K);
+  };
+  const bool interior = i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1;
+  if (!interior) {
+    for (int K = 1; K <= KE; ++K) {
+      AT(To, i, j, K) = AT(T, i, j, K);
+      AT(Vo, i, j, K) = v0(K);
+    }
+    return;
+  }
+  const long long ijp = G.L.at2(i, j);
+  const double cdt = 0.5 * G.dt * G.dlyp[ijp] * G.dlxp[ijp];
+  auto flux = [&](int K, double vol) {
+    const int klo = K + 1 < KE ? K + 1 : KE;
+    const int kup = K - 1 > 1 ? K - 1 : 1;
+    const double wup = 0.5 * (AT(wo, i, j, K) + AT(wo, i + 1, j, K));
+    const double wlo = 0.5 * (AT(wo, i, j, K + 1) + AT(wo, i + 1, j, K + 1));
+    const double up = cdt * (wup + fabs(wup));
+    const double um = cdt * (fabs(wlo) - wlo);
+    return limited_nm(up, um, AT(T, i, j, K), AT(T, i, j, kup), AT(T, i, j, klo), vol, 1.);
+  };
+  Fl fm = zero_fl();
+  double vk = v0(1);
+  Fl fc = flux(1, vk);
+  for (int K = 1; K <= KE; ++K) {
+    double vn = 0.;
+    Fl fp = zero_fl();
+    if (K < KE) {
+      vn = v0(K + 1);
+      fp = flux(K + 1, vn);
+    }
+    const double t = AT(T, i, j, K);
+    double tn = t, vv = vk;
+    if (wetb(G.gu, ij, K)) apply_z(t, vk, fm, fc, fp, tn, vv);
+    AT(To, i, j, K) = tn;
+    AT(Vo, i, j, K) = vv;
+    fm = fc;
+    fc = fp;
+    vk = vn;
+  }
+}
+
+// x-face transports of u-cell q, ocuad.f90:99-148
+__device__ __forceinline__ Fl uad_xflux(const Geo& G, const double* T, const double* V,
+                                        const double* uko, int q, int j, int K) {
+  const int IE = G.L.ie;
+  auto ud = [&](int ii) { return AT(uko, ii, j, K) * thick(G.gu, G.dzw, G.L.at2(ii, j), K); };
+  if (q >= 1 && q <= IE - 1) {
+    const double uos = 0.5 * (ud(q) + ud(q + 1));
+    const double uwe = 0.5 * (ud(q - 1) + ud(q));
+    const double up = 0.5 * G.dt * G.dlyp[G.L.at2(q + 1, j)] * (uos + fabs(uos));
+    const double um = 0.5 * G.dt * (fabs(uwe) - uwe) * G.dlyp[G.L.at2(q, j)];
+    return limited_nm(up, um, AT(T, q, j, K), AT(T, q + 1, j, K), AT(T, q - 1, j, K),
+                      AT(V, q, j, K), 1.);
+  }
+  if (q == 0) {
+    const double uos = 0.5 * (ud(0) + ud(1));
+    const double uwe = ud(0);
+    const double up = 0.5 * G.dt * G.dlyp[G.L.at2(1, j)] * (uos + fabs(uos));
+    const double um = 0.5 * G.dt * (fabs(uwe) - uwe) * G.dlyu[G.L.at2(0, j)];
+    return upwind(up, um, AT(T, 0, j, K));
+  }
+  if (q == IE) {
+    const double uos = ud(IE);
+    const double uwe = 0.5 * (ud(IE - 1) + ud(IE));
+    const double up = 0.5 * G.dt * G.dlyp[G.L.at2(IE, j)] * (uos + fabs(uos));
+    const double um = 0.5 * G.dt * (fabs(uwe) - uwe) * G.dlyu[G.L.at2(IE, j)];
+    return upwind(up, um, AT(T, IE, j, K));
+  }
+  return zero_fl();
+}
+
+// y-face transports of u-cell (i, q), ocuad.f90:184-233
+__device__ __forceinline__ Fl uad_yflux(const Geo& G, const double* T, const double* V,
+                                        const double* vke, int i, int q, int K) {
+  const int JE = G.L.je;
+  if (q < 1 || q > JE) return zero_fl();
+  auto vd = [&](int ii, int jj) { return AT(vke, ii, jj, K) * thick(G.gv, G.dzw, G.L.at2(ii, jj), K); };
+  const double vsu = 0.5 * (vd(i, q) + vd(i + 1, q));
+  const double vno = 0.5 * (vd(i, q - 1) + vd(i + 1, q - 1));
+  const double up = 0.5 * G.dt * (0.5 * (G.dlxv[G.L.at2(i, q - 1)] + G.dlxv[G.L.at2(i + 1, q - 1)])) *
+                    (vno + fabs(vno));
+  const double um = 0.5 * G.dt * (0.5 * (G.dlxv[G.L.at2(i, q)] + G.dlxv[G.L.at2(i + 1, q)])) *
+                    (fabs(vsu) - vsu);
+  if (q == 1 || q == JE) return upwind(up, um, AT(T, i, q, K));
+  return limited_nm(up, um, AT(T, i, q, K), AT(T, i, q - 1, K), AT(T, i, q + 1, K),
+                    AT(V, i, q, K), 1.);
+}
+
+template <int DIR>
+__global__ void k_uad_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
+                        const double* __restrict__ vel, double* __restrict__ To,
+                        double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  const double t = AT(T, i, j, K), v = AT(V, i, j, K);
+  double tn = t, vn = v;
+  if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1 && wetb(G.gu, G.L.at2(i, j), K)) {
+    if (DIR == 0) {
+      const Fl m = uad_xflux(G, T, V, vel, i - 1, j, K);
+      const Fl c = uad_xflux(G, T, V, vel, i, j, K);
+      const Fl p = uad_xflux(G, T, V, vel, i + 1, j, K);
+      apply(t, v, m, c, p, tn, vn);
+    } else {
+      const Fl m = uad_yflux(G, T, V, vel, i, j + 1, K);
+      const Fl c = uad_yflux(G, T, V, vel, i, j, K);
+      const Fl p = uad_yflux(G, T, V, vel, i, j - 1, K);
+      apply(t, v, m, c, p, tn, vn);
+    }
+  }
+  AT(To, i, j, K) = tn;
+  if (Vo) AT(Vo, i, j, K) = vn;
+}
+
+// ----------------------------------------------------------------- OCVAD ---
+// vertical sweep, ocvad.f90:20-86; v-columns j in [0, JE]
+__global__ void k_vad_z(Geo G, const double* __restrict__ T, const double* __restrict__ wo,
+                        double* __restrict__ To, double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const long long ij = G.L.at2(i, j);
+  auto v0 = [&](int K) {
+    return wet(G.gv, ij, K) * G.dlxv[ij] * G.dlyv[ij] * thick(G.gv, G.dzw, ij, K);
+  };
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1;
+  if (!interior) {
+    for (int K = 1; K <= KE; ++K) {
+      AT(To, i, j, K) = AT(T, i, j, K);
+      AT(Vo, i, j, K) = v0(K);
+    }
+    return;
+  }
+  const double cdt = 0.5 * G.dt * G.dlyp[ij] * G.dlxp[ij];
+  auto flux = [&](int K, double vol) {
+    const int klo = K + 1 < KE ? K + 1 : KE;
+    const int kup = K - 1 > 1 ? K - 1 : 1;
+    const double wup = 0.5 * (AT(wo, i, j, K) + AT(wo, i, j + 1, K));
+    const double wlo = 0.5 * (AT(wo, i, j, K + 1) + AT(wo, i, j + 1, K + 1));
+    const double up = cdt * (wup + fabs(wup));
+    const double um = cdt * (fabs(wlo) - wlo);
+    return limited_nm(up, um, AT(T, i, j, K), AT(T, i, j, kup), AT(T, i, j, klo), vol, 1.);
+  };
+  Fl fm = zero_fl();
+  double vk = v0(1);
+  Fl fc = flux(1, vk);
+  for (int K = 1; K <= KE; ++K) {
+    double vn = 0.;
+    Fl fp = zero_fl();
+    if (K < KE) {
+      vn = v0(K + 1);
+      fp = flux(K + 1, vn);
+    }
+    const double t = AT(T, i, j, K);
+    double tn = t, vv = vk;
+    if (wetb(G.gv, ij, K)) apply_z(t, vk, fm, fc, fp, tn, vv);
+    AT(To, i, j, K) = tn;
+    AT(Vo, i, j, K) = vv;
+    fm = fc;
+    fc = fp;
+    vk = vn;
+  }
+}
+
+// x-face transports of v-cell (q, j), ocvad.f90:99-148
+__device__ __forceinline__ Fl vad_xflux(const Geo& G, const double* T, const double* V,
+                                        const double* uko, int q, int j, int K) {
+  const int IE = G.L.ie;
+  if (q < 1 || q > IE) return zero_fl();
+  auto ud = [&](int ii, int jj) { return AT(uko, ii, jj, K) * thick(G.gu, G.dzw, G.L.at2(ii, jj), K); };
+  const double uos = 0.5 * (ud(q, j) + ud(q, j + 1));
+  const double uwe = 0.5 * (ud(q - 1, j) + ud(q - 1, j + 1));
+  const double up = 0.5 * G.dt * (0.5 * (G.dlyu[G.L.at2(q, j)] + G.dlyu[G.L.at2(q, j + 1)])) *
+                    (uos + fabs(uos));
+  const double um = 0.5 * G.dt * (fabs(uwe) - uwe) *
+                    (0.5 * (G.dlyu[G.L.at2(q - 1, j)] + G.dlyu[G.L.at2(q - 1, j + 1)]));
+  if (q == 1 || q == IE) return upwind(up, um, AT(T, q, j, K));
+  return limited_nm(up, um, AT(T, q, j, K), AT(T, q + 1, j, K), AT(T, q - 1, j, K),
+                    AT(V, q, j, K), 1.);
+}
+
+// y-face transports of v-cell (i, q), ocvad.f90:184-233.  The J = 0 edge
+// reads DLXU(I,0) in the reference, outside DLXU's bounds; DLXV(I,0) is used.
+__device__ __forceinline__ Fl vad_yflux(const Geo& G, const double* T, const double* V,
+                                        const double* vke, int i, int q, int K) {
+  const int JE = G.L.je;
+  auto vd = [&](int jj) { return AT(vke, i, jj, K) * thick(G.gv, G.dzw, G.L.at2(i, jj), K); };
+  if (q >= 1 && q <= JE - 1) {
+    const double vno = 0.5 * (vd(q) + vd(q - 1));
+    const double vsu = 0.5 * (vd(q) + vd(q + 1));
+    const double up = 0.5 * G.dt * G.dlxp[G.L.at2(i, q)] * (vno + fabs(vno));
+    const double um = 0.5 * G.dt * G.dlxp[G.L.at2(i, q + 1)] * (fabs(vsu) - vsu);
+    return limited_nm(up, um, AT(T, i, q, K), AT(T, i, q - 1, K), AT(T, i, q + 1, K),
+                      AT(V, i, q, K), 1.);
+  }
+  if (q == 0) {
+    const double vno = vd(0);
+    const double vsu = 0.5 * (vd(0) + vd(1));
+    const double up = 0.5 * G.dt * G.dlxv[G.L.at2(i, 0)] * (vno + fabs(vno));
+    const double um = 0.5 * G.dt * G.dlxp[G.L.at2(i, 1)] * (fabs(vsu) - vsu);
+    return upwind(up, um, AT(T, i, 0, K));
+  }
+  if (q == JE) {
+    const double vno = 0.5 * (vd(JE) + vd(JE - 1));
+    const double vsu = vd(JE);
+    const double up = 0.5 * G.dt * G.dlxp[G.L.at2(i, JE)] * (vno + fabs(vno));
+    const double um = 0.5 * G.dt * G.dlxu[G.L.at2(i, JE)] * (fabs(vsu) - vsu);
+    return upwind(up, um, AT(T, i, JE, K));
+  }
+  return zero_fl();
+}
+
+template <int DIR>
+__global__ void k_vad_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
+                        const double* __restrict__ vel, double* __restrict__ To,
+                        double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int K = blockIdx.z + 1;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  const double t = AT(T, i, j, K), v = AT(V, i, j, K);
+  double tn = t, vn = v;
+  if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1 && wetb(G.gv, G.L.at2(i, j), K)) {
+    if (DIR == 0) {
+      const Fl m = vad_xflux(G, T, V, vel, i - 1, j, K);
+      const Fl c = vad_xflux(G, T, V, vel, i, j, K);
+      const Fl p = vad_xflux(G, T, V, vel, i + 1, j, K);
+      apply(t, v, m, c, p, tn, vn);
+    } else {
+      const Fl m = vad_yflux(G, T, V, vel, i, j + 1, K);
+      const Fl c = vad_yflux(G, T, V, vel, i, j, K);
+      const Fl p = vad_yflux(G, T, V, vel, i, j - 1, K);
+      apply(t, v, m, c, p, tn, vn);
+    }
+  }
+  AT(To, i, j, K) = tn;
+  if (Vo) AT(Vo, i, j, K) = vn;
+}
+
+// ----------------------------------------------------------------- OCWAD ---
+// vertical sweep, ocwad.f90:14-102; w-columns, levels 1..KEP.  WETO(KEP),
+// read one level past WETO in the reference (ocwad.f90:63), is taken as 0.
+__global__ void k_wad_z(Geo G, const double* __restrict__ T, const double* __restrict__ wo,
+                        const double* __restrict__ zo, double* __restrict__ To,
+                        double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const long long ij = G.L.at2(i, j);
+  const double dlxp = G.dlxp[ij], dlyp = G.dlyp[ij];
+  auto v0 = [&](int K) {
+    const double a = wet(G.gp, ij, K) * dlxp * dlyp;
+    if (K == 1) return a * (thick(G.gp, G.dzw, ij, 1) + zo[ij]) / 2.0;
+    if (K == 2)
+      return a * (thick(G.gp, G.dzw, ij, 1) + thick(G.gp, G.dzw, ij, 2) + zo[ij]) / 2.0;
+    return a * (thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K)) / 2.0;
+  };
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1;
+  AT(To, i, j, KE + 1) = AT(T, i, j, KE + 1);
+  AT(To, i, j, 1) = AT(T, i, j, 1);
+  AT(Vo, i, j, 1) = v0(1);
+  if (!interior || KE < 2) {
+    for (int K = 2; K <= KE; ++K) {
+      AT(To, i, j, K) = AT(T, i, j, K);
+      AT(Vo, i, j, K) = v0(K);
+    }
+    return;
+  }
+  const double cdt = 0.5 * G.dt * dlyp * dlxp;
+  auto flux = [&](int K, double vol) {
+    const double wup = 0.5 * (AT(wo, i, j, K) + AT(wo, i, j, K - 1));
+    const double wum = 0.5 * (AT(wo, i, j, K) + AT(wo, i, j, K + 1));
+    const double up = cdt * (wup + fabs(wup));
+    const double um = cdt * (fabs(wum) - wum);
+    const double cap = K + 1 <= KE ? wet(G.gp, ij, K + 1) : 0.0;
+    return limited_nm(up, um, AT(T, i, j, K), AT(T, i, j, K - 1), AT(T, i, j, K + 1), vol, cap);
+  };
+  // edge transports, ocwad.f90:72-83
+  Fl fm;  // level 1: only TRM/WTM used
+  {
+    const double wum = 0.5 * (AT(wo, i, j, 1) + AT(wo, i, j, 2));
+    const double um = cdt * (fabs(wum) - wum);
+    fm = Fl{0., um * (0.5 * (AT(T, i, j, 1) + AT(T, i, j, 2))), 0., um};
+  }
+  Fl fkep;
+  {
+    const double wup = 0.5 * (AT(wo, i, j, KE + 1) + AT(wo, i, j, KE));
+    const double up = cdt * (wup + fabs(wup));
+    fkep = Fl{up * (0.5 * (AT(T, i, j, KE) + AT(T, i, j, KE + 1))), 0., up, 0.};
+  }
+  double vk = v0(2);
+  Fl fc = flux(2, vk);
+  for (int K = 2; K <= KE; ++K) {
+    double vn = 0.;
+    Fl fp = fkep;
+    if (K < KE) {
+      vn = v0(K + 1);
+      fp = flux(K + 1, vn);
+    }
+    const double t = AT(T, i, j, K);
+    double tn = t, vv = vk;
+    if (wetb(G.gp, ij, K)) apply_z(t, vk, fm, fc, fp, tn, vv);
+    AT(To, i, j, K) = tn;
+    AT(Vo, i, j, K) = vv;
+    fm = fc;
+    fc = fp;
+    vk = vn;
+  }
+}
+
+__device__ __forceinline__ Fl wad_xflux(const Geo& G, const double* T, const double* V,
+                                        const double* uko, int q, int j, int K) {
+  if (q < 2 || q > G.L.ie - 1) return zero_fl();
+  auto ud = [&](int ii, int KK) { return AT(uko, ii, j, KK) * thick(G.gu, G.dzw, G.L.at2(ii, j), KK); };
+  const double uos = 0.5 * (ud(q, K) + ud(q, K - 1));
+  const double uwe = 0.5 * (ud(q - 1, K) + ud(q - 1, K - 1));
+  const double up = 0.5 * G.dt * G.dlyu[G.L.at2(q, j)] * (uos + fabs(uos));
+  const double um = 0.5 * G.dt * G.dlyu[G.L.at2(q - 1, j)] * (fabs(uwe) - uwe);
+  const double t = AT(T, q, j, K), te = AT(T, q + 1, j, K), tw = AT(T, q - 1, j, K);
+  const double abl = fabs(te - tw);
+  const double zwabl = fabs(te + tw - 2. * t);
+  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, G.L.at2(q, j), K) *
+                      wet(G.gp, G.L.at2(q + 1, j), K) * wet(G.gp, G.L.at2(q - 1, j), K);
+  const double sch = fmn(1., scha * AT(V, q, j, K) / (up + um + 1.E-20));
+  const double schi = 1. - sch;
+  return Fl{up * (schi * t + sch * 0.5 * (t + te)), um * (schi * t + sch * 0.5 * (t + tw)), up, um};
+}
+
+__device__ __forceinline__ Fl wad_yflux(const Geo& G, const double* T, const double* V,
+                                        const double* vke, int i, int q, int K) {
+  if (q < 2 || q > G.L.je - 1) return zero_fl();
+  auto vd = [&](int jj, int KK) { return AT(vke, i, jj, KK) * thick(G.gv, G.dzw, G.L.at2(i, jj), KK); };
+  const double vsu = 0.5 * (vd(q, K) + vd(q, K - 1));
+  const double vno = 0.5 * (vd(q - 1, K) + vd(q - 1, K - 1));
+  const double up = 0.5 * G.dt * G.dlxv[G.L.at2(i, q - 1)] * (vno + fabs(vno));
+  const double um = 0.5 * G.dt * G.dlxv[G.L.at2(i, q)] * (fabs(vsu) - vsu);
+  const double t = AT(T, i, q, K), tn = AT(T, i, q - 1, K), ts = AT(T, i, q + 1, K);
+  const double abl = fabs(tn - ts);
+  const double zwabl = fabs(tn + ts - 2. * t);
+  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, G.L.at2(i, q), K) *
+                      wet(G.gp, G.L.at2(i, q - 1), K) * wet(G.gp, G.L.at2(i, q + 1), K);
+  const double sch = fmn(1., scha * AT(V, i, q, K) / (up + um + 1.E-20));
+  const double schi = 1. - sch;
+  return Fl{up * (schi * t + sch * 0.5 * (t + tn)), um * (schi * t + sch * 0.5 * (t + ts)), up, um};
+}
+
+template <int DIR>
+__global__ void k_wad_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
+                        const double* __restrict__ vel, double* __restrict__ To,
+                        double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;  // 1..KE+1
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const double t = AT(T, i, j, K);
+  double tn = t;
+  double v = K <= KE ? AT(V, i, j, K) : 0.0, vn = v;
+  if (K >= 2 && K <= KE && i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1 &&
+      wetb(G.gp, G.L.at2(i, j), K)) {
+    if (DIR == 0) {
+      const Fl m = wad_xflux(G, T, V, vel, i - 1, j, K);
+      const Fl c = wad_xflux(G, T, V, vel, i, j, K);
+      const Fl p = wad_xflux(G, T, V, vel, i + 1, j, K);
+      apply(t, v, m, c, p, tn, vn);
+    } else {
+      const Fl m = wad_yflux(G, T, V, vel, i, j + 1, K);
+      const Fl c = wad_yflux(G, T, V, vel, i, j, K);
+      const Fl p = wad_yflux(G, T, V, vel, i, j - 1, K);
+      apply(t, v, m, c, p, tn, vn);
+    }
+  }
+  AT(To, i, j, K) = tn;
+  if (Vo && K <= KE) AT(Vo, i, j, K) = vn;
+}
+
+inline dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, 1); }
+inline dim3 grid3(int nx, int ny, int nz, dim3 b) {
+  return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz);
+}
+
+}  // namespace
+
+// T -> out through the z, x and y sweeps; tA, vA, vB: scratch fields
+void launch_ocadpo(const Geo& G, const double* T, const double* uko, const double* vke,
+                   const double* wo, const double* zo, double* out, double* tA, double* vA,
+                   double* vB, cudaStream_t st) {
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const dim3 bc(32, 4), bh(32, 4);
+  k_adpo_z<<<grid2(IE, JE, bc), bc, 0, st>>>(G, T, wo, zo, out, vA);
+  count_launch();
+  k_adpo_h<0><<<grid3(IE, JE, KE, bh), bh, 0, st>>>(G, out, vA, uko, tA, vB);
+  count_launch();
+  k_adpo_h<1><<<grid3(IE, JE, KE, bh), bh, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  count_launch();
+}
+
+void launch_ocuad(const Geo& G, const double* T, const double* uko, const double* vke,
+                  const double* wo, double* out, double* tA, double* vA, double* vB,
+                  cudaStream_t st) {
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const dim3 b(32, 4);
+  k_uad_z<<<grid2(IE + 1, JE, b), b, 0, st>>>(G, T, wo, out, vA);
+  count_launch();
+  k_uad_h<0><<<grid3(IE + 1, JE, KE, b), b, 0, st>>>(G, out, vA, uko, tA, vB);
+  count_launch();
+  k_uad_h<1><<<grid3(IE + 1, JE, KE, b), b, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  count_launch();
+}
+
+void launch_ocvad(const Geo& G, const double* T, const double* uko, const double* vke,
+                  const double* wo, double* out, double* tA, double* vA, double* vB,
+                  cudaStream_t st) {
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const dim3 b(32, 4);
+  k_vad_z<<<grid2(IE, JE + 1, b), b, 0, st>>>(G, T, wo, out, vA);
+  count_launch();
+  k_vad_h<0><<<grid3(IE, JE + 1, KE, b), b, 0, st>>>(G, out, vA, uko, tA, vB);
+  count_launch();
+  k_vad_h<1><<<grid3(IE, JE + 1, KE, b), b, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  count_launch();
+}
+
+void launch_ocwad(const Geo& G, const double* T, const double* uko, const double* vke,
+                  const double* wo, const double* zo, double* out, double* tA, double* vA,
+                  double* vB, cudaStream_t st) {
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const dim3 b(32, 4);
+  k_wad_z<<<grid2(IE, JE, b), b, 0, st>>>(G, T, wo, zo, out, vA);
+  count_launch();
+  k_wad_h<0><<<grid3(IE, JE, KE + 1, b), b, 0, st>>>(G, out, vA, uko, tA, vB);
+  count_launch();
+  k_wad_h<1><<<grid3(IE, JE, KE + 1, b), b, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  count_launch();
+}
+
+}  // namespace orctm

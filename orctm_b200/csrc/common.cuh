@@ -1,0 +1,76 @@
+// Device layout, geometry views and helpers shared by every kernel.
+//
+// Every 3D field lives on the device in one padded layout that covers the
+// union of the reference's p-, u-, v- and w-point index ranges on a
+// single-rank domain:
+//     i in [0, IE]   (u-points start at I_start = 0, p/v/w at 1)
+//     j in [0, JE]   (v-points start at J_start = 0)
+//     level l in [0, KE]  (l = Fortran K-1; w-points use all KE+1 levels)
+// offset(i, j, l) = i + P * (j + JN * l), P = IE+1 rounded up to 32 doubles
+// (rows start 256-byte aligned, i is the coalescing axis), JN = JE + 1.
+// 2D fields use the same (i, j) plane.  Slots a field does not use (i = 0 of
+// a p-point field, say) are carried along untouched.
+//
+// Geometry is stored compressed: BODEN makes every thickness/mask column
+// monotone (wet from the surface down to a bottom level, then land), so
+//     DDPO(i,j,K) = K <  kb(i,j) ? DZW(K) : K == kb(i,j) ? bot(i,j) : 0
+//     WETO(i,j,K) = K <= kb(i,j)
+// and likewise DDUO/AMSUO and DDUE/AMSUE: 3D geometry costs no HBM traffic.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace orctm {
+
+constexpr int kMaxKe = 320;  // longest column a handle accepts (the reference runs KE = 300)
+
+struct Layout {
+  int ie, je, ke;   // IE, JE, KE (halos included)
+  int P, JN;        // pitch (elements) and rows per level
+  long long plane;  // P * JN
+  __host__ __device__ long long at(int i, int j, int l) const {
+    return (long long)i + (long long)P * ((long long)j + (long long)JN * (long long)l);
+  }
+  __host__ __device__ long long at2(int i, int j) const { return (long long)i + (long long)P * j; }
+  __host__ __device__ long long n3() const { return plane * (ke + 1); }
+};
+
+// Compressed column geometry of one staggering (p, u or v points).
+struct ColGeo {
+  const int* kb;      // number of wet levels (0 = land column)
+  const double* bot;  // thickness of the deepest wet level
+};
+
+// Read-only geometry view passed by value to kernels.
+struct Geo {
+  Layout L;
+  double dt, dti, almzer, aulapts, aulapuv, minvalue;
+  int ob_w, ob_e, ob_n, ob_s;
+  ColGeo gp, gu, gv;
+  const double* dzw;   // [KE]     DZW(K) at index K-1
+  const double* di;    // [KE+1]   DI(K)  at index K-1
+  // 2D metrics, padded plane layout
+  const double *dlxp, *dlyp, *dlxu, *dlyu, *dlxv, *dlyv;
+  const double *dtdxpo, *dtdyo, *dtdxuo, *dpye;
+};
+
+__device__ __forceinline__ double thick(const ColGeo& c, const double* dzw, long long ij, int K) {
+  const int kb = c.kb[ij];
+  return K < kb ? dzw[K - 1] : (K == kb ? c.bot[ij] : 0.0);
+}
+__device__ __forceinline__ double wet(const ColGeo& c, long long ij, int K) {
+  return K <= c.kb[ij] ? 1.0 : 0.0;
+}
+__device__ __forceinline__ bool wetb(const ColGeo& c, long long ij, int K) { return K <= c.kb[ij]; }
+
+// Fortran MAX/MIN for non-NaN operands, evaluated exactly as the oracle does.
+__device__ __forceinline__ double fmx(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double fmn(double a, double b) { return b < a ? b : a; }
+
+}  // namespace orctm
+
+#define ORCTM_CUDA_OK(expr)                                   \
+  do {                                                        \
+    cudaError_t e_ = (expr);                                  \
+    if (e_ != cudaSuccess) return orctm::cuda_status(e_);     \
+  } while (0)

@@ -1,0 +1,537 @@
+// Tracer diffusion (OCTDIFF_BASE + OCTDIFF_TS: octdiff_base.f90:182-221,
+// octdiff_ts.f90:51-59, 294-407) and momentum diffusion with quadratic
+// bottom drag (OCVISC, FREESLIP branch: ocvisc.f90:37-478, 615-688).
+//
+// Implicit vertical diffusion is one Thomas solve per water column, one
+// thread per column with the column's tridiagonal system in thread-local
+// arrays.  The horizontal biharmonic operator is two passes (a masked
+// Laplacian into a scratch field, then the flux-form update), one thread per
+// cell.  Arithmetic follows the reference's operation order in IEEE binary64.
+#include "common.cuh"
+#include "ops.h"
+
+namespace orctm {
+
+namespace {
+
+#define AT(a, i, j, K) (a)[G.L.at((i), (j), (K)-1)]
+
+inline dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, 1); }
+inline dim3 grid3(int nx, int ny, int nz, dim3 b) {
+  return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz);
+}
+
+// ------------------------------------------------------------- OCTDIFF ----
+// Implicit vertical diffusion of ntr tracers (TRIDSY built once per column).
+// Columns outside i in [2,IE1], j in [2,JE1] are copied unchanged.
+struct TrPtrs {
+  const double* in[8];
+  double* out[8];
+};
+
+__global__ void k_tdiff_vert(Geo G, TrPtrs tp, int ntr, const double* __restrict__ dvo,
+                             const double* __restrict__ zo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1;
+  if (!interior) {
+    for (int n = 0; n < ntr; ++n)
+      for (int K = 1; K <= KE; ++K) AT(tp.out[n], i, j, K) = AT(tp.in[n], i, j, K);
+    return;
+  }
+  const long long ij = G.L.at2(i, j);
+  double t1[kMaxKe], t2[kMaxKe], t3[kMaxKe];
+  for (int K = 1; K <= KE; ++K) {
+    const double zzsurf = K == 1 ? 1. : 0.;
+    const double den = thick(G.gp, G.dzw, ij, K) + zzsurf * (zo[ij]) + G.almzer;
+    t1[K - 1] = -G.dt * AT(dvo, i, j, K) * wet(G.gp, ij, K) * G.di[K - 1] / den;
+    t3[K - 1] = -G.dt * AT(dvo, i, j, K + 1) * G.di[K] / den;
+    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
+  }
+  for (int K = 2; K <= KE; ++K) {
+    const double a = t1[K - 1];
+    t1[K - 2] = a / t2[K - 2];
+    t2[K - 1] = t2[K - 1] - t3[K - 2] * a / t2[K - 2];
+  }
+  for (int n = 0; n < ntr; ++n) {
+    const double* T = tp.in[n];
+    double* O = tp.out[n];
+    double prev = AT(T, i, j, 1);
+    AT(O, i, j, 1) = prev;  // T1O(1)
+    for (int K = 2; K <= KE; ++K) {
+      prev = AT(T, i, j, K) - t1[K - 2] * prev;
+      AT(O, i, j, K) = prev;  // T1O(K)
+    }
+    double nxt = AT(O, i, j, KE) / t2[KE - 1];
+    AT(O, i, j, KE) = nxt;
+    for (int l = KE - 1; l >= 1; --l) {
+      nxt = (AT(O, i, j, l) - t3[l - 1] * nxt) / t2[l - 1];
+      AT(O, i, j, l) = nxt;
+    }
+  }
+}
+
+// masked Laplacian T1O (octdiff_ts.f90:346-362); halo cells hold 0
+__global__ void k_tdiff_lap(Geo G, const double* __restrict__ T, double* __restrict__ L1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  double r = 0.0;
+  if (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
+    const double c = AT(T, i, j, K);
+    auto w = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
+    r = w(i, j) *
+        ((w(i - 1, j) * (AT(T, i - 1, j, K) - c) / G.dlxu[G.L.at2(i - 1, j)] +
+          w(i + 1, j) * (AT(T, i + 1, j, K) - c) / G.dlxu[G.L.at2(i, j)]) /
+             G.dlxp[G.L.at2(i, j)] +
+         (w(i, j - 1) * (AT(T, i, j - 1, K) - c) / G.dlyv[G.L.at2(i, j - 1)] +
+          w(i, j + 1) * (AT(T, i, j + 1, K) - c) / G.dlyv[G.L.at2(i, j)]) /
+             G.dlyp[G.L.at2(i, j)]);
+  }
+  AT(L1, i, j, K) = r;
+}
+
+// biharmonic update (octdiff_ts.f90:369-399); AULX = AULAPTS*DLXU**4 etc.
+__global__ void k_tdiff_bih(Geo G, const double* __restrict__ T, const double* __restrict__ L1,
+                            const double* __restrict__ zo, double* __restrict__ O) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  const double t = AT(T, i, j, K);
+  double r = t;
+  if (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
+    auto w = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
+    auto aulx = [&](int ii, int jj) {
+      const double x = G.dlxu[G.L.at2(ii, jj)];
+      return G.aulapts * ((x * x) * (x * x));
+    };
+    auto auly = [&](int ii, int jj) {
+      const double y = G.dlyv[G.L.at2(ii, jj)];
+      return G.aulapts * ((y * y) * (y * y));
+    };
+    const long long ij = G.L.at2(i, j);
+    const double zzsurf = K == 1 ? 1. : 0.;
+    const double c = AT(L1, i, j, K);
+    const double den = (thick(G.gp, G.dzw, ij, K) + G.almzer + zzsurf * (zo[ij])) * G.dlxp[ij] *
+                       G.dlyp[ij];
+    r = t - (w(i, j) / den) * G.dzw[K - 1] *
+                (w(i - 1, j) * aulx(i - 1, j) * G.dlyu[G.L.at2(i - 1, j)] *
+                     (AT(L1, i - 1, j, K) - c) / G.dlxu[G.L.at2(i - 1, j)] +
+                 w(i + 1, j) * aulx(i, j) * G.dlyu[ij] * (AT(L1, i + 1, j, K) - c) / G.dlxu[ij] +
+                 w(i, j - 1) * auly(i, j - 1) * G.dlxv[G.L.at2(i, j - 1)] *
+                     (AT(L1, i, j - 1, K) - c) / G.dlyv[G.L.at2(i, j - 1)] +
+                 w(i, j + 1) * auly(i, j) * G.dlxv[ij] * (AT(L1, i, j + 1, K) - c) / G.dlyv[ij]);
+  }
+  AT(O, i, j, K) = r;
+}
+
+// -------------------------------------------------------------- OCVISC ----
+// bottom speeds SPEEDU/SPEEDV (ocvisc.f90:53-104): evaluated at the single
+// level where the mask drops from 1 to 0 (or at KE when the column is full)
+__global__ void k_visc_speed(Geo G, const double* __restrict__ uoo, const double* __restrict__ voe,
+                             double* __restrict__ spu, double* __restrict__ spv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  const long long ij = G.L.at2(i, j);
+  double su = 0., sv = 0.;
+  if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
+    const int K = G.gu.kb[ij];
+    if (K >= 1) {
+      const double a = 0.25 * (AT(voe, i, j, K) + AT(voe, i + 1, j, K) + AT(voe, i, j - 1, K) +
+                               AT(voe, i + 1, j - 1, K));
+      const double u = AT(uoo, i, j, K);
+      su = fmx(sqrt(u * u + a * a), 1.E-3);
+    }
+  }
+  if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
+    const int K = G.gv.kb[ij];
+    if (K >= 1) {
+      const double a = 0.25 * (AT(uoo, i, j, K) + AT(uoo, i - 1, j, K) + AT(uoo, i, j + 1, K) +
+                               AT(uoo, i - 1, j + 1, K));
+      const double v = AT(voe, i, j, K);
+      sv = fmx(sqrt(v * v + a * a), 1.E-3);
+    }
+  }
+  spu[ij] = su;
+  spv[ij] = sv;
+}
+
+// implicit vertical diffusion of u (DIR = 0, ocvisc.f90:168-218) or v
+// (DIR = 1, ocvisc.f90:114-165) with quadratic bottom drag in the last row
+template <int DIR>
+__global__ void k_visc_uv(Geo G, const double* __restrict__ X, const double* __restrict__ keep,
+                          const double* __restrict__ avo, const double* __restrict__ speed,
+                          double* __restrict__ O) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const bool interior = DIR == 0 ? (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1)
+                                 : (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1);
+  const bool valid = DIR == 0 ? (j >= 1) : (i >= 1);
+  if (!valid) return;
+  if (!interior) {
+    for (int K = 1; K <= KE; ++K) AT(O, i, j, K) = AT(keep, i, j, K);
+    return;
+  }
+  const ColGeo& cg = DIR == 0 ? G.gu : G.gv;
+  const long long ij = G.L.at2(i, j);
+  const long long ij2 = DIR == 0 ? G.L.at2(i + 1, j) : G.L.at2(i, j + 1);
+  const double BOFRIC = 3.E-3, RAYFRIC = 3.E-3;
+  const double sp = speed[ij];
+  double t1[kMaxKe], t2[kMaxKe], t3[kMaxKe];
+  auto avo_at = [&](long long q, int K) { return avo[q + G.L.plane * (K - 1)]; };
+  for (int K = 1; K <= KE - 1; ++K) {
+    const double am = wet(cg, ij, K), am1 = wet(cg, ij, K + 1), dd = thick(cg, G.dzw, ij, K);
+    const double avup = 0.5 * (avo_at(ij, K) + avo_at(ij2, K)) * am;
+    const double avlo = 0.5 * (avo_at(ij, K + 1) + avo_at(ij2, K + 1)) * am1 +
+                        (BOFRIC + RAYFRIC * dd * sp) * (am - am1);
+    t1[K - 1] = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
+    t3[K - 1] = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
+    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
+    t3[K - 1] = t3[K - 1] * am1;
+  }
+  {
+    const int K = KE;
+    const double am = wet(cg, ij, K), dd = thick(cg, G.dzw, ij, K);
+    const double avup = 0.5 * (avo_at(ij, K) + avo_at(ij2, K)) * am;
+    const double avlo = (BOFRIC + RAYFRIC * dd * sp) * am;
+    t1[K - 1] = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
+    t3[K - 1] = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
+    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
+    t3[K - 1] = 0.;
+  }
+  for (int K = 2; K <= KE; ++K) {
+    const double a = t1[K - 1];
+    t1[K - 2] = a / t2[K - 2];
+    t2[K - 1] = t2[K - 1] - t3[K - 2] * a / t2[K - 2];
+  }
+  double prev = AT(X, i, j, 1);
+  AT(O, i, j, 1) = prev;
+  for (int K = 2; K <= KE; ++K) {
+    prev = AT(X, i, j, K) - t1[K - 2] * prev;
+    AT(O, i, j, K) = prev;
+  }
+  double nxt = wet(cg, ij, KE) * AT(O, i, j, KE) / t2[KE - 1];
+  AT(O, i, j, KE) = nxt;
+  for (int l = KE - 1; l >= 1; --l) {
+    nxt = (AT(O, i, j, l) - t3[l - 1] * nxt) * wet(cg, ij, l) / t2[l - 1];
+    AT(O, i, j, l) = nxt;
+  }
+}
+
+// implicit vertical diffusion of w, levels 2..KE (ocvisc.f90:225-270)
+__global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __restrict__ avo,
+                         double* __restrict__ O) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1 && KE >= 2;
+  if (!interior) {
+    for (int K = 1; K <= KE + 1; ++K) AT(O, i, j, K) = AT(W, i, j, K);
+    return;
+  }
+  const long long ij = G.L.at2(i, j);
+  double t1[kMaxKe], t2[kMaxKe], t3[kMaxKe];
+  for (int K = 2; K <= KE - 1; ++K) {
+    const double avup = 0.5 * (AT(avo, i, j, K - 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K - 1);
+    const double avlo = 0.5 * (AT(avo, i, j, K + 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K);
+    const double den = 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
+    t1[K - 1] = -2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2] / den;
+    t3[K - 1] = -2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1] / den;
+    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
+  }
+  {
+    const int K = KE;
+    const double avup = 0.5 * (AT(avo, i, j, K - 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K - 1);
+    const double avlo = 0.0;
+    const double den = 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
+    t1[K - 1] = -2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2] / den;
+    t3[K - 1] = -2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1] / den;
+    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
+    t3[K - 1] = 0.;
+  }
+  for (int K = 3; K <= KE; ++K) {
+    const double a = t1[K - 1];
+    t1[K - 2] = a / t2[K - 2];
+    t2[K - 1] = t2[K - 1] - t3[K - 2] * a / t2[K - 2];
+  }
+  AT(O, i, j, 1) = AT(W, i, j, 1);
+  AT(O, i, j, KE + 1) = AT(W, i, j, KE + 1);
+  double prev = AT(W, i, j, 2);
+  AT(O, i, j, 2) = prev;
+  for (int K = 3; K <= KE; ++K) {
+    prev = AT(W, i, j, K) - t1[K - 2] * prev;
+    AT(O, i, j, K) = prev;
+  }
+  double nxt = wet(G.gp, ij, KE) * AT(O, i, j, KE) / t2[KE - 1];
+  AT(O, i, j, KE) = nxt;
+  for (int K = KE - 1; K >= 2; --K) {
+    nxt = (AT(O, i, j, K) - t3[K - 1] * nxt) * wet(G.gp, ij, K) / t2[K - 1];
+    AT(O, i, j, K) = nxt;
+  }
+}
+
+__device__ __forceinline__ double dlypsi(const Geo& G, int i, int j) {  // u-points, i in [0,IE]
+  if (i == 0) return G.dlyv[G.L.at2(1, j)];
+  if (i == G.L.ie) return G.dlyv[G.L.at2(G.L.ie, j)];
+  return 0.5 * (G.dlyv[G.L.at2(i, j)] + G.dlyv[G.L.at2(i + 1, j)]);
+}
+__device__ __forceinline__ double dlxpsi(const Geo& G, int i, int j) {  // v-points, j in [0,JE]
+  if (j == 0) return G.dlxu[G.L.at2(i, 1)];
+  if (j == G.L.je) return G.dlxu[G.L.at2(i, G.L.je)];
+  return 0.5 * (G.dlxu[G.L.at2(i, j)] + G.dlxu[G.L.at2(i, j + 1)]);
+}
+__device__ __forceinline__ double pow4(double x) { return (x * x) * (x * x); }
+
+// first Laplacians UK1O (u), VK1E (v), WN1O (w), ocvisc.f90:350-438, 617-669
+__global__ void k_visc_lap(Geo G, const double* __restrict__ uk, const double* __restrict__ vk,
+                           const double* __restrict__ wn, double* __restrict__ u1,
+                           double* __restrict__ v1, double* __restrict__ w1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int K = blockIdx.z + 1;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  // ---- u-points
+  if (j >= 1) {
+    auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
+    auto UK = [&](int ii, int jj) { return AT(uk, ii, jj, K); };
+    const bool jin = j >= 2 && j <= JE - 1, iin = i >= 1 && i <= IE - 1;
+    double r = 0.0;
+    auto ypart = [&]() {
+      return (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / dlypsi(G, i, j - 1) -
+              AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / dlypsi(G, i, j)) /
+             G.dlyu[G.L.at2(i, j)];
+    };
+    auto xpart = [&]() {
+      return (AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / G.dlxp[G.L.at2(i + 1, j)] -
+              AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / G.dlxp[G.L.at2(i, j)]) /
+             G.dlxu[G.L.at2(i, j)];
+    };
+    if (jin && iin) {
+      r = AO(i, j) * (xpart() + ypart());
+    } else if (jin && i == 0) {
+      r = AO(i, j) * ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / G.dlxp[G.L.at2(i + 1, j)]) /
+                          G.dlxu[G.L.at2(i, j)] +
+                      ypart());
+    } else if (jin && i == IE) {
+      r = AO(i, j) * ((-AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / G.dlxp[G.L.at2(i, j)]) /
+                          G.dlxu[G.L.at2(i, j)] +
+                      ypart());
+    } else if (iin && j == 1) {
+      r = AO(i, j) * (xpart() + (-AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / dlypsi(G, i, j)) /
+                                    G.dlyu[G.L.at2(i, j)]);
+    } else if (iin && j == JE) {
+      r = AO(i, j) * (xpart() + (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / dlypsi(G, i, j - 1)) /
+                                    G.dlyu[G.L.at2(i, j)]);
+    }
+    AT(u1, i, j, K) = r;
+  }
+  // ---- v-points
+  if (i >= 1) {
+    auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
+    auto VK = [&](int ii, int jj) { return AT(vk, ii, jj, K); };
+    const bool jin = j >= 1 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
+    double r = 0.0;
+    auto xpart = [&]() {
+      return (AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / dlxpsi(G, i, j) -
+              AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / dlxpsi(G, i - 1, j)) /
+             G.dlxv[G.L.at2(i, j)];
+    };
+    auto ypart = [&]() {
+      return (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / G.dlyp[G.L.at2(i, j)] -
+              AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / G.dlyp[G.L.at2(i, j + 1)]) /
+             G.dlyv[G.L.at2(i, j)];
+    };
+    if (jin && iin) {
+      r = AE(i, j) * (xpart() + ypart());
+    } else if (jin && i == 1) {
+      r = AE(i, j) * ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / dlxpsi(G, i, j)) /
+                          G.dlxv[G.L.at2(i, j)] +
+                      ypart());
+    } else if (jin && i == IE) {
+      r = AE(i, j) * ((-AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / dlxpsi(G, i - 1, j)) /
+                          G.dlxv[G.L.at2(i, j)] +
+                      ypart());
+    } else if (iin && j == 0) {
+      r = AE(i, j) * (xpart() + (-AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / G.dlyp[G.L.at2(i, j + 1)]) /
+                                    G.dlyv[G.L.at2(i, j)]);
+    } else if (iin && j == JE) {
+      r = AE(i, j) * (xpart() + (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / G.dlyp[G.L.at2(i, j)]) /
+                                    G.dlyv[G.L.at2(i, j)]);
+    }
+    AT(v1, i, j, K) = r;
+  }
+  // ---- w-points (levels 1..KE)
+  if (i >= 1 && j >= 1) {
+    auto WE = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
+    auto WN = [&](int ii, int jj) { return AT(wn, ii, jj, K); };
+    const bool jin = j >= 2 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
+    double r = 0.0;
+    auto xpart = [&]() {
+      return (WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / G.dlxu[G.L.at2(i, j)] -
+              WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / G.dlxu[G.L.at2(i - 1, j)]) /
+             G.dlxp[G.L.at2(i, j)];
+    };
+    auto ypart = [&]() {
+      return (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / G.dlyv[G.L.at2(i, j - 1)] -
+              WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / G.dlyv[G.L.at2(i, j)]) /
+             G.dlyp[G.L.at2(i, j)];
+    };
+    if (jin && iin) {
+      r = WE(i, j) * (xpart() + ypart());
+    } else if (jin && i == 1) {
+      r = WE(i, j) * ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / G.dlxu[G.L.at2(i, j)]) /
+                          G.dlxp[G.L.at2(i, j)] +
+                      ypart());
+    } else if (jin && i == IE) {
+      r = WE(i, j) * ((-WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / G.dlxu[G.L.at2(i - 1, j)]) /
+                          G.dlxp[G.L.at2(i, j)] +
+                      ypart());
+    } else if (iin && j == 1) {
+      r = WE(i, j) * (xpart() + (-WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / G.dlyv[G.L.at2(i, j)]) /
+                                    G.dlyp[G.L.at2(i, j)]);
+    } else if (iin && j == JE) {
+      r = WE(i, j) * (xpart() + (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / G.dlyv[G.L.at2(i, j - 1)]) /
+                                    G.dlyp[G.L.at2(i, j)]);
+    }
+    AT(w1, i, j, K) = r;
+  }
+}
+
+// second passes, ocvisc.f90:445-477 (u, v) and 673-688 (w)
+__global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* __restrict__ voe,
+                           const double* __restrict__ uk, const double* __restrict__ vk,
+                           const double* __restrict__ wn, const double* __restrict__ u1,
+                           const double* __restrict__ v1, const double* __restrict__ w1,
+                           double* __restrict__ uo, double* __restrict__ vo,
+                           double* __restrict__ wo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int K = blockIdx.z + 1;  // 1..KE+1
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const double A = G.aulapuv, mv = G.minvalue;
+  if (K <= KE) {
+    // ---- u
+    if (j >= 1) {
+      double r = AT(uoo, i, j, K);
+      if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
+        auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
+        auto U1 = [&](int ii, int jj) { return AT(u1, ii, jj, K); };
+        auto aulux = [&](int ii, int jj) { return A * pow4(fmx(G.dlxp[G.L.at2(ii, jj)], mv)); };
+        auto auluy = [&](int ii, int jj) { return A * pow4(fmx(mv, dlypsi(G, ii, jj))); };
+        const long long ij = G.L.at2(i, j);
+        r = (AO(i, j) / (G.dlxu[ij] * G.dlyu[ij])) *
+            (G.dlxu[ij] * G.dlyu[ij] * AT(uk, i, j, K) -
+             (aulux(i + 1, j) * G.dlyp[G.L.at2(i + 1, j)] * AO(i + 1, j) * (U1(i + 1, j) - U1(i, j)) /
+                  G.dlxp[G.L.at2(i + 1, j)] -
+              aulux(i, j) * G.dlyp[ij] * AO(i - 1, j) * (U1(i, j) - U1(i - 1, j)) / G.dlxp[ij] +
+              auluy(i, j - 1) * dlxpsi(G, i, j - 1) * AO(i, j - 1) * (U1(i, j - 1) - U1(i, j)) /
+                  dlypsi(G, i, j - 1) -
+              auluy(i, j) * dlxpsi(G, i, j) * AO(i, j + 1) * (U1(i, j) - U1(i, j + 1)) /
+                  dlypsi(G, i, j)));
+      }
+      AT(uo, i, j, K) = r;
+    }
+    // ---- v
+    if (i >= 1) {
+      double r = AT(voe, i, j, K);
+      if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
+        auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
+        auto V1 = [&](int ii, int jj) { return AT(v1, ii, jj, K); };
+        auto aulvx = [&](int ii, int jj) { return A * pow4(fmx(dlxpsi(G, ii, jj), mv)); };
+        auto aulvy = [&](int ii, int jj) { return A * pow4(fmx(mv, G.dlyp[G.L.at2(ii, jj)])); };
+        const long long ij = G.L.at2(i, j);
+        r = (AE(i, j) / (G.dlxv[ij] * G.dlyv[ij])) *
+            (G.dlxv[ij] * G.dlyv[ij] * AT(vk, i, j, K) -
+             (aulvx(i, j) * dlypsi(G, i, j) * AE(i + 1, j) * (V1(i + 1, j) - V1(i, j)) / dlxpsi(G, i, j) -
+              aulvx(i - 1, j) * dlypsi(G, i - 1, j) * AE(i - 1, j) * (V1(i, j) - V1(i - 1, j)) /
+                  dlxpsi(G, i - 1, j) +
+              aulvy(i, j) * G.dlxp[ij] * AE(i, j - 1) * (V1(i, j - 1) - V1(i, j)) / G.dlyp[ij] -
+              aulvy(i, j + 1) * G.dlxp[G.L.at2(i, j + 1)] * AE(i, j + 1) * (V1(i, j) - V1(i, j + 1)) /
+                  G.dlyp[G.L.at2(i, j + 1)]));
+      }
+      AT(vo, i, j, K) = r;
+    }
+  }
+  // ---- w (levels 1..KE updated, KEP carried)
+  if (i >= 1 && j >= 1) {
+    double r = AT(wn, i, j, K);
+    if (K <= KE && i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
+      auto WE = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
+      auto W1 = [&](int ii, int jj) { return AT(w1, ii, jj, K); };
+      auto dzu = [&](int ii, int jj) { return fmx(thick(G.gu, G.dzw, G.L.at2(ii, jj), K), mv); };
+      auto dzv = [&](int ii, int jj) { return fmx(thick(G.gv, G.dzw, G.L.at2(ii, jj), K), mv); };
+      auto aulwx = [&](int ii, int jj) { return A * pow4(fmx(G.dlxu[G.L.at2(ii, jj)], mv)); };
+      auto aulwy = [&](int ii, int jj) { return A * pow4(fmx(G.dlyv[G.L.at2(ii, jj)], mv)); };
+      const long long ij = G.L.at2(i, j);
+      const double dzp = fmx(thick(G.gp, G.dzw, ij, K), mv);
+      r = (WE(i, j) / (G.dlxp[ij] * G.dlyp[ij] * dzp)) *
+          (G.dlxp[ij] * G.dlyp[ij] * dzp * AT(wn, i, j, K) -
+           (+aulwx(i, j) * G.dlyu[ij] * dzu(i, j) * WE(i + 1, j) * (W1(i + 1, j) - W1(i, j)) / G.dlxu[ij] -
+            aulwx(i - 1, j) * G.dlyu[G.L.at2(i - 1, j)] * dzu(i - 1, j) * WE(i - 1, j) *
+                (W1(i, j) - W1(i - 1, j)) / G.dlxu[G.L.at2(i - 1, j)] +
+            aulwy(i, j - 1) * G.dlxv[G.L.at2(i, j - 1)] * dzv(i, j - 1) * WE(i, j - 1) *
+                (W1(i, j - 1) - W1(i, j)) / G.dlyv[G.L.at2(i, j - 1)] -
+            aulwy(i, j) * G.dlxv[ij] * dzv(i, j) * WE(i, j + 1) * (W1(i, j) - W1(i, j + 1)) / G.dlyv[ij]));
+    }
+    AT(wo, i, j, K) = r;
+  }
+}
+
+}  // namespace
+
+void launch_octdiff_vert(const Geo& G, int ntr, const double* const* in, double* const* out,
+                         const double* dvo, const double* zo, cudaStream_t st) {
+  TrPtrs tp{};
+  for (int n = 0; n < ntr; ++n) {
+    tp.in[n] = in[n];
+    tp.out[n] = out[n];
+  }
+  const dim3 b(32, 2);
+  k_tdiff_vert<<<grid2(G.L.ie, G.L.je, b), b, 0, st>>>(G, tp, ntr, dvo, zo);
+  count_launch();
+}
+
+void launch_octdiff_bih(const Geo& G, const double* T, const double* zo, double* lap, double* out,
+                        cudaStream_t st) {
+  const dim3 b(32, 4);
+  k_tdiff_lap<<<grid3(G.L.ie, G.L.je, G.L.ke, b), b, 0, st>>>(G, T, lap);
+  count_launch();
+  k_tdiff_bih<<<grid3(G.L.ie, G.L.je, G.L.ke, b), b, 0, st>>>(G, T, lap, zo, out);
+  count_launch();
+}
+
+void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const double* wno,
+                   const double* uko, const double* vke, const double* avo, double* spu,
+                   double* spv, double* ukv, double* vkv, double* wnv, double* u1, double* v1,
+                   double* w1, double* uo, double* vo, double* wo, cudaStream_t st) {
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const dim3 b2(32, 4), bc(32, 2), b3(32, 4);
+  k_visc_speed<<<grid2(IE + 1, JE + 1, b2), b2, 0, st>>>(G, uoo, voe, spu, spv);
+  count_launch();
+  k_visc_uv<0><<<grid2(IE + 1, JE + 1, bc), bc, 0, st>>>(G, uoo, uko, avo, spu, ukv);
+  count_launch();
+  k_visc_uv<1><<<grid2(IE + 1, JE + 1, bc), bc, 0, st>>>(G, voe, vke, avo, spv, vkv);
+  count_launch();
+  k_visc_w<<<grid2(IE, JE, bc), bc, 0, st>>>(G, wno, avo, wnv);
+  count_launch();
+  k_visc_lap<<<grid3(IE + 1, JE + 1, KE, b3), b3, 0, st>>>(G, ukv, vkv, wnv, u1, v1, w1);
+  count_launch();
+  k_visc_bih<<<grid3(IE + 1, JE + 1, KE + 1, b3), b3, 0, st>>>(G, uoo, voe, ukv, vkv, wnv, u1, v1,
+                                                               w1, uo, vo, wo);
+  count_launch();
+}
+
+}  // namespace orctm

@@ -1,0 +1,923 @@
+// Handle, device memory, geometry compression, routine sequencing, Poisson
+// solver driver and the extern "C" entry points of include/orctm_gpu.h.
+//
+// Device memory.  All 3D fields share one padded layout (common.cuh) and
+// hence one buffer size, so buffers come from a single pool.  A field slot
+// points at a reference-counted buffer; routines never update a field in
+// place but write a fresh buffer and rebind the slot, which lets OCTIMF and
+// the state rotation of OCVTOT_NH (UOO_1 <- UOO, WO <- WNO, ...) alias buffers
+// instead of copying them.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/orctm_gpu.h"
+#include "common.cuh"
+#include "ops.h"
+
+namespace orctm {
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return ORCTM_OK;
+  if (e == cudaErrorMemoryAllocation) return ORCTM_E_NOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ORCTM_E_NODEVICE;
+  return ORCTM_E_CUDA;
+}
+
+namespace {
+
+thread_local std::string g_create_error;
+
+enum Kind { KP = 0, KU = 1, KV = 2, KW = 3, K2P = 4 };
+
+constexpr int kNumFixed = ORCTM_F_THO;  // fields before the tracers
+constexpr int kMaxTracers = 8;
+
+Kind field_kind(int f) {
+  switch (f) {
+    case ORCTM_F_UOO: case ORCTM_F_UKO: case ORCTM_F_UOO_1: return KU;
+    case ORCTM_F_VOE: case ORCTM_F_VKE: case ORCTM_F_VOE_1: return KV;
+    case ORCTM_F_WNO: case ORCTM_F_WO: case ORCTM_F_WNO_1: case ORCTM_F_DVO: case ORCTM_F_AVO:
+      return KW;
+    case ORCTM_F_ZO: return K2P;
+    default: return KP;
+  }
+}
+
+}  // namespace
+}  // namespace orctm
+
+using namespace orctm;
+
+struct orctm_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Layout L{};
+  Geo G{};
+  PoissonGeo P{};
+  int ntr = 2;
+  std::string err;
+
+  // geometry / tables (device)
+  std::vector<void*> owned;  // freed at destroy
+  // pool of 3D buffers (double, L.n3() elements)
+  std::vector<double*> free_;
+  std::unordered_map<double*, int> refs;
+  std::vector<double*> slot;  // per field id
+  double* zo = nullptr;       // 2D
+
+  // solver
+  int solver_mode = ORCTM_SOLVER_FP64;
+  double rtol = 1e-10;
+  int maxit = 5000;
+  double* b = nullptr;
+  double *xs = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
+  double *d = nullptr, *rw = nullptr;
+  float *r32b = nullptr, *r32 = nullptr, *z32 = nullptr, *p32a = nullptr, *p32b = nullptr,
+        *q32 = nullptr, *d32 = nullptr;
+  SolverState* S = nullptr;
+  double* partials = nullptr;
+  SolverState* hS = nullptr;  // pinned mirror
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t tm0 = nullptr, tm1 = nullptr;  // orctm_timer_start / _stop
+
+  // optional per-launcher device timing (orctm_set_profiling)
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs[ORCTM_PROF_KINDS];
+  double prof_ms[ORCTM_PROF_KINDS] = {};
+  long long prof_n[ORCTM_PROF_KINDS] = {};
+  cudaEvent_t get_event() {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void prof_begin(cudaEvent_t* e0) {
+    *e0 = nullptr;
+    if (!prof) return;
+    *e0 = get_event();
+    cudaEventRecord(*e0, stream);
+  }
+  void prof_end(int kind, cudaEvent_t e0) {
+    if (!prof || !e0) return;
+    cudaEvent_t e1 = get_event();
+    cudaEventRecord(e1, stream);
+    prof_pairs[kind].push_back({e0, e1});
+    if (prof_pairs[kind].size() > 4096) prof_flush();
+  }
+  void prof_flush() {
+    cudaStreamSynchronize(stream);
+    for (int k = 0; k < ORCTM_PROF_KINDS; ++k) {
+      for (auto& pr : prof_pairs[k]) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, pr.first, pr.second);
+        prof_ms[k] += ms;
+        prof_n[k] += 1;
+        ev_pool.push_back(pr.first);
+        ev_pool.push_back(pr.second);
+      }
+      prof_pairs[k].clear();
+    }
+  }
+
+  // ---------------------------------------------------------------- pool
+  int alloc(double** out) {
+    if (!free_.empty()) {
+      *out = free_.back();
+      free_.pop_back();
+      refs[*out] = 1;
+      return ORCTM_OK;
+    }
+    double* p = nullptr;
+    ORCTM_CUDA_OK(cudaMalloc(&p, sizeof(double) * L.n3()));
+    ORCTM_CUDA_OK(cudaMemsetAsync(p, 0, sizeof(double) * L.n3(), stream));
+    refs[p] = 1;
+    *out = p;
+    return ORCTM_OK;
+  }
+  void unref(double* p) {
+    if (!p) return;
+    auto it = refs.find(p);
+    if (it == refs.end()) return;
+    if (--it->second == 0) {
+      refs.erase(it);
+      free_.push_back(p);
+    }
+  }
+  void bind(int f, double* p) {  // slot takes ownership of one reference
+    unref(slot[f]);
+    slot[f] = p;
+  }
+  void alias(int dst, int src) {
+    double* p = slot[src];
+    refs[p]++;
+    unref(slot[dst]);
+    slot[dst] = p;
+  }
+  int fail(int st, const char* msg) {
+    err = msg;
+    return st;
+  }
+  template <typename T>
+  int dev_alloc(T** p, size_t n) {
+    ORCTM_CUDA_OK(cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(n, 1)));
+    ORCTM_CUDA_OK(cudaMemset(*p, 0, sizeof(T) * std::max<size_t>(n, 1)));
+    owned.push_back(*p);
+    return ORCTM_OK;
+  }
+};
+
+namespace {
+
+// wraps one launcher call in device events when profiling is on
+#define PROF(h, kind, call)        \
+  do {                             \
+    cudaEvent_t e0_;               \
+    (h)->prof_begin(&e0_);         \
+    call;                          \
+    (h)->prof_end((kind), e0_);    \
+  } while (0)
+
+// field extent in the reference's host layout
+void extent(const orctm_handle* h, int f, int& i0, int& ni, int& j0, int& nj, int& nk) {
+  const int IE = h->L.ie, JE = h->L.je, KE = h->L.ke;
+  i0 = 1; ni = IE; j0 = 1; nj = JE; nk = KE;
+  switch (field_kind(f)) {
+    case KU: i0 = 0; ni = IE + 1; break;
+    case KV: j0 = 0; nj = JE + 1; break;
+    case KW: nk = KE + 1; break;
+    case K2P: nk = 1; break;
+    default: break;
+  }
+}
+
+// Geometry checks and compression -------------------------------------------
+struct Ix {
+  int IE, JE, KE;
+  size_t p3(int i, int j, int k) const { return ((size_t)(k - 1) * JE + (j - 1)) * IE + (i - 1); }
+  size_t u3(int i, int j, int k) const { return ((size_t)(k - 1) * JE + (j - 1)) * (IE + 1) + i; }
+  size_t v3(int i, int j, int k) const { return ((size_t)(k - 1) * (JE + 1) + j) * IE + (i - 1); }
+  size_t p2(int i, int j) const { return (size_t)(j - 1) * IE + (i - 1); }
+  size_t u2(int i, int j) const { return (size_t)(j - 1) * (IE + 1) + i; }
+  size_t v2(int i, int j) const { return (size_t)j * IE + (i - 1); }
+};
+
+// Finds kb (wet levels) and the bottom thickness of one column and checks the
+// column has the BODEN form: thickness DZW(K) above kb, bot at kb, 0 below,
+// mask 1 down to kb and 0 below.
+bool compress_column(const double* dd, const double* mk, size_t stride, const double* dzw, int KE,
+                     int& kb, double& bot) {
+  kb = 0;
+  while (kb < KE && dd[stride * kb] > 0.) ++kb;
+  bot = kb > 0 ? dd[stride * (kb - 1)] : 0.0;
+  for (int K = 1; K <= KE; ++K) {
+    const double want = K < kb ? dzw[K - 1] : (K == kb ? bot : 0.0);
+    if (dd[stride * (K - 1)] != want) return false;
+    if (mk[stride * (K - 1)] != (K <= kb ? 1.0 : 0.0)) return false;
+  }
+  return true;
+}
+
+// ZW(K) of compute_matrix (mo_petsc.f90:557-583) for one column
+double zw_ref(const double* ddcol, const double* dzw, int KE, int K) {
+  double dd;
+  if (K == 1) {
+    dd = ddcol[0] == 0 ? dzw[0] / 2.0 : ddcol[0] / 2.0;
+  } else if (K == KE + 1) {
+    dd = ddcol[KE - 1] == 0 ? dzw[KE - 1] : ddcol[KE - 1];
+  } else {
+    if (ddcol[K - 2] == 0)
+      dd = (dzw[K - 1] + dzw[K - 2]) / 2.0;
+    else if (ddcol[K - 1] == 0)
+      dd = ddcol[K - 2];
+    else
+      dd = (ddcol[K - 2] + ddcol[K - 1]) / 2.0;
+  }
+  return 1.0 / dd;
+}
+
+int upload_2d(orctm_handle* h, double* dst, const double* src, int i0, int ni, int j0, int nj) {
+  ORCTM_CUDA_OK(cudaMemcpy2DAsync(dst + h->L.at2(i0, j0), sizeof(double) * h->L.P, src,
+                                  sizeof(double) * ni, sizeof(double) * ni, nj,
+                                  cudaMemcpyHostToDevice, h->stream));
+  return ORCTM_OK;
+}
+
+int setup(orctm_handle* h, const orctm_desc* d) {
+  const int IE = d->ie, JE = d->je, KE = d->ke;
+  const Ix x{IE, JE, KE};
+  Layout& L = h->L;
+  L.ie = IE; L.je = JE; L.ke = KE;
+  L.P = ((IE + 1) + 31) / 32 * 32;
+  L.JN = JE + 1;
+  L.plane = (long long)L.P * L.JN;
+  h->ntr = d->ntracers;
+  Geo& G = h->G;
+  G.L = L;
+  G.dt = d->dt;
+  G.dti = 1. / d->dt;
+  G.almzer = d->almzer;
+  G.aulapts = d->aulapts;
+  G.aulapuv = d->aulapuv;
+  G.minvalue = d->dzw[0] / 10.0 < 1.0 ? d->dzw[0] / 10.0 : 1.0;  // MIN(1.0, DZW(1)/10.0)
+  G.ob_w = d->ob_west; G.ob_e = d->ob_east; G.ob_n = d->ob_north; G.ob_s = d->ob_south;
+
+  // compressed columns
+  const size_t n2 = (size_t)L.plane;
+  std::vector<int> kbp(n2, 0), kbu(n2, 0), kbv(n2, 0);
+  std::vector<double> botp(n2, 0.), botu(n2, 0.), botv(n2, 0.);
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      const size_t s = L.at2(i, j);
+      if (!compress_column(d->ddpo + x.p3(i, j, 1), d->weto + x.p3(i, j, 1), (size_t)IE * JE, d->dzw,
+                           KE, kbp[s], botp[s]))
+        return h->fail(ORCTM_E_GEOMETRY, "DDPO/WETO column is not of the BODEN form");
+    }
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i) {
+      const size_t s = L.at2(i, j);
+      if (!compress_column(d->dduo + x.u3(i, j, 1), d->amsuo + x.u3(i, j, 1), (size_t)(IE + 1) * JE,
+                           d->dzw, KE, kbu[s], botu[s]))
+        return h->fail(ORCTM_E_GEOMETRY, "DDUO/AMSUO column is not of the BODEN form");
+    }
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      const size_t s = L.at2(i, j);
+      if (!compress_column(d->ddue + x.v3(i, j, 1), d->amsue + x.v3(i, j, 1), (size_t)IE * (JE + 1),
+                           d->dzw, KE, kbv[s], botv[s]))
+        return h->fail(ORCTM_E_GEOMETRY, "DDUE/AMSUE column is not of the BODEN form");
+    }
+  int* dk = nullptr;
+  double* db = nullptr;
+  int st;
+  auto up_col = [&](ColGeo& cg, const std::vector<int>& kb, const std::vector<double>& bot) -> int {
+    int s2;
+    if ((s2 = h->dev_alloc(&dk, n2))) return s2;
+    if ((s2 = h->dev_alloc(&db, n2))) return s2;
+    ORCTM_CUDA_OK(cudaMemcpy(dk, kb.data(), sizeof(int) * n2, cudaMemcpyHostToDevice));
+    ORCTM_CUDA_OK(cudaMemcpy(db, bot.data(), sizeof(double) * n2, cudaMemcpyHostToDevice));
+    cg.kb = dk;
+    cg.bot = db;
+    return ORCTM_OK;
+  };
+  if ((st = up_col(G.gp, kbp, botp))) return st;
+  if ((st = up_col(G.gu, kbu, botu))) return st;
+  if ((st = up_col(G.gv, kbv, botv))) return st;
+
+  // 1D tables
+  double *ddzw, *ddi;
+  if ((st = h->dev_alloc(&ddzw, KE))) return st;
+  if ((st = h->dev_alloc(&ddi, KE + 1))) return st;
+  ORCTM_CUDA_OK(cudaMemcpy(ddzw, d->dzw, sizeof(double) * KE, cudaMemcpyHostToDevice));
+  ORCTM_CUDA_OK(cudaMemcpy(ddi, d->di, sizeof(double) * (KE + 1), cudaMemcpyHostToDevice));
+  G.dzw = ddzw;
+  G.di = ddi;
+
+  // 2D metrics into the padded plane
+  auto up2 = [&](const double*& dst, const double* src, Kind k) -> int {
+    double* p;
+    int s2;
+    if ((s2 = h->dev_alloc(&p, n2))) return s2;
+    const int i0 = k == KU ? 0 : 1, ni = k == KU ? IE + 1 : IE;
+    const int j0 = k == KV ? 0 : 1, nj = k == KV ? JE + 1 : JE;
+    if ((s2 = upload_2d(h, p, src, i0, ni, j0, nj))) return s2;
+    dst = p;
+    return ORCTM_OK;
+  };
+  if ((st = up2(G.dlxp, d->dlxp, KP)) || (st = up2(G.dlyp, d->dlyp, KP)) ||
+      (st = up2(G.dtdxpo, d->dtdxpo, KP)) || (st = up2(G.dtdyo, d->dtdyo, KP)) ||
+      (st = up2(G.dlxu, d->dlxu, KU)) || (st = up2(G.dlyu, d->dlyu, KU)) ||
+      (st = up2(G.dtdxuo, d->dtdxuo, KU)) || (st = up2(G.dlxv, d->dlxv, KV)) ||
+      (st = up2(G.dlyv, d->dlyv, KV)) || (st = up2(G.dpye, d->dpye, KV)))
+    return st;
+
+  // Poisson tables (mo_petsc.f90:557-599)
+  std::vector<double> xu(n2, 0.), xp(n2, 0.), yv(n2, 0.), yp(n2, 0.);
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      const size_t s = L.at2(i, j);
+      xu[s] = 1.0 / d->dlxu[x.u2(i, j)];
+      xp[s] = 1.0 / d->dlxp[x.p2(i, j)];
+      yv[s] = 1.0 / d->dlyv[x.v2(i, j)];
+      yp[s] = 1.0 / d->dlyp[x.p2(i, j)];
+    }
+  std::vector<double> zwn(KE + 1), zpn(KE);
+  {
+    std::vector<double> zero(KE, 0.0);
+    for (int K = 1; K <= KE + 1; ++K) zwn[K - 1] = zw_ref(zero.data(), d->dzw, KE, K);
+    // nominal wet column: DDPO(K) = DZW(K) everywhere except the last level
+    std::vector<double> full(d->dzw, d->dzw + KE);
+    for (int K = 2; K <= KE; ++K) zwn[K - 1] = zw_ref(full.data(), d->dzw, KE, K);
+    zwn[0] = zw_ref(full.data(), d->dzw, KE, 1);
+    for (int K = 1; K <= KE; ++K) zpn[K - 1] = 1.0 / ((1.0 / zwn[K - 1] + 1.0 / zwn[K]) / 2.0);
+  }
+  std::vector<double> izn(KE);
+  for (int K = 1; K <= KE; ++K) izn[K - 1] = (1.0 / zwn[K - 1] + 1.0 / zwn[K]) / 2.0;
+  std::vector<double> zwa(n2, 0.), zwb(n2, 0.), zpa(n2, 0.), zpb(n2, 0.), zpc(n2, 0.);
+  std::vector<double> iza(n2, 0.), izb(n2, 0.), izc(n2, 0.);
+  std::vector<double> col(KE), zw(KE + 1), zp(KE), iz(KE);
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      const size_t s = L.at2(i, j);
+      for (int K = 1; K <= KE; ++K) col[K - 1] = d->ddpo[x.p3(i, j, K)];
+      for (int K = 1; K <= KE + 1; ++K) zw[K - 1] = zw_ref(col.data(), d->dzw, KE, K);
+      for (int K = 1; K <= KE; ++K) {
+        iz[K - 1] = (1.0 / zw[K - 1] + 1.0 / zw[K]) / 2.0;  // dddpo, mo_petsc.f90:588
+        zp[K - 1] = 1.0 / iz[K - 1];
+      }
+      const int kb = kbp[s];
+      if (kb >= 1) {
+        zwa[s] = zw[kb - 1];
+        zwb[s] = zw[kb];
+        if (kb >= 2) { zpa[s] = zp[kb - 2]; iza[s] = iz[kb - 2]; }
+        zpb[s] = zp[kb - 1];
+        izb[s] = iz[kb - 1];
+        if (kb + 1 <= KE) { zpc[s] = zp[kb]; izc[s] = iz[kb]; }
+      }
+      // the selection used on the device must reproduce every level exactly
+      for (int K = 1; K <= KE + 1; ++K) {
+        double sel = zwn[K - 1];
+        if (kb >= 1 && K == kb) sel = zwa[s];
+        if (kb >= 1 && K == kb + 1) sel = zwb[s];
+        if (sel != zw[K - 1]) return h->fail(ORCTM_E_GEOMETRY, "ZW table selection mismatch");
+      }
+      for (int K = 1; K <= KE; ++K) {
+        double sel = zpn[K - 1];
+        if (kb >= 1 && K == kb - 1) sel = zpa[s];
+        if (kb >= 1 && K == kb) sel = zpb[s];
+        if (kb >= 1 && K == kb + 1) sel = zpc[s];
+        if (sel != zp[K - 1]) return h->fail(ORCTM_E_GEOMETRY, "ZP table selection mismatch");
+        double isel = izn[K - 1];
+        if (kb >= 1 && K == kb - 1) isel = iza[s];
+        if (kb >= 1 && K == kb) isel = izb[s];
+        if (kb >= 1 && K == kb + 1) isel = izc[s];
+        if (isel != iz[K - 1]) return h->fail(ORCTM_E_GEOMETRY, "1/ZP table selection mismatch");
+      }
+    }
+  auto upv = [&](const double*& dst, const std::vector<double>& v) -> int {
+    double* p;
+    int s2;
+    if ((s2 = h->dev_alloc(&p, v.size()))) return s2;
+    ORCTM_CUDA_OK(cudaMemcpy(p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+    dst = p;
+    return ORCTM_OK;
+  };
+  PoissonGeo& P = h->P;
+  if ((st = upv(P.xu, xu)) || (st = upv(P.xp, xp)) || (st = upv(P.yv, yv)) ||
+      (st = upv(P.yp, yp)) || (st = upv(P.zwa, zwa)) || (st = upv(P.zwb, zwb)) ||
+      (st = upv(P.zpa, zpa)) || (st = upv(P.zpb, zpb)) || (st = upv(P.zpc, zpc)) ||
+      (st = upv(P.zwn, zwn)) || (st = upv(P.zpn, zpn)) || (st = upv(P.iza, iza)) ||
+      (st = upv(P.izb, izb)) || (st = upv(P.izc, izc)) || (st = upv(P.izn, izn)))
+    return st;
+
+  // state slots
+  h->slot.assign(kNumFixed + h->ntr, nullptr);
+  for (int f = 0; f < kNumFixed + h->ntr; ++f) {
+    if (f == ORCTM_F_ZO) continue;
+    double* p;
+    if ((st = h->alloc(&p))) return st;
+    h->slot[f] = p;
+  }
+  if ((st = h->dev_alloc(&h->zo, n2))) return st;
+
+  // solver scalars
+  const int nbx1 = (IE - 2 + 31) / 32, nby1 = (JE - 2 + 3) / 4;
+  const int nbx2 = (IE - 2 + 31) / 32, nby2 = JE - 2;  // column kernel, 32 or 64 wide
+  const int maxb = std::max(nbx1 * nby1, nbx2 * nby2);
+  if ((st = h->dev_alloc(&h->S, 1))) return st;
+  if ((st = h->dev_alloc(&h->partials, (size_t)4 * maxb))) return st;
+  ORCTM_CUDA_OK(cudaMallocHost(&h->hS, sizeof(SolverState)));
+  std::memset(h->hS, 0, sizeof(SolverState));
+  h->hS->max_blocks = maxb;
+  h->hS->partials = h->partials;
+  ORCTM_CUDA_OK(cudaMemcpy(h->S, h->hS, sizeof(SolverState), cudaMemcpyHostToDevice));
+  ORCTM_CUDA_OK(cudaEventCreate(&h->ev0));
+  ORCTM_CUDA_OK(cudaEventCreate(&h->ev1));
+  ORCTM_CUDA_OK(cudaEventCreate(&h->tm0));
+  ORCTM_CUDA_OK(cudaEventCreate(&h->tm1));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return ORCTM_OK;
+}
+
+int ensure_solver_buffers(orctm_handle* h) {
+  int st;
+  const size_t n = (size_t)h->L.n3();
+  if (!h->b) {
+    if ((st = h->dev_alloc(&h->b, n)) || (st = h->dev_alloc(&h->xs, n)) ||
+        (st = h->dev_alloc(&h->r, n)) || (st = h->dev_alloc(&h->z, n)) ||
+        (st = h->dev_alloc(&h->p0, n)) || (st = h->dev_alloc(&h->p1, n)) ||
+        (st = h->dev_alloc(&h->q, n)) || (st = h->dev_alloc(&h->d, n)) ||
+        (st = h->dev_alloc(&h->rw, n)))
+      return st;
+  }
+  if (h->solver_mode == ORCTM_SOLVER_FP32_REFINED && !h->r32) {
+    if ((st = h->dev_alloc(&h->r32b, n)) || (st = h->dev_alloc(&h->r32, n)) ||
+        (st = h->dev_alloc(&h->z32, n)) || (st = h->dev_alloc(&h->p32a, n)) ||
+        (st = h->dev_alloc(&h->p32b, n)) || (st = h->dev_alloc(&h->q32, n)) ||
+        (st = h->dev_alloc(&h->d32, n)))
+      return st;
+  }
+  return ORCTM_OK;
+}
+
+int read_state(orctm_handle* h) {
+  ORCTM_CUDA_OK(cudaMemcpyAsync(h->hS, h->S, sizeof(SolverState), cudaMemcpyDeviceToHost, h->stream));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return ORCTM_OK;
+}
+
+template <typename T, typename TX>
+int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* pa, T* pb, T* q,
+             int maxit, int* iters, int* conv) {
+  const Geo& G = h->G;
+  launch_pcg_col<T, TX>(G, h->P, h->S, init_mode, b, x, r, nullptr, nullptr, z, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  const int check = 8;
+  int it = 0;
+  T *pc = pa, *pn = pb;
+  for (; it < maxit; ++it) {
+    PROF(h, ORCTM_PROF_PCG_SPMV, (launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, h->stream)));
+    PROF(h, ORCTM_PROF_PCG_COL, (launch_pcg_col<T, TX>(G, h->P, h->S, 2, b, x, r, pn, q, z, h->stream)));
+    std::swap(pc, pn);
+    if ((it + 1) % check == 0 || it + 1 == maxit) {
+      int st;
+      ORCTM_CUDA_OK(cudaGetLastError());
+      if ((st = read_state(h))) return st;
+      if (h->hS->converged) break;
+    }
+  }
+  int st;
+  if ((st = read_state(h))) return st;
+  *iters = h->hS->iter;
+  *conv = h->hS->converged;
+  return ORCTM_OK;
+}
+
+// Solves A x = b (b in h->b, x in h->xs holding the warm start) by iterative
+// refinement: r = b - A x in double-double against the exact operator, then
+// a PCG correction on the row-scaled operator (FP64, or FP32 for the refined
+// form), until ||r||_2 <= rtol ||b||_2.
+int poisson_solve(orctm_handle* h, orctm_solve_stats* stats) {
+  const Geo& G = h->G;
+  int st;
+  orctm_solve_stats s{};
+  const bool f32 = h->solver_mode == ORCTM_SOLVER_FP32_REFINED;
+  const size_t n3 = (size_t)h->L.n3();
+  ORCTM_CUDA_OK(cudaEventRecord(h->ev0, h->stream));
+  int total = 0, outer = 0;
+  double prev = 1e300, rel = 0.0;
+  for (;; ++outer) {
+    launch_solver_reset(h->S, h->rtol, 0, h->stream);
+    PROF(h, ORCTM_PROF_RESID, launch_resid(G, h->P, h->S, h->b, h->xs, h->r, h->stream));
+    ORCTM_CUDA_OK(cudaGetLastError());
+    if ((st = read_state(h))) return st;
+    const double bnorm = std::sqrt(h->hS->res_bb);
+    if (bnorm == 0.0) {  // zero right-hand side: the solution is zero
+      ORCTM_CUDA_OK(cudaMemsetAsync(h->xs, 0, sizeof(double) * n3, h->stream));
+      rel = 0.0;
+      if (outer == 0) s.relres_initial = 0.0;
+      break;
+    }
+    rel = std::sqrt(h->hS->res_rr) / bnorm;
+    if (outer == 0) s.relres_initial = rel;
+    if (rel <= h->rtol || total >= h->maxit || outer >= 40 || !(rel < 0.5 * prev)) break;
+    prev = rel;
+    double inner = 0.3 * h->rtol / rel;
+    inner = std::min(0.5, std::max(inner, f32 ? 2e-5 : 1e-13));
+    int its = 0, conv = 0;
+    if (f32) {
+      launch_scale_to_f32(G, h->r, h->S, h->r32b, h->stream);
+      ORCTM_CUDA_OK(cudaMemsetAsync(h->d32, 0, sizeof(float) * n3, h->stream));
+      launch_solver_reset(h->S, inner, 0, h->stream);
+      if ((st = pcg_loop<float, float>(h, 1, h->r32b, h->d32, h->r32, h->z32, h->p32a, h->p32b,
+                                       h->q32, h->maxit - total, &its, &conv)))
+        return st;
+      launch_axpy_f32(G, h->d32, h->S, h->xs, h->stream);
+    } else {
+      ORCTM_CUDA_OK(cudaMemsetAsync(h->d, 0, sizeof(double) * n3, h->stream));
+      launch_solver_reset(h->S, inner, 0, h->stream);
+      if ((st = pcg_loop<double, double>(h, 1, h->r, h->d, h->rw, h->z, h->p0, h->p1, h->q,
+                                         h->maxit - total, &its, &conv)))
+        return st;
+      launch_axpy_f64(G, h->d, h->xs, h->stream);
+    }
+    ORCTM_CUDA_OK(cudaGetLastError());
+    total += its;
+  }
+  ORCTM_CUDA_OK(cudaEventRecord(h->ev1, h->stream));
+  ORCTM_CUDA_OK(cudaEventSynchronize(h->ev1));
+  s.relres = rel;
+  s.iterations = total;
+  s.outer_iterations = outer;
+  s.converged = rel <= h->rtol;
+  float ms = 0.f;
+  ORCTM_CUDA_OK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  s.solve_ms = ms;
+  if (stats) *stats = s;
+  return s.converged ? ORCTM_OK : ORCTM_E_NOT_CONVERGED;
+}
+
+// ------------------------------------------------------------- routines
+int r_ocadpo(orctm_handle* h, int n) {
+  int st;
+  double *out, *tA, *vA, *vB;
+  if ((st = h->alloc(&out)) || (st = h->alloc(&tA)) || (st = h->alloc(&vA)) || (st = h->alloc(&vB)))
+    return st;
+  const int f = ORCTM_F_THO + n;
+  PROF(h, ORCTM_PROF_OCADPO,
+       launch_ocadpo(h->G, h->slot[f], h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE],
+                     h->slot[ORCTM_F_WO], h->zo, out, tA, vA, vB, h->stream));
+  ORCTM_CUDA_OK(cudaGetLastError());
+  h->bind(f, out);
+  h->unref(tA); h->unref(vA); h->unref(vB);
+  return ORCTM_OK;
+}
+
+template <int WHICH>
+int r_momadv(orctm_handle* h) {
+  int st;
+  double *out, *tA, *vA, *vB;
+  if ((st = h->alloc(&out)) || (st = h->alloc(&tA)) || (st = h->alloc(&vA)) || (st = h->alloc(&vB)))
+    return st;
+  const double *uko = h->slot[ORCTM_F_UKO], *vke = h->slot[ORCTM_F_VKE], *wo = h->slot[ORCTM_F_WO];
+  int f;
+  if (WHICH == 0) {
+    f = ORCTM_F_UOO;
+    PROF(h, ORCTM_PROF_OCUAD, launch_ocuad(h->G, h->slot[f], uko, vke, wo, out, tA, vA, vB, h->stream));
+  } else if (WHICH == 1) {
+    f = ORCTM_F_VOE;
+    PROF(h, ORCTM_PROF_OCVAD, launch_ocvad(h->G, h->slot[f], uko, vke, wo, out, tA, vA, vB, h->stream));
+  } else {
+    f = ORCTM_F_WNO;
+    PROF(h, ORCTM_PROF_OCWAD, launch_ocwad(h->G, h->slot[f], uko, vke, wo, h->zo, out, tA, vA, vB, h->stream));
+  }
+  ORCTM_CUDA_OK(cudaGetLastError());
+  h->bind(f, out);
+  h->unref(tA); h->unref(vA); h->unref(vB);
+  return ORCTM_OK;
+}
+
+int r_octdiff(orctm_handle* h) {
+  int st;
+  const int ntr = h->ntr;
+  const double* in[kMaxTracers];
+  double* outv[kMaxTracers];
+  for (int n = 0; n < ntr; ++n) {
+    in[n] = h->slot[ORCTM_F_THO + n];
+    if ((st = h->alloc(&outv[n]))) return st;
+  }
+  PROF(h, ORCTM_PROF_OCTDIFF, launch_octdiff_vert(h->G, ntr, in, outv, h->slot[ORCTM_F_DVO], h->zo, h->stream));
+  ORCTM_CUDA_OK(cudaGetLastError());
+  for (int n = 0; n < ntr; ++n) h->bind(ORCTM_F_THO + n, outv[n]);
+  if (h->G.aulapts > h->G.almzer) {
+    double* lap;
+    if ((st = h->alloc(&lap))) return st;
+    for (int n = 0; n < ntr; ++n) {
+      double* out;
+      if ((st = h->alloc(&out))) return st;
+      PROF(h, ORCTM_PROF_OCTDIFF, launch_octdiff_bih(h->G, h->slot[ORCTM_F_THO + n], h->zo, lap, out, h->stream));
+      h->bind(ORCTM_F_THO + n, out);
+    }
+    ORCTM_CUDA_OK(cudaGetLastError());
+    h->unref(lap);
+  }
+  return ORCTM_OK;
+}
+
+int r_octimf(orctm_handle* h) {
+  h->alias(ORCTM_F_UKO, ORCTM_F_UOO);
+  h->alias(ORCTM_F_VKE, ORCTM_F_VOE);
+  return ORCTM_OK;
+}
+
+int r_ocvisc(orctm_handle* h) {
+  int st;
+  double *sp, *ukv, *vkv, *wnv, *u1, *v1, *w1, *uo, *vo, *wo;
+  if ((st = h->alloc(&sp)) || (st = h->alloc(&ukv)) || (st = h->alloc(&vkv)) ||
+      (st = h->alloc(&wnv)) || (st = h->alloc(&u1)) || (st = h->alloc(&v1)) ||
+      (st = h->alloc(&w1)) || (st = h->alloc(&uo)) || (st = h->alloc(&vo)) || (st = h->alloc(&wo)))
+    return st;
+  // the two 2D speed fields live in the first two planes of one scratch buffer
+  PROF(h, ORCTM_PROF_OCVISC,
+       launch_ocvisc(h->G, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE], h->slot[ORCTM_F_WNO],
+                     h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], h->slot[ORCTM_F_AVO], sp,
+                     sp + h->L.plane, ukv, vkv, wnv, u1, v1, w1, uo, vo, wo, h->stream));
+  ORCTM_CUDA_OK(cudaGetLastError());
+  h->bind(ORCTM_F_UOO, uo);
+  h->bind(ORCTM_F_VOE, vo);
+  h->bind(ORCTM_F_WNO, wo);
+  h->unref(sp); h->unref(ukv); h->unref(vkv); h->unref(wnv);
+  h->unref(u1); h->unref(v1); h->unref(w1);
+  return r_octimf(h);  // ocvisc.f90:767
+}
+
+int r_ocvtot_nh(orctm_handle* h, orctm_solve_stats* stats) {
+  int st;
+  if ((st = ensure_solver_buffers(h))) return st;
+  PROF(h, ORCTM_PROF_NH_RHS,
+       launch_nh_rhs(h->G, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_UOO_1], h->slot[ORCTM_F_VOE],
+                     h->slot[ORCTM_F_VOE_1], h->slot[ORCTM_F_WNO], h->slot[ORCTM_F_WNO_1], h->zo,
+                     h->b, h->stream));
+  // warm start from the previous PNH (KSPSetInitialGuessNonzero, mo_petsc.f90:232)
+  ORCTM_CUDA_OK(cudaMemcpyAsync(h->xs, h->slot[ORCTM_F_PNH], sizeof(double) * h->L.n3(),
+                                cudaMemcpyDeviceToDevice, h->stream));
+  ORCTM_CUDA_OK(cudaGetLastError());
+  const int solve_status = poisson_solve(h, stats);
+  if (solve_status != ORCTM_OK && solve_status != ORCTM_E_NOT_CONVERGED) return solve_status;
+  double *pnh, *uo, *vo, *wn;
+  if ((st = h->alloc(&pnh)) || (st = h->alloc(&uo)) || (st = h->alloc(&vo)) || (st = h->alloc(&wn)))
+    return st;
+  PROF(h, ORCTM_PROF_NH_POST,
+       launch_nh_post(h->G, h->xs, h->slot[ORCTM_F_PNH], pnh, h->slot[ORCTM_F_UOO],
+                      h->slot[ORCTM_F_VOE], uo, vo, wn, h->stream));
+  ORCTM_CUDA_OK(cudaGetLastError());
+  h->bind(ORCTM_F_PNH, pnh);
+  h->bind(ORCTM_F_UOO, uo);
+  h->bind(ORCTM_F_VOE, vo);
+  h->bind(ORCTM_F_WNO, wn);
+  // UOO_1 <- UOO, VOE_1 <- VOE, WNO_1 <- WNO, WO <- WNO (ocvtot_nh.f90:238-255)
+  h->alias(ORCTM_F_UOO_1, ORCTM_F_UOO);
+  h->alias(ORCTM_F_VOE_1, ORCTM_F_VOE);
+  h->alias(ORCTM_F_WNO_1, ORCTM_F_WNO);
+  h->alias(ORCTM_F_WO, ORCTM_F_WNO);
+  return solve_status;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int orctm_abi_version(void) { return ORCTM_ABI_VERSION; }
+
+const char* orctm_status_string(int s) {
+  switch (s) {
+    case ORCTM_OK: return "ok";
+    case ORCTM_E_ARG: return "invalid argument";
+    case ORCTM_E_CUDA: return "CUDA runtime error";
+    case ORCTM_E_NOMEM: return "device memory exhausted";
+    case ORCTM_E_NOT_CONVERGED: return "Poisson solve did not reach the residual target";
+    case ORCTM_E_GEOMETRY: return "geometry is not of the BODEN form";
+    case ORCTM_E_UNSUPPORTED: return "option outside the implemented path";
+    case ORCTM_E_NODEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* orctm_last_error(const orctm_handle* h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int orctm_destroy(orctm_handle* h) {
+  if (!h) return ORCTM_E_ARG;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  std::vector<double*> all(h->free_.begin(), h->free_.end());
+  for (auto& kv : h->refs) all.push_back(kv.first);
+  std::sort(all.begin(), all.end());
+  all.erase(std::unique(all.begin(), all.end()), all.end());
+  for (double* p : all) cudaFree(p);
+  for (void* p : h->owned) cudaFree(p);
+  if (h->hS) cudaFreeHost(h->hS);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int k = 0; k < ORCTM_PROF_KINDS; ++k)
+    for (auto& pr : h->prof_pairs[k]) {
+      h->ev_pool.push_back(pr.first);
+      h->ev_pool.push_back(pr.second);
+    }
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  if (h->tm0) cudaEventDestroy(h->tm0);
+  if (h->tm1) cudaEventDestroy(h->tm1);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return ORCTM_OK;
+}
+
+int orctm_create(const orctm_desc* d, orctm_handle** out) {
+  g_create_error.clear();
+  if (!d || !out) return ORCTM_E_ARG;
+  *out = nullptr;
+  auto bad = [&](int st, const char* m) {
+    g_create_error = m;
+    return st;
+  };
+  if (d->ie < 4 || d->je < 3 || d->ke < 2 || d->ke > kMaxKe) return bad(ORCTM_E_ARG, "grid size out of range");
+  if (d->i_start != 0 || d->j_start != 0) return bad(ORCTM_E_UNSUPPORTED, "only single-rank domains (I_start = J_start = 0)");
+  if (d->ntracers < 2 || d->ntracers > kMaxTracers) return bad(ORCTM_E_ARG, "ntracers must be in [2, 8]");
+  if (!(d->dt > 0)) return bad(ORCTM_E_ARG, "dt must be positive");
+  if (d->ah00 > d->almzer) return bad(ORCTM_E_UNSUPPORTED, "harmonic tracer diffusion (AH00 > ALMZER) is not implemented");
+  const void* req[] = {d->dzw, d->di, d->dlxp, d->dlyp, d->dtdxpo, d->dtdyo, d->dlxu, d->dlyu,
+                       d->dtdxuo, d->dlxv, d->dlyv, d->dpye, d->ddpo, d->weto, d->dduo,
+                       d->amsuo, d->ddue, d->amsue};
+  for (const void* p : req)
+    if (!p) return bad(ORCTM_E_ARG, "missing geometry array");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bad(ORCTM_E_NODEVICE, "no CUDA device");
+  if (d->device < 0 || d->device >= ndev) return bad(ORCTM_E_ARG, "device ordinal out of range");
+  orctm_handle* h = new orctm_handle();
+  h->device = d->device;
+  int st = cuda_status(cudaSetDevice(h->device));
+  if (!st) st = cuda_status(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  if (!st) st = setup(h, d);
+  if (st) {
+    g_create_error = h->err.empty() ? orctm_status_string(st) : h->err;
+    orctm_destroy(h);
+    return st;
+  }
+  *out = h;
+  return ORCTM_OK;
+}
+
+int orctm_field_size(const orctm_handle* h, int f, size_t* n) {
+  if (!h || !n || f < 0 || f >= kNumFixed + h->ntr) return ORCTM_E_ARG;
+  int i0, ni, j0, nj, nk;
+  extent(h, f, i0, ni, j0, nj, nk);
+  *n = (size_t)ni * nj * nk;
+  return ORCTM_OK;
+}
+
+int orctm_upload(orctm_handle* h, int f, const double* host, size_t n) {
+  size_t want;
+  if (!host || orctm_field_size(h, f, &want) != ORCTM_OK || n != want) return ORCTM_E_ARG;
+  cudaSetDevice(h->device);
+  int i0, ni, j0, nj, nk;
+  extent(h, f, i0, ni, j0, nj, nk);
+  double* dst;
+  if (f == ORCTM_F_ZO) {
+    dst = h->zo;
+  } else {
+    int st;
+    if (h->refs[h->slot[f]] > 1) {  // shared with another field: copy on write
+      double* p;
+      if ((st = h->alloc(&p))) return st;
+      h->bind(f, p);
+    }
+    dst = h->slot[f];
+  }
+  for (int k = 0; k < nk; ++k)
+    ORCTM_CUDA_OK(cudaMemcpy2DAsync(dst + h->L.at(i0, j0, k), sizeof(double) * h->L.P,
+                                    host + (size_t)k * ni * nj, sizeof(double) * ni,
+                                    sizeof(double) * ni, nj, cudaMemcpyHostToDevice, h->stream));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return ORCTM_OK;
+}
+
+int orctm_download(orctm_handle* h, int f, double* host, size_t n) {
+  size_t want;
+  if (!host || orctm_field_size(h, f, &want) != ORCTM_OK || n != want) return ORCTM_E_ARG;
+  cudaSetDevice(h->device);
+  int i0, ni, j0, nj, nk;
+  extent(h, f, i0, ni, j0, nj, nk);
+  const double* src = f == ORCTM_F_ZO ? h->zo : h->slot[f];
+  for (int k = 0; k < nk; ++k)
+    ORCTM_CUDA_OK(cudaMemcpy2DAsync(host + (size_t)k * ni * nj, sizeof(double) * ni,
+                                    src + h->L.at(i0, j0, k), sizeof(double) * h->L.P,
+                                    sizeof(double) * ni, nj, cudaMemcpyDeviceToHost, h->stream));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return ORCTM_OK;
+}
+
+#define ORCTM_ENTER(h)             \
+  if (!(h)) return ORCTM_E_ARG;    \
+  cudaSetDevice((h)->device)
+
+int orctm_ocuad(orctm_handle* h) { ORCTM_ENTER(h); return r_momadv<0>(h); }
+int orctm_ocvad(orctm_handle* h) { ORCTM_ENTER(h); return r_momadv<1>(h); }
+int orctm_ocwad(orctm_handle* h) { ORCTM_ENTER(h); return r_momadv<2>(h); }
+int orctm_ocadpo(orctm_handle* h, int tracer) {
+  ORCTM_ENTER(h);
+  if (tracer < 0 || tracer >= h->ntr) return ORCTM_E_ARG;
+  return r_ocadpo(h, tracer);
+}
+int orctm_octdiff(orctm_handle* h) { ORCTM_ENTER(h); return r_octdiff(h); }
+int orctm_octimf(orctm_handle* h) { ORCTM_ENTER(h); return r_octimf(h); }
+int orctm_ocvisc(orctm_handle* h) { ORCTM_ENTER(h); return r_ocvisc(h); }
+int orctm_ocvtot_nh(orctm_handle* h, orctm_solve_stats* s) { ORCTM_ENTER(h); return r_ocvtot_nh(h, s); }
+
+int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* s) {
+  ORCTM_ENTER(h);
+  int st;
+  if ((st = r_momadv<0>(h)) || (st = r_momadv<1>(h)) || (st = r_momadv<2>(h))) return st;
+  for (int n = 0; n < h->ntr; ++n)
+    if ((st = r_ocadpo(h, n))) return st;
+  if ((st = r_octdiff(h)) || (st = r_octimf(h)) || (st = r_ocvisc(h))) return st;
+  const int ns = r_ocvtot_nh(h, s);
+  if (ns != ORCTM_OK && ns != ORCTM_E_NOT_CONVERGED) return ns;
+  r_octimf(h);
+  return ns;
+}
+
+int orctm_set_solver(orctm_handle* h, int mode, double rtol, int maxit) {
+  if (!h || (mode != ORCTM_SOLVER_FP64 && mode != ORCTM_SOLVER_FP32_REFINED) || !(rtol > 0) ||
+      maxit < 1)
+    return ORCTM_E_ARG;
+  h->solver_mode = mode;
+  h->rtol = rtol;
+  h->maxit = maxit;
+  return ORCTM_OK;
+}
+
+int orctm_synchronize(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+int orctm_timer_start(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  ORCTM_CUDA_OK(cudaEventRecord(h->tm0, h->stream));
+  return ORCTM_OK;
+}
+
+int orctm_timer_stop(orctm_handle* h, double* ms) {
+  ORCTM_ENTER(h);
+  if (!ms) return ORCTM_E_ARG;
+  ORCTM_CUDA_OK(cudaEventRecord(h->tm1, h->stream));
+  ORCTM_CUDA_OK(cudaEventSynchronize(h->tm1));
+  float f = 0.f;
+  ORCTM_CUDA_OK(cudaEventElapsedTime(&f, h->tm0, h->tm1));
+  *ms = f;
+  return ORCTM_OK;
+}
+
+int orctm_set_profiling(orctm_handle* h, int on) {
+  ORCTM_ENTER(h);
+  h->prof_flush();
+  for (int k = 0; k < ORCTM_PROF_KINDS; ++k) {
+    h->prof_ms[k] = 0.0;
+    h->prof_n[k] = 0;
+  }
+  h->prof = on != 0;
+  return ORCTM_OK;
+}
+
+int orctm_profile_get(orctm_handle* h, int kind, long long* launches, double* total_ms) {
+  ORCTM_ENTER(h);
+  if (kind < 0 || kind >= ORCTM_PROF_KINDS || !launches || !total_ms) return ORCTM_E_ARG;
+  h->prof_flush();
+  *launches = h->prof_n[kind];
+  *total_ms = h->prof_ms[kind];
+  return ORCTM_OK;
+}
+
+unsigned long long orctm_kernel_launches(void) { return launch_count(); }
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// Kernel launchers shared between the kernel files and the handle code.
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace orctm {
+
+// Vertical factors and reciprocal metrics of the matrix-free Poisson operator.
+struct PoissonGeo {
+  const double *xu, *xp, *yv, *yp;             // 1/DLXU, 1/DLXP, 1/DLYV, 1/DLYP (2D)
+  const double *zwa, *zwb;                     // ZW at levels kb and kb+1 (2D)
+  const double *zpa, *zpb, *zpc;               // ZP at levels kb-1, kb, kb+1 (2D)
+  const double *zwn, *zpn;                     // ZW(K), K=1..KE+1 and ZP(K), K=1..KE elsewhere
+  const double *iza, *izb, *izc, *izn;         // 1/ZP = (1/ZW(K) + 1/ZW(K+1))/2, same selection
+};
+
+// Device-resident scalars of one Krylov solve.
+struct SolverState {
+  double rho, beta, alpha, pq, rr, bb, tol, res_rr, res_bb;
+  int converged;  // 0 running, 1 converged, 2 NaN, 3 breakdown
+  int iter;
+  unsigned ticket;
+  int max_blocks;
+  double* partials;  // [4 * max_blocks]
+};
+
+// advect.cu
+void launch_ocadpo(const Geo& G, const double* T, const double* uko, const double* vke,
+                   const double* wo, const double* zo, double* out, double* tA, double* vA,
+                   double* vB, cudaStream_t st);
+void launch_ocuad(const Geo& G, const double* T, const double* uko, const double* vke,
+                  const double* wo, double* out, double* tA, double* vA, double* vB,
+                  cudaStream_t st);
+void launch_ocvad(const Geo& G, const double* T, const double* uko, const double* vke,
+                  const double* wo, double* out, double* tA, double* vA, double* vB,
+                  cudaStream_t st);
+void launch_ocwad(const Geo& G, const double* T, const double* uko, const double* vke,
+                  const double* wo, const double* zo, double* out, double* tA, double* vA,
+                  double* vB, cudaStream_t st);
+
+// diffuse.cu
+void launch_octdiff_vert(const Geo& G, int ntr, const double* const* in, double* const* out,
+                         const double* dvo, const double* zo, cudaStream_t st);
+void launch_octdiff_bih(const Geo& G, const double* T, const double* zo, double* lap, double* out,
+                        cudaStream_t st);
+void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const double* wno,
+                   const double* uko, const double* vke, const double* avo, double* spu,
+                   double* spv, double* ukv, double* vkv, double* wnv, double* u1, double* v1,
+                   double* w1, double* uo, double* vo, double* wo, cudaStream_t st);
+
+// nh.cu
+void launch_nh_rhs(const Geo& G, const double* uoo, const double* uoo1, const double* voe,
+                   const double* voe1, const double* wno, const double* wno1, const double* zo,
+                   double* b, cudaStream_t st);
+size_t pcg_col_smem(const Geo& G, bool f32);
+template <typename T, typename TX>
+void launch_pcg_col(const Geo& G, const PoissonGeo& P, SolverState* S, int mode, const T* b, TX* x,
+                    T* r, const T* p, const T* q, T* z, cudaStream_t st);
+template <typename T>
+void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
+                     T* pnew, T* q, int first, cudaStream_t st);
+void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b,
+                  const double* x, double* r, cudaStream_t st);
+void launch_axpy_f64(const Geo& G, const double* d, double* x, cudaStream_t st);
+void launch_scale_to_f32(const Geo& G, const double* r, const SolverState* S, float* r32,
+                         cudaStream_t st);
+void launch_axpy_f32(const Geo& G, const float* d, const SolverState* S, double* x,
+                     cudaStream_t st);
+void launch_solver_reset(SolverState* S, double tol, int keep_bb, cudaStream_t st);
+void launch_nh_post(const Geo& G, const double* x, const double* pold, double* pnh,
+                    const double* uoo, const double* voe, double* uo, double* vo, double* wno,
+                    cudaStream_t st);
+
+int cuda_status(cudaError_t e);
+
+// number of kernels launched by this library (all handles, this process)
+void count_launch();
+unsigned long long launch_count();
+
+}  // namespace orctm
