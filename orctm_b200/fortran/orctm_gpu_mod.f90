@@ -1,0 +1,99 @@
+! ISO_C_BINDING interface to liborctm_gpu.so (include/orctm_gpu.h) for the
+! ORCTM Fortran host.  The reference's subroutines keep their names; their
+! bodies become the calls shown in INTEGRATION.md.  Compile with the model
+! (-fdefault-real-8 / -r8 as the model itself) and link -lorctm_gpu -lcudart.
+module orctm_gpu_mod
+  use, intrinsic :: iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: ORCTM_OK = 0, ORCTM_E_NOT_CONVERGED = -4
+  integer(c_int), parameter :: ORCTM_F_UOO = 0, ORCTM_F_VOE = 1, ORCTM_F_WNO = 2, &
+       ORCTM_F_UKO = 3, ORCTM_F_VKE = 4, ORCTM_F_WO = 5, ORCTM_F_UOO_1 = 6, &
+       ORCTM_F_VOE_1 = 7, ORCTM_F_WNO_1 = 8, ORCTM_F_PNH = 9, ORCTM_F_ZO = 10, &
+       ORCTM_F_DVO = 11, ORCTM_F_AVO = 12, ORCTM_F_THO = 13, ORCTM_F_SAO = 14
+
+  type, bind(c) :: orctm_desc
+     integer(c_int) :: ie, je, ke, i_start, j_start, ntracers
+     integer(c_int) :: ob_west, ob_east, ob_north, ob_south
+     real(c_double) :: dt, almzer, aulapts, aulapuv, ah00
+     type(c_ptr) :: dzw, di
+     type(c_ptr) :: dlxp, dlyp, dtdxpo, dtdyo
+     type(c_ptr) :: dlxu, dlyu, dtdxuo
+     type(c_ptr) :: dlxv, dlyv, dpye
+     type(c_ptr) :: ddpo, weto, dduo, amsuo, ddue, amsue
+     integer(c_int) :: device
+  end type orctm_desc
+
+  type, bind(c) :: orctm_solve_stats
+     integer(c_int) :: iterations, outer_iterations, converged
+     real(c_double) :: relres, relres_initial, solve_ms
+  end type orctm_solve_stats
+
+  interface
+     integer(c_int) function orctm_create(desc, h) bind(c, name="orctm_create")
+       import :: c_int, c_ptr, orctm_desc
+       type(orctm_desc), intent(in) :: desc
+       type(c_ptr), intent(out) :: h
+     end function
+     integer(c_int) function orctm_destroy(h) bind(c, name="orctm_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_upload(h, field, host, n) bind(c, name="orctm_upload")
+       import :: c_int, c_ptr, c_size_t
+       type(c_ptr), value :: h
+       integer(c_int), value :: field
+       type(c_ptr), value :: host
+       integer(c_size_t), value :: n
+     end function
+     integer(c_int) function orctm_download(h, field, host, n) bind(c, name="orctm_download")
+       import :: c_int, c_ptr, c_size_t
+       type(c_ptr), value :: h
+       integer(c_int), value :: field
+       type(c_ptr), value :: host
+       integer(c_size_t), value :: n
+     end function
+     integer(c_int) function orctm_ocuad(h) bind(c, name="orctm_ocuad")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocvad(h) bind(c, name="orctm_ocvad")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocwad(h) bind(c, name="orctm_ocwad")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocadpo(h, tracer) bind(c, name="orctm_ocadpo")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: tracer
+     end function
+     integer(c_int) function orctm_octdiff(h) bind(c, name="orctm_octdiff")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_octimf(h) bind(c, name="orctm_octimf")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocvisc(h) bind(c, name="orctm_ocvisc")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocvtot_nh(h, stats) bind(c, name="orctm_ocvtot_nh")
+       import :: c_int, c_ptr, orctm_solve_stats
+       type(c_ptr), value :: h
+       type(orctm_solve_stats), intent(out) :: stats
+     end function
+     integer(c_int) function orctm_set_solver(h, mode, rtol, maxit) bind(c, name="orctm_set_solver")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: mode, maxit
+       real(c_double), value :: rtol
+     end function
+  end interface
+
+  type(c_ptr), save :: orctm_h = c_null_ptr
+end module orctm_gpu_mod
