@@ -65,6 +65,7 @@ extern "C" {
 #define ORCTM_E_GEOMETRY (-5)      /* masks/thicknesses not of the BODEN form */
 #define ORCTM_E_UNSUPPORTED (-6)   /* option outside the restated path */
 #define ORCTM_E_NODEVICE (-7)      /* no usable CUDA device */
+#define ORCTM_E_TOO_LARGE (-8)     /* size beyond orctm_octdiff_noalloc's fixed scratch */
 
 /* field ids for orctm_upload / orctm_download (MO_COMMO1 array names) */
 enum {
@@ -176,6 +177,42 @@ int orctm_build_grid(int ie, int je, int ke, double dt, const double* dzw, doubl
                      double* dtdyo, double* dtdxuo, double* dpyo, double* dtdxue, double* dpye,
                      double* ddpo, double* weto, double* dduo, double* amsuo, double* ddue,
                      double* amsue);
+
+/* ---- Scratch-free tracer diffusion -------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory -- code that runs while a CUDA graph is being
+ * captured, hosts whose device memory belongs to another runtime or pool (an
+ * OpenACC / OpenMP-offload Fortran model, a framework allocator), loops that
+ * must not block on the driver's allocator.  It computes OCTDIFF_BASE +
+ * OCTDIFF_TS (implicit vertical diffusion, then the biharmonic operator) for
+ * ONE tracer on caller-owned device arrays in the reference's Fortran
+ * layouts, without a handle and without allocating anything.
+ *
+ * Its two scratch fields live in a fixed array compiled into the library
+ * (32 MiB, held on every GPU that loads the library until the process
+ * exits), which limits IE*JE*KE to 2,097,152 cells; larger grids return
+ * ORCTM_E_TOO_LARGE.  The first call on each device looks up that array's
+ * device address (cudaGetSymbolAddress) with the device current: make that
+ * first call before any stream capture.  All calls share the array and it
+ * keeps the last call's contents; every value a call reads is written earlier
+ * in the same call.  Calls that overlap on the GPU race on the array: order
+ * them on one stream.  The kernels are enqueued on args->stream and the call
+ * returns without waiting for them. */
+typedef struct orctm_octdiff_noalloc_args {
+  int ie, je, ke;                 /* IE, JE, KE including halos */
+  double dt, almzer, aulapts, ah00; /* as in orctm_desc; ah00 must be <= almzer */
+  const double* tracer_in;        /* device, p-points IE*JE*KE */
+  double* tracer_out;             /* device, p-points, a different buffer */
+  const double* dvo;              /* device, w-points IE*JE*(KE+1) */
+  const double *ddpo, *weto;      /* device, p-points IE*JE*KE */
+  const double *di, *dzw;         /* device, DI(KE+1), DZW(KE) */
+  const double *dlxp, *dlyp;      /* device, 2D p-points IE*JE */
+  const double *dlxu, *dlyu;      /* device, 2D u-points (IE+1)*JE */
+  const double *dlxv, *dlyv;      /* device, 2D v-points IE*(JE+1) */
+  const double* zo;               /* device, 2D p-points IE*JE */
+  void* stream;                   /* cudaStream_t; NULL = legacy default stream */
+} orctm_octdiff_noalloc_args;
+int orctm_octdiff_noalloc(const orctm_octdiff_noalloc_args* args);
 
 #ifdef __cplusplus
 }

@@ -715,6 +715,7 @@ const char* orctm_status_string(int s) {
     case ORCTM_E_GEOMETRY: return "geometry is not of the BODEN form";
     case ORCTM_E_UNSUPPORTED: return "option outside the implemented path";
     case ORCTM_E_NODEVICE: return "no usable CUDA device";
+    case ORCTM_E_TOO_LARGE: return "grid larger than the scratch-free entry point's limit";
     default: return "unknown status";
   }
 }
