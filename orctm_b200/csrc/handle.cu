@@ -435,10 +435,19 @@ int setup(orctm_handle* h, const orctm_desc* d) {
   }
   if ((st = h->dev_alloc(&h->zo, n2))) return st;
 
+  // pivots of the preconditioner (the operator is constant: factorise once)
+  {
+    double* d64;
+    float* d32;
+    if ((st = h->dev_alloc(&d64, (size_t)L.n3())) || (st = h->dev_alloc(&d32, (size_t)L.n3())))
+      return st;
+    P.dinv64 = d64;
+    P.dinv32 = d32;
+    launch_factor(G, P, d64, d32, h->stream);
+    ORCTM_CUDA_OK(cudaGetLastError());
+  }
   // solver scalars
-  const int nbx1 = (IE - 2 + 31) / 32, nby1 = (JE - 2 + 3) / 4;
-  const int nbx2 = (IE - 2 + 31) / 32, nby2 = JE - 2;  // column kernel, 32 or 64 wide
-  const int maxb = std::max(nbx1 * nby1, nbx2 * nby2);
+  const int maxb = (int)solver_max_blocks(G);
   if ((st = h->dev_alloc(&h->S, 1))) return st;
   if ((st = h->dev_alloc(&h->partials, (size_t)4 * maxb))) return st;
   ORCTM_CUDA_OK(cudaMallocHost(&h->hS, sizeof(SolverState)));

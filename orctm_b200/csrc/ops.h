@@ -14,6 +14,8 @@ struct PoissonGeo {
   const double *zpa, *zpb, *zpc;               // ZP at levels kb-1, kb, kb+1 (2D)
   const double *zwn, *zpn;                     // ZW(K), K=1..KE+1 and ZP(K), K=1..KE elsewhere
   const double *iza, *izb, *izc, *izn;         // 1/ZP = (1/ZW(K) + 1/ZW(K+1))/2, same selection
+  const double* dinv64;                        // pivots 1/d'(K) of the column tridiagonal of B (3D)
+  const float* dinv32;                         // the same rounded to FP32
 };
 
 // Device-resident scalars of one Krylov solve.
@@ -54,7 +56,10 @@ void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const dou
 void launch_nh_rhs(const Geo& G, const double* uoo, const double* uoo1, const double* voe,
                    const double* voe1, const double* wno, const double* wno1, const double* zo,
                    double* b, cudaStream_t st);
-size_t pcg_col_smem(const Geo& G, bool f32);
+// poisson.cu
+void launch_factor(const Geo& G, const PoissonGeo& P, double* dinv64, float* dinv32,
+                   cudaStream_t st);
+size_t solver_max_blocks(const Geo& G);
 template <typename T, typename TX>
 void launch_pcg_col(const Geo& G, const PoissonGeo& P, SolverState* S, int mode, const T* b, TX* x,
                     T* r, const T* p, const T* q, T* z, cudaStream_t st);
