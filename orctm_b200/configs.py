@@ -229,6 +229,9 @@ def initial_state(inst: dict, cfl: float | None = None) -> dict:
     dvo *= 1.0 + 0.1 * g.uniform(-1, 1, (ie, je, kep))
     avo = np.asfortranarray(np.broadcast_to(2e-4 + 5e-3 * np.exp(-lev / 5.0), (ie, je, kep)).copy())
     avo *= 1.0 + 0.1 * g.uniform(-1, 1, (ie, je, kep))
+    # OCTHER masks both with WETO (octher.f90:382-393) and zeroes DVO(KEP)
+    dvo[:, :, :ke] *= inst["weto"]
+    avo[:, :, :ke] *= inst["weto"]
     dvo[:, :, 0] = 0.0
     dvo[:, :, -1] = 0.0
     return {

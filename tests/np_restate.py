@@ -1,0 +1,172 @@
+"""Independent numpy restatements used to cross-check the C oracle.
+
+Written from the reference Fortran, not from oracle/orctm_oracle.c, and
+vectorised over (i, j): OCADPO (ocadpo.f90:94-348) and the operator of
+compute_matrix (mo_petsc.f90:543-782).  Test infrastructure only.
+Arrays are 0-based numpy views of the Fortran arrays: p-point index
+i-1 <-> Fortran I, u-point index i <-> Fortran I (I_start = 0).
+"""
+import numpy as np
+import scipy.sparse as sp
+
+
+def ocadpo(g, trf, uko, vke, wo, zo):
+    """Returns the advected tracer (float64, same layout as trf)."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    dt = g["dt"]
+    weto, ddpo = g["weto"], g["ddpo"]
+    dlxp, dlyp = g["dlxp"], g["dlyp"]
+    dduo, dlyu, ddue, dlxv = g["dduo"], g["dlyu"], g["ddue"], g["dlxv"]
+    T = trf.copy()
+    s1o = weto * dlxp[:, :, None] * dlyp[:, :, None] * ddpo
+    s1o[:, :, 0] = s1o[:, :, 0] + dlxp * dlyp * weto[:, :, 0] * (zo - wo[:, :, 0] * dt)
+    I = slice(1, ie - 1)
+    J = slice(1, je - 1)
+    # vertical
+    trp = np.zeros((ie, je, ke + 1))   # index k-1 <-> TRP(K), K = 1..KEP
+    wtp = np.zeros((ie, je, ke + 1))
+    trm = np.zeros((ie, je, ke + 1))   # index k   <-> TRM(K), K = 0..KE
+    wtm = np.zeros((ie, je, ke + 1))
+    for k in range(ke):
+        kup, klo = max(k - 1, 0), min(k + 1, ke - 1)
+        t, tu, tl = T[I, J, k], T[I, J, kup], T[I, J, klo]
+        abl = np.abs(tu - tl)
+        zwabl = np.abs(tu + tl - 2. * t)
+        c = 0.5 * dt * dlyp[I, J] * dlxp[I, J]
+        up = c * (wo[I, J, k] + np.abs(wo[I, J, k]))
+        um = c * (np.abs(wo[I, J, k + 1]) - wo[I, J, k + 1])
+        scha = np.where(0. > (abl - zwabl) / (abl + 1e-20), 0., (abl - zwabl) / (abl + 1e-20))
+        x = scha * s1o[I, J, k] / (up + um + 1e-20)
+        w = weto[I, J, klo]
+        sch = np.where(x < w, x, w)
+        if k == 0 or k == ke - 1:
+            sch = np.zeros_like(sch)
+        schi = 1. - sch
+        trp[I, J, k] = up * (schi * t + sch * 0.5 * (t + tu))
+        trm[I, J, k + 1] = um * (schi * t + sch * 0.5 * (t + tl))
+        wtp[I, J, k] = up
+        wtm[I, J, k + 1] = um
+    new = T.copy()
+    for k in range(ke):
+        m = weto[I, J, k] > 0.5
+        rn = s1o[I, J, k] + wtp[I, J, k + 1] - wtp[I, J, k] - wtm[I, J, k + 1] + wtm[I, J, k]
+        t1 = (T[I, J, k] * s1o[I, J, k] + trp[I, J, k + 1] - trp[I, J, k] - trm[I, J, k + 1]
+              + trm[I, J, k]) / np.where(m, rn, 1.0)
+        new[I, J, k] = np.where(m, t1, T[I, J, k])
+        s1o[I, J, k] = np.where(m, rn, s1o[I, J, k])
+    T = new
+    # x: face arrays indexed by p-index
+    for direction in ("x", "y"):
+        trp = np.zeros((ie, je, ke))
+        trm = np.zeros((ie, je, ke))
+        wtp = np.zeros((ie, je, ke))
+        wtm = np.zeros((ie, je, ke))
+        if direction == "x":
+            t, tp_, tm_ = T[I, J, :], T[2:, J, :], T[:-2, J, :]   # tp_: I+1, tm_: I-1
+            u0 = uko[2:ie, J, :]        # u-point I   (u index I)
+            um1 = uko[1:ie - 1, J, :]   # u-point I-1
+            up = 0.5 * dt * dduo[2:ie, J, :] * dlyu[2:ie, J][:, :, None] * (u0 + np.abs(u0))
+            um = 0.5 * dt * dduo[1:ie - 1, J, :] * (np.abs(um1) - um1) * dlyu[1:ie - 1, J][:, :, None]
+            mask = weto[I, J, :] * weto[2:, J, :] * weto[:-2, J, :]
+        else:
+            t, tp_, tm_ = T[I, J, :], T[I, :-2, :], T[I, 2:, :]   # tp_: J-1, tm_: J+1
+            vn = vke[I, 1:je - 1, :]    # v-point J-1 (v index J-1)
+            vs = vke[I, 2:je, :]        # v-point J
+            up = 0.5 * dt * ddue[I, 1:je - 1, :] * dlxv[I, 1:je - 1][:, :, None] * (vn + np.abs(vn))
+            um = 0.5 * dt * ddue[I, 2:je, :] * dlxv[I, 2:je][:, :, None] * (np.abs(vs) - vs)
+            mask = weto[I, J, :] * weto[I, :-2, :] * weto[I, 2:, :]
+        abl = np.abs(tp_ - tm_)
+        zwabl = np.abs(tp_ + tm_ - 2. * t)
+        q = (abl - zwabl) / (abl + 1e-20)
+        if direction == "x":
+            scha = np.where(0. > q, 0., q) * weto[I, J, :] * weto[2:, J, :] * weto[:-2, J, :]
+        else:
+            scha = np.where(0. > q, 0., q) * weto[I, J, :] * weto[I, :-2, :] * weto[I, 2:, :]
+        x = scha * s1o[I, J, :] / (up + um + 1e-20)
+        sch = np.where(x < 1., x, 1.)
+        schi = 1. - sch
+        trp[I, J, :] = up * (schi * t + sch * 0.5 * (t + tp_))
+        trm[I, J, :] = um * (schi * t + sch * 0.5 * (t + tm_))
+        wtp[I, J, :] = up
+        wtm[I, J, :] = um
+        if direction == "x":
+            rn = s1o[I, J] + wtp[:-2, J] - wtp[I, J] - wtm[I, J] + wtm[2:, J]
+            t1 = (T[I, J] * s1o[I, J] + trp[:-2, J] - trp[I, J] - trm[I, J] + trm[2:, J])
+        else:
+            rn = s1o[I, J] + wtp[I, 2:] - wtp[I, J] - wtm[I, J] + wtm[I, :-2]
+            t1 = (T[I, J] * s1o[I, J] + trp[I, 2:] - trp[I, J] - trm[I, J] + trm[I, :-2])
+        m = weto[I, J, :] > 0.5
+        new = T.copy()
+        new[I, J, :] = np.where(m, t1 / np.where(m, rn, 1.0), T[I, J, :])
+        s1o[I, J, :] = np.where(m, rn, s1o[I, J, :])
+        T = new
+    return T
+
+
+def _zw(ddpo, dzw):
+    ie, je, ke = ddpo.shape
+    zw = np.zeros((ie, je, ke + 1))
+    for K in range(1, ke + 2):
+        if K == 1:
+            d = np.where(ddpo[:, :, 0] == 0, dzw[0] / 2.0, ddpo[:, :, 0] / 2.0)
+        elif K == ke + 1:
+            d = np.where(ddpo[:, :, ke - 1] == 0, dzw[ke - 1], ddpo[:, :, ke - 1])
+        else:
+            a, b = ddpo[:, :, K - 2], ddpo[:, :, K - 1]
+            d = np.where(a == 0, (dzw[K - 1] + dzw[K - 2]) / 2.0, np.where(b == 0, a, (a + b) / 2.0))
+        zw[:, :, K - 1] = 1.0 / d
+    return zw
+
+
+def matrix(g):
+    """compute_matrix as scipy CSR (single rank, no cyclic boundaries)."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    nx, ny = ie - 2, je - 2
+    w = g["weto"]
+    zw = _zw(g["ddpo"], g["dzw"])
+    zp = 1.0 / ((1.0 / zw[:, :, :-1] + 1.0 / zw[:, :, 1:]) / 2.0)
+    xu = 1.0 / g["dlxu"][1:, :]      # XU(I,J), I = 1..IE
+    xp = 1.0 / g["dlxp"]
+    yv = 1.0 / g["dlyv"][:, 1:]      # YV(I,J), J = 1..JE
+    yp = 1.0 / g["dlyp"]
+    rows, cols, vals = [], [], []
+    idx = lambda i, j, k: (i - 1) + nx * ((j - 1) + ny * k)   # i, j: p-index 1..nx
+    for k in range(ke):
+        for j in range(1, je - 1):
+            for i in range(1, ie - 1):
+                r = idx(i, j, k)
+                XW = xu[i - 1, j] * xp[i, j]; XC = (xu[i - 1, j] + xu[i, j]) * xp[i, j]; XE = xu[i, j] * xp[i, j]
+                YN = yv[i, j - 1] * yp[i, j]; YC = (yv[i, j - 1] + yv[i, j]) * yp[i, j]; YS = yv[i, j] * yp[i, j]
+                ZU = zw[i, j, k] * zp[i, j, k]; ZC = (zw[i, j, k] + zw[i, j, k + 1]) * zp[i, j, k]
+                ZD = zw[i, j, k + 1] * zp[i, j, k]
+                if w[i, j, k] == 0:
+                    rows.append(r); cols.append(r); vals.append(-(XC + YC + ZC))
+                    continue
+                if w[i - 1, j, k] == 0 and w[i + 1, j, k] == 1:
+                    XW = 0.0; XC = xu[i, j] * xp[i, j]
+                elif w[i - 1, j, k] == 1 and w[i + 1, j, k] == 0:
+                    XE = 0.0; XC = xu[i - 1, j] * xp[i, j]
+                elif w[i - 1, j, k] == 0 and w[i + 1, j, k] == 0:
+                    XW = XE = XC = 0.0
+                if w[i, j - 1, k] == 0 and w[i, j + 1, k] == 1:
+                    YN = 0.0; YC = yv[i, j] * yp[i, j]
+                elif w[i, j - 1, k] == 1 and w[i, j + 1, k] == 0:
+                    YS = 0.0; YC = yv[i, j - 1] * yp[i, j]
+                elif w[i, j - 1, k] == 0 and w[i, j + 1, k] == 0:
+                    YN = YS = YC = 0.0
+                if k == 0:
+                    ZU = 0.0
+                elif k == ke - 1 or w[i, j, k + 1] == 0:
+                    ZD = 0.0; ZC = zw[i, j, k] * zp[i, j, k]
+                ent = []
+                if w[i - 1, j, k] == 1 and i - 1 != 0: ent.append((r - 1, XW))
+                if w[i, j - 1, k] == 1 and j - 1 != 0: ent.append((r - nx, YN))
+                if k != 0: ent.append((r - nx * ny, ZU))
+                ent.append((r, -(XC + YC + ZC)))
+                if k != ke - 1 and w[i, j, k + 1] == 1: ent.append((r + nx * ny, ZD))
+                if w[i, j + 1, k] == 1 and j - 1 != ny - 1: ent.append((r + nx, YS))
+                if w[i + 1, j, k] == 1 and i - 1 != nx - 1: ent.append((r + 1, XE))
+                for c, v in ent:
+                    rows.append(r); cols.append(c); vals.append(v)
+    n = nx * ny * ke
+    return sp.csr_matrix((vals, (rows, cols)), shape=(n, n))

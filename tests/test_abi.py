@@ -1,0 +1,86 @@
+"""The C ABI without a GPU: the library loads, exports every function the
+header declares, the host-side BELEG/BODEN builder equals the oracle's, and
+argument checks fail cleanly.  CPU only."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+from orctm_b200 import _lib, configs, grid
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "orctm_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(orctm_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_functions_exported():
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_python_export_list_matches_header():
+    names = set(declared_functions())
+    assert set(_lib.EXPORTS) <= names
+
+
+@pytest.mark.parametrize("name,over", [("c1", dict(nx=40)), ("c2", dict(nx=30, ny=22, nz=17)),
+                                       ("c4", dict()), ("c3", dict(nx=48, ny=40))])
+def test_grid_builder_equals_oracle(name, over):
+    r = configs.raw_instance(name, **over)
+    args = (r["ie"], r["je"], r["ke"], r["dt"], r["dzw"], r["depto_raw"], r["dlxp"], r["dlyp"],
+            r["dlxu"], r["dlyu"], r["dlxv"], r["dlyv"])
+    d1, g1 = O.build_grid(*args)
+    d2, g2 = grid.build_grid(*args)
+    assert np.array_equal(d1, d2)
+    for k in g1:
+        assert np.array_equal(g1[k], g2[k]), k
+
+
+def test_status_strings():
+    lib = _lib.load()
+    for s in range(0, -9, -1):
+        assert lib.orctm_status_string(s)
+    assert lib.orctm_abi_version() == 1
+
+
+def test_argument_checks_without_device():
+    lib = _lib.load()
+    d = _lib.Desc()
+    d.ie, d.je, d.ke, d.ntracers = 2, 2, 1, 2
+    h = C.c_void_p()
+    assert lib.orctm_create(C.byref(d), C.byref(h)) == -1          # grid too small
+    d.ie, d.je, d.ke, d.ntracers = 10, 10, 5, 1
+    assert lib.orctm_create(C.byref(d), C.byref(h)) == -1          # too few tracers
+    d.ntracers, d.dt, d.ah00, d.almzer = 2, 1.0, 1.0, 1e-19
+    assert lib.orctm_create(C.byref(d), C.byref(h)) == -6          # harmonic diffusion
+    n = C.c_size_t()
+    assert lib.orctm_field_size(None, 0, C.byref(n)) == -1
+    assert lib.orctm_ocuad(None) == -1
+    assert lib.orctm_set_solver(None, 0, 1e-10, 10) == -1
+
+
+def test_create_reports_missing_device():
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except Exception:
+        pass
+    inst = configs.make_instance("c2", builder=grid.build_grid, nx=12, ny=10, nz=6)
+    from orctm_b200.api import Instance
+
+    with pytest.raises(_lib.OrctmError) as e:
+        Instance(inst)
+    assert e.value.status in (-7, -2)
