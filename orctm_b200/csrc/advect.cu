@@ -7,8 +7,9 @@
 //     RN = V + WTP(-) - WTP(0) - WTM(0) + WTM(+)
 //     T' = (T*V + TRP(-) - TRP(0) - TRM(0) + TRM(+)) / RN
 // The z sweep runs one thread per column marching down the column with the
-// transports of the level below carried in registers; the x and y sweeps run
-// one thread per cell.  Every sweep writes a fresh buffer (never in place), so
+// transports of the level below carried in registers; the x and y sweeps
+// compute each face's transports once per block into shared memory and then
+// update one cell per thread.  Every sweep writes a fresh buffer (never in place), so
 // neighbouring columns always read the previous sweep's values.  Arithmetic is
 // IEEE binary64 in the reference's operation order (built with --fmad=false),
 // so results match the CPU restatement bit for bit.
@@ -23,22 +24,6 @@ struct Fl { double trp, trm, wtp, wtm; };
 
 #define AT(a, i, j, K) (a)[G.L.at((i), (j), (K)-1)]
 #define A2(a, i, j) (a)[G.L.at2((i), (j))]
-
-// one face transport pair with the curvature limiter
-__device__ __forceinline__ Fl limited(double up, double um, double t, double tprev, double tnext,
-                                      double vol, double cap, double mask) {
-  const double abl = fabs(tprev - tnext);
-  const double zwabl = fabs(tprev + tnext - 2. * t);
-  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * mask;
-  const double sch = fmn(cap, scha * vol / (up + um + 1.E-20));
-  const double schi = 1. - sch;
-  Fl f;
-  f.trp = up * (schi * t + sch * 0.5 * (t + tprev));
-  f.trm = um * (schi * t + sch * 0.5 * (t + tnext));
-  f.wtp = up;
-  f.wtm = um;
-  return f;
-}
 
 // the same without a mask factor (OCUAD/OCVAD forms: SCHA has no WETO product)
 __device__ __forceinline__ Fl limited_nm(double up, double um, double t, double tprev, double tnext,
@@ -195,33 +180,6 @@ __device__ __forceinline__ Fl adpo_yflux(const Geo& G, const double* T, const do
   return f;
 }
 
-template <int DIR>  // 0: x (ocadpo.f90:181-258), 1: y (ocadpo.f90:266-345)
-__global__ void k_adpo_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
-                         const double* __restrict__ vel, double* __restrict__ To,
-                         double* __restrict__ Vo) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int K = blockIdx.z + 1;
-  const int IE = G.L.ie, JE = G.L.je;
-  if (i > IE || j > JE) return;
-  const double t = AT(T, i, j, K), v = AT(V, i, j, K);
-  double tn = t, vn = v;
-  if (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1 && wetb(G.gp, G.L.at2(i, j), K)) {
-    if (DIR == 0) {
-      const Fl m = adpo_xflux(G, T, V, vel, i - 1, j, K);
-      const Fl c = adpo_xflux(G, T, V, vel, i, j, K);
-      const Fl p = adpo_xflux(G, T, V, vel, i + 1, j, K);
-      apply(t, v, m, c, p, tn, vn);
-    } else {
-      const Fl m = adpo_yflux(G, T, V, vel, i, j + 1, K);  // RN uses WTP(J+1), WTM(J-1)
-      const Fl c = adpo_yflux(G, T, V, vel, i, j, K);
-      const Fl p = adpo_yflux(G, T, V, vel, i, j - 1, K);
-      apply(t, v, m, c, p, tn, vn);
-    }
-  }
-  AT(To, i, j, K) = tn;
-  if (Vo) AT(Vo, i, j, K) = vn;
-}
 
 // ----------------------------------------------------------------- OCUAD ---
 // vertical sweep, ocuad.f90:20-86; u-columns i in [0, IE]
@@ -322,33 +280,6 @@ __device__ __forceinline__ Fl uad_yflux(const Geo& G, const double* T, const dou
                     AT(V, i, q, K), 1.);
 }
 
-template <int DIR>
-__global__ void k_uad_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
-                        const double* __restrict__ vel, double* __restrict__ To,
-                        double* __restrict__ Vo) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int K = blockIdx.z + 1;
-  const int IE = G.L.ie, JE = G.L.je;
-  if (i > IE || j > JE) return;
-  const double t = AT(T, i, j, K), v = AT(V, i, j, K);
-  double tn = t, vn = v;
-  if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1 && wetb(G.gu, G.L.at2(i, j), K)) {
-    if (DIR == 0) {
-      const Fl m = uad_xflux(G, T, V, vel, i - 1, j, K);
-      const Fl c = uad_xflux(G, T, V, vel, i, j, K);
-      const Fl p = uad_xflux(G, T, V, vel, i + 1, j, K);
-      apply(t, v, m, c, p, tn, vn);
-    } else {
-      const Fl m = uad_yflux(G, T, V, vel, i, j + 1, K);
-      const Fl c = uad_yflux(G, T, V, vel, i, j, K);
-      const Fl p = uad_yflux(G, T, V, vel, i, j - 1, K);
-      apply(t, v, m, c, p, tn, vn);
-    }
-  }
-  AT(To, i, j, K) = tn;
-  if (Vo) AT(Vo, i, j, K) = vn;
-}
 
 // ----------------------------------------------------------------- OCVAD ---
 // vertical sweep, ocvad.f90:20-86; v-columns j in [0, JE]
@@ -449,33 +380,6 @@ __device__ __forceinline__ Fl vad_yflux(const Geo& G, const double* T, const dou
   return zero_fl();
 }
 
-template <int DIR>
-__global__ void k_vad_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
-                        const double* __restrict__ vel, double* __restrict__ To,
-                        double* __restrict__ Vo) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int K = blockIdx.z + 1;
-  const int IE = G.L.ie, JE = G.L.je;
-  if (i > IE || j > JE) return;
-  const double t = AT(T, i, j, K), v = AT(V, i, j, K);
-  double tn = t, vn = v;
-  if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1 && wetb(G.gv, G.L.at2(i, j), K)) {
-    if (DIR == 0) {
-      const Fl m = vad_xflux(G, T, V, vel, i - 1, j, K);
-      const Fl c = vad_xflux(G, T, V, vel, i, j, K);
-      const Fl p = vad_xflux(G, T, V, vel, i + 1, j, K);
-      apply(t, v, m, c, p, tn, vn);
-    } else {
-      const Fl m = vad_yflux(G, T, V, vel, i, j + 1, K);
-      const Fl c = vad_yflux(G, T, V, vel, i, j, K);
-      const Fl p = vad_yflux(G, T, V, vel, i, j - 1, K);
-      apply(t, v, m, c, p, tn, vn);
-    }
-  }
-  AT(To, i, j, K) = tn;
-  if (Vo) AT(Vo, i, j, K) = vn;
-}
 
 // ----------------------------------------------------------------- OCWAD ---
 // vertical sweep, ocwad.f90:14-102; w-columns, levels 1..KEP.  WETO(KEP),
@@ -585,34 +489,81 @@ __device__ __forceinline__ Fl wad_yflux(const Geo& G, const double* T, const dou
   return Fl{up * (schi * t + sch * 0.5 * (t + tn)), um * (schi * t + sch * 0.5 * (t + ts)), up, um};
 }
 
-template <int DIR>
-__global__ void k_wad_h(Geo G, const double* __restrict__ T, const double* __restrict__ V,
-                        const double* __restrict__ vel, double* __restrict__ To,
-                        double* __restrict__ Vo) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int K = blockIdx.z + 1;  // 1..KE+1
+
+
+// ---------------------------------------------------- horizontal sweeps ---
+// One kernel per (routine, direction).  A block of 32 x 8 cells of one level
+// first computes the face transports of every position its cells need (its
+// own cells plus one halo position on each side along the sweep) once, into
+// shared memory; then each cell applies RN / T' from its neighbours' entries.
+enum { V_ADPO = 0, V_UAD = 1, V_VAD = 2, V_WAD = 3 };
+
+template <int VAR> struct Rng;
+template <> struct Rng<V_ADPO> { static constexpr int i0 = 1, j0 = 1, iL = 2, jL = 2, iH = 1, jH = 1, kL = 1; };
+template <> struct Rng<V_UAD>  { static constexpr int i0 = 0, j0 = 1, iL = 1, jL = 2, iH = 1, jH = 1, kL = 1; };
+template <> struct Rng<V_VAD>  { static constexpr int i0 = 1, j0 = 0, iL = 2, jL = 1, iH = 1, jH = 1, kL = 1; };
+template <> struct Rng<V_WAD>  { static constexpr int i0 = 1, j0 = 1, iL = 2, jL = 2, iH = 1, jH = 1, kL = 2; };
+// (iH, jH: the update range ends at IE - iH, JE - jH)
+
+template <int VAR, int DIR>
+__device__ __forceinline__ Fl face(const Geo& G, const double* T, const double* V,
+                                   const double* vel, int qi, int qj, int K) {
+  if (VAR == V_ADPO) return DIR == 0 ? adpo_xflux(G, T, V, vel, qi, qj, K) : adpo_yflux(G, T, V, vel, qi, qj, K);
+  if (VAR == V_UAD) return DIR == 0 ? uad_xflux(G, T, V, vel, qi, qj, K) : uad_yflux(G, T, V, vel, qi, qj, K);
+  if (VAR == V_VAD) return DIR == 0 ? vad_xflux(G, T, V, vel, qi, qj, K) : vad_yflux(G, T, V, vel, qi, qj, K);
+  return DIR == 0 ? wad_xflux(G, T, V, vel, qi, qj, K) : wad_yflux(G, T, V, vel, qi, qj, K);
+}
+
+template <int VAR>
+__device__ __forceinline__ bool wet_var(const Geo& G, long long ij, int K) {
+  if (VAR == V_UAD) return wetb(G.gu, ij, K);
+  if (VAR == V_VAD) return wetb(G.gv, ij, K);
+  return wetb(G.gp, ij, K);
+}
+
+constexpr int kSx = 32, kSy = 8;
+
+template <int VAR, int DIR>
+__global__ void __launch_bounds__(kSx * kSy) k_hsweep(Geo G, const double* __restrict__ T,
+                                                      const double* __restrict__ V,
+                                                      const double* __restrict__ vel,
+                                                      double* __restrict__ To,
+                                                      double* __restrict__ Vo) {
+  using R = Rng<VAR>;
+  constexpr int HX = DIR == 0 ? kSx + 2 : kSx, HY = DIR == 0 ? kSy : kSy + 2;
+  __shared__ Fl fl[HY][HX];
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
-  if (i > IE || j > JE) return;
-  const double t = AT(T, i, j, K);
-  double tn = t;
-  double v = K <= KE ? AT(V, i, j, K) : 0.0, vn = v;
-  if (K >= 2 && K <= KE && i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1 &&
-      wetb(G.gp, G.L.at2(i, j), K)) {
-    if (DIR == 0) {
-      const Fl m = wad_xflux(G, T, V, vel, i - 1, j, K);
-      const Fl c = wad_xflux(G, T, V, vel, i, j, K);
-      const Fl p = wad_xflux(G, T, V, vel, i + 1, j, K);
-      apply(t, v, m, c, p, tn, vn);
-    } else {
-      const Fl m = wad_yflux(G, T, V, vel, i, j + 1, K);
-      const Fl c = wad_yflux(G, T, V, vel, i, j, K);
-      const Fl p = wad_yflux(G, T, V, vel, i, j - 1, K);
-      apply(t, v, m, c, p, tn, vn);
+  const int K = blockIdx.z + 1;
+  const int ib = blockIdx.x * kSx + R::i0, jb = blockIdx.y * kSy + R::j0;
+  const int iLo = R::iL, iHi = IE - R::iH, jLo = R::jL, jHi = JE - R::jH;
+  const bool klev = K >= R::kL && K <= KE;
+  const int tid = threadIdx.x + kSx * threadIdx.y;
+  if (klev) {
+    for (int e = tid; e < HX * HY; e += kSx * kSy) {
+      const int hy = e / HX, hx = e - hy * HX;
+      const int qi = ib + hx - (DIR == 0), qj = jb + hy - (DIR == 1);
+      // only positions a cell in the update range reads
+      const bool need = DIR == 0 ? (qj >= jLo && qj <= jHi) : (qi >= iLo && qi <= iHi);
+      fl[hy][hx] = need ? face<VAR, DIR>(G, T, V, vel, qi, qj, K) : zero_fl();
     }
   }
+  __syncthreads();
+  const int i = ib + threadIdx.x, j = jb + threadIdx.y;
+  const int iMax = VAR == V_UAD ? IE : IE, jMax = JE;
+  if (i > iMax || j > jMax) return;
+  const double t = AT(T, i, j, K);
+  double tn = t;
+  const bool hasv = K <= KE;
+  double v = hasv ? AT(V, i, j, K) : 0.0, vn = v;
+  if (klev && i >= iLo && i <= iHi && j >= jLo && j <= jHi && wet_var<VAR>(G, G.L.at2(i, j), K)) {
+    const int hx = threadIdx.x + (DIR == 0), hy = threadIdx.y + (DIR == 1);
+    if (DIR == 0)  // RN = V + WTP(I-1) - WTP(I) - WTM(I) + WTM(I+1)
+      apply(t, v, fl[hy][hx - 1], fl[hy][hx], fl[hy][hx + 1], tn, vn);
+    else           // RN = V + WTP(J+1) - WTP(J) - WTM(J) + WTM(J-1)
+      apply(t, v, fl[hy + 1][hx], fl[hy][hx], fl[hy - 1][hx], tn, vn);
+  }
   AT(To, i, j, K) = tn;
-  if (Vo && K <= KE) AT(Vo, i, j, K) = vn;
+  if (Vo && hasv) AT(Vo, i, j, K) = vn;
 }
 
 inline dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, 1); }
@@ -627,12 +578,13 @@ void launch_ocadpo(const Geo& G, const double* T, const double* uko, const doubl
                    const double* wo, const double* zo, double* out, double* tA, double* vA,
                    double* vB, cudaStream_t st) {
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
-  const dim3 bc(32, 4), bh(32, 4);
+  const dim3 bc(32, 4);
   k_adpo_z<<<grid2(IE, JE, bc), bc, 0, st>>>(G, T, wo, zo, out, vA);
   count_launch();
-  k_adpo_h<0><<<grid3(IE, JE, KE, bh), bh, 0, st>>>(G, out, vA, uko, tA, vB);
+  const dim3 bs(kSx, kSy);
+  k_hsweep<V_ADPO, 0><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_adpo_h<1><<<grid3(IE, JE, KE, bh), bh, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_ADPO, 1><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 
@@ -643,9 +595,10 @@ void launch_ocuad(const Geo& G, const double* T, const double* uko, const double
   const dim3 b(32, 4);
   k_uad_z<<<grid2(IE + 1, JE, b), b, 0, st>>>(G, T, wo, out, vA);
   count_launch();
-  k_uad_h<0><<<grid3(IE + 1, JE, KE, b), b, 0, st>>>(G, out, vA, uko, tA, vB);
+  const dim3 bs(kSx, kSy);
+  k_hsweep<V_UAD, 0><<<grid3(IE + 1, JE, KE, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_uad_h<1><<<grid3(IE + 1, JE, KE, b), b, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_UAD, 1><<<grid3(IE + 1, JE, KE, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 
@@ -656,9 +609,10 @@ void launch_ocvad(const Geo& G, const double* T, const double* uko, const double
   const dim3 b(32, 4);
   k_vad_z<<<grid2(IE, JE + 1, b), b, 0, st>>>(G, T, wo, out, vA);
   count_launch();
-  k_vad_h<0><<<grid3(IE, JE + 1, KE, b), b, 0, st>>>(G, out, vA, uko, tA, vB);
+  const dim3 bs(kSx, kSy);
+  k_hsweep<V_VAD, 0><<<grid3(IE, JE + 1, KE, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_vad_h<1><<<grid3(IE, JE + 1, KE, b), b, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_VAD, 1><<<grid3(IE, JE + 1, KE, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 
@@ -669,9 +623,10 @@ void launch_ocwad(const Geo& G, const double* T, const double* uko, const double
   const dim3 b(32, 4);
   k_wad_z<<<grid2(IE, JE, b), b, 0, st>>>(G, T, wo, zo, out, vA);
   count_launch();
-  k_wad_h<0><<<grid3(IE, JE, KE + 1, b), b, 0, st>>>(G, out, vA, uko, tA, vB);
+  const dim3 bs(kSx, kSy);
+  k_hsweep<V_WAD, 0><<<grid3(IE, JE, KE + 1, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_wad_h<1><<<grid3(IE, JE, KE + 1, b), b, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_WAD, 1><<<grid3(IE, JE, KE + 1, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 

@@ -52,6 +52,12 @@ struct Geo {
   // 2D metrics, padded plane layout
   const double *dlxp, *dlyp, *dlxu, *dlyu, *dlxv, *dlyv;
   const double *dtdxpo, *dtdyo, *dtdxuo, *dpye;
+  // biharmonic coefficients and psi-point widths, computed once at set-up
+  // exactly as octdiff_base.f90:210-219 and ocvisc.f90:286-327 compute them
+  const double *aulx, *auly;                          // AULAPTS*DLXU**4, AULAPTS*DLYV**4 (p plane)
+  const double *aulux, *auluy, *aulvx, *aulvy, *aulwx, *aulwy;  // (p plane)
+  const double *dlypsi;                               // u-points, i in [0,IE]
+  const double *dlxpsi;                               // v-points, j in [0,JE]
 };
 
 __device__ __forceinline__ double thick(const ColGeo& c, const double* dzw, long long ij, int K) {

@@ -29,8 +29,9 @@ struct TrPtrs {
   double* out[8];
 };
 
-__global__ void k_tdiff_vert(Geo G, TrPtrs tp, int ntr, const double* __restrict__ dvo,
-                             const double* __restrict__ zo) {
+__global__ void __launch_bounds__(64) k_tdiff_vert(Geo G, TrPtrs tp, int ntr,
+                                                   const double* __restrict__ dvo,
+                                                   const double* __restrict__ zo) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
@@ -42,33 +43,53 @@ __global__ void k_tdiff_vert(Geo G, TrPtrs tp, int ntr, const double* __restrict
     return;
   }
   const long long ij = G.L.at2(i, j);
-  double t1[kMaxKe], t2[kMaxKe], t3[kMaxKe];
-  for (int K = 1; K <= KE; ++K) {
+  const double zij = zo[ij];
+  // TRIDSY(K,1..3) of octdiff_base.f90:188-194; only the eliminated diagonal
+  // is kept per level, TRIDSY(K,3) is recomputed by the same expression
+  auto den = [&](int K) {
     const double zzsurf = K == 1 ? 1. : 0.;
-    const double den = thick(G.gp, G.dzw, ij, K) + zzsurf * (zo[ij]) + G.almzer;
-    t1[K - 1] = -G.dt * AT(dvo, i, j, K) * wet(G.gp, ij, K) * G.di[K - 1] / den;
-    t3[K - 1] = -G.dt * AT(dvo, i, j, K + 1) * G.di[K] / den;
-    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
-  }
-  for (int K = 2; K <= KE; ++K) {
-    const double a = t1[K - 1];
-    t1[K - 2] = a / t2[K - 2];
-    t2[K - 1] = t2[K - 1] - t3[K - 2] * a / t2[K - 2];
-  }
-  for (int n = 0; n < ntr; ++n) {
-    const double* T = tp.in[n];
-    double* O = tp.out[n];
-    double prev = AT(T, i, j, 1);
-    AT(O, i, j, 1) = prev;  // T1O(1)
-    for (int K = 2; K <= KE; ++K) {
-      prev = AT(T, i, j, K) - t1[K - 2] * prev;
-      AT(O, i, j, K) = prev;  // T1O(K)
+    return thick(G.gp, G.dzw, ij, K) + zzsurf * (zij) + G.almzer;
+  };
+  auto tri3 = [&](int K, double dn) { return -G.dt * AT(dvo, i, j, K + 1) * G.di[K] / dn; };
+  double t2p[kMaxKe];
+  double ylast[8];
+  double t2prev = 1.0, t3prev = 0.0;
+  for (int K = 1; K <= KE; ++K) {
+    const double dn = den(K);
+    const double t1 = -G.dt * AT(dvo, i, j, K) * wet(G.gp, ij, K) * G.di[K - 1] / dn;
+    const double t3 = tri3(K, dn);
+    double t2 = 1. - t1 - t3;
+    double m = 0.0;
+    if (K >= 2) {
+      m = t1 / t2prev;                       // TRIDSY(K-1,1) after elimination
+      t2 = t2 - t3prev * t1 / t2prev;        // TRIDSY(K,2) after elimination
     }
-    double nxt = AT(O, i, j, KE) / t2[KE - 1];
-    AT(O, i, j, KE) = nxt;
-    for (int l = KE - 1; l >= 1; --l) {
-      nxt = (AT(O, i, j, l) - t3[l - 1] * nxt) / t2[l - 1];
-      AT(O, i, j, l) = nxt;
+    t2p[K - 1] = t2;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      if (n >= ntr) break;
+      const double tk = AT(tp.in[n], i, j, K);
+      const double y = K == 1 ? tk : tk - m * ylast[n];  // T1O(K)
+      AT(tp.out[n], i, j, K) = y;
+      ylast[n] = y;
+    }
+    t2prev = t2;
+    t3prev = t3;
+  }
+  double nxt[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    if (n >= ntr) break;
+    nxt[n] = AT(tp.out[n], i, j, KE) / t2p[KE - 1];
+    AT(tp.out[n], i, j, KE) = nxt[n];
+  }
+  for (int l = KE - 1; l >= 1; --l) {
+    const double t3 = tri3(l, den(l));
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      if (n >= ntr) break;
+      nxt[n] = (AT(tp.out[n], i, j, l) - t3 * nxt[n]) / t2p[l - 1];
+      AT(tp.out[n], i, j, l) = nxt[n];
     }
   }
 }
@@ -107,14 +128,8 @@ __global__ void k_tdiff_bih(Geo G, const double* __restrict__ T, const double* _
   double r = t;
   if (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
     auto w = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
-    auto aulx = [&](int ii, int jj) {
-      const double x = G.dlxu[G.L.at2(ii, jj)];
-      return G.aulapts * ((x * x) * (x * x));
-    };
-    auto auly = [&](int ii, int jj) {
-      const double y = G.dlyv[G.L.at2(ii, jj)];
-      return G.aulapts * ((y * y) * (y * y));
-    };
+    auto aulx = [&](int ii, int jj) { return G.aulx[G.L.at2(ii, jj)]; };
+    auto auly = [&](int ii, int jj) { return G.auly[G.L.at2(ii, jj)]; };
     const long long ij = G.L.at2(i, j);
     const double zzsurf = K == 1 ? 1. : 0.;
     const double c = AT(L1, i, j, K);
@@ -167,9 +182,11 @@ __global__ void k_visc_speed(Geo G, const double* __restrict__ uoo, const double
 // implicit vertical diffusion of u (DIR = 0, ocvisc.f90:168-218) or v
 // (DIR = 1, ocvisc.f90:114-165) with quadratic bottom drag in the last row
 template <int DIR>
-__global__ void k_visc_uv(Geo G, const double* __restrict__ X, const double* __restrict__ keep,
-                          const double* __restrict__ avo, const double* __restrict__ speed,
-                          double* __restrict__ O) {
+__global__ void __launch_bounds__(64) k_visc_uv(Geo G, const double* __restrict__ X,
+                                                const double* __restrict__ keep,
+                                                const double* __restrict__ avo,
+                                                const double* __restrict__ speed,
+                                                double* __restrict__ O) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
@@ -187,43 +204,51 @@ __global__ void k_visc_uv(Geo G, const double* __restrict__ X, const double* __r
   const long long ij2 = DIR == 0 ? G.L.at2(i + 1, j) : G.L.at2(i, j + 1);
   const double BOFRIC = 3.E-3, RAYFRIC = 3.E-3;
   const double sp = speed[ij];
-  double t1[kMaxKe], t2[kMaxKe], t3[kMaxKe];
   auto avo_at = [&](long long q, int K) { return avo[q + G.L.plane * (K - 1)]; };
-  for (int K = 1; K <= KE - 1; ++K) {
-    const double am = wet(cg, ij, K), am1 = wet(cg, ij, K + 1), dd = thick(cg, G.dzw, ij, K);
-    const double avup = 0.5 * (avo_at(ij, K) + avo_at(ij2, K)) * am;
-    const double avlo = 0.5 * (avo_at(ij, K + 1) + avo_at(ij2, K + 1)) * am1 +
-                        (BOFRIC + RAYFRIC * dd * sp) * (am - am1);
-    t1[K - 1] = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
-    t3[K - 1] = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
-    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
-    t3[K - 1] = t3[K - 1] * am1;
-  }
-  {
-    const int K = KE;
+  // TRIDSY(K,1) and TRIDSY(K,3) (after the AMS(K+1) factor) of
+  // ocvisc.f90:117-140 / 171-193
+  auto tri = [&](int K, double& t1, double& t3) {
     const double am = wet(cg, ij, K), dd = thick(cg, G.dzw, ij, K);
     const double avup = 0.5 * (avo_at(ij, K) + avo_at(ij2, K)) * am;
-    const double avlo = (BOFRIC + RAYFRIC * dd * sp) * am;
-    t1[K - 1] = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
-    t3[K - 1] = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
-    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
-    t3[K - 1] = 0.;
+    if (K < KE) {
+      const double am1 = wet(cg, ij, K + 1);
+      const double avlo = 0.5 * (avo_at(ij, K + 1) + avo_at(ij2, K + 1)) * am1 +
+                          (BOFRIC + RAYFRIC * dd * sp) * (am - am1);
+      t1 = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
+      t3 = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
+    } else {
+      const double avlo = (BOFRIC + RAYFRIC * dd * sp) * am;
+      t1 = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
+      t3 = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
+    }
+  };
+  double t2p[kMaxKe];
+  double t2prev = 1.0, t3prev = 0.0, yprev = 0.0;
+  for (int K = 1; K <= KE; ++K) {
+    double t1, t3;
+    tri(K, t1, t3);
+    double t2 = 1. - t1 - t3;
+    t3 = K < KE ? t3 * wet(cg, ij, K + 1) : 0.;
+    const double xk = AT(X, i, j, K);
+    double y = xk;
+    if (K >= 2) {
+      const double m = t1 / t2prev;
+      t2 = t2 - t3prev * t1 / t2prev;
+      y = xk - m * yprev;
+    }
+    t2p[K - 1] = t2;
+    AT(O, i, j, K) = y;
+    yprev = y;
+    t2prev = t2;
+    t3prev = t3;
   }
-  for (int K = 2; K <= KE; ++K) {
-    const double a = t1[K - 1];
-    t1[K - 2] = a / t2[K - 2];
-    t2[K - 1] = t2[K - 1] - t3[K - 2] * a / t2[K - 2];
-  }
-  double prev = AT(X, i, j, 1);
-  AT(O, i, j, 1) = prev;
-  for (int K = 2; K <= KE; ++K) {
-    prev = AT(X, i, j, K) - t1[K - 2] * prev;
-    AT(O, i, j, K) = prev;
-  }
-  double nxt = wet(cg, ij, KE) * AT(O, i, j, KE) / t2[KE - 1];
+  double nxt = wet(cg, ij, KE) * AT(O, i, j, KE) / t2p[KE - 1];
   AT(O, i, j, KE) = nxt;
   for (int l = KE - 1; l >= 1; --l) {
-    nxt = (AT(O, i, j, l) - t3[l - 1] * nxt) * wet(cg, ij, l) / t2[l - 1];
+    double t1, t3;
+    tri(l, t1, t3);
+    t3 = t3 * wet(cg, ij, l + 1);
+    nxt = (AT(O, i, j, l) - t3 * nxt) * wet(cg, ij, l) / t2p[l - 1];
     AT(O, i, j, l) = nxt;
   }
 }
@@ -282,16 +307,11 @@ __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __re
 }
 
 __device__ __forceinline__ double dlypsi(const Geo& G, int i, int j) {  // u-points, i in [0,IE]
-  if (i == 0) return G.dlyv[G.L.at2(1, j)];
-  if (i == G.L.ie) return G.dlyv[G.L.at2(G.L.ie, j)];
-  return 0.5 * (G.dlyv[G.L.at2(i, j)] + G.dlyv[G.L.at2(i + 1, j)]);
+  return G.dlypsi[G.L.at2(i, j)];
 }
 __device__ __forceinline__ double dlxpsi(const Geo& G, int i, int j) {  // v-points, j in [0,JE]
-  if (j == 0) return G.dlxu[G.L.at2(i, 1)];
-  if (j == G.L.je) return G.dlxu[G.L.at2(i, G.L.je)];
-  return 0.5 * (G.dlxu[G.L.at2(i, j)] + G.dlxu[G.L.at2(i, j + 1)]);
+  return G.dlxpsi[G.L.at2(i, j)];
 }
-__device__ __forceinline__ double pow4(double x) { return (x * x) * (x * x); }
 
 // first Laplacians UK1O (u), VK1E (v), WN1O (w), ocvisc.f90:350-438, 617-669
 __global__ void k_visc_lap(Geo G, const double* __restrict__ uk, const double* __restrict__ vk,
@@ -421,7 +441,7 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
   const int K = blockIdx.z + 1;  // 1..KE+1
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const double A = G.aulapuv, mv = G.minvalue;
+  const double mv = G.minvalue;
   if (K <= KE) {
     // ---- u
     if (j >= 1) {
@@ -429,8 +449,8 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
         auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
         auto U1 = [&](int ii, int jj) { return AT(u1, ii, jj, K); };
-        auto aulux = [&](int ii, int jj) { return A * pow4(fmx(G.dlxp[G.L.at2(ii, jj)], mv)); };
-        auto auluy = [&](int ii, int jj) { return A * pow4(fmx(mv, dlypsi(G, ii, jj))); };
+        auto aulux = [&](int ii, int jj) { return G.aulux[G.L.at2(ii, jj)]; };
+        auto auluy = [&](int ii, int jj) { return G.auluy[G.L.at2(ii, jj)]; };
         const long long ij = G.L.at2(i, j);
         r = (AO(i, j) / (G.dlxu[ij] * G.dlyu[ij])) *
             (G.dlxu[ij] * G.dlyu[ij] * AT(uk, i, j, K) -
@@ -450,8 +470,8 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
         auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
         auto V1 = [&](int ii, int jj) { return AT(v1, ii, jj, K); };
-        auto aulvx = [&](int ii, int jj) { return A * pow4(fmx(dlxpsi(G, ii, jj), mv)); };
-        auto aulvy = [&](int ii, int jj) { return A * pow4(fmx(mv, G.dlyp[G.L.at2(ii, jj)])); };
+        auto aulvx = [&](int ii, int jj) { return G.aulvx[G.L.at2(ii, jj)]; };
+        auto aulvy = [&](int ii, int jj) { return G.aulvy[G.L.at2(ii, jj)]; };
         const long long ij = G.L.at2(i, j);
         r = (AE(i, j) / (G.dlxv[ij] * G.dlyv[ij])) *
             (G.dlxv[ij] * G.dlyv[ij] * AT(vk, i, j, K) -
@@ -473,8 +493,8 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       auto W1 = [&](int ii, int jj) { return AT(w1, ii, jj, K); };
       auto dzu = [&](int ii, int jj) { return fmx(thick(G.gu, G.dzw, G.L.at2(ii, jj), K), mv); };
       auto dzv = [&](int ii, int jj) { return fmx(thick(G.gv, G.dzw, G.L.at2(ii, jj), K), mv); };
-      auto aulwx = [&](int ii, int jj) { return A * pow4(fmx(G.dlxu[G.L.at2(ii, jj)], mv)); };
-      auto aulwy = [&](int ii, int jj) { return A * pow4(fmx(G.dlyv[G.L.at2(ii, jj)], mv)); };
+      auto aulwx = [&](int ii, int jj) { return G.aulwx[G.L.at2(ii, jj)]; };
+      auto aulwy = [&](int ii, int jj) { return G.aulwy[G.L.at2(ii, jj)]; };
       const long long ij = G.L.at2(i, j);
       const double dzp = fmx(thick(G.gp, G.dzw, ij, K), mv);
       r = (WE(i, j) / (G.dlxp[ij] * G.dlyp[ij] * dzp)) *

@@ -346,6 +346,52 @@ int setup(orctm_handle* h, const orctm_desc* d) {
       (st = up2(G.dlyv, d->dlyv, KV)) || (st = up2(G.dpye, d->dpye, KV)))
     return st;
 
+  // biharmonic coefficients (octdiff_base.f90:210-219, ocvisc.f90:286-327)
+  {
+    auto pow4 = [](double x) { return (x * x) * (x * x); };
+    auto fmx = [](double a, double b) { return a > b ? a : b; };
+    const double mv = G.minvalue, A = d->aulapuv, At = d->aulapts;
+    std::vector<double> aulx(n2, 0.), auly(n2, 0.), aulux(n2, 0.), auluy(n2, 0.), aulvx(n2, 0.),
+        aulvy(n2, 0.), aulwx(n2, 0.), aulwy(n2, 0.), dlypsi(n2, 0.), dlxpsi(n2, 0.);
+    for (int j = 1; j <= JE; ++j) {
+      for (int i = 1; i <= IE - 1; ++i)
+        dlypsi[L.at2(i, j)] = 0.5 * (d->dlyv[x.v2(i, j)] + d->dlyv[x.v2(i + 1, j)]);
+      dlypsi[L.at2(0, j)] = d->dlyv[x.v2(1, j)];
+      dlypsi[L.at2(IE, j)] = d->dlyv[x.v2(IE, j)];
+    }
+    for (int i = 1; i <= IE; ++i) {
+      for (int j = 1; j <= JE - 1; ++j)
+        dlxpsi[L.at2(i, j)] = 0.5 * (d->dlxu[x.u2(i, j)] + d->dlxu[x.u2(i, j + 1)]);
+      dlxpsi[L.at2(i, 0)] = d->dlxu[x.u2(i, 1)];
+      dlxpsi[L.at2(i, JE)] = d->dlxu[x.u2(i, JE)];
+    }
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        const size_t s = L.at2(i, j);
+        aulx[s] = At * pow4(d->dlxu[x.u2(i, j)]);
+        auly[s] = At * pow4(d->dlyv[x.v2(i, j)]);
+        aulux[s] = A * pow4(fmx(d->dlxp[x.p2(i, j)], mv));
+        auluy[s] = A * pow4(fmx(mv, dlypsi[s]));
+        aulvy[s] = A * pow4(fmx(mv, d->dlyp[x.p2(i, j)]));
+        aulvx[s] = A * pow4(fmx(dlxpsi[s], mv));
+        aulwx[s] = A * pow4(fmx(d->dlxu[x.u2(i, j)], mv));
+        aulwy[s] = A * pow4(fmx(d->dlyv[x.v2(i, j)], mv));
+      }
+    auto upg = [&](const double*& dst, const std::vector<double>& v) -> int {
+      double* q;
+      int s2;
+      if ((s2 = h->dev_alloc(&q, v.size()))) return s2;
+      ORCTM_CUDA_OK(cudaMemcpy(q, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+      dst = q;
+      return ORCTM_OK;
+    };
+    if ((st = upg(G.aulx, aulx)) || (st = upg(G.auly, auly)) || (st = upg(G.aulux, aulux)) ||
+        (st = upg(G.auluy, auluy)) || (st = upg(G.aulvx, aulvx)) || (st = upg(G.aulvy, aulvy)) ||
+        (st = upg(G.aulwx, aulwx)) || (st = upg(G.aulwy, aulwy)) || (st = upg(G.dlypsi, dlypsi)) ||
+        (st = upg(G.dlxpsi, dlxpsi)))
+      return st;
+  }
+
   // Poisson tables (mo_petsc.f90:557-599)
   std::vector<double> xu(n2, 0.), xp(n2, 0.), yv(n2, 0.), yp(n2, 0.);
   for (int j = 1; j <= JE; ++j)

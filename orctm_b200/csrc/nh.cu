@@ -141,12 +141,6 @@ void launch_nh_rhs(const Geo& G, const double* uoo, const double* uoo1, const do
   count_launch();
 }
 
-// columns per block of the column kernel: 64, or 32 when 64 columns of
-// factorisation would not fit in shared memory
-static int pcg_col_width(const Geo& G, bool f32) {
-  const size_t per = (size_t)2 * G.L.ke * (f32 ? sizeof(float) : sizeof(double));
-  return per * 64 <= 200 * 1024 ? 64 : 32;
-}
 
 void launch_nh_post(const Geo& G, const double* x, const double* pold, double* pnh,
                     const double* uoo, const double* voe, double* uo, double* vo, double* wno,

@@ -27,6 +27,7 @@
 // needs no host round trip.  A device flag marks convergence; kernels of an
 // already converged solve return at once.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "ops.h"
@@ -51,6 +52,7 @@ struct Coef {
 struct ColC {
   long long ij;
   int kb, kbw, kbe, kbn, kbs;
+  int kreg;                            // levels 2..kreg have the regular (all-wet) row
   bool iw, ie, in, is;                 // couplings the DMDA allows (not at the domain edge)
   double cw, ce, cn, cs, xcf, ycf;     // XU(I-1)XP, XU(I)XP, YV(J-1)YP, YV(J)YP, sums
   double zwa, zwb, zpa, zpb, zpc, iza, izb, izc;
@@ -80,6 +82,10 @@ __device__ __forceinline__ ColC load_col(const Geo& G, const PoissonGeo& P, int 
   c.zwa = P.zwa[c.ij]; c.zwb = P.zwb[c.ij];
   c.zpa = P.zpa[c.ij]; c.zpb = P.zpb[c.ij]; c.zpc = P.zpc[c.ij];
   c.iza = P.iza[c.ij]; c.izb = P.izb[c.ij]; c.izc = P.izc[c.ij];
+  // below kreg every neighbour is wet and ZW/ZP are the 1D tables: K < kb - 1
+  // keeps K, K+1 and the ZP selections away from the bottom specials
+  const int km = min(min(c.kbw, c.kbe), min(c.kbn, c.kbs));
+  c.kreg = min(km, c.kb - 2);
   return c;
 }
 
@@ -142,6 +148,22 @@ __device__ __forceinline__ Coef row(const ColC& c, const PoissonGeo& P, int K, i
   if (c.is && ws) r.s = c.cs * hs;
   if (K != 1) r.u = zw0 * zp;
   if (K != KE && wd) r.d = zw1 * zp;
+  return r;
+}
+
+// Row K of B for a regular level (2 <= K <= kreg): all six neighbours wet,
+// vertical factors from the 1D tables.  Same values as row<true>.
+__device__ __forceinline__ Coef row_regular(const ColC& c, const double* zw, const double* iz,
+                                            int K) {
+  const double zw0 = zw[K - 1], zw1 = zw[K], hs = iz[K - 1];
+  Coef r;
+  r.u = zw0;
+  r.d = zw1;
+  r.w = c.iw ? c.cw * hs : 0.0;
+  r.e = c.ie ? c.ce * hs : 0.0;
+  r.n = c.in ? c.cn * hs : 0.0;
+  r.s = c.is ? c.cs * hs : 0.0;
+  r.dc = -((c.xcf + c.ycf) * hs + (zw0 + zw1));
   return r;
 }
 
@@ -228,9 +250,6 @@ __global__ void k_factor(Geo G, PoissonGeo P, double* __restrict__ dinv64,
 }
 
 // ------------------------------------------------------- PCG kernels -----
-template <typename T> __device__ __forceinline__ const T* dinv_of(const PoissonGeo& P);
-template <> __device__ __forceinline__ const double* dinv_of<double>(const PoissonGeo& P) { return P.dinv64; }
-template <> __device__ __forceinline__ const float* dinv_of<float>(const PoissonGeo& P) { return P.dinv32; }
 
 // Column kernel: residual update, z = M^-1 r (exact column tridiagonal of B),
 // dots r.z and r.r.
@@ -246,39 +265,83 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const double alpha = MODE == 2 ? S->alpha : 0.0;
-  const T* __restrict__ dinv = dinv_of<T>(P);
+  // pivots rounded to FP32 in both precisions: a fixed preconditioner that
+  // moves half the bytes (the operator apply and the vectors keep precision T)
+  const float* __restrict__ dinv = P.dinv32;
   double rz = 0.0, rr = 0.0, bb = 0.0;
   if (i <= IE - 1 && j <= JE - 1) {
     const ColC c = load_col(G, P, i, j);
     double yprev = 0.0, dprev = 0.0;
-    for (int K = 1; K <= KE; ++K) {
-      double rk;
-      if (MODE == 1) {
-        rk = (double)AT(b, i, j, K) * izp_of(c, P, K);
-        bb += rk * rk;
-      } else {
-        const double pk = (double)AT(p, i, j, K), qk = (double)AT(q, i, j, K);
-        AT(x, i, j, K) = (T)((double)AT(x, i, j, K) + alpha * pk);
-        rk = (double)AT(r, i, j, K) - alpha * qk;
+    const long long base = G.L.at(i, j, 0), plane = G.L.plane;
+    constexpr int U = 4;  // levels whose loads are issued together
+    for (int K0 = 1; K0 <= KE; K0 += U) {
+      double lb[U], lr[U], lp[U], lq[U], lx[U], ld[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int K = K0 + u;
+        lb[u] = lr[u] = lp[u] = lq[u] = lx[u] = ld[u] = 0.0;
+        if (K <= KE) {
+          const long long o = base + plane * (K - 1);
+          if (MODE == 1) {
+            lb[u] = (double)b[o];
+          } else {
+            lr[u] = (double)r[o];
+            lp[u] = (double)p[o];
+            lq[u] = (double)q[o];
+            lx[u] = (double)x[o];
+          }
+          ld[u] = (double)dinv[o];
+        }
       }
-      const T rkt = (T)rk;
-      AT(r, i, j, K) = rkt;
-      rk = (double)rkt;
-      rr += rk * rk;
-      const double up = (K == 1 || K > c.kb) ? 0.0 : zw_of(c, P, K);  // a(K) of B
-      const double y = rk - (up * dprev) * yprev;
-      AT(z, i, j, K) = (T)y;  // y' kept in z until the backward sweep
-      yprev = (double)(T)y;
-      dprev = (double)AT(dinv, i, j, K);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int K = K0 + u;
+        if (K > KE) break;
+        const long long o = base + plane * (K - 1);
+        double rk;
+        if (MODE == 1) {
+          rk = lb[u] * izp_of(c, P, K);
+          bb += rk * rk;
+        } else {
+          x[o] = (T)(lx[u] + alpha * lp[u]);
+          rk = lr[u] - alpha * lq[u];
+        }
+        const T rkt = (T)rk;
+        r[o] = rkt;
+        rk = (double)rkt;
+        rr += rk * rk;
+        const double up = (K == 1 || K > c.kb) ? 0.0 : zw_of(c, P, K);  // a(K) of B
+        const double y = rk - (up * dprev) * yprev;
+        z[o] = (T)y;  // y' kept in z until the backward sweep
+        yprev = (double)(T)y;
+        dprev = ld[u];
+      }
     }
     double znext = 0.0;
-    for (int K = KE; K >= 1; --K) {
-      const double dn = down_of<true>(c, P, K, KE);
-      const double zk = ((double)AT(z, i, j, K) - dn * znext) * (double)AT(dinv, i, j, K);
-      const T zt = (T)zk;
-      AT(z, i, j, K) = zt;
-      znext = (double)zt;
-      rz += (double)AT(r, i, j, K) * znext;
+    for (int K1 = KE; K1 >= 1; K1 -= U) {
+      double ly[U], ld[U], lr[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int K = K1 - u;
+        ly[u] = ld[u] = lr[u] = 0.0;
+        if (K >= 1) {
+          const long long o = base + plane * (K - 1);
+          ly[u] = (double)z[o];
+          ld[u] = (double)dinv[o];
+          lr[u] = (double)r[o];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int K = K1 - u;
+        if (K < 1) break;
+        const double dn = down_of<true>(c, P, K, KE);
+        const double zk = (ly[u] - dn * znext) * ld[u];
+        const T zt = (T)zk;
+        z[base + plane * (K - 1)] = zt;
+        znext = (double)zt;
+        rz += lr[u] * znext;
+      }
     }
   }
   double v[3] = {rz, rr, bb};
@@ -298,43 +361,111 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
 }
 
 // Stencil kernel: p = z + beta p_old (first iteration: p = z), q = B p, and
-// the dot p.q; alpha = rho / (p.q).
+// the dot p.q; alpha = rho / (p.q).  A block of 32 x 4 columns marches down
+// the levels; p of its 34 x 6 halo tile is formed once per level into a
+// three-level shared-memory ring, and the 7-point product reads the ring.
+constexpr int kTx = 32, kTy = 4, kHx = kTx + 2, kHy = kTy + 2;
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_pcg_spmv(Geo G, PoissonGeo P, SolverState* S,
                                                   const T* __restrict__ z,
                                                   const T* __restrict__ pold, T* __restrict__ pnew,
                                                   T* __restrict__ q, int first) {
+  constexpr int kH = kHx * kHy, kNt = kTx * kTy, kF = (kH + kNt - 1) / kNt;
+  __shared__ T ring[3][kH];
+  __shared__ double szw[kMaxKe + 1], siz[kMaxKe];
   if (S->converged) return;
+  for (int e = threadIdx.x + kTx * threadIdx.y; e <= G.L.ke; e += kTx * kTy) {
+    szw[e] = P.zwn[e];
+    if (e < G.L.ke) siz[e] = P.izn[e];
+  }
   const int KE = G.L.ke, IE = G.L.ie, JE = G.L.je;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const long long plane = G.L.plane;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kTx * ty;
+  const int i0 = blockIdx.x * kTx + 2, j0 = blockIdx.y * kTy + 2;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool act = i <= IE - 1 && j <= JE - 1;
   const double beta = first ? 0.0 : S->beta;
-  double pq = 0.0;
-  if (i <= IE - 1 && j <= JE - 1) {
-    const ColC c = load_col(G, P, i, j);
-    auto pv = [&](int ii, int jj, int K) -> double {
-      const double zz = (double)AT(z, ii, jj, K);
-      return first ? zz : (double)(T)(zz + beta * (double)AT(pold, ii, jj, K));
-    };
-    double pm = 0.0, p0 = pv(i, j, 1), pp = 0.0;
-    for (int K = 1; K <= KE; ++K) {
-      pp = K < KE ? pv(i, j, K + 1) : 0.0;
-      const Coef rw = row<true>(c, P, K, KE);
-      double s = 0.0;
-      if (rw.u != 0.0) s += rw.u * pm;
-      if (rw.n != 0.0) s += rw.n * pv(i, j - 1, K);
-      if (rw.w != 0.0) s += rw.w * pv(i - 1, j, K);
-      s += rw.dc * p0;
-      if (rw.e != 0.0) s += rw.e * pv(i + 1, j, K);
-      if (rw.s != 0.0) s += rw.s * pv(i, j + 1, K);
-      if (rw.d != 0.0) s += rw.d * pp;
-      AT(pnew, i, j, K) = (T)p0;
-      const T qt = (T)s;
-      AT(q, i, j, K) = qt;
-      pq += p0 * (double)qt;
-      pm = p0;
-      p0 = pp;
+  // halo-tile entries this thread fills: offsets at level 1, validity
+  long long fo[kF];
+  int fs[kF];
+  bool fv[kF];
+#pragma unroll
+  for (int f = 0; f < kF; ++f) {
+    const int e = tid + f * kNt;
+    const int hy = e / kHx, hx = e - hy * kHx;
+    const int ii = i0 - 1 + hx, jj = j0 - 1 + hy;
+    fs[f] = e < kH ? e : -1;
+    fv[f] = e < kH && ii >= 2 && ii <= IE - 1 && jj >= 2 && jj <= JE - 1;
+    fo[f] = fv[f] ? G.L.at(ii, jj, 0) : 0;
+  }
+  // the halo values of two levels ahead are held in registers, so the loads of
+  // level K+3 are in flight while level K is computed
+  double qz[2][kF], qp[2][kF];
+  auto load = [&](int slot, int K) {
+#pragma unroll
+    for (int f = 0; f < kF; ++f) {
+      qz[slot][f] = 0.0;
+      qp[slot][f] = 0.0;
+      if (fv[f] && K <= KE) {
+        const long long o = fo[f] + plane * (K - 1);
+        qz[slot][f] = (double)z[o];
+        if (!first) qp[slot][f] = (double)pold[o];
+      }
     }
+  };
+  auto store = [&](T* dst, int slot) {
+#pragma unroll
+    for (int f = 0; f < kF; ++f)
+      if (fs[f] >= 0)
+        dst[fs[f]] = first ? (T)qz[slot][f] : (T)(qz[slot][f] + beta * qp[slot][f]);
+  };
+  ColC c;
+  if (act) c = load_col(G, P, i, j);
+  const long long own = act ? G.L.at(i, j, 0) : 0;
+  const int me = (ty + 1) * kHx + (tx + 1);
+  T* prv = ring[0];
+  T* cur = ring[1];
+  T* nxt = ring[2];
+  for (int e = threadIdx.x + kTx * threadIdx.y; e < kH; e += kNt) prv[e] = (T)0;
+  load(0, 1);
+  store(cur, 0);
+  load(0, 2);
+  load(1, 3);
+  double pq = 0.0;
+  // one level; SA (the register slot holding level K+1) is a literal at every
+  // call so the register queue is never indexed dynamically
+  auto level = [&](int K, auto sa_c) {
+    constexpr int SA = decltype(sa_c)::value;
+    __syncthreads();  // the slot of level K-2 is free; level K is complete
+    store(nxt, SA);
+    load(SA, K + 3);
+    __syncthreads();
+    if (act) {
+      const Coef rw = (K >= 2 && K <= c.kreg) ? row_regular(c, szw, siz, K) : row<true>(c, P, K, KE);
+      const double p0 = (double)cur[me];
+      // entries that are not inserted are exactly 0 and their neighbours finite
+      double s = rw.dc * p0;
+      s = __fma_rn(rw.u, (double)prv[me], s);
+      s = __fma_rn(rw.n, (double)cur[me - kHx], s);
+      s = __fma_rn(rw.w, (double)cur[me - 1], s);
+      s = __fma_rn(rw.e, (double)cur[me + 1], s);
+      s = __fma_rn(rw.s, (double)cur[me + kHx], s);
+      s = __fma_rn(rw.d, (double)nxt[me], s);
+      const long long o = own + plane * (K - 1);
+      pnew[o] = (T)p0;
+      const T qt = (T)s;
+      q[o] = qt;
+      pq += p0 * (double)qt;
+    }
+    T* t = prv;
+    prv = cur;
+    cur = nxt;
+    nxt = t;
+  };
+  for (int K = 1; K <= KE; K += 2) {
+    level(K, std::integral_constant<int, 0>{});
+    if (K + 1 <= KE) level(K + 1, std::integral_constant<int, 1>{});
   }
   double v[1] = {pq};
   if (grid_sum<1>(v, S)) {
@@ -469,8 +600,9 @@ template void launch_pcg_col<float, float>(const Geo&, const PoissonGeo&, Solver
 template <typename T>
 void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
                      T* pnew, T* q, int first, cudaStream_t st) {
-  k_pcg_spmv<T><<<grid2(G.L.ie - 2, G.L.je - 2, kColBlock), kColBlock, 0, st>>>(G, P, S, z, pold,
-                                                                                 pnew, q, first);
+  const dim3 blk(kTx, kTy);
+  k_pcg_spmv<T><<<grid2(G.L.ie - 2, G.L.je - 2, blk), blk, 0, st>>>(G, P, S, z, pold, pnew, q,
+                                                                     first);
   count_launch();
 }
 template void launch_pcg_spmv<double>(const Geo&, const PoissonGeo&, SolverState*, const double*,
