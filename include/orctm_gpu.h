@@ -167,6 +167,27 @@ int orctm_profile_get(orctm_handle* h, int kind, long long* launches, double* to
 /* Number of CUDA kernels this library has launched in the calling process. */
 unsigned long long orctm_kernel_launches(void);
 
+/* Kernel variants of the Poisson solver: 4 column-kernel variants (forward
+ * values in global or shared memory, 4 or 8 levels per load batch) and 4
+ * stencil variants (shared-memory ring or L1 form, 32x8 or 32x4 blocks).
+ * All variants give bit-identical results.  A variant of -1 (the default)
+ * lets the handle time the variants on its own grid before its first solve
+ * in each precision and keep the fastest (the choice is cached per grid size
+ * in the process).  orctm_get_tuning returns the variants in use for a
+ * precision (0 FP64, 1 FP32), -1 before the first solve.  A shared-memory
+ * column variant that does not fit the grid's KE falls back to variant 0. */
+int orctm_set_tuning(orctm_handle* h, int col_variant, int spmv_variant);
+int orctm_get_tuning(const orctm_handle* h, int precision, int* col_variant, int* spmv_variant);
+
+/* Device memory.  A handle allocates from a stream-ordered pool that the
+ * library keeps per device; destroying a handle returns its blocks to the
+ * pool without a device-wide synchronisation.  orctm_device_bytes gives the
+ * bytes a handle holds now (it grows on the first step and the first solve
+ * of each solver mode); orctm_trim_device_memory hands the pool's unused
+ * blocks of a device back to the driver. */
+int orctm_device_bytes(const orctm_handle* h, unsigned long long* bytes);
+int orctm_trim_device_memory(int device);
+
 /* BELEG + BODEN restated on the host.  depto (IE*JE) is adjusted in place as
  * BODEN does (ISTART == 0).  Output arrays are caller-allocated in the host
  * layouts above; tiestu, tiestw, dz and di hold KE+1 values. */

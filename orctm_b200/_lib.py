@@ -50,7 +50,8 @@ EXPORTS = (
     "orctm_ocvad", "orctm_ocwad", "orctm_ocadpo", "orctm_octdiff", "orctm_octimf",
     "orctm_ocvisc", "orctm_ocvtot_nh", "orctm_step_hotpath", "orctm_set_solver",
     "orctm_synchronize", "orctm_build_grid", "orctm_timer_start", "orctm_timer_stop",
-    "orctm_set_profiling", "orctm_profile_get", "orctm_kernel_launches",
+    "orctm_set_profiling", "orctm_profile_get", "orctm_kernel_launches", "orctm_device_bytes",
+    "orctm_trim_device_memory", "orctm_set_tuning", "orctm_get_tuning",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -92,6 +93,10 @@ def load(build_if_missing: bool = True):
                                       C.POINTER(C.c_double)]
     lib.orctm_kernel_launches.restype = C.c_ulonglong
     lib.orctm_kernel_launches.argtypes = []
+    lib.orctm_device_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
+    lib.orctm_trim_device_memory.argtypes = [C.c_int]
+    lib.orctm_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.orctm_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     _lib = lib
     return lib
 

@@ -153,6 +153,22 @@ class Instance:
     def synchronize(self):
         _lib.check(self.lib.orctm_synchronize(self.h), self.h)
 
+    def set_tuning(self, col: int = -1, spmv: int = -1):
+        """Forces the Poisson kernel variants (-1: autotune on the first solve)."""
+        _lib.check(self.lib.orctm_set_tuning(self.h, col, spmv), self.h)
+
+    def tuning(self, precision: str = "fp64") -> tuple:
+        c, s = C.c_int(), C.c_int()
+        pr = 1 if precision == "fp32_refined" else 0
+        _lib.check(self.lib.orctm_get_tuning(self.h, pr, C.byref(c), C.byref(s)), self.h)
+        return c.value, s.value
+
+    def device_bytes(self) -> int:
+        """Device bytes this instance holds (state, tables, solver vectors)."""
+        n = C.c_ulonglong()
+        _lib.check(self.lib.orctm_device_bytes(self.h, C.byref(n)), self.h)
+        return int(n.value)
+
     # -- device timing -------------------------------------------------------
     def timer_start(self):
         _lib.check(self.lib.orctm_timer_start(self.h), self.h)

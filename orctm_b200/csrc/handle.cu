@@ -13,6 +13,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -38,6 +41,54 @@ namespace {
 
 thread_local std::string g_create_error;
 
+// One stream-ordered memory pool per device, owned by the library.  Freed
+// blocks stay reserved in the pool (release threshold: unlimited), so a
+// handle created after another was destroyed reuses its memory without
+// mapping new pages; orctm_trim_device_memory returns them to the driver.
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[256] = {};
+
+int device_pool(int dev, cudaMemPool_t* out) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (dev < 0 || dev >= 256) return ORCTM_E_ARG;
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t mp = nullptr;
+    ORCTM_CUDA_OK(cudaMemPoolCreate(&mp, &props));
+    unsigned long long thr = ~0ULL;
+    ORCTM_CUDA_OK(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr));
+    g_pools[dev] = mp;
+  }
+  *out = g_pools[dev];
+  return ORCTM_OK;
+}
+
+// Pinned host mirrors of the solver scalars come from slabs that are never
+// freed: cudaFreeHost would wait for the whole device.
+std::mutex g_pin_mu;
+std::vector<SolverState*> g_pin_free;
+
+SolverState* pinned_state_get() {
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  if (g_pin_free.empty()) {
+    constexpr int kSlab = 64;
+    SolverState* slab = nullptr;
+    if (cudaMallocHost((void**)&slab, sizeof(SolverState) * kSlab) != cudaSuccess) return nullptr;
+    for (int k = kSlab - 1; k >= 0; --k) g_pin_free.push_back(slab + k);
+  }
+  SolverState* s = g_pin_free.back();
+  g_pin_free.pop_back();
+  return s;
+}
+
+void pinned_state_put(SolverState* s) {
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  g_pin_free.push_back(s);
+}
+
 enum Kind { KP = 0, KU = 1, KV = 2, KW = 3, K2P = 4 };
 
 constexpr int kNumFixed = ORCTM_F_THO;  // fields before the tracers
@@ -62,6 +113,8 @@ using namespace orctm;
 struct orctm_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t mempool = nullptr;  // the library's stream-ordered pool of this device
+  size_t bytes = 0;                 // device bytes allocated by this handle
   Layout L{};
   Geo G{};
   PoissonGeo P{};
@@ -86,7 +139,12 @@ struct orctm_handle {
   float *r32b = nullptr, *r32 = nullptr, *z32 = nullptr, *p32a = nullptr, *p32b = nullptr,
         *q32 = nullptr, *d32 = nullptr;
   SolverState* S = nullptr;
+  SolverState* S_tune = nullptr;  // scratch scalars for the autotuner
+  SolverState* S_tune0 = nullptr; // their initial value
   double* partials = nullptr;
+  // kernel variants per precision (0 FP64, 1 FP32); -1 = not chosen yet
+  int col_var[2] = {-1, -1}, spmv_var[2] = {-1, -1};
+  int force_col = -1, force_spmv = -1;  // orctm_set_tuning
   SolverState* hS = nullptr;  // pinned mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t tm0 = nullptr, tm1 = nullptr;  // orctm_timer_start / _stop
@@ -144,8 +202,9 @@ struct orctm_handle {
       return ORCTM_OK;
     }
     double* p = nullptr;
-    ORCTM_CUDA_OK(cudaMalloc(&p, sizeof(double) * L.n3()));
+    ORCTM_CUDA_OK(cudaMallocFromPoolAsync((void**)&p, sizeof(double) * L.n3(), mempool, stream));
     ORCTM_CUDA_OK(cudaMemsetAsync(p, 0, sizeof(double) * L.n3(), stream));
+    bytes += sizeof(double) * L.n3();
     refs[p] = 1;
     *out = p;
     return ORCTM_OK;
@@ -175,8 +234,10 @@ struct orctm_handle {
   }
   template <typename T>
   int dev_alloc(T** p, size_t n) {
-    ORCTM_CUDA_OK(cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(n, 1)));
-    ORCTM_CUDA_OK(cudaMemset(*p, 0, sizeof(T) * std::max<size_t>(n, 1)));
+    const size_t nb = sizeof(T) * std::max<size_t>(n, 1);
+    ORCTM_CUDA_OK(cudaMallocFromPoolAsync((void**)p, nb, mempool, stream));
+    ORCTM_CUDA_OK(cudaMemsetAsync(*p, 0, nb, stream));
+    bytes += nb;
     owned.push_back(*p);
     return ORCTM_OK;
   }
@@ -309,8 +370,8 @@ int setup(orctm_handle* h, const orctm_desc* d) {
     int s2;
     if ((s2 = h->dev_alloc(&dk, n2))) return s2;
     if ((s2 = h->dev_alloc(&db, n2))) return s2;
-    ORCTM_CUDA_OK(cudaMemcpy(dk, kb.data(), sizeof(int) * n2, cudaMemcpyHostToDevice));
-    ORCTM_CUDA_OK(cudaMemcpy(db, bot.data(), sizeof(double) * n2, cudaMemcpyHostToDevice));
+    ORCTM_CUDA_OK(cudaMemcpyAsync(dk, kb.data(), sizeof(int) * n2, cudaMemcpyHostToDevice, h->stream));
+    ORCTM_CUDA_OK(cudaMemcpyAsync(db, bot.data(), sizeof(double) * n2, cudaMemcpyHostToDevice, h->stream));
     cg.kb = dk;
     cg.bot = db;
     return ORCTM_OK;
@@ -323,8 +384,8 @@ int setup(orctm_handle* h, const orctm_desc* d) {
   double *ddzw, *ddi;
   if ((st = h->dev_alloc(&ddzw, KE))) return st;
   if ((st = h->dev_alloc(&ddi, KE + 1))) return st;
-  ORCTM_CUDA_OK(cudaMemcpy(ddzw, d->dzw, sizeof(double) * KE, cudaMemcpyHostToDevice));
-  ORCTM_CUDA_OK(cudaMemcpy(ddi, d->di, sizeof(double) * (KE + 1), cudaMemcpyHostToDevice));
+  ORCTM_CUDA_OK(cudaMemcpyAsync(ddzw, d->dzw, sizeof(double) * KE, cudaMemcpyHostToDevice, h->stream));
+  ORCTM_CUDA_OK(cudaMemcpyAsync(ddi, d->di, sizeof(double) * (KE + 1), cudaMemcpyHostToDevice, h->stream));
   G.dzw = ddzw;
   G.di = ddi;
 
@@ -381,7 +442,7 @@ int setup(orctm_handle* h, const orctm_desc* d) {
       double* q;
       int s2;
       if ((s2 = h->dev_alloc(&q, v.size()))) return s2;
-      ORCTM_CUDA_OK(cudaMemcpy(q, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+      ORCTM_CUDA_OK(cudaMemcpyAsync(q, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, h->stream));
       dst = q;
       return ORCTM_OK;
     };
@@ -459,7 +520,7 @@ int setup(orctm_handle* h, const orctm_desc* d) {
     double* p;
     int s2;
     if ((s2 = h->dev_alloc(&p, v.size()))) return s2;
-    ORCTM_CUDA_OK(cudaMemcpy(p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+    ORCTM_CUDA_OK(cudaMemcpyAsync(p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, h->stream));
     dst = p;
     return ORCTM_OK;
   };
@@ -496,11 +557,12 @@ int setup(orctm_handle* h, const orctm_desc* d) {
   const int maxb = (int)solver_max_blocks(G);
   if ((st = h->dev_alloc(&h->S, 1))) return st;
   if ((st = h->dev_alloc(&h->partials, (size_t)4 * maxb))) return st;
-  ORCTM_CUDA_OK(cudaMallocHost(&h->hS, sizeof(SolverState)));
+  if (!(h->hS = pinned_state_get())) return h->fail(ORCTM_E_NOMEM, "pinned host memory exhausted");
   std::memset(h->hS, 0, sizeof(SolverState));
   h->hS->max_blocks = maxb;
+  h->hS->rows = G.L.je - 2;
   h->hS->partials = h->partials;
-  ORCTM_CUDA_OK(cudaMemcpy(h->S, h->hS, sizeof(SolverState), cudaMemcpyHostToDevice));
+  ORCTM_CUDA_OK(cudaMemcpyAsync(h->S, h->hS, sizeof(SolverState), cudaMemcpyHostToDevice, h->stream));
   ORCTM_CUDA_OK(cudaEventCreate(&h->ev0));
   ORCTM_CUDA_OK(cudaEventCreate(&h->ev1));
   ORCTM_CUDA_OK(cudaEventCreate(&h->tm0));
@@ -540,14 +602,16 @@ template <typename T, typename TX>
 int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* pa, T* pb, T* q,
              int maxit, int* iters, int* conv) {
   const Geo& G = h->G;
-  launch_pcg_col<T, TX>(G, h->P, h->S, init_mode, b, x, r, nullptr, nullptr, z, h->stream);
+  const int pr = sizeof(T) == 4;
+  const int cv = h->col_var[pr], sv = h->spmv_var[pr];
+  launch_pcg_col<T, TX>(G, h->P, h->S, init_mode, b, x, r, nullptr, nullptr, z, cv, h->stream);
   ORCTM_CUDA_OK(cudaGetLastError());
   const int check = 8;
   int it = 0;
   T *pc = pa, *pn = pb;
   for (; it < maxit; ++it) {
-    PROF(h, ORCTM_PROF_PCG_SPMV, (launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, h->stream)));
-    PROF(h, ORCTM_PROF_PCG_COL, (launch_pcg_col<T, TX>(G, h->P, h->S, 2, b, x, r, pn, q, z, h->stream)));
+    PROF(h, ORCTM_PROF_PCG_SPMV, (launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, sv, h->stream)));
+    PROF(h, ORCTM_PROF_PCG_COL, (launch_pcg_col<T, TX>(G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream)));
     std::swap(pc, pn);
     if ((it + 1) % check == 0 || it + 1 == maxit) {
       int st;
@@ -563,6 +627,102 @@ int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* p
   return ORCTM_OK;
 }
 
+// Autotuner.  Times every usable variant of the column kernel and of the
+// stencil kernel on this handle's grid in precision T and keeps the fastest
+// (two untimed launches, then three timed with CUDA events).  It runs before
+// the first solve of the precision, on solver vectors that the solve writes
+// before it reads them (x is zeroed before every inner solve), with scratch
+// solver scalars.  The variants compute bit-identical results (the dot
+// products are summed in a fixed order), so the choice changes only speed.
+// Choices are cached per grid size and precision for later handles.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tune_cache;
+
+template <typename T>
+int autotune(orctm_handle* h, T* x, T* r, T* z, T* pa, T* pb, T* q) {
+  const Geo& G = h->G;
+  const int pr = sizeof(T) == 4;
+  const auto key = std::make_tuple(G.L.ie, G.L.je, G.L.ke, pr);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      h->col_var[pr] = h->force_col >= 0 ? h->force_col : it->second.first;
+      h->spmv_var[pr] = h->force_spmv >= 0 ? h->force_spmv : it->second.second;
+      return ORCTM_OK;
+    }
+  }
+  if (!h->S_tune) {
+    int st;
+    if ((st = h->dev_alloc(&h->S_tune, 1)) || (st = h->dev_alloc(&h->S_tune0, 1))) return st;
+    SolverState s0 = *h->hS;
+    s0.converged = 0;
+    s0.alpha = 0.0;
+    s0.beta = 0.0;
+    s0.rho = 1.0;
+    s0.bb = 1.0;
+    s0.tol = 0.0;
+    s0.ticket = 0;
+    ORCTM_CUDA_OK(cudaMemcpyAsync(h->S_tune0, &s0, sizeof(SolverState), cudaMemcpyHostToDevice,
+                                  h->stream));
+  }
+  auto timed = [&](auto launch, float* best_ms) -> int {
+    float tot = 0.f;
+    for (int rep = 0; rep < 5; ++rep) {
+      ORCTM_CUDA_OK(cudaMemcpyAsync(h->S_tune, h->S_tune0, sizeof(SolverState),
+                                    cudaMemcpyDeviceToDevice, h->stream));
+      if (rep >= 2) ORCTM_CUDA_OK(cudaEventRecord(h->ev0, h->stream));
+      launch();
+      ORCTM_CUDA_OK(cudaGetLastError());
+      if (rep >= 2) {
+        ORCTM_CUDA_OK(cudaEventRecord(h->ev1, h->stream));
+        ORCTM_CUDA_OK(cudaEventSynchronize(h->ev1));
+        float ms = 0.f;
+        ORCTM_CUDA_OK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        tot += ms;
+      }
+    }
+    *best_ms = tot;
+    return ORCTM_OK;
+  };
+  int st, best_c = 0, best_s = 0;
+  float bc = 1e30f, bs = 1e30f;
+  for (int v = 0; v < pcg_col_variants(); ++v) {
+    if (!pcg_col_variant_ok<T>(G, v)) continue;
+    float ms;
+    if ((st = timed([&] { launch_pcg_col<T, T>(G, h->P, h->S_tune, 2, nullptr, x, r, pa, q, z, v,
+                                               h->stream); }, &ms)))
+      return st;
+    if (ms < bc) { bc = ms; best_c = v; }
+  }
+  for (int v = 0; v < pcg_spmv_variants(); ++v) {
+    float ms;
+    if ((st = timed([&] { launch_pcg_spmv<T>(G, h->P, h->S_tune, z, pa, pb, q, 0, v, h->stream); },
+                    &ms)))
+      return st;
+    if (ms < bs) { bs = ms; best_s = v; }
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = {best_c, best_s};
+  }
+  h->col_var[pr] = h->force_col >= 0 ? h->force_col : best_c;
+  h->spmv_var[pr] = h->force_spmv >= 0 ? h->force_spmv : best_s;
+  return ORCTM_OK;
+}
+
+int ensure_tuned(orctm_handle* h, bool f32) {
+  const int pr = f32 ? 1 : 0;
+  if (h->col_var[pr] >= 0 && h->spmv_var[pr] >= 0) return ORCTM_OK;
+  if (h->force_col >= 0 && h->force_spmv >= 0) {
+    h->col_var[pr] = h->force_col;
+    h->spmv_var[pr] = h->force_spmv;
+    return ORCTM_OK;
+  }
+  if (f32) return autotune<float>(h, h->d32, h->r32, h->z32, h->p32a, h->p32b, h->q32);
+  return autotune<double>(h, h->d, h->rw, h->z, h->p0, h->p1, h->q);
+}
+
 // Solves A x = b (b in h->b, x in h->xs holding the warm start) by iterative
 // refinement: r = b - A x in double-double against the exact operator, then
 // a PCG correction on the row-scaled operator (FP64, or FP32 for the refined
@@ -573,6 +733,7 @@ int poisson_solve(orctm_handle* h, orctm_solve_stats* stats) {
   orctm_solve_stats s{};
   const bool f32 = h->solver_mode == ORCTM_SOLVER_FP32_REFINED;
   const size_t n3 = (size_t)h->L.n3();
+  if ((st = ensure_tuned(h, f32))) return st;
   ORCTM_CUDA_OK(cudaEventRecord(h->ev0, h->stream));
   int total = 0, outer = 0;
   double prev = 1e300, rel = 0.0;
@@ -770,7 +931,7 @@ const char* orctm_status_string(int s) {
     case ORCTM_E_GEOMETRY: return "geometry is not of the BODEN form";
     case ORCTM_E_UNSUPPORTED: return "option outside the implemented path";
     case ORCTM_E_NODEVICE: return "no usable CUDA device";
-    case ORCTM_E_TOO_LARGE: return "grid larger than the scratch-free entry point's limit";
+    case ORCTM_E_TOO_LARGE: return "grid too large (2^31 elements per padded field, or the scratch-free entry point's limit)";
     default: return "unknown status";
   }
 }
@@ -787,10 +948,14 @@ int orctm_destroy(orctm_handle* h) {
   for (auto& kv : h->refs) all.push_back(kv.first);
   std::sort(all.begin(), all.end());
   all.erase(std::unique(all.begin(), all.end()), all.end());
-  for (double* p : all) cudaFree(p);
-  for (void* p : h->owned) cudaFree(p);
-  if (h->hS) cudaFreeHost(h->hS);
-  if (h->stream) cudaStreamSynchronize(h->stream);
+  // stream-ordered frees: no device-wide synchronisation, so other handles'
+  // work in flight on the device is not stalled
+  if (h->stream) {
+    for (double* p : all) cudaFreeAsync(p, h->stream);
+    for (void* p : h->owned) cudaFreeAsync(p, h->stream);
+    cudaStreamSynchronize(h->stream);
+  }
+  if (h->hS) pinned_state_put(h->hS);
   for (int k = 0; k < ORCTM_PROF_KINDS; ++k)
     for (auto& pr : h->prof_pairs[k]) {
       h->ev_pool.push_back(pr.first);
@@ -815,6 +980,12 @@ int orctm_create(const orctm_desc* d, orctm_handle** out) {
     return st;
   };
   if (d->ie < 4 || d->je < 3 || d->ke < 2 || d->ke > kMaxKe) return bad(ORCTM_E_ARG, "grid size out of range");
+  {
+    // the solver kernels index a padded field with 32-bit offsets
+    const long long pitch = ((long long)d->ie + 1 + 31) / 32 * 32;
+    if (pitch * ((long long)d->je + 1) * ((long long)d->ke + 1) >= (1LL << 31))
+      return bad(ORCTM_E_TOO_LARGE, "padded field exceeds 2^31 elements");
+  }
   if (d->i_start != 0 || d->j_start != 0) return bad(ORCTM_E_UNSUPPORTED, "only single-rank domains (I_start = J_start = 0)");
   if (d->ntracers < 2 || d->ntracers > kMaxTracers) return bad(ORCTM_E_ARG, "ntracers must be in [2, 8]");
   if (!(d->dt > 0)) return bad(ORCTM_E_ARG, "dt must be positive");
@@ -831,6 +1002,7 @@ int orctm_create(const orctm_desc* d, orctm_handle** out) {
   h->device = d->device;
   int st = cuda_status(cudaSetDevice(h->device));
   if (!st) st = cuda_status(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  if (!st) st = device_pool(h->device, &h->mempool);
   if (!st) st = setup(h, d);
   if (st) {
     g_create_error = h->err.empty() ? orctm_status_string(st) : h->err;
@@ -975,5 +1147,36 @@ int orctm_profile_get(orctm_handle* h, int kind, long long* launches, double* to
 }
 
 unsigned long long orctm_kernel_launches(void) { return launch_count(); }
+
+int orctm_set_tuning(orctm_handle* h, int col_variant, int spmv_variant) {
+  if (!h || col_variant < -1 || col_variant >= pcg_col_variants() || spmv_variant < -1 ||
+      spmv_variant >= pcg_spmv_variants())
+    return ORCTM_E_ARG;
+  h->force_col = col_variant;
+  h->force_spmv = spmv_variant;
+  for (int pr = 0; pr < 2; ++pr) h->col_var[pr] = h->spmv_var[pr] = -1;
+  return ORCTM_OK;
+}
+
+int orctm_get_tuning(const orctm_handle* h, int precision, int* col_variant, int* spmv_variant) {
+  if (!h || precision < 0 || precision > 1 || !col_variant || !spmv_variant) return ORCTM_E_ARG;
+  *col_variant = h->col_var[precision];
+  *spmv_variant = h->spmv_var[precision];
+  return ORCTM_OK;
+}
+
+int orctm_device_bytes(const orctm_handle* h, unsigned long long* bytes) {
+  if (!h || !bytes) return ORCTM_E_ARG;
+  *bytes = h->bytes;
+  return ORCTM_OK;
+}
+
+int orctm_trim_device_memory(int device) {
+  cudaMemPool_t mp = nullptr;
+  int st = device_pool(device, &mp);
+  if (st) return st;
+  ORCTM_CUDA_OK(cudaMemPoolTrimTo(mp, 0));
+  return ORCTM_OK;
+}
 
 }  // extern "C"

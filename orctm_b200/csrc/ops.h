@@ -24,7 +24,8 @@ struct SolverState {
   int converged;  // 0 running, 1 converged, 2 NaN, 3 breakdown
   int iter;
   unsigned ticket;
-  int max_blocks;
+  int rows;          // JE - 2: rows of unknowns, the reduction's row count
+  int max_blocks;    // partial sums per quantity: 32-column chunks x rows
   double* partials;  // [4 * max_blocks]
 };
 
@@ -62,10 +63,16 @@ void launch_factor(const Geo& G, const PoissonGeo& P, double* dinv64, float* din
 size_t solver_max_blocks(const Geo& G);
 template <typename T, typename TX>
 void launch_pcg_col(const Geo& G, const PoissonGeo& P, SolverState* S, int mode, const T* b, TX* x,
-                    T* r, const T* p, const T* q, T* z, cudaStream_t st);
+                    T* r, const T* p, const T* q, T* z, int variant, cudaStream_t st);
 template <typename T>
 void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
-                     T* pnew, T* q, int first, cudaStream_t st);
+                     T* pnew, T* q, int first, int variant, cudaStream_t st);
+// kernel variants the autotuner chooses between (a variant a grid cannot use
+// falls back to variant 0)
+int pcg_col_variants();
+template <typename T>
+bool pcg_col_variant_ok(const Geo& G, int variant);
+int pcg_spmv_variants();
 void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b,
                   const double* x, double* r, cudaStream_t st);
 void launch_axpy_f64(const Geo& G, const double* d, double* x, cudaStream_t st);

@@ -151,22 +151,6 @@ __device__ __forceinline__ Coef row(const ColC& c, const PoissonGeo& P, int K, i
   return r;
 }
 
-// Row K of B for a regular level (2 <= K <= kreg): all six neighbours wet,
-// vertical factors from the 1D tables.  Same values as row<true>.
-__device__ __forceinline__ Coef row_regular(const ColC& c, const double* zw, const double* iz,
-                                            int K) {
-  const double zw0 = zw[K - 1], zw1 = zw[K], hs = iz[K - 1];
-  Coef r;
-  r.u = zw0;
-  r.d = zw1;
-  r.w = c.iw ? c.cw * hs : 0.0;
-  r.e = c.ie ? c.ce * hs : 0.0;
-  r.n = c.in ? c.cn * hs : 0.0;
-  r.s = c.is ? c.cs * hs : 0.0;
-  r.dc = -((c.xcf + c.ycf) * hs + (zw0 + zw1));
-  return r;
-}
-
 // vertical entries only (the preconditioner's tridiagonal)
 template <bool SCALED>
 __device__ __forceinline__ double down_of(const ColC& c, const PoissonGeo& P, int K, int KE) {
@@ -176,54 +160,55 @@ __device__ __forceinline__ double down_of(const ColC& c, const PoissonGeo& P, in
 }
 
 // ------------------------------------------------------- reductions ------
-// Stores this block's partials; returns true in thread 0 of the last block
-// to finish, which then holds the totals (added in block order) in v.
+// Every kernel that reduces has blocks of 32 x BY threads, a warp being 32
+// consecutive columns i of one row j.  Each warp writes one partial sum at
+// its canonical index (row j, 32-column chunk), and the last block to finish
+// (atomic ticket) adds the partials in index order with a fixed 64-thread
+// pattern, so the totals do not depend on the block shape of the variant that
+// ran.  Returns true in thread 0 of the last block, which then holds the
+// totals in v.
 template <int NV>
 __device__ bool grid_sum(double (&v)[NV], SolverState* S) {
-  __shared__ double sh[NV * 32];
+  __shared__ double sh[NV * 2];
   __shared__ bool last;
-  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  const int nthreads = blockDim.x * blockDim.y;
-  const int nw = (nthreads + 31) >> 5;
+  const int lane = threadIdx.x, tid = threadIdx.x + 32 * threadIdx.y;
+  const unsigned nchunk = gridDim.x;
+  const unsigned nrow = (unsigned)S->rows;  // JE - 2 rows of unknowns
+  const unsigned row = blockIdx.y * blockDim.y + threadIdx.y;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     double x = v[q];
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) sh[q * 32 + warp] = x;
+    if (lane == 0 && row < nrow) S->partials[(size_t)q * S->max_blocks + row * nchunk + blockIdx.x] = x;
   }
+  __threadfence();
   __syncthreads();
   const unsigned nb = gridDim.x * gridDim.y;
-  const unsigned bid = blockIdx.x + gridDim.x * blockIdx.y;
   if (tid == 0) {
-    for (int q = 0; q < NV; ++q) {
-      double x = 0.0;
-      for (int w = 0; w < nw; ++w) x += sh[q * 32 + w];
-      S->partials[(size_t)q * S->max_blocks + bid] = x;
-    }
-    __threadfence();
     const unsigned t = atomicAdd(&S->ticket, 1u);
     last = (t == nb - 1);
   }
   __syncthreads();
   if (!last) return false;
   __threadfence();
+  const unsigned n = nrow * nchunk;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     double x = 0.0;
-    for (unsigned b = tid; b < nb; b += nthreads)
-      x += ((volatile double*)S->partials)[(size_t)q * S->max_blocks + b];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    __syncthreads();
-    if (lane == 0) sh[q * 32 + warp] = x;
-    __syncthreads();
-    if (tid == 0) {
-      double y = 0.0;
-      for (int w = 0; w < nw; ++w) y += sh[q * 32 + w];
-      v[q] = y;
+    if (tid < 64)
+      for (unsigned b = tid; b < n; b += 64)
+        x += ((volatile double*)S->partials)[(size_t)q * S->max_blocks + b];
+    if (tid < 64) {
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[q * 2 + (tid >> 5)] = x;
     }
   }
-  if (tid == 0) S->ticket = 0;
+  __syncthreads();
+  if (tid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = sh[q * 2] + sh[q * 2 + 1];
+    S->ticket = 0;
+  }
   return tid == 0;
 }
 
@@ -255,92 +240,118 @@ __global__ void k_factor(Geo G, PoissonGeo P, double* __restrict__ dinv64,
 // dots r.z and r.r.
 //   MODE 1 (init, x = 0):   r = b / ZP   (the right-hand side of B x = b / ZP)
 //   MODE 2 (iteration):     x += alpha p ; r -= alpha q
-template <typename T, int MODE>
+// The column tridiagonal is symmetric (a(K+1) = c(K) = ZW(K+1)), so
+// M = L D L^T with y = L^-1 r from the forward sweep and r.z = sum dinv y^2:
+// the dot needs no second pass over r.  With SM the forward values y are
+// kept in shared memory ([level][thread], blockDim.x * blockDim.y * KE
+// elements) for the backward sweep; otherwise they go through z.
+template <typename T, int MODE, bool SM, int U>
 __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverState* S,
                                                  const T* __restrict__ b, T* __restrict__ x,
                                                  T* __restrict__ r, const T* __restrict__ p,
                                                  const T* __restrict__ q, T* __restrict__ z) {
+  extern __shared__ __align__(16) unsigned char col_smem[];
+  T* ys = reinterpret_cast<T*>(col_smem);
+  __shared__ T szw[kMaxKe + 1];
   if (S->converged) return;
   const int KE = G.L.ke, IE = G.L.ie, JE = G.L.je;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  const double alpha = MODE == 2 ? S->alpha : 0.0;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+  for (int e = tid; e <= KE; e += nt) szw[e] = (T)P.zwn[e];
+  __syncthreads();
+  // arithmetic in T: the FP32 inner solve computes in FP32 (dots summed in T
+  // over U levels, then in FP64)
+  const T alpha = MODE == 2 ? (T)S->alpha : T(0);
   // pivots rounded to FP32 in both precisions: a fixed preconditioner that
   // moves half the bytes (the operator apply and the vectors keep precision T)
   const float* __restrict__ dinv = P.dinv32;
   double rz = 0.0, rr = 0.0, bb = 0.0;
   if (i <= IE - 1 && j <= JE - 1) {
     const ColC c = load_col(G, P, i, j);
-    double yprev = 0.0, dprev = 0.0;
-    const long long base = G.L.at(i, j, 0), plane = G.L.plane;
-    constexpr int U = 4;  // levels whose loads are issued together
+    const T zwa = (T)c.zwa;
+    const int kb = c.kb;
+    T yprev = 0, dprev = 0;
+    const unsigned base = (unsigned)G.L.at(i, j, 0), plane = (unsigned)G.L.plane;
+    // U: levels whose loads are issued together
     for (int K0 = 1; K0 <= KE; K0 += U) {
-      double lb[U], lr[U], lp[U], lq[U], lx[U], ld[U];
+      T lb[U], lr[U], lp[U], lq[U], lx[U], ld[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int K = K0 + u;
-        lb[u] = lr[u] = lp[u] = lq[u] = lx[u] = ld[u] = 0.0;
+        lb[u] = lr[u] = lp[u] = lq[u] = lx[u] = ld[u] = T(0);
         if (K <= KE) {
-          const long long o = base + plane * (K - 1);
+          const unsigned o = base + plane * (unsigned)(K - 1);
           if (MODE == 1) {
-            lb[u] = (double)b[o];
+            lb[u] = b[o];
           } else {
-            lr[u] = (double)r[o];
-            lp[u] = (double)p[o];
-            lq[u] = (double)q[o];
-            lx[u] = (double)x[o];
+            lr[u] = r[o];
+            lp[u] = p[o];
+            lq[u] = q[o];
+            lx[u] = x[o];
           }
-          ld[u] = (double)dinv[o];
+          ld[u] = (T)dinv[o];
         }
       }
+      // partial dots are flushed to FP64 at every fourth level (K = 4, 8, ...)
+      // and at the end, whatever U is
+      T rzt = 0, rrt = 0, bbt = 0;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int K = K0 + u;
         if (K > KE) break;
-        const long long o = base + plane * (K - 1);
-        double rk;
-        if (MODE == 1) {
-          rk = lb[u] * izp_of(c, P, K);
-          bb += rk * rk;
-        } else {
-          x[o] = (T)(lx[u] + alpha * lp[u]);
-          rk = lr[u] - alpha * lq[u];
+        if (u == 4) {
+          rz += (double)rzt;
+          rr += (double)rrt;
+          bb += (double)bbt;
+          rzt = rrt = bbt = 0;
         }
-        const T rkt = (T)rk;
-        r[o] = rkt;
-        rk = (double)rkt;
-        rr += rk * rk;
-        const double up = (K == 1 || K > c.kb) ? 0.0 : zw_of(c, P, K);  // a(K) of B
-        const double y = rk - (up * dprev) * yprev;
-        z[o] = (T)y;  // y' kept in z until the backward sweep
-        yprev = (double)(T)y;
+        const unsigned o = base + plane * (unsigned)(K - 1);
+        T rk;
+        if (MODE == 1) {
+          rk = (T)((double)lb[u] * izp_of(c, P, K));
+          bbt = fma(rk, rk, bbt);
+        } else {
+          x[o] = fma(alpha, lp[u], lx[u]);
+          rk = fma(-alpha, lq[u], lr[u]);
+        }
+        r[o] = rk;
+        rrt = fma(rk, rk, rrt);
+        // a(K) of B: ZW(K) above a wet level below the surface
+        const T up = (K == 1 || K > kb) ? T(0) : (K == kb ? zwa : szw[K - 1]);
+        const T yt = fma(-(up * dprev), yprev, rk);
+        if (SM) ys[(K - 1) * nt + tid] = yt;
+        else z[o] = yt;  // y kept in z until the backward sweep
+        yprev = yt;
         dprev = ld[u];
+        rzt = fma(yt * yt, dprev, rzt);
       }
+      rz += (double)rzt;
+      rr += (double)rrt;
+      bb += (double)bbt;
     }
-    double znext = 0.0;
+    T znext = 0;
     for (int K1 = KE; K1 >= 1; K1 -= U) {
-      double ly[U], ld[U], lr[U];
+      T ly[U], ld[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int K = K1 - u;
-        ly[u] = ld[u] = lr[u] = 0.0;
+        ly[u] = ld[u] = T(0);
         if (K >= 1) {
-          const long long o = base + plane * (K - 1);
-          ly[u] = (double)z[o];
-          ld[u] = (double)dinv[o];
-          lr[u] = (double)r[o];
+          const unsigned o = base + plane * (unsigned)(K - 1);
+          ly[u] = SM ? ys[(K - 1) * nt + tid] : z[o];
+          ld[u] = (T)dinv[o];
         }
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int K = K1 - u;
         if (K < 1) break;
-        const double dn = down_of<true>(c, P, K, KE);
-        const double zk = (ly[u] - dn * znext) * ld[u];
-        const T zt = (T)zk;
-        z[base + plane * (K - 1)] = zt;
-        znext = (double)zt;
-        rz += lr[u] * znext;
+        // c(K) of B: ZW(K+1) when level K+1 is wet
+        const T dn = (K >= kb || K == KE) ? T(0) : (K + 1 == kb ? zwa : szw[K]);
+        const T zt = fma(-dn, znext, ly[u]) * ld[u];
+        z[base + plane * (unsigned)(K - 1)] = zt;
+        znext = zt;
       }
     }
   }
@@ -361,33 +372,39 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
 }
 
 // Stencil kernel: p = z + beta p_old (first iteration: p = z), q = B p, and
-// the dot p.q; alpha = rho / (p.q).  A block of 32 x 4 columns marches down
-// the levels; p of its 34 x 6 halo tile is formed once per level into a
+// the dot p.q; alpha = rho / (p.q).  A block of 32 x kTy columns marches down
+// the levels; p of its 34 x (kTy+2) halo tile is formed once per level into a
 // three-level shared-memory ring, and the 7-point product reads the ring.
-constexpr int kTx = 32, kTy = 4, kHx = kTx + 2, kHy = kTy + 2;
+// Arithmetic is in the storage type T (the FP32 inner solve computes in
+// FP32; the dot is accumulated per thread in T over 8 levels, then in FP64).
+// Offsets are 32-bit: a padded field has fewer than 2^31 elements
+// (checked when the handle is created).
+constexpr int kTx = 32;
 
-template <typename T>
-__global__ void __launch_bounds__(128) k_pcg_spmv(Geo G, PoissonGeo P, SolverState* S,
-                                                  const T* __restrict__ z,
-                                                  const T* __restrict__ pold, T* __restrict__ pnew,
-                                                  T* __restrict__ q, int first) {
+template <typename T, int kTy>
+__global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, SolverState* S,
+                                                       const T* __restrict__ z,
+                                                       const T* __restrict__ pold,
+                                                       T* __restrict__ pnew, T* __restrict__ q,
+                                                       int first) {
+  constexpr int kHx = kTx + 2, kHy = kTy + 2;
   constexpr int kH = kHx * kHy, kNt = kTx * kTy, kF = (kH + kNt - 1) / kNt;
   __shared__ T ring[3][kH];
-  __shared__ double szw[kMaxKe + 1], siz[kMaxKe];
+  __shared__ T szw[kMaxKe + 1], siz[kMaxKe];
   if (S->converged) return;
-  for (int e = threadIdx.x + kTx * threadIdx.y; e <= G.L.ke; e += kTx * kTy) {
-    szw[e] = P.zwn[e];
-    if (e < G.L.ke) siz[e] = P.izn[e];
-  }
   const int KE = G.L.ke, IE = G.L.ie, JE = G.L.je;
-  const long long plane = G.L.plane;
+  const unsigned plane = (unsigned)G.L.plane;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kTx * ty;
+  for (int e = tid; e <= KE; e += kNt) {
+    szw[e] = (T)P.zwn[e];
+    if (e < KE) siz[e] = (T)P.izn[e];
+  }
   const int i0 = blockIdx.x * kTx + 2, j0 = blockIdx.y * kTy + 2;
   const int i = i0 + tx, j = j0 + ty;
   const bool act = i <= IE - 1 && j <= JE - 1;
-  const double beta = first ? 0.0 : S->beta;
+  const T beta = first ? T(0) : (T)S->beta;
   // halo-tile entries this thread fills: offsets at level 1, validity
-  long long fo[kF];
+  unsigned fo[kF];
   int fs[kF];
   bool fv[kF];
 #pragma unroll
@@ -397,42 +414,52 @@ __global__ void __launch_bounds__(128) k_pcg_spmv(Geo G, PoissonGeo P, SolverSta
     const int ii = i0 - 1 + hx, jj = j0 - 1 + hy;
     fs[f] = e < kH ? e : -1;
     fv[f] = e < kH && ii >= 2 && ii <= IE - 1 && jj >= 2 && jj <= JE - 1;
-    fo[f] = fv[f] ? G.L.at(ii, jj, 0) : 0;
+    fo[f] = fv[f] ? (unsigned)G.L.at(ii, jj, 0) : 0u;
   }
   // the halo values of two levels ahead are held in registers, so the loads of
   // level K+3 are in flight while level K is computed
-  double qz[2][kF], qp[2][kF];
+  T qz[2][kF], qp[2][kF];
   auto load = [&](int slot, int K) {
 #pragma unroll
     for (int f = 0; f < kF; ++f) {
-      qz[slot][f] = 0.0;
-      qp[slot][f] = 0.0;
+      qz[slot][f] = T(0);
+      qp[slot][f] = T(0);
       if (fv[f] && K <= KE) {
-        const long long o = fo[f] + plane * (K - 1);
-        qz[slot][f] = (double)z[o];
-        if (!first) qp[slot][f] = (double)pold[o];
+        const unsigned o = fo[f] + plane * (unsigned)(K - 1);
+        qz[slot][f] = z[o];
+        if (!first) qp[slot][f] = pold[o];
       }
     }
   };
   auto store = [&](T* dst, int slot) {
 #pragma unroll
     for (int f = 0; f < kF; ++f)
-      if (fs[f] >= 0)
-        dst[fs[f]] = first ? (T)qz[slot][f] : (T)(qz[slot][f] + beta * qp[slot][f]);
+      if (fs[f] >= 0) dst[fs[f]] = first ? qz[slot][f] : fma(beta, qp[slot][f], qz[slot][f]);
   };
   ColC c;
-  if (act) c = load_col(G, P, i, j);
-  const long long own = act ? G.L.at(i, j, 0) : 0;
+  T cw = 0, ce = 0, cn = 0, cs = 0, xyc = 0;
+  int kreg = 0;
+  if (act) {
+    c = load_col(G, P, i, j);
+    cw = c.iw ? (T)c.cw : T(0);
+    ce = c.ie ? (T)c.ce : T(0);
+    cn = c.in ? (T)c.cn : T(0);
+    cs = c.is ? (T)c.cs : T(0);
+    xyc = (T)(c.xcf + c.ycf);
+    kreg = c.kreg;
+  }
+  const unsigned own = act ? (unsigned)G.L.at(i, j, 0) : 0u;
   const int me = (ty + 1) * kHx + (tx + 1);
   T* prv = ring[0];
   T* cur = ring[1];
   T* nxt = ring[2];
-  for (int e = threadIdx.x + kTx * threadIdx.y; e < kH; e += kNt) prv[e] = (T)0;
+  for (int e = tid; e < kH; e += kNt) prv[e] = T(0);
   load(0, 1);
   store(cur, 0);
   load(0, 2);
   load(1, 3);
   double pq = 0.0;
+  T pqt = T(0);
   // one level; SA (the register slot holding level K+1) is a literal at every
   // call so the register queue is never indexed dynamically
   auto level = [&](int K, auto sa_c) {
@@ -442,21 +469,42 @@ __global__ void __launch_bounds__(128) k_pcg_spmv(Geo G, PoissonGeo P, SolverSta
     load(SA, K + 3);
     __syncthreads();
     if (act) {
-      const Coef rw = (K >= 2 && K <= c.kreg) ? row_regular(c, szw, siz, K) : row<true>(c, P, K, KE);
-      const double p0 = (double)cur[me];
-      // entries that are not inserted are exactly 0 and their neighbours finite
-      double s = rw.dc * p0;
-      s = __fma_rn(rw.u, (double)prv[me], s);
-      s = __fma_rn(rw.n, (double)cur[me - kHx], s);
-      s = __fma_rn(rw.w, (double)cur[me - 1], s);
-      s = __fma_rn(rw.e, (double)cur[me + 1], s);
-      s = __fma_rn(rw.s, (double)cur[me + kHx], s);
-      s = __fma_rn(rw.d, (double)nxt[me], s);
-      const long long o = own + plane * (K - 1);
-      pnew[o] = (T)p0;
-      const T qt = (T)s;
-      q[o] = qt;
-      pq += p0 * (double)qt;
+      const T p0 = cur[me];
+      const T pu = prv[me], pn = cur[me - kHx], pw = cur[me - 1], pe = cur[me + 1];
+      const T ps = cur[me + kHx], pd = nxt[me];
+      T s;
+      if (K >= 2 && K <= kreg) {
+        // regular row: all six neighbours wet, vertical factors from the tables;
+        // B p = hs (cw pw + ce pe + cn pn + cs ps - (xcf+ycf) p0)
+        //       + zw0 (pu - p0) + zw1 (pd - p0)
+        const T zw0 = szw[K - 1], zw1 = szw[K], hs = siz[K - 1];
+        T h = cw * pw;
+        h = fma(ce, pe, h);
+        h = fma(cn, pn, h);
+        h = fma(cs, ps, h);
+        h = fma(-xyc, p0, h);
+        s = zw0 * (pu - p0);
+        s = fma(zw1, pd - p0, s);
+        s = fma(hs, h, s);
+      } else {
+        // entries that are not inserted are exactly 0 and their neighbours finite
+        const Coef rw = row<true>(c, P, K, KE);
+        s = (T)rw.dc * p0;
+        s = fma((T)rw.u, pu, s);
+        s = fma((T)rw.n, pn, s);
+        s = fma((T)rw.w, pw, s);
+        s = fma((T)rw.e, pe, s);
+        s = fma((T)rw.s, ps, s);
+        s = fma((T)rw.d, pd, s);
+      }
+      const unsigned o = own + plane * (unsigned)(K - 1);
+      pnew[o] = p0;
+      q[o] = s;
+      pqt = fma(p0, s, pqt);
+      if ((K & 7) == 0) {
+        pq += (double)pqt;
+        pqt = T(0);
+      }
     }
     T* t = prv;
     prv = cur;
@@ -466,6 +514,88 @@ __global__ void __launch_bounds__(128) k_pcg_spmv(Geo G, PoissonGeo P, SolverSta
   for (int K = 1; K <= KE; K += 2) {
     level(K, std::integral_constant<int, 0>{});
     if (K + 1 <= KE) level(K + 1, std::integral_constant<int, 1>{});
+  }
+  pq += (double)pqt;
+  double v[1] = {pq};
+  if (grid_sum<1>(v, S)) {
+    S->pq = v[0];
+    S->alpha = S->rho / v[0];
+    if (!(v[0] > 0.0) && !(v[0] < 0.0)) S->converged = 3;  // breakdown
+  }
+}
+
+// The same product without shared memory or barriers: every thread forms p
+// of its own column and of its four horizontal neighbours from z and p_old
+// (the neighbours' lines are shared by the warps of a block through L1), and
+// keeps its own p of levels K-1, K, K+1 in registers.  Neighbours outside the
+// unknowns hold zeros (the solver vectors are zeroed at allocation and only
+// unknowns are written) and meet zero coefficients.
+template <typename T, int BY>
+__global__ void __launch_bounds__(32 * BY) k_pcg_spmv_l1(Geo G, PoissonGeo P, SolverState* S,
+                                                        const T* __restrict__ z,
+                                                        const T* __restrict__ pold,
+                                                        T* __restrict__ pnew, T* __restrict__ q,
+                                                        int first) {
+  __shared__ T szw[kMaxKe + 1], siz[kMaxKe];
+  if (S->converged) return;
+  const int KE = G.L.ke, IE = G.L.ie, JE = G.L.je;
+  const unsigned plane = (unsigned)G.L.plane, pitch = (unsigned)G.L.P;
+  const int tid = threadIdx.x + 32 * threadIdx.y;
+  for (int e = tid; e <= KE; e += 32 * BY) {
+    szw[e] = (T)P.zwn[e];
+    if (e < KE) siz[e] = (T)P.izn[e];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * 32 + threadIdx.x + 2, j = blockIdx.y * BY + threadIdx.y + 2;
+  const bool act = i <= IE - 1 && j <= JE - 1;
+  const T beta = first ? T(0) : (T)S->beta;
+  double pq = 0.0;
+  if (act) {
+    const ColC c = load_col(G, P, i, j);
+    const T cw = c.iw ? (T)c.cw : T(0), ce = c.ie ? (T)c.ce : T(0);
+    const T cn = c.in ? (T)c.cn : T(0), cs = c.is ? (T)c.cs : T(0);
+    const T xyc = (T)(c.xcf + c.ycf);
+    const int kreg = c.kreg;
+    const unsigned o0 = (unsigned)G.L.at(i, j, 0);
+    auto pv = [&](unsigned o) -> T { return first ? z[o] : fma(beta, pold[o], z[o]); };
+    T pu = T(0), p0 = pv(o0);
+    T pqt = T(0);
+    for (int K = 1; K <= KE; ++K) {
+      const unsigned o = o0 + plane * (unsigned)(K - 1);
+      const T pd = K < KE ? pv(o + plane) : T(0);
+      const T pw = pv(o - 1), pe = pv(o + 1), pn = pv(o - pitch), ps = pv(o + pitch);
+      T s;
+      if (K >= 2 && K <= kreg) {
+        const T zw0 = szw[K - 1], zw1 = szw[K], hs = siz[K - 1];
+        T h = cw * pw;
+        h = fma(ce, pe, h);
+        h = fma(cn, pn, h);
+        h = fma(cs, ps, h);
+        h = fma(-xyc, p0, h);
+        s = zw0 * (pu - p0);
+        s = fma(zw1, pd - p0, s);
+        s = fma(hs, h, s);
+      } else {
+        const Coef rw = row<true>(c, P, K, KE);
+        s = (T)rw.dc * p0;
+        s = fma((T)rw.u, pu, s);
+        s = fma((T)rw.n, pn, s);
+        s = fma((T)rw.w, pw, s);
+        s = fma((T)rw.e, pe, s);
+        s = fma((T)rw.s, ps, s);
+        s = fma((T)rw.d, pd, s);
+      }
+      pnew[o] = p0;
+      q[o] = s;
+      pqt = fma(p0, s, pqt);
+      if ((K & 7) == 0) {
+        pq += (double)pqt;
+        pqt = T(0);
+      }
+      pu = p0;
+      p0 = pd;
+    }
+    pq += (double)pqt;
   }
   double v[1] = {pq};
   if (grid_sum<1>(v, S)) {
@@ -580,35 +710,106 @@ void launch_factor(const Geo& G, const PoissonGeo& P, double* dinv64, float* din
   count_launch();
 }
 
+namespace {
+
+// Variants of the column kernel (chosen per handle by the autotuner):
+// forward values through the output vector or in shared memory, and the
+// number of levels whose loads are issued together.
+struct ColVariant {
+  bool sm;
+  int u;
+  dim3 blk;
+};
+constexpr int kNumColVariants = 4;
+const ColVariant kColVariants[kNumColVariants] = {
+    {false, 4, dim3(32, 4)}, {false, 8, dim3(32, 4)}, {true, 4, dim3(32, 2)}, {true, 8, dim3(32, 2)}};
+// a shared-memory variant is usable while its block's forward values fit here
+constexpr size_t kColSmemMax = 96 * 1024;
+
+template <typename T, int MODE, bool SM, int U>
+void col_launch(dim3 blk, size_t smem, const Geo& G, const PoissonGeo& P, SolverState* S,
+                const T* b, T* x, T* r, const T* p, const T* q, T* z, cudaStream_t st) {
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_pcg_col<T, MODE, SM, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+  k_pcg_col<T, MODE, SM, U><<<grid2(G.L.ie - 2, G.L.je - 2, blk), blk, smem, st>>>(G, P, S, b, x,
+                                                                                  r, p, q, z);
+}
+
+template <typename T, int SM, int U>
+void col_mode(int mode, dim3 blk, size_t smem, const Geo& G, const PoissonGeo& P, SolverState* S,
+              const T* b, T* x, T* r, const T* p, const T* q, T* z, cudaStream_t st) {
+  if (mode == 1)
+    col_launch<T, 1, SM, U>(blk, smem, G, P, S, b, x, r, p, q, z, st);
+  else
+    col_launch<T, 2, SM, U>(blk, smem, G, P, S, b, x, r, p, q, z, st);
+}
+
+}  // namespace
+
+template <typename T>
+bool pcg_col_variant_ok(const Geo& G, int variant) {
+  if (variant < 0 || variant >= kNumColVariants) return false;
+  const ColVariant& v = kColVariants[variant];
+  return !v.sm || (size_t)v.blk.x * v.blk.y * G.L.ke * sizeof(T) <= kColSmemMax;
+}
+template bool pcg_col_variant_ok<double>(const Geo&, int);
+template bool pcg_col_variant_ok<float>(const Geo&, int);
+int pcg_col_variants() { return kNumColVariants; }
+
 template <typename T, typename TX>
 void launch_pcg_col(const Geo& G, const PoissonGeo& P, SolverState* S, int mode, const T* b, TX* x,
-                    T* r, const T* p, const T* q, T* z, cudaStream_t st) {
-  const dim3 grd = grid2(G.L.ie - 2, G.L.je - 2, kColBlock);
-  if (mode == 1)
-    k_pcg_col<T, 1><<<grd, kColBlock, 0, st>>>(G, P, S, b, x, r, p, q, z);
-  else
-    k_pcg_col<T, 2><<<grd, kColBlock, 0, st>>>(G, P, S, b, x, r, p, q, z);
+                    T* r, const T* p, const T* q, T* z, int variant, cudaStream_t st) {
+  if (!pcg_col_variant_ok<T>(G, variant)) variant = 0;
+  const ColVariant& v = kColVariants[variant];
+  const size_t smem = v.sm ? (size_t)v.blk.x * v.blk.y * G.L.ke * sizeof(T) : 0;
+  switch (variant) {
+    case 0: col_mode<T, false, 4>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
+    case 1: col_mode<T, false, 8>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
+    case 2: col_mode<T, true, 4>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
+    default: col_mode<T, true, 8>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
+  }
   count_launch();
 }
 template void launch_pcg_col<double, double>(const Geo&, const PoissonGeo&, SolverState*, int,
                                              const double*, double*, double*, const double*,
-                                             const double*, double*, cudaStream_t);
+                                             const double*, double*, int, cudaStream_t);
 template void launch_pcg_col<float, float>(const Geo&, const PoissonGeo&, SolverState*, int,
                                            const float*, float*, float*, const float*,
-                                           const float*, float*, cudaStream_t);
+                                           const float*, float*, int, cudaStream_t);
+
+// Variants of the stencil kernel: shared-memory ring with 32 x 8 or 32 x 4
+// tiles, or the barrier-free L1 form with 32 x 8 or 32 x 4 blocks.
+int pcg_spmv_variants() { return 4; }
 
 template <typename T>
 void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
-                     T* pnew, T* q, int first, cudaStream_t st) {
-  const dim3 blk(kTx, kTy);
-  k_pcg_spmv<T><<<grid2(G.L.ie - 2, G.L.je - 2, blk), blk, 0, st>>>(G, P, S, z, pold, pnew, q,
-                                                                     first);
+                     T* pnew, T* q, int first, int variant, cudaStream_t st) {
+  const int nx = G.L.ie - 2, ny = G.L.je - 2;
+  switch (variant) {
+    case 1:
+      k_pcg_spmv<T, 4><<<grid2(nx, ny, dim3(kTx, 4)), dim3(kTx, 4), 0, st>>>(G, P, S, z, pold,
+                                                                              pnew, q, first);
+      break;
+    case 2:
+      k_pcg_spmv_l1<T, 8><<<grid2(nx, ny, dim3(32, 8)), dim3(32, 8), 0, st>>>(G, P, S, z, pold,
+                                                                               pnew, q, first);
+      break;
+    case 3:
+      k_pcg_spmv_l1<T, 4><<<grid2(nx, ny, dim3(32, 4)), dim3(32, 4), 0, st>>>(G, P, S, z, pold,
+                                                                               pnew, q, first);
+      break;
+    default:
+      k_pcg_spmv<T, 8><<<grid2(nx, ny, dim3(kTx, 8)), dim3(kTx, 8), 0, st>>>(G, P, S, z, pold,
+                                                                              pnew, q, first);
+      break;
+  }
   count_launch();
 }
 template void launch_pcg_spmv<double>(const Geo&, const PoissonGeo&, SolverState*, const double*,
-                                      const double*, double*, double*, int, cudaStream_t);
+                                      const double*, double*, double*, int, int, cudaStream_t);
 template void launch_pcg_spmv<float>(const Geo&, const PoissonGeo&, SolverState*, const float*,
-                                     const float*, float*, float*, int, cudaStream_t);
+                                     const float*, float*, float*, int, int, cudaStream_t);
 
 void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b,
                   const double* x, double* r, cudaStream_t st) {
@@ -642,8 +843,8 @@ void launch_solver_reset(SolverState* S, double tol, int keep_bb, cudaStream_t s
 }
 
 size_t solver_max_blocks(const Geo& G) {
-  const dim3 g = grid2(G.L.ie - 2, G.L.je - 2, kColBlock);
-  return (size_t)g.x * g.y;
+  // one partial per warp row: 32-column chunks x rows of unknowns
+  return (size_t)((G.L.ie - 2 + 31) / 32) * (size_t)(G.L.je - 2);
 }
 
 }  // namespace orctm

@@ -100,8 +100,10 @@ def test_nh_correction(case, mode):
 
 
 def test_solver_residual_target(case):
-    """At the production target (1e-10) both solver forms reach the residual,
-    and the solution is within 1e-9 (relative 2-norm) of the direct solve."""
+    """At the production target (1e-10) both solver forms reach the residual;
+    the solution error is then bounded by the conditioning (checked at 1e-6
+    in the relative 2-norm; the 1e-9 solution bound is checked at the 1e-12
+    target by test_nh_correction)."""
     _, inst = case
     ref = None
     for mode in ("fp64", "fp32_refined"):
@@ -129,3 +131,30 @@ def test_step_hotpath(case):
         assert_close(got[k], st[k], 1e-8, f"step {k}")
     for n, t in enumerate(st["tracers"]):
         assert_close(got["tracers"][n], t, 1e-10, f"step tracer {n}")
+
+
+@pytest.mark.parametrize("mode", ["fp64", "fp32_refined"])
+@pytest.mark.parametrize("case_name", ["c2s", "c1s"])
+def test_solver_variants_bit_identical(case_name, mode):
+    """Every column-kernel and stencil-kernel variant the autotuner chooses
+    between gives the same pressure bit for bit, with the same iteration
+    count, as the autotuned solve."""
+    inst = instance(case_name)
+    combos = [(-1, -1)] + [(c, 0) for c in range(4)] + [(0, s) for s in range(1, 4)]
+    ref = None
+    for c, s in combos:
+        gpu = Instance(inst)
+        gpu.upload_state(C.copy_state(inst))
+        gpu.set_solver(mode, rtol=1e-12, maxit=20000)
+        gpu.set_tuning(c, s)
+        stats = gpu.ocvtot_nh()
+        used = gpu.tuning(mode)
+        assert all(v >= 0 for v in used), used
+        if c >= 0:
+            assert used == (c, s) or (c >= 2 and used[0] == 0), (used, c, s)
+        got = (gpu.download("pnh"), stats["iterations"], stats["outer_iterations"])
+        if ref is None:
+            ref = got
+        else:
+            assert np.array_equal(got[0], ref[0]), (c, s)
+            assert got[1:] == ref[1:], (c, s, got[1:], ref[1:])
