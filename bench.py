@@ -276,6 +276,9 @@ def main():
              "outer_iterations": statistics.mean(s["outer_iterations"] for s in stats_m),
              "relres_max": max(s["relres"] for s in stats_m)}
     mixed["speedup_vs_fp64"] = mixed["value"] / value
+    mixed["solver_speedup_vs_fp64"] = poisson_ms / mixed["poisson_ms"]
+    tuning = {"fp64": list(gpu.tuning("fp64")), "fp32_refined": list(gpu.tuning("fp32_refined")),
+              "meaning": "(column-kernel variant, stencil-kernel variant) picked by the autotuner"}
     gpu.set_solver("fp64", rtol=1e-10, maxit=5000)
 
     # ---- roofline of the dominant kernel --------------------------------
@@ -327,7 +330,7 @@ def main():
                        "solver": "FP64 PCG (line preconditioner, scaled operator) in "
                                  "double-double-residual refinement"},
             "poisson_ms": poisson_ms, "poisson_iterations": iters, "relres_max": relres,
-            "mixed": mixed, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "mixed": mixed, "solver_tuning": tuning, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": ck,
         }
         print(json.dumps(line), flush=True)

@@ -188,6 +188,90 @@ int orctm_get_tuning(const orctm_handle* h, int precision, int* col_variant, int
 int orctm_device_bytes(const orctm_handle* h, unsigned long long* bytes);
 int orctm_trim_device_memory(int device);
 
+/* ---- Batched and served execution of independent instances ----------------
+ * A server runs independent regional instances on one device (the serving
+ * loop of an ensemble; the reference runs one domain per MPI job, so these
+ * entry points have no counterpart in it).  A request carries a descriptor,
+ * the fields to upload, a number of hot-path steps and the fields to
+ * download afterwards.  The server admits requests in submission order when a
+ * slot is free and the request's estimated device memory fits the budget
+ * (memory_fraction of the device memory free when the server was created; a
+ * request is always admitted when nothing else is in flight).  Each slot is a
+ * host thread with its own handle and stream, so the device work of the
+ * requests in flight overlaps; every instance's state stays on the device
+ * from upload to download.  A request's results do not depend on what else
+ * is in flight (each instance's kernels and reductions are deterministic).
+ * Host buffers named by a request must stay valid until orctm_serve_wait or
+ * orctm_serve_poll reports it done; input sizes are those of
+ * orctm_field_size.  The server is internally synchronised: any thread may
+ * submit, poll or wait. */
+typedef struct orctm_server orctm_server;
+
+typedef struct orctm_serve_opts {
+  int device;             /* CUDA device ordinal */
+  int slots;              /* requests in flight at once, >= 1 */
+  double memory_fraction; /* share of the free device memory admitted requests may use, (0, 1] */
+  int solver;             /* ORCTM_SOLVER_FP64 or ORCTM_SOLVER_FP32_REFINED */
+  double rtol;            /* Poisson relative-residual target */
+  int maxit;              /* Krylov iteration limit per solve */
+} orctm_serve_opts;
+
+typedef struct orctm_request {
+  const orctm_desc* desc;      /* geometry and parameters (desc->device is ignored) */
+  int nsteps;                  /* orctm_step_hotpath calls, >= 0 */
+  int nin;                     /* fields uploaded before the first step */
+  const int* in_fields;
+  const double* const* in_data;
+  int nout;                    /* fields downloaded after the last step */
+  const int* out_fields;
+  double* const* out_data;
+} orctm_request;
+
+typedef struct orctm_request_stats {
+  int status;                  /* ORCTM_OK or the first error of the request */
+  int steps_done;
+  int iterations;              /* Krylov iterations summed over the steps */
+  double relres_max;           /* largest final relative residual of its solves */
+  double queued_ms;            /* submission to admission */
+  double run_ms;               /* admission to results written */
+  double step_ms_p50, step_ms_p99, step_ms_max; /* per-step latency (host clock, step + sync) */
+  unsigned long long device_bytes;             /* device memory the instance held */
+  unsigned long long estimated_bytes;          /* what admission reserved for it */
+} orctm_request_stats;
+
+typedef struct orctm_serve_stats {
+  long long submitted, completed, failed;
+  long long steps;             /* steps completed over all requests */
+  double cell_steps;           /* interior cells x steps, summed over completed steps */
+  double elapsed_ms;           /* first submission to last completion */
+  double step_ms_p50, step_ms_p99; /* per-step latency over all steps */
+  int peak_in_flight;
+  unsigned long long peak_reserved_bytes;
+  unsigned long long budget_bytes;
+} orctm_serve_stats;
+
+int orctm_serve_create(const orctm_serve_opts* opts, orctm_server** out);
+int orctm_serve_submit(orctm_server* s, const orctm_request* req, unsigned long long* id);
+/* blocks until request id is done; its record is released */
+int orctm_serve_wait(orctm_server* s, unsigned long long id, orctm_request_stats* stats);
+/* *done = 1 (and stats filled, record released) when request id is done */
+int orctm_serve_poll(orctm_server* s, unsigned long long id, int* done, orctm_request_stats* stats);
+/* blocks until every submitted request is done */
+int orctm_serve_drain(orctm_server* s);
+int orctm_serve_get_stats(orctm_server* s, orctm_serve_stats* stats);
+/* drains, then stops the slots */
+int orctm_serve_destroy(orctm_server* s);
+
+/* Runs n requests submitted together (an ensemble batch) and waits for all;
+ * per_request may be NULL.  With opts->slots == 1 the requests run one at a
+ * time. */
+int orctm_batch_run(const orctm_serve_opts* opts, int n, const orctm_request* reqs,
+                    orctm_request_stats* per_request, orctm_serve_stats* total);
+
+/* Upper bound of the device bytes one instance needs (fields, geometry
+ * tables and the solver vectors of the given solver mode). */
+int orctm_estimate_device_bytes(const orctm_desc* desc, int solver, unsigned long long* bytes);
+
 /* BELEG + BODEN restated on the host.  depto (IE*JE) is adjusted in place as
  * BODEN does (ISTART == 0).  Output arrays are caller-allocated in the host
  * layouts above; tiestu, tiestw, dz and di hold KE+1 values. */

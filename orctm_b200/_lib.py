@@ -52,6 +52,9 @@ EXPORTS = (
     "orctm_synchronize", "orctm_build_grid", "orctm_timer_start", "orctm_timer_stop",
     "orctm_set_profiling", "orctm_profile_get", "orctm_kernel_launches", "orctm_device_bytes",
     "orctm_trim_device_memory", "orctm_set_tuning", "orctm_get_tuning",
+    "orctm_serve_create", "orctm_serve_submit", "orctm_serve_wait", "orctm_serve_poll",
+    "orctm_serve_drain", "orctm_serve_get_stats", "orctm_serve_destroy", "orctm_batch_run",
+    "orctm_estimate_device_bytes",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",

@@ -30,6 +30,39 @@ def _p(a):
     return a.ctypes.data_as(_D)
 
 
+GEOMETRY_KEYS = ("dzw", "di", "dlxp", "dlyp", "dtdxpo", "dtdyo", "dlxu", "dlyu", "dtdxuo", "dlxv",
+                 "dlyv", "dpye", "ddpo", "weto", "dduo", "amsuo", "ddue", "amsue")
+
+
+def make_desc(inst: dict, device: int = 0):
+    """The orctm_desc of an instance dict, and the arrays its pointers refer
+    to (keep them alive while the descriptor is in use)."""
+    d = _lib.Desc()
+    d.ie, d.je, d.ke = inst["ie"], inst["je"], inst["ke"]
+    d.i_start = d.j_start = 0
+    d.ntracers = int(inst.get("ntracers", len(inst.get("tracers", [])) or 2))
+    ob = inst["ob"]
+    d.ob_west, d.ob_east, d.ob_north, d.ob_south = (int(ob[k]) for k in
+                                                    ("west", "east", "north", "south"))
+    d.dt, d.almzer, d.aulapts, d.aulapuv, d.ah00 = (inst["dt"], inst["almzer"], inst["aulapts"],
+                                                    inst["aulapuv"], inst["ah00"])
+    keep = []
+    for k in GEOMETRY_KEYS:
+        a = np.asfortranarray(inst[k], dtype=np.float64)
+        keep.append(a)
+        setattr(d, k, _p(a))
+    d.device = device
+    return d, keep
+
+
+def field_id(name) -> int:
+    if isinstance(name, int):
+        return name
+    if name.startswith("tracer"):
+        return F_THO + int(name[6:])
+    return FIELDS[name]
+
+
 class Instance:
     """One regional domain resident on a GPU (an orctm_handle)."""
 
@@ -37,27 +70,12 @@ class Instance:
         self.lib = _lib.load()
         self.ie, self.je, self.ke = inst["ie"], inst["je"], inst["ke"]
         self.ntr = int(inst.get("ntracers", len(inst.get("tracers", [])) or 2))
-        self._keep = []
-        d = _lib.Desc()
-        d.ie, d.je, d.ke = self.ie, self.je, self.ke
-        d.i_start = d.j_start = 0
-        d.ntracers = self.ntr
-        ob = inst["ob"]
-        d.ob_west, d.ob_east, d.ob_north, d.ob_south = (int(ob[k]) for k in
-                                                        ("west", "east", "north", "south"))
-        d.dt, d.almzer, d.aulapts, d.aulapuv, d.ah00 = (inst["dt"], inst["almzer"], inst["aulapts"],
-                                                        inst["aulapuv"], inst["ah00"])
-        for k in ("dzw", "di", "dlxp", "dlyp", "dtdxpo", "dtdyo", "dlxu", "dlyu", "dtdxuo", "dlxv",
-                  "dlyv", "dpye", "ddpo", "weto", "dduo", "amsuo", "ddue", "amsue"):
-            a = np.asfortranarray(inst[k], dtype=np.float64)
-            self._keep.append(a)
-            setattr(d, k, _p(a))
-        d.device = device
+        d, keep = make_desc(inst, device)
         h = C.c_void_p()
         st = self.lib.orctm_create(C.byref(d), C.byref(h))
+        del keep
         _lib.check(st, None)
         self.h = h
-        self._keep = []
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
@@ -84,11 +102,7 @@ class Instance:
                 "w": (ie, je, ke + 1), "2": (ie, je)}[SHAPES.get(name, "p")]
 
     def _fid(self, name):
-        if isinstance(name, int):
-            return name
-        if name.startswith("tracer"):
-            return F_THO + int(name[6:])
-        return FIELDS[name]
+        return field_id(name)
 
     def upload(self, name, arr: np.ndarray):
         a = np.asfortranarray(arr, dtype=np.float64)

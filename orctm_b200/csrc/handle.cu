@@ -1171,6 +1171,21 @@ int orctm_device_bytes(const orctm_handle* h, unsigned long long* bytes) {
   return ORCTM_OK;
 }
 
+int orctm_estimate_device_bytes(const orctm_desc* d, int solver, unsigned long long* bytes) {
+  if (!d || !bytes || d->ie < 4 || d->je < 3 || d->ke < 2 || d->ntracers < 2) return ORCTM_E_ARG;
+  const double P = (double)(((long long)d->ie + 1 + 31) / 32 * 32);
+  const double plane = P * (d->je + 1), n3 = plane * (d->ke + 1);
+  // 3D buffers: 12 state fields and the tracers, up to 8 routine temporaries
+  // of the field pool, 9 FP64 solver vectors, the FP64 + FP32 pivots, and 7
+  // FP32 vectors for the refined solver
+  const double f3 = 12.0 + d->ntracers + 8.0 + 9.0 + 1.5 +
+                    (solver == ORCTM_SOLVER_FP32_REFINED ? 3.5 : 0.0);
+  // 2D tables (compressed columns, metrics, biharmonic and Poisson factors)
+  const double f2 = 64.0;
+  *bytes = (unsigned long long)((f3 * n3 + f2 * plane) * 8.0) + (1ULL << 20);
+  return ORCTM_OK;
+}
+
 int orctm_trim_device_memory(int device) {
   cudaMemPool_t mp = nullptr;
   int st = device_pool(device, &mp);
