@@ -224,6 +224,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3")
+    ap.add_argument("--workload", default="step", choices=["step", "c4", "c5"],
+                    help="step: one instance per GPU (the headline); c4: ensemble batch vs one at "
+                         "a time; c5: served requests with Poisson arrivals")
+    ap.add_argument("--members", type=int, default=64, help="c4/c5: requests")
+    ap.add_argument("--distinct", type=int, default=16,
+                    help="c4/c5: distinct seeded instances the requests cycle through")
+    ap.add_argument("--member-steps", type=int, default=20, help="c4/c5: steps per request")
+    ap.add_argument("--slots", type=int, default=16, help="c4/c5: requests in flight")
+    ap.add_argument("--rate", type=float, default=20.0, help="c5: Poisson arrival rate (1/s)")
     ap.add_argument("--size", default=None, help="override nx x ny x nz (e.g. 256x256x60)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -235,6 +244,8 @@ def main():
     ws, rank, local, pg = dist_setup()
     if args.impl == "reference":
         return run_reference(args, ws, rank, pg)
+    if args.workload != "step":
+        return run_ensemble(args, ws, rank, local, pg)
 
     from orctm_b200 import configs
     from orctm_b200.api import Instance
@@ -393,6 +404,145 @@ def run_e2e(gpu, inst, cells, args, ws, pg):
     return {"value": ws * cells * k_steps / (ms / 1e3), "unit": "cell-steps/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "steps": k_steps, "ms_per_step": ms / k_steps}
+
+
+# ---------------------------------------------------------------- ensembles --
+ENSEMBLE_OUT = ("pnh", "tracers")
+
+
+def _gen_member(arg):
+    """One seeded instance of config c4/c5 with the arrays a request needs
+    (geometry of the descriptor, the state; shared where the state repeats a
+    field).  Runs in a spawned worker process."""
+    name, index = arg
+    from orctm_b200 import configs
+
+    inst = configs.make_instance(name, index=index)
+    from orctm_b200.api import GEOMETRY_KEYS
+
+    keep = ("ie", "je", "ke", "nx", "ny", "nz", "ntracers", "ob", "dt", "almzer", "aulapts",
+            "aulapuv", "ah00") + GEOMETRY_KEYS
+    slim = {k: inst[k] for k in keep}
+    st = configs.copy_state(inst)
+    del inst
+    st["uko"], st["vke"], st["wo"] = st["uoo"], st["voe"], st["wno"]  # equal at the start
+    return slim, st
+
+
+def _members(args):
+    import multiprocessing as mp
+
+    name = "c4" if args.workload == "c4" else "c5"
+    idx = [(name, k) for k in range(min(args.distinct, args.members))]
+    t = time.time()
+    with mp.get_context("spawn").Pool(min(len(idx), os.cpu_count() or 1)) as pool:
+        pool_insts = pool.map(_gen_member, idx)
+    log(f"[bench] {len(pool_insts)} distinct {name} instances generated in {time.time() - t:.1f}s")
+    return [pool_insts[k % len(pool_insts)] for k in range(args.members)]
+
+
+def _one_at_a_time(members, nsteps, solver):
+    """The plain path: each instance created, uploaded, stepped, read back and
+    destroyed before the next starts."""
+    from orctm_b200.api import Instance
+
+    lat = []
+    cells = 0
+    t = time.perf_counter()
+    for inst, st in members:
+        g = Instance(inst)
+        g.upload_state(st)
+        g.set_solver(solver, rtol=1e-10, maxit=5000)
+        for _ in range(nsteps):
+            t0 = time.perf_counter()
+            g.step_hotpath()
+            g.synchronize()
+            lat.append((time.perf_counter() - t0) * 1e3)
+        g.download("pnh")
+        for n in range(g.ntr):
+            g.download(f"tracer{n}")
+        g.close()
+        cells += (inst["ie"] - 2) * (inst["je"] - 2) * inst["ke"] * nsteps
+    el = time.perf_counter() - t
+    lat.sort()
+    return {"value": cells / el, "elapsed_s": el, "step_ms_p50": lat[len(lat) // 2],
+            "step_ms_p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
+
+
+def run_ensemble(args, ws, rank, local, pg):
+    """c4: the ensemble batch (all requests submitted together) against the
+    same requests one at a time on the plain path; c5: requests arriving as a
+    seeded Poisson process into the served loop.  Replicas per GPU."""
+    members = _members(args)
+    from orctm_b200 import serve
+
+    nsteps = args.member_steps
+    total_cells = sum((i["ie"] - 2) * (i["je"] - 2) * i["ke"] for i, _ in members) * nsteps
+    res = {}
+    for solver in ("fp64", "fp32_refined"):
+        if args.workload == "c4":
+            base = _one_at_a_time(members, nsteps, solver)
+            jobs = [serve.Job(i, st, nsteps, outputs=ENSEMBLE_OUT) for i, st in members]
+            barrier(pg)
+            t = time.perf_counter()
+            tot = serve.run_batch(jobs, device=local, slots=args.slots, solver=solver)
+            el = time.perf_counter() - t
+            el = max_over_ranks(pg, el)
+            res[solver] = {"batched": {"value": ws * tot["cell_steps"] / el, "elapsed_s": el,
+                                       "step_ms_p50": tot["step_ms_p50"],
+                                       "step_ms_p99": tot["step_ms_p99"],
+                                       "peak_in_flight": tot["peak_in_flight"],
+                                       "failed": tot["failed"]},
+                           "one_at_a_time": {**base, "value": ws * base["value"]},
+                           "speedup": (tot["cell_steps"] / el) / base["value"]}
+        else:
+            g = np.random.Generator(np.random.PCG64(20261203 + 5))
+            gaps = g.exponential(1.0 / args.rate, size=len(members))
+            jobs = []
+            barrier(pg)
+            with serve.Server(device=local, slots=args.slots, solver=solver) as srv:
+                t = time.perf_counter()
+                due = 0.0
+                for (inst, st), gap in zip(members, gaps):
+                    due += gap
+                    now = time.perf_counter() - t
+                    if due > now:
+                        time.sleep(due - now)
+                    jobs.append(srv.submit(serve.Job(inst, st, nsteps, outputs=ENSEMBLE_OUT)))
+                for j in jobs:
+                    srv.wait(j)
+                el = time.perf_counter() - t
+                tot = srv.stats()
+            q = sorted(j.stats["queued_ms"] for j in jobs)
+            rl = sorted(j.stats["queued_ms"] + j.stats["run_ms"] for j in jobs)
+            el = max_over_ranks(pg, el)
+            res[solver] = {"value": ws * tot["cell_steps"] / el, "elapsed_s": el,
+                           "step_ms_p50": tot["step_ms_p50"], "step_ms_p99": tot["step_ms_p99"],
+                           "request_ms_p50": rl[len(rl) // 2],
+                           "request_ms_p99": rl[min(len(rl) - 1, int(0.99 * len(rl)))],
+                           "queued_ms_p50": q[len(q) // 2],
+                           "queued_ms_p99": q[min(len(q) - 1, int(0.99 * len(q)))],
+                           "peak_in_flight": tot["peak_in_flight"], "failed": tot["failed"]}
+    if rank == 0:
+        sizes = [(i["nx"], i["ny"], i["nz"]) for i, _ in members[:args.distinct]]
+        head = res["fp64"]["batched"] if args.workload == "c4" else res["fp64"]
+        line = {"metric": f"cell-steps/s ({args.workload} "
+                          f"{'ensemble batch' if args.workload == 'c4' else 'served requests'})",
+                "value": head["value"], "unit": "cell-steps/s", "n_gpus": ws,
+                "steps": nsteps, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded PCG64, base seed 20261203; generators of BASELINE configs)",
+                "config": {"workload": f"{args.workload}: {args.members} requests over "
+                                       f"{len(sizes)} distinct seeded instances, "
+                                       f"{nsteps} steps each, {args.slots} slots"
+                                       + (f", Poisson arrivals {args.rate}/s"
+                                          if args.workload == "c5" else ""),
+                           "distinct_sizes": sizes, "cell_steps_per_gpu": total_cells},
+                "results": res}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
 
 
 if __name__ == "__main__":

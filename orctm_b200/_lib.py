@@ -13,7 +13,14 @@ SO = os.path.join(_HERE, "liborctm_gpu.so")
 _D = C.POINTER(C.c_double)
 
 ORCTM_OK = 0
+ORCTM_E_ARG = -1
+ORCTM_E_CUDA = -2
+ORCTM_E_NOMEM = -3
 ORCTM_E_NOT_CONVERGED = -4
+ORCTM_E_GEOMETRY = -5
+ORCTM_E_UNSUPPORTED = -6
+ORCTM_E_NODEVICE = -7
+ORCTM_E_TOO_LARGE = -8
 
 F_UOO, F_VOE, F_WNO, F_UKO, F_VKE, F_WO, F_UOO_1, F_VOE_1, F_WNO_1, F_PNH, F_ZO, F_DVO, F_AVO, \
     F_THO, F_SAO = range(15)

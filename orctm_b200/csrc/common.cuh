@@ -58,6 +58,17 @@ struct Geo {
   const double *aulux, *auluy, *aulvx, *aulvy, *aulwx, *aulwy;  // (p plane)
   const double *dlypsi;                               // u-points, i in [0,IE]
   const double *dlxpsi;                               // v-points, j in [0,JE]
+  // reciprocals of the metrics (0 where a metric is undefined), so the
+  // Laplacian and biharmonic stencils multiply instead of dividing
+  const double *rdlxp, *rdlyp, *rdlxu, *rdlyu, *rdlxv, *rdlyv, *rdlxpsi, *rdlypsi;
+  // per-face biharmonic coefficients, each shared by the two cells of a face:
+  //   tfx = AULX DLYU / DLXU, tfy = AULY DLXV / DLYV           (tracers)
+  //   ugx = AULUX DLYP / DLXP, ugy = AULUY DLXPSI / DLYPSI      (u)
+  //   vgx = AULVX DLYPSI / DLXPSI, vgy = AULVY DLXP / DLYP      (v)
+  //   wgx = AULWX DLYU / DLXU, wgy = AULWY DLXV / DLYV          (w, times DZ)
+  // and reciprocal cell areas 1/(DLXU DLYU), 1/(DLXV DLYV), 1/(DLXP DLYP)
+  const double *tfx, *tfy, *ugx, *ugy, *vgx, *vgy, *wgx, *wgy;
+  const double *rareau, *rareav, *rareap;
 };
 
 __device__ __forceinline__ double thick(const ColGeo& c, const double* dzw, long long ij, int K) {

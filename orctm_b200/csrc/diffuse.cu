@@ -106,12 +106,12 @@ __global__ void k_tdiff_lap(Geo G, const double* __restrict__ T, double* __restr
     const double c = AT(T, i, j, K);
     auto w = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
     r = w(i, j) *
-        ((w(i - 1, j) * (AT(T, i - 1, j, K) - c) / G.dlxu[G.L.at2(i - 1, j)] +
-          w(i + 1, j) * (AT(T, i + 1, j, K) - c) / G.dlxu[G.L.at2(i, j)]) /
-             G.dlxp[G.L.at2(i, j)] +
-         (w(i, j - 1) * (AT(T, i, j - 1, K) - c) / G.dlyv[G.L.at2(i, j - 1)] +
-          w(i, j + 1) * (AT(T, i, j + 1, K) - c) / G.dlyv[G.L.at2(i, j)]) /
-             G.dlyp[G.L.at2(i, j)]);
+        ((w(i - 1, j) * (AT(T, i - 1, j, K) - c) * G.rdlxu[G.L.at2(i - 1, j)] +
+          w(i + 1, j) * (AT(T, i + 1, j, K) - c) * G.rdlxu[G.L.at2(i, j)]) *
+             G.rdlxp[G.L.at2(i, j)] +
+         (w(i, j - 1) * (AT(T, i, j - 1, K) - c) * G.rdlyv[G.L.at2(i, j - 1)] +
+          w(i, j + 1) * (AT(T, i, j + 1, K) - c) * G.rdlyv[G.L.at2(i, j)]) *
+             G.rdlyp[G.L.at2(i, j)]);
   }
   AT(L1, i, j, K) = r;
 }
@@ -128,20 +128,18 @@ __global__ void k_tdiff_bih(Geo G, const double* __restrict__ T, const double* _
   double r = t;
   if (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
     auto w = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
-    auto aulx = [&](int ii, int jj) { return G.aulx[G.L.at2(ii, jj)]; };
-    auto auly = [&](int ii, int jj) { return G.auly[G.L.at2(ii, jj)]; };
     const long long ij = G.L.at2(i, j);
     const double zzsurf = K == 1 ? 1. : 0.;
     const double c = AT(L1, i, j, K);
-    const double den = (thick(G.gp, G.dzw, ij, K) + G.almzer + zzsurf * (zo[ij])) * G.dlxp[ij] *
-                       G.dlyp[ij];
-    r = t - (w(i, j) / den) * G.dzw[K - 1] *
-                (w(i - 1, j) * aulx(i - 1, j) * G.dlyu[G.L.at2(i - 1, j)] *
-                     (AT(L1, i - 1, j, K) - c) / G.dlxu[G.L.at2(i - 1, j)] +
-                 w(i + 1, j) * aulx(i, j) * G.dlyu[ij] * (AT(L1, i + 1, j, K) - c) / G.dlxu[ij] +
-                 w(i, j - 1) * auly(i, j - 1) * G.dlxv[G.L.at2(i, j - 1)] *
-                     (AT(L1, i, j - 1, K) - c) / G.dlyv[G.L.at2(i, j - 1)] +
-                 w(i, j + 1) * auly(i, j) * G.dlxv[ij] * (AT(L1, i, j + 1, K) - c) / G.dlyv[ij]);
+    // W / ((DDPO + ALMZER + ZZSURF ZO) DLXP DLYP) with 1/(DLXP DLYP) precomputed;
+    // face terms AULX DLYU / DLXU and AULY DLXV / DLYV precomputed per face
+    const double fac = (w(i, j) * G.rareap[ij]) /
+                       (thick(G.gp, G.dzw, ij, K) + G.almzer + zzsurf * (zo[ij]));
+    r = t - fac * G.dzw[K - 1] *
+                (w(i - 1, j) * G.tfx[G.L.at2(i - 1, j)] * (AT(L1, i - 1, j, K) - c) +
+                 w(i + 1, j) * G.tfx[ij] * (AT(L1, i + 1, j, K) - c) +
+                 w(i, j - 1) * G.tfy[G.L.at2(i, j - 1)] * (AT(L1, i, j - 1, K) - c) +
+                 w(i, j + 1) * G.tfy[ij] * (AT(L1, i, j + 1, K) - c));
   }
   AT(O, i, j, K) = r;
 }
@@ -306,12 +304,8 @@ __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __re
   }
 }
 
-__device__ __forceinline__ double dlypsi(const Geo& G, int i, int j) {  // u-points, i in [0,IE]
-  return G.dlypsi[G.L.at2(i, j)];
-}
-__device__ __forceinline__ double dlxpsi(const Geo& G, int i, int j) {  // v-points, j in [0,JE]
-  return G.dlxpsi[G.L.at2(i, j)];
-}
+__device__ __forceinline__ double rdlypsi(const Geo& G, int i, int j) { return G.rdlypsi[G.L.at2(i, j)]; }
+__device__ __forceinline__ double rdlxpsi(const Geo& G, int i, int j) { return G.rdlxpsi[G.L.at2(i, j)]; }
 
 // first Laplacians UK1O (u), VK1E (v), WN1O (w), ocvisc.f90:350-438, 617-669
 __global__ void k_visc_lap(Geo G, const double* __restrict__ uk, const double* __restrict__ vk,
@@ -329,31 +323,31 @@ __global__ void k_visc_lap(Geo G, const double* __restrict__ uk, const double* _
     const bool jin = j >= 2 && j <= JE - 1, iin = i >= 1 && i <= IE - 1;
     double r = 0.0;
     auto ypart = [&]() {
-      return (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / dlypsi(G, i, j - 1) -
-              AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / dlypsi(G, i, j)) /
-             G.dlyu[G.L.at2(i, j)];
+      return (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) * rdlypsi(G, i, j - 1) -
+              AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) * rdlypsi(G, i, j)) *
+             G.rdlyu[G.L.at2(i, j)];
     };
     auto xpart = [&]() {
-      return (AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / G.dlxp[G.L.at2(i + 1, j)] -
-              AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / G.dlxp[G.L.at2(i, j)]) /
-             G.dlxu[G.L.at2(i, j)];
+      return (AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) * G.rdlxp[G.L.at2(i + 1, j)] -
+              AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) * G.rdlxp[G.L.at2(i, j)]) *
+             G.rdlxu[G.L.at2(i, j)];
     };
     if (jin && iin) {
       r = AO(i, j) * (xpart() + ypart());
     } else if (jin && i == 0) {
-      r = AO(i, j) * ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) / G.dlxp[G.L.at2(i + 1, j)]) /
-                          G.dlxu[G.L.at2(i, j)] +
+      r = AO(i, j) * ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) * G.rdlxp[G.L.at2(i + 1, j)]) *
+                          G.rdlxu[G.L.at2(i, j)] +
                       ypart());
     } else if (jin && i == IE) {
-      r = AO(i, j) * ((-AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) / G.dlxp[G.L.at2(i, j)]) /
-                          G.dlxu[G.L.at2(i, j)] +
+      r = AO(i, j) * ((-AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) * G.rdlxp[G.L.at2(i, j)]) *
+                          G.rdlxu[G.L.at2(i, j)] +
                       ypart());
     } else if (iin && j == 1) {
-      r = AO(i, j) * (xpart() + (-AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) / dlypsi(G, i, j)) /
-                                    G.dlyu[G.L.at2(i, j)]);
+      r = AO(i, j) * (xpart() + (-AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) * rdlypsi(G, i, j)) *
+                                    G.rdlyu[G.L.at2(i, j)]);
     } else if (iin && j == JE) {
-      r = AO(i, j) * (xpart() + (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) / dlypsi(G, i, j - 1)) /
-                                    G.dlyu[G.L.at2(i, j)]);
+      r = AO(i, j) * (xpart() + (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) * rdlypsi(G, i, j - 1)) *
+                                    G.rdlyu[G.L.at2(i, j)]);
     }
     AT(u1, i, j, K) = r;
   }
@@ -364,31 +358,31 @@ __global__ void k_visc_lap(Geo G, const double* __restrict__ uk, const double* _
     const bool jin = j >= 1 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
     double r = 0.0;
     auto xpart = [&]() {
-      return (AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / dlxpsi(G, i, j) -
-              AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / dlxpsi(G, i - 1, j)) /
-             G.dlxv[G.L.at2(i, j)];
+      return (AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) * rdlxpsi(G, i, j) -
+              AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) * rdlxpsi(G, i - 1, j)) *
+             G.rdlxv[G.L.at2(i, j)];
     };
     auto ypart = [&]() {
-      return (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / G.dlyp[G.L.at2(i, j)] -
-              AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / G.dlyp[G.L.at2(i, j + 1)]) /
-             G.dlyv[G.L.at2(i, j)];
+      return (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) * G.rdlyp[G.L.at2(i, j)] -
+              AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) * G.rdlyp[G.L.at2(i, j + 1)]) *
+             G.rdlyv[G.L.at2(i, j)];
     };
     if (jin && iin) {
       r = AE(i, j) * (xpart() + ypart());
     } else if (jin && i == 1) {
-      r = AE(i, j) * ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) / dlxpsi(G, i, j)) /
-                          G.dlxv[G.L.at2(i, j)] +
+      r = AE(i, j) * ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) * rdlxpsi(G, i, j)) *
+                          G.rdlxv[G.L.at2(i, j)] +
                       ypart());
     } else if (jin && i == IE) {
-      r = AE(i, j) * ((-AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) / dlxpsi(G, i - 1, j)) /
-                          G.dlxv[G.L.at2(i, j)] +
+      r = AE(i, j) * ((-AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) * rdlxpsi(G, i - 1, j)) *
+                          G.rdlxv[G.L.at2(i, j)] +
                       ypart());
     } else if (iin && j == 0) {
-      r = AE(i, j) * (xpart() + (-AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) / G.dlyp[G.L.at2(i, j + 1)]) /
-                                    G.dlyv[G.L.at2(i, j)]);
+      r = AE(i, j) * (xpart() + (-AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) * G.rdlyp[G.L.at2(i, j + 1)]) *
+                                    G.rdlyv[G.L.at2(i, j)]);
     } else if (iin && j == JE) {
-      r = AE(i, j) * (xpart() + (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) / G.dlyp[G.L.at2(i, j)]) /
-                                    G.dlyv[G.L.at2(i, j)]);
+      r = AE(i, j) * (xpart() + (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) * G.rdlyp[G.L.at2(i, j)]) *
+                                    G.rdlyv[G.L.at2(i, j)]);
     }
     AT(v1, i, j, K) = r;
   }
@@ -399,31 +393,31 @@ __global__ void k_visc_lap(Geo G, const double* __restrict__ uk, const double* _
     const bool jin = j >= 2 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
     double r = 0.0;
     auto xpart = [&]() {
-      return (WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / G.dlxu[G.L.at2(i, j)] -
-              WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / G.dlxu[G.L.at2(i - 1, j)]) /
-             G.dlxp[G.L.at2(i, j)];
+      return (WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) * G.rdlxu[G.L.at2(i, j)] -
+              WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) * G.rdlxu[G.L.at2(i - 1, j)]) *
+             G.rdlxp[G.L.at2(i, j)];
     };
     auto ypart = [&]() {
-      return (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / G.dlyv[G.L.at2(i, j - 1)] -
-              WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / G.dlyv[G.L.at2(i, j)]) /
-             G.dlyp[G.L.at2(i, j)];
+      return (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) * G.rdlyv[G.L.at2(i, j - 1)] -
+              WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) * G.rdlyv[G.L.at2(i, j)]) *
+             G.rdlyp[G.L.at2(i, j)];
     };
     if (jin && iin) {
       r = WE(i, j) * (xpart() + ypart());
     } else if (jin && i == 1) {
-      r = WE(i, j) * ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) / G.dlxu[G.L.at2(i, j)]) /
-                          G.dlxp[G.L.at2(i, j)] +
+      r = WE(i, j) * ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) * G.rdlxu[G.L.at2(i, j)]) *
+                          G.rdlxp[G.L.at2(i, j)] +
                       ypart());
     } else if (jin && i == IE) {
-      r = WE(i, j) * ((-WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) / G.dlxu[G.L.at2(i - 1, j)]) /
-                          G.dlxp[G.L.at2(i, j)] +
+      r = WE(i, j) * ((-WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) * G.rdlxu[G.L.at2(i - 1, j)]) *
+                          G.rdlxp[G.L.at2(i, j)] +
                       ypart());
     } else if (iin && j == 1) {
-      r = WE(i, j) * (xpart() + (-WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) / G.dlyv[G.L.at2(i, j)]) /
-                                    G.dlyp[G.L.at2(i, j)]);
+      r = WE(i, j) * (xpart() + (-WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) * G.rdlyv[G.L.at2(i, j)]) *
+                                    G.rdlyp[G.L.at2(i, j)]);
     } else if (iin && j == JE) {
-      r = WE(i, j) * (xpart() + (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) / G.dlyv[G.L.at2(i, j - 1)]) /
-                                    G.dlyp[G.L.at2(i, j)]);
+      r = WE(i, j) * (xpart() + (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) * G.rdlyv[G.L.at2(i, j - 1)]) *
+                                    G.rdlyp[G.L.at2(i, j)]);
     }
     AT(w1, i, j, K) = r;
   }
@@ -442,6 +436,9 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
   const double mv = G.minvalue;
+  // The face terms AUL.. * width / length of ocvisc.f90:445-477, 673-688 are
+  // precomputed per face (G.ugx .. G.wgy) and the cell areas' reciprocals per
+  // cell, so a cell needs no division except by its thickness (w).
   if (K <= KE) {
     // ---- u
     if (j >= 1) {
@@ -449,18 +446,13 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
         auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
         auto U1 = [&](int ii, int jj) { return AT(u1, ii, jj, K); };
-        auto aulux = [&](int ii, int jj) { return G.aulux[G.L.at2(ii, jj)]; };
-        auto auluy = [&](int ii, int jj) { return G.auluy[G.L.at2(ii, jj)]; };
         const long long ij = G.L.at2(i, j);
-        r = (AO(i, j) / (G.dlxu[ij] * G.dlyu[ij])) *
+        r = (AO(i, j) * G.rareau[ij]) *
             (G.dlxu[ij] * G.dlyu[ij] * AT(uk, i, j, K) -
-             (aulux(i + 1, j) * G.dlyp[G.L.at2(i + 1, j)] * AO(i + 1, j) * (U1(i + 1, j) - U1(i, j)) /
-                  G.dlxp[G.L.at2(i + 1, j)] -
-              aulux(i, j) * G.dlyp[ij] * AO(i - 1, j) * (U1(i, j) - U1(i - 1, j)) / G.dlxp[ij] +
-              auluy(i, j - 1) * dlxpsi(G, i, j - 1) * AO(i, j - 1) * (U1(i, j - 1) - U1(i, j)) /
-                  dlypsi(G, i, j - 1) -
-              auluy(i, j) * dlxpsi(G, i, j) * AO(i, j + 1) * (U1(i, j) - U1(i, j + 1)) /
-                  dlypsi(G, i, j)));
+             (G.ugx[G.L.at2(i + 1, j)] * AO(i + 1, j) * (U1(i + 1, j) - U1(i, j)) -
+              G.ugx[ij] * AO(i - 1, j) * (U1(i, j) - U1(i - 1, j)) +
+              G.ugy[G.L.at2(i, j - 1)] * AO(i, j - 1) * (U1(i, j - 1) - U1(i, j)) -
+              G.ugy[ij] * AO(i, j + 1) * (U1(i, j) - U1(i, j + 1))));
       }
       AT(uo, i, j, K) = r;
     }
@@ -470,17 +462,13 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
         auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
         auto V1 = [&](int ii, int jj) { return AT(v1, ii, jj, K); };
-        auto aulvx = [&](int ii, int jj) { return G.aulvx[G.L.at2(ii, jj)]; };
-        auto aulvy = [&](int ii, int jj) { return G.aulvy[G.L.at2(ii, jj)]; };
         const long long ij = G.L.at2(i, j);
-        r = (AE(i, j) / (G.dlxv[ij] * G.dlyv[ij])) *
+        r = (AE(i, j) * G.rareav[ij]) *
             (G.dlxv[ij] * G.dlyv[ij] * AT(vk, i, j, K) -
-             (aulvx(i, j) * dlypsi(G, i, j) * AE(i + 1, j) * (V1(i + 1, j) - V1(i, j)) / dlxpsi(G, i, j) -
-              aulvx(i - 1, j) * dlypsi(G, i - 1, j) * AE(i - 1, j) * (V1(i, j) - V1(i - 1, j)) /
-                  dlxpsi(G, i - 1, j) +
-              aulvy(i, j) * G.dlxp[ij] * AE(i, j - 1) * (V1(i, j - 1) - V1(i, j)) / G.dlyp[ij] -
-              aulvy(i, j + 1) * G.dlxp[G.L.at2(i, j + 1)] * AE(i, j + 1) * (V1(i, j) - V1(i, j + 1)) /
-                  G.dlyp[G.L.at2(i, j + 1)]));
+             (G.vgx[ij] * AE(i + 1, j) * (V1(i + 1, j) - V1(i, j)) -
+              G.vgx[G.L.at2(i - 1, j)] * AE(i - 1, j) * (V1(i, j) - V1(i - 1, j)) +
+              G.vgy[ij] * AE(i, j - 1) * (V1(i, j - 1) - V1(i, j)) -
+              G.vgy[G.L.at2(i, j + 1)] * AE(i, j + 1) * (V1(i, j) - V1(i, j + 1))));
       }
       AT(vo, i, j, K) = r;
     }
@@ -493,18 +481,14 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       auto W1 = [&](int ii, int jj) { return AT(w1, ii, jj, K); };
       auto dzu = [&](int ii, int jj) { return fmx(thick(G.gu, G.dzw, G.L.at2(ii, jj), K), mv); };
       auto dzv = [&](int ii, int jj) { return fmx(thick(G.gv, G.dzw, G.L.at2(ii, jj), K), mv); };
-      auto aulwx = [&](int ii, int jj) { return G.aulwx[G.L.at2(ii, jj)]; };
-      auto aulwy = [&](int ii, int jj) { return G.aulwy[G.L.at2(ii, jj)]; };
       const long long ij = G.L.at2(i, j);
       const double dzp = fmx(thick(G.gp, G.dzw, ij, K), mv);
-      r = (WE(i, j) / (G.dlxp[ij] * G.dlyp[ij] * dzp)) *
+      r = ((WE(i, j) * G.rareap[ij]) / dzp) *
           (G.dlxp[ij] * G.dlyp[ij] * dzp * AT(wn, i, j, K) -
-           (+aulwx(i, j) * G.dlyu[ij] * dzu(i, j) * WE(i + 1, j) * (W1(i + 1, j) - W1(i, j)) / G.dlxu[ij] -
-            aulwx(i - 1, j) * G.dlyu[G.L.at2(i - 1, j)] * dzu(i - 1, j) * WE(i - 1, j) *
-                (W1(i, j) - W1(i - 1, j)) / G.dlxu[G.L.at2(i - 1, j)] +
-            aulwy(i, j - 1) * G.dlxv[G.L.at2(i, j - 1)] * dzv(i, j - 1) * WE(i, j - 1) *
-                (W1(i, j - 1) - W1(i, j)) / G.dlyv[G.L.at2(i, j - 1)] -
-            aulwy(i, j) * G.dlxv[ij] * dzv(i, j) * WE(i, j + 1) * (W1(i, j) - W1(i, j + 1)) / G.dlyv[ij]));
+           (G.wgx[ij] * dzu(i, j) * WE(i + 1, j) * (W1(i + 1, j) - W1(i, j)) -
+            G.wgx[G.L.at2(i - 1, j)] * dzu(i - 1, j) * WE(i - 1, j) * (W1(i, j) - W1(i - 1, j)) +
+            G.wgy[G.L.at2(i, j - 1)] * dzv(i, j - 1) * WE(i, j - 1) * (W1(i, j - 1) - W1(i, j)) -
+            G.wgy[ij] * dzv(i, j) * WE(i, j + 1) * (W1(i, j) - W1(i, j + 1))));
     }
     AT(wo, i, j, K) = r;
   }

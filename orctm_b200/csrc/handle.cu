@@ -30,8 +30,13 @@ static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
+// text of the calling thread's last CUDA failure (orctm_last_error)
+thread_local std::string g_cuda_error;
+
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return ORCTM_OK;
+  g_cuda_error = std::string("CUDA error ") + std::to_string((int)e) + " (" + cudaGetErrorName(e) +
+                 "): " + cudaGetErrorString(e);
   if (e == cudaErrorMemoryAllocation) return ORCTM_E_NOMEM;
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ORCTM_E_NODEVICE;
   return ORCTM_E_CUDA;
@@ -193,6 +198,36 @@ struct orctm_handle {
     }
   }
 
+  // Every device array is allocated with a zero-filled guard zone of one
+  // plane plus two rows of elements on each side.  Stencils that evaluate a
+  // neighbour outside an array's index range (a value a zero mask or
+  // coefficient then discards) read the guard, never memory of another
+  // allocation, so results never depend on other instances' data.
+  std::unordered_map<void*, void*> base_of;  // user pointer -> allocation
+  size_t guard_elems() const { return (size_t)L.plane + 2 * (size_t)L.P + 64; }
+  int guarded_alloc(void** out, size_t elem, size_t n) {
+    const size_t g = guard_elems() * elem;
+    const size_t total = n * elem + 2 * g;
+    char* base = nullptr;
+    ORCTM_CUDA_OK(cudaMallocFromPoolAsync((void**)&base, total, mempool, stream));
+#ifdef ORCTM_GUARD_NAN
+    // diagnostic build: guards hold NaN (bytes 0xFF), so any read of a guard
+    // that reaches a result shows up as NaN
+    ORCTM_CUDA_OK(cudaMemsetAsync(base, 0xFF, total, stream));
+    ORCTM_CUDA_OK(cudaMemsetAsync(base + g, 0, n * elem, stream));
+#else
+    ORCTM_CUDA_OK(cudaMemsetAsync(base, 0, total, stream));
+#endif
+    bytes += total;
+    *out = base + g;
+    base_of[*out] = base;
+    return ORCTM_OK;
+  }
+  void* base(void* p) const {
+    auto it = base_of.find(p);
+    return it == base_of.end() ? p : it->second;
+  }
+
   // ---------------------------------------------------------------- pool
   int alloc(double** out) {
     if (!free_.empty()) {
@@ -202,9 +237,8 @@ struct orctm_handle {
       return ORCTM_OK;
     }
     double* p = nullptr;
-    ORCTM_CUDA_OK(cudaMallocFromPoolAsync((void**)&p, sizeof(double) * L.n3(), mempool, stream));
-    ORCTM_CUDA_OK(cudaMemsetAsync(p, 0, sizeof(double) * L.n3(), stream));
-    bytes += sizeof(double) * L.n3();
+    int st;
+    if ((st = guarded_alloc((void**)&p, sizeof(double), (size_t)L.n3()))) return st;
     refs[p] = 1;
     *out = p;
     return ORCTM_OK;
@@ -234,10 +268,8 @@ struct orctm_handle {
   }
   template <typename T>
   int dev_alloc(T** p, size_t n) {
-    const size_t nb = sizeof(T) * std::max<size_t>(n, 1);
-    ORCTM_CUDA_OK(cudaMallocFromPoolAsync((void**)p, nb, mempool, stream));
-    ORCTM_CUDA_OK(cudaMemsetAsync(*p, 0, nb, stream));
-    bytes += nb;
+    int st;
+    if ((st = guarded_alloc((void**)p, sizeof(T), std::max<size_t>(n, 1)))) return st;
     owned.push_back(*p);
     return ORCTM_OK;
   }
@@ -451,6 +483,55 @@ int setup(orctm_handle* h, const orctm_desc* d) {
         (st = upg(G.aulwx, aulwx)) || (st = upg(G.aulwy, aulwy)) || (st = upg(G.dlypsi, dlypsi)) ||
         (st = upg(G.dlxpsi, dlxpsi)))
       return st;
+
+    // reciprocal metrics over each staggering's own index range
+    auto rec = [](double v) { return v != 0.0 ? 1.0 / v : 0.0; };
+    std::vector<double> rdlxp(n2, 0.), rdlyp(n2, 0.), rdlxu(n2, 0.), rdlyu(n2, 0.),
+        rdlxv(n2, 0.), rdlyv(n2, 0.), rdlxpsi(n2, 0.), rdlypsi(n2, 0.), tfx(n2, 0.), tfy(n2, 0.),
+        ugx(n2, 0.), ugy(n2, 0.), vgx(n2, 0.), vgy(n2, 0.), wgx(n2, 0.), wgy(n2, 0.),
+        rareau(n2, 0.), rareav(n2, 0.), rareap(n2, 0.);
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {  // u-points
+        const size_t s = L.at2(i, j);
+        const double xu = d->dlxu[x.u2(i, j)], yu = d->dlyu[x.u2(i, j)];
+        rdlxu[s] = rec(xu);
+        rdlyu[s] = rec(yu);
+        rdlypsi[s] = rec(dlypsi[s]);
+        rareau[s] = rec(xu * yu);
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {  // v-points
+        const size_t s = L.at2(i, j);
+        const double xv = d->dlxv[x.v2(i, j)], yv = d->dlyv[x.v2(i, j)];
+        rdlxv[s] = rec(xv);
+        rdlyv[s] = rec(yv);
+        rdlxpsi[s] = rec(dlxpsi[s]);
+        rareav[s] = rec(xv * yv);
+      }
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {  // p-points and the face coefficients
+        const size_t s = L.at2(i, j);
+        const double xp = d->dlxp[x.p2(i, j)], yp = d->dlyp[x.p2(i, j)];
+        rdlxp[s] = rec(xp);
+        rdlyp[s] = rec(yp);
+        rareap[s] = rec(xp * yp);
+        tfx[s] = aulx[s] * d->dlyu[x.u2(i, j)] * rec(d->dlxu[x.u2(i, j)]);
+        tfy[s] = auly[s] * d->dlxv[x.v2(i, j)] * rec(d->dlyv[x.v2(i, j)]);
+        ugx[s] = aulux[s] * yp * rec(xp);
+        ugy[s] = auluy[s] * dlxpsi[s] * rec(dlypsi[s]);
+        vgx[s] = aulvx[s] * dlypsi[s] * rec(dlxpsi[s]);
+        vgy[s] = aulvy[s] * xp * rec(yp);
+        wgx[s] = aulwx[s] * d->dlyu[x.u2(i, j)] * rec(d->dlxu[x.u2(i, j)]);
+        wgy[s] = aulwy[s] * d->dlxv[x.v2(i, j)] * rec(d->dlyv[x.v2(i, j)]);
+      }
+    if ((st = upg(G.rdlxp, rdlxp)) || (st = upg(G.rdlyp, rdlyp)) || (st = upg(G.rdlxu, rdlxu)) ||
+        (st = upg(G.rdlyu, rdlyu)) || (st = upg(G.rdlxv, rdlxv)) || (st = upg(G.rdlyv, rdlyv)) ||
+        (st = upg(G.rdlxpsi, rdlxpsi)) || (st = upg(G.rdlypsi, rdlypsi)) ||
+        (st = upg(G.tfx, tfx)) || (st = upg(G.tfy, tfy)) || (st = upg(G.ugx, ugx)) ||
+        (st = upg(G.ugy, ugy)) || (st = upg(G.vgx, vgx)) || (st = upg(G.vgy, vgy)) ||
+        (st = upg(G.wgx, wgx)) || (st = upg(G.wgy, wgy)) || (st = upg(G.rareau, rareau)) ||
+        (st = upg(G.rareav, rareav)) || (st = upg(G.rareap, rareap)))
+      return st;
   }
 
   // Poisson tables (mo_petsc.f90:557-599)
@@ -550,6 +631,7 @@ int setup(orctm_handle* h, const orctm_desc* d) {
       return st;
     P.dinv64 = d64;
     P.dinv32 = d32;
+    ORCTM_CUDA_OK(pcg_prepare_device());
     launch_factor(G, P, d64, d32, h->stream);
     ORCTM_CUDA_OK(cudaGetLastError());
   }
@@ -612,6 +694,7 @@ int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* p
   for (; it < maxit; ++it) {
     PROF(h, ORCTM_PROF_PCG_SPMV, (launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, sv, h->stream)));
     PROF(h, ORCTM_PROF_PCG_COL, (launch_pcg_col<T, TX>(G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream)));
+    ORCTM_CUDA_OK(cudaGetLastError());  // a rejected launch is reported at once
     std::swap(pc, pn);
     if ((it + 1) % check == 0 || it + 1 == maxit) {
       int st;
@@ -937,6 +1020,8 @@ const char* orctm_status_string(int s) {
 }
 
 const char* orctm_last_error(const orctm_handle* h) {
+  if (h && !h->err.empty()) return h->err.c_str();
+  if (!g_cuda_error.empty()) return g_cuda_error.c_str();
   return h ? h->err.c_str() : g_create_error.c_str();
 }
 
@@ -951,8 +1036,8 @@ int orctm_destroy(orctm_handle* h) {
   // stream-ordered frees: no device-wide synchronisation, so other handles'
   // work in flight on the device is not stalled
   if (h->stream) {
-    for (double* p : all) cudaFreeAsync(p, h->stream);
-    for (void* p : h->owned) cudaFreeAsync(p, h->stream);
+    for (double* p : all) cudaFreeAsync(h->base(p), h->stream);
+    for (void* p : h->owned) cudaFreeAsync(h->base(p), h->stream);
     cudaStreamSynchronize(h->stream);
   }
   if (h->hS) pinned_state_put(h->hS);
@@ -973,6 +1058,7 @@ int orctm_destroy(orctm_handle* h) {
 
 int orctm_create(const orctm_desc* d, orctm_handle** out) {
   g_create_error.clear();
+  g_cuda_error.clear();
   if (!d || !out) return ORCTM_E_ARG;
   *out = nullptr;
   auto bad = [&](int st, const char* m) {
@@ -1181,8 +1267,11 @@ int orctm_estimate_device_bytes(const orctm_desc* d, int solver, unsigned long l
   const double f3 = 12.0 + d->ntracers + 8.0 + 9.0 + 1.5 +
                     (solver == ORCTM_SOLVER_FP32_REFINED ? 3.5 : 0.0);
   // 2D tables (compressed columns, metrics, biharmonic and Poisson factors)
-  const double f2 = 64.0;
-  *bytes = (unsigned long long)((f3 * n3 + f2 * plane) * 8.0) + (1ULL << 20);
+  const double f2 = 96.0;
+  // every array carries two guard zones of about one plane
+  const double guard = 2.0 * (plane + 2.0 * P + 64.0);
+  *bytes = (unsigned long long)((f3 * (n3 + guard) + f2 * (plane + guard) + 16.0 * guard) * 8.0) +
+           (1ULL << 20);
   return ORCTM_OK;
 }
 

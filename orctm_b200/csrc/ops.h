@@ -70,6 +70,9 @@ void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T*
 // kernel variants the autotuner chooses between (a variant a grid cannot use
 // falls back to variant 0)
 int pcg_col_variants();
+// raises the shared-memory opt-in of the column-kernel variants on the
+// current device (called once per handle at creation)
+cudaError_t pcg_prepare_device();
 template <typename T>
 bool pcg_col_variant_ok(const Geo& G, int variant);
 int pcg_spmv_variants();

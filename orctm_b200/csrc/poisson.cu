@@ -729,11 +729,14 @@ constexpr size_t kColSmemMax = 96 * 1024;
 template <typename T, int MODE, bool SM, int U>
 void col_launch(dim3 blk, size_t smem, const Geo& G, const PoissonGeo& P, SolverState* S,
                 const T* b, T* x, T* r, const T* p, const T* q, T* z, cudaStream_t st) {
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_pcg_col<T, MODE, SM, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
   k_pcg_col<T, MODE, SM, U><<<grid2(G.L.ie - 2, G.L.je - 2, blk), blk, smem, st>>>(G, P, S, b, x,
                                                                                   r, p, q, z);
+}
+
+template <typename T, int MODE, int U>
+cudaError_t col_optin() {
+  return cudaFuncSetAttribute(k_pcg_col<T, MODE, true, U>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kColSmemMax);
 }
 
 template <typename T, int SM, int U>
@@ -756,6 +759,21 @@ bool pcg_col_variant_ok(const Geo& G, int variant) {
 template bool pcg_col_variant_ok<double>(const Geo&, int);
 template bool pcg_col_variant_ok<float>(const Geo&, int);
 int pcg_col_variants() { return kNumColVariants; }
+
+// The shared-memory variants' dynamic shared memory (plus about 2.6 KB of
+// static) may exceed the 48 KB default, so their opt-in is raised to the
+// variants' fixed maximum on the current device.  Every caller sets the same
+// value (the attribute is process-wide per kernel), so handles created on
+// several threads never lower it under one another's launches.
+cudaError_t pcg_prepare_device() {
+  const cudaError_t e[] = {col_optin<double, 1, 4>(), col_optin<double, 2, 4>(),
+                           col_optin<double, 1, 8>(), col_optin<double, 2, 8>(),
+                           col_optin<float, 1, 4>(),  col_optin<float, 2, 4>(),
+                           col_optin<float, 1, 8>(),  col_optin<float, 2, 8>()};
+  for (cudaError_t x : e)
+    if (x != cudaSuccess) return x;
+  return cudaSuccess;
+}
 
 template <typename T, typename TX>
 void launch_pcg_col(const Geo& G, const PoissonGeo& P, SolverState* S, int mode, const T* b, TX* x,

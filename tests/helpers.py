@@ -11,6 +11,8 @@ SMALL = {
     "c2s": ("c2", dict(nx=40, ny=33, nz=24), None),
     "c2cfl": ("c2", dict(nx=37, ny=29, nz=18), 0.45),
     "c4m": ("c4", dict(nx=50, ny=41, nz=31), None),
+    # deep columns: the shared-memory solver variants need the opt-in above 48 KB
+    "c4deep": ("c4", dict(nx=37, ny=29, nz=97), None),
 }
 
 

@@ -134,7 +134,7 @@ def test_step_hotpath(case):
 
 
 @pytest.mark.parametrize("mode", ["fp64", "fp32_refined"])
-@pytest.mark.parametrize("case_name", ["c2s", "c1s"])
+@pytest.mark.parametrize("case_name", ["c2s", "c1s", "c4deep"])
 def test_solver_variants_bit_identical(case_name, mode):
     """Every column-kernel and stencil-kernel variant the autotuner chooses
     between gives the same pressure bit for bit, with the same iteration
