@@ -167,6 +167,11 @@ int orctm_profile_get(orctm_handle* h, int kind, long long* launches, double* to
 /* Number of CUDA kernels this library has launched in the calling process. */
 unsigned long long orctm_kernel_launches(void);
 
+/* Numerical self-check: q[k] = a[k] / b[k] computed on the device by the
+ * division the stencil kernels use (Newton-Raphson refinement of a reciprocal
+ * estimate, within 1 ulp of IEEE division).  Test support; allocates. */
+int orctm_check_division(int device, const double* a, const double* b, double* q, size_t n);
+
 /* Kernel variants of the Poisson solver: 4 column-kernel variants (forward
  * values in global or shared memory, 4 or 8 levels per load batch) and 4
  * stencil variants (shared-memory ring or L1 form, 32x8 or 32x4 blocks).

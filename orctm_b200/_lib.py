@@ -61,7 +61,7 @@ EXPORTS = (
     "orctm_trim_device_memory", "orctm_set_tuning", "orctm_get_tuning",
     "orctm_serve_create", "orctm_serve_submit", "orctm_serve_wait", "orctm_serve_poll",
     "orctm_serve_drain", "orctm_serve_get_stats", "orctm_serve_destroy", "orctm_batch_run",
-    "orctm_estimate_device_bytes",
+    "orctm_estimate_device_bytes", "orctm_check_division",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -106,6 +106,7 @@ def load(build_if_missing: bool = True):
     lib.orctm_device_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
     lib.orctm_trim_device_memory.argtypes = [C.c_int]
     lib.orctm_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.orctm_check_division.argtypes = [C.c_int, _D, _D, _D, C.c_size_t]
     lib.orctm_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     _lib = lib
     return lib

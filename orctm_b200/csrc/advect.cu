@@ -12,7 +12,8 @@
 // update one cell per thread.  Every sweep writes a fresh buffer (never in place), so
 // neighbouring columns always read the previous sweep's values.  Arithmetic is
 // IEEE binary64 in the reference's operation order (built with --fmad=false),
-// so results match the CPU restatement bit for bit.
+// except that the three divisions of a face and a cell use div_nr (within
+// 1 ulp of IEEE division), so results match the CPU restatement to a few ulp.
 #include "common.cuh"
 #include "ops.h"
 
@@ -30,8 +31,8 @@ __device__ __forceinline__ Fl limited_nm(double up, double um, double t, double 
                                          double vol, double cap) {
   const double abl = fabs(tprev - tnext);
   const double zwabl = fabs(tprev + tnext - 2. * t);
-  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
-  const double sch = fmn(cap, scha * vol / (up + um + 1.E-20));
+  const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20));
+  const double sch = fmn(cap, div_nr(scha * vol, up + um + 1.E-20));
   const double schi = 1. - sch;
   Fl f;
   f.trp = up * (schi * t + sch * 0.5 * (t + tprev));
@@ -56,7 +57,7 @@ __device__ __forceinline__ Fl zero_fl() { return Fl{0., 0., 0., 0.}; }
 __device__ __forceinline__ void apply(double t, double v, const Fl& m, const Fl& c, const Fl& p,
                                       double& tn, double& vn) {
   const double rn = v + m.wtp - c.wtp - c.wtm + p.wtm;
-  tn = (t * v + m.trp - c.trp - c.trm + p.trm) / rn;
+  tn = div_nr(t * v + m.trp - c.trp - c.trm + p.trm, rn);
   vn = rn;
 }
 
@@ -64,7 +65,7 @@ __device__ __forceinline__ void apply(double t, double v, const Fl& m, const Fl&
 __device__ __forceinline__ void apply_z(double t, double v, const Fl& fm, const Fl& fc,
                                         const Fl& fp, double& tn, double& vn) {
   const double rn = v + fp.wtp - fc.wtp - fc.wtm + fm.wtm;
-  tn = (t * v + fp.trp - fc.trp - fc.trm + fm.trm) / rn;
+  tn = div_nr(t * v + fp.trp - fc.trp - fc.trm + fm.trm, rn);
   vn = rn;
 }
 
@@ -102,8 +103,8 @@ __global__ void k_adpo_z(Geo G, const double* __restrict__ T, const double* __re
     const double um = cdt * (fabs(w1) - w1);
     const double abl = fabs(tu - tl);
     const double zwabl = fabs(tu + tl - 2. * t);
-    const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20));
-    double sch = fmn(wet(G.gp, ij, klo), scha * vol / (up + um + 1.E-20));
+    const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20));
+    double sch = fmn(wet(G.gp, ij, klo), div_nr(scha * vol, up + um + 1.E-20));
     if (K == 1 || K == KE) sch = 0.;
     const double schi = 1. - sch;
     Fl f;
@@ -146,9 +147,9 @@ __device__ __forceinline__ Fl adpo_xflux(const Geo& G, const double* T, const do
   const double t = AT(T, q, j, K), te = AT(T, q + 1, j, K), tw = AT(T, q - 1, j, K);
   const double abl = fabs(te - tw);
   const double zwabl = fabs(te + tw - 2. * t);
-  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, ij, K) *
+  const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20)) * wet(G.gp, ij, K) *
                       wet(G.gp, G.L.at2(q + 1, j), K) * wet(G.gp, G.L.at2(q - 1, j), K);
-  const double sch = fmn(1., scha * AT(V, q, j, K) / (up + um + 1.E-20));
+  const double sch = fmn(1., div_nr(scha * AT(V, q, j, K), up + um + 1.E-20));
   const double schi = 1. - sch;
   Fl f;
   f.trp = up * (schi * t + sch * 0.5 * (t + te));
@@ -168,9 +169,9 @@ __device__ __forceinline__ Fl adpo_yflux(const Geo& G, const double* T, const do
   const double t = AT(T, i, q, K), tn = AT(T, i, q - 1, K), ts = AT(T, i, q + 1, K);
   const double abl = fabs(tn - ts);
   const double zwabl = fabs(tn + ts - 2. * t);
-  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, ij, K) *
+  const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20)) * wet(G.gp, ij, K) *
                       wet(G.gp, G.L.at2(i, q - 1), K) * wet(G.gp, G.L.at2(i, q + 1), K);
-  const double sch = fmn(1., scha * AT(V, i, q, K) / (up + um + 1.E-20));
+  const double sch = fmn(1., div_nr(scha * AT(V, i, q, K), up + um + 1.E-20));
   const double schi = 1. - sch;
   Fl f;
   f.trp = up * (schi * t + sch * 0.5 * (t + tn));
@@ -464,9 +465,9 @@ __device__ __forceinline__ Fl wad_xflux(const Geo& G, const double* T, const dou
   const double t = AT(T, q, j, K), te = AT(T, q + 1, j, K), tw = AT(T, q - 1, j, K);
   const double abl = fabs(te - tw);
   const double zwabl = fabs(te + tw - 2. * t);
-  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, G.L.at2(q, j), K) *
+  const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20)) * wet(G.gp, G.L.at2(q, j), K) *
                       wet(G.gp, G.L.at2(q + 1, j), K) * wet(G.gp, G.L.at2(q - 1, j), K);
-  const double sch = fmn(1., scha * AT(V, q, j, K) / (up + um + 1.E-20));
+  const double sch = fmn(1., div_nr(scha * AT(V, q, j, K), up + um + 1.E-20));
   const double schi = 1. - sch;
   return Fl{up * (schi * t + sch * 0.5 * (t + te)), um * (schi * t + sch * 0.5 * (t + tw)), up, um};
 }
@@ -482,9 +483,9 @@ __device__ __forceinline__ Fl wad_yflux(const Geo& G, const double* T, const dou
   const double t = AT(T, i, q, K), tn = AT(T, i, q - 1, K), ts = AT(T, i, q + 1, K);
   const double abl = fabs(tn - ts);
   const double zwabl = fabs(tn + ts - 2. * t);
-  const double scha = fmx(0., (abl - zwabl) / (abl + 1.E-20)) * wet(G.gp, G.L.at2(i, q), K) *
+  const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20)) * wet(G.gp, G.L.at2(i, q), K) *
                       wet(G.gp, G.L.at2(i, q - 1), K) * wet(G.gp, G.L.at2(i, q + 1), K);
-  const double sch = fmn(1., scha * AT(V, i, q, K) / (up + um + 1.E-20));
+  const double sch = fmn(1., div_nr(scha * AT(V, i, q, K), up + um + 1.E-20));
   const double schi = 1. - sch;
   return Fl{up * (schi * t + sch * 0.5 * (t + tn)), um * (schi * t + sch * 0.5 * (t + ts)), up, um};
 }

@@ -6,7 +6,11 @@
 // thread per column with the column's tridiagonal system in thread-local
 // arrays.  The horizontal biharmonic operator is two passes (a masked
 // Laplacian into a scratch field, then the flux-form update), one thread per
-// cell.  Arithmetic follows the reference's operation order in IEEE binary64.
+// cell.  Arithmetic follows the reference's operation order in IEEE binary64,
+// with two changes that stay within a few ulp: the stencils multiply by
+// reciprocal metrics and per-face coefficients computed once at set-up
+// instead of dividing by the metrics, and the remaining divisions (by
+// thicknesses and Thomas pivots) use div_nr (within 1 ulp of IEEE division).
 #include "common.cuh"
 #include "ops.h"
 
@@ -50,19 +54,19 @@ __global__ void __launch_bounds__(64) k_tdiff_vert(Geo G, TrPtrs tp, int ntr,
     const double zzsurf = K == 1 ? 1. : 0.;
     return thick(G.gp, G.dzw, ij, K) + zzsurf * (zij) + G.almzer;
   };
-  auto tri3 = [&](int K, double dn) { return -G.dt * AT(dvo, i, j, K + 1) * G.di[K] / dn; };
+  auto tri3 = [&](int K, double dn) { return div_nr(-G.dt * AT(dvo, i, j, K + 1) * G.di[K], dn); };
   double t2p[kMaxKe];
   double ylast[8];
   double t2prev = 1.0, t3prev = 0.0;
   for (int K = 1; K <= KE; ++K) {
     const double dn = den(K);
-    const double t1 = -G.dt * AT(dvo, i, j, K) * wet(G.gp, ij, K) * G.di[K - 1] / dn;
+    const double t1 = div_nr(-G.dt * AT(dvo, i, j, K) * wet(G.gp, ij, K) * G.di[K - 1], dn);
     const double t3 = tri3(K, dn);
     double t2 = 1. - t1 - t3;
     double m = 0.0;
     if (K >= 2) {
-      m = t1 / t2prev;                       // TRIDSY(K-1,1) after elimination
-      t2 = t2 - t3prev * t1 / t2prev;        // TRIDSY(K,2) after elimination
+      m = div_nr(t1, t2prev);                       // TRIDSY(K-1,1) after elimination
+      t2 = t2 - div_nr(t3prev * t1, t2prev);        // TRIDSY(K,2) after elimination
     }
     t2p[K - 1] = t2;
 #pragma unroll
@@ -80,7 +84,7 @@ __global__ void __launch_bounds__(64) k_tdiff_vert(Geo G, TrPtrs tp, int ntr,
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     if (n >= ntr) break;
-    nxt[n] = AT(tp.out[n], i, j, KE) / t2p[KE - 1];
+    nxt[n] = div_nr(AT(tp.out[n], i, j, KE), t2p[KE - 1]);
     AT(tp.out[n], i, j, KE) = nxt[n];
   }
   for (int l = KE - 1; l >= 1; --l) {
@@ -88,7 +92,7 @@ __global__ void __launch_bounds__(64) k_tdiff_vert(Geo G, TrPtrs tp, int ntr,
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
       if (n >= ntr) break;
-      nxt[n] = (AT(tp.out[n], i, j, l) - t3 * nxt[n]) / t2p[l - 1];
+      nxt[n] = div_nr(AT(tp.out[n], i, j, l) - t3 * nxt[n], t2p[l - 1]);
       AT(tp.out[n], i, j, l) = nxt[n];
     }
   }
@@ -133,8 +137,8 @@ __global__ void k_tdiff_bih(Geo G, const double* __restrict__ T, const double* _
     const double c = AT(L1, i, j, K);
     // W / ((DDPO + ALMZER + ZZSURF ZO) DLXP DLYP) with 1/(DLXP DLYP) precomputed;
     // face terms AULX DLYU / DLXU and AULY DLXV / DLYV precomputed per face
-    const double fac = (w(i, j) * G.rareap[ij]) /
-                       (thick(G.gp, G.dzw, ij, K) + G.almzer + zzsurf * (zo[ij]));
+    const double fac = div_nr(w(i, j) * G.rareap[ij],
+                              thick(G.gp, G.dzw, ij, K) + G.almzer + zzsurf * (zo[ij]));
     r = t - fac * G.dzw[K - 1] *
                 (w(i - 1, j) * G.tfx[G.L.at2(i - 1, j)] * (AT(L1, i - 1, j, K) - c) +
                  w(i + 1, j) * G.tfx[ij] * (AT(L1, i + 1, j, K) - c) +
@@ -212,12 +216,12 @@ __global__ void __launch_bounds__(64) k_visc_uv(Geo G, const double* __restrict_
       const double am1 = wet(cg, ij, K + 1);
       const double avlo = 0.5 * (avo_at(ij, K + 1) + avo_at(ij2, K + 1)) * am1 +
                           (BOFRIC + RAYFRIC * dd * sp) * (am - am1);
-      t1 = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
-      t3 = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
+      t1 = div_nr(-G.dt * avup * am * G.di[K - 1], G.almzer + dd);
+      t3 = div_nr(-G.dt * avlo * am * G.di[K], G.almzer + dd);
     } else {
       const double avlo = (BOFRIC + RAYFRIC * dd * sp) * am;
-      t1 = -G.dt * avup * am * G.di[K - 1] / (G.almzer + dd);
-      t3 = -G.dt * avlo * am * G.di[K] / (G.almzer + dd);
+      t1 = div_nr(-G.dt * avup * am * G.di[K - 1], G.almzer + dd);
+      t3 = div_nr(-G.dt * avlo * am * G.di[K], G.almzer + dd);
     }
   };
   double t2p[kMaxKe];
@@ -230,8 +234,8 @@ __global__ void __launch_bounds__(64) k_visc_uv(Geo G, const double* __restrict_
     const double xk = AT(X, i, j, K);
     double y = xk;
     if (K >= 2) {
-      const double m = t1 / t2prev;
-      t2 = t2 - t3prev * t1 / t2prev;
+      const double m = div_nr(t1, t2prev);
+      t2 = t2 - div_nr(t3prev * t1, t2prev);
       y = xk - m * yprev;
     }
     t2p[K - 1] = t2;
@@ -240,13 +244,13 @@ __global__ void __launch_bounds__(64) k_visc_uv(Geo G, const double* __restrict_
     t2prev = t2;
     t3prev = t3;
   }
-  double nxt = wet(cg, ij, KE) * AT(O, i, j, KE) / t2p[KE - 1];
+  double nxt = div_nr(wet(cg, ij, KE) * AT(O, i, j, KE), t2p[KE - 1]);
   AT(O, i, j, KE) = nxt;
   for (int l = KE - 1; l >= 1; --l) {
     double t1, t3;
     tri(l, t1, t3);
     t3 = t3 * wet(cg, ij, l + 1);
-    nxt = (AT(O, i, j, l) - t3 * nxt) * wet(cg, ij, l) / t2p[l - 1];
+    nxt = div_nr((AT(O, i, j, l) - t3 * nxt) * wet(cg, ij, l), t2p[l - 1]);
     AT(O, i, j, l) = nxt;
   }
 }
@@ -269,8 +273,8 @@ __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __re
     const double avup = 0.5 * (AT(avo, i, j, K - 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K - 1);
     const double avlo = 0.5 * (AT(avo, i, j, K + 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K);
     const double den = 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
-    t1[K - 1] = -2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2] / den;
-    t3[K - 1] = -2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1] / den;
+    t1[K - 1] = div_nr(-2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2], den);
+    t3[K - 1] = div_nr(-2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1], den);
     t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
   }
   {
@@ -278,15 +282,15 @@ __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __re
     const double avup = 0.5 * (AT(avo, i, j, K - 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K - 1);
     const double avlo = 0.0;
     const double den = 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
-    t1[K - 1] = -2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2] / den;
-    t3[K - 1] = -2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1] / den;
+    t1[K - 1] = div_nr(-2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2], den);
+    t3[K - 1] = div_nr(-2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1], den);
     t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
     t3[K - 1] = 0.;
   }
   for (int K = 3; K <= KE; ++K) {
     const double a = t1[K - 1];
-    t1[K - 2] = a / t2[K - 2];
-    t2[K - 1] = t2[K - 1] - t3[K - 2] * a / t2[K - 2];
+    t1[K - 2] = div_nr(a, t2[K - 2]);
+    t2[K - 1] = t2[K - 1] - div_nr(t3[K - 2] * a, t2[K - 2]);
   }
   AT(O, i, j, 1) = AT(W, i, j, 1);
   AT(O, i, j, KE + 1) = AT(W, i, j, KE + 1);
@@ -296,10 +300,10 @@ __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __re
     prev = AT(W, i, j, K) - t1[K - 2] * prev;
     AT(O, i, j, K) = prev;
   }
-  double nxt = wet(G.gp, ij, KE) * AT(O, i, j, KE) / t2[KE - 1];
+  double nxt = div_nr(wet(G.gp, ij, KE) * AT(O, i, j, KE), t2[KE - 1]);
   AT(O, i, j, KE) = nxt;
   for (int K = KE - 1; K >= 2; --K) {
-    nxt = (AT(O, i, j, K) - t3[K - 1] * nxt) * wet(G.gp, ij, K) / t2[K - 1];
+    nxt = div_nr((AT(O, i, j, K) - t3[K - 1] * nxt) * wet(G.gp, ij, K), t2[K - 1]);
     AT(O, i, j, K) = nxt;
   }
 }
@@ -483,7 +487,7 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       auto dzv = [&](int ii, int jj) { return fmx(thick(G.gv, G.dzw, G.L.at2(ii, jj), K), mv); };
       const long long ij = G.L.at2(i, j);
       const double dzp = fmx(thick(G.gp, G.dzw, ij, K), mv);
-      r = ((WE(i, j) * G.rareap[ij]) / dzp) *
+      r = div_nr(WE(i, j) * G.rareap[ij], dzp) *
           (G.dlxp[ij] * G.dlyp[ij] * dzp * AT(wn, i, j, K) -
            (G.wgx[ij] * dzu(i, j) * WE(i + 1, j) * (W1(i + 1, j) - W1(i, j)) -
             G.wgx[G.L.at2(i - 1, j)] * dzu(i - 1, j) * WE(i - 1, j) * (W1(i, j) - W1(i - 1, j)) +

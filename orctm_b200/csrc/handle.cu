@@ -999,8 +999,32 @@ int r_ocvtot_nh(orctm_handle* h, orctm_solve_stats* stats) {
 
 }  // namespace
 
+__global__ void k_div_nr(const double* __restrict__ a, const double* __restrict__ b,
+                         double* __restrict__ q, size_t n) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) q[k] = div_nr(a[k], b[k]);
+}
+
 // ====================================================================== C ABI
 extern "C" {
+
+int orctm_check_division(int device, const double* a, const double* b, double* q, size_t n) {
+  if (!a || !b || !q) return ORCTM_E_ARG;
+  if (n == 0) return ORCTM_OK;
+  ORCTM_CUDA_OK(cudaSetDevice(device));
+  double* d = nullptr;
+  ORCTM_CUDA_OK(cudaMalloc(&d, 3 * n * sizeof(double)));
+  int st = cuda_status(cudaMemcpy(d, a, n * sizeof(double), cudaMemcpyHostToDevice));
+  if (!st) st = cuda_status(cudaMemcpy(d + n, b, n * sizeof(double), cudaMemcpyHostToDevice));
+  if (!st) {
+    k_div_nr<<<(unsigned)((n + 255) / 256), 256>>>(d, d + n, d + 2 * n, n);
+    count_launch();
+    st = cuda_status(cudaGetLastError());
+  }
+  if (!st) st = cuda_status(cudaMemcpy(q, d + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  return st;
+}
 
 int orctm_abi_version(void) { return ORCTM_ABI_VERSION; }
 
