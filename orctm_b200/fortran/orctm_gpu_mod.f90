@@ -93,6 +93,22 @@ module orctm_gpu_mod
        integer(c_int), value :: mode, maxit
        real(c_double), value :: rtol
      end function
+     integer(c_int) function orctm_set_tuning(h, col_variant, spmv_variant) &
+         bind(c, name="orctm_set_tuning")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: col_variant, spmv_variant
+     end function
+     integer(c_int) function orctm_device_bytes(h, bytes) bind(c, name="orctm_device_bytes")
+       import :: c_int, c_ptr, c_long_long
+       type(c_ptr), value :: h
+       integer(c_long_long), intent(out) :: bytes
+     end function
+     integer(c_int) function orctm_trim_device_memory(device) &
+         bind(c, name="orctm_trim_device_memory")
+       import :: c_int
+       integer(c_int), value :: device
+     end function
   end interface
 
   type(c_ptr), save :: orctm_h = c_null_ptr
