@@ -28,6 +28,7 @@ namespace orctm {
 
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void add_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 // text of the calling thread's last CUDA failure (orctm_last_error)
@@ -150,6 +151,9 @@ struct orctm_handle {
   // kernel variants per precision (0 FP64, 1 FP32); -1 = not chosen yet
   int col_var[2] = {-1, -1}, spmv_var[2] = {-1, -1};
   int force_col = -1, force_spmv = -1;  // orctm_set_tuning
+  // replayed chunk of PCG iterations per precision and the variants it holds
+  cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
+  int pcg_graph_key[2][2] = {{-1, -1}, {-1, -1}};
   SolverState* hS = nullptr;  // pinned mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t tm0 = nullptr, tm1 = nullptr;  // orctm_timer_start / _stop
@@ -680,6 +684,52 @@ int read_state(orctm_handle* h) {
   return ORCTM_OK;
 }
 
+// Eight PCG iterations (stencil + column kernel each) are captured once per
+// precision into a CUDA graph and replayed between convergence checks: the
+// vectors, the solver scalars and the kernel variants of a handle are fixed,
+// and after an even number of iterations the two p buffers are back in their
+// starting roles, so every chunk from iteration 8 on issues the same launches.
+// The graph is rebuilt when the variants change; with profiling on, the
+// launches go one by one (they are bracketed by events).
+constexpr int kPcgChunk = 8;
+
+template <typename T, typename TX>
+int pcg_chunk_graph(orctm_handle* h, const T* b, TX* x, T* r, T* z, T* pa, T* pb, T* q,
+                    cudaGraphExec_t* out) {
+  const int pr = sizeof(T) == 4;
+  const int cv = h->col_var[pr], sv = h->spmv_var[pr];
+  if (h->pcg_graph[pr] && h->pcg_graph_key[pr][0] == cv && h->pcg_graph_key[pr][1] == sv) {
+    *out = h->pcg_graph[pr];
+    return ORCTM_OK;
+  }
+  if (h->pcg_graph[pr]) {
+    cudaGraphExecDestroy(h->pcg_graph[pr]);
+    h->pcg_graph[pr] = nullptr;
+  }
+  const unsigned long long before = launch_count();
+  ORCTM_CUDA_OK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  T *pc = pa, *pn = pb;
+  for (int k = 0; k < kPcgChunk; ++k) {
+    launch_pcg_spmv<T>(h->G, h->P, h->S, z, pc, pn, q, 0, sv, h->stream);
+    launch_pcg_col<T, TX>(h->G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream);
+    std::swap(pc, pn);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e1 = cudaStreamEndCapture(h->stream, &g);
+  // launches are counted when the graph runs, not when it is recorded
+  add_launches(-(long long)(launch_count() - before));
+  ORCTM_CUDA_OK(e1);
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0ULL);
+  cudaGraphDestroy(g);
+  ORCTM_CUDA_OK(e2);
+  h->pcg_graph[pr] = ex;
+  h->pcg_graph_key[pr][0] = cv;
+  h->pcg_graph_key[pr][1] = sv;
+  *out = ex;
+  return ORCTM_OK;
+}
+
 template <typename T, typename TX>
 int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* pa, T* pb, T* q,
              int maxit, int* iters, int* conv) {
@@ -688,15 +738,25 @@ int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* p
   const int cv = h->col_var[pr], sv = h->spmv_var[pr];
   launch_pcg_col<T, TX>(G, h->P, h->S, init_mode, b, x, r, nullptr, nullptr, z, cv, h->stream);
   ORCTM_CUDA_OK(cudaGetLastError());
-  const int check = 8;
+  const int check = kPcgChunk;
   int it = 0;
   T *pc = pa, *pn = pb;
-  for (; it < maxit; ++it) {
-    PROF(h, ORCTM_PROF_PCG_SPMV, (launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, sv, h->stream)));
-    PROF(h, ORCTM_PROF_PCG_COL, (launch_pcg_col<T, TX>(G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream)));
-    ORCTM_CUDA_OK(cudaGetLastError());  // a rejected launch is reported at once
-    std::swap(pc, pn);
-    if ((it + 1) % check == 0 || it + 1 == maxit) {
+  while (it < maxit) {
+    if (it > 0 && it % kPcgChunk == 0 && it + kPcgChunk <= maxit && !h->prof) {
+      cudaGraphExec_t ex;
+      int st;
+      if ((st = pcg_chunk_graph<T, TX>(h, b, x, r, z, pa, pb, q, &ex))) return st;
+      ORCTM_CUDA_OK(cudaGraphLaunch(ex, h->stream));
+      add_launches(2 * kPcgChunk);
+      it += kPcgChunk;  // pc, pn end where they started
+    } else {
+      PROF(h, ORCTM_PROF_PCG_SPMV, (launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, sv, h->stream)));
+      PROF(h, ORCTM_PROF_PCG_COL, (launch_pcg_col<T, TX>(G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream)));
+      ORCTM_CUDA_OK(cudaGetLastError());  // a rejected launch is reported at once
+      std::swap(pc, pn);
+      ++it;
+    }
+    if (it % check == 0 || it == maxit) {
       int st;
       ORCTM_CUDA_OK(cudaGetLastError());
       if ((st = read_state(h))) return st;
@@ -1064,6 +1124,8 @@ int orctm_destroy(orctm_handle* h) {
     for (void* p : h->owned) cudaFreeAsync(h->base(p), h->stream);
     cudaStreamSynchronize(h->stream);
   }
+  for (int pr = 0; pr < 2; ++pr)
+    if (h->pcg_graph[pr]) cudaGraphExecDestroy(h->pcg_graph[pr]);
   if (h->hS) pinned_state_put(h->hS);
   for (int k = 0; k < ORCTM_PROF_KINDS; ++k)
     for (auto& pr : h->prof_pairs[k]) {

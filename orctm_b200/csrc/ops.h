@@ -92,6 +92,7 @@ int cuda_status(cudaError_t e);
 
 // number of kernels launched by this library (all handles, this process)
 void count_launch();
+void add_launches(long long n);  // kernels run by a replayed graph (negative: undo a capture's count)
 unsigned long long launch_count();
 
 }  // namespace orctm
