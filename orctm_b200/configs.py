@@ -147,11 +147,14 @@ def default_builder():
 
 
 def make_instance(name: str, index: int = 0, seed: int | None = None, builder=None,
-                  cfl: float | None = None, **over) -> dict:
+                  cfl: float | None = None, cfl_w="auto", **over) -> dict:
     """Raw inputs + geometry (via ``builder``) + a seeded initial state.
 
     ``cfl`` rescales the horizontal velocities to that Courant number (kernel
-    stress tests); by default velocities are O(0.1-0.3 m/s)."""
+    stress tests); by default velocities are O(0.1-0.3 m/s).  ``cfl_w`` caps
+    the vertical Courant number of the initial w (the scheme is stable below
+    1): by default at VERTICAL_CFL unless ``cfl`` is given; None leaves it
+    uncapped."""
     inst = raw_instance(name, index=index, seed=seed, **over)
     builder = builder or default_builder()
     depto, geo = builder(inst["ie"], inst["je"], inst["ke"], inst["dt"], inst["dzw"],
@@ -159,8 +162,12 @@ def make_instance(name: str, index: int = 0, seed: int | None = None, builder=No
                          inst["dlyu"], inst["dlxv"], inst["dlyv"])
     inst["depto"] = depto
     inst.update(geo)
-    inst.update(initial_state(inst, cfl=cfl))
+    inst.update(initial_state(inst, cfl=cfl, cfl_w=cfl_w))
     return inst
+
+
+# default cap on the vertical Courant number |w| dt / DDPO of initial states
+VERTICAL_CFL = 0.5
 
 
 def _wdiag(inst: dict, u: np.ndarray, v: np.ndarray) -> np.ndarray:
@@ -176,7 +183,12 @@ def _wdiag(inst: dict, u: np.ndarray, v: np.ndarray) -> np.ndarray:
     return w
 
 
-def initial_state(inst: dict, cfl: float | None = None) -> dict:
+def initial_state(inst: dict, cfl: float | None = None, cfl_w="auto") -> dict:
+    # cfl_w: cap on the vertical Courant number of the initial w; "auto" is
+    # 0.5 for workloads (many steps) and no cap for kernel stress cases that
+    # set a horizontal Courant number (single routine applications)
+    if cfl_w == "auto":
+        cfl_w = None if cfl is not None else VERTICAL_CFL
     g = rng(inst["seed"] + 7919)
     ie, je, ke, dt = inst["ie"], inst["je"], inst["ke"], inst["dt"]
     dx = float(inst["dlxp"][0, 0])
@@ -214,6 +226,23 @@ def initial_state(inst: dict, cfl: float | None = None) -> dict:
     u = np.asfortranarray(u * inst["amsuo"])
     v = np.asfortranarray(v * inst["amsue"])
     w = _wdiag(inst, u, v)
+    if cfl_w is not None:
+        # The smooth random (u, v) are not divergence-free, and w integrated
+        # from continuity over thousands of metres can reach tenths of m/s;
+        # across the thin upper layers that exceeds the limited advection's
+        # stability limit (vertical Courant number 1).  Scale (u, v) -- and
+        # with them w, which is linear in them -- so that |w| dt / DDPO stays
+        # below cfl_w on both cells of every interface.
+        d = inst["ddpo"]
+        thin = np.where(d > 0.0, d, np.inf)
+        lim = np.minimum(thin[:, :, :-1], thin[:, :, 1:])
+        cz = max(float((np.abs(w[:, :, 1:ke]) * dt / lim).max()),
+                 float((np.abs(w[:, :, 0]) * dt / thin[:, :, 0]).max()))
+        if cz > cfl_w:
+            s = cfl_w / cz
+            u = np.asfortranarray(u * s)
+            v = np.asfortranarray(v * s)
+            w = np.asfortranarray(w * s)
     # synthetic hydrostatic increment: the state one step before (drives the NH RHS)
     du = 1e-3 * smooth3((ie + 1, je, ke), 4.0) * inst["amsuo"]
     dv = 1e-3 * smooth3((ie, je + 1, ke), 4.0) * inst["amsue"]

@@ -1,5 +1,6 @@
 """Seeded synthetic instance generators.  CPU only."""
 import numpy as np
+import pytest
 
 import oracle as O
 from orctm_b200 import configs as C
@@ -52,3 +53,28 @@ def test_cfl_scaling():
     assert 0.3 < c <= 0.45 + 1e-12
     # velocities vanish on land faces
     assert np.all(inst["uoo"][inst["amsuo"] == 0] == 0)
+
+
+@pytest.mark.parametrize("name,over", [("c4", dict(nx=48, ny=40, nz=40)),
+                                       ("c2", dict(nx=30, ny=26, nz=20))])
+def test_initial_vertical_courant_number_capped(name, over):
+    inst = C.make_instance(name, builder=O.build_grid, **over)
+    w, d, dt, ke = inst["wno"], inst["ddpo"], inst["dt"], inst["ke"]
+    thin = np.where(d > 0.0, d, np.inf)
+    cz = (np.abs(w[:, :, 1:ke]) * dt / np.minimum(thin[:, :, :-1], thin[:, :, 1:])).max()
+    assert cz <= C.VERTICAL_CFL + 1e-12
+
+
+def test_workload_state_stays_bounded():
+    """Ten hot-path steps of a c4 member keep the tracers within their initial
+    range: the workload respects the scheme's stability limit (an uncapped
+    state of this member grew T by 1e3 per step)."""
+    inst = C.make_instance("c4", index=22, builder=O.build_grid, nx=40, ny=32, nz=30)
+    st = C.copy_state(inst)
+    lo, hi = st["tracers"][0][inst["weto"] > 0].min(), st["tracers"][0].max()
+    orc = O.Oracle(inst)
+    for _ in range(10):
+        orc.step_hotpath(st, solver="direct")
+    t = st["tracers"][0][inst["weto"] > 0]
+    assert np.isfinite(t).all()
+    assert t.max() <= hi + 1e-3 and t.min() >= lo - 1e-3
