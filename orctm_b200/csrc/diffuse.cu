@@ -255,7 +255,11 @@ __global__ void __launch_bounds__(64) k_visc_uv(Geo G, const double* __restrict_
   }
 }
 
-// implicit vertical diffusion of w, levels 2..KE (ocvisc.f90:225-270)
+// implicit vertical diffusion of w, levels 2..KE (ocvisc.f90:225-270).  One
+// forward sweep forms each level's coefficients, eliminates (the multiplier
+// TRIDSY(K-1,1)/TRIDSY(K-1,2) and the new diagonal, in the reference's
+// operation order) and substitutes; only the eliminated diagonal is kept per
+// level, and the backward sweep recomputes TRIDSY(K,3) by the same expression.
 __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __restrict__ avo,
                          double* __restrict__ O) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -268,42 +272,43 @@ __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __re
     return;
   }
   const long long ij = G.L.at2(i, j);
-  double t1[kMaxKe], t2[kMaxKe], t3[kMaxKe];
-  for (int K = 2; K <= KE - 1; ++K) {
+  auto den = [&](int K) {
+    return 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
+  };
+  auto tri1 = [&](int K, double dn) {
     const double avup = 0.5 * (AT(avo, i, j, K - 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K - 1);
-    const double avlo = 0.5 * (AT(avo, i, j, K + 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K);
-    const double den = 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
-    t1[K - 1] = div_nr(-2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2], den);
-    t3[K - 1] = div_nr(-2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1], den);
-    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
-  }
-  {
-    const int K = KE;
-    const double avup = 0.5 * (AT(avo, i, j, K - 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K - 1);
-    const double avlo = 0.0;
-    const double den = 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
-    t1[K - 1] = div_nr(-2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2], den);
-    t3[K - 1] = div_nr(-2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1], den);
-    t2[K - 1] = 1. - t1[K - 1] - t3[K - 1];
-    t3[K - 1] = 0.;
-  }
-  for (int K = 3; K <= KE; ++K) {
-    const double a = t1[K - 1];
-    t1[K - 2] = div_nr(a, t2[K - 2]);
-    t2[K - 1] = t2[K - 1] - div_nr(t3[K - 2] * a, t2[K - 2]);
-  }
+    return div_nr(-2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2], dn);
+  };
+  auto tri3 = [&](int K, double dn) {
+    const double avlo =
+        K < KE ? 0.5 * (AT(avo, i, j, K + 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K) : 0.0;
+    return div_nr(-2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1], dn);
+  };
+  double t2p[kMaxKe];
   AT(O, i, j, 1) = AT(W, i, j, 1);
   AT(O, i, j, KE + 1) = AT(W, i, j, KE + 1);
-  double prev = AT(W, i, j, 2);
-  AT(O, i, j, 2) = prev;
-  for (int K = 3; K <= KE; ++K) {
-    prev = AT(W, i, j, K) - t1[K - 2] * prev;
-    AT(O, i, j, K) = prev;
+  double prev = 0.0, t2prev = 1.0, t3prev = 0.0;
+  for (int K = 2; K <= KE; ++K) {
+    const double dn = den(K);
+    const double t1 = tri1(K, dn), t3 = tri3(K, dn);
+    double t2 = 1. - t1 - t3;
+    double y = AT(W, i, j, K);
+    if (K >= 3) {
+      const double m = div_nr(t1, t2prev);
+      t2 = t2 - div_nr(t3prev * t1, t2prev);
+      y = y - m * prev;
+    }
+    t2p[K - 1] = t2;
+    AT(O, i, j, K) = y;
+    prev = y;
+    t2prev = t2;
+    t3prev = K < KE ? t3 : 0.;
   }
-  double nxt = div_nr(wet(G.gp, ij, KE) * AT(O, i, j, KE), t2[KE - 1]);
+  double nxt = div_nr(wet(G.gp, ij, KE) * AT(O, i, j, KE), t2p[KE - 1]);
   AT(O, i, j, KE) = nxt;
   for (int K = KE - 1; K >= 2; --K) {
-    nxt = div_nr((AT(O, i, j, K) - t3[K - 1] * nxt) * wet(G.gp, ij, K), t2[K - 1]);
+    const double t3 = tri3(K, den(K));
+    nxt = div_nr((AT(O, i, j, K) - t3 * nxt) * wet(G.gp, ij, K), t2p[K - 1]);
     AT(O, i, j, K) = nxt;
   }
 }

@@ -605,6 +605,107 @@ __global__ void __launch_bounds__(32 * BY) k_pcg_spmv_l1(Geo G, PoissonGeo P, So
   }
 }
 
+// Warp-row form: a warp holds 32 consecutive columns of one row j and keeps
+// its own p of levels K-1, K, K+1 in registers; the west and east neighbours
+// come from the adjacent lanes by shuffle (the two edge lanes load theirs),
+// the north and south neighbours are formed from z and p_old of rows j-1 and
+// j+1 (shared with the neighbouring warps through L1).  No shared-memory tile
+// and no barrier in the level loop.  The arithmetic is that of the other
+// forms, so the results are the same bit for bit.
+template <typename T, int BY>
+__global__ void __launch_bounds__(32 * BY) k_pcg_spmv_wr(Geo G, PoissonGeo P, SolverState* S,
+                                                        const T* __restrict__ z,
+                                                        const T* __restrict__ pold,
+                                                        T* __restrict__ pnew, T* __restrict__ q,
+                                                        int first) {
+  __shared__ T szw[kMaxKe + 1], siz[kMaxKe];
+  if (S->converged) return;
+  const int KE = G.L.ke, IE = G.L.ie, JE = G.L.je;
+  const unsigned plane = (unsigned)G.L.plane, pitch = (unsigned)G.L.P;
+  const int lane = threadIdx.x, tid = threadIdx.x + 32 * threadIdx.y;
+  for (int e = tid; e <= KE; e += 32 * BY) {
+    szw[e] = (T)P.zwn[e];
+    if (e < KE) siz[e] = (T)P.izn[e];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * 32 + lane + 2, j = blockIdx.y * BY + threadIdx.y + 2;
+  const bool row_ok = j <= JE - 1;           // the same for the whole warp
+  const bool in_arr = row_ok && i <= IE;     // column i = IE holds zeros (not an unknown)
+  const bool act = row_ok && i <= IE - 1;
+  const T beta = first ? T(0) : (T)S->beta;
+  double pq = 0.0;
+  if (row_ok) {
+    ColC c;
+    T cw = 0, ce = 0, cn = 0, cs = 0, xyc = 0;
+    int kreg = 0;
+    if (act) {
+      c = load_col(G, P, i, j);
+      cw = c.iw ? (T)c.cw : T(0);
+      ce = c.ie ? (T)c.ce : T(0);
+      cn = c.in ? (T)c.cn : T(0);
+      cs = c.is ? (T)c.cs : T(0);
+      xyc = (T)(c.xcf + c.ycf);
+      kreg = c.kreg;
+    }
+    const unsigned o0 = in_arr ? (unsigned)G.L.at(i, j, 0) : 0u;
+    auto pv = [&](unsigned o) -> T { return first ? z[o] : fma(beta, pold[o], z[o]); };
+    T pu = T(0), p0 = in_arr ? pv(o0) : T(0);
+    T pqt = T(0);
+    for (int K = 1; K <= KE; ++K) {
+      const unsigned o = o0 + plane * (unsigned)(K - 1);
+      const T pd = (in_arr && K < KE) ? pv(o + plane) : T(0);
+      T pn = T(0), ps = T(0);
+      if (act) {
+        pn = pv(o - pitch);
+        ps = pv(o + pitch);
+      }
+      T pw = __shfl_up_sync(0xffffffffu, p0, 1);
+      T pe = __shfl_down_sync(0xffffffffu, p0, 1);
+      if (act && lane == 0) pw = pv(o - 1);
+      if (act && lane == 31) pe = pv(o + 1);
+      if (act) {
+        T s;
+        if (K >= 2 && K <= kreg) {
+          const T zw0 = szw[K - 1], zw1 = szw[K], hs = siz[K - 1];
+          T h = cw * pw;
+          h = fma(ce, pe, h);
+          h = fma(cn, pn, h);
+          h = fma(cs, ps, h);
+          h = fma(-xyc, p0, h);
+          s = zw0 * (pu - p0);
+          s = fma(zw1, pd - p0, s);
+          s = fma(hs, h, s);
+        } else {
+          const Coef rw = row<true>(c, P, K, KE);
+          s = (T)rw.dc * p0;
+          s = fma((T)rw.u, pu, s);
+          s = fma((T)rw.n, pn, s);
+          s = fma((T)rw.w, pw, s);
+          s = fma((T)rw.e, pe, s);
+          s = fma((T)rw.s, ps, s);
+          s = fma((T)rw.d, pd, s);
+        }
+        pnew[o] = p0;
+        q[o] = s;
+        pqt = fma(p0, s, pqt);
+        if ((K & 7) == 0) {
+          pq += (double)pqt;
+          pqt = T(0);
+        }
+      }
+      pu = p0;
+      p0 = pd;
+    }
+    pq += (double)pqt;
+  }
+  double v[1] = {pq};
+  if (grid_sum<1>(v, S)) {
+    S->pq = v[0];
+    S->alpha = S->rho / v[0];
+    if (!(v[0] > 0.0) && !(v[0] < 0.0)) S->converged = 3;  // breakdown
+  }
+}
+
 // r = b - A x with the exact FP64 entries of compute_matrix, accumulated in
 // double-double (products split exactly with an FMA), then rounded once; and
 // ||r||^2, ||b||^2.  This is the outer residual of the refinement loop and
@@ -797,8 +898,9 @@ template void launch_pcg_col<float, float>(const Geo&, const PoissonGeo&, Solver
                                            const float*, float*, int, cudaStream_t);
 
 // Variants of the stencil kernel: shared-memory ring with 32 x 8 or 32 x 4
-// tiles, or the barrier-free L1 form with 32 x 8 or 32 x 4 blocks.
-int pcg_spmv_variants() { return 4; }
+// tiles, the barrier-free L1 form, or the warp-row form, each with 32 x 8 or
+// 32 x 4 blocks.
+int pcg_spmv_variants() { return 6; }
 
 template <typename T>
 void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
@@ -815,6 +917,14 @@ void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T*
       break;
     case 3:
       k_pcg_spmv_l1<T, 4><<<grid2(nx, ny, dim3(32, 4)), dim3(32, 4), 0, st>>>(G, P, S, z, pold,
+                                                                               pnew, q, first);
+      break;
+    case 4:
+      k_pcg_spmv_wr<T, 8><<<grid2(nx, ny, dim3(32, 8)), dim3(32, 8), 0, st>>>(G, P, S, z, pold,
+                                                                               pnew, q, first);
+      break;
+    case 5:
+      k_pcg_spmv_wr<T, 4><<<grid2(nx, ny, dim3(32, 4)), dim3(32, 4), 0, st>>>(G, P, S, z, pold,
                                                                                pnew, q, first);
       break;
     default:
