@@ -42,6 +42,22 @@ BYTES_PER_CELL_F64 = {
 }
 
 
+METRIC = "cell-steps/s (hot path incl. Poisson solve @1e-10 rel. residual)"
+DATA = "synthetic (seeded PCG64, base seed 20261203; generators of BASELINE configs)"
+
+
+def workload_config(inst: dict) -> dict:
+    """The config object of the bench line (both arms)."""
+    cells = inst["nx"] * inst["ny"] * inst["nz"]
+    return {"workload": f"{inst['name']} {inst['nx']}x{inst['ny']}x{inst['nz']} "
+                        f"dt={inst['dt']:g}s, one instance per GPU",
+            "cells_per_gpu": cells, "tracers": inst["ntracers"],
+            "l2": "inputs larger than L2 (each 3D field "
+                  f"{8 * cells / 1e9:.2f} GB vs 126 MB L2)",
+            "solver": "FP64 PCG (line preconditioner, scaled operator) in "
+                      "double-double-residual refinement"}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -154,10 +170,12 @@ def workload(args, rank):
     return inst
 
 
-def cpu_sample(args, solver_rtol=1e-10):
+def cpu_sample(args, solver_rtol=1e-10, steps=None, warmup=1):
     """The CPU restatement (oracle) timed on the host cores on a bounded sample
-    of the same workload: one hot-path step of a sub-domain generated with the
-    same generators (same dx, dz, dt, bathymetry statistics)."""
+    of the same workload: hot-path steps of a sub-domain generated with the
+    same generators (same dx, dz, dt, bathymetry statistics).  With ``steps``
+    it times exactly that many after ``warmup`` untimed ones; otherwise it
+    runs for about ``args.cpu_seconds``."""
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -168,14 +186,18 @@ def cpu_sample(args, solver_rtol=1e-10):
     inst = configs.make_instance(args.config, builder=O.build_grid, nx=nx, ny=ny, nz=nz)
     orc = O.Oracle(inst)
     st = configs.copy_state(inst)
-    orc.step_hotpath(st, solver="fgmres", rtol=solver_rtol)  # warm-up (and warm start)
+    for _ in range(max(warmup, 1)):  # warm-up (and warm start)
+        orc.step_hotpath(st, solver="fgmres", rtol=solver_rtol)
     t0 = time.perf_counter()
+    target = steps
     steps = 0
-    solve_s = 0.0
     while True:
         info = orc.step_hotpath(st, solver="fgmres", rtol=solver_rtol)
         steps += 1
-        if time.perf_counter() - t0 > args.cpu_seconds or steps >= 50:
+        if target is not None:
+            if steps >= target:
+                break
+        elif time.perf_counter() - t0 > args.cpu_seconds or steps >= 50:
             break
     dt_ = time.perf_counter() - t0
     cells = nx * ny * nz
@@ -188,14 +210,25 @@ def cpu_sample(args, solver_rtol=1e-10):
 
 
 def run_reference(args, ws, rank, pg):
+    """The reference arm: the reference's Fortran/PETSc path cannot be built on
+    this image, so its CPU restatement (the oracle, OpenMP on every host core)
+    runs the same workload's generators on a bounded sub-domain, one hot-path
+    step per bench step (W untimed, K timed).  Rank 0 only."""
     if rank != 0:
         return 0
-    cb = cpu_sample(args)
-    line = {"impl": "reference", "metric": "cell-steps/s", "value": cb["value"],
+    from orctm_b200 import configs
+
+    over = {}
+    if args.size:
+        nx, ny, nz = (int(v) for v in args.size.split("x"))
+        over = {"nx": nx, "ny": ny, "nz": nz}
+    inst = configs.raw_instance(args.config, index=0, **over)
+    cb = cpu_sample(args, steps=args.steps, warmup=args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"],
             "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
-            "data": "synthetic (seeded PCG64, base seed 20261203)",
-            "config": {"workload": f"{args.config} hot path, CPU sample"},
+            "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": workload_config(inst),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -328,18 +361,12 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": "cell-steps/s (hot path incl. Poisson solve @1e-10 rel. residual)",
+            "metric": METRIC,
             "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded PCG64, base seed 20261203; generators of BASELINE configs)",
-            "config": {"workload": f"{args.config} {inst['nx']}x{inst['ny']}x{inst['nz']} "
-                                   f"dt={inst['dt']:g}s, one instance per GPU",
-                       "cells_per_gpu": cells, "tracers": inst["ntracers"],
-                       "l2": "inputs larger than L2 (each 3D field "
-                             f"{8 * cells / 1e9:.2f} GB vs 126 MB L2)",
-                       "solver": "FP64 PCG (line preconditioner, scaled operator) in "
-                                 "double-double-residual refinement"},
+            "data": DATA,
+            "config": workload_config(inst),
             "poisson_ms": poisson_ms, "poisson_iterations": iters, "relres_max": relres,
             "mixed": mixed, "solver_tuning": tuning, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": ck,
