@@ -78,7 +78,7 @@ __global__ void k_adpo_z(Geo G, const double* __restrict__ T, const double* __re
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   const double dlxp = G.dlxp[ij], dlyp = G.dlyp[ij];
   auto v0 = [&](int K) {
     double s = wet(G.gp, ij, K) * dlxp * dlyp * thick(G.gp, G.dzw, ij, K);
@@ -140,7 +140,7 @@ __device__ __forceinline__ Fl adpo_xflux(const Geo& G, const double* T, const do
                                          const double* uko, int q, int j, int K) {
   if (q < 2 || q > G.L.ie - 1) return zero_fl();
   const double u0 = AT(uko, q, j, K), um1 = AT(uko, q - 1, j, K);
-  const long long ij = G.L.at2(q, j), ijm = G.L.at2(q - 1, j);
+  const int ij = G.L.at2(q, j), ijm = G.L.at2(q - 1, j);
   const double up = 0.5 * G.dt * thick(G.gu, G.dzw, ij, K) * G.dlyu[ij] * (u0 + fabs(u0));
   const double um = 0.5 * G.dt * thick(G.gu, G.dzw, ijm, K) * (fabs(um1) - um1) * G.dlyu[ijm];
   // SCHA = MAX(...)*WETO(I)*WETO(I+1)*WETO(I-1), factors applied in that order
@@ -162,7 +162,7 @@ __device__ __forceinline__ Fl adpo_xflux(const Geo& G, const double* T, const do
 __device__ __forceinline__ Fl adpo_yflux(const Geo& G, const double* T, const double* V,
                                          const double* vke, int i, int q, int K) {
   if (q < 2 || q > G.L.je - 1) return zero_fl();
-  const long long ijn = G.L.at2(i, q - 1), ij = G.L.at2(i, q);
+  const int ijn = G.L.at2(i, q - 1), ij = G.L.at2(i, q);
   const double vn = AT(vke, i, q - 1, K), vs = AT(vke, i, q, K);
   const double up = 0.5 * G.dt * thick(G.gv, G.dzw, ijn, K) * G.dlxv[ijn] * (vn + fabs(vn));
   const double um = 0.5 * G.dt * thick(G.gv, G.dzw, ij, K) * G.dlxv[ij] * (fabs(vs) - vs);
@@ -190,7 +190,7 @@ __global__ void k_uad_z(Geo G, const double* __restrict__ T, const double* __res
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   auto v0 = [&](int K) {
     return wet(G.gu, ij, K) * G.dlxu[ij] * G.dlyu[ij] * thick(G.gu, G.dzw, ij, K);
   };
@@ -202,7 +202,7 @@ __global__ void k_uad_z(Geo G, const double* __restrict__ T, const double* __res
     }
     return;
   }
-  const long long ijp = G.L.at2(i, j);
+  const int ijp = G.L.at2(i, j);
   const double cdt = 0.5 * G.dt * G.dlyp[ijp] * G.dlxp[ijp];
   auto flux = [&](int K, double vol) {
     const int klo = K + 1 < KE ? K + 1 : KE;
@@ -290,7 +290,7 @@ __global__ void k_vad_z(Geo G, const double* __restrict__ T, const double* __res
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   auto v0 = [&](int K) {
     return wet(G.gv, ij, K) * G.dlxv[ij] * G.dlyv[ij] * thick(G.gv, G.dzw, ij, K);
   };
@@ -392,7 +392,7 @@ __global__ void k_wad_z(Geo G, const double* __restrict__ T, const double* __res
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   const double dlxp = G.dlxp[ij], dlyp = G.dlyp[ij];
   auto v0 = [&](int K) {
     const double a = wet(G.gp, ij, K) * dlxp * dlyp;
@@ -516,7 +516,7 @@ __device__ __forceinline__ Fl face(const Geo& G, const double* T, const double* 
 }
 
 template <int VAR>
-__device__ __forceinline__ bool wet_var(const Geo& G, long long ij, int K) {
+__device__ __forceinline__ bool wet_var(const Geo& G, int ij, int K) {
   if (VAR == V_UAD) return wetb(G.gu, ij, K);
   if (VAR == V_VAD) return wetb(G.gv, ij, K);
   return wetb(G.gp, ij, K);

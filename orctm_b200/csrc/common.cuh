@@ -27,12 +27,13 @@ constexpr int kMaxKe = 320;  // longest column a handle accepts (the reference r
 struct Layout {
   int ie, je, ke;   // IE, JE, KE (halos included)
   int P, JN;        // pitch (elements) and rows per level
-  long long plane;  // P * JN
-  __host__ __device__ long long at(int i, int j, int l) const {
-    return (long long)i + (long long)P * ((long long)j + (long long)JN * (long long)l);
-  }
-  __host__ __device__ long long at2(int i, int j) const { return (long long)i + (long long)P * j; }
-  __host__ __device__ long long n3() const { return plane * (ke + 1); }
+  // Offsets are 32-bit: orctm_create rejects a padded field of 2^31 elements
+  // or more, so every offset (and the small negative ones a stencil forms at
+  // an array's edge, which land in the allocation's guard zone) fits an int.
+  int plane;  // P * JN
+  __host__ __device__ int at(int i, int j, int l) const { return i + P * (j + JN * l); }
+  __host__ __device__ int at2(int i, int j) const { return i + P * j; }
+  __host__ __device__ long long n3() const { return (long long)plane * (ke + 1); }
 };
 
 // Compressed column geometry of one staggering (p, u or v points).
@@ -71,14 +72,14 @@ struct Geo {
   const double *rareau, *rareav, *rareap;
 };
 
-__device__ __forceinline__ double thick(const ColGeo& c, const double* dzw, long long ij, int K) {
+__device__ __forceinline__ double thick(const ColGeo& c, const double* dzw, int ij, int K) {
   const int kb = c.kb[ij];
   return K < kb ? dzw[K - 1] : (K == kb ? c.bot[ij] : 0.0);
 }
-__device__ __forceinline__ double wet(const ColGeo& c, long long ij, int K) {
+__device__ __forceinline__ double wet(const ColGeo& c, int ij, int K) {
   return K <= c.kb[ij] ? 1.0 : 0.0;
 }
-__device__ __forceinline__ bool wetb(const ColGeo& c, long long ij, int K) { return K <= c.kb[ij]; }
+__device__ __forceinline__ bool wetb(const ColGeo& c, int ij, int K) { return K <= c.kb[ij]; }
 
 // a / b by Newton-Raphson refinement of a hardware reciprocal estimate
 // (rcp.approx.ftz.f64), two iterations r <- r + r (1 - b r), then one

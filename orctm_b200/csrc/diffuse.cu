@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(64) k_tdiff_vert(Geo G, TrPtrs tp, int ntr,
       for (int K = 1; K <= KE; ++K) AT(tp.out[n], i, j, K) = AT(tp.in[n], i, j, K);
     return;
   }
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   const double zij = zo[ij];
   // TRIDSY(K,1..3) of octdiff_base.f90:188-194; only the eliminated diagonal
   // is kept per level, TRIDSY(K,3) is recomputed by the same expression
@@ -132,7 +132,7 @@ __global__ void k_tdiff_bih(Geo G, const double* __restrict__ T, const double* _
   double r = t;
   if (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
     auto w = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
-    const long long ij = G.L.at2(i, j);
+    const int ij = G.L.at2(i, j);
     const double zzsurf = K == 1 ? 1. : 0.;
     const double c = AT(L1, i, j, K);
     // W / ((DDPO + ALMZER + ZZSURF ZO) DLXP DLYP) with 1/(DLXP DLYP) precomputed;
@@ -157,7 +157,7 @@ __global__ void k_visc_speed(Geo G, const double* __restrict__ uoo, const double
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int IE = G.L.ie, JE = G.L.je;
   if (i > IE || j > JE) return;
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   double su = 0., sv = 0.;
   if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
     const int K = G.gu.kb[ij];
@@ -202,11 +202,11 @@ __global__ void __launch_bounds__(64) k_visc_uv(Geo G, const double* __restrict_
     return;
   }
   const ColGeo& cg = DIR == 0 ? G.gu : G.gv;
-  const long long ij = G.L.at2(i, j);
-  const long long ij2 = DIR == 0 ? G.L.at2(i + 1, j) : G.L.at2(i, j + 1);
+  const int ij = G.L.at2(i, j);
+  const int ij2 = DIR == 0 ? G.L.at2(i + 1, j) : G.L.at2(i, j + 1);
   const double BOFRIC = 3.E-3, RAYFRIC = 3.E-3;
   const double sp = speed[ij];
-  auto avo_at = [&](long long q, int K) { return avo[q + G.L.plane * (K - 1)]; };
+  auto avo_at = [&](int q, int K) { return avo[q + G.L.plane * (K - 1)]; };
   // TRIDSY(K,1) and TRIDSY(K,3) (after the AMS(K+1) factor) of
   // ocvisc.f90:117-140 / 171-193
   auto tri = [&](int K, double& t1, double& t3) {
@@ -271,7 +271,7 @@ __global__ void k_visc_w(Geo G, const double* __restrict__ W, const double* __re
     for (int K = 1; K <= KE + 1; ++K) AT(O, i, j, K) = AT(W, i, j, K);
     return;
   }
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   auto den = [&](int K) {
     return 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
   };
@@ -455,7 +455,7 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
         auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
         auto U1 = [&](int ii, int jj) { return AT(u1, ii, jj, K); };
-        const long long ij = G.L.at2(i, j);
+        const int ij = G.L.at2(i, j);
         r = (AO(i, j) * G.rareau[ij]) *
             (G.dlxu[ij] * G.dlyu[ij] * AT(uk, i, j, K) -
              (G.ugx[G.L.at2(i + 1, j)] * AO(i + 1, j) * (U1(i + 1, j) - U1(i, j)) -
@@ -471,7 +471,7 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
         auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
         auto V1 = [&](int ii, int jj) { return AT(v1, ii, jj, K); };
-        const long long ij = G.L.at2(i, j);
+        const int ij = G.L.at2(i, j);
         r = (AE(i, j) * G.rareav[ij]) *
             (G.dlxv[ij] * G.dlyv[ij] * AT(vk, i, j, K) -
              (G.vgx[ij] * AE(i + 1, j) * (V1(i + 1, j) - V1(i, j)) -
@@ -490,7 +490,7 @@ __global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* 
       auto W1 = [&](int ii, int jj) { return AT(w1, ii, jj, K); };
       auto dzu = [&](int ii, int jj) { return fmx(thick(G.gu, G.dzw, G.L.at2(ii, jj), K), mv); };
       auto dzv = [&](int ii, int jj) { return fmx(thick(G.gv, G.dzw, G.L.at2(ii, jj), K), mv); };
-      const long long ij = G.L.at2(i, j);
+      const int ij = G.L.at2(i, j);
       const double dzp = fmx(thick(G.gp, G.dzw, ij, K), mv);
       r = div_nr(WE(i, j) * G.rareap[ij], dzp) *
           (G.dlxp[ij] * G.dlyp[ij] * dzp * AT(wn, i, j, K) -

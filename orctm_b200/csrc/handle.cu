@@ -362,7 +362,7 @@ int setup(orctm_handle* h, const orctm_desc* d) {
   L.ie = IE; L.je = JE; L.ke = KE;
   L.P = ((IE + 1) + 31) / 32 * 32;
   L.JN = JE + 1;
-  L.plane = (long long)L.P * L.JN;
+  L.plane = L.P * L.JN;  // below 2^31: checked by orctm_create
   h->ntr = d->ntracers;
   Geo& G = h->G;
   G.L = L;
@@ -1153,7 +1153,7 @@ int orctm_create(const orctm_desc* d, orctm_handle** out) {
   };
   if (d->ie < 4 || d->je < 3 || d->ke < 2 || d->ke > kMaxKe) return bad(ORCTM_E_ARG, "grid size out of range");
   {
-    // the solver kernels index a padded field with 32-bit offsets
+    // the kernels index a padded field with 32-bit offsets
     const long long pitch = ((long long)d->ie + 1 + 31) / 32 * 32;
     if (pitch * ((long long)d->je + 1) * ((long long)d->ke + 1) >= (1LL << 31))
       return bad(ORCTM_E_TOO_LARGE, "padded field exceeds 2^31 elements");

@@ -32,7 +32,7 @@ __global__ void k_nh_rhs(Geo G, const double* __restrict__ uoo, const double* __
   const int IE = G.L.ie, JE = G.L.je;
   if (i > IE - 1 || j > JE - 1) return;
   const double DT = G.dt;
-  const long long ij = G.L.at2(i, j);
+  const int ij = G.L.at2(i, j);
   const double gu0 = (AT(uoo, i, j, K) - AT(uoo1, i, j, K)) / DT;
   const double gum = (AT(uoo, i - 1, j, K) - AT(uoo1, i - 1, j, K)) / DT;
   const double divgu = (gu0 - gum) / G.dlxp[ij];
@@ -88,7 +88,7 @@ __global__ void k_nh_uv(Geo G, const double* __restrict__ pnh, const double* __r
   if (j >= 1) {
     double u = AT(uoo, i, j, K);
     if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
-      const long long ij = G.L.at2(i, j);
+      const int ij = G.L.at2(i, j);
       u = u + wet(G.gu, ij, K) * G.dtdxuo[ij] * (AT(pnh, i, j, K) - AT(pnh, i + 1, j, K));
     }
     AT(uo, i, j, K) = u;
@@ -96,7 +96,7 @@ __global__ void k_nh_uv(Geo G, const double* __restrict__ pnh, const double* __r
   if (i >= 1) {
     double v = AT(voe, i, j, K);
     if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
-      const long long ij = G.L.at2(i, j);
+      const int ij = G.L.at2(i, j);
       v = v + wet(G.gv, ij, K) * G.dpye[ij] * (AT(pnh, i, j + 1, K) - AT(pnh, i, j, K));
     }
     AT(vo, i, j, K) = v;
@@ -110,7 +110,7 @@ __global__ void k_nh_w(Geo G, const double* __restrict__ uoo, const double* __re
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const long long ij = G.L.at2(i, j), ijw = G.L.at2(i - 1, j), ijn = G.L.at2(i, j - 1);
+  const int ij = G.L.at2(i, j), ijw = G.L.at2(i - 1, j), ijn = G.L.at2(i, j - 1);
   double w = 0.0;
   AT(wno, i, j, KE + 1) = 0.0;
   for (int K = KE; K >= 1; --K) {

@@ -50,7 +50,7 @@ struct Coef {
 
 // 2D data of one column (i, j), i in [2, IE-1], j in [2, JE-1]
 struct ColC {
-  long long ij;
+  int ij;
   int kb, kbw, kbe, kbn, kbs;
   int kreg;                            // levels 2..kreg have the regular (all-wet) row
   bool iw, ie, in, is;                 // couplings the DMDA allows (not at the domain edge)
