@@ -138,6 +138,11 @@ int orctm_ocuad(orctm_handle* h);
 int orctm_ocvad(orctm_handle* h);
 int orctm_ocwad(orctm_handle* h);
 int orctm_ocadpo(orctm_handle* h, int tracer);
+/* OCADPO for every tracer of the handle in one call: the driver calls OCADPO
+ * once per tracer with unchanged velocities (orctm.f90:1459-1460), so the
+ * transports and volumes are formed once and shared; the results equal one
+ * orctm_ocadpo call per tracer, bit for bit.  orctm_step_hotpath uses it. */
+int orctm_ocadpo_all(orctm_handle* h);
 int orctm_octdiff(orctm_handle* h);
 int orctm_octimf(orctm_handle* h);
 int orctm_ocvisc(orctm_handle* h);

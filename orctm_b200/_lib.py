@@ -61,7 +61,7 @@ EXPORTS = (
     "orctm_trim_device_memory", "orctm_set_tuning", "orctm_get_tuning",
     "orctm_serve_create", "orctm_serve_submit", "orctm_serve_wait", "orctm_serve_poll",
     "orctm_serve_drain", "orctm_serve_get_stats", "orctm_serve_destroy", "orctm_batch_run",
-    "orctm_estimate_device_bytes", "orctm_check_division",
+    "orctm_estimate_device_bytes", "orctm_check_division", "orctm_ocadpo_all",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -87,7 +87,7 @@ def load(build_if_missing: bool = True):
     lib.orctm_last_error.argtypes = [C.c_void_p]
     lib.orctm_create.argtypes = [C.POINTER(Desc), C.POINTER(C.c_void_p)]
     for name in ("orctm_destroy", "orctm_ocuad", "orctm_ocvad", "orctm_ocwad", "orctm_octdiff",
-                 "orctm_octimf", "orctm_ocvisc", "orctm_synchronize"):
+                 "orctm_octimf", "orctm_ocvisc", "orctm_synchronize", "orctm_ocadpo_all"):
         getattr(lib, name).argtypes = [C.c_void_p]
     lib.orctm_ocadpo.argtypes = [C.c_void_p, C.c_int]
     lib.orctm_ocvtot_nh.argtypes = [C.c_void_p, C.POINTER(SolveStats)]

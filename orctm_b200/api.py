@@ -139,6 +139,10 @@ class Instance:
     def ocadpo(self, tracer: int):
         _lib.check(self.lib.orctm_ocadpo(self.h, tracer), self.h)
 
+    def ocadpo_all(self):
+        """OCADPO for every tracer at once (shared transports and volumes)."""
+        _lib.check(self.lib.orctm_ocadpo_all(self.h), self.h)
+
     def octdiff(self):
         _lib.check(self.lib.orctm_octdiff(self.h), self.h)
 

@@ -567,6 +567,209 @@ __global__ void __launch_bounds__(kSx * kSy) k_hsweep(Geo G, const double* __res
   if (Vo && hasv) AT(Vo, i, j, K) = vn;
 }
 
+// ---------------------------------------------------- OCADPO, all tracers ---
+// The driver calls OCADPO once per tracer with unchanged velocities
+// (orctm.f90:1459-1460 and the passive tracers after them).  The transports
+// WTP/WTM, the volumes RN and the geometry factors depend on the velocities
+// and the geometry only, so these sweeps form them once and advect up to
+// kMaxFused tracers with them.  Each tracer's arithmetic is, expression for
+// expression, that of k_adpo_z, adpo_xflux / adpo_yflux and apply, so the
+// results equal separate OCADPO calls bit for bit.
+constexpr int kMaxFused = 4;
+
+struct TrIO {
+  const double* in[kMaxFused];
+  double* out[kMaxFused];
+};
+
+template <int NT>
+struct FlN {
+  double wtp, wtm;
+  double trp[NT], trm[NT];
+};
+
+template <int NT>
+__device__ __forceinline__ FlN<NT> zero_fln() {
+  FlN<NT> f;
+  f.wtp = f.wtm = 0.;
+#pragma unroll
+  for (int n = 0; n < NT; ++n) f.trp[n] = f.trm[n] = 0.;
+  return f;
+}
+
+template <int NT>
+__device__ __forceinline__ Fl pick(const FlN<NT>& f, int n) {
+  return Fl{f.trp[n], f.trm[n], f.wtp, f.wtm};
+}
+
+template <int NT>
+__global__ void k_adpo_z_all(Geo G, TrIO io, const double* __restrict__ wo,
+                             const double* __restrict__ zo, double* __restrict__ Vo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const int ij = G.L.at2(i, j);
+  const double dlxp = G.dlxp[ij], dlyp = G.dlyp[ij];
+  auto v0 = [&](int K) {
+    double s = wet(G.gp, ij, K) * dlxp * dlyp * thick(G.gp, G.dzw, ij, K);
+    if (K == 1) s = s + dlxp * dlyp * wet(G.gp, ij, 1) * (zo[ij] - AT(wo, i, j, 1) * G.dt);
+    return s;
+  };
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1;
+  if (!interior) {
+    for (int K = 1; K <= KE; ++K) {
+#pragma unroll
+      for (int n = 0; n < NT; ++n) AT(io.out[n], i, j, K) = AT(io.in[n], i, j, K);
+      AT(Vo, i, j, K) = v0(K);
+    }
+    return;
+  }
+  const double cdt = 0.5 * G.dt * dlyp * dlxp;
+  auto flux = [&](int K, double vol) {
+    const int klo = K + 1 < KE ? K + 1 : KE;
+    const int kup = K - 1 > 1 ? K - 1 : 1;
+    const double w0 = AT(wo, i, j, K), w1 = AT(wo, i, j, K + 1);
+    const double up = cdt * (w0 + fabs(w0));
+    const double um = cdt * (fabs(w1) - w1);
+    const double cap = wet(G.gp, ij, klo);
+    FlN<NT> f;
+    f.wtp = up;
+    f.wtm = um;
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+      const double* T = io.in[n];
+      const double t = AT(T, i, j, K), tu = AT(T, i, j, kup), tl = AT(T, i, j, klo);
+      const double abl = fabs(tu - tl);
+      const double zwabl = fabs(tu + tl - 2. * t);
+      const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20));
+      double sch = fmn(cap, div_nr(scha * vol, up + um + 1.E-20));
+      if (K == 1 || K == KE) sch = 0.;
+      const double schi = 1. - sch;
+      f.trp[n] = up * (schi * t + sch * 0.5 * (t + tu));
+      f.trm[n] = um * (schi * t + sch * 0.5 * (t + tl));
+    }
+    return f;
+  };
+  FlN<NT> fm = zero_fln<NT>();
+  double vk = v0(1);
+  FlN<NT> fc = flux(1, vk);
+  for (int K = 1; K <= KE; ++K) {
+    double vn = 0.;
+    FlN<NT> fp = zero_fln<NT>();
+    if (K < KE) {
+      vn = v0(K + 1);
+      fp = flux(K + 1, vn);
+    }
+    const bool w = wetb(G.gp, ij, K);
+    double vv = vk;
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+      const double t = AT(io.in[n], i, j, K);
+      double tn = t, vt = vk;
+      if (w) apply_z(t, vk, pick(fm, n), pick(fc, n), pick(fp, n), tn, vt);
+      AT(io.out[n], i, j, K) = tn;
+      vv = vt;
+    }
+    AT(Vo, i, j, K) = vv;
+    fm = fc;
+    fc = fp;
+    vk = vn;
+  }
+}
+
+// the face transports of adpo_xflux (DIR 0) / adpo_yflux (DIR 1) for NT tracers
+template <int NT, int DIR>
+__device__ __forceinline__ FlN<NT> adpo_face_all(const Geo& G, const TrIO& io,
+                                                 const double* V, const double* vel, int qi,
+                                                 int qj, int K) {
+  const int q = DIR == 0 ? qi : qj;
+  const int qmax = DIR == 0 ? G.L.ie - 1 : G.L.je - 1;
+  if (q < 2 || q > qmax) return zero_fln<NT>();
+  const int i = qi, j = qj;
+  double up, um;
+  int ij, ijp, ijm;  // the cell, its neighbour in +DIR and in -DIR
+  if (DIR == 0) {
+    const double u0 = AT(vel, q, j, K), um1 = AT(vel, q - 1, j, K);
+    ij = G.L.at2(q, j);
+    ijm = G.L.at2(q - 1, j);
+    ijp = G.L.at2(q + 1, j);
+    up = 0.5 * G.dt * thick(G.gu, G.dzw, ij, K) * G.dlyu[ij] * (u0 + fabs(u0));
+    um = 0.5 * G.dt * thick(G.gu, G.dzw, ijm, K) * (fabs(um1) - um1) * G.dlyu[ijm];
+  } else {
+    const int ijn = G.L.at2(i, q - 1);
+    ij = G.L.at2(i, q);
+    const double vn = AT(vel, i, q - 1, K), vs = AT(vel, i, q, K);
+    up = 0.5 * G.dt * thick(G.gv, G.dzw, ijn, K) * G.dlxv[ijn] * (vn + fabs(vn));
+    um = 0.5 * G.dt * thick(G.gv, G.dzw, ij, K) * G.dlxv[ij] * (fabs(vs) - vs);
+    ijp = G.L.at2(i, q - 1);  // factor order of adpo_yflux: WETO(J), WETO(J-1), WETO(J+1)
+    ijm = G.L.at2(i, q + 1);
+  }
+  const double w1 = wet(G.gp, ij, K), w2 = wet(G.gp, ijp, K), w3 = wet(G.gp, ijm, K);
+  const double vol = AT(V, i, j, K);
+  FlN<NT> f;
+  f.wtp = up;
+  f.wtm = um;
+#pragma unroll
+  for (int n = 0; n < NT; ++n) {
+    const double* T = io.in[n];
+    // x: t, east, west (TRP uses the east value); y: t, north (q-1), south (q+1)
+    const double t = AT(T, i, j, K);
+    const double ta = DIR == 0 ? AT(T, q + 1, j, K) : AT(T, i, q - 1, K);
+    const double tb = DIR == 0 ? AT(T, q - 1, j, K) : AT(T, i, q + 1, K);
+    const double abl = fabs(ta - tb);
+    const double zwabl = fabs(ta + tb - 2. * t);
+    const double scha = fmx(0., div_nr(abl - zwabl, abl + 1.E-20)) * w1 * w2 * w3;
+    const double sch = fmn(1., div_nr(scha * vol, up + um + 1.E-20));
+    const double schi = 1. - sch;
+    f.trp[n] = up * (schi * t + sch * 0.5 * (t + ta));
+    f.trm[n] = um * (schi * t + sch * 0.5 * (t + tb));
+  }
+  return f;
+}
+
+template <int NT, int DIR>
+__global__ void __launch_bounds__(kSx * kSy) k_hsweep_adpo_all(Geo G, TrIO io,
+                                                               const double* __restrict__ V,
+                                                               const double* __restrict__ vel,
+                                                               double* __restrict__ Vo) {
+  using R = Rng<V_ADPO>;
+  constexpr int HX = DIR == 0 ? kSx + 2 : kSx, HY = DIR == 0 ? kSy : kSy + 2;
+  __shared__ FlN<NT> fl[HY][HX];
+  const int IE = G.L.ie, JE = G.L.je;
+  const int K = blockIdx.z + 1;
+  const int ib = blockIdx.x * kSx + R::i0, jb = blockIdx.y * kSy + R::j0;
+  const int iLo = R::iL, iHi = IE - R::iH, jLo = R::jL, jHi = JE - R::jH;
+  const int tid = threadIdx.x + kSx * threadIdx.y;
+  for (int e = tid; e < HX * HY; e += kSx * kSy) {
+    const int hy = e / HX, hx = e - hy * HX;
+    const int qi = ib + hx - (DIR == 0), qj = jb + hy - (DIR == 1);
+    const bool need = DIR == 0 ? (qj >= jLo && qj <= jHi) : (qi >= iLo && qi <= iHi);
+    fl[hy][hx] = need ? adpo_face_all<NT, DIR>(G, io, V, vel, qi, qj, K) : zero_fln<NT>();
+  }
+  __syncthreads();
+  const int i = ib + threadIdx.x, j = jb + threadIdx.y;
+  if (i > IE || j > JE) return;
+  const double v = AT(V, i, j, K);
+  double vn = v;
+  const bool upd = i >= iLo && i <= iHi && j >= jLo && j <= jHi && wetb(G.gp, G.L.at2(i, j), K);
+  const int hx = threadIdx.x + (DIR == 0), hy = threadIdx.y + (DIR == 1);
+#pragma unroll
+  for (int n = 0; n < NT; ++n) {
+    const double t = AT(io.in[n], i, j, K);
+    double tn = t, vt = v;
+    if (upd) {
+      if (DIR == 0)  // RN = V + WTP(I-1) - WTP(I) - WTM(I) + WTM(I+1)
+        apply(t, v, pick(fl[hy][hx - 1], n), pick(fl[hy][hx], n), pick(fl[hy][hx + 1], n), tn, vt);
+      else           // RN = V + WTP(J+1) - WTP(J) - WTM(J) + WTM(J-1)
+        apply(t, v, pick(fl[hy + 1][hx], n), pick(fl[hy][hx], n), pick(fl[hy - 1][hx], n), tn, vt);
+    }
+    AT(io.out[n], i, j, K) = tn;
+    vn = vt;
+  }
+  if (Vo) AT(Vo, i, j, K) = vn;
+}
+
 inline dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, 1); }
 inline dim3 grid3(int nx, int ny, int nz, dim3 b) {
   return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz);
@@ -587,6 +790,51 @@ void launch_ocadpo(const Geo& G, const double* T, const double* uko, const doubl
   count_launch();
   k_hsweep<V_ADPO, 1><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
+}
+
+namespace {
+template <int NT>
+void adpo_all_group(const Geo& G, TrIO zio, TrIO xio, TrIO yio, const double* uko,
+                    const double* vke, const double* wo, const double* zo, double* vA, double* vB,
+                    cudaStream_t st) {
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const dim3 bc(32, 4);
+  k_adpo_z_all<NT><<<grid2(IE, JE, bc), bc, 0, st>>>(G, zio, wo, zo, vA);
+  count_launch();
+  const dim3 bs(kSx, kSy);
+  k_hsweep_adpo_all<NT, 0><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, xio, vA, uko, vB);
+  count_launch();
+  k_hsweep_adpo_all<NT, 1><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, yio, vB, vke, nullptr);
+  count_launch();
+}
+}  // namespace
+
+int adpo_max_fused() { return kMaxFused; }
+
+// ntr tracers T[n] -> out[n] through the z, x and y sweeps, kMaxFused at a
+// time; mid[n]: the x-sweep outputs; vA, vB: scratch volumes
+void launch_ocadpo_all(const Geo& G, int ntr, const double* const* T, double* const* out,
+                       double* const* mid, const double* uko, const double* vke,
+                       const double* wo, const double* zo, double* vA, double* vB,
+                       cudaStream_t st) {
+  for (int n0 = 0; n0 < ntr; n0 += kMaxFused) {
+    const int nt = ntr - n0 < kMaxFused ? ntr - n0 : kMaxFused;
+    TrIO zio{}, xio{}, yio{};
+    for (int n = 0; n < nt; ++n) {
+      zio.in[n] = T[n0 + n];
+      zio.out[n] = out[n0 + n];
+      xio.in[n] = out[n0 + n];
+      xio.out[n] = mid[n0 + n];
+      yio.in[n] = mid[n0 + n];
+      yio.out[n] = out[n0 + n];
+    }
+    switch (nt) {
+      case 1: adpo_all_group<1>(G, zio, xio, yio, uko, vke, wo, zo, vA, vB, st); break;
+      case 2: adpo_all_group<2>(G, zio, xio, yio, uko, vke, wo, zo, vA, vB, st); break;
+      case 3: adpo_all_group<3>(G, zio, xio, yio, uko, vke, wo, zo, vA, vB, st); break;
+      default: adpo_all_group<4>(G, zio, xio, yio, uko, vke, wo, zo, vA, vB, st); break;
+    }
+  }
 }
 
 void launch_ocuad(const Geo& G, const double* T, const double* uko, const double* vke,

@@ -947,6 +947,32 @@ int r_ocadpo(orctm_handle* h, int n) {
   return ORCTM_OK;
 }
 
+// OCADPO for every tracer: one set of sweeps per group of tracers shares the
+// transports and volumes (launch_ocadpo_all); the same results as r_ocadpo
+// tracer by tracer
+int r_ocadpo_all(orctm_handle* h) {
+  int st;
+  const int ntr = h->ntr;
+  double *out[kMaxTracers] = {}, *mid[kMaxTracers] = {}, *vA = nullptr, *vB = nullptr;
+  const double* in[kMaxTracers] = {};
+  for (int n = 0; n < ntr; ++n) {
+    if ((st = h->alloc(&out[n])) || (st = h->alloc(&mid[n]))) return st;
+    in[n] = h->slot[ORCTM_F_THO + n];
+  }
+  if ((st = h->alloc(&vA)) || (st = h->alloc(&vB))) return st;
+  PROF(h, ORCTM_PROF_OCADPO,
+       launch_ocadpo_all(h->G, ntr, in, out, mid, h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE],
+                         h->slot[ORCTM_F_WO], h->zo, vA, vB, h->stream));
+  ORCTM_CUDA_OK(cudaGetLastError());
+  for (int n = 0; n < ntr; ++n) {
+    h->bind(ORCTM_F_THO + n, out[n]);
+    h->unref(mid[n]);
+  }
+  h->unref(vA);
+  h->unref(vB);
+  return ORCTM_OK;
+}
+
 template <int WHICH>
 int r_momadv(orctm_handle* h) {
   int st;
@@ -1246,6 +1272,11 @@ int orctm_ocadpo(orctm_handle* h, int tracer) {
   if (tracer < 0 || tracer >= h->ntr) return ORCTM_E_ARG;
   return r_ocadpo(h, tracer);
 }
+
+int orctm_ocadpo_all(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  return r_ocadpo_all(h);
+}
 int orctm_octdiff(orctm_handle* h) { ORCTM_ENTER(h); return r_octdiff(h); }
 int orctm_octimf(orctm_handle* h) { ORCTM_ENTER(h); return r_octimf(h); }
 int orctm_ocvisc(orctm_handle* h) { ORCTM_ENTER(h); return r_ocvisc(h); }
@@ -1255,8 +1286,7 @@ int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* s) {
   ORCTM_ENTER(h);
   int st;
   if ((st = r_momadv<0>(h)) || (st = r_momadv<1>(h)) || (st = r_momadv<2>(h))) return st;
-  for (int n = 0; n < h->ntr; ++n)
-    if ((st = r_ocadpo(h, n))) return st;
+  if ((st = r_ocadpo_all(h))) return st;  // OCADPO(THO), OCADPO(SAO), passive tracers
   if ((st = r_octdiff(h)) || (st = r_octimf(h)) || (st = r_ocvisc(h))) return st;
   const int ns = r_ocvtot_nh(h, s);
   if (ns != ORCTM_OK && ns != ORCTM_E_NOT_CONVERGED) return ns;
@@ -1347,10 +1377,12 @@ int orctm_estimate_device_bytes(const orctm_desc* d, int solver, unsigned long l
   if (!d || !bytes || d->ie < 4 || d->je < 3 || d->ke < 2 || d->ntracers < 2) return ORCTM_E_ARG;
   const double P = (double)(((long long)d->ie + 1 + 31) / 32 * 32);
   const double plane = P * (d->je + 1), n3 = plane * (d->ke + 1);
-  // 3D buffers: 12 state fields and the tracers, up to 8 routine temporaries
-  // of the field pool, 9 FP64 solver vectors, the FP64 + FP32 pivots, and 7
+  // 3D buffers: 12 state fields and the tracers, the routine temporaries of
+  // the field pool (at most max(8, 2 ntracers + 2), the advection of all
+  // tracers at once), 9 FP64 solver vectors, the FP64 + FP32 pivots, and 7
   // FP32 vectors for the refined solver
-  const double f3 = 12.0 + d->ntracers + 8.0 + 9.0 + 1.5 +
+  const double tmp = std::max(8.0, 2.0 * d->ntracers + 2.0);
+  const double f3 = 12.0 + d->ntracers + tmp + 9.0 + 1.5 +
                     (solver == ORCTM_SOLVER_FP32_REFINED ? 3.5 : 0.0);
   // 2D tables (compressed columns, metrics, biharmonic and Poisson factors)
   const double f2 = 96.0;

@@ -33,6 +33,13 @@ struct SolverState {
 void launch_ocadpo(const Geo& G, const double* T, const double* uko, const double* vke,
                    const double* wo, const double* zo, double* out, double* tA, double* vA,
                    double* vB, cudaStream_t st);
+// OCADPO for ntr tracers at once (shared transports and volumes); equals
+// ntr launch_ocadpo calls bit for bit
+void launch_ocadpo_all(const Geo& G, int ntr, const double* const* T, double* const* out,
+                       double* const* mid, const double* uko, const double* vke,
+                       const double* wo, const double* zo, double* vA, double* vB,
+                       cudaStream_t st);
+int adpo_max_fused();
 void launch_ocuad(const Geo& G, const double* T, const double* uko, const double* vke,
                   const double* wo, double* out, double* tA, double* vA, double* vB,
                   cudaStream_t st);
