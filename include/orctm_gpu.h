@@ -133,6 +133,24 @@ int orctm_destroy(orctm_handle* h);
 int orctm_field_size(const orctm_handle* h, int field, size_t* n);
 int orctm_upload(orctm_handle* h, int field, const double* host, size_t n);
 int orctm_download(orctm_handle* h, int field, double* host, size_t n);
+/* Asynchronous copies on the handle's copy stream, overlapping the kernels.
+ * An upload is ordered after the work already issued on the handle and
+ * before the first routine that reads the field; routines that read other
+ * fields do not wait for it (the tracers can upload while the momentum
+ * advection runs).  A download is ordered after the work issued so far.  For
+ * the copies to be asynchronous the host arrays must be page-locked
+ * (cudaHostAlloc / cudaHostRegister); they must stay valid until
+ * orctm_wait_copies returns, which waits for every copy of the handle.
+ * orctm_set_step_outputs registers fields that orctm_step_hotpath downloads
+ * as soon as they are final in the step (the tracers after OCTDIFF, while
+ * OCVISC and the Poisson solve run; the rest at its end); n = 0 clears the
+ * list.  These are extensions with no counterpart in the reference (its
+ * model arrays live on the host). */
+int orctm_upload_async(orctm_handle* h, int field, const double* host, size_t n);
+int orctm_download_async(orctm_handle* h, int field, double* host, size_t n);
+int orctm_set_step_outputs(orctm_handle* h, int n, const int* fields, double* const* host,
+                           const size_t* sizes);
+int orctm_wait_copies(orctm_handle* h);
 
 int orctm_ocuad(orctm_handle* h);
 int orctm_ocvad(orctm_handle* h);

@@ -76,6 +76,8 @@ class Instance:
         del keep
         _lib.check(st, None)
         self.h = h
+        self._inflight = []
+        self._step_out = {}
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
@@ -113,6 +115,36 @@ class Instance:
         a = np.zeros(shp, dtype=np.float64, order="F") if out is None else out
         _lib.check(self.lib.orctm_download(self.h, self._fid(name), _p(a), a.size), self.h)
         return a
+
+    # -- asynchronous copies (page-locked host arrays; see orctm_gpu.h) -------
+    def upload_async(self, name, arr: np.ndarray):
+        """Queues the upload of a Fortran-ordered float64 array; the array must
+        stay alive and unchanged until wait_copies()."""
+        if not (arr.flags.f_contiguous and arr.dtype == np.float64):
+            raise ValueError("upload_async needs a Fortran-contiguous float64 array")
+        self._inflight.append(arr)
+        _lib.check(self.lib.orctm_upload_async(self.h, self._fid(name), _p(arr), arr.size), self.h)
+
+    def download_async(self, name, out: np.ndarray):
+        if not (out.flags.f_contiguous and out.dtype == np.float64):
+            raise ValueError("download_async needs a Fortran-contiguous float64 array")
+        self._inflight.append(out)
+        _lib.check(self.lib.orctm_download_async(self.h, self._fid(name), _p(out), out.size),
+                   self.h)
+
+    def set_step_outputs(self, outputs: dict):
+        """{field name: Fortran-ordered float64 array}: downloaded by each
+        step_hotpath as soon as the field is final (empty dict: none)."""
+        names = list(outputs)
+        ids = (C.c_int * max(len(names), 1))(*[self._fid(k) for k in names])
+        ptrs = (_D * max(len(names), 1))(*[_p(outputs[k]) for k in names])
+        sizes = (C.c_size_t * max(len(names), 1))(*[outputs[k].size for k in names])
+        self._step_out = dict(outputs)
+        _lib.check(self.lib.orctm_set_step_outputs(self.h, len(names), ids, ptrs, sizes), self.h)
+
+    def wait_copies(self):
+        _lib.check(self.lib.orctm_wait_copies(self.h), self.h)
+        self._inflight = []
 
     def upload_state(self, st: dict):
         for k in FIELDS:

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -151,6 +152,17 @@ struct orctm_handle {
   // kernel variants per precision (0 FP64, 1 FP32); -1 = not chosen yet
   int col_var[2] = {-1, -1}, spmv_var[2] = {-1, -1};
   int force_col = -1, force_spmv = -1;  // orctm_set_tuning
+  // asynchronous copies (orctm_upload_async / orctm_download_async): a copy
+  // stream, per-field "upload landed" events the compute stream waits for
+  // before a routine reads the field, buffers held until their download ends,
+  // and the outputs orctm_step_hotpath downloads as soon as they are final
+  cudaStream_t cstream = nullptr;
+  cudaEvent_t field_ready[64] = {};
+  bool pending[64] = {};
+  std::vector<double*> held;
+  std::vector<cudaEvent_t> copy_events;
+  struct StepOut { int field; double* host; size_t n; };
+  std::vector<StepOut> step_out;
   // replayed chunk of PCG iterations per precision and the variants it holds
   cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
   int pcg_graph_key[2][2] = {{-1, -1}, {-1, -1}};
@@ -932,8 +944,71 @@ int poisson_solve(orctm_handle* h, orctm_solve_stats* stats) {
 }
 
 // ------------------------------------------------------------- routines
+// ------------------------------------------------------ asynchronous copies
+// The compute stream waits for the uploads in flight of the listed fields
+// (a negative id ends the list) or of every field.
+int wait_uploads(orctm_handle* h, std::initializer_list<int> fields) {
+  for (int f : fields) {
+    if (f < 0 || f >= 64 || !h->pending[f]) continue;
+    ORCTM_CUDA_OK(cudaStreamWaitEvent(h->stream, h->field_ready[f], 0));
+    h->pending[f] = false;
+  }
+  return ORCTM_OK;
+}
+
+int wait_all_uploads(orctm_handle* h) {
+  for (int f = 0; f < 64; ++f)
+    if (h->pending[f]) {
+      ORCTM_CUDA_OK(cudaStreamWaitEvent(h->stream, h->field_ready[f], 0));
+      h->pending[f] = false;
+    }
+  return ORCTM_OK;
+}
+
+// copy stream after everything queued so far on the compute stream
+int copy_after_compute(orctm_handle* h) {
+  cudaEvent_t e = h->get_event();
+  h->copy_events.push_back(e);
+  ORCTM_CUDA_OK(cudaEventRecord(e, h->stream));
+  ORCTM_CUDA_OK(cudaStreamWaitEvent(h->cstream, e, 0));
+  return ORCTM_OK;
+}
+
+int download_async(orctm_handle* h, int f, double* host) {
+  int st;
+  if ((st = wait_uploads(h, {f}))) return st;
+  int i0, ni, j0, nj, nk;
+  extent(h, f, i0, ni, j0, nj, nk);
+  double* src = f == ORCTM_F_ZO ? h->zo : h->slot[f];
+  if ((st = copy_after_compute(h))) return st;
+  for (int k = 0; k < nk; ++k)
+    ORCTM_CUDA_OK(cudaMemcpy2DAsync(host + (size_t)k * ni * nj, sizeof(double) * ni,
+                                    src + h->L.at(i0, j0, k), sizeof(double) * h->L.P,
+                                    sizeof(double) * ni, nj, cudaMemcpyDeviceToHost, h->cstream));
+  // routines never write a buffer in place, and a referenced buffer is never
+  // handed out again: holding a reference keeps the source intact until the
+  // copy has ended
+  if (f != ORCTM_F_ZO) {
+    h->refs[src]++;
+    h->held.push_back(src);
+  }
+  return ORCTM_OK;
+}
+
+// the registered step outputs that are final at this point of the step
+int step_outputs(orctm_handle* h, bool tracers) {
+  int st;
+  for (const auto& o : h->step_out) {
+    const bool is_tracer = o.field >= ORCTM_F_THO;
+    if (is_tracer == tracers && (st = download_async(h, o.field, o.host))) return st;
+  }
+  return ORCTM_OK;
+}
+
 int r_ocadpo(orctm_handle* h, int n) {
   int st;
+  if ((st = wait_uploads(h, {ORCTM_F_THO + n, ORCTM_F_UKO, ORCTM_F_VKE, ORCTM_F_WO, ORCTM_F_ZO})))
+    return st;
   double *out, *tA, *vA, *vB;
   if ((st = h->alloc(&out)) || (st = h->alloc(&tA)) || (st = h->alloc(&vA)) || (st = h->alloc(&vB)))
     return st;
@@ -953,6 +1028,9 @@ int r_ocadpo(orctm_handle* h, int n) {
 int r_ocadpo_all(orctm_handle* h) {
   int st;
   const int ntr = h->ntr;
+  for (int n = 0; n < ntr; ++n)
+    if ((st = wait_uploads(h, {ORCTM_F_THO + n}))) return st;
+  if ((st = wait_uploads(h, {ORCTM_F_UKO, ORCTM_F_VKE, ORCTM_F_WO, ORCTM_F_ZO}))) return st;
   double *out[kMaxTracers] = {}, *mid[kMaxTracers] = {}, *vA = nullptr, *vB = nullptr;
   const double* in[kMaxTracers] = {};
   for (int n = 0; n < ntr; ++n) {
@@ -975,6 +1053,11 @@ int r_ocadpo_all(orctm_handle* h) {
 
 template <int WHICH>
 int r_momadv(orctm_handle* h) {
+  {
+    const int own = WHICH == 0 ? ORCTM_F_UOO : WHICH == 1 ? ORCTM_F_VOE : ORCTM_F_WNO;
+    const int st0 = wait_uploads(h, {own, ORCTM_F_UKO, ORCTM_F_VKE, ORCTM_F_WO, ORCTM_F_ZO});
+    if (st0) return st0;
+  }
   int st;
   double *out, *tA, *vA, *vB;
   if ((st = h->alloc(&out)) || (st = h->alloc(&tA)) || (st = h->alloc(&vA)) || (st = h->alloc(&vB)))
@@ -998,6 +1081,10 @@ int r_momadv(orctm_handle* h) {
 }
 
 int r_octdiff(orctm_handle* h) {
+  {
+    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
+    if (st0) return st0;
+  }
   int st;
   const int ntr = h->ntr;
   const double* in[kMaxTracers];
@@ -1025,12 +1112,20 @@ int r_octdiff(orctm_handle* h) {
 }
 
 int r_octimf(orctm_handle* h) {
+  {
+    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
+    if (st0) return st0;
+  }
   h->alias(ORCTM_F_UKO, ORCTM_F_UOO);
   h->alias(ORCTM_F_VKE, ORCTM_F_VOE);
   return ORCTM_OK;
 }
 
 int r_ocvisc(orctm_handle* h) {
+  {
+    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
+    if (st0) return st0;
+  }
   int st;
   double *sp, *ukv, *vkv, *wnv, *u1, *v1, *w1, *uo, *vo, *wo;
   if ((st = h->alloc(&sp)) || (st = h->alloc(&ukv)) || (st = h->alloc(&vkv)) ||
@@ -1052,6 +1147,10 @@ int r_ocvisc(orctm_handle* h) {
 }
 
 int r_ocvtot_nh(orctm_handle* h, orctm_solve_stats* stats) {
+  {
+    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
+    if (st0) return st0;
+  }
   int st;
   if ((st = ensure_solver_buffers(h))) return st;
   PROF(h, ORCTM_PROF_NH_RHS,
@@ -1138,6 +1237,9 @@ const char* orctm_last_error(const orctm_handle* h) {
 int orctm_destroy(orctm_handle* h) {
   if (!h) return ORCTM_E_ARG;
   cudaSetDevice(h->device);
+  if (h->cstream) cudaStreamSynchronize(h->cstream);
+  for (double* p : h->held) h->unref(p);
+  h->held.clear();
   if (h->stream) cudaStreamSynchronize(h->stream);
   std::vector<double*> all(h->free_.begin(), h->free_.end());
   for (auto& kv : h->refs) all.push_back(kv.first);
@@ -1163,6 +1265,10 @@ int orctm_destroy(orctm_handle* h) {
   if (h->tm1) cudaEventDestroy(h->tm1);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  for (cudaEvent_t e : h->copy_events) cudaEventDestroy(e);
+  for (int f = 0; f < 64; ++f)
+    if (h->field_ready[f]) cudaEventDestroy(h->field_ready[f]);
+  if (h->cstream) cudaStreamDestroy(h->cstream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return ORCTM_OK;
@@ -1200,6 +1306,7 @@ int orctm_create(const orctm_desc* d, orctm_handle** out) {
   h->device = d->device;
   int st = cuda_status(cudaSetDevice(h->device));
   if (!st) st = cuda_status(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  if (!st) st = cuda_status(cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking));
   if (!st) st = device_pool(h->device, &h->mempool);
   if (!st) st = setup(h, d);
   if (st) {
@@ -1223,6 +1330,10 @@ int orctm_upload(orctm_handle* h, int f, const double* host, size_t n) {
   size_t want;
   if (!host || orctm_field_size(h, f, &want) != ORCTM_OK || n != want) return ORCTM_E_ARG;
   cudaSetDevice(h->device);
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
   int i0, ni, j0, nj, nk;
   extent(h, f, i0, ni, j0, nj, nk);
   double* dst;
@@ -1249,6 +1360,10 @@ int orctm_download(orctm_handle* h, int f, double* host, size_t n) {
   size_t want;
   if (!host || orctm_field_size(h, f, &want) != ORCTM_OK || n != want) return ORCTM_E_ARG;
   cudaSetDevice(h->device);
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
   int i0, ni, j0, nj, nk;
   extent(h, f, i0, ni, j0, nj, nk);
   const double* src = f == ORCTM_F_ZO ? h->zo : h->slot[f];
@@ -1257,6 +1372,74 @@ int orctm_download(orctm_handle* h, int f, double* host, size_t n) {
                                     src + h->L.at(i0, j0, k), sizeof(double) * h->L.P,
                                     sizeof(double) * ni, nj, cudaMemcpyDeviceToHost, h->stream));
   ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return ORCTM_OK;
+}
+
+int orctm_upload_async(orctm_handle* h, int f, const double* host, size_t n) {
+  size_t want;
+  if (!host || orctm_field_size(h, f, &want) != ORCTM_OK || n != want) return ORCTM_E_ARG;
+  cudaSetDevice(h->device);
+  int st, i0, ni, j0, nj, nk;
+  extent(h, f, i0, ni, j0, nj, nk);
+  double* dst;
+  if (f == ORCTM_F_ZO) {
+    dst = h->zo;
+  } else {
+    if (h->refs[h->slot[f]] > 1) {  // shared with another field: copy on write
+      double* p;
+      if ((st = h->alloc(&p))) return st;
+      h->bind(f, p);
+    }
+    dst = h->slot[f];
+  }
+  // after the kernels queued so far (which may still read the old contents)
+  // and after the allocation above, which is ordered on the compute stream
+  if ((st = copy_after_compute(h))) return st;
+  for (int k = 0; k < nk; ++k)
+    ORCTM_CUDA_OK(cudaMemcpy2DAsync(dst + h->L.at(i0, j0, k), sizeof(double) * h->L.P,
+                                    host + (size_t)k * ni * nj, sizeof(double) * ni,
+                                    sizeof(double) * ni, nj, cudaMemcpyHostToDevice, h->cstream));
+  if (!h->field_ready[f]) ORCTM_CUDA_OK(cudaEventCreateWithFlags(&h->field_ready[f], cudaEventDisableTiming));
+  ORCTM_CUDA_OK(cudaEventRecord(h->field_ready[f], h->cstream));
+  h->pending[f] = true;
+  return ORCTM_OK;
+}
+
+int orctm_download_async(orctm_handle* h, int f, double* host, size_t n) {
+  size_t want;
+  if (!host || orctm_field_size(h, f, &want) != ORCTM_OK || n != want) return ORCTM_E_ARG;
+  cudaSetDevice(h->device);
+  return download_async(h, f, host);
+}
+
+int orctm_set_step_outputs(orctm_handle* h, int n, const int* fields, double* const* host,
+                           const size_t* sizes) {
+  if (!h || n < 0 || (n > 0 && (!fields || !host || !sizes))) return ORCTM_E_ARG;
+  std::vector<orctm_handle::StepOut> v;
+  for (int k = 0; k < n; ++k) {
+    size_t want;
+    if (!host[k] || orctm_field_size(h, fields[k], &want) != ORCTM_OK || sizes[k] != want)
+      return ORCTM_E_ARG;
+    v.push_back({fields[k], host[k], sizes[k]});
+  }
+  h->step_out = v;
+  return ORCTM_OK;
+}
+
+int orctm_wait_copies(orctm_handle* h) {
+  if (!h) return ORCTM_E_ARG;
+  cudaSetDevice(h->device);
+  // later work on the compute stream (a timer's stop event, say) comes after
+  // the copies
+  cudaEvent_t e = h->get_event();
+  ORCTM_CUDA_OK(cudaEventRecord(e, h->cstream));
+  ORCTM_CUDA_OK(cudaStreamWaitEvent(h->stream, e, 0));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->cstream));
+  h->ev_pool.push_back(e);
+  for (cudaEvent_t x : h->copy_events) h->ev_pool.push_back(x);
+  h->copy_events.clear();
+  for (double* p : h->held) h->unref(p);
+  h->held.clear();
   return ORCTM_OK;
 }
 
@@ -1287,10 +1470,15 @@ int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* s) {
   int st;
   if ((st = r_momadv<0>(h)) || (st = r_momadv<1>(h)) || (st = r_momadv<2>(h))) return st;
   if ((st = r_ocadpo_all(h))) return st;  // OCADPO(THO), OCADPO(SAO), passive tracers
-  if ((st = r_octdiff(h)) || (st = r_octimf(h)) || (st = r_ocvisc(h))) return st;
+  if ((st = r_octdiff(h))) return st;
+  // tracers are final here: registered tracer outputs start downloading
+  // while OCVISC and the Poisson solve run
+  if ((st = step_outputs(h, true))) return st;
+  if ((st = r_octimf(h)) || (st = r_ocvisc(h))) return st;
   const int ns = r_ocvtot_nh(h, s);
   if (ns != ORCTM_OK && ns != ORCTM_E_NOT_CONVERGED) return ns;
   r_octimf(h);
+  if ((st = step_outputs(h, false))) return st;
   return ns;
 }
 

@@ -78,6 +78,36 @@ def test_tracer_advection_all_equals_one_by_one(case):
         assert np.array_equal(one.download(f"tracer{n}"), fused.download(f"tracer{n}")), n
 
 
+def test_async_copies_and_step_outputs_equal_synchronous(case):
+    """Uploads queued on the copy stream, outputs downloaded while the step
+    still runs: the same state, bit for bit, as synchronous copies."""
+    _, inst = case
+    _, ref, st = _pair(inst)
+    ref.set_solver("fp64", rtol=1e-12, maxit=20000)
+    asy = Instance(inst)
+    asy.set_solver("fp64", rtol=1e-12, maxit=20000)
+    src = C.copy_state(inst)
+    for k in ("uoo", "voe", "wno", "uko", "vke", "wo", "uoo1", "voe1", "wno1", "pnh", "zo",
+              "dvo", "avo"):
+        asy.upload_async(k, np.asfortranarray(src[k]))
+    for n, t in enumerate(src["tracers"]):
+        asy.upload_async(f"tracer{n}", np.asfortranarray(t))
+    outs = {k: np.zeros(asy.shape(k), order="F") for k in ("uoo", "voe", "wno", "pnh")}
+    for n in range(asy.ntr):
+        outs[f"tracer{n}"] = np.zeros(asy.shape("pnh"), order="F")
+    asy.set_step_outputs(outs)
+    for _ in range(2):
+        ref.step_hotpath()
+        asy.step_hotpath()
+        asy.wait_copies()
+    for k, a in outs.items():
+        assert np.array_equal(a, ref.download(k)), k
+    back = np.zeros(asy.shape("voe1"), order="F")
+    asy.download_async("voe1", back)
+    asy.wait_copies()
+    assert np.array_equal(back, ref.download("voe1"))
+
+
 def test_tracer_diffusion(case):
     _, inst = case
     orc, gpu, st = _pair(inst)
