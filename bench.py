@@ -130,6 +130,13 @@ def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    try:  # one rank per GPU; ranks beyond the visible GPUs share them (replicas)
+        import torch
+
+        if torch.cuda.is_available() and torch.cuda.device_count() > 0:
+            local = local % torch.cuda.device_count()
+    except Exception:
+        pass
     pg = None
     if ws > 1:
         import datetime
