@@ -152,6 +152,23 @@ int orctm_set_step_outputs(orctm_handle* h, int n, const int* fields, double* co
                            const size_t* sizes);
 int orctm_wait_copies(orctm_handle* h);
 
+/* EXTRA-format output, the reference's restart and output format (aufw.f90,
+ * write_slice in mo_parallel.f90:733-779): per level a header record
+ * (IDATE, ICODE, KCODE, IEDIM) of 4-byte integers and a record of the values
+ * as 4-byte reals, Fortran sequential unformatted records, big-endian
+ * (Makefile:75 builds with -convert big_endian), so the files read with the
+ * same cdo scripts.  orctm_write_extra writes the given fields of a handle
+ * (codes from ORCTM/code_output.txt: THO 2, SAO 5, UKO 3, VKE 4, ZO 1, WO and
+ * WNO 7, DVO 111, AVO 110), with KCODE = INT(TIESTU(K)) for p, u and v
+ * levels, INT(TIESTW(K)) for w levels and -100 for 2D fields, and IEDIM the
+ * values of a level in the host layout; the first field truncates the file
+ * unless append is set.  orctm_write_extra_host writes nlev levels of one
+ * field from a host array (levels consecutive, iedim values each). */
+int orctm_write_extra(orctm_handle* h, const char* path, int append, int idate, int nfield,
+                      const int* fields, const int* codes);
+int orctm_write_extra_host(const char* path, int append, int idate, int code, int nlev,
+                           const int* kcodes, int iedim, const double* data);
+
 int orctm_ocuad(orctm_handle* h);
 int orctm_ocvad(orctm_handle* h);
 int orctm_ocwad(orctm_handle* h);

@@ -207,3 +207,43 @@ class Oracle:
         info = self.ocvtot_nh(st, solver=solver, rtol=rtol)
         self.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
         return info
+
+
+# ------------------------------------------------------------------ EXTRA ---
+def write_extra(path, records, append=False):
+    """EXTRA-format records as the reference writes them: for each
+    (idate, code, kcode, values) a header record of four big-endian int32
+    (IDATE, ICODE, KCODE, IEDIM) and a record of the values as big-endian
+    float32 (REAL(x, sp)), each record framed by its big-endian int32 length
+    (Fortran sequential unformatted, -convert big_endian: write_slice,
+    mo_parallel.f90:733-779; aufw.f90:54-160; Makefile:75)."""
+    with open(path, "ab" if append else "wb") as f:
+        for idate, code, kcode, values in records:
+            v = np.asarray(values, dtype=np.float64).ravel(order="F").astype(">f4")
+            hdr = np.array([idate, code, kcode, v.size], dtype=">i4").tobytes()
+            for payload in (hdr, v.tobytes()):
+                m = np.array([len(payload)], dtype=">i4").tobytes()
+                f.write(m + payload + m)
+
+
+def read_extra(path):
+    """The records of an EXTRA file: [(idate, code, kcode, float32 values)]."""
+    out = []
+    data = open(path, "rb").read()
+    pos = 0
+
+    def record():
+        nonlocal pos
+        n = int(np.frombuffer(data, ">i4", 1, pos)[0])
+        payload = data[pos + 4:pos + 4 + n]
+        tail = int(np.frombuffer(data, ">i4", 1, pos + 4 + n)[0])
+        assert tail == n, "record markers differ"
+        pos += n + 8
+        return payload
+
+    while pos < len(data):
+        hdr = np.frombuffer(record(), ">i4")
+        vals = np.frombuffer(record(), ">f4")
+        assert vals.size == hdr[3]
+        out.append((int(hdr[0]), int(hdr[1]), int(hdr[2]), vals.astype(np.float32)))
+    return out

@@ -146,6 +146,19 @@ class Instance:
         _lib.check(self.lib.orctm_wait_copies(self.h), self.h)
         self._inflight = []
 
+    # reference output format; codes from ORCTM/code_output.txt
+    EXTRA_CODES = {"tracer0": 2, "tracer1": 5, "uko": 3, "vke": 4, "uoo": 3, "voe": 4, "zo": 1,
+                   "wo": 7, "wno": 7, "dvo": 111, "avo": 110}
+
+    def write_extra(self, path: str, fields, codes=None, idate: int = 0, append: bool = False):
+        """Writes device-resident fields to an EXTRA file (orctm_write_extra)."""
+        fields = list(fields)
+        codes = list(codes) if codes is not None else [self.EXTRA_CODES[k] for k in fields]
+        ids = (C.c_int * len(fields))(*[self._fid(k) for k in fields])
+        cs = (C.c_int * len(codes))(*codes)
+        _lib.check(self.lib.orctm_write_extra(self.h, path.encode(), int(append), idate,
+                                              len(fields), ids, cs), self.h)
+
     def upload_state(self, st: dict):
         for k in FIELDS:
             if k in st:

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 SO = os.path.join(HERE, "liborctm_gpu.so")
-SOURCES = ["advect.cu", "diffuse.cu", "nh.cu", "poisson.cu", "handle.cu", "grid.cpp", "serve.cpp",
+SOURCES = ["advect.cu", "diffuse.cu", "nh.cu", "poisson.cu", "handle.cu", "grid.cpp", "serve.cpp", "extra.cpp",
            "noalloc.cu"]
 HEADERS = ["common.cuh", "ops.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

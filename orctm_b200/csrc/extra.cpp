@@ -1,0 +1,57 @@
+// EXTRA-format records, the reference's output and restart format: a header
+// record of four 4-byte integers (IDATE, ICODE, KCODE, IEDIM) followed by a
+// record of the field's values as 4-byte reals, REAL(x, sp)
+// (write_slice, mo_parallel.f90:733-779, called after the header as in
+// aufw.f90:54-160).  The records are Fortran sequential unformatted records
+// (a 4-byte length before and after the payload), and the model is built with
+// -convert big_endian (ORCTM/src_orctm/Makefile:75), so every integer, real
+// and record length is written big-endian.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/orctm_gpu.h"
+
+namespace {
+
+uint32_t be32(uint32_t v) {
+  return ((v & 0xffu) << 24) | ((v & 0xff00u) << 8) | ((v >> 8) & 0xff00u) | (v >> 24);
+}
+
+bool put_record(FILE* f, const void* payload, uint32_t bytes) {
+  const uint32_t m = be32(bytes);
+  return fwrite(&m, 4, 1, f) == 1 && (bytes == 0 || fwrite(payload, 1, bytes, f) == bytes) &&
+         fwrite(&m, 4, 1, f) == 1;
+}
+
+}  // namespace
+
+extern "C" int orctm_write_extra_host(const char* path, int append, int idate, int code, int nlev,
+                                      const int* kcodes, int iedim, const double* data) {
+  if (!path || nlev < 1 || iedim < 1 || !kcodes || !data) return ORCTM_E_ARG;
+  FILE* f = fopen(path, append ? "ab" : "wb");
+  if (!f) return ORCTM_E_ARG;
+  std::vector<uint32_t> vals((size_t)iedim);
+  bool ok = true;
+  for (int l = 0; l < nlev && ok; ++l) {
+    const int32_t hdr[4] = {idate, code, kcodes[l], iedim};
+    uint32_t bhdr[4];
+    for (int k = 0; k < 4; ++k) {
+      uint32_t u;
+      std::memcpy(&u, &hdr[k], 4);
+      bhdr[k] = be32(u);
+    }
+    ok = put_record(f, bhdr, 16);
+    const double* src = data + (size_t)l * iedim;
+    for (int n = 0; n < iedim && ok; ++n) {
+      const float x = (float)src[n];  // REAL(x, sp): round to nearest
+      uint32_t u;
+      std::memcpy(&u, &x, 4);
+      vals[(size_t)n] = be32(u);
+    }
+    if (ok) ok = put_record(f, vals.data(), (uint32_t)(4 * (size_t)iedim));
+  }
+  if (fclose(f) != 0) ok = false;
+  return ok ? ORCTM_OK : ORCTM_E_ARG;
+}

@@ -127,6 +127,7 @@ struct orctm_handle {
   PoissonGeo P{};
   int ntr = 2;
   std::string err;
+  std::vector<double> tiestu, tiestw;  // level depths (BELEG), the EXTRA level codes
 
   // geometry / tables (device)
   std::vector<void*> owned;  // freed at destroy
@@ -376,6 +377,13 @@ int setup(orctm_handle* h, const orctm_desc* d) {
   L.JN = JE + 1;
   L.plane = L.P * L.JN;  // below 2^31: checked by orctm_create
   h->ntr = d->ntracers;
+  // TIESTW / TIESTU of BELEG (beleg.f90:87-139): interface and layer-centre depths
+  h->tiestw.assign(KE + 1, 0.0);
+  h->tiestu.assign(KE + 1, 0.0);
+  for (int k = 1; k <= KE; ++k) h->tiestw[k] = h->tiestw[k - 1] + d->dzw[k - 1];
+  h->tiestu[0] = 0.5 * d->dzw[0];
+  for (int k = 2; k <= KE; ++k) h->tiestu[k - 1] = 0.5 * (h->tiestw[k] + h->tiestw[k - 1]);
+  h->tiestu[KE] = 9000.;
   Geo& G = h->G;
   G.L = L;
   G.dt = d->dt;
@@ -1440,6 +1448,30 @@ int orctm_wait_copies(orctm_handle* h) {
   h->copy_events.clear();
   for (double* p : h->held) h->unref(p);
   h->held.clear();
+  return ORCTM_OK;
+}
+
+int orctm_write_extra(orctm_handle* h, const char* path, int append, int idate, int nfield,
+                      const int* fields, const int* codes) {
+  if (!h || !path || nfield < 1 || !fields || !codes) return ORCTM_E_ARG;
+  int st;
+  for (int k = 0; k < nfield; ++k) {
+    size_t n;
+    if ((st = orctm_field_size(h, fields[k], &n))) return st;
+    std::vector<double> buf(n);
+    if ((st = orctm_download(h, fields[k], buf.data(), n))) return st;
+    int i0, ni, j0, nj, nk;
+    extent(h, fields[k], i0, ni, j0, nj, nk);
+    // KCODE: INT(TIESTU(K)) for p/u/v levels, INT(TIESTW(K)) for w levels,
+    // -100 for 2D fields (aufw.f90:63-160)
+    std::vector<int> kc((size_t)nk);
+    const Kind kind = field_kind(fields[k]);
+    for (int l = 0; l < nk; ++l)
+      kc[(size_t)l] = kind == K2P ? -100 : (int)(kind == KW ? h->tiestw[l] : h->tiestu[l]);
+    if ((st = orctm_write_extra_host(path, append || k > 0, idate, codes[k], nk, kc.data(),
+                                     ni * nj, buf.data())))
+      return st;
+  }
   return ORCTM_OK;
 }
 

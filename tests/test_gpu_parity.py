@@ -201,3 +201,31 @@ def test_solver_variants_bit_identical(case_name, mode):
         else:
             assert np.array_equal(got[0], ref[0]), (c, s)
             assert got[1:] == ref[1:], (c, s, got[1:], ref[1:])
+
+
+def test_extra_snapshot_of_device_fields(case, tmp_path):
+    """orctm_write_extra writes the device-resident fields in the reference's
+    EXTRA layout: per level the oracle reader finds IDATE, ICODE, KCODE =
+    INT(TIESTU/TIESTW) and the values rounded to float32."""
+    _, inst = case
+    _, gpu, st = _pair(inst)
+    gpu.step_hotpath()
+    fields = ["tracer0", "uko", "vke", "wo", "zo"]
+    path = str(tmp_path / "snap.ext")
+    gpu.write_extra(path, fields, idate=20261203)
+    recs = O.read_extra(path)
+    ke = inst["ke"]
+    exp = []
+    for k in fields:
+        a = gpu.download(k)
+        if k == "zo":
+            exp.append((gpu.EXTRA_CODES[k], -100, a))
+            continue
+        nk = a.shape[2]
+        for l in range(nk):
+            kc = int(inst["tiestw"][l]) if k == "wo" else int(inst["tiestu"][l])
+            exp.append((gpu.EXTRA_CODES[k], kc, a[:, :, l]))
+    assert len(recs) == len(exp) == 4 * ke + 1 + 1
+    for (idate, code, kcode, v), (ecode, ekc, ea) in zip(recs, exp):
+        assert (idate, code, kcode) == (20261203, ecode, ekc)
+        assert np.array_equal(v, ea.ravel(order="F").astype(np.float32))
