@@ -168,6 +168,15 @@ int orctm_write_extra(orctm_handle* h, const char* path, int append, int idate, 
                       const int* fields, const int* codes);
 int orctm_write_extra_host(const char* path, int append, int idate, int code, int nlev,
                            const int* kcodes, int iedim, const double* data);
+/* Restart reading (the role of AUFR, aufr.f90:103-167, which reads the same
+ * records in a fixed order): for each field the first records of its code
+ * and level size, in file order, are read as 4-byte reals, converted to
+ * double exactly and uploaded.  orctm_read_extra_host reads nlev such records
+ * of one code into a host array (kcodes may be NULL). */
+int orctm_read_extra(orctm_handle* h, const char* path, int nfield, const int* fields,
+                     const int* codes);
+int orctm_read_extra_host(const char* path, int code, int nlev, int iedim, double* out,
+                          int* kcodes);
 
 int orctm_ocuad(orctm_handle* h);
 int orctm_ocvad(orctm_handle* h);

@@ -63,7 +63,7 @@ EXPORTS = (
     "orctm_serve_drain", "orctm_serve_get_stats", "orctm_serve_destroy", "orctm_batch_run",
     "orctm_estimate_device_bytes", "orctm_check_division", "orctm_ocadpo_all",
     "orctm_upload_async", "orctm_download_async", "orctm_set_step_outputs", "orctm_wait_copies",
-    "orctm_write_extra", "orctm_write_extra_host",
+    "orctm_write_extra", "orctm_write_extra_host", "orctm_read_extra", "orctm_read_extra_host",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -107,6 +107,10 @@ def load(build_if_missing: bool = True):
                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.orctm_write_extra_host.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                            C.POINTER(C.c_int), C.c_int, _D]
+    lib.orctm_read_extra.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]
+    lib.orctm_read_extra_host.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _D,
+                                          C.POINTER(C.c_int)]
     lib.orctm_timer_start.argtypes = [C.c_void_p]
     lib.orctm_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.orctm_set_profiling.argtypes = [C.c_void_p, C.c_int]

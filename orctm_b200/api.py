@@ -159,6 +159,14 @@ class Instance:
         _lib.check(self.lib.orctm_write_extra(self.h, path.encode(), int(append), idate,
                                               len(fields), ids, cs), self.h)
 
+    def read_extra(self, path: str, fields, codes=None):
+        """Uploads fields from an EXTRA file (orctm_read_extra)."""
+        fields = list(fields)
+        codes = list(codes) if codes is not None else [self.EXTRA_CODES[k] for k in fields]
+        ids = (C.c_int * len(fields))(*[self._fid(k) for k in fields])
+        cs = (C.c_int * len(codes))(*codes)
+        _lib.check(self.lib.orctm_read_extra(self.h, path.encode(), len(fields), ids, cs), self.h)
+
     def upload_state(self, st: dict):
         for k in FIELDS:
             if k in st:

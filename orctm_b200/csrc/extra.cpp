@@ -55,3 +55,58 @@ extern "C" int orctm_write_extra_host(const char* path, int append, int idate, i
   if (fclose(f) != 0) ok = false;
   return ok ? ORCTM_OK : ORCTM_E_ARG;
 }
+
+namespace {
+
+bool get_record(FILE* f, std::vector<unsigned char>& payload) {
+  uint32_t m0, m1;
+  if (fread(&m0, 4, 1, f) != 1) return false;
+  const uint32_t n = be32(m0);
+  payload.resize(n);
+  if (n && fread(payload.data(), 1, n, f) != n) return false;
+  if (fread(&m1, 4, 1, f) != 1 || m1 != m0) return false;
+  return true;
+}
+
+}  // namespace
+
+// Reads the first nlev records of field code `code` and size iedim (in file
+// order) into out (levels consecutive), converting the 4-byte reals to double
+// exactly as the reference's read_slice assigns REAL(sp) to its REAL arrays
+// (aufr.f90:103-167); kcodes (may be NULL) receives their KCODE.
+extern "C" int orctm_read_extra_host(const char* path, int code, int nlev, int iedim,
+                                     double* out, int* kcodes) {
+  if (!path || nlev < 1 || iedim < 1 || !out) return ORCTM_E_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return ORCTM_E_ARG;
+  std::vector<unsigned char> hdr, vals;
+  int found = 0;
+  bool ok = true;
+  while (found < nlev && (ok = get_record(f, hdr))) {
+    if (hdr.size() != 16 || !(ok = get_record(f, vals))) {
+      ok = false;
+      break;
+    }
+    int32_t h[4];
+    for (int k = 0; k < 4; ++k) {
+      uint32_t u;
+      std::memcpy(&u, hdr.data() + 4 * k, 4);
+      u = be32(u);
+      std::memcpy(&h[k], &u, 4);
+    }
+    if (h[1] != code || h[3] != iedim || vals.size() != (size_t)4 * iedim) continue;
+    double* dst = out + (size_t)found * iedim;
+    for (int n = 0; n < iedim; ++n) {
+      uint32_t u;
+      std::memcpy(&u, vals.data() + 4 * (size_t)n, 4);
+      u = be32(u);
+      float x;
+      std::memcpy(&x, &u, 4);
+      dst[n] = (double)x;
+    }
+    if (kcodes) kcodes[found] = h[2];
+    ++found;
+  }
+  fclose(f);
+  return found == nlev ? ORCTM_OK : ORCTM_E_ARG;
+}

@@ -1475,6 +1475,25 @@ int orctm_write_extra(orctm_handle* h, const char* path, int append, int idate, 
   return ORCTM_OK;
 }
 
+int orctm_read_extra(orctm_handle* h, const char* path, int nfield, const int* fields,
+                     const int* codes) {
+  if (!h || !path || nfield < 1 || !fields || !codes) return ORCTM_E_ARG;
+  int st;
+  for (int k = 0; k < nfield; ++k) {
+    size_t n;
+    if ((st = orctm_field_size(h, fields[k], &n))) return st;
+    int i0, ni, j0, nj, nk;
+    extent(h, fields[k], i0, ni, j0, nj, nk);
+    std::vector<double> buf(n);
+    if ((st = orctm_read_extra_host(path, codes[k], nk, ni * nj, buf.data(), nullptr))) {
+      h->err = "EXTRA file lacks the levels of a requested field";
+      return st;
+    }
+    if ((st = orctm_upload(h, fields[k], buf.data(), n))) return st;
+  }
+  return ORCTM_OK;
+}
+
 #define ORCTM_ENTER(h)             \
   if (!(h)) return ORCTM_E_ARG;    \
   cudaSetDevice((h)->device)

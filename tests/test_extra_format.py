@@ -53,3 +53,24 @@ def test_extra_record_layout(tmp_path):
     assert np.frombuffer(raw[:4], ">i4")[0] == 16
     assert list(np.frombuffer(raw[4:20], ">i4")) == [7, 5, 3, 4]
     assert list(np.frombuffer(raw[28:44], ">f4")) == [1.0, 3.0, 2.0, 4.0]  # column-major
+
+
+def test_host_reader_reads_oracle_file(tmp_path):
+    g = np.random.Generator(np.random.PCG64(7))
+    a = g.normal(0.0, 1.0, (11, 6, 4))
+    b = g.normal(0.0, 1.0, (11, 6))
+    p = tmp_path / "r.ext"
+    recs = [(1, 2, 10 * k, a[:, :, k]) for k in range(4)] + [(1, 1, -100, b)]
+    O.write_extra(p, recs)
+    lib = _lib.load()
+    out = np.zeros(11 * 6 * 4)
+    kc = (C.c_int * 4)()
+    assert lib.orctm_read_extra_host(str(p).encode(), 2, 4, 66, out.ctypes.data_as(_D), kc) == 0
+    assert list(kc) == [0, 10, 20, 30]
+    assert np.array_equal(out.reshape((11, 6, 4), order="F"), a.astype(np.float32).astype(np.float64))
+    one = np.zeros(66)
+    assert lib.orctm_read_extra_host(str(p).encode(), 1, 1, 66, one.ctypes.data_as(_D), None) == 0
+    assert np.array_equal(one, b.ravel(order="F").astype(np.float32).astype(np.float64))
+    # a code that is not there, or too few levels
+    assert lib.orctm_read_extra_host(str(p).encode(), 5, 1, 66, one.ctypes.data_as(_D), None) != 0
+    assert lib.orctm_read_extra_host(str(p).encode(), 1, 2, 66, out.ctypes.data_as(_D), None) != 0

@@ -229,3 +229,20 @@ def test_extra_snapshot_of_device_fields(case, tmp_path):
     for (idate, code, kcode, v), (ecode, ekc, ea) in zip(recs, exp):
         assert (idate, code, kcode) == (20261203, ecode, ekc)
         assert np.array_equal(v, ea.ravel(order="F").astype(np.float32))
+
+
+def test_extra_restart_round_trip(case, tmp_path):
+    """A snapshot written by one instance and read into another (the AUFW /
+    AUFR pair): the second instance holds the first one's fields rounded to
+    float32."""
+    _, inst = case
+    _, a, _ = _pair(inst)
+    a.step_hotpath()
+    _, b, _ = _pair(inst)
+    fields = ["tracer0", "tracer1", "uko", "vke", "zo", "wo", "dvo", "avo"]
+    path = str(tmp_path / "restart.ext")
+    a.write_extra(path, fields, idate=1)
+    b.read_extra(path, fields)
+    for k in fields:
+        want = a.download(k).astype(np.float32).astype(np.float64)
+        assert np.array_equal(b.download(k), want), k
