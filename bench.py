@@ -343,7 +343,11 @@ def main():
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
         if top in tj:
-            traffic = tj[top]["dram_bytes_per_cell"] * cells
+            per = tj[top]["dram_bytes_per_cell"]
+            # the column kernel's traffic depends on the variant the tuner picked
+            var = str(tuning["fp64"][0]) if top == "pcg_col" else None
+            per = tj[top].get("by_variant", {}).get(var, per)
+            traffic = per * cells
     except Exception:
         pass
     roofline = {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": hbm,
