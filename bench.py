@@ -43,7 +43,7 @@ BYTES_PER_CELL_F64 = {
 
 
 METRIC = "cell-steps/s (hot path incl. Poisson solve @1e-10 rel. residual)"
-DATA = "synthetic (seeded PCG64, base seed 20261203; generators of BASELINE configs)"
+DATA = "synthetic (seeded PCG64, base seed 20261203; generators of the c1-c5 workloads)"
 
 
 def workload_config(inst: dict) -> dict:
@@ -577,7 +577,7 @@ def run_ensemble(args, ws, rank, local, pg):
                 "value": head["value"], "unit": "cell-steps/s", "n_gpus": ws,
                 "steps": nsteps, "warmup": 0, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded PCG64, base seed 20261203; generators of BASELINE configs)",
+                "data": "synthetic (seeded PCG64, base seed 20261203; generators of the c1-c5 workloads)",
                 "config": {"workload": f"{args.workload}: {args.members} requests over "
                                        f"{len(sizes)} distinct seeded instances, "
                                        f"{nsteps} steps each, {args.slots} slots"

@@ -1,4 +1,4 @@
-"""Seeded synthetic instance generators.  CPU only."""
+"""Seeded synthetic instance generators of the c1-c5 workloads.  CPU only."""
 import numpy as np
 import pytest
 
