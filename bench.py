@@ -264,9 +264,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3")
-    ap.add_argument("--workload", default="step", choices=["step", "c4", "c5"],
+    ap.add_argument("--workload", default="step", choices=["step", "c4", "c5", "obc"],
                     help="step: one instance per GPU (the headline); c4: ensemble batch vs one at "
-                         "a time; c5: served requests with Poisson arrivals")
+                         "a time; c5: served requests with Poisson arrivals; obc: open-boundary "
+                         "tide forcing and sponge on the tidally forced c2 box")
     ap.add_argument("--members", type=int, default=64, help="c4/c5: requests")
     ap.add_argument("--distinct", type=int, default=16,
                     help="c4/c5: distinct seeded instances the requests cycle through")
@@ -284,6 +285,8 @@ def main():
     ws, rank, local, pg = dist_setup()
     if args.impl == "reference":
         return run_reference(args, ws, rank, pg)
+    if args.workload == "obc":
+        return run_obc(args, ws, rank, local, pg)
     if args.workload != "step":
         return run_ensemble(args, ws, rank, local, pg)
 
@@ -382,6 +385,114 @@ def main():
             "mixed": mixed, "solver_tuning": tuning, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": ck,
         }
+        print(json.dumps(line), flush=True)
+    gpu.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def _band_cells(inst, obc):
+    """Cells of the u-, v- and p-point (2D) sponge bands: the cells
+    orctm_obc_uv / orctm_obc_eta read and write."""
+    ie, je, ke = inst["ie"], inst["je"], inst["ke"]
+    out = {}
+    for kind, (ilo, jlo, ni, nj) in {"u": (0, 1, ie + 1, je), "v": (1, 0, ie, je + 1),
+                                     "z": (1, 1, ie, je)}.items():
+        I = np.arange(ni)[:, None] + ilo
+        J = np.arange(nj)[None, :] + jlo
+        d = [I + 1 if kind == "u" else I, ie - I + 1, J + 1 if kind == "v" else J, je - J + 1]
+        on = [bool(inst["ob"][k]) and bool(obc["sponge"][b])
+              for b, k in enumerate(("west", "east", "north", "south"))]
+        band = np.zeros((ni, nj), dtype=bool)
+        for b in range(4):
+            if on[b]:
+                band |= np.broadcast_to(d[b] <= obc["width"][b], (ni, nj))
+        out[kind] = int(band.sum()) * (1 if kind == "z" else ke)
+    return out
+
+
+def run_obc(args, ws, rank, local, pg):
+    """Open-boundary tide forcing + 1/x sponge (orctm_obc_uv, orctm_obc_eta;
+    mo_obcs.f90) on the tidally forced c2 box (W+S open, 30-cell sponges):
+    device time per call (CUDA events on the handle's stream, max over
+    ranks), the band bytes it moves, and its share of a hot-path step.  The
+    velocity call is timed with private buffers (as after the host uploads
+    the fields) and in the driver's order right after OCTIMF, where UKO/VKE
+    share the buffers and the call copies them first."""
+    from orctm_b200 import configs
+    from orctm_b200.api import Instance
+
+    over = {}
+    if args.size:
+        nx, ny, nz = (int(v) for v in args.size.split("x"))
+        over = dict(nx=nx, ny=ny, nz=nz)
+    inst = configs.make_instance("c2", index=rank, **over)
+    obc = configs.make_obc(inst)
+    gpu = Instance(inst, device=local)
+    gpu.upload_state(configs.copy_state(inst))
+    gpu.set_solver("fp64", rtol=1e-10, maxit=5000)
+    gpu.set_obc(obc)
+    K = max(args.steps, 1) * 10
+    for s in range(args.warmup):
+        gpu.obc_uv(s)
+        gpu.obc_eta(s)
+        gpu.step_hotpath()
+
+    def timed(fn):
+        barrier(pg)
+        gpu.synchronize()
+        gpu.timer_start()
+        for s in range(K):
+            fn(s)
+        ms = gpu.timer_stop() / K
+        return max_over_ranks(pg, ms)
+
+    gpu.upload("uoo", np.asfortranarray(inst["uoo"]))   # private buffers again
+    gpu.upload("voe", np.asfortranarray(inst["voe"]))
+    n0 = Instance.kernel_launches()
+    ms_uv = timed(gpu.obc_uv)
+    launches_uv = (Instance.kernel_launches() - n0) / K
+    ms_eta = timed(gpu.obc_eta)
+
+    def uv_after_octimf(s):
+        gpu.octimf()
+        gpu.obc_uv(s)
+
+    ms_uv_shared = timed(uv_after_octimf)
+    barrier(pg)
+    gpu.synchronize()
+    gpu.timer_start()
+    for _ in range(args.steps):
+        gpu.step_hotpath()
+    ms_step = max_over_ranks(pg, gpu.timer_stop() / args.steps)
+    cells = _band_cells(inst, obc)
+    # algorithmic bytes: each band cell of UOO / VOE / ZO read and written once
+    # (masks are per-column level counts, the tidal constants a few KB)
+    bytes_uv = 16 * (cells["u"] + cells["v"])
+    bytes_eta = 16 * cells["z"]
+    hbm, peak_kind = peaks()
+    if rank == 0:
+        ach = bytes_uv / (ms_uv / 1e3) / 1e9
+        line = {"metric": "open-boundary tide forcing + sponge, device time per call "
+                          "(orctm_obc_uv; orctm_obc_eta beside it)",
+                "value": ms_uv, "unit": "ms", "n_gpus": ws, "steps": K, "warmup": args.warmup,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": DATA,
+                "config": dict(workload_config(inst), sponge_widths=obc["width"],
+                               open_sides="".join(k[0].upper() for k in ("west", "east", "north",
+                                                                        "south") if inst["ob"][k]),
+                               ntide=obc["ntide"]),
+                "obc_eta_ms": ms_eta, "obc_uv_after_octimf_ms": ms_uv_shared,
+                "step_hotpath_ms": ms_step,
+                "share_of_step": (ms_uv + ms_eta) / ms_step,
+                "band_cells": cells, "gpu_launches_per_call": launches_uv,
+                "roofline": {"bound": "hbm", "kernel": "k_obc_sponge (u and v)",
+                             "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                             "frac": round(ach / hbm, 4), "traffic": None,
+                             "bytes_per_call": bytes_uv,
+                             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                             if peak_kind == "measured" else "fallback 6.65 TB/s"}}
         print(json.dumps(line), flush=True)
     gpu.close()
     if pg is not None:

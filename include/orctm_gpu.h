@@ -20,6 +20,12 @@
  *                       petsc_solve_3D / ComputeRHS / compute_matrix
  *                                            mo_petsc.f90:211-397, 543-782
  *   orctm_step_hotpath  the driver's call sequence orctm.f90:1454-1562
+ *   orctm_set_obc       INI_OBCS (tidal constants, 1/x sponge parameters)
+ *                                            mo_obcs.f90:263-506
+ *   orctm_obc_eta       FORC_OBCS_ETA + SPONGE_OBCS_ETA(ZO)  orctm.f90:1347-1351,
+ *                                            mo_obcs.f90:569-642, 1561-1720
+ *   orctm_obc_uv        FORC_OBCS_UV + SPONGE_OBCS_UV(UOO,VOE) orctm.f90:1358-1362,
+ *                                            mo_obcs.f90:1881-2032, 2295-2582
  *   orctm_upload / orctm_download   the module arrays of MO_COMMO1
  *                                   (mo_commo1.f90:32-146) that the path reads
  *                                   and writes, moved between host and device
@@ -192,6 +198,42 @@ int orctm_octimf(orctm_handle* h);
 int orctm_ocvisc(orctm_handle* h);
 int orctm_ocvtot_nh(orctm_handle* h, orctm_solve_stats* stats);
 int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* stats);
+
+/* ---- Open-boundary tide forcing and sponge (mo_obcs.f90) -------------------
+ * The reference's build forces the open boundaries with tidal harmonics and
+ * relaxes a sponge band towards them with the 1/x weights (OBC_TIDE on,
+ * OBC_SPONGE_EXP off, Makefile:49-50); the driver calls the pair before
+ * OCTIMF (orctm.f90:1347-1362).  Sides s: 0 west, 1 east, 2 north, 3 south
+ * (open when the descriptor's ob_* switch is set); variables v: 0 z
+ * (p-points), 1 u, 2 v.  amp[s][v] / pha[s][v] are OB{W,E,N,S}{Z,U,V}am /
+ * ...ph as read by INI_OBCS (amplitude; phase as a time in s), each an
+ * (n, ntide) array, column-major, n the points along the side:
+ *     west/east   z JE (j = 1..JE)   u JE (j = 1..JE)     v JE+1 (j = 0..JE)
+ *     north/south z IE (i = 1..IE)   u IE+1 (i = 0..IE)   v IE (i = 1..IE)
+ * They are needed for the open, sponged sides only (others may be NULL).
+ * The boundary value of a point is
+ *     sum_td AM(q,td) * MASK * COS(2 PI (LDTRUN * DT - PH(q,td)) / T(td))
+ * with MASK the level-1 mask of the boundary cell; in a band of width w the
+ * cell at distance d = 1..w from the boundary cell relaxes towards it with
+ * rate DT / ((s1 Urelaxbound + s2 Urelaxinner) / w), s1 = w - d + 1,
+ * s2 = d - 1, and the nearer band wins where two bands cross. */
+#define ORCTM_OBC_MAX_TIDES 8
+typedef struct orctm_obc {
+  int ntide;                 /* tidalnumber (mo_obcs.f90:19), 1..ORCTM_OBC_MAX_TIDES */
+  const double* period;      /* tidalPeriod(ntide), s, nonzero */
+  int sponge[4];             /* SpongeWest, SpongeEast, SpongeNorth, SpongeSouth */
+  int width[4];              /* spongew, spongee, spongen, sponges: 1..IE (w/e), 1..JE (n/s) */
+  double relax_inner;        /* Urelaxinner, s */
+  double relax_bound;        /* Urelaxbound, s */
+  const double* amp[4][3];
+  const double* pha[4][3];
+} orctm_obc;
+/* Copies the constants to the device (INI_OBCS); may be called again. */
+int orctm_set_obc(orctm_handle* h, const orctm_obc* obc);
+/* ZO relaxed towards the tidal elevation at time step ldtrun, in place. */
+int orctm_obc_eta(orctm_handle* h, int ldtrun);
+/* UOO and VOE relaxed towards the tidal velocities at time step ldtrun. */
+int orctm_obc_uv(orctm_handle* h, int ldtrun);
 
 /* solver mode and relative-residual target (default FP64, 1e-10, 5000) */
 int orctm_set_solver(orctm_handle* h, int mode, double rtol, int maxit);

@@ -48,6 +48,38 @@ class _Grid(C.Structure):
     ]
 
 
+class _Obc(C.Structure):
+    _fields_ = [
+        ("ntide", C.c_int), ("period", _D), ("sponge", C.c_int * 4), ("width", C.c_int * 4),
+        ("relax_inner", C.c_double), ("relax_bound", C.c_double),
+        ("amp", (_D * 3) * 4), ("pha", (_D * 3) * 4),
+    ]
+
+
+def obc_struct(obc: dict):
+    """og_obc of an open-boundary dict (orctm_b200.configs.make_obc); returns
+    the structure and the arrays it points into."""
+    keep = [np.ascontiguousarray(obc["period"], dtype=np.float64)]
+    o = _Obc()
+    o.ntide = int(obc["ntide"])
+    o.period = _p(keep[0])
+    for b in range(4):
+        o.sponge[b] = int(obc["sponge"][b])
+        o.width[b] = int(obc["width"][b])
+        for v in range(3):
+            for dst, src in ((o.amp, obc["amp"]), (o.pha, obc["pha"])):
+                a = src[b][v]
+                if a is None:
+                    dst[b][v] = _D()
+                else:
+                    a = np.asfortranarray(a, dtype=np.float64)
+                    keep.append(a)
+                    dst[b][v] = _p(a)
+    o.relax_inner = float(obc["relax_inner"])
+    o.relax_bound = float(obc["relax_bound"])
+    return o, keep
+
+
 _lib = None
 
 
@@ -130,6 +162,15 @@ class Oracle:
 
     def ocvisc(self, uoo, voe, wno, uko, vke, avo):
         lib().og_ocvisc(C.byref(self.g), _p(uoo), _p(voe), _p(wno), _p(uko), _p(vke), _p(avo))
+
+    # -- open boundaries (mo_obcs.f90) ---------------------------------------
+    def obc_eta(self, obc, step, zo):
+        o, keep = obc_struct(obc)
+        lib().og_obc_eta(C.byref(self.g), C.byref(o), int(step), _p(zo))
+
+    def obc_uv(self, obc, step, uoo, voe):
+        o, keep = obc_struct(obc)
+        lib().og_obc_uv(C.byref(self.g), C.byref(o), int(step), _p(uoo), _p(voe))
 
     def octimf(self, uoo, voe, uko, vke):
         lib().og_octimf(C.byref(self.g), _p(uoo), _p(voe), _p(uko), _p(vke))

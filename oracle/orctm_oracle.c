@@ -1663,3 +1663,264 @@ int og_solve(const og_grid *g, const int *rp, const int *ci, const double *val,
   free(pc.a); free(pc.d); free(pc.c);
   return converged ? it : -it - 1;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Open-boundary tides and sponge (mo_obcs.f90, OBC_TIDE on, 1/x sponge).   */
+/* ------------------------------------------------------------------------ */
+/* One boundary value of the tidal sum (mo_obcs.f90:578-584 and the like):
+ * sum over td of AM(idx,td) * MASK * COS(2 PI (t - PH(idx,td)) / T(td)). */
+static double og_tide(const og_obc *o, const double *am, const double *ph, int n, int idx,
+                      double mask, double t, double pi) {
+  double s = 0.0;
+  for (int td = 0; td < o->ntide; ++td) {
+    const size_t q = (size_t)idx + (size_t)n * (size_t)td;
+    s = s + am[q] * mask * cos(2.0 * pi * (t - ph[q]) / o->period[td]);
+  }
+  return s;
+}
+
+/* lambda of one sponge row (mo_obcs.f90:1578-1583): DT / the interpolated
+ * relaxation time, 0 where that time is 0 */
+static double og_lambda(double s1, double s2, double relb, double reli, int w, double dt) {
+  double lambda = (s1 * relb + s2 * reli) / (double)w;
+  return lambda != 0.0 ? dt / lambda : 0.0;
+}
+
+void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo) {
+  DIMS;
+  const double pi = 4.0 * atan(1.0);     /* orctm.f90:525 */
+  const double t = (double)step * g->dt; /* mytime = i_step * DT, mo_obcs.f90:574 */
+  const int W = g->ob_west, E = g->ob_east, N = g->ob_north, S = g->ob_south;
+  const double relb = o->relax_bound, reli = o->relax_inner; /* rel_eta*, mo_obcs.f90:499-506 */
+  const double dt = g->dt;
+  /* FORC_OBCS_ETA, mo_obcs.f90:569-642 */
+  double *zw = zalloc(JE), *ze = zalloc(JE), *zn = zalloc(IE), *zs = zalloc(IE);
+  for (int j = 1; j <= JE; ++j) {
+    if (W) zw[j - 1] = og_tide(o, o->amp[0][0], o->pha[0][0], JE, j - 1, P3(g->weto, 1, j, 1), t, pi);
+    if (E) ze[j - 1] = og_tide(o, o->amp[1][0], o->pha[1][0], JE, j - 1, P3(g->weto, IE, j, 1), t, pi);
+  }
+  for (int i = 1; i <= IE; ++i) {
+    if (N) zn[i - 1] = og_tide(o, o->amp[2][0], o->pha[2][0], IE, i - 1, P3(g->weto, i, 1, 1), t, pi);
+    if (S) zs[i - 1] = og_tide(o, o->amp[3][0], o->pha[3][0], IE, i - 1, P3(g->weto, i, JE, 1), t, pi);
+  }
+  /* SPONGE_OBCS_ETA, mo_obcs.f90:1561-1720 */
+  const size_t n2 = (size_t)IE * JE;
+  double *zz = zalloc(n2), *fo = zalloc(n2), *fw = zalloc(n2), *fe = zalloc(n2), *fn = zalloc(n2),
+         *fs = zalloc(n2);
+  memcpy(zz, zo, sizeof(double) * n2);
+  const int sw = o->width[0], se = o->width[1], sn = o->width[2], ss = o->width[3];
+  const int SW_ = W && o->sponge[0], SE_ = E && o->sponge[1], SN_ = N && o->sponge[2],
+            SS_ = S && o->sponge[3];
+  if (SW_)
+    for (int i = 1; i <= sw; ++i) {
+      const double s1 = (double)(sw - i + 1), s2 = (double)(i - 1);
+      const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
+      for (int j = 1; j <= JE; ++j) {
+        const double zr = (s1 * zw[j - 1] + s2 * P2(zz, i, j)) / (double)sw;
+        P2(fw, i, j) = P3(g->weto, 1, j, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
+      }
+    }
+  if (SE_)
+    for (int i = IE; i >= IE - se + 1; --i) {
+      const double s1 = (double)(i - IE + se), s2 = (double)(IE - i);
+      const double lambda = og_lambda(s1, s2, relb, reli, se, dt);
+      for (int j = 1; j <= JE; ++j) {
+        const double zr = (s1 * ze[j - 1] + s2 * P2(zz, i, j)) / (double)se;
+        P2(fe, i, j) = P3(g->weto, IE, j, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
+      }
+    }
+  if (SN_)
+    for (int j = 1; j <= sn; ++j) {
+      const double s1 = (double)(sn - j + 1), s2 = (double)(j - 1);
+      const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
+      for (int i = 1; i <= IE; ++i) {
+        const double zr = (s1 * zn[i - 1] + s2 * P2(zz, i, j)) / (double)sn;
+        P2(fn, i, j) = P3(g->weto, i, 1, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
+      }
+    }
+  if (SS_)
+    for (int j = JE; j >= JE - ss + 1; --j) {
+      const double s1 = (double)(j - JE + ss), s2 = (double)(JE - j);
+      const double lambda = og_lambda(s1, s2, relb, reli, ss, dt);
+      for (int i = 1; i <= IE; ++i) {
+        const double zr = (s1 * zs[i - 1] + s2 * P2(zz, i, j)) / (double)ss;
+        P2(fs, i, j) = P3(g->weto, i, JE, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
+      }
+    }
+  for (size_t q = 0; q < n2; ++q) fo[q] = fw[q] + fe[q] + fn[q] + fs[q];
+  /* corners: the band nearer to the cell wins (mo_obcs.f90:1646-1714) */
+  if (SN_ && SW_)
+    for (int i = 1; i <= sw; ++i)
+      for (int j = 1; j <= sn; ++j) P2(fo, i, j) = i < j ? P2(fw, i, j) : P2(fn, i, j);
+  if (SS_ && SW_)
+    for (int i = 1; i <= sw; ++i)
+      for (int j = JE; j >= JE - ss + 1; --j)
+        P2(fo, i, j) = i < (JE - j + 1) ? P2(fw, i, j) : P2(fs, i, j);
+  if (SN_ && SE_)
+    for (int i = IE; i >= IE - se + 1; --i)
+      for (int j = 1; j <= sn; ++j) P2(fo, i, j) = (IE - i + 1) < j ? P2(fe, i, j) : P2(fn, i, j);
+  if (SS_ && SE_)
+    for (int i = IE; i >= IE - se + 1; --i)
+      for (int j = JE; j >= JE - ss + 1; --j)
+        P2(fo, i, j) = (IE - i + 1) < (JE - j + 1) ? P2(fe, i, j) : P2(fs, i, j);
+  for (size_t q = 0; q < n2; ++q) zo[q] = zz[q] + fo[q];
+  free(zw); free(ze); free(zn); free(zs);
+  free(zz); free(fo); free(fw); free(fe); free(fn); free(fs);
+}
+
+void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double *voe) {
+  DIMS;
+  const double pi = 4.0 * atan(1.0);     /* orctm.f90:525 */
+  const double t = (double)step * g->dt; /* mytime = i_step * DT, mo_obcs.f90:1886 */
+  const int W = g->ob_west, E = g->ob_east, N = g->ob_north, S = g->ob_south;
+  const double relb = o->relax_bound, reli = o->relax_inner; /* rel_uv*, mo_obcs.f90:499-500 */
+  const double dt = g->dt;
+  /* FORC_OBCS_UV, mo_obcs.f90:1881-1994 (add_tide is .FALSE., line 18) */
+  double *uzw = zalloc(JE), *uze = zalloc(JE), *vzw = zalloc(JE + 1), *vze = zalloc(JE + 1);
+  double *uzn = zalloc(IE + 1), *uzs = zalloc(IE + 1), *vzn = zalloc(IE), *vzs = zalloc(IE);
+  for (int j = 1; j <= JE; ++j) {
+    if (W) uzw[j - 1] = og_tide(o, o->amp[0][1], o->pha[0][1], JE, j - 1, U3(g->amsuo, 0, j, 1), t, pi);
+    if (E) uze[j - 1] = og_tide(o, o->amp[1][1], o->pha[1][1], JE, j - 1, U3(g->amsuo, IE, j, 1), t, pi);
+  }
+  for (int j = 0; j <= JE; ++j) {
+    if (W) vzw[j] = og_tide(o, o->amp[0][2], o->pha[0][2], JE + 1, j, V3(g->amsue, 1, j, 1), t, pi);
+    if (E) vze[j] = og_tide(o, o->amp[1][2], o->pha[1][2], JE + 1, j, V3(g->amsue, IE, j, 1), t, pi);
+  }
+  for (int i = 0; i <= IE; ++i) {
+    if (N) uzn[i] = og_tide(o, o->amp[2][1], o->pha[2][1], IE + 1, i, U3(g->amsuo, i, 1, 1), t, pi);
+    if (S) uzs[i] = og_tide(o, o->amp[3][1], o->pha[3][1], IE + 1, i, U3(g->amsuo, i, JE, 1), t, pi);
+  }
+  for (int i = 1; i <= IE; ++i) {
+    if (N) vzn[i - 1] = og_tide(o, o->amp[2][2], o->pha[2][2], IE, i - 1, V3(g->amsue, i, 0, 1), t, pi);
+    if (S) vzs[i - 1] = og_tide(o, o->amp[3][2], o->pha[3][2], IE, i - 1, V3(g->amsue, i, JE, 1), t, pi);
+  }
+  /* SPONGE_OBCS_UV, mo_obcs.f90:2295-2582, with the level values of
+   * UPGRADE_OBCS_UV (mo_obcs.f90:1997-2032) formed in place:
+   * obc_uw(j,k) = obc_uzw(j) * AMSUO(0,j,k) and so on */
+  const size_t nu = (size_t)(IE + 1) * JE * KE, nv = (size_t)IE * (JE + 1) * KE;
+  double *uu = zalloc(nu), *uf = zalloc(nu), *uw = zalloc(nu), *ue = zalloc(nu), *un = zalloc(nu),
+         *us = zalloc(nu);
+  double *vv = zalloc(nv), *vf = zalloc(nv), *vw = zalloc(nv), *ve = zalloc(nv), *vn = zalloc(nv),
+         *vs = zalloc(nv);
+  memcpy(uu, uoo, sizeof(double) * nu);
+  memcpy(vv, voe, sizeof(double) * nv);
+  const int sw = o->width[0], se = o->width[1], sn = o->width[2], ss = o->width[3];
+  const int SW_ = W && o->sponge[0], SE_ = E && o->sponge[1], SN_ = N && o->sponge[2],
+            SS_ = S && o->sponge[3];
+  for (int k = 1; k <= KE; ++k) {
+    if (SW_) {
+      for (int i = 0; i <= sw - 1; ++i) {
+        const double s1 = (double)(sw - i), s2 = (double)i;
+        const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
+        for (int j = 1; j <= JE; ++j) {
+          const double ob = uzw[j - 1] * U3(g->amsuo, 0, j, k);
+          const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)sw;
+          U3(uw, i, j, k) = U3(g->amsuo, 0, j, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
+        }
+      }
+      for (int i = 1; i <= sw; ++i) {
+        const double s1 = (double)(sw - i + 1), s2 = (double)(i - 1);
+        const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
+        for (int j = 0; j <= JE; ++j) {
+          const double ob = vzw[j] * V3(g->amsue, 1, j, k);
+          const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)sw;
+          V3(vw, i, j, k) = V3(g->amsue, 1, j, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
+        }
+      }
+    }
+    if (SE_) {
+      for (int i = IE; i >= IE - se + 1; --i) {
+        const double s1 = (double)(i - IE + se), s2 = (double)(IE - i);
+        const double lambda = og_lambda(s1, s2, relb, reli, se, dt);
+        for (int j = 1; j <= JE; ++j) {
+          const double ob = uze[j - 1] * U3(g->amsuo, IE, j, k);
+          const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)se;
+          U3(ue, i, j, k) = U3(g->amsuo, IE, j, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
+        }
+        for (int j = 0; j <= JE; ++j) {
+          const double ob = vze[j] * V3(g->amsue, IE, j, k);
+          const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)se;
+          V3(ve, i, j, k) = V3(g->amsue, IE, j, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
+        }
+      }
+    }
+    if (SN_) {
+      for (int j = 1; j <= sn; ++j) {
+        const double s1 = (double)(sn - j + 1), s2 = (double)(j - 1);
+        const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
+        for (int i = 0; i <= IE; ++i) {
+          const double ob = uzn[i] * U3(g->amsuo, i, 1, k);
+          const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)sn;
+          U3(un, i, j, k) = U3(g->amsuo, i, 1, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
+        }
+      }
+      for (int j = 0; j <= sn - 1; ++j) {
+        const double s1 = (double)(sn - j), s2 = (double)j;
+        const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
+        for (int i = 1; i <= IE; ++i) {
+          const double ob = vzn[i - 1] * V3(g->amsue, i, 0, k);
+          const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)sn;
+          V3(vn, i, j, k) = V3(g->amsue, i, 0, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
+        }
+      }
+    }
+    if (SS_) {
+      for (int j = JE; j >= JE - ss + 1; --j) {
+        const double s1 = (double)(j - JE + ss), s2 = (double)(JE - j);
+        const double lambda = og_lambda(s1, s2, relb, reli, ss, dt);
+        for (int i = 0; i <= IE; ++i) {
+          const double ob = uzs[i] * U3(g->amsuo, i, JE, k);
+          const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)ss;
+          U3(us, i, j, k) = U3(g->amsuo, i, JE, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
+        }
+        for (int i = 1; i <= IE; ++i) {
+          const double ob = vzs[i - 1] * V3(g->amsue, i, JE, k);
+          const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)ss;
+          V3(vs, i, j, k) = V3(g->amsue, i, JE, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
+        }
+      }
+    }
+  }
+  for (size_t q = 0; q < nu; ++q) uf[q] = uw[q] + ue[q] + un[q] + us[q];
+  for (size_t q = 0; q < nv; ++q) vf[q] = vw[q] + ve[q] + vn[q] + vs[q];
+  /* corners, mo_obcs.f90:2453-2566 */
+  for (int k = 1; k <= KE; ++k) {
+    if (SN_ && SW_) {
+      for (int i = 0; i <= sw - 1; ++i)
+        for (int j = 1; j <= sn; ++j)
+          U3(uf, i, j, k) = (i + 1) < j ? U3(uw, i, j, k) : U3(un, i, j, k);
+      for (int i = 1; i <= sw; ++i)
+        for (int j = 0; j <= sn - 1; ++j)
+          V3(vf, i, j, k) = i < (j + 1) ? V3(vw, i, j, k) : V3(vn, i, j, k);
+    }
+    if (SS_ && SW_) {
+      for (int i = 0; i <= sw - 1; ++i)
+        for (int j = JE; j >= JE - ss + 1; --j)
+          U3(uf, i, j, k) = (i + 1) < (JE - j + 1) ? U3(uw, i, j, k) : U3(us, i, j, k);
+      for (int i = 1; i <= sw; ++i)
+        for (int j = JE; j >= JE - ss + 1; --j)
+          V3(vf, i, j, k) = i < (JE - j + 1) ? V3(vw, i, j, k) : V3(vs, i, j, k);
+    }
+    if (SN_ && SE_) {
+      for (int i = IE; i >= IE - se + 1; --i)
+        for (int j = 1; j <= sn; ++j)
+          U3(uf, i, j, k) = (IE - i + 1) < j ? U3(ue, i, j, k) : U3(un, i, j, k);
+      for (int i = IE; i >= IE - se + 1; --i)
+        for (int j = 0; j <= sn - 1; ++j)
+          V3(vf, i, j, k) = (IE - i + 1) < (j + 1) ? V3(ve, i, j, k) : V3(vn, i, j, k);
+    }
+    if (SS_ && SE_) {
+      for (int i = IE; i >= IE - se + 1; --i)
+        for (int j = JE; j >= JE - ss + 1; --j)
+          U3(uf, i, j, k) = (IE - i + 1) < (JE - j + 1) ? U3(ue, i, j, k) : U3(us, i, j, k);
+      for (int i = IE; i >= IE - se + 1; --i)
+        for (int j = JE; j >= JE - ss + 1; --j)
+          V3(vf, i, j, k) = (IE - i + 1) < (JE - j + 1) ? V3(ve, i, j, k) : V3(vs, i, j, k);
+    }
+  }
+  for (size_t q = 0; q < nu; ++q) uoo[q] = uu[q] + uf[q];
+  for (size_t q = 0; q < nv; ++q) voe[q] = vv[q] + vf[q];
+  free(uzw); free(uze); free(vzw); free(vze); free(uzn); free(uzs); free(vzn); free(vzs);
+  free(uu); free(uf); free(uw); free(ue); free(un); free(us);
+  free(vv); free(vf); free(vw); free(ve); free(vn); free(vs);
+}

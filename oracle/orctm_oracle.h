@@ -93,6 +93,29 @@ int og_solve(const og_grid *g, const int *rowptr, const int *colind,
              const double *val, const double *b, double *x, double rtol,
              int maxit, double *relres);
 
+/* Open-boundary tide forcing and 1/x sponge relaxation (mo_obcs.f90 as built
+ * with OBC_TIDE on and OBC_SPONGE_EXP off, Makefile:49-50).  Boundaries b:
+ * 0 west, 1 east, 2 north, 3 south; variables v: 0 z (p-points), 1 u, 2 v.
+ * amp[b][v] / pha[b][v] are OB{W,E,N,S}{Z,U,V}am / ...ph (mo_obcs.f90:40-46)
+ * as (n, ntide) arrays, column-major, n the points along the boundary:
+ * west/east z JE (j = 1..JE), u JE (j = 1..JE), v JE+1 (j = 0..JE);
+ * north/south z IE (i = 1..IE), u IE+1 (i = 0..IE), v IE (i = 1..IE).
+ * The open-boundary switches are og_grid's ob_*. */
+typedef struct og_obc {
+  int ntide;                        /* tidalnumber */
+  const double *period;             /* tidalPeriod(ntide), s */
+  int sponge[4];                    /* SpongeWest, SpongeEast, SpongeNorth, SpongeSouth */
+  int width[4];                     /* spongew, spongee, spongen, sponges */
+  double relax_inner, relax_bound;  /* Urelaxinner, Urelaxbound, s */
+  const double *amp[4][3], *pha[4][3];
+} og_obc;
+
+/* FORC_OBCS_ETA + SPONGE_OBCS_ETA(ZO) at time step `step` (orctm.f90:1347-1351). */
+void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo);
+/* FORC_OBCS_UV (with UPGRADE_OBCS_UV) + SPONGE_OBCS_UV(UOO, VOE) at time step
+ * `step` (orctm.f90:1358-1362). */
+void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double *voe);
+
 /* Applies OCTIMF (octimf.f90:1-22): uko <- uoo, vke <- voe. */
 void og_octimf(const og_grid *g, const double *uoo, const double *voe,
                double *uko, double *vke);

@@ -51,6 +51,18 @@ class SolveStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+OBC_MAX_TIDES = 8
+
+
+class Obc(C.Structure):
+    """orctm_obc: open-boundary tidal constants and sponge parameters."""
+    _fields_ = [
+        ("ntide", C.c_int), ("period", _D), ("sponge", C.c_int * 4), ("width", C.c_int * 4),
+        ("relax_inner", C.c_double), ("relax_bound", C.c_double),
+        ("amp", (_D * 3) * 4), ("pha", (_D * 3) * 4),
+    ]
+
+
 EXPORTS = (
     "orctm_abi_version", "orctm_status_string", "orctm_last_error", "orctm_create",
     "orctm_destroy", "orctm_field_size", "orctm_upload", "orctm_download", "orctm_ocuad",
@@ -64,6 +76,7 @@ EXPORTS = (
     "orctm_estimate_device_bytes", "orctm_check_division", "orctm_ocadpo_all",
     "orctm_upload_async", "orctm_download_async", "orctm_set_step_outputs", "orctm_wait_copies",
     "orctm_write_extra", "orctm_write_extra_host", "orctm_read_extra", "orctm_read_extra_host",
+    "orctm_set_obc", "orctm_obc_eta", "orctm_obc_uv",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -111,6 +124,9 @@ def load(build_if_missing: bool = True):
                                      C.POINTER(C.c_int)]
     lib.orctm_read_extra_host.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _D,
                                           C.POINTER(C.c_int)]
+    lib.orctm_set_obc.argtypes = [C.c_void_p, C.POINTER(Obc)]
+    lib.orctm_obc_eta.argtypes = [C.c_void_p, C.c_int]
+    lib.orctm_obc_uv.argtypes = [C.c_void_p, C.c_int]
     lib.orctm_timer_start.argtypes = [C.c_void_p]
     lib.orctm_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.orctm_set_profiling.argtypes = [C.c_void_p, C.c_int]

@@ -55,6 +55,79 @@ def make_desc(inst: dict, device: int = 0):
     return d, keep
 
 
+OBC_SIDES = ("West", "East", "North", "South")
+OBC_VARS = ("z", "u", "v")
+
+
+def make_obc(obc: dict):
+    """The orctm_obc of an open-boundary dict (keys ntide, period, sponge,
+    width, relax_inner, relax_bound, amp, pha as orctm_b200.configs.make_obc
+    returns them; amp[s][v] / pha[s][v] are (n, ntide) arrays or None), and
+    the arrays its pointers refer to."""
+    o = _lib.Obc()
+    keep = [np.ascontiguousarray(obc["period"], dtype=np.float64)]
+    o.ntide = int(obc["ntide"])
+    o.period = _p(keep[0])
+    for b in range(4):
+        o.sponge[b] = int(obc["sponge"][b])
+        o.width[b] = int(obc["width"][b])
+        for v in range(3):
+            for dst, src in ((o.amp, obc["amp"]), (o.pha, obc["pha"])):
+                a = src[b][v]
+                if a is None:
+                    dst[b][v] = _D()
+                    continue
+                a = np.asfortranarray(a, dtype=np.float64)
+                keep.append(a)
+                dst[b][v] = _p(a)
+    o.relax_inner = float(obc["relax_inner"])
+    o.relax_bound = float(obc["relax_bound"])
+    return o, keep
+
+
+def obc_file_name(side: int, var: int, phase: bool) -> str:
+    """The file INI_OBCS reads one array from (mo_obcs.f90:270-398), e.g.
+    OB_West_u_Amp.bin / OB_West_u_Gph.bin."""
+    return f"OB_{OBC_SIDES[side]}_{OBC_VARS[var]}_{'Gph' if phase else 'Amp'}.bin"
+
+
+def read_obc_files(dirname: str, ie: int, je: int, ob: dict, ntide: int):
+    """amp[s][v], pha[s][v] from the reference's harmonic-constant files of the
+    open sides: unformatted stream files (FORM='BINARY') of ntide columns of
+    n values, 8-byte big-endian reals (-r8, -convert big_endian, Makefile:75)."""
+    import os
+
+    from .configs import OBC_BOUNDARIES, obc_points
+
+    amp = [[None] * 3 for _ in range(4)]
+    pha = [[None] * 3 for _ in range(4)]
+    for b, name in enumerate(OBC_BOUNDARIES):
+        if not ob[name]:
+            continue
+        for v in range(3):
+            n = obc_points(ie, je, b, v)
+            for dst, ph in ((amp, False), (pha, True)):
+                path = os.path.join(dirname, obc_file_name(b, v, ph))
+                a = np.fromfile(path, dtype=">f8")
+                if a.size != n * ntide:
+                    raise ValueError(f"{path}: {a.size} values, expected {n} x {ntide}")
+                dst[b][v] = np.asfortranarray(a.astype(np.float64).reshape((n, ntide), order="F"))
+    return amp, pha
+
+
+def write_obc_files(dirname: str, amp, pha) -> None:
+    """Writes amp / pha in the layout read_obc_files (and INI_OBCS) reads."""
+    import os
+
+    for b in range(4):
+        for v in range(3):
+            for src, ph in ((amp, False), (pha, True)):
+                a = src[b][v]
+                if a is not None:
+                    np.asarray(a, dtype=np.float64).ravel(order="F").astype(">f8").tofile(
+                        os.path.join(dirname, obc_file_name(b, v, ph)))
+
+
 def field_id(name) -> int:
     if isinstance(name, int):
         return name
@@ -201,6 +274,20 @@ class Instance:
 
     def octimf(self):
         _lib.check(self.lib.orctm_octimf(self.h), self.h)
+
+    # -- open boundaries (mo_obcs.f90) -----------------------------------------
+    def set_obc(self, obc: dict):
+        """INI_OBCS: tidal constants and sponge parameters to the device."""
+        o, keep = make_obc(obc)
+        _lib.check(self.lib.orctm_set_obc(self.h, C.byref(o)), self.h)
+
+    def obc_eta(self, ldtrun: int):
+        """FORC_OBCS_ETA + SPONGE_OBCS_ETA(ZO) at time step ldtrun."""
+        _lib.check(self.lib.orctm_obc_eta(self.h, int(ldtrun)), self.h)
+
+    def obc_uv(self, ldtrun: int):
+        """FORC_OBCS_UV + UPGRADE_OBCS_UV + SPONGE_OBCS_UV(UOO, VOE) at time step ldtrun."""
+        _lib.check(self.lib.orctm_obc_uv(self.h, int(ldtrun)), self.h)
 
     def ocvisc(self):
         _lib.check(self.lib.orctm_ocvisc(self.h), self.h)

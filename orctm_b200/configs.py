@@ -166,6 +166,63 @@ def make_instance(name: str, index: int = 0, seed: int | None = None, builder=No
     return inst
 
 
+# Open-boundary namelist OCEOBC of the verification runs
+# (verification/Sect.3.5/OCECTL): sponge widths, relaxation times and the two
+# tidal periods (semidiurnal and diurnal, s).
+OBC_WIDTH = 30
+OBC_RELAX_INNER = 44714.1643
+OBC_PERIODS = (44714.1643, 86164.0906)
+OBC_BOUNDARIES = ("west", "east", "north", "south")
+
+
+def obc_points(ie: int, je: int, b: int, v: int) -> int:
+    """Points along boundary b (0 W, 1 E, 2 N, 3 S) of variable v (0 z, 1 u,
+    2 v), as the reference dimensions OB{W,E,N,S}{Z,U,V}am (mo_obcs.f90:124-138)."""
+    if b < 2:
+        return je + 1 if v == 2 else je
+    return ie + 1 if v == 1 else ie
+
+
+def make_obc(inst: dict, seed: int | None = None, width: int | None = None,
+             relax_bound: float | None = None) -> dict:
+    """Seeded tidal harmonic constants and 1/x sponge parameters for the open
+    boundaries of ``inst`` (the inputs INI_OBCS reads from OB_*_Amp.bin /
+    OB_*_Gph.bin and namelist OCEOBC, mo_obcs.f90:263-506).
+
+    Amplitudes vary smoothly along each boundary around the instance's tide
+    amplitude (elevation, m) and its shallow-water velocity (m/s); phases are
+    times (s) that lag along the boundary like a progressive wave.  The
+    boundary relaxation time defaults to DT, so that the sponge sets the
+    outermost cell to the tidal value."""
+    ie, je = inst["ie"], inst["je"]
+    g = rng((inst["seed"] if seed is None else seed) + 7919)
+    tide = inst.get("tide") or {"amplitude": 1.0, "phase": 0.0}
+    ntide = len(OBC_PERIODS)
+    amp = [[None] * 3 for _ in range(4)]
+    pha = [[None] * 3 for _ in range(4)]
+    depth = float(np.max(inst["depto"])) if "depto" in inst else 4000.0
+    uscale = math.sqrt(9.81 / max(depth, 1.0))
+    for b, name in enumerate(OBC_BOUNDARIES):
+        if not inst["ob"][name]:
+            continue
+        for v in range(3):
+            n = obc_points(ie, je, b, v)
+            s = np.linspace(0.0, 1.0, n)
+            a = np.empty((n, ntide), order="F")
+            p = np.empty((n, ntide), order="F")
+            for td, per in enumerate(OBC_PERIODS):
+                base = tide["amplitude"] * (1.0 if td == 0 else 0.3) * (1.0 if v == 0 else uscale)
+                a[:, td] = base * (1.0 + 0.2 * np.sin(2 * math.pi * (s + g.uniform())))
+                p[:, td] = (tide["phase"] / (2 * math.pi) + 0.25 * s + g.uniform(0, 0.05)) * per
+            amp[b][v], pha[b][v] = a, p
+    w = width if width is not None else min(OBC_WIDTH, max(1, (ie - 2) // 3), max(1, (je - 2) // 3))
+    return {"ntide": ntide, "period": np.array(OBC_PERIODS, dtype=np.float64),
+            "sponge": [int(inst["ob"][k]) for k in OBC_BOUNDARIES], "width": [w] * 4,
+            "relax_inner": OBC_RELAX_INNER,
+            "relax_bound": float(inst["dt"] if relax_bound is None else relax_bound),
+            "amp": amp, "pha": pha}
+
+
 # default cap on the vertical Courant number |w| dt / DDPO of initial states
 VERTICAL_CFL = 0.5
 

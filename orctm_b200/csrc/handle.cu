@@ -6,7 +6,10 @@
 // points at a reference-counted buffer; routines never update a field in
 // place but write a fresh buffer and rebind the slot, which lets OCTIMF and
 // the state rotation of OCVTOT_NH (UOO_1 <- UOO, WO <- WNO, ...) alias buffers
-// instead of copying them.
+// instead of copying them.  The one exception, the open-boundary sponge,
+// touches a few bands of UOO / VOE: it updates them in place when no other
+// slot or pending copy holds the buffer, and copies the buffer first
+// otherwise.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -164,6 +167,12 @@ struct orctm_handle {
   std::vector<cudaEvent_t> copy_events;
   struct StepOut { int field; double* host; size_t n; };
   std::vector<StepOut> step_out;
+  // open-boundary tides and sponge (orctm_set_obc): launch arguments per
+  // variable (z, u, v), the constants in one device buffer
+  bool obc_ready = false;
+  ObcArgs obc[3] = {};
+  double* obc_buf = nullptr;
+  size_t obc_cap = 0;
   // replayed chunk of PCG iterations per precision and the variants it holds
   cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
   int pcg_graph_key[2][2] = {{-1, -1}, {-1, -1}};
@@ -1515,6 +1524,134 @@ int orctm_octdiff(orctm_handle* h) { ORCTM_ENTER(h); return r_octdiff(h); }
 int orctm_octimf(orctm_handle* h) { ORCTM_ENTER(h); return r_octimf(h); }
 int orctm_ocvisc(orctm_handle* h) { ORCTM_ENTER(h); return r_ocvisc(h); }
 int orctm_ocvtot_nh(orctm_handle* h, orctm_solve_stats* s) { ORCTM_ENTER(h); return r_ocvtot_nh(h, s); }
+
+// ---------------------------------------------------------------------------
+// Open-boundary tides and sponge (mo_obcs.f90)
+namespace {
+// points along side b (0 W, 1 E, 2 N, 3 S) of variable v (0 z, 1 u, 2 v),
+// the dimensions of OB{W,E,N,S}{Z,U,V}am (mo_obcs.f90:124-138)
+int obc_points(const orctm_handle* h, int b, int v) {
+  const int IE = h->L.ie, JE = h->L.je;
+  if (b < 2) return v == 2 ? JE + 1 : JE;
+  return v == 1 ? IE + 1 : IE;
+}
+bool obc_open(const orctm_handle* h, int b) {
+  const int sw[4] = {h->G.ob_w, h->G.ob_e, h->G.ob_n, h->G.ob_s};
+  return sw[b] != 0;
+}
+// the compute stream waits for every copy queued so far (a routine about to
+// overwrite a buffer that a pending download reads)
+int compute_after_copies(orctm_handle* h) {
+  cudaEvent_t e = h->get_event();
+  h->copy_events.push_back(e);
+  ORCTM_CUDA_OK(cudaEventRecord(e, h->cstream));
+  ORCTM_CUDA_OK(cudaStreamWaitEvent(h->stream, e, 0));
+  return ORCTM_OK;
+}
+// field f's buffer, made private to the slot (copied when shared)
+int own_buffer(orctm_handle* h, int f) {
+  if (h->refs[h->slot[f]] <= 1) return ORCTM_OK;
+  double* p;
+  int st;
+  if ((st = h->alloc(&p))) return st;
+  ORCTM_CUDA_OK(cudaMemcpyAsync(h->base(p), h->base(h->slot[f]),
+                                sizeof(double) * ((size_t)h->L.n3() + 2 * h->guard_elems()),
+                                cudaMemcpyDeviceToDevice, h->stream));
+  h->bind(f, p);
+  return ORCTM_OK;
+}
+}  // namespace
+
+int orctm_set_obc(orctm_handle* h, const orctm_obc* o) {
+  ORCTM_ENTER(h);
+  if (!o || o->ntide < 1 || o->ntide > ORCTM_OBC_MAX_TIDES || !o->period)
+    return h->fail(ORCTM_E_ARG, "orctm_set_obc: ntide out of range or no periods");
+  for (int td = 0; td < o->ntide; ++td)
+    if (!std::isfinite(o->period[td]) || o->period[td] == 0.0)
+      return h->fail(ORCTM_E_ARG, "orctm_set_obc: tidal periods must be finite and nonzero");
+  if (!std::isfinite(o->relax_inner) || !std::isfinite(o->relax_bound))
+    return h->fail(ORCTM_E_ARG, "orctm_set_obc: relaxation times must be finite");
+  const int IE = h->L.ie, JE = h->L.je;
+  size_t total = 0;
+  bool on[4];
+  for (int b = 0; b < 4; ++b) {
+    on[b] = obc_open(h, b) && o->sponge[b];
+    if (!on[b]) continue;
+    const int wmax = b < 2 ? IE : JE;
+    if (o->width[b] < 1 || o->width[b] > wmax)
+      return h->fail(ORCTM_E_ARG, "orctm_set_obc: sponge width out of range");
+    for (int v = 0; v < 3; ++v) {
+      if (!o->amp[b][v] || !o->pha[b][v])
+        return h->fail(ORCTM_E_ARG, "orctm_set_obc: missing constants of an open, sponged side");
+      total += 2 * (size_t)obc_points(h, b, v) * (size_t)o->ntide;
+    }
+  }
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
+  if (total > h->obc_cap) {
+    int st;
+    double* p;
+    if ((st = h->dev_alloc(&p, total))) return st;
+    h->obc_buf = p;
+    h->obc_cap = total;
+  }
+  // the previous constants may still be read by queued launches
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  size_t off = 0;
+  for (int v = 0; v < 3; ++v) {
+    ObcArgs& a = h->obc[v];
+    a = ObcArgs{};
+    a.ntide = o->ntide;
+    for (int td = 0; td < o->ntide; ++td) a.period[td] = o->period[td];
+    a.pi = 4.0 * std::atan(1.0);  // PI = 4.*ATAN(1.), orctm.f90:525
+    a.dt = h->G.dt;
+    // rel_uv* = rel_ts* = rel_eta* = Urelax* (mo_obcs.f90:499-506)
+    a.relb = o->relax_bound;
+    a.reli = o->relax_inner;
+    for (int b = 0; b < 4; ++b) {
+      a.on[b] = on[b] ? 1 : 0;
+      a.width[b] = on[b] ? o->width[b] : 1;
+      if (!on[b]) continue;
+      const size_t n = (size_t)obc_points(h, b, v) * (size_t)o->ntide;
+      double* amp = h->obc_buf + off;
+      double* pha = amp + n;
+      off += 2 * n;
+      ORCTM_CUDA_OK(cudaMemcpy(amp, o->amp[b][v], sizeof(double) * n, cudaMemcpyHostToDevice));
+      ORCTM_CUDA_OK(cudaMemcpy(pha, o->pha[b][v], sizeof(double) * n, cudaMemcpyHostToDevice));
+      a.side[b] = ObcSide{amp, pha, obc_points(h, b, v)};
+    }
+  }
+  h->obc_ready = true;
+  return ORCTM_OK;
+}
+
+int orctm_obc_eta(orctm_handle* h, int ldtrun) {
+  ORCTM_ENTER(h);
+  if (!h->obc_ready) return h->fail(ORCTM_E_ARG, "orctm_obc_eta: orctm_set_obc not called");
+  int st;
+  if ((st = wait_uploads(h, {ORCTM_F_ZO})) || (st = compute_after_copies(h))) return st;
+  ObcArgs a = h->obc[0];
+  a.t = (double)ldtrun * h->G.dt;  // mytime = i_step * DT
+  launch_obc_eta(h->G, a, h->zo, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+int orctm_obc_uv(orctm_handle* h, int ldtrun) {
+  ORCTM_ENTER(h);
+  if (!h->obc_ready) return h->fail(ORCTM_E_ARG, "orctm_obc_uv: orctm_set_obc not called");
+  int st;
+  if ((st = wait_uploads(h, {ORCTM_F_UOO, ORCTM_F_VOE})) || (st = own_buffer(h, ORCTM_F_UOO)) ||
+      (st = own_buffer(h, ORCTM_F_VOE)))
+    return st;
+  ObcArgs au = h->obc[1], av = h->obc[2];
+  au.t = av.t = (double)ldtrun * h->G.dt;
+  launch_obc_uv(h->G, au, av, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE], h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
 
 int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* s) {
   ORCTM_ENTER(h);

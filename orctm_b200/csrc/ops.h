@@ -29,6 +29,24 @@ struct SolverState {
   double* partials;  // [4 * max_blocks]
 };
 
+// Open-boundary tidal constants of one side for one variable (device arrays,
+// (n, ntide) column-major: OB{W,E,N,S}{Z,U,V}am / ...ph of mo_obcs.f90:40-46).
+constexpr int kObcMaxTides = 8;
+struct ObcSide {
+  const double* amp;
+  const double* pha;
+  int n;  // points along the side
+};
+// Arguments of one open-boundary sponge launch (one staggering), by value.
+struct ObcArgs {
+  int ntide;
+  double period[kObcMaxTides];
+  double pi, t, dt, relb, reli;  // PI, i_step * DT, DT, rel_*b, rel_*i
+  int on[4];                     // west, east, north, south: open and sponged
+  int width[4];                  // spongew, spongee, spongen, sponges
+  ObcSide side[4];
+};
+
 // advect.cu
 void launch_ocadpo(const Geo& G, const double* T, const double* uko, const double* vke,
                    const double* wo, const double* zo, double* out, double* tA, double* vA,
@@ -59,6 +77,12 @@ void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const dou
                    const double* uko, const double* vke, const double* avo, double* spu,
                    double* spv, double* ukv, double* vkv, double* wnv, double* u1, double* v1,
                    double* w1, double* uo, double* vo, double* wo, cudaStream_t st);
+
+// obc.cu: FORC_OBCS_ETA + SPONGE_OBCS_ETA on ZO, and FORC_OBCS_UV +
+// UPGRADE_OBCS_UV + SPONGE_OBCS_UV on UOO / VOE, in place
+void launch_obc_eta(const Geo& G, const ObcArgs& a, double* zo, cudaStream_t st);
+void launch_obc_uv(const Geo& G, const ObcArgs& au, const ObcArgs& av, double* uoo, double* voe,
+                   cudaStream_t st);
 
 // nh.cu
 void launch_nh_rhs(const Geo& G, const double* uoo, const double* uoo1, const double* voe,

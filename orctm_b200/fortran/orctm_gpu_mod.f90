@@ -29,6 +29,16 @@ module orctm_gpu_mod
      real(c_double) :: relres, relres_initial, solve_ms
   end type orctm_solve_stats
 
+  ! open-boundary tidal constants and sponge parameters; amp(v, s), pha(v, s)
+  ! with v = 1..3 (z, u, v) and s = 1..4 (west, east, north, south)
+  type, bind(c) :: orctm_obc
+     integer(c_int) :: ntide
+     type(c_ptr) :: period
+     integer(c_int) :: sponge(4), width(4)
+     real(c_double) :: relax_inner, relax_bound
+     type(c_ptr) :: amp(3, 4), pha(3, 4)
+  end type orctm_obc
+
   interface
      integer(c_int) function orctm_create(desc, h) bind(c, name="orctm_create")
        import :: c_int, c_ptr, orctm_desc
@@ -77,6 +87,21 @@ module orctm_gpu_mod
      integer(c_int) function orctm_octimf(h) bind(c, name="orctm_octimf")
        import :: c_int, c_ptr
        type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_set_obc(h, obc) bind(c, name="orctm_set_obc")
+       import :: c_int, c_ptr, orctm_obc
+       type(c_ptr), value :: h
+       type(orctm_obc), intent(in) :: obc
+     end function
+     integer(c_int) function orctm_obc_eta(h, ldtrun) bind(c, name="orctm_obc_eta")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: ldtrun
+     end function
+     integer(c_int) function orctm_obc_uv(h, ldtrun) bind(c, name="orctm_obc_uv")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: ldtrun
      end function
      integer(c_int) function orctm_ocvisc(h) bind(c, name="orctm_ocvisc")
        import :: c_int, c_ptr

@@ -170,3 +170,81 @@ def matrix(g):
                     rows.append(r); cols.append(c); vals.append(v)
     n = nx * ny * ke
     return sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+
+
+def obc_sponge(g, obc, step, x, kind):
+    """Open-boundary tide forcing + 1/x sponge (mo_obcs.f90:569-642 and
+    1561-1720 for kind "z" on ZO; 1881-2032 and 2295-2582 for "u" / "v" on
+    UOO / VOE), restated per cell from the cell's distance d to each side's
+    boundary cell: band weights s1 = w - d + 1, s2 = d - 1, and in the
+    corners the band with the smaller d (the later corner loop on equal d).
+    Returns the relaxed copy of x."""
+    IE, JE = g["ie"], g["je"]
+    ilo = 0 if kind == "u" else 1
+    jlo = 0 if kind == "v" else 1
+    mask = {"z": g["weto"], "u": g["amsuo"], "v": g["amsue"]}[kind]
+    v = "zuv".index(kind)
+    x = np.array(x, dtype=np.float64, copy=True)
+    x3 = x[:, :, None] if kind == "z" else x
+    ni, nj, nk = x3.shape
+    I = np.arange(ni)[:, None] + ilo          # Fortran indices
+    J = np.arange(nj)[None, :] + jlo
+    d = [np.broadcast_to(I + 1 if kind == "u" else I, (ni, nj)),
+         np.broadcast_to(IE - I + 1, (ni, nj)),
+         np.broadcast_to(J + 1 if kind == "v" else J, (ni, nj)),
+         np.broadcast_to(JE - J + 1, (ni, nj))]
+    ob = g["ob"]
+    on = [bool(ob[s]) and bool(obc["sponge"][b])
+          for b, s in enumerate(("west", "east", "north", "south"))]
+    w = [int(obc["width"][b]) for b in range(4)]
+    inb = [on[b] & (d[b] <= w[b]) for b in range(4)]
+    pi = 4.0 * np.arctan(1.0)
+    t = float(step) * g["dt"]
+
+    # boundary-cell masks as (ni, nj) arrays for level k (array indices)
+    def bmask(b, k):
+        m = mask[:, :, k]
+        if b == 0:
+            return np.broadcast_to(m[0:1, :], (ni, nj))
+        if b == 1:
+            return np.broadcast_to(m[ni - 1:ni, :], (ni, nj))
+        if b == 2:
+            return np.broadcast_to(m[:, 0:1], (ni, nj))
+        return np.broadcast_to(m[:, nj - 1:nj], (ni, nj))
+
+    # tidal boundary values (level-1 mask of the boundary cell)
+    zb = []
+    for b in range(4):
+        if not on[b]:
+            zb.append(np.zeros((ni, nj)))
+            continue
+        am, ph = obc["amp"][b][v], obc["pha"][b][v]
+        m1 = bmask(b, 0)[:, 0] if b >= 2 else bmask(b, 0)[0, :]
+        s = np.zeros(m1.shape)
+        for td in range(int(obc["ntide"])):
+            s = s + am[:, td] * m1 * np.cos(2.0 * pi * (t - ph[:, td]) / obc["period"][td])
+        zb.append(np.broadcast_to(s[None, :] if b < 2 else s[:, None], (ni, nj)))
+    s1 = [(w[b] - d[b] + 1).astype(np.float64) for b in range(4)]
+    s2 = [(d[b] - 1).astype(np.float64) for b in range(4)]
+    lam = []
+    for b in range(4):
+        l = (s1[b] * obc["relax_bound"] + s2[b] * obc["relax_inner"]) / float(w[b])
+        with np.errstate(divide="ignore"):
+            lam.append(np.where(l != 0.0, g["dt"] / np.where(l != 0.0, l, 1.0), 0.0))
+    anyb = inb[0] | inb[1] | inb[2] | inb[3]
+    for k in range(nk):
+        X = x3[:, :, k]
+        mi = mask[:, :, k]
+        f = []
+        for b in range(4):
+            mb = bmask(b, k)
+            obk = zb[b] if kind == "z" else zb[b] * mb
+            xr = (s1[b] * obk + s2[b] * X) / float(w[b])
+            f.append(np.where(inb[b], mb * mi * lam[b] * (xr - X), 0.0))
+        fo = f[0] + f[1] + f[2] + f[3]
+        fo = np.where(inb[0] & inb[2], np.where(d[0] < d[2], f[0], f[2]), fo)
+        fo = np.where(inb[0] & inb[3], np.where(d[0] < d[3], f[0], f[3]), fo)
+        fo = np.where(inb[1] & inb[2], np.where(d[1] < d[2], f[1], f[2]), fo)
+        fo = np.where(inb[1] & inb[3], np.where(d[1] < d[3], f[1], f[3]), fo)
+        x3[:, :, k] = np.where(anyb, X + fo, X)
+    return x

@@ -1,0 +1,106 @@
+"""Open-boundary tide forcing and sponge on the GPU (orctm_set_obc,
+orctm_obc_eta, orctm_obc_uv) against the oracle's restatement of
+mo_obcs.f90, on the reference's W+S layout and on every-side layouts with
+crossing, uneven, unsponged and zero-relaxation bands.  The kernels and the
+oracle evaluate the same expressions in the same order; they differ only
+through COS (CUDA's cos against the C library's), hence the 1e-13 bound.
+Also: a buffer shared with UKO after OCTIMF, and pending downloads, keep
+their contents."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import assert_close
+from orctm_b200 import configs as C
+from orctm_b200.api import Instance
+from test_obc import CASES, _case
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13
+
+
+def _pair(inst, obc):
+    orc = O.Oracle(inst)
+    gpu = Instance(inst)
+    st = C.copy_state(inst)
+    gpu.upload_state(st)
+    gpu.set_obc(obc)
+    return orc, gpu, st
+
+
+@pytest.mark.parametrize("kind", CASES)
+def test_obc_uv_parity(kind):
+    inst, obc = _case(kind)
+    orc, gpu, st = _pair(inst, obc)
+    for step in (1, 4321, 100000):
+        gpu.obc_uv(step)
+        orc.obc_uv(obc, step, st["uoo"], st["voe"])
+        assert_close(gpu.download("uoo"), st["uoo"], TOL, f"UOO step {step}")
+        assert_close(gpu.download("voe"), st["voe"], TOL, f"VOE step {step}")
+
+
+@pytest.mark.parametrize("kind", CASES)
+def test_obc_eta_parity(kind):
+    inst, obc = _case(kind)
+    orc, gpu, st = _pair(inst, obc)
+    for step in (3, 86400):
+        gpu.obc_eta(step)
+        orc.obc_eta(obc, step, st["zo"])
+        assert_close(gpu.download("zo"), st["zo"], TOL, f"ZO step {step}")
+
+
+def test_obc_then_step_matches_oracle():
+    """The driver's order (orctm.f90:1358-1369, 1454-1562): sponge, OCTIMF,
+    then the hot path, on the c2 layout."""
+    inst, obc = _case("reference")
+    orc, gpu, st = _pair(inst, obc)
+    gpu.obc_uv(10)
+    gpu.octimf()
+    orc.obc_uv(obc, 10, st["uoo"], st["voe"])
+    orc.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
+    for k in ("uoo", "voe", "uko", "vke"):
+        assert_close(gpu.download(k), st[k], TOL, k)
+    gpu.set_solver("fp64", rtol=1e-13, maxit=20000)
+    gpu.step_hotpath()
+    orc.step_hotpath(st, solver="direct")
+    for k in ("uoo", "voe", "wno", "pnh"):
+        assert_close(gpu.download(k), st[k], 1e-8, k)
+
+
+def test_shared_and_held_buffers_keep_their_contents():
+    inst, obc = _case("crossing")
+    _, gpu, st = _pair(inst, obc)
+    gpu.octimf()                       # UKO, VKE now share UOO's, VOE's buffers
+    u_before = gpu.download("uoo")
+    held = np.zeros(gpu.shape("voe"), order="F")
+    gpu.download_async("voe", held)    # pending download of VOE
+    z_held = np.zeros(gpu.shape("zo"), order="F")
+    gpu.download_async("zo", z_held)   # pending download of ZO
+    gpu.obc_uv(50)
+    gpu.obc_eta(50)
+    gpu.wait_copies()
+    assert np.array_equal(gpu.download("uko"), u_before)
+    assert np.array_equal(held, st["voe"])
+    assert np.array_equal(z_held, st["zo"])
+    assert not np.array_equal(gpu.download("uoo"), u_before)
+    assert not np.array_equal(gpu.download("zo"), st["zo"])
+
+
+def test_set_obc_rejects_bad_arguments():
+    inst, obc = _case("reference")
+    gpu = Instance(inst)
+    with pytest.raises(Exception):
+        gpu.obc_uv(1)                  # constants not set
+    bad = dict(obc, width=[0, 1, 1, 1])
+    with pytest.raises(Exception):
+        gpu.set_obc(bad)
+    bad = dict(obc, width=[inst["ie"] + 1, 1, 1, 1])
+    with pytest.raises(Exception):
+        gpu.set_obc(bad)
+    bad = dict(obc, ntide=9)
+    with pytest.raises(Exception):
+        gpu.set_obc(bad)
+    amp = [list(r) for r in obc["amp"]]
+    amp[0][1] = None
+    with pytest.raises(Exception):
+        gpu.set_obc(dict(obc, amp=amp))
