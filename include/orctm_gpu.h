@@ -29,6 +29,7 @@
  *   orctm_upload / orctm_download   the module arrays of MO_COMMO1
  *                                   (mo_commo1.f90:32-146) that the path reads
  *                                   and writes, moved between host and device
+ *   orctm_write_gridinfo  SUBROUTINE WRTE_GRIDINFO  wrte_gridinfo.f90:1-175
  *   orctm_build_grid    BELEG + BODEN geometry (beleg.f90:48-139,
  *                       boden.f90:38-286), a set-up helper for callers that
  *                       have no Fortran host
@@ -174,6 +175,25 @@ int orctm_write_extra(orctm_handle* h, const char* path, int append, int idate, 
                       const int* fields, const int* codes);
 int orctm_write_extra_host(const char* path, int append, int idate, int code, int nlev,
                            const int* kcodes, int iedim, const double* data);
+/* GRID_INFO.ext, the grid file of WRTE_GRIDINFO (wrte_gridinfo.f90:19-172),
+ * in the same records (IDATE 0): LONP/LATP 110/120, LONU/LATU 111/121,
+ * LONV/LATV 112/122 (degrees), DEPTO/DEUTO/DEUTE 200-202, DLXP/DLXU/DLXV
+ * 410-412 and DLYP/DLYU/DLYV 420-422 as 2D records (KCODE -100), then per
+ * level (KCODE = K) WETO/AMSUO/AMSUE 300-302 and DDPO/DDUO/DDUE 430-432.
+ * Spacings, masks and thicknesses come from the descriptor; the
+ * coordinates and depths, which the hot path does not use, from g.  The
+ * coordinates are GILA_G/GIPH_G at the points divided by PI/180, as
+ * wrte_gridinfo.f90:26-44 forms them.  Host only; truncates the file. */
+typedef struct orctm_gridinfo {
+  const double *lonp, *latp;   /* IE*JE */
+  const double *lonu, *latu;   /* (IE+1)*JE */
+  const double *lonv, *latv;   /* IE*(JE+1) */
+  const double *depto;         /* IE*JE, DEPTO after BODEN */
+  const double *deuto;         /* (IE+1)*JE */
+  const double *deute;         /* IE*(JE+1) */
+} orctm_gridinfo;
+int orctm_write_gridinfo(const char* path, const orctm_desc* desc, const orctm_gridinfo* g);
+
 /* Restart reading (the role of AUFR, aufr.f90:103-167, which reads the same
  * records in a fixed order): for each field the first records of its code
  * and level size, in file order, are read as 4-byte reals, converted to

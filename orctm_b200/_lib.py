@@ -63,6 +63,12 @@ class Obc(C.Structure):
     ]
 
 
+class GridInfo(C.Structure):
+    """orctm_gridinfo: coordinates and depths of GRID_INFO.ext."""
+    _fields_ = [(k, _D) for k in ("lonp", "latp", "lonu", "latu", "lonv", "latv", "depto",
+                                  "deuto", "deute")]
+
+
 EXPORTS = (
     "orctm_abi_version", "orctm_status_string", "orctm_last_error", "orctm_create",
     "orctm_destroy", "orctm_field_size", "orctm_upload", "orctm_download", "orctm_ocuad",
@@ -76,7 +82,7 @@ EXPORTS = (
     "orctm_estimate_device_bytes", "orctm_check_division", "orctm_ocadpo_all",
     "orctm_upload_async", "orctm_download_async", "orctm_set_step_outputs", "orctm_wait_copies",
     "orctm_write_extra", "orctm_write_extra_host", "orctm_read_extra", "orctm_read_extra_host",
-    "orctm_set_obc", "orctm_obc_eta", "orctm_obc_uv",
+    "orctm_set_obc", "orctm_obc_eta", "orctm_obc_uv", "orctm_write_gridinfo",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -124,6 +130,7 @@ def load(build_if_missing: bool = True):
                                      C.POINTER(C.c_int)]
     lib.orctm_read_extra_host.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _D,
                                           C.POINTER(C.c_int)]
+    lib.orctm_write_gridinfo.argtypes = [C.c_char_p, C.POINTER(Desc), C.POINTER(GridInfo)]
     lib.orctm_set_obc.argtypes = [C.c_void_p, C.POINTER(Obc)]
     lib.orctm_obc_eta.argtypes = [C.c_void_p, C.c_int]
     lib.orctm_obc_uv.argtypes = [C.c_void_p, C.c_int]

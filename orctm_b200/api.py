@@ -128,6 +128,29 @@ def write_obc_files(dirname: str, amp, pha) -> None:
                         os.path.join(dirname, obc_file_name(b, v, ph)))
 
 
+def write_gridinfo(path: str, inst: dict, lon: dict, lat: dict, deuto, deute) -> None:
+    """GRID_INFO.ext of an instance (WRTE_GRIDINFO, wrte_gridinfo.f90):
+    lon / lat map "p", "u", "v" to the coordinates (degrees) at those points
+    in the reference layouts; deuto / deute are the depths at u and v points
+    (DEPTO comes from the instance).  Host only."""
+    d, keep = make_desc(inst)
+    g = _lib.GridInfo()
+    arrs = {"lonp": lon["p"], "latp": lat["p"], "lonu": lon["u"], "latu": lat["u"],
+            "lonv": lon["v"], "latv": lat["v"], "depto": inst["depto"], "deuto": deuto,
+            "deute": deute}
+    shapes = {"p": (inst["ie"], inst["je"]), "u": (inst["ie"] + 1, inst["je"]),
+              "v": (inst["ie"], inst["je"] + 1)}
+    for k, a in arrs.items():
+        a = np.asfortranarray(a, dtype=np.float64)
+        want = shapes["p" if k == "depto" else k[-1] if k.startswith(("lon", "lat")) else
+                      {"deuto": "u", "deute": "v"}[k]]
+        if a.shape != want:
+            raise ValueError(f"{k}: shape {a.shape}, expected {want}")
+        keep.append(a)
+        setattr(g, k, _p(a))
+    _lib.check(_lib.load().orctm_write_gridinfo(path.encode(), C.byref(d), C.byref(g)))
+
+
 def field_id(name) -> int:
     if isinstance(name, int):
         return name

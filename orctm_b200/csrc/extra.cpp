@@ -110,3 +110,40 @@ extern "C" int orctm_read_extra_host(const char* path, int code, int nlev, int i
   fclose(f);
   return found == nlev ? ORCTM_OK : ORCTM_E_ARG;
 }
+
+// GRID_INFO.ext (WRTE_GRIDINFO, wrte_gridinfo.f90:19-172): the grid in the
+// same EXTRA records, IDATE 0, codes by the ABC rule of
+// ORCTM/code_output.txt (A 1 lon/lat, 2 depth, 3 mask, 4 spacing; B 0/1/2/3
+// none/x/y/z; C 0/1/2 p/u/v point): longitudes and latitudes 110-122, depths
+// 200-202 and spacings 410-422 as 2D records (KCODE -100), then per level
+// K = 1..KE (KCODE K) the masks 300-302 and thicknesses 430-432.
+extern "C" int orctm_write_gridinfo(const char* path, const orctm_desc* d,
+                                    const orctm_gridinfo* g) {
+  if (!path || !d || !g || d->ie < 1 || d->je < 1 || d->ke < 1) return ORCTM_E_ARG;
+  const int IE = d->ie, JE = d->je, KE = d->ke;
+  const int np = IE * JE, nu = (IE + 1) * JE, nv = IE * (JE + 1);
+  struct Rec2 { int code; int n; const double* a; };
+  const Rec2 flat[] = {
+      {110, np, g->lonp}, {120, np, g->latp}, {111, nu, g->lonu}, {121, nu, g->latu},
+      {112, nv, g->lonv}, {122, nv, g->latv}, {200, np, g->depto}, {201, nu, g->deuto},
+      {202, nv, g->deute}, {410, np, d->dlxp}, {411, nu, d->dlxu}, {412, nv, d->dlxv},
+      {420, np, d->dlyp}, {421, nu, d->dlyu}, {422, nv, d->dlyv}};
+  const Rec2 levels[] = {{300, np, d->weto}, {301, nu, d->amsuo}, {302, nv, d->amsue},
+                         {430, np, d->ddpo}, {431, nu, d->dduo}, {432, nv, d->ddue}};
+  for (const Rec2& r : flat)
+    if (!r.a) return ORCTM_E_ARG;
+  for (const Rec2& r : levels)
+    if (!r.a) return ORCTM_E_ARG;
+  std::vector<int> kc((size_t)KE);
+  for (int k = 0; k < KE; ++k) kc[(size_t)k] = k + 1;
+  const int m100 = -100;
+  bool first = true;
+  int st;
+  for (const Rec2& r : flat) {
+    if ((st = orctm_write_extra_host(path, first ? 0 : 1, 0, r.code, 1, &m100, r.n, r.a))) return st;
+    first = false;
+  }
+  for (const Rec2& r : levels)
+    if ((st = orctm_write_extra_host(path, 1, 0, r.code, KE, kc.data(), r.n, r.a))) return st;
+  return ORCTM_OK;
+}

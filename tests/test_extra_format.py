@@ -74,3 +74,34 @@ def test_host_reader_reads_oracle_file(tmp_path):
     # a code that is not there, or too few levels
     assert lib.orctm_read_extra_host(str(p).encode(), 5, 1, 66, one.ctypes.data_as(_D), None) != 0
     assert lib.orctm_read_extra_host(str(p).encode(), 1, 2, 66, out.ctypes.data_as(_D), None) != 0
+
+
+def test_gridinfo_equals_oracle_bytes(tmp_path):
+    """GRID_INFO.ext (wrte_gridinfo.f90:52-172): the library's writer against
+    the oracle's record restatement in the reference's record order."""
+    from orctm_b200 import api, configs
+
+    inst = configs.make_instance("c2", nx=11, ny=8, nz=5)
+    ie, je, ke = inst["ie"], inst["je"], inst["ke"]
+    g = np.random.Generator(np.random.PCG64(7))
+    lon = {"p": g.uniform(110, 120, (ie, je)), "u": g.uniform(110, 120, (ie + 1, je)),
+           "v": g.uniform(110, 120, (ie, je + 1))}
+    lat = {"p": g.uniform(10, 20, (ie, je)), "u": g.uniform(10, 20, (ie + 1, je)),
+           "v": g.uniform(10, 20, (ie, je + 1))}
+    deuto = g.uniform(0, 4000, (ie + 1, je))
+    deute = g.uniform(0, 4000, (ie, je + 1))
+    a, b = tmp_path / "lib.ext", tmp_path / "oracle.ext"
+    api.write_gridinfo(str(a), inst, lon, lat, deuto, deute)
+    flat = [(110, lon["p"]), (120, lat["p"]), (111, lon["u"]), (121, lat["u"]),
+            (112, lon["v"]), (122, lat["v"]), (200, inst["depto"]), (201, deuto),
+            (202, deute), (410, inst["dlxp"]), (411, inst["dlxu"]), (412, inst["dlxv"]),
+            (420, inst["dlyp"]), (421, inst["dlyu"]), (422, inst["dlyv"])]
+    recs = [(0, code, -100, v) for code, v in flat]
+    for code, key in ((300, "weto"), (301, "amsuo"), (302, "amsue"), (430, "ddpo"),
+                      (431, "dduo"), (432, "ddue")):
+        recs += [(0, code, k + 1, inst[key][:, :, k]) for k in range(ke)]
+    O.write_extra(b, recs)
+    assert a.read_bytes() == b.read_bytes()
+    back = O.read_extra(a)
+    assert len(back) == 15 + 6 * ke
+    assert [r[1] for r in back[:3]] == [110, 120, 111]
