@@ -524,32 +524,49 @@ __device__ __forceinline__ bool wet_var(const Geo& G, int ij, int K) {
 
 constexpr int kSx = 32, kSy = 8;
 
+// Block shape of a sweep: one thread per face position, so the face phase
+// is a single pass.  x sweeps: (kSx + 2) x kSy threads hold the faces of
+// kSx + 2 columns and update the kSx cells between them; y sweeps: kSx x kSy
+// threads hold kSy rows of faces and update the kSy - 2 rows between them.
+template <int DIR>
+struct Sweep {
+  static constexpr int BX = DIR == 0 ? kSx + 2 : kSx, BY = kSy;  // threads = faces
+  static constexpr int CX = kSx, CY = DIR == 0 ? kSy : kSy - 2;  // cells
+};
+
+template <int DIR>
+inline dim3 sweep_block() {
+  return dim3(Sweep<DIR>::BX, Sweep<DIR>::BY);
+}
+template <int DIR>
+inline dim3 sweep_grid(int nx, int ny, int nz) {
+  using S = Sweep<DIR>;
+  return dim3((nx + S::CX - 1) / S::CX, (ny + S::CY - 1) / S::CY, nz);
+}
+
 template <int VAR, int DIR>
-__global__ void __launch_bounds__(kSx * kSy) k_hsweep(Geo G, const double* __restrict__ T,
-                                                      const double* __restrict__ V,
-                                                      const double* __restrict__ vel,
-                                                      double* __restrict__ To,
-                                                      double* __restrict__ Vo) {
+__global__ void __launch_bounds__(Sweep<DIR>::BX * Sweep<DIR>::BY)
+    k_hsweep(Geo G, const double* __restrict__ T, const double* __restrict__ V,
+             const double* __restrict__ vel, double* __restrict__ To, double* __restrict__ Vo) {
   using R = Rng<VAR>;
-  constexpr int HX = DIR == 0 ? kSx + 2 : kSx, HY = DIR == 0 ? kSy : kSy + 2;
-  __shared__ Fl fl[HY][HX];
+  using S = Sweep<DIR>;
+  __shared__ Fl fl[S::BY][S::BX];
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   const int K = blockIdx.z + 1;
-  const int ib = blockIdx.x * kSx + R::i0, jb = blockIdx.y * kSy + R::j0;
+  const int ib = blockIdx.x * S::CX + R::i0, jb = blockIdx.y * S::CY + R::j0;
   const int iLo = R::iL, iHi = IE - R::iH, jLo = R::jL, jHi = JE - R::jH;
   const bool klev = K >= R::kL && K <= KE;
-  const int tid = threadIdx.x + kSx * threadIdx.y;
+  const int hx = threadIdx.x, hy = threadIdx.y;
   if (klev) {
-    for (int e = tid; e < HX * HY; e += kSx * kSy) {
-      const int hy = e / HX, hx = e - hy * HX;
-      const int qi = ib + hx - (DIR == 0), qj = jb + hy - (DIR == 1);
-      // only positions a cell in the update range reads
-      const bool need = DIR == 0 ? (qj >= jLo && qj <= jHi) : (qi >= iLo && qi <= iHi);
-      fl[hy][hx] = need ? face<VAR, DIR>(G, T, V, vel, qi, qj, K) : zero_fl();
-    }
+    const int qi = ib + hx - (DIR == 0), qj = jb + hy - (DIR == 1);
+    // only positions a cell in the update range reads
+    const bool need = DIR == 0 ? (qj >= jLo && qj <= jHi) : (qi >= iLo && qi <= iHi);
+    fl[hy][hx] = need ? face<VAR, DIR>(G, T, V, vel, qi, qj, K) : zero_fl();
   }
   __syncthreads();
-  const int i = ib + threadIdx.x, j = jb + threadIdx.y;
+  const int ci = hx - (DIR == 0), cj = hy - (DIR == 1);  // the thread's cell in the tile
+  if (ci < 0 || ci >= S::CX || cj < 0 || cj >= S::CY) return;
+  const int i = ib + ci, j = jb + cj;
   const int iMax = VAR == V_UAD ? IE : IE, jMax = JE;
   if (i > iMax || j > jMax) return;
   const double t = AT(T, i, j, K);
@@ -557,7 +574,6 @@ __global__ void __launch_bounds__(kSx * kSy) k_hsweep(Geo G, const double* __res
   const bool hasv = K <= KE;
   double v = hasv ? AT(V, i, j, K) : 0.0, vn = v;
   if (klev && i >= iLo && i <= iHi && j >= jLo && j <= jHi && wet_var<VAR>(G, G.L.at2(i, j), K)) {
-    const int hx = threadIdx.x + (DIR == 0), hy = threadIdx.y + (DIR == 1);
     if (DIR == 0)  // RN = V + WTP(I-1) - WTP(I) - WTM(I) + WTM(I+1)
       apply(t, v, fl[hy][hx - 1], fl[hy][hx], fl[hy][hx + 1], tn, vn);
     else           // RN = V + WTP(J+1) - WTP(J) - WTM(J) + WTM(J-1)
@@ -729,31 +745,30 @@ __device__ __forceinline__ FlN<NT> adpo_face_all(const Geo& G, const TrIO& io,
 }
 
 template <int NT, int DIR>
-__global__ void __launch_bounds__(kSx * kSy) k_hsweep_adpo_all(Geo G, TrIO io,
-                                                               const double* __restrict__ V,
-                                                               const double* __restrict__ vel,
-                                                               double* __restrict__ Vo) {
+__global__ void __launch_bounds__(Sweep<DIR>::BX * Sweep<DIR>::BY)
+    k_hsweep_adpo_all(Geo G, TrIO io, const double* __restrict__ V,
+                      const double* __restrict__ vel, double* __restrict__ Vo) {
   using R = Rng<V_ADPO>;
-  constexpr int HX = DIR == 0 ? kSx + 2 : kSx, HY = DIR == 0 ? kSy : kSy + 2;
-  __shared__ FlN<NT> fl[HY][HX];
+  using S = Sweep<DIR>;
+  __shared__ FlN<NT> fl[S::BY][S::BX];
   const int IE = G.L.ie, JE = G.L.je;
   const int K = blockIdx.z + 1;
-  const int ib = blockIdx.x * kSx + R::i0, jb = blockIdx.y * kSy + R::j0;
+  const int ib = blockIdx.x * S::CX + R::i0, jb = blockIdx.y * S::CY + R::j0;
   const int iLo = R::iL, iHi = IE - R::iH, jLo = R::jL, jHi = JE - R::jH;
-  const int tid = threadIdx.x + kSx * threadIdx.y;
-  for (int e = tid; e < HX * HY; e += kSx * kSy) {
-    const int hy = e / HX, hx = e - hy * HX;
+  const int hx = threadIdx.x, hy = threadIdx.y;
+  {
     const int qi = ib + hx - (DIR == 0), qj = jb + hy - (DIR == 1);
     const bool need = DIR == 0 ? (qj >= jLo && qj <= jHi) : (qi >= iLo && qi <= iHi);
     fl[hy][hx] = need ? adpo_face_all<NT, DIR>(G, io, V, vel, qi, qj, K) : zero_fln<NT>();
   }
   __syncthreads();
-  const int i = ib + threadIdx.x, j = jb + threadIdx.y;
+  const int ci = hx - (DIR == 0), cj = hy - (DIR == 1);  // the thread's cell in the tile
+  if (ci < 0 || ci >= S::CX || cj < 0 || cj >= S::CY) return;
+  const int i = ib + ci, j = jb + cj;
   if (i > IE || j > JE) return;
   const double v = AT(V, i, j, K);
   double vn = v;
   const bool upd = i >= iLo && i <= iHi && j >= jLo && j <= jHi && wetb(G.gp, G.L.at2(i, j), K);
-  const int hx = threadIdx.x + (DIR == 0), hy = threadIdx.y + (DIR == 1);
 #pragma unroll
   for (int n = 0; n < NT; ++n) {
     const double t = AT(io.in[n], i, j, K);
@@ -771,9 +786,6 @@ __global__ void __launch_bounds__(kSx * kSy) k_hsweep_adpo_all(Geo G, TrIO io,
 }
 
 inline dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, 1); }
-inline dim3 grid3(int nx, int ny, int nz, dim3 b) {
-  return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz);
-}
 
 }  // namespace
 
@@ -785,10 +797,9 @@ void launch_ocadpo(const Geo& G, const double* T, const double* uko, const doubl
   const dim3 bc(32, 4);
   k_adpo_z<<<grid2(IE, JE, bc), bc, 0, st>>>(G, T, wo, zo, out, vA);
   count_launch();
-  const dim3 bs(kSx, kSy);
-  k_hsweep<V_ADPO, 0><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
+  k_hsweep<V_ADPO, 0><<<sweep_grid<0>(IE, JE, KE), sweep_block<0>(), 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_hsweep<V_ADPO, 1><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_ADPO, 1><<<sweep_grid<1>(IE, JE, KE), sweep_block<1>(), 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 
@@ -801,10 +812,9 @@ void adpo_all_group(const Geo& G, TrIO zio, TrIO xio, TrIO yio, const double* uk
   const dim3 bc(32, 4);
   k_adpo_z_all<NT><<<grid2(IE, JE, bc), bc, 0, st>>>(G, zio, wo, zo, vA);
   count_launch();
-  const dim3 bs(kSx, kSy);
-  k_hsweep_adpo_all<NT, 0><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, xio, vA, uko, vB);
+  k_hsweep_adpo_all<NT, 0><<<sweep_grid<0>(IE, JE, KE), sweep_block<0>(), 0, st>>>(G, xio, vA, uko, vB);
   count_launch();
-  k_hsweep_adpo_all<NT, 1><<<grid3(IE, JE, KE, bs), bs, 0, st>>>(G, yio, vB, vke, nullptr);
+  k_hsweep_adpo_all<NT, 1><<<sweep_grid<1>(IE, JE, KE), sweep_block<1>(), 0, st>>>(G, yio, vB, vke, nullptr);
   count_launch();
 }
 }  // namespace
@@ -844,10 +854,9 @@ void launch_ocuad(const Geo& G, const double* T, const double* uko, const double
   const dim3 b(32, 4);
   k_uad_z<<<grid2(IE + 1, JE, b), b, 0, st>>>(G, T, wo, out, vA);
   count_launch();
-  const dim3 bs(kSx, kSy);
-  k_hsweep<V_UAD, 0><<<grid3(IE + 1, JE, KE, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
+  k_hsweep<V_UAD, 0><<<sweep_grid<0>(IE + 1, JE, KE), sweep_block<0>(), 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_hsweep<V_UAD, 1><<<grid3(IE + 1, JE, KE, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_UAD, 1><<<sweep_grid<1>(IE + 1, JE, KE), sweep_block<1>(), 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 
@@ -858,10 +867,9 @@ void launch_ocvad(const Geo& G, const double* T, const double* uko, const double
   const dim3 b(32, 4);
   k_vad_z<<<grid2(IE, JE + 1, b), b, 0, st>>>(G, T, wo, out, vA);
   count_launch();
-  const dim3 bs(kSx, kSy);
-  k_hsweep<V_VAD, 0><<<grid3(IE, JE + 1, KE, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
+  k_hsweep<V_VAD, 0><<<sweep_grid<0>(IE, JE + 1, KE), sweep_block<0>(), 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_hsweep<V_VAD, 1><<<grid3(IE, JE + 1, KE, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_VAD, 1><<<sweep_grid<1>(IE, JE + 1, KE), sweep_block<1>(), 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 
@@ -872,10 +880,9 @@ void launch_ocwad(const Geo& G, const double* T, const double* uko, const double
   const dim3 b(32, 4);
   k_wad_z<<<grid2(IE, JE, b), b, 0, st>>>(G, T, wo, zo, out, vA);
   count_launch();
-  const dim3 bs(kSx, kSy);
-  k_hsweep<V_WAD, 0><<<grid3(IE, JE, KE + 1, bs), bs, 0, st>>>(G, out, vA, uko, tA, vB);
+  k_hsweep<V_WAD, 0><<<sweep_grid<0>(IE, JE, KE + 1), sweep_block<0>(), 0, st>>>(G, out, vA, uko, tA, vB);
   count_launch();
-  k_hsweep<V_WAD, 1><<<grid3(IE, JE, KE + 1, bs), bs, 0, st>>>(G, tA, vB, vke, out, nullptr);
+  k_hsweep<V_WAD, 1><<<sweep_grid<1>(IE, JE, KE + 1), sweep_block<1>(), 0, st>>>(G, tA, vB, vke, out, nullptr);
   count_launch();
 }
 

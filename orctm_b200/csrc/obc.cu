@@ -5,8 +5,9 @@
 //
 // The reference forms the boundary values (tidal sums), then per open side a
 // correction array over its sponge band, sums the four arrays and lets the
-// nearer band win in the corners.  Here one thread owns one (i, j) column of
-// a staggering and does all of that for its own cells: a cell's position in a
+// nearer band win in the corners.  Here one thread owns kLz levels of one
+// (i, j) column of a staggering and does all of that for its own cells (the
+// columns' levels are split over gridDim.z): a cell's position in a
 // band is its distance d = 1, 2, ... from the boundary cell of that side
 // (west: i + 1 for u-points, i for v- and p-points; north: j + 1 for v-points,
 // j otherwise; east IE - i + 1; south JE - j + 1), which gives the weights
@@ -43,6 +44,10 @@ __device__ __forceinline__ double band_lambda(double s1, double s2, int w, const
   return l != 0.0 ? a.dt / l : 0.0;
 }
 
+// levels per thread: the band columns are few, so the levels are spread
+// over gridDim.z; a thread forms its columns' tidal sums once for kLz levels
+constexpr int kLz = 4;
+
 template <int FK>
 __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
   const int IE = G.L.ie, JE = G.L.je;
@@ -77,7 +82,8 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
     lam[b] = in[b] ? band_lambda(s1[b], s2[b], a.width[b], a) : 0.0;
   }
   const int nk = FK == FK_P ? 1 : G.L.ke;
-  for (int K = 1; K <= nk; ++K) {
+  const int k0 = (int)blockIdx.z * kLz + 1, k1 = min(nk, k0 + kLz - 1);
+  for (int K = k0; K <= k1; ++K) {
     double* px = FK == FK_P ? x + ij : x + G.L.at(i, j, K - 1);
     const double X = *px;
     // the mask products use level K of the cell and its boundary cell; ZO
@@ -107,8 +113,9 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
 template <int FK>
 void launch_one(const Geo& G, const ObcArgs& a, double* x, cudaStream_t st) {
   const int ni = FK == FK_U ? G.L.ie + 1 : G.L.ie, nj = FK == FK_V ? G.L.je + 1 : G.L.je;
+  const int nk = FK == FK_P ? 1 : G.L.ke;
   const dim3 b(32, 8);
-  k_obc_sponge<FK><<<dim3((ni + 31) / 32, (nj + 7) / 8), b, 0, st>>>(G, a, x);
+  k_obc_sponge<FK><<<dim3((ni + 31) / 32, (nj + 7) / 8, (nk + kLz - 1) / kLz), b, 0, st>>>(G, a, x);
   count_launch();
 }
 
