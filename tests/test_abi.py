@@ -84,3 +84,22 @@ def test_create_reports_missing_device():
     with pytest.raises(_lib.OrctmError) as e:
         Instance(inst)
     assert e.value.status in (-7, -2)
+
+
+def test_open_boundary_and_gridinfo_argument_checks(tmp_path):
+    """Null handles and missing arrays fail with ORCTM_E_ARG before any device
+    call; the GRID_INFO writer is host-only and refuses missing arrays."""
+    from orctm_b200 import api
+
+    lib = _lib.load()
+    o = _lib.Obc()
+    assert lib.orctm_set_obc(None, C.byref(o)) == -1
+    assert lib.orctm_obc_uv(None, 1) == -1
+    assert lib.orctm_obc_eta(None, 1) == -1
+    inst = configs.make_instance("c2", builder=grid.build_grid, nx=9, ny=7, nz=4)
+    d, keep = api.make_desc(inst)
+    g = _lib.GridInfo()                      # every coordinate pointer NULL
+    path = str(tmp_path / "GRID_INFO.ext").encode()
+    assert lib.orctm_write_gridinfo(path, C.byref(d), C.byref(g)) == -1
+    assert lib.orctm_write_gridinfo(None, C.byref(d), C.byref(g)) == -1
+    assert not (tmp_path / "GRID_INFO.ext").exists()
