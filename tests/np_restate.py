@@ -248,3 +248,77 @@ def obc_sponge(g, obc, step, x, kind):
         fo = np.where(inb[1] & inb[3], np.where(d[1] < d[3], f[1], f[3]), fo)
         x3[:, :, k] = np.where(anyb, X + fo, X)
     return x
+
+
+def octdiff(g, tracers, dvo, zo):
+    """OCTDIFF_BASE (tracer-independent factors, octdiff_base.f90:178-226)
+    and OCTDIFF_TS (octdiff_ts.f90:294-404) with AH00 <= ALMZER and no sea
+    ice: implicit vertical diffusion by the pre-eliminated tridiagonal
+    TRIDSY, then the explicit biharmonic term when AULAPTS > ALMZER.
+    Returns the diffused copies of the tracers."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    dt, almzer, aulapts = g["dt"], g["almzer"], g["aulapts"]
+    weto, ddpo, di, dzw = g["weto"], g["ddpo"], g["di"], g["dzw"]
+    dlxp, dlyp, dlxu, dlyu = g["dlxp"], g["dlyp"], g["dlxu"], g["dlyu"]
+    dlxv, dlyv = g["dlxv"], g["dlyv"]
+    I, J = slice(1, ie - 1), slice(1, je - 1)          # I = 2..IE1, J = 2..JE1
+    zzsurf = np.zeros(ke)
+    zzsurf[0] = 1.0
+    ice = 0.0                                          # RHOICWA*SICTHO + RHOSNWA*SICSNO
+    # TRIDSY, octdiff_base.f90:182-201
+    t1 = np.zeros((ie - 2, je - 2, ke))
+    t2 = np.zeros((ie - 2, je - 2, ke))
+    t3 = np.zeros((ie - 2, je - 2, ke))
+    for k in range(ke):
+        den = ddpo[I, J, k] + zzsurf[k] * (zo[I, J] - ice - ice) + almzer
+        t1[:, :, k] = -dt * dvo[I, J, k] * weto[I, J, k] * di[k] / den
+        t3[:, :, k] = -dt * dvo[I, J, k + 1] * di[k + 1] / den
+        t2[:, :, k] = 1. - t1[:, :, k] - t3[:, :, k]
+    for k in range(1, ke):
+        a = t1[:, :, k].copy()
+        t1[:, :, k - 1] = a / t2[:, :, k - 1]
+        t2[:, :, k] = t2[:, :, k] - t3[:, :, k - 1] * a / t2[:, :, k - 1]
+    out = []
+    for tr in tracers:
+        x = np.array(tr, dtype=np.float64, copy=True)
+        # implicit vertical diffusion, octdiff_ts.f90:296-323
+        r = x[I, J, :].copy()
+        for k in range(1, ke):
+            r[:, :, k] = r[:, :, k] - t1[:, :, k - 1] * r[:, :, k - 1]
+        y = np.zeros_like(r)
+        y[:, :, ke - 1] = r[:, :, ke - 1] / t2[:, :, ke - 1]
+        for l in range(ke - 2, -1, -1):
+            y[:, :, l] = (r[:, :, l] - t3[:, :, l] * y[:, :, l + 1]) / t2[:, :, l]
+        x[I, J, :] = y
+        x[I, J, :] = x[I, J, :] + 0.0                 # THTEN = 0 (AH00 <= ALMZER)
+        if aulapts > almzer:
+            # AULX(I,J) = AULAPTS*DLXU(I,J)**4, AULY(I,J) = AULAPTS*DLYV(I,J)**4
+            # (octdiff_base.f90:208-219), the power as (x*x)*(x*x).  u arrays are
+            # indexed by Fortran I (I_start = 0), v arrays by Fortran J.
+            aulx = aulapts * ((dlxu * dlxu) * (dlxu * dlxu))
+            auly = aulapts * ((dlyv * dlyv) * (dlyv * dlyv))
+            Im, Ip, Jm, Jp = slice(0, ie - 2), slice(2, ie), slice(0, je - 2), slice(2, je)
+            uW, uE = slice(1, ie - 1), slice(2, ie)      # u-point I-1 and I of p-cell I
+            vS, vN = slice(1, je - 1), slice(2, je)      # v-point J-1 and J of p-cell J
+            # Laplacian, octdiff_ts.f90:344-358 (T1O stays 0 outside 2..IE1 x 2..JE1)
+            lap = np.zeros_like(x)
+            for k in range(ke):
+                c = x[I, J, k]
+                ex = (weto[Im, J, k] * (x[Im, J, k] - c) / dlxu[uW, J]
+                      + weto[Ip, J, k] * (x[Ip, J, k] - c) / dlxu[uE, J]) / dlxp[I, J]
+                ey = (weto[I, Jm, k] * (x[I, Jm, k] - c) / dlyv[I, vS]
+                      + weto[I, Jp, k] * (x[I, Jp, k] - c) / dlyv[I, vN]) / dlyp[I, J]
+                lap[I, J, k] = weto[I, J, k] * (ex + ey)
+            # biharmonic update, octdiff_ts.f90:366-392
+            for k in range(ke):
+                L = lap[:, :, k]
+                c = L[I, J]
+                den = (ddpo[I, J, k] + almzer + zzsurf[k] * (zo[I, J] - ice - ice)) \
+                    * dlxp[I, J] * dlyp[I, J]
+                s = (weto[Im, J, k] * aulx[uW, J] * dlyu[uW, J] * (L[Im, J] - c) / dlxu[uW, J]
+                     + weto[Ip, J, k] * aulx[uE, J] * dlyu[uE, J] * (L[Ip, J] - c) / dlxu[uE, J]
+                     + weto[I, Jm, k] * auly[I, vS] * dlxv[I, vS] * (L[I, Jm] - c) / dlyv[I, vS]
+                     + weto[I, Jp, k] * auly[I, vN] * dlxv[I, vN] * (L[I, Jp] - c) / dlyv[I, vN])
+                x[I, J, k] = x[I, J, k] - (weto[I, J, k] / den) * dzw[k] * s
+        out.append(x)
+    return out

@@ -129,3 +129,13 @@ def test_solve_matches_direct():
     assert its > 0 and rel <= 1e-12
     xd = orc.direct_solve(A, b)
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) <= 1e-8
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_octdiff_matches_numpy_restatement(case):
+    inst = _inst(case)
+    st = C.copy_state(inst)
+    want = np_restate.octdiff(inst, st["tracers"], st["dvo"], st["zo"])
+    O.Oracle(inst).octdiff(st["tracers"], st["dvo"], st["zo"])
+    for n, (got, w) in enumerate(zip(st["tracers"], want)):
+        assert np.array_equal(got, w), (n, float(np.abs(got - w).max()))
