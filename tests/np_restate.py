@@ -322,3 +322,111 @@ def octdiff(g, tracers, dvo, zo):
                 x[I, J, k] = x[I, J, k] - (weto[I, J, k] / den) * dzw[k] * s
         out.append(x)
     return out
+
+
+def _mx0(x):
+    """MAX(0., x) as the Fortran intrinsic evaluates it for non-NaN x."""
+    return np.where(0.0 > x, 0.0, x)
+
+
+def _mn1(x):
+    """MIN(1., x) for non-NaN x."""
+    return np.where(x < 1.0, x, 1.0)
+
+
+def _limited(t, ta, tb, up, um, vol):
+    """The limited upwind pair of ocuad.f90:41-52 (TRP uses ta, TRM tb)."""
+    abl = np.abs(ta - tb)
+    zwabl = np.abs(ta + tb - 2. * t)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        scha = _mx0((abl - zwabl) / (abl + 1.E-20))
+        sch = _mn1(scha * vol / (up + um + 1.E-20))
+    schi = 1. - sch
+    return up * (schi * t + sch * 0.5 * (t + ta)), um * (schi * t + sch * 0.5 * (t + tb))
+
+
+def ocuad(g, uoo, uko, vke, wo):
+    """OCUAD (ocuad.f90:1-271) on u-points: the vertical, x and y sweeps of
+    the limited scheme with the boundary faces at I = 0, IE and J = 1, JE.
+    Arrays: u (IE+1, JE, KE) indexed by Fortran I and J-1; p and w by I-1,
+    J-1; v by I-1, J.  Returns the advected copy of uoo."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    dt = g["dt"]
+    amsuo, dduo, ddue = g["amsuo"], g["dduo"], g["ddue"]
+    dlxu, dlyu, dlxp, dlyp, dlxv = g["dlxu"], g["dlyu"], g["dlxp"], g["dlyp"], g["dlxv"]
+    trf = np.array(uoo, dtype=np.float64, copy=True)
+    trvol = amsuo * dlxu[:, :, None] * dlyu[:, :, None] * dduo
+    I, J = slice(1, ie), slice(1, je - 1)        # Fortran I = 1..IE1, J = 2..JE1
+    wet = amsuo[I, J, :] > 0.5
+
+    def update(rn, num):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            tr1 = num / rn
+        trf[I, J, :] = np.where(wet, tr1, trf[I, J, :])
+        trvol[I, J, :] = np.where(wet, rn, trvol[I, J, :])
+
+    # vertical sweep (ocuad.f90:33-83); TRP(K) at index K-1, TRM(K) at index K
+    trp = np.zeros((ie - 1, je - 2, ke + 1))
+    trm = np.zeros((ie - 1, je - 2, ke + 1))
+    wtp = np.zeros((ie - 1, je - 2, ke + 1))
+    wtm = np.zeros((ie - 1, je - 2, ke + 1))
+    c = 0.5 * dt * dlyp[0:ie - 1, J] * dlxp[0:ie - 1, J]     # DLYP(I,J), DLXP(I,J)
+    for k in range(ke):
+        kup, klo = max(k - 1, 0), min(k + 1, ke - 1)
+        t = trf[I, J, k]
+        wup = 0.5 * (wo[0:ie - 1, J, k] + wo[1:ie, J, k])
+        wlo = 0.5 * (wo[0:ie - 1, J, k + 1] + wo[1:ie, J, k + 1])
+        up = c * (wup + np.abs(wup))
+        um = c * (np.abs(wlo) - wlo)
+        p, m = _limited(t, trf[I, J, kup], trf[I, J, klo], up, um, trvol[I, J, k])
+        trp[:, :, k], trm[:, :, k + 1], wtp[:, :, k], wtm[:, :, k + 1] = p, m, up, um
+    V = trvol[I, J, :]
+    rn = V + wtp[:, :, 1:] - wtp[:, :, :ke] - wtm[:, :, 1:] + wtm[:, :, :ke]
+    update(rn, trf[I, J, :] * V + trp[:, :, 1:] - trp[:, :, :ke] - trm[:, :, 1:] + trm[:, :, :ke])
+
+    # x sweep (ocuad.f90:92-175): faces at u-points I = 0..IE
+    trp = np.zeros((ie + 1, je - 2, ke))
+    trm = np.zeros((ie + 1, je - 2, ke))
+    wtp = np.zeros((ie + 1, je - 2, ke))
+    wtm = np.zeros((ie + 1, je - 2, ke))
+    ud = uko[:, J, :] * dduo[:, J, :]
+    uos = 0.5 * (ud[1:ie] + ud[2:ie + 1])
+    uwe = 0.5 * (ud[0:ie - 1] + ud[1:ie])
+    up = 0.5 * dt * dlyp[1:ie, J][:, :, None] * (uos + np.abs(uos))
+    um = 0.5 * dt * (np.abs(uwe) - uwe) * dlyp[0:ie - 1, J][:, :, None]
+    p, m = _limited(trf[I, J, :], trf[2:ie + 1, J, :], trf[0:ie - 1, J, :], up, um,
+                    trvol[I, J, :])
+    trp[1:ie], trm[1:ie], wtp[1:ie], wtm[1:ie] = p, m, up, um
+    for i, uos_, uwe_, dyp, dyu in (
+            (0, 0.5 * (ud[0] + ud[1]), ud[0], dlyp[0, J], dlyu[0, J]),
+            (ie, ud[ie], 0.5 * (ud[ie - 1] + ud[ie]), dlyp[ie - 1, J], dlyu[ie, J])):
+        upb = 0.5 * dt * dyp[:, None] * (uos_ + np.abs(uos_))
+        umb = 0.5 * dt * (np.abs(uwe_) - uwe_) * dyu[:, None]
+        trp[i], trm[i], wtp[i], wtm[i] = upb * trf[i, J, :], umb * trf[i, J, :], upb, umb
+    V = trvol[I, J, :]
+    rn = V + wtp[0:ie - 1] - wtp[1:ie] - wtm[1:ie] + wtm[2:ie + 1]
+    update(rn, trf[I, J, :] * V + trp[0:ie - 1] - trp[1:ie] - trm[1:ie] + trm[2:ie + 1])
+
+    # y sweep (ocuad.f90:187-255): faces at J = 1..JE (index J-1)
+    trp = np.zeros((ie - 1, je, ke))
+    trm = np.zeros((ie - 1, je, ke))
+    wtp = np.zeros((ie - 1, je, ke))
+    wtm = np.zeros((ie - 1, je, ke))
+    vd = vke[:, :, :] * ddue                       # v index (I-1, J)
+    dx = 0.5 * (dlxv[0:ie - 1, :] + dlxv[1:ie, :])  # 0.5*(DLXV(I,J)+DLXV(I+1,J)), J = 0..JE
+    vs = 0.5 * (vd[0:ie - 1] + vd[1:ie])           # 0.5*(VKE(I,J)DDUE(I,J)+VKE(I+1,J)DDUE(I+1,J))
+    for jj in range(1, je + 1):                    # Fortran J = 1..JE
+        vsu, vno = vs[:, jj], vs[:, jj - 1]
+        upj = 0.5 * dt * dx[:, jj - 1][:, None] * (vno + np.abs(vno))
+        umj = 0.5 * dt * dx[:, jj][:, None] * (np.abs(vsu) - vsu)
+        t = trf[I, jj - 1, :]
+        if 2 <= jj <= je - 1:
+            p, m = _limited(t, trf[I, jj - 2, :], trf[I, jj, :], upj, umj, trvol[I, jj - 1, :])
+        else:
+            p, m = upj * t, umj * t
+        trp[:, jj - 1], trm[:, jj - 1], wtp[:, jj - 1], wtm[:, jj - 1] = p, m, upj, umj
+    V = trvol[I, J, :]
+    rn = V + wtp[:, 2:je] - wtp[:, 1:je - 1] - wtm[:, 1:je - 1] + wtm[:, 0:je - 2]
+    update(rn, trf[I, J, :] * V + trp[:, 2:je] - trp[:, 1:je - 1] - trm[:, 1:je - 1]
+           + trm[:, 0:je - 2])
+    return trf

@@ -139,3 +139,12 @@ def test_octdiff_matches_numpy_restatement(case):
     O.Oracle(inst).octdiff(st["tracers"], st["dvo"], st["zo"])
     for n, (got, w) in enumerate(zip(st["tracers"], want)):
         assert np.array_equal(got, w), (n, float(np.abs(got - w).max()))
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ocuad_matches_numpy_restatement(case):
+    inst = _inst(case)
+    st = C.copy_state(inst)
+    want = np_restate.ocuad(inst, st["uoo"], st["uko"], st["vke"], st["wo"])
+    O.Oracle(inst).ocuad(st["uoo"], st["uko"], st["vke"], st["wo"])
+    assert np.array_equal(st["uoo"], want), float(np.abs(st["uoo"] - want).max())
