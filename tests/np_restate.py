@@ -430,3 +430,101 @@ def ocuad(g, uoo, uko, vke, wo):
     update(rn, trf[I, J, :] * V + trp[:, 2:je] - trp[:, 1:je - 1] - trm[:, 1:je - 1]
            + trm[:, 0:je - 2])
     return trf
+
+
+def ocvad(g, voe, uko, vke, wo):
+    """OCVAD (ocvad.f90:1-271) on v-points, the transposed OCUAD with its own
+    edge faces at I = 1, IE and J = 0, JE.  The J = 0 face reads DLXU(I,0),
+    outside DLXU (ocvad.f90:211); as in the oracle, DLXV(I,0) stands in.
+    Arrays: v (IE, JE+1, KE) indexed by I-1 and Fortran J; u by I and J-1;
+    p and w by I-1, J-1.  Returns the advected copy of voe."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    dt = g["dt"]
+    amsue, dduo, ddue = g["amsue"], g["dduo"], g["ddue"]
+    dlxv, dlyv, dlxp, dlyp, dlyu, dlxu = (g["dlxv"], g["dlyv"], g["dlxp"], g["dlyp"],
+                                          g["dlyu"], g["dlxu"])
+    trf = np.array(voe, dtype=np.float64, copy=True)
+    trvol = amsue * dlxv[:, :, None] * dlyv[:, :, None] * ddue
+    I, J = slice(1, ie - 1), slice(1, je)        # Fortran I = 2..IE1, J = 1..JE1
+    pI, pJ = slice(1, ie - 1), slice(0, je - 1)  # p-point I-1, J-1 of those cells
+    wet = amsue[I, J, :] > 0.5
+
+    def update(rn, num):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            tr1 = num / rn
+        trf[I, J, :] = np.where(wet, tr1, trf[I, J, :])
+        trvol[I, J, :] = np.where(wet, rn, trvol[I, J, :])
+
+    # vertical sweep: TRP(K) at index K-1, TRM(K) at index K
+    trp = np.zeros((ie - 2, je - 1, ke + 1))
+    trm = np.zeros((ie - 2, je - 1, ke + 1))
+    wtp = np.zeros((ie - 2, je - 1, ke + 1))
+    wtm = np.zeros((ie - 2, je - 1, ke + 1))
+    c = 0.5 * dt * dlyp[pI, pJ] * dlxp[pI, pJ]
+    for k in range(ke):
+        kup, klo = max(k - 1, 0), min(k + 1, ke - 1)
+        wup = 0.5 * (wo[pI, 0:je - 1, k] + wo[pI, 1:je, k])
+        wlo = 0.5 * (wo[pI, 0:je - 1, k + 1] + wo[pI, 1:je, k + 1])
+        up = c * (wup + np.abs(wup))
+        um = c * (np.abs(wlo) - wlo)
+        p, m = _limited(trf[I, J, k], trf[I, J, kup], trf[I, J, klo], up, um, trvol[I, J, k])
+        trp[:, :, k], trm[:, :, k + 1], wtp[:, :, k], wtm[:, :, k + 1] = p, m, up, um
+    V = trvol[I, J, :]
+    rn = V + wtp[:, :, 1:] - wtp[:, :, :ke] - wtm[:, :, 1:] + wtm[:, :, :ke]
+    update(rn, trf[I, J, :] * V + trp[:, :, 1:] - trp[:, :, :ke] - trm[:, :, 1:] + trm[:, :, :ke])
+
+    # x sweep: faces at v-point I = 1..IE (index I-1)
+    trp = np.zeros((ie, je - 1, ke))
+    trm = np.zeros((ie, je - 1, ke))
+    wtp = np.zeros((ie, je - 1, ke))
+    wtm = np.zeros((ie, je - 1, ke))
+    ud = uko * dduo                                   # u index (I, J-1)
+    uu = 0.5 * (ud[:, 0:je - 1] + ud[:, 1:je])        # at v-row J: UKO(I,J), UKO(I,J+1)
+    dyu = 0.5 * (dlyu[:, 0:je - 1] + dlyu[:, 1:je])   # 0.5*(DLYU(I,J)+DLYU(I,J+1))
+    for ii in range(1, ie + 1):                        # Fortran I = 1..IE
+        uos, uwe = uu[ii], uu[ii - 1]
+        upi = 0.5 * dt * dyu[ii][:, None] * (uos + np.abs(uos))
+        umi = 0.5 * dt * (np.abs(uwe) - uwe) * dyu[ii - 1][:, None]
+        t = trf[ii - 1, J, :]
+        if 2 <= ii <= ie - 1:
+            p, m = _limited(t, trf[ii, J, :], trf[ii - 2, J, :], upi, umi, trvol[ii - 1, J, :])
+        else:
+            p, m = upi * t, umi * t
+        trp[ii - 1], trm[ii - 1], wtp[ii - 1], wtm[ii - 1] = p, m, upi, umi
+    V = trvol[I, J, :]
+    rn = V + wtp[0:ie - 2] - wtp[1:ie - 1] - wtm[1:ie - 1] + wtm[2:ie]
+    update(rn, trf[I, J, :] * V + trp[0:ie - 2] - trp[1:ie - 1] - trm[1:ie - 1] + trm[2:ie])
+
+    # y sweep: faces at v-point J = 0..JE
+    trp = np.zeros((ie - 2, je + 1, ke))
+    trm = np.zeros((ie - 2, je + 1, ke))
+    wtp = np.zeros((ie - 2, je + 1, ke))
+    wtm = np.zeros((ie - 2, je + 1, ke))
+    vd = vke[I] * ddue[I]                              # (IE-2, JE+1, KE), index Fortran J
+    for jj in range(0, je + 1):
+        t = trf[I, jj, :]
+        if jj == 0:
+            vno = vd[:, 0]
+            vsu = 0.5 * (vd[:, 0] + vd[:, 1])
+            upj = 0.5 * dt * dlxv[I, 0][:, None] * (vno + np.abs(vno))     # DLXU(I,0) in ref
+            umj = 0.5 * dt * dlxp[pI, 0][:, None] * (np.abs(vsu) - vsu)
+        elif jj == je:
+            vno = 0.5 * (vd[:, je] + vd[:, je - 1])
+            vsu = vd[:, je]
+            upj = 0.5 * dt * dlxp[pI, je - 1][:, None] * (vno + np.abs(vno))
+            umj = 0.5 * dt * dlxu[2:ie, je - 1][:, None] * (np.abs(vsu) - vsu)
+        else:
+            vno = 0.5 * (vd[:, jj] + vd[:, jj - 1])
+            vsu = 0.5 * (vd[:, jj] + vd[:, jj + 1])
+            upj = 0.5 * dt * dlxp[pI, jj - 1][:, None] * (vno + np.abs(vno))
+            umj = 0.5 * dt * dlxp[pI, jj][:, None] * (np.abs(vsu) - vsu)
+        if 1 <= jj <= je - 1:
+            p, m = _limited(t, trf[I, jj - 1, :], trf[I, jj + 1, :], upj, umj, trvol[I, jj, :])
+        else:
+            p, m = upj * t, umj * t
+        trp[:, jj], trm[:, jj], wtp[:, jj], wtm[:, jj] = p, m, upj, umj
+    V = trvol[I, J, :]
+    rn = V + wtp[:, 2:je + 1] - wtp[:, 1:je] - wtm[:, 1:je] + wtm[:, 0:je - 1]
+    update(rn, trf[I, J, :] * V + trp[:, 2:je + 1] - trp[:, 1:je] - trm[:, 1:je]
+           + trm[:, 0:je - 1])
+    return trf

@@ -148,3 +148,12 @@ def test_ocuad_matches_numpy_restatement(case):
     want = np_restate.ocuad(inst, st["uoo"], st["uko"], st["vke"], st["wo"])
     O.Oracle(inst).ocuad(st["uoo"], st["uko"], st["vke"], st["wo"])
     assert np.array_equal(st["uoo"], want), float(np.abs(st["uoo"] - want).max())
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ocvad_matches_numpy_restatement(case):
+    inst = _inst(case)
+    st = C.copy_state(inst)
+    want = np_restate.ocvad(inst, st["voe"], st["uko"], st["vke"], st["wo"])
+    O.Oracle(inst).ocvad(st["voe"], st["uko"], st["vke"], st["wo"])
+    assert np.array_equal(st["voe"], want), float(np.abs(st["voe"] - want).max())
