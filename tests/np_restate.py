@@ -528,3 +528,127 @@ def ocvad(g, voe, uko, vke, wo):
     update(rn, trf[I, J, :] * V + trp[:, 2:je + 1] - trp[:, 1:je] - trm[:, 1:je]
            + trm[:, 0:je - 1])
     return trf
+
+
+def ocwad(g, wno, uko, vke, wo, zo):
+    """OCWAD (ocwad.f90:1-238) on w-points, levels 2..KE updated.  The
+    limiter's MIN(WETO(I,J,KLO), ...) reads WETO(KEP), one level past WETO
+    (ocwad.f90:63); as in the oracle it is taken as 0.  The x and y sweeps
+    reuse the flux arrays of the vertical step, whose edge faces (I = 1, IE;
+    J = 1, JE) are 0 on levels 2..KE.  Arrays: w (IE, JE, KE+1) and p by
+    I-1, J-1; u by I, J-1; v by I-1, J.  Returns the advected copy of wno."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    dt = g["dt"]
+    weto, ddpo, dduo, ddue = g["weto"], g["ddpo"], g["dduo"], g["ddue"]
+    dlxp, dlyp, dlyu, dlxv = g["dlxp"], g["dlyp"], g["dlyu"], g["dlxv"]
+    trf = np.array(wno, dtype=np.float64, copy=True)
+    I, J = slice(1, ie - 1), slice(1, je - 1)        # Fortran 2..IE1, 2..JE1
+    wet_k = np.concatenate([weto, np.zeros((ie, je, 1))], axis=2)  # WETO(KEP) := 0
+    # S1O, ocwad.f90:24-36
+    a = weto * dlxp[:, :, None] * dlyp[:, :, None]
+    s1o = np.empty((ie, je, ke))
+    s1o[:, :, 0] = a[:, :, 0] * (ddpo[:, :, 0] + zo) / 2.0
+    if ke > 1:
+        s1o[:, :, 1] = a[:, :, 1] * (ddpo[:, :, 0] + ddpo[:, :, 1] + zo) / 2.0
+    for k in range(2, ke):
+        s1o[:, :, k] = a[:, :, k] * (ddpo[:, :, k - 1] + ddpo[:, :, k]) / 2.0
+
+    def update(k, rn, num):
+        wet = weto[I, J, k] > 0.5
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t1 = num / rn
+        trf[I, J, k] = np.where(wet, t1, trf[I, J, k])
+        s1o[I, J, k] = np.where(wet, rn, s1o[I, J, k])
+
+    # vertical (ocwad.f90:44-103): TRP(K), WTP(K) at index K-1 (K = 1..KEP);
+    # TRM(K), WTM(K) at index K (K = 0..KE); all zero but what is set below
+    trp = np.zeros((ie, je, ke + 1))
+    trm = np.zeros((ie, je, ke + 1))
+    wtp = np.zeros((ie, je, ke + 1))
+    wtm = np.zeros((ie, je, ke + 1))
+    c = 0.5 * dt * dlyp * dlxp
+    for k in range(1, ke):                          # Fortran K = 2..KE
+        kup, klo = k - 1, k + 1
+        t, tu, tl = trf[I, J, k], trf[I, J, kup], trf[I, J, klo]
+        abl = np.abs(tu - tl)
+        zwabl = np.abs(tu + tl - 2. * t)
+        wup = 0.5 * (wo[I, J, k] + wo[I, J, kup])
+        wum = 0.5 * (wo[I, J, k] + wo[I, J, klo])
+        up = c[I, J] * (wup + np.abs(wup))
+        um = c[I, J] * (np.abs(wum) - wum)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scha = _mx0((abl - zwabl) / (abl + 1.E-20))
+            x = scha * s1o[I, J, k] / (up + um + 1.E-20)
+        cap = wet_k[I, J, klo]
+        sch = np.where(x < cap, x, cap)
+        schi = 1. - sch
+        trp[I, J, k] = up * (schi * t + sch * 0.5 * (t + tu))
+        trm[I, J, k + 1] = um * (schi * t + sch * 0.5 * (t + tl))
+        wtp[I, J, k], wtm[I, J, k + 1] = up, um
+    wup = 0.5 * (wo[:, :, ke] + wo[:, :, ke - 1])
+    up = c * (wup + np.abs(wup))
+    trp[:, :, ke] = up * (0.5 * (trf[:, :, ke - 1] + trf[:, :, ke]))
+    wtp[:, :, ke] = up
+    wum = 0.5 * (wo[:, :, 0] + wo[:, :, 1])
+    um = c * (np.abs(wum) - wum)
+    trm[:, :, 1] = um * (0.5 * (trf[:, :, 0] + trf[:, :, 1]))
+    wtm[:, :, 1] = um
+    for k in range(1, ke):
+        rn = s1o[I, J, k] + wtp[I, J, k + 1] - wtp[I, J, k] - wtm[I, J, k + 1] + wtm[I, J, k]
+        update(k, rn, trf[I, J, k] * s1o[I, J, k] + trp[I, J, k + 1] - trp[I, J, k]
+               - trm[I, J, k + 1] + trm[I, J, k])
+
+    # x sweep (ocwad.f90:110-164): interior faces overwrite the arrays
+    trp, trm, wtp, wtm = trp[:, :, :ke], trm[:, :, 1:], wtp[:, :, :ke], wtm[:, :, 1:]
+    trp, trm, wtp, wtm = (np.array(a_, copy=True) for a_ in (trp, trm, wtp, wtm))
+    for arr in (trp, trm, wtp, wtm):               # levels 2..KE: edges are 0
+        arr[0, :, 1:] = 0.0
+        arr[ie - 1, :, 1:] = 0.0
+    ud = uko * dduo
+    for k in range(1, ke):
+        t, te, tw = trf[I, J, k], trf[2:ie, J, k], trf[0:ie - 2, J, k]
+        abl = np.abs(te - tw)
+        zwabl = np.abs(te + tw - 2. * t)
+        uos = 0.5 * (ud[2:ie, J, k] + ud[2:ie, J, k - 1])
+        uwe = 0.5 * (ud[1:ie - 1, J, k] + ud[1:ie - 1, J, k - 1])
+        up = 0.5 * dt * dlyu[2:ie, J] * (uos + np.abs(uos))
+        um = 0.5 * dt * dlyu[1:ie - 1, J] * (np.abs(uwe) - uwe)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scha = _mx0((abl - zwabl) / (abl + 1.E-20)) * weto[I, J, k] \
+                * weto[2:ie, J, k] * weto[0:ie - 2, J, k]
+            sch = _mn1(scha * s1o[I, J, k] / (up + um + 1.E-20))
+        schi = 1. - sch
+        trp[I, J, k] = up * (schi * t + sch * 0.5 * (t + te))
+        trm[I, J, k] = um * (schi * t + sch * 0.5 * (t + tw))
+        wtp[I, J, k], wtm[I, J, k] = up, um
+    for k in range(1, ke):
+        rn = s1o[I, J, k] + wtp[0:ie - 2, J, k] - wtp[I, J, k] - wtm[I, J, k] + wtm[2:ie, J, k]
+        update(k, rn, trf[I, J, k] * s1o[I, J, k] + trp[0:ie - 2, J, k] - trp[I, J, k]
+               - trm[I, J, k] + trm[2:ie, J, k])
+
+    # y sweep (ocwad.f90:171-227)
+    for arr in (trp, trm, wtp, wtm):
+        arr[:, 0, 1:] = 0.0
+        arr[:, je - 1, 1:] = 0.0
+    vd = vke * ddue
+    for k in range(1, ke):
+        t, tn, ts = trf[I, J, k], trf[I, 0:je - 2, k], trf[I, 2:je, k]
+        abl = np.abs(tn - ts)
+        zwabl = np.abs(tn + ts - 2. * t)
+        vsu = 0.5 * (vd[I, 2:je, k] + vd[I, 2:je, k - 1])
+        vno = 0.5 * (vd[I, 1:je - 1, k] + vd[I, 1:je - 1, k - 1])
+        up = 0.5 * dt * dlxv[I, 1:je - 1] * (vno + np.abs(vno))
+        um = 0.5 * dt * dlxv[I, 2:je] * (np.abs(vsu) - vsu)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scha = _mx0((abl - zwabl) / (abl + 1.E-20)) * weto[I, J, k] \
+                * weto[I, 0:je - 2, k] * weto[I, 2:je, k]
+            sch = _mn1(scha * s1o[I, J, k] / (up + um + 1.E-20))
+        schi = 1. - sch
+        trp[I, J, k] = up * (schi * t + sch * 0.5 * (t + tn))
+        trm[I, J, k] = um * (schi * t + sch * 0.5 * (t + ts))
+        wtp[I, J, k], wtm[I, J, k] = up, um
+    for k in range(1, ke):
+        rn = s1o[I, J, k] + wtp[I, 2:je, k] - wtp[I, J, k] - wtm[I, J, k] + wtm[I, 0:je - 2, k]
+        update(k, rn, trf[I, J, k] * s1o[I, J, k] + trp[I, 2:je, k] - trp[I, J, k]
+               - trm[I, J, k] + trm[I, 0:je - 2, k])
+    return trf

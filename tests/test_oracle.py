@@ -157,3 +157,14 @@ def test_ocvad_matches_numpy_restatement(case):
     want = np_restate.ocvad(inst, st["voe"], st["uko"], st["vke"], st["wo"])
     O.Oracle(inst).ocvad(st["voe"], st["uko"], st["vke"], st["wo"])
     assert np.array_equal(st["voe"], want), float(np.abs(st["voe"] - want).max())
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ocwad_matches_numpy_restatement(case):
+    inst = _inst(case)
+    st = C.copy_state(inst)
+    w0 = st["wno"].copy()
+    want = np_restate.ocwad(inst, st["wno"], st["uko"], st["vke"], st["wo"], st["zo"])
+    O.Oracle(inst).ocwad(st["wno"], st["uko"], st["vke"], st["wo"], st["zo"])
+    assert np.array_equal(st["wno"], want), float(np.abs(st["wno"] - want).max())
+    assert not np.array_equal(st["wno"], w0)
