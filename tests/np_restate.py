@@ -652,3 +652,61 @@ def ocwad(g, wno, uko, vke, wo, zo):
         update(k, rn, trf[I, J, k] * s1o[I, J, k] + trp[I, 2:je, k] - trp[I, J, k]
                - trm[I, J, k] + trm[I, 0:je - 2, k])
     return trf
+
+
+def nh_rhs(g, uoo, uoo1, voe, voe1, wno, wno1, zo):
+    """OCVTOT_NH up to the solve (ocvtot_nh.f90:11-62) and ComputeRHS with
+    CG2D4NONHY off (mo_petsc.f90:298-376): DIVG*WETO over I = 2..IE1,
+    J = 2..JE1, K = 1..KE in DMDA natural order (x fastest)."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    dt = g["dt"]
+    gu = (uoo - uoo1) / dt
+    gv = (voe - voe1) / dt
+    gw = (wno - wno1) / dt
+    divgu = (gu[1:ie + 1] - gu[0:ie]) / g["dlxp"][:, :, None]
+    divgv = (gv[:, 0:je] - gv[:, 1:je + 1]) / g["dlyp"][:, :, None]
+    dd = np.maximum(g["ddpo"], 1.E-3)
+    divgw = np.empty((ie, je, ke))
+    divgw[:, :, 1:] = (gw[:, :, 1:ke] - gw[:, :, 2:ke + 1]) / dd[:, :, 1:]
+    divgw[:, :, 0] = (gw[:, :, 0] - gw[:, :, 1]) / (dd[:, :, 0] + zo)
+    divg = divgu + divgv + divgw
+    rhs = divg[1:ie - 1, 1:je - 1, :] * g["weto"][1:ie - 1, 1:je - 1, :]
+    return rhs.reshape(-1, order="F")
+
+
+def nh_post(g, x, pnh, uoo, voe):
+    """OCVTOT_NH after the solve (ocvtot_nh.f90:150-255; mo_petsc.f90:223-227
+    writes the solution into PNH's interior): open-boundary fill of PNH, u/v
+    corrected by the PNH gradient, WNO re-integrated from the bottom, and the
+    rotation UOO_1 = UOO, VOE_1 = VOE, WNO_1 = WO = WNO.  Returns (pnh, uoo,
+    voe, wno) as new arrays."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    ob = g["ob"]
+    pnh = np.array(pnh, copy=True)
+    uoo = np.array(uoo, copy=True)
+    voe = np.array(voe, copy=True)
+    pnh[1:ie - 1, 1:je - 1, :] = np.asarray(x).reshape((ie - 2, je - 2, ke), order="F")
+    if ob["west"]:
+        pnh[0, 1:je - 1, :] = pnh[1, 1:je - 1, :]
+    if ob["east"]:
+        pnh[ie - 1, 1:je - 1, :] = pnh[ie - 2, 1:je - 1, :]
+    if ob["north"]:
+        pnh[:, 0, :] = pnh[:, 1, :]
+    if ob["south"]:
+        pnh[:, je - 1, :] = pnh[:, je - 2, :]
+    J = slice(1, je - 1)
+    uoo[1:ie, J, :] = uoo[1:ie, J, :] + g["amsuo"][1:ie, J, :] * g["dtdxuo"][1:ie, J][:, :, None] \
+        * (pnh[0:ie - 1, J, :] - pnh[1:ie, J, :])
+    I = slice(1, ie - 1)
+    voe[I, 1:je, :] = voe[I, 1:je, :] + g["amsue"][I, 1:je, :] * g["dpye"][I, 1:je][:, :, None] \
+        * (pnh[I, 1:je, :] - pnh[I, 0:je - 1, :])
+    dti = 1. / g["dt"]
+    ud = uoo * g["dduo"] * g["dlyu"][:, :, None]
+    vd = voe * g["ddue"] * g["dlxv"][:, :, None]
+    wno = np.zeros((ie, je, ke + 1))
+    weto = g["weto"]
+    for k in range(ke - 1, -1, -1):
+        t1 = dti * weto[:, :, k] * (g["dtdxpo"] * (ud[0:ie, :, k] - ud[1:ie + 1, :, k]) / g["dlyp"])
+        t2 = dti * weto[:, :, k] * (+ g["dtdyo"] * (vd[:, 1:je + 1, k] - vd[:, 0:je, k]) / g["dlxp"])
+        wno[:, :, k] = wno[:, :, k + 1] + t1 + t2
+    return pnh, uoo, voe, wno

@@ -168,3 +168,25 @@ def test_ocwad_matches_numpy_restatement(case):
     O.Oracle(inst).ocwad(st["wno"], st["uko"], st["vke"], st["wo"], st["zo"])
     assert np.array_equal(st["wno"], want), float(np.abs(st["wno"] - want).max())
     assert not np.array_equal(st["wno"], w0)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ocvtot_nh_parts_match_numpy_restatement(case):
+    inst = _inst(case)
+    st = C.copy_state(inst)
+    orc = O.Oracle(inst)
+    b = orc.nh_rhs(st["uoo"], st["uoo1"], st["voe"], st["voe1"], st["wno"], st["wno1"],
+                   st["zo"])
+    want = np_restate.nh_rhs(inst, st["uoo"], st["uoo1"], st["voe"], st["voe1"], st["wno"],
+                             st["wno1"], st["zo"])
+    assert np.array_equal(b, want)
+    assert np.abs(b).max() > 0
+    x = np.random.Generator(np.random.PCG64(3)).normal(0.0, 1.0, b.size)
+    pnh, uoo, voe, wno = np_restate.nh_post(inst, x, st["pnh"], st["uoo"], st["voe"])
+    orc.nh_post(x, st["pnh"], st["uoo"], st["voe"], st["wno"], st["uoo1"], st["voe1"],
+                st["wno1"], st["wo"])
+    for name, got, w in (("pnh", st["pnh"], pnh), ("uoo", st["uoo"], uoo),
+                         ("voe", st["voe"], voe), ("wno", st["wno"], wno),
+                         ("uoo1", st["uoo1"], uoo), ("voe1", st["voe1"], voe),
+                         ("wno1", st["wno1"], wno), ("wo", st["wo"], wno)):
+        assert np.array_equal(got, w), (name, float(np.abs(got - w).max()))
