@@ -710,3 +710,262 @@ def nh_post(g, x, pnh, uoo, voe):
         t2 = dti * weto[:, :, k] * (+ g["dtdyo"] * (vd[:, 1:je + 1, k] - vd[:, 0:je, k]) / g["dlxp"])
         wno[:, :, k] = wno[:, :, k + 1] + t1 + t2
     return pnh, uoo, voe, wno
+
+
+def _fmx(a, b):
+    """Fortran MAX(a, b) for non-NaN operands (a when not b > a)."""
+    return np.where(a > b, a, b)
+
+
+def _col_solve(t1, t2, t3, rhs, mask, k0):
+    """Pre-eliminated tridiagonal column solve of ocvisc.f90:142-160 over
+    levels k0..KE-1 (0-based): t1, t2, t3 (..., KE) are TRIDSY(:,1..3) after
+    the elimination; returns the solution times the masks as the reference
+    forms it."""
+    ke = rhs.shape[-1]
+    r = rhs.copy()
+    for k in range(k0 + 1, ke):
+        r[..., k] = r[..., k] - t1[..., k - 1] * r[..., k - 1]
+    x = np.zeros_like(r)
+    x[..., ke - 1] = mask[..., ke - 1] * r[..., ke - 1] / t2[..., ke - 1]
+    for l in range(ke - 2, k0 - 1, -1):
+        x[..., l] = (r[..., l] - t3[..., l] * x[..., l + 1]) * mask[..., l] / t2[..., l]
+    return x
+
+
+def _eliminate(t1, t2, t3, k0):
+    ke = t1.shape[-1]
+    for k in range(k0 + 1, ke):
+        a = t1[..., k].copy()
+        t1[..., k - 1] = a / t2[..., k - 1]
+        t2[..., k] = t2[..., k] - t3[..., k - 1] * a / t2[..., k - 1]
+
+
+def ocvisc(g, uoo, voe, wno, uko, vke, avo):
+    """OCVISC with FREESLIP and NON_HYDROSTATIC (ocvisc.f90:37-767): bottom
+    speeds, implicit vertical diffusion of u, v (with quadratic bottom
+    friction) and w, biharmonic horizontal diffusion, then OCTIMF.  Returns
+    (uoo, voe, wno, uko, vke) as new arrays.  u arrays are indexed by
+    Fortran I and J-1, v by I-1 and J, p and w by I-1 and J-1."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    dt, almzer, aulapuv = g["dt"], g["almzer"], g["aulapuv"]
+    amsuo, amsue, weto = g["amsuo"], g["amsue"], g["weto"]
+    dduo, ddue, ddpo, di = g["dduo"], g["ddue"], g["ddpo"], g["di"]
+    dlxp, dlyp, dlxu, dlyu, dlxv, dlyv = (g["dlxp"], g["dlyp"], g["dlxu"], g["dlyu"],
+                                          g["dlxv"], g["dlyv"])
+    uoo = np.array(uoo, copy=True)
+    voe = np.array(voe, copy=True)
+    wno = np.array(wno, copy=True)
+    uko = np.array(uko, copy=True)
+    vke = np.array(vke, copy=True)
+    mv10 = g["dzw"][0] / 10.0
+    minvalue = mv10 if mv10 < 1.0 else 1.0              # MIN(1.0, DZW(1)/10.0)
+    bofric = rayfric = 3.E-3
+
+    # bottom speeds (ocvisc.f90:49-102): SPEEDU on u-points I = 1..IE1,
+    # J = 2..JE1; SPEEDV on v-points I = 2..IE1, J = 1..JE1
+    speedu = np.zeros((ie + 1, je))
+    speedv = np.zeros((ie, je + 1))
+    uI, uJ = slice(1, ie), slice(1, je - 1)
+    for k in range(ke):
+        bot = amsuo[uI, uJ, k] > 0.5 if k == ke - 1 else \
+            (amsuo[uI, uJ, k] - amsuo[uI, uJ, k + 1]) > 0.5
+        q = 0.25 * (voe[0:ie - 1, 2:je, k] + voe[1:ie, 2:je, k] + voe[0:ie - 1, 1:je - 1, k]
+                    + voe[1:ie, 1:je - 1, k])
+        u = uoo[uI, uJ, k]
+        s = _fmx(np.sqrt(u * u + q * q), 1.E-3)
+        speedu[uI, uJ] = np.where(bot, s, speedu[uI, uJ])
+    vI, vJ = slice(1, ie - 1), slice(1, je)
+    for k in range(ke):
+        bot = amsue[vI, vJ, k] > 0.5 if k == ke - 1 else \
+            (amsue[vI, vJ, k] - amsue[vI, vJ, k + 1]) > 0.5
+        q = 0.25 * (uoo[2:ie, 0:je - 1, k] + uoo[1:ie - 1, 0:je - 1, k] + uoo[2:ie, 1:je, k]
+                    + uoo[1:ie - 1, 1:je, k])
+        v = voe[vI, vJ, k]
+        s = _fmx(np.sqrt(v * v + q * q), 1.E-3)
+        speedv[vI, vJ] = np.where(bot, s, speedv[vI, vJ])
+
+    def uv_tridsy(avo_a, avo_b, m, dd, sp):
+        """TRIDSY of ocvisc.f90:113-140 / 165-190 for one staggering."""
+        n = m.shape[:-1]
+        t1, t2, t3 = np.zeros(n + (ke,)), np.zeros(n + (ke,)), np.zeros(n + (ke,))
+        for k in range(ke):
+            avup = 0.5 * (avo_a[..., k] + avo_b[..., k]) * m[..., k]
+            if k < ke - 1:
+                avlo = 0.5 * (avo_a[..., k + 1] + avo_b[..., k + 1]) * m[..., k + 1] \
+                    + (bofric + rayfric * dd[..., k] * sp) * (m[..., k] - m[..., k + 1])
+            else:
+                avlo = (bofric + rayfric * dd[..., k] * sp) * m[..., k]
+            den = almzer + dd[..., k]
+            t1[..., k] = -dt * avup * m[..., k] * di[k] / den
+            t3[..., k] = -dt * avlo * m[..., k] * di[k + 1] / den
+            t2[..., k] = 1. - t1[..., k] - t3[..., k]
+            t3[..., k] = t3[..., k] * m[..., k + 1] if k < ke - 1 else 0.0
+        _eliminate(t1, t2, t3, 0)
+        return t1, t2, t3
+
+    # V (ocvisc.f90:108-164): v-points I = 2..IE1, J = 1..JE1
+    t1, t2, t3 = uv_tridsy(avo[1:ie - 1, 0:je - 1, :], avo[1:ie - 1, 1:je, :], amsue[vI, vJ, :],
+                           ddue[vI, vJ, :], speedv[vI, vJ])
+    vke[vI, vJ, :] = _col_solve(t1, t2, t3, voe[vI, vJ, :], amsue[vI, vJ, :], 0)
+    # U (ocvisc.f90:166-215): u-points I = 1..IE1, J = 2..JE1
+    t1, t2, t3 = uv_tridsy(avo[0:ie - 1, uJ, :], avo[1:ie, uJ, :], amsuo[uI, uJ, :],
+                           dduo[uI, uJ, :], speedu[uI, uJ])
+    uko[uI, uJ, :] = _col_solve(t1, t2, t3, uoo[uI, uJ, :], amsuo[uI, uJ, :], 0)
+    # W (ocvisc.f90:223-271): p-points I = 2..IE1, J = 2..JE1, levels 2..KE
+    pI, pJ = slice(1, ie - 1), slice(1, je - 1)
+    a, w, dp = avo[pI, pJ, :], weto[pI, pJ, :], ddpo[pI, pJ, :]
+    n = w.shape[:-1]
+    t1, t2, t3 = np.zeros(n + (ke,)), np.zeros(n + (ke,)), np.zeros(n + (ke,))
+    for k in range(1, ke):
+        avup = 0.5 * (a[..., k - 1] + a[..., k]) * w[..., k - 1]
+        avlo = 0.5 * (a[..., k + 1] + a[..., k]) * w[..., k] if k < ke - 1 else 0.0
+        den = 2.0 * almzer + dp[..., k - 1] + dp[..., k]
+        t1[..., k] = -2.0 * dt * avup * w[..., k] * di[k - 1] / den
+        t3[..., k] = -2.0 * dt * avlo * w[..., k] * di[k] / den
+        t2[..., k] = 1. - t1[..., k] - t3[..., k]
+        if k == ke - 1:
+            t3[..., k] = 0.0
+    _eliminate(t1, t2, t3, 1)
+    wnew = _col_solve(t1, t2, t3, wno[pI, pJ, :ke], w, 1)
+    wno[pI, pJ, 1:ke] = wnew[..., 1:ke]
+
+    # psi-point widths and coefficients (ocvisc.f90:286-339)
+    dlypsi = np.zeros((ie + 1, je))
+    dlypsi[1:ie] = 0.5 * (dlyv[0:ie - 1, 1:je + 1] + dlyv[1:ie, 1:je + 1])
+    dlypsi[0] = dlyv[0, 1:je + 1]
+    dlypsi[ie] = dlyv[ie - 1, 1:je + 1]
+    dlxpsi = np.zeros((ie, je + 1))
+    dlxpsi[:, 1:je] = 0.5 * (dlxu[1:ie + 1, 0:je - 1] + dlxu[1:ie + 1, 1:je])
+    dlxpsi[:, 0] = dlxu[1:ie + 1, 0]
+    dlxpsi[:, je] = dlxu[1:ie + 1, je - 1]
+    p4 = lambda x: (x * x) * (x * x)
+    mv = np.float64(minvalue)
+    aulux = aulapuv * p4(_fmx(dlxp, mv))
+    auluy = aulapuv * p4(_fmx(mv, dlypsi[1:ie + 1, :]))
+    aulvy = aulapuv * p4(_fmx(mv, dlyp))
+    aulvx = aulapuv * p4(_fmx(dlxpsi[:, 1:je + 1], mv))
+    aulwx = aulapuv * p4(_fmx(dlxu[1:ie + 1, :], mv))
+    aulwy = aulapuv * p4(_fmx(dlyv[:, 1:je + 1], mv))
+    dzu = _fmx(dduo[1:ie + 1], mv)            # p-shaped (IE, JE, KE)
+    dzv = _fmx(ddue[:, 1:je + 1], mv)
+    dzp = _fmx(ddpo, mv)
+
+    # Laplacians (FREESLIP, ocvisc.f90:347-430), every level
+    uk1o = np.zeros_like(uko)
+    vk1e = np.zeros_like(vke)
+    for k in range(ke):
+        U, M = uko[:, :, k], amsuo[:, :, k]
+        # interior u-points I = 1..IE1, J = 2..JE1
+        i0, j0 = uI, uJ
+        xt = (M[2:ie + 1, j0] * (U[2:ie + 1, j0] - U[i0, j0]) / dlxp[1:ie, j0]
+              - M[0:ie - 1, j0] * (U[i0, j0] - U[0:ie - 1, j0]) / dlxp[0:ie - 1, j0]) / dlxu[i0, j0]
+        yt = (M[i0, 0:je - 2] * (U[i0, 0:je - 2] - U[i0, j0]) / dlypsi[i0, 0:je - 2]
+              - M[i0, 2:je] * (U[i0, j0] - U[i0, 2:je]) / dlypsi[i0, j0]) / dlyu[i0, j0]
+        uk1o[i0, j0, k] = M[i0, j0] * (xt + yt)
+        # I = 0 and I = IE, J = 2..JE1
+        ytI = lambda i: (M[i, 0:je - 2] * (U[i, 0:je - 2] - U[i, j0]) / dlypsi[i, 0:je - 2]
+                         - M[i, 2:je] * (U[i, j0] - U[i, 2:je]) / dlypsi[i, j0]) / dlyu[i, j0]
+        uk1o[0, j0, k] = M[0, j0] * ((M[1, j0] * (U[1, j0] - U[0, j0]) / dlxp[0, j0]) / dlxu[0, j0]
+                                     + ytI(0))
+        uk1o[ie, j0, k] = M[ie, j0] * ((-M[ie - 1, j0] * (U[ie, j0] - U[ie - 1, j0])
+                                        / dlxp[ie - 1, j0]) / dlxu[ie, j0] + ytI(ie))
+        # J = 1 and J = JE, I = 1..IE1
+        xtJ = lambda j: (M[2:ie + 1, j] * (U[2:ie + 1, j] - U[i0, j]) / dlxp[1:ie, j]
+                         - M[0:ie - 1, j] * (U[i0, j] - U[0:ie - 1, j]) / dlxp[0:ie - 1, j]) \
+            / dlxu[i0, j]
+        uk1o[i0, 0, k] = M[i0, 0] * (xtJ(0) + (-M[i0, 1] * (U[i0, 0] - U[i0, 1]) / dlypsi[i0, 0])
+                                     / dlyu[i0, 0])
+        uk1o[i0, je - 1, k] = M[i0, je - 1] * (xtJ(je - 1) + (M[i0, je - 2] * (
+            U[i0, je - 2] - U[i0, je - 1]) / dlypsi[i0, je - 2]) / dlyu[i0, je - 1])
+
+        V, N = vke[:, :, k], amsue[:, :, k]
+        # interior v-points I = 2..IE1, J = 1..JE1 (array rows 1..IE-2, cols 1..JE-1)
+        a0, b0 = slice(1, ie - 1), slice(1, je)
+        xt = (N[2:ie, b0] * (V[2:ie, b0] - V[a0, b0]) / dlxpsi[a0, b0]
+              - N[0:ie - 2, b0] * (V[a0, b0] - V[0:ie - 2, b0]) / dlxpsi[0:ie - 2, b0]) / dlxv[a0, b0]
+        yt = (N[a0, 0:je - 1] * (V[a0, 0:je - 1] - V[a0, b0]) / dlyp[a0, 0:je - 1]
+              - N[a0, 2:je + 1] * (V[a0, b0] - V[a0, 2:je + 1]) / dlyp[a0, 1:je]) / dlyv[a0, b0]
+        vk1e[a0, b0, k] = N[a0, b0] * (xt + yt)
+        ytV = lambda r: (N[r, 0:je - 1] * (V[r, 0:je - 1] - V[r, b0]) / dlyp[r, 0:je - 1]
+                         - N[r, 2:je + 1] * (V[r, b0] - V[r, 2:je + 1]) / dlyp[r, 1:je]) / dlyv[r, b0]
+        # I = 1 (row 0) and I = IE (row IE-1), J = 1..JE1
+        vk1e[0, b0, k] = N[0, b0] * ((N[1, b0] * (V[1, b0] - V[0, b0]) / dlxpsi[0, b0])
+                                     / dlxv[0, b0] + ytV(0))
+        vk1e[ie - 1, b0, k] = N[ie - 1, b0] * ((-N[ie - 2, b0] * (V[ie - 1, b0] - V[ie - 2, b0])
+                                                / dlxpsi[ie - 2, b0]) / dlxv[ie - 1, b0]
+                                               + ytV(ie - 1))
+        # J = 0 and J = JE, I = 2..IE1
+        xtV = lambda c: (N[2:ie, c] * (V[2:ie, c] - V[a0, c]) / dlxpsi[a0, c]
+                         - N[0:ie - 2, c] * (V[a0, c] - V[0:ie - 2, c]) / dlxpsi[0:ie - 2, c]) \
+            / dlxv[a0, c]
+        vk1e[a0, 0, k] = N[a0, 0] * (xtV(0) + (-N[a0, 1] * (V[a0, 0] - V[a0, 1]) / dlyp[a0, 0])
+                                     / dlyv[a0, 0])
+        vk1e[a0, je, k] = N[a0, je] * (xtV(je) + (N[a0, je - 1] * (V[a0, je - 1] - V[a0, je])
+                                                   / dlyp[a0, je - 1]) / dlyv[a0, je])
+
+    # biharmonic updates of UOO and VOE (ocvisc.f90:435-478)
+    for k in range(ke):
+        L, M = uk1o[:, :, k], amsuo[:, :, k]
+        i0, j0 = uI, uJ
+        area = dlxu[i0, j0] * dlyu[i0, j0]
+        t = (aulux[1:ie, j0] * dlyp[1:ie, j0] * M[2:ie + 1, j0] * (L[2:ie + 1, j0] - L[i0, j0])
+             / dlxp[1:ie, j0]
+             - aulux[0:ie - 1, j0] * dlyp[0:ie - 1, j0] * M[0:ie - 1, j0]
+             * (L[i0, j0] - L[0:ie - 1, j0]) / dlxp[0:ie - 1, j0]
+             + auluy[0:ie - 1, 0:je - 2] * dlxpsi[0:ie - 1, 1:je - 1] * M[i0, 0:je - 2]
+             * (L[i0, 0:je - 2] - L[i0, j0]) / dlypsi[i0, 0:je - 2]
+             - auluy[0:ie - 1, j0] * dlxpsi[0:ie - 1, 2:je] * M[i0, 2:je]
+             * (L[i0, j0] - L[i0, 2:je]) / dlypsi[i0, j0])
+        uoo[i0, j0, k] = (M[i0, j0] / area) * (dlxu[i0, j0] * dlyu[i0, j0] * uko[i0, j0, k] - t)
+
+        L, N = vk1e[:, :, k], amsue[:, :, k]
+        a0, b0 = slice(1, ie - 1), slice(1, je)
+        area = dlxv[a0, b0] * dlyv[a0, b0]
+        t = (aulvx[a0, 0:je - 1] * dlypsi[2:ie, 0:je - 1] * N[2:ie, b0] * (L[2:ie, b0] - L[a0, b0])
+             / dlxpsi[a0, b0]
+             - aulvx[0:ie - 2, 0:je - 1] * dlypsi[1:ie - 1, 0:je - 1] * N[0:ie - 2, b0]
+             * (L[a0, b0] - L[0:ie - 2, b0]) / dlxpsi[0:ie - 2, b0]
+             + aulvy[a0, 0:je - 1] * dlxp[a0, 0:je - 1] * N[a0, 0:je - 1]
+             * (L[a0, 0:je - 1] - L[a0, b0]) / dlyp[a0, 0:je - 1]
+             - aulvy[a0, 1:je] * dlxp[a0, 1:je] * N[a0, 2:je + 1]
+             * (L[a0, b0] - L[a0, 2:je + 1]) / dlyp[a0, 1:je])
+        voe[a0, b0, k] = (N[a0, b0] / area) * (dlxv[a0, b0] * dlyv[a0, b0] * vke[a0, b0, k] - t)
+
+    # w: Laplacian with its edge rows, then the biharmonic update
+    # (FREESLIP + NON_HYDROSTATIC, ocvisc.f90:616-687), levels 1..KE
+    wn1o = np.zeros((ie, je, ke))
+    for k in range(ke):
+        W, E = wno[:, :, k], weto[:, :, k]
+        xtW = lambda r, c: (E[r + 1, c] * (W[r + 1, c] - W[r, c]) / dlxu[r + 1, c]
+                            - E[r - 1, c] * (W[r, c] - W[r - 1, c]) / dlxu[r, c]) / dlxp[r, c]
+        ytW = lambda r, c: (E[r, c - 1] * (W[r, c - 1] - W[r, c]) / dlyv[r, c]
+                            - E[r, c + 1] * (W[r, c] - W[r, c + 1]) / dlyv[r, c + 1]) / dlyp[r, c]
+        r, c = np.meshgrid(np.arange(1, ie - 1), np.arange(1, je - 1), indexing="ij")
+        wn1o[1:ie - 1, 1:je - 1, k] = E[r, c] * (xtW(r, c) + ytW(r, c))
+        cJ = np.arange(1, je - 1)
+        wn1o[0, 1:je - 1, k] = E[0, cJ] * ((E[1, cJ] * (W[1, cJ] - W[0, cJ]) / dlxu[1, cJ])
+                                           / dlxp[0, cJ] + ytW(0, cJ))
+        wn1o[ie - 1, 1:je - 1, k] = E[ie - 1, cJ] * ((-E[ie - 2, cJ] * (W[ie - 1, cJ] - W[ie - 2, cJ])
+                                                     / dlxu[ie - 1, cJ]) / dlxp[ie - 1, cJ]
+                                                    + ytW(ie - 1, cJ))
+        rI = np.arange(1, ie - 1)
+        wn1o[1:ie - 1, 0, k] = E[rI, 0] * (xtW(rI, 0) + (-E[rI, 1] * (W[rI, 0] - W[rI, 1])
+                                                        / dlyv[rI, 1]) / dlyp[rI, 0])
+        wn1o[1:ie - 1, je - 1, k] = E[rI, je - 1] * (xtW(rI, je - 1) + (
+            E[rI, je - 2] * (W[rI, je - 2] - W[rI, je - 1]) / dlyv[rI, je - 1]) / dlyp[rI, je - 1])
+    for k in range(ke):
+        L, E = wn1o[:, :, k], weto[:, :, k]
+        r, c = pI, pJ
+        vol = dlxp[r, c] * dlyp[r, c] * dzp[r, c, k]
+        t = (+aulwx[r, c] * dlyu[2:ie, c] * dzu[r, c, k] * E[2:ie, c] * (L[2:ie, c] - L[r, c])
+             / dlxu[2:ie, c]
+             - aulwx[0:ie - 2, c] * dlyu[1:ie - 1, c] * dzu[0:ie - 2, c, k] * E[0:ie - 2, c]
+             * (L[r, c] - L[0:ie - 2, c]) / dlxu[1:ie - 1, c]
+             + aulwy[r, 0:je - 2] * dlxv[r, 1:je - 1] * dzv[r, 0:je - 2, k] * E[r, 0:je - 2]
+             * (L[r, 0:je - 2] - L[r, c]) / dlyv[r, 1:je - 1]
+             - aulwy[r, c] * dlxv[r, 2:je] * dzv[r, c, k] * E[r, 2:je]
+             * (L[r, c] - L[r, 2:je]) / dlyv[r, 2:je])
+        wno[r, c, k] = (E[r, c] / vol) * (dlxp[r, c] * dlyp[r, c] * dzp[r, c, k] * wno[r, c, k] - t)
+    # OCTIMF (ocvisc.f90:767)
+    return uoo, voe, wno, uoo.copy(), voe.copy()

@@ -190,3 +190,14 @@ def test_ocvtot_nh_parts_match_numpy_restatement(case):
                          ("uoo1", st["uoo1"], uoo), ("voe1", st["voe1"], voe),
                          ("wno1", st["wno1"], wno), ("wo", st["wo"], wno)):
         assert np.array_equal(got, w), (name, float(np.abs(got - w).max()))
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ocvisc_matches_numpy_restatement(case):
+    inst = _inst(case)
+    st = C.copy_state(inst)
+    want = np_restate.ocvisc(inst, st["uoo"], st["voe"], st["wno"], st["uko"], st["vke"],
+                             st["avo"])
+    O.Oracle(inst).ocvisc(st["uoo"], st["voe"], st["wno"], st["uko"], st["vke"], st["avo"])
+    for name, w in zip(("uoo", "voe", "wno", "uko", "vke"), want):
+        assert np.array_equal(st[name], w), (name, float(np.abs(st[name] - w).max()))
