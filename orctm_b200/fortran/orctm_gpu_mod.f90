@@ -29,6 +29,11 @@ module orctm_gpu_mod
      real(c_double) :: relres, relres_initial, solve_ms
   end type orctm_solve_stats
 
+  ! coordinates and depths of GRID_INFO.ext (orctm_write_gridinfo)
+  type, bind(c) :: orctm_gridinfo
+     type(c_ptr) :: lonp, latp, lonu, latu, lonv, latv, depto, deuto, deute
+  end type orctm_gridinfo
+
   ! open-boundary tidal constants and sponge parameters; amp(v, s), pha(v, s)
   ! with v = 1..3 (z, u, v) and s = 1..4 (west, east, north, south)
   type, bind(c) :: orctm_obc
@@ -111,6 +116,42 @@ module orctm_gpu_mod
        import :: c_int, c_ptr, orctm_solve_stats
        type(c_ptr), value :: h
        type(orctm_solve_stats), intent(out) :: stats
+     end function
+     integer(c_int) function orctm_ocadpo_all(h) bind(c, name="orctm_ocadpo_all")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_step_hotpath(h, stats) bind(c, name="orctm_step_hotpath")
+       import :: c_int, c_ptr, orctm_solve_stats
+       type(c_ptr), value :: h
+       type(orctm_solve_stats), intent(out) :: stats
+     end function
+     integer(c_int) function orctm_synchronize(h) bind(c, name="orctm_synchronize")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     ! path: a NUL-terminated string, e.g. 'fort.71'//c_null_char
+     integer(c_int) function orctm_write_extra(h, path, append, idate, nfield, fields, codes) &
+         bind(c, name="orctm_write_extra")
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), dimension(*), intent(in) :: path
+       integer(c_int), value :: append, idate, nfield
+       integer(c_int), dimension(*), intent(in) :: fields, codes
+     end function
+     integer(c_int) function orctm_read_extra(h, path, nfield, fields, codes) &
+         bind(c, name="orctm_read_extra")
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), dimension(*), intent(in) :: path
+       integer(c_int), value :: nfield
+       integer(c_int), dimension(*), intent(in) :: fields, codes
+     end function
+     integer(c_int) function orctm_write_gridinfo(path, desc, g) bind(c, name="orctm_write_gridinfo")
+       import :: c_int, c_char, orctm_desc, orctm_gridinfo
+       character(kind=c_char), dimension(*), intent(in) :: path
+       type(orctm_desc), intent(in) :: desc
+       type(orctm_gridinfo), intent(in) :: g
      end function
      integer(c_int) function orctm_set_solver(h, mode, rtol, maxit) bind(c, name="orctm_set_solver")
        import :: c_int, c_ptr, c_double

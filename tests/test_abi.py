@@ -103,3 +103,48 @@ def test_open_boundary_and_gridinfo_argument_checks(tmp_path):
     assert lib.orctm_write_gridinfo(path, C.byref(d), C.byref(g)) == -1
     assert lib.orctm_write_gridinfo(None, C.byref(d), C.byref(g)) == -1
     assert not (tmp_path / "GRID_INFO.ext").exists()
+
+
+FORTRAN = os.path.join(ROOT, "orctm_b200", "fortran", "orctm_gpu_mod.f90")
+
+
+def _fortran_type_fields(src, name):
+    body = re.search(r"type, bind\(c\) :: %s\n(.*?)end type %s" % (name, name), src, re.S).group(1)
+    fields = []
+    for line in body.splitlines():
+        line = line.split("!")[0]
+        if "::" not in line:
+            continue
+        decl = re.sub(r"\([^)]*\)", "", line.split("::")[1])   # drop dimensions
+        fields += [f.strip() for f in decl.split(",") if f.strip()]
+    return fields
+
+
+def _c_struct_fields(src, name):
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), src, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        decl = re.sub(r"^(const\s+)?(int|double|size_t)\s*\**", "", decl)
+        for f in decl.split(","):
+            fields.append(re.sub(r"[\[\*].*|\s", "", f.replace("*", "")))
+    return [f for f in fields if f]
+
+
+def test_fortran_module_binds_exported_symbols_and_matching_types():
+    """The ISO_C_BINDING module (no Fortran compiler here): every bound name
+    exists in the library and every bind(c) type lists the C struct's fields
+    in the same order."""
+    lib = _lib.load()
+    src = open(FORTRAN).read()
+    names = re.findall(r'bind\(c, name="(orctm_[a-z0-9_]+)"\)', src)
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in declared_functions(), n
+    hdr = open(HEADER).read()
+    for t in ("orctm_desc", "orctm_solve_stats", "orctm_obc", "orctm_gridinfo"):
+        assert _fortran_type_fields(src, t) == _c_struct_fields(hdr, t), t
