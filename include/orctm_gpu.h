@@ -26,6 +26,8 @@
  *                                            mo_obcs.f90:569-642, 1561-1720
  *   orctm_obc_uv        FORC_OBCS_UV + SPONGE_OBCS_UV(UOO,VOE) orctm.f90:1358-1362,
  *                                            mo_obcs.f90:1881-2032, 2295-2582
+ *   orctm_set_obc_ts / orctm_obc_ts  FORC_OBCS_TS + SPONGE_OBCS_TS(THO,SAO)
+ *                       octher.f90:114-119, mo_obcs.f90:932-1272
  *   orctm_upload / orctm_download   the module arrays of MO_COMMO1
  *                                   (mo_commo1.f90:32-146) that the path reads
  *                                   and writes, moved between host and device
@@ -248,12 +250,24 @@ typedef struct orctm_obc {
   const double* amp[4][3];
   const double* pha[4][3];
 } orctm_obc;
-/* Copies the constants to the device (INI_OBCS); may be called again. */
+/* Copies the constants to the device (INI_OBCS); may be called again, which
+ * discards the T/S records of orctm_set_obc_ts. */
 int orctm_set_obc(orctm_handle* h, const orctm_obc* obc);
 /* ZO relaxed towards the tidal elevation at time step ldtrun, in place. */
 int orctm_obc_eta(orctm_handle* h, int ldtrun);
 /* UOO and VOE relaxed towards the tidal velocities at time step ldtrun. */
 int orctm_obc_uv(orctm_handle* h, int ldtrun);
+/* T/S boundary forcing, which the reference calls from OCTHER
+ * (octher.f90:114-119).  orctm_set_obc_ts is FORC_OBCS_TS for one tracer
+ * (0 THO, 1 SAO; mo_obcs.f90:932-1012): cli[s] is the climatology record of
+ * side s that FORC_OBCS_TS reads every CLI_STEP / DT steps from
+ * OB_<Side>_T.bin / OB_<Side>_S.bin, an (n, KE) array, column-major, n = JE
+ * west/east and IE north/south (NULL for sides that are not open and
+ * sponged); the boundary value at level K is the record times the boundary
+ * cell's WETO.  orctm_obc_ts is SPONGE_OBCS_TS (mo_obcs.f90:1019-1272): the
+ * tracers with a record relax in the bands of orctm_set_obc, in place. */
+int orctm_set_obc_ts(orctm_handle* h, int tracer, const double* const* cli);
+int orctm_obc_ts(orctm_handle* h);
 
 /* solver mode and relative-residual target (default FP64, 1e-10, 5000) */
 int orctm_set_solver(orctm_handle* h, int mode, double rtol, int maxit);

@@ -172,6 +172,14 @@ class Oracle:
         o, keep = obc_struct(obc)
         lib().og_obc_uv(C.byref(self.g), C.byref(o), int(step), _p(uoo), _p(voe))
 
+    def obc_ts(self, obc, cli, trf):
+        """FORC_OBCS_TS + SPONGE_OBCS_TS on one tracer; cli[b] is side b's
+        climatology record (n, KE) or None."""
+        o, keep = obc_struct(obc)
+        arrs = [None if c is None else np.asfortranarray(c, dtype=np.float64) for c in cli]
+        ptrs = (_D * 4)(*[_D() if a is None else _p(a) for a in arrs])
+        lib().og_obc_ts(C.byref(self.g), C.byref(o), ptrs, _p(trf))
+
     def octimf(self, uoo, voe, uko, vke):
         lib().og_octimf(C.byref(self.g), _p(uoo), _p(voe), _p(uko), _p(vke))
 

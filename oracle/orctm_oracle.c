@@ -1924,3 +1924,92 @@ void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double 
   free(uu); free(uf); free(uw); free(ue); free(un); free(us);
   free(vv); free(vf); free(vw); free(ve); free(vn); free(vs);
 }
+
+void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], double *trf) {
+  DIMS;
+  const int W = g->ob_west, E = g->ob_east, N = g->ob_north, S = g->ob_south;
+  const double relb = o->relax_bound, reli = o->relax_inner; /* rel_ts*, mo_obcs.f90:502-503 */
+  const double dt = g->dt;
+  const int sw = o->width[0], se = o->width[1], sn = o->width[2], ss = o->width[3];
+  const int SW_ = W && o->sponge[0], SE_ = E && o->sponge[1], SN_ = N && o->sponge[2],
+            SS_ = S && o->sponge[3];
+  /* FORC_OBCS_TS: obc_tw(j,k) = cli_twg(j,k) * WETO(1,j,k) and so on */
+  double *bw = zalloc((size_t)JE * KE), *be = zalloc((size_t)JE * KE);
+  double *bn = zalloc((size_t)IE * KE), *bs = zalloc((size_t)IE * KE);
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j) {
+      const size_t q = (size_t)(j - 1) + (size_t)JE * (k - 1);
+      if (SW_) bw[q] = cli[0][q] * P3(g->weto, 1, j, k);
+      if (SE_) be[q] = cli[1][q] * P3(g->weto, IE, j, k);
+    }
+    for (int i = 1; i <= IE; ++i) {
+      const size_t q = (size_t)(i - 1) + (size_t)IE * (k - 1);
+      if (SN_) bn[q] = cli[2][q] * P3(g->weto, i, 1, k);
+      if (SS_) bs[q] = cli[3][q] * P3(g->weto, i, JE, k);
+    }
+  }
+  const size_t n3 = (size_t)IE * JE * KE;
+  double *tt = zalloc(n3), *fo = zalloc(n3), *fw = zalloc(n3), *fe = zalloc(n3), *fn = zalloc(n3),
+         *fs = zalloc(n3);
+  memcpy(tt, trf, sizeof(double) * n3);
+  for (int k = 1; k <= KE; ++k) {
+    if (SW_)
+      for (int i = 1; i <= sw; ++i) {
+        const double s1 = (double)(sw - i + 1), s2 = (double)(i - 1);
+        const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
+        for (int j = 1; j <= JE; ++j) {
+          const double tr = (s1 * bw[(j - 1) + (size_t)JE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)sw;
+          P3(fw, i, j, k) = P3(g->weto, 1, j, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
+        }
+      }
+    if (SE_)
+      for (int i = IE; i >= IE - se + 1; --i) {
+        const double s1 = (double)(i - IE + se), s2 = (double)(IE - i);
+        const double lambda = og_lambda(s1, s2, relb, reli, se, dt);
+        for (int j = 1; j <= JE; ++j) {
+          const double tr = (s1 * be[(j - 1) + (size_t)JE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)se;
+          P3(fe, i, j, k) = P3(g->weto, IE, j, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
+        }
+      }
+    if (SN_)
+      for (int j = 1; j <= sn; ++j) {
+        const double s1 = (double)(sn - j + 1), s2 = (double)(j - 1);
+        const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
+        for (int i = 1; i <= IE; ++i) {
+          const double tr = (s1 * bn[(i - 1) + (size_t)IE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)sn;
+          P3(fn, i, j, k) = P3(g->weto, i, 1, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
+        }
+      }
+    if (SS_)
+      for (int j = JE; j >= JE - ss + 1; --j) {
+        const double s1 = (double)(j - JE + ss), s2 = (double)(JE - j);
+        const double lambda = og_lambda(s1, s2, relb, reli, ss, dt);
+        for (int i = 1; i <= IE; ++i) {
+          const double tr = (s1 * bs[(i - 1) + (size_t)IE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)ss;
+          P3(fs, i, j, k) = P3(g->weto, i, JE, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
+        }
+      }
+  }
+  for (size_t q = 0; q < n3; ++q) fo[q] = fw[q] + fe[q] + fn[q] + fs[q];
+  /* corners, mo_obcs.f90:1190-1250 */
+  for (int k = 1; k <= KE; ++k) {
+    if (SN_ && SW_)
+      for (int i = 1; i <= sw; ++i)
+        for (int j = 1; j <= sn; ++j) P3(fo, i, j, k) = i < j ? P3(fw, i, j, k) : P3(fn, i, j, k);
+    if (SS_ && SW_)
+      for (int i = 1; i <= sw; ++i)
+        for (int j = JE; j >= JE - ss + 1; --j)
+          P3(fo, i, j, k) = i < (JE - j + 1) ? P3(fw, i, j, k) : P3(fs, i, j, k);
+    if (SN_ && SE_)
+      for (int i = IE; i >= IE - se + 1; --i)
+        for (int j = 1; j <= sn; ++j)
+          P3(fo, i, j, k) = (IE - i + 1) < j ? P3(fe, i, j, k) : P3(fn, i, j, k);
+    if (SS_ && SE_)
+      for (int i = IE; i >= IE - se + 1; --i)
+        for (int j = JE; j >= JE - ss + 1; --j)
+          P3(fo, i, j, k) = (IE - i + 1) < (JE - j + 1) ? P3(fe, i, j, k) : P3(fs, i, j, k);
+  }
+  for (size_t q = 0; q < n3; ++q) trf[q] = tt[q] + fo[q];
+  free(bw); free(be); free(bn); free(bs);
+  free(tt); free(fo); free(fw); free(fe); free(fn); free(fs);
+}

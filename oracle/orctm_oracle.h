@@ -116,6 +116,13 @@ void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo);
  * `step` (orctm.f90:1358-1362). */
 void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double *voe);
 
+/* FORC_OBCS_TS's boundary values (obc_t? = CLI_T?G * WETO of the boundary
+ * cell, level by level, mo_obcs.f90:964-1012) and SPONGE_OBCS_TS
+ * (mo_obcs.f90:1019-1272) on one tracer (octher.f90:114-119).  cli[b] is the
+ * climatology record of side b as (n, KE), column-major, n = JE west/east,
+ * IE north/south; NULL where the side is not open and sponged. */
+void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], double *trf);
+
 /* Applies OCTIMF (octimf.f90:1-22): uko <- uoo, vke <- voe. */
 void og_octimf(const og_grid *g, const double *uoo, const double *voe,
                double *uko, double *vke);

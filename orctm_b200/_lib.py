@@ -83,6 +83,7 @@ EXPORTS = (
     "orctm_upload_async", "orctm_download_async", "orctm_set_step_outputs", "orctm_wait_copies",
     "orctm_write_extra", "orctm_write_extra_host", "orctm_read_extra", "orctm_read_extra_host",
     "orctm_set_obc", "orctm_obc_eta", "orctm_obc_uv", "orctm_write_gridinfo",
+    "orctm_set_obc_ts", "orctm_obc_ts",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -134,6 +135,8 @@ def load(build_if_missing: bool = True):
     lib.orctm_set_obc.argtypes = [C.c_void_p, C.POINTER(Obc)]
     lib.orctm_obc_eta.argtypes = [C.c_void_p, C.c_int]
     lib.orctm_obc_uv.argtypes = [C.c_void_p, C.c_int]
+    lib.orctm_set_obc_ts.argtypes = [C.c_void_p, C.c_int, C.POINTER(_D)]
+    lib.orctm_obc_ts.argtypes = [C.c_void_p]
     lib.orctm_timer_start.argtypes = [C.c_void_p]
     lib.orctm_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.orctm_set_profiling.argtypes = [C.c_void_p, C.c_int]

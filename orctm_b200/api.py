@@ -308,6 +308,16 @@ class Instance:
         """FORC_OBCS_ETA + SPONGE_OBCS_ETA(ZO) at time step ldtrun."""
         _lib.check(self.lib.orctm_obc_eta(self.h, int(ldtrun)), self.h)
 
+    def set_obc_ts(self, tracer: int, cli):
+        """FORC_OBCS_TS: side s's climatology record cli[s], (n, KE) or None."""
+        arrs = [None if c is None else np.asfortranarray(c, dtype=np.float64) for c in cli]
+        ptrs = (_D * 4)(*[_D() if a is None else _p(a) for a in arrs])
+        _lib.check(self.lib.orctm_set_obc_ts(self.h, int(tracer), ptrs), self.h)
+
+    def obc_ts(self):
+        """SPONGE_OBCS_TS(THO, SAO) towards the records of set_obc_ts."""
+        _lib.check(self.lib.orctm_obc_ts(self.h), self.h)
+
     def obc_uv(self, ldtrun: int):
         """FORC_OBCS_UV + UPGRADE_OBCS_UV + SPONGE_OBCS_UV(UOO, VOE) at time step ldtrun."""
         _lib.check(self.lib.orctm_obc_uv(self.h, int(ldtrun)), self.h)

@@ -223,6 +223,30 @@ def make_obc(inst: dict, seed: int | None = None, width: int | None = None,
             "amp": amp, "pha": pha}
 
 
+def make_obc_ts(inst: dict, tracer: int, seed: int | None = None) -> list:
+    """Seeded boundary climatology of one tracer (0 temperature, 1 salinity):
+    per open side an (n, KE) record (n = JE west/east, IE north/south) as
+    FORC_OBCS_TS reads from OB_<Side>_T.bin / OB_<Side>_S.bin
+    (mo_obcs.f90:932-1012), near the instance's own profile with a smooth
+    along-boundary variation; None for closed sides."""
+    ie, je, ke = inst["ie"], inst["je"], inst["ke"]
+    g = rng((inst["seed"] if seed is None else seed) + 104729 + tracer)
+    t = inst["tracers"][tracer]
+    prof = np.array([float(np.mean(t[:, :, k])) for k in range(ke)])
+    out = []
+    for b, name in enumerate(OBC_BOUNDARIES):
+        if not inst["ob"][name]:
+            out.append(None)
+            continue
+        n = je if b < 2 else ie
+        s = np.linspace(0.0, 1.0, n)[:, None]
+        amp = 0.5 if tracer == 0 else 0.1
+        c = prof[None, :] + amp * np.sin(2 * math.pi * (s + g.uniform())) \
+            + g.normal(0.0, 0.01 * amp, (n, ke))
+        out.append(np.asfortranarray(c))
+    return out
+
+
 # default cap on the vertical Courant number |w| dt / DDPO of initial states
 VERTICAL_CFL = 0.5
 

@@ -173,6 +173,11 @@ struct orctm_handle {
   ObcArgs obc[3] = {};
   double* obc_buf = nullptr;
   size_t obc_cap = 0;
+  // T/S boundary climatology records (orctm_set_obc_ts) of tracers 0 and 1
+  bool obc_ts_ready[2] = {false, false};
+  ObcArgs obc_ts[2] = {};
+  double* obc_ts_buf[2] = {nullptr, nullptr};
+  size_t obc_ts_cap[2] = {0, 0};
   // replayed chunk of PCG iterations per precision and the variants it holds
   cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
   int pcg_graph_key[2][2] = {{-1, -1}, {-1, -1}};
@@ -1624,6 +1629,66 @@ int orctm_set_obc(orctm_handle* h, const orctm_obc* o) {
     }
   }
   h->obc_ready = true;
+  // the T/S records follow the sides and widths set here: set them again
+  h->obc_ts_ready[0] = h->obc_ts_ready[1] = false;
+  return ORCTM_OK;
+}
+
+int orctm_set_obc_ts(orctm_handle* h, int tracer, const double* const* cli) {
+  ORCTM_ENTER(h);
+  if (!h->obc_ready) return h->fail(ORCTM_E_ARG, "orctm_set_obc_ts: orctm_set_obc not called");
+  if (tracer < 0 || tracer > 1 || tracer >= h->ntr || !cli)
+    return h->fail(ORCTM_E_ARG, "orctm_set_obc_ts: tracer must be 0 (THO) or 1 (SAO)");
+  const int IE = h->L.ie, JE = h->L.je, KE = h->L.ke;
+  const ObcArgs& base = h->obc[0];
+  size_t total = 0;
+  for (int b = 0; b < 4; ++b) {
+    if (!base.on[b]) continue;
+    if (!cli[b]) return h->fail(ORCTM_E_ARG, "orctm_set_obc_ts: missing record of an open, sponged side");
+    total += (size_t)(b < 2 ? JE : IE) * (size_t)KE;
+  }
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
+  if (total > h->obc_ts_cap[tracer]) {
+    int st;
+    double* p;
+    if ((st = h->dev_alloc(&p, total))) return st;
+    h->obc_ts_buf[tracer] = p;
+    h->obc_ts_cap[tracer] = total;
+  }
+  // the previous record may still be read by queued launches
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  ObcArgs a = base;
+  size_t off = 0;
+  for (int b = 0; b < 4; ++b) {
+    a.side[b] = ObcSide{nullptr, nullptr, 0};
+    if (!base.on[b]) continue;
+    const int n = b < 2 ? JE : IE;
+    const size_t cnt = (size_t)n * (size_t)KE;
+    double* d = h->obc_ts_buf[tracer] + off;
+    off += cnt;
+    ORCTM_CUDA_OK(cudaMemcpy(d, cli[b], sizeof(double) * cnt, cudaMemcpyHostToDevice));
+    a.side[b] = ObcSide{d, nullptr, n};
+  }
+  h->obc_ts[tracer] = a;
+  h->obc_ts_ready[tracer] = true;
+  return ORCTM_OK;
+}
+
+int orctm_obc_ts(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  if (!h->obc_ts_ready[0] && !h->obc_ts_ready[1])
+    return h->fail(ORCTM_E_ARG, "orctm_obc_ts: orctm_set_obc_ts not called");
+  int st;
+  for (int n = 0; n < 2; ++n) {
+    if (!h->obc_ts_ready[n]) continue;
+    const int f = ORCTM_F_THO + n;
+    if ((st = wait_uploads(h, {f})) || (st = own_buffer(h, f))) return st;
+    launch_obc_ts(h->G, h->obc_ts[n], h->slot[f], h->stream);
+    ORCTM_CUDA_OK(cudaGetLastError());
+  }
   return ORCTM_OK;
 }
 

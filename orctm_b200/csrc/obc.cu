@@ -2,6 +2,7 @@
 // them with OBC_TIDE on and OBC_SPONGE_EXP off (Makefile:49-50):
 //   FORC_OBCS_ETA + SPONGE_OBCS_ETA(ZO)              mo_obcs.f90:569-642, 1561-1720
 //   FORC_OBCS_UV + UPGRADE_OBCS_UV + SPONGE_OBCS_UV  mo_obcs.f90:1881-2032, 2295-2582
+//   FORC_OBCS_TS + SPONGE_OBCS_TS                    mo_obcs.f90:932-1272
 //
 // The reference forms the boundary values (tidal sums), then per open side a
 // correction array over its sponge band, sums the four arrays and lets the
@@ -48,7 +49,11 @@ __device__ __forceinline__ double band_lambda(double s1, double s2, int w, const
 // over gridDim.z; a thread forms its columns' tidal sums once for kLz levels
 constexpr int kLz = 4;
 
-template <int FK>
+// CLI: the boundary values are climatology records (FORC_OBCS_TS,
+// mo_obcs.f90:964-1012: side.amp holds CLI_T?G as (n, KE), and the value at
+// level K is CLI_T?G(q, K) * WETO of the boundary cell at K) instead of tidal
+// sums; the field is a 3D p-point tracer (SPONGE_OBCS_TS, mo_obcs.f90:1019-1272).
+template <int FK, bool CLI>
 __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
   const int IE = G.L.ie, JE = G.L.je;
   const int ilo = FK == FK_U ? 0 : 1, jlo = FK == FK_V ? 0 : 1;
@@ -67,10 +72,12 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
   const int ij = G.L.at2(i, j);
   // boundary values (FORC_OBCS_*): level-1 masks of the boundary cells
   double zW = 0., zE = 0., zN = 0., zS = 0.;
-  if (inW) zW = tide_sum(a.side[0], j - jlo, wet(c, ijW, 1), a);
-  if (inE) zE = tide_sum(a.side[1], j - jlo, wet(c, ijE, 1), a);
-  if (inN) zN = tide_sum(a.side[2], i - ilo, wet(c, ijN, 1), a);
-  if (inS) zS = tide_sum(a.side[3], i - ilo, wet(c, ijS, 1), a);
+  if (!CLI) {
+    if (inW) zW = tide_sum(a.side[0], j - jlo, wet(c, ijW, 1), a);
+    if (inE) zE = tide_sum(a.side[1], j - jlo, wet(c, ijE, 1), a);
+    if (inN) zN = tide_sum(a.side[2], i - ilo, wet(c, ijN, 1), a);
+    if (inS) zS = tide_sum(a.side[3], i - ilo, wet(c, ijS, 1), a);
+  }
   // band weights and relaxation rates
   double s1[4], s2[4], lam[4];
   const int d[4] = {dW, dE, dN, dS};
@@ -81,10 +88,12 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
     s2[b] = (double)(d[b] - 1);
     lam[b] = in[b] ? band_lambda(s1[b], s2[b], a.width[b], a) : 0.0;
   }
-  const int nk = FK == FK_P ? 1 : G.L.ke;
+  constexpr bool k2d = FK == FK_P && !CLI;  // ZO
+  const int nk = k2d ? 1 : G.L.ke;
   const int k0 = (int)blockIdx.z * kLz + 1, k1 = min(nk, k0 + kLz - 1);
+  const int q[4] = {j - jlo, j - jlo, i - ilo, i - ilo};  // position along each side
   for (int K = k0; K <= k1; ++K) {
-    double* px = FK == FK_P ? x + ij : x + G.L.at(i, j, K - 1);
+    double* px = k2d ? x + ij : x + G.L.at(i, j, K - 1);
     const double X = *px;
     // the mask products use level K of the cell and its boundary cell; ZO
     // (2D) uses WETO(.,.,1)
@@ -96,8 +105,13 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
     for (int b = 0; b < 4; ++b) {
       f[b] = 0.0;
       if (!in[b]) continue;
-      // UPGRADE_OBCS_UV: obc_u*(.,k) = obc_uz*(.) * mask of the boundary cell at k
-      const double ob = FK == FK_P ? zb[b] : zb[b] * mb[b];
+      // UPGRADE_OBCS_UV: obc_u*(.,k) = obc_uz*(.) * mask of the boundary cell at
+      // k; FORC_OBCS_TS: obc_t*(.,k) = CLI_T*G(.,k) * WETO of the boundary cell
+      double ob;
+      if (CLI)
+        ob = a.side[b].amp[q[b] + a.side[b].n * (K - 1)] * mb[b];
+      else
+        ob = FK == FK_P ? zb[b] : zb[b] * mb[b];
       const double xr = (s1[b] * ob + s2[b] * X) / (double)a.width[b];
       f[b] = mb[b] * mi * lam[b] * (xr - X);
     }
@@ -110,12 +124,13 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
   }
 }
 
-template <int FK>
+template <int FK, bool CLI = false>
 void launch_one(const Geo& G, const ObcArgs& a, double* x, cudaStream_t st) {
   const int ni = FK == FK_U ? G.L.ie + 1 : G.L.ie, nj = FK == FK_V ? G.L.je + 1 : G.L.je;
-  const int nk = FK == FK_P ? 1 : G.L.ke;
+  const int nk = FK == FK_P && !CLI ? 1 : G.L.ke;
   const dim3 b(32, 8);
-  k_obc_sponge<FK><<<dim3((ni + 31) / 32, (nj + 7) / 8, (nk + kLz - 1) / kLz), b, 0, st>>>(G, a, x);
+  k_obc_sponge<FK, CLI>
+      <<<dim3((ni + 31) / 32, (nj + 7) / 8, (nk + kLz - 1) / kLz), b, 0, st>>>(G, a, x);
   count_launch();
 }
 
@@ -129,6 +144,10 @@ void launch_obc_uv(const Geo& G, const ObcArgs& au, const ObcArgs& av, double* u
                    cudaStream_t st) {
   launch_one<FK_U>(G, au, uoo, st);
   launch_one<FK_V>(G, av, voe, st);
+}
+
+void launch_obc_ts(const Geo& G, const ObcArgs& a, double* tracer, cudaStream_t st) {
+  launch_one<FK_P, true>(G, a, tracer, st);
 }
 
 }  // namespace orctm

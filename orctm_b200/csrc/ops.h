@@ -83,6 +83,9 @@ void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const dou
 void launch_obc_eta(const Geo& G, const ObcArgs& a, double* zo, cudaStream_t st);
 void launch_obc_uv(const Geo& G, const ObcArgs& au, const ObcArgs& av, double* uoo, double* voe,
                    cudaStream_t st);
+// FORC_OBCS_TS + SPONGE_OBCS_TS on one tracer: a.side[s].amp holds side s's
+// climatology record (n, KE)
+void launch_obc_ts(const Geo& G, const ObcArgs& a, double* tracer, cudaStream_t st);
 
 // nh.cu
 void launch_nh_rhs(const Geo& G, const double* uoo, const double* uoo1, const double* voe,

@@ -108,6 +108,17 @@ module orctm_gpu_mod
        type(c_ptr), value :: h
        integer(c_int), value :: ldtrun
      end function
+     ! cli(s): c_loc of side s's climatology record (n, KE), c_null_ptr if unused
+     integer(c_int) function orctm_set_obc_ts(h, tracer, cli) bind(c, name="orctm_set_obc_ts")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: tracer
+       type(c_ptr), dimension(4), intent(in) :: cli
+     end function
+     integer(c_int) function orctm_obc_ts(h) bind(c, name="orctm_obc_ts")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
      integer(c_int) function orctm_ocvisc(h) bind(c, name="orctm_ocvisc")
        import :: c_int, c_ptr
        type(c_ptr), value :: h

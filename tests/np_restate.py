@@ -172,7 +172,14 @@ def matrix(g):
     return sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
 
 
-def obc_sponge(g, obc, step, x, kind):
+def obc_sponge_ts(g, obc, cli, x):
+    """FORC_OBCS_TS + SPONGE_OBCS_TS (mo_obcs.f90:932-1272) on one tracer in
+    the same per-cell distance form as obc_sponge, the boundary value of
+    level k being cli[b][q, k] times the boundary cell's WETO at level k."""
+    return obc_sponge(g, obc, 0, x, "t", cli=cli)
+
+
+def obc_sponge(g, obc, step, x, kind, cli=None):
     """Open-boundary tide forcing + 1/x sponge (mo_obcs.f90:569-642 and
     1561-1720 for kind "z" on ZO; 1881-2032 and 2295-2582 for "u" / "v" on
     UOO / VOE), restated per cell from the cell's distance d to each side's
@@ -182,8 +189,8 @@ def obc_sponge(g, obc, step, x, kind):
     IE, JE = g["ie"], g["je"]
     ilo = 0 if kind == "u" else 1
     jlo = 0 if kind == "v" else 1
-    mask = {"z": g["weto"], "u": g["amsuo"], "v": g["amsue"]}[kind]
-    v = "zuv".index(kind)
+    mask = {"z": g["weto"], "t": g["weto"], "u": g["amsuo"], "v": g["amsue"]}[kind]
+    v = "zuv".index(kind) if kind != "t" else 0
     x = np.array(x, dtype=np.float64, copy=True)
     x3 = x[:, :, None] if kind == "z" else x
     ni, nj, nk = x3.shape
@@ -215,6 +222,9 @@ def obc_sponge(g, obc, step, x, kind):
     # tidal boundary values (level-1 mask of the boundary cell)
     zb = []
     for b in range(4):
+        if kind == "t":
+            zb.append(None)
+            continue
         if not on[b]:
             zb.append(np.zeros((ni, nj)))
             continue
@@ -238,7 +248,14 @@ def obc_sponge(g, obc, step, x, kind):
         f = []
         for b in range(4):
             mb = bmask(b, k)
-            obk = zb[b] if kind == "z" else zb[b] * mb
+            if kind == "t":
+                if not on[b]:
+                    f.append(np.zeros((ni, nj)))
+                    continue
+                c = cli[b][:, k]
+                obk = np.broadcast_to(c[None, :] if b < 2 else c[:, None], (ni, nj)) * mb
+            else:
+                obk = zb[b] if kind == "z" else zb[b] * mb
             xr = (s1[b] * obk + s2[b] * X) / float(w[b])
             f.append(np.where(inb[b], mb * mi * lam[b] * (xr - X), 0.0))
         fo = f[0] + f[1] + f[2] + f[3]

@@ -104,3 +104,40 @@ def test_set_obc_rejects_bad_arguments():
     amp[0][1] = None
     with pytest.raises(Exception):
         gpu.set_obc(dict(obc, amp=amp))
+
+
+@pytest.mark.parametrize("kind", CASES)
+def test_obc_ts_parity(kind):
+    """FORC_OBCS_TS + SPONGE_OBCS_TS on THO and SAO: the same expressions as
+    the oracle and no transcendental function, so equal bit for bit."""
+    inst, obc = _case(kind)
+    orc, gpu, st = _pair(inst, obc)
+    cli = [C.make_obc_ts(inst, n) for n in (0, 1)]
+    for n in (0, 1):
+        gpu.set_obc_ts(n, cli[n])
+    for _ in range(2):
+        gpu.obc_ts()
+        for n in (0, 1):
+            orc.obc_ts(obc, cli[n], st["tracers"][n])
+    for n in (0, 1):
+        got = gpu.download(f"tracer{n}")
+        assert np.array_equal(got, st["tracers"][n]), (n, float(np.abs(got - st["tracers"][n]).max()))
+    # the passive tracer has no boundary forcing
+    assert np.array_equal(gpu.download("tracer2"), st["tracers"][2])
+
+
+def test_obc_ts_keeps_pending_download_and_needs_records():
+    inst, obc = _case("reference")
+    _, gpu, st = _pair(inst, obc)
+    with pytest.raises(Exception):
+        gpu.obc_ts()                   # no record set
+    gpu.set_obc_ts(0, C.make_obc_ts(inst, 0))
+    held = np.zeros(gpu.shape("pnh"), order="F")
+    gpu.download_async("tracer0", held)
+    gpu.obc_ts()
+    gpu.wait_copies()
+    assert np.array_equal(held, st["tracers"][0])
+    assert not np.array_equal(gpu.download("tracer0"), st["tracers"][0])
+    gpu.set_obc(obc)                   # discards the records
+    with pytest.raises(Exception):
+        gpu.obc_ts()

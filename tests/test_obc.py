@@ -124,3 +124,16 @@ def test_obc_points_match_reference_dimensions():
     ie, je = 30, 20
     assert [configs.obc_points(ie, je, 0, v) for v in range(3)] == [je, je, je + 1]
     assert [configs.obc_points(ie, je, 3, v) for v in range(3)] == [ie, ie + 1, ie]
+
+
+@pytest.mark.parametrize("kind", CASES)
+@pytest.mark.parametrize("tracer", [0, 1])
+def test_oracle_ts_equals_numpy(kind, tracer):
+    inst, obc = _case(kind)
+    cli = configs.make_obc_ts(inst, tracer)
+    o = O.Oracle(inst)
+    t = np.array(inst["tracers"][tracer], order="F", copy=True)
+    t0 = t.copy()
+    o.obc_ts(obc, cli, t)
+    assert_close(t, NR.obc_sponge_ts(inst, obc, cli, t0), 0.0, "tracer")
+    assert not np.array_equal(t, t0)
