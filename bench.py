@@ -414,7 +414,8 @@ def _band_cells(inst, obc):
 
 def run_obc(args, ws, rank, local, pg):
     """Open-boundary tide forcing + 1/x sponge (orctm_obc_uv, orctm_obc_eta;
-    mo_obcs.f90) on the tidally forced c2 box (W+S open, 30-cell sponges):
+    mo_obcs.f90) and the T/S sponge (orctm_obc_ts) on the tidally forced c2
+    box (W+S open, 30-cell sponges):
     device time per call (CUDA events on the handle's stream, max over
     ranks), the band bytes it moves, and its share of a hot-path step.  The
     velocity call is timed with private buffers (as after the host uploads
@@ -460,6 +461,9 @@ def run_obc(args, ws, rank, local, pg):
         gpu.obc_uv(s)
 
     ms_uv_shared = timed(uv_after_octimf)
+    for n in (0, 1):                                   # FORC_OBCS_TS records
+        gpu.set_obc_ts(n, configs.make_obc_ts(inst, n))
+    ms_ts = timed(lambda s: gpu.obc_ts())
     barrier(pg)
     gpu.synchronize()
     gpu.timer_start()
@@ -471,6 +475,7 @@ def run_obc(args, ws, rank, local, pg):
     # (masks are per-column level counts, the tidal constants a few KB)
     bytes_uv = 16 * (cells["u"] + cells["v"])
     bytes_eta = 16 * cells["z"]
+    bytes_ts = 2 * 16 * cells["z"] * inst["ke"]      # THO and SAO, every level
     hbm, peak_kind = peaks()
     if rank == 0:
         ach = bytes_uv / (ms_uv / 1e3) / 1e9
@@ -484,8 +489,10 @@ def run_obc(args, ws, rank, local, pg):
                                                                         "south") if inst["ob"][k]),
                                ntide=obc["ntide"]),
                 "obc_eta_ms": ms_eta, "obc_uv_after_octimf_ms": ms_uv_shared,
+                "obc_ts_ms": ms_ts,
+                "obc_ts_gbs": round(bytes_ts / (ms_ts / 1e3) / 1e9, 1),
                 "step_hotpath_ms": ms_step,
-                "share_of_step": (ms_uv + ms_eta) / ms_step,
+                "share_of_step": (ms_uv + ms_eta + ms_ts) / ms_step,
                 "band_cells": cells, "gpu_launches_per_call": launches_uv,
                 "roofline": {"bound": "hbm", "kernel": "k_obc_sponge (u and v)",
                              "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
