@@ -1,6 +1,7 @@
 ! ISO_C_BINDING interface to liborctm_gpu.so (include/orctm_gpu.h) for the
 ! ORCTM Fortran host.  The reference's subroutines keep their names; their
-! bodies become the calls shown in INTEGRATION.md.  Compile with the model
+! bodies become calls of the entry points below (OCVTOT_NH calls
+! orctm_ocvtot_nh, petsc_start orctm_create, ...).  Compile with the model
 ! (-fdefault-real-8 / -r8 as the model itself) and link -lorctm_gpu -lcudart.
 module orctm_gpu_mod
   use, intrinsic :: iso_c_binding
