@@ -33,12 +33,19 @@ def test_golden_fixtures(golden_case):
             assert np.array_equal(got, want), k
 
 
+# The golden cases plus two more for the second restatement: a c4 ensemble
+# member (another seed, KE = 31) and deep columns (KE = 97).
+XCASES = dict(CASES)
+XCASES["c4m"] = ("c4", dict(nx=50, ny=41, nz=31), None)
+XCASES["c4deep"] = ("c4", dict(nx=21, ny=17, nz=97), None)
+
+
 def _inst(case):
-    name, over, cfl = CASES[case]
+    name, over, cfl = XCASES[case]
     return C.make_instance(name, builder=O.build_grid, cfl=cfl, **over)
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_ocadpo_matches_numpy_restatement(case):
     inst = _inst(case)
     st = C.copy_state(inst)
@@ -49,7 +56,7 @@ def test_ocadpo_matches_numpy_restatement(case):
         assert np.array_equal(t, want)
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_matrix_matches_numpy_restatement(case):
     inst = _inst(case)
     A = O.Oracle(inst).matrix().tocsr()
@@ -131,7 +138,7 @@ def test_solve_matches_direct():
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) <= 1e-8
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_octdiff_matches_numpy_restatement(case):
     inst = _inst(case)
     st = C.copy_state(inst)
@@ -141,7 +148,7 @@ def test_octdiff_matches_numpy_restatement(case):
         assert np.array_equal(got, w), (n, float(np.abs(got - w).max()))
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_ocuad_matches_numpy_restatement(case):
     inst = _inst(case)
     st = C.copy_state(inst)
@@ -150,7 +157,7 @@ def test_ocuad_matches_numpy_restatement(case):
     assert np.array_equal(st["uoo"], want), float(np.abs(st["uoo"] - want).max())
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_ocvad_matches_numpy_restatement(case):
     inst = _inst(case)
     st = C.copy_state(inst)
@@ -159,7 +166,7 @@ def test_ocvad_matches_numpy_restatement(case):
     assert np.array_equal(st["voe"], want), float(np.abs(st["voe"] - want).max())
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_ocwad_matches_numpy_restatement(case):
     inst = _inst(case)
     st = C.copy_state(inst)
@@ -170,7 +177,7 @@ def test_ocwad_matches_numpy_restatement(case):
     assert not np.array_equal(st["wno"], w0)
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_ocvtot_nh_parts_match_numpy_restatement(case):
     inst = _inst(case)
     st = C.copy_state(inst)
@@ -192,7 +199,7 @@ def test_ocvtot_nh_parts_match_numpy_restatement(case):
         assert np.array_equal(got, w), (name, float(np.abs(got - w).max()))
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(XCASES))
 def test_ocvisc_matches_numpy_restatement(case):
     inst = _inst(case)
     st = C.copy_state(inst)
