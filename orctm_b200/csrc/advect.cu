@@ -493,10 +493,11 @@ __device__ __forceinline__ Fl wad_yflux(const Geo& G, const double* T, const dou
 
 
 // ---------------------------------------------------- horizontal sweeps ---
-// One kernel per (routine, direction).  A block of 32 x 8 cells of one level
-// first computes the face transports of every position its cells need (its
-// own cells plus one halo position on each side along the sweep) once, into
-// shared memory; then each cell applies RN / T' from its neighbours' entries.
+// One kernel per (routine, direction).  A block of one level first computes,
+// one thread per position, the face transports of every position its cells
+// need (its own cells plus one halo position on each side along the sweep)
+// into shared memory; then each cell applies RN / T' from its neighbours'
+// entries (block shapes in Sweep below).
 enum { V_ADPO = 0, V_UAD = 1, V_VAD = 2, V_WAD = 3 };
 
 template <int VAR> struct Rng;
