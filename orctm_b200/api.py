@@ -151,6 +151,32 @@ def write_gridinfo(path: str, inst: dict, lon: dict, lat: dict, deuto, deute) ->
     _lib.check(_lib.load().orctm_write_gridinfo(path.encode(), C.byref(d), C.byref(g)))
 
 
+def read_obc_ts_record(dirname: str, side: int, tracer: int, n: int, ke: int, record: int):
+    """Record `record` (0-based: the one FORC_OBCS_TS reads at its
+    record-th call, mo_obcs.f90:937-960) of OB_<Side>_T.bin (tracer 0) or
+    OB_<Side>_S.bin (tracer 1): a stream file of 8-byte big-endian reals in
+    which each record is KE levels of n values (n = JE west/east, IE
+    north/south).  Returns the (n, KE) array set_obc_ts takes."""
+    import os
+
+    path = os.path.join(dirname, f"OB_{OBC_SIDES[side]}_{'TS'[tracer]}.bin")
+    count = n * ke
+    a = np.fromfile(path, dtype=">f8", count=count, offset=8 * count * record)
+    if a.size != count:
+        raise ValueError(f"{path}: record {record} is incomplete")
+    return np.asfortranarray(a.astype(np.float64).reshape((n, ke), order="F"))
+
+
+def write_obc_ts_records(dirname: str, side: int, tracer: int, records) -> None:
+    """Writes (n, KE) records in the layout read_obc_ts_record reads."""
+    import os
+
+    path = os.path.join(dirname, f"OB_{OBC_SIDES[side]}_{'TS'[tracer]}.bin")
+    with open(path, "wb") as f:
+        for r in records:
+            f.write(np.asarray(r, dtype=np.float64).ravel(order="F").astype(">f8").tobytes())
+
+
 def field_id(name) -> int:
     if isinstance(name, int):
         return name

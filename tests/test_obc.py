@@ -137,3 +137,19 @@ def test_oracle_ts_equals_numpy(kind, tracer):
     o.obc_ts(obc, cli, t)
     assert_close(t, NR.obc_sponge_ts(inst, obc, cli, t0), 0.0, "tracer")
     assert not np.array_equal(t, t0)
+
+
+def test_obc_ts_records_round_trip(tmp_path):
+    inst, _ = _case("reference")
+    ie, je, ke = inst["ie"], inst["je"], inst["ke"]
+    recs = [configs.make_obc_ts(inst, 0, seed=s)[0] for s in (1, 2, 3)]   # west, 3 times
+    api.write_obc_ts_records(str(tmp_path), 0, 0, recs)
+    for r in range(3):
+        assert np.array_equal(api.read_obc_ts_record(str(tmp_path), 0, 0, je, ke, r), recs[r])
+    raw = (tmp_path / "OB_West_T.bin").read_bytes()
+    assert len(raw) == 3 * 8 * je * ke
+    # level 2 of record 1 starts after record 0 and level 1 of record 1
+    off = 8 * (je * ke + je)
+    assert np.frombuffer(raw[off:off + 8], dtype=">f8")[0] == recs[1][0, 1]
+    with pytest.raises(ValueError):
+        api.read_obc_ts_record(str(tmp_path), 0, 0, je, ke, 3)
