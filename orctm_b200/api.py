@@ -91,10 +91,13 @@ def obc_file_name(side: int, var: int, phase: bool) -> str:
     return f"OB_{OBC_SIDES[side]}_{OBC_VARS[var]}_{'Gph' if phase else 'Amp'}.bin"
 
 
-def read_obc_files(dirname: str, ie: int, je: int, ob: dict, ntide: int):
+def read_obc_files(dirname: str, ie: int, je: int, ob: dict, ntide: int, variables=(0, 1, 2)):
     """amp[s][v], pha[s][v] from the reference's harmonic-constant files of the
     open sides: unformatted stream files (FORM='BINARY') of ntide columns of
-    n values, 8-byte big-endian reals (-r8, -convert big_endian, Makefile:75)."""
+    n values, 8-byte big-endian reals (-r8, -convert big_endian, Makefile:75).
+    ``variables`` lists the ones to read (0 z, 1 u, 2 v): INI_OBCS reads the z
+    files only with OBC_ETA_FORC and the u/v files only with OBC_UV_FORC
+    (mo_obcs.f90:266-398); the others stay None."""
     import os
 
     from .configs import OBC_BOUNDARIES, obc_points
@@ -104,7 +107,7 @@ def read_obc_files(dirname: str, ie: int, je: int, ob: dict, ntide: int):
     for b, name in enumerate(OBC_BOUNDARIES):
         if not ob[name]:
             continue
-        for v in range(3):
+        for v in variables:
             n = obc_points(ie, je, b, v)
             for dst, ph in ((amp, False), (pha, True)):
                 path = os.path.join(dirname, obc_file_name(b, v, ph))
@@ -113,6 +116,17 @@ def read_obc_files(dirname: str, ie: int, je: int, ob: dict, ntide: int):
                     raise ValueError(f"{path}: {a.size} values, expected {n} x {ntide}")
                 dst[b][v] = np.asfortranarray(a.astype(np.float64).reshape((n, ntide), order="F"))
     return amp, pha
+
+
+def read_ts_profile(path: str, ke: int) -> np.ndarray:
+    """A reference stratification profile (TRef.bin / SRef.bin): KE values,
+    one per level from the surface down, each read by its own READ of a
+    FORM='BINARY' file, i.e. a stream of 8-byte big-endian reals
+    (BT_forc/mkgrid.f90:222-233 of the Sect. 3.5 experiment)."""
+    a = np.fromfile(path, dtype=">f8")
+    if a.size != ke:
+        raise ValueError(f"{path}: {a.size} values, expected KE = {ke}")
+    return a.astype(np.float64)
 
 
 def write_obc_files(dirname: str, amp, pha) -> None:
@@ -350,6 +364,45 @@ class Instance:
 
     def ocvisc(self):
         _lib.check(self.lib.orctm_ocvisc(self.h), self.h)
+
+    # -- barotropic solve (itprep.f90, troneu.f90, ocvtro.f90, ocvtot.f90) -------
+    BARO_FIELDS = {"z1o": ("p", _lib.B_Z1O), "b1o": ("p", _lib.B_B1O), "uso": ("u", _lib.B_USO),
+                   "vse": ("v", _lib.B_VSE), "uzo": ("u", _lib.B_UZO), "vze": ("v", _lib.B_VZE)}
+
+    def set_barotropic(self, deuto, deute, minvalue: float, grav=9.806, stabn=0.6, conn=0.5,
+                       rlsa1=1.0 - 0.085, sorpar=1.75, niter=250, eta_forc=False):
+        """ITPREP: the SOR coefficients and inverse depths on the device from
+        the u/v depths DEUTO (IE+1, JE) and DEUTE (IE, JE+1)."""
+        du = np.asfortranarray(deuto, dtype=np.float64)
+        dv = np.asfortranarray(deute, dtype=np.float64)
+        if du.shape != (self.ie + 1, self.je) or dv.shape != (self.ie, self.je + 1):
+            raise ValueError("DEUTO must be (IE+1, JE) and DEUTE (IE, JE+1)")
+        b = _lib.Barotropic(_p(du), _p(dv), minvalue, grav, stabn, conn, rlsa1, sorpar,
+                            int(niter), int(bool(eta_forc)))
+        _lib.check(self.lib.orctm_set_barotropic(self.h, C.byref(b)), self.h)
+
+    def troneu(self, u1o, v1e, uzo, vze):
+        """TRONEU: B1O and Z1O from the transports (u: (IE+1, JE), v: (IE, JE+1))."""
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (u1o, v1e, uzo, vze)]
+        for a, k in zip(arrs, "uvuv"):
+            want = (self.ie + 1, self.je) if k == "u" else (self.ie, self.je + 1)
+            if a.shape != want:
+                raise ValueError(f"transport shape {a.shape}, expected {want}")
+        _lib.check(self.lib.orctm_troneu(self.h, *[_p(a) for a in arrs]), self.h)
+
+    def ocvtro(self):
+        _lib.check(self.lib.orctm_ocvtro(self.h), self.h)
+
+    def ocvtot(self):
+        _lib.check(self.lib.orctm_ocvtot(self.h), self.h)
+
+    def download_barotropic(self, name: str) -> np.ndarray:
+        kind, which = self.BARO_FIELDS[name]
+        shp = {"p": (self.ie, self.je), "u": (self.ie + 1, self.je),
+               "v": (self.ie, self.je + 1)}[kind]
+        a = np.zeros(shp, dtype=np.float64, order="F")
+        _lib.check(self.lib.orctm_download_barotropic(self.h, which, _p(a), a.size), self.h)
+        return a
 
     def ocvtot_nh(self) -> dict:
         s = SolveStats()

@@ -141,3 +141,37 @@ def test_obc_ts_keeps_pending_download_and_needs_records():
     gpu.set_obc(obc)                   # discards the records
     with pytest.raises(Exception):
         gpu.obc_ts()
+
+
+def test_reference_sect35_files_drive_the_sponges():
+    """The reference's own Sect. 3.5 boundary files (tests/golden/sect35)
+    on a grid of that experiment's size (IE = 4000, JE = 5, KE = 300; W and
+    E open, 30-cell sponges, relaxation times of its OCECTL): the u/v tide
+    sponge and the T/S climatology sponge accept them and match the oracle
+    (1e-13 for u/v, whose tidal sums call COS; bit for bit for T/S)."""
+    from orctm_b200 import api, grid
+    from test_reference_fixtures import HERE, JE, KE, NTIDE, OB, PERIODS
+
+    inst = C.make_instance("c2", builder=grid.build_grid, nx=4000 - 2, ny=JE - 2, nz=KE)
+    inst["ob"] = dict(OB)
+    amp, pha = api.read_obc_files(HERE, inst["ie"], inst["je"], OB, NTIDE, variables=(1, 2))
+    for b in (0, 1):             # OBC_ETA_FORC off: the elevation constants stay zero
+        amp[b][0] = np.zeros((JE, NTIDE), order="F")
+        pha[b][0] = np.zeros((JE, NTIDE), order="F")
+    obc = {"ntide": NTIDE, "period": np.array(PERIODS), "sponge": [1, 1, 0, 0],
+           "width": [30, 30, 1, 1], "relax_inner": 44714.1643, "relax_bound": 2.0,
+           "amp": amp, "pha": pha}
+    orc, gpu, st = _pair(inst, obc)
+    for step in (1, 7200, 43200):
+        gpu.obc_uv(step)
+        orc.obc_uv(obc, step, st["uoo"], st["voe"])
+    assert_close(gpu.download("uoo"), st["uoo"], TOL, "UOO")
+    assert_close(gpu.download("voe"), st["voe"], TOL, "VOE")
+    for n in (0, 1):
+        cli = [api.read_obc_ts_record(HERE, s, n, JE, KE, 3) for s in (0, 1)] + [None, None]
+        gpu.set_obc_ts(n, cli)
+    gpu.obc_ts()
+    for n in (0, 1):
+        cli = [api.read_obc_ts_record(HERE, s, n, JE, KE, 3) for s in (0, 1)] + [None, None]
+        orc.obc_ts(obc, cli, st["tracers"][n])
+        assert np.array_equal(gpu.download(f"tracer{n}"), st["tracers"][n]), n
