@@ -69,6 +69,28 @@ class GridInfo(C.Structure):
                                   "deuto", "deute")]
 
 
+class Barotropic(C.Structure):
+    """orctm_barotropic: ITPREP's inputs and the barotropic solve's constants."""
+    _fields_ = [("deuto", _D), ("deute", _D), ("minvalue", C.c_double), ("grav", C.c_double),
+                ("stabn", C.c_double), ("conn", C.c_double), ("rlsa1", C.c_double),
+                ("sorpar", C.c_double), ("niter", C.c_int), ("eta_forc", C.c_int)]
+
+
+B_Z1O, B_B1O, B_USO, B_VSE, B_UZO, B_VZE = range(6)
+
+
+class NoAllocArgs(C.Structure):
+    """orctm_octdiff_noalloc_args: device pointers in the reference's layouts."""
+    _fields_ = [("ie", C.c_int), ("je", C.c_int), ("ke", C.c_int),
+                ("dt", C.c_double), ("almzer", C.c_double), ("aulapts", C.c_double),
+                ("ah00", C.c_double),
+                ("tracer_in", C.c_void_p), ("tracer_out", C.c_void_p), ("dvo", C.c_void_p),
+                ("ddpo", C.c_void_p), ("weto", C.c_void_p), ("di", C.c_void_p),
+                ("dzw", C.c_void_p), ("dlxp", C.c_void_p), ("dlyp", C.c_void_p),
+                ("dlxu", C.c_void_p), ("dlyu", C.c_void_p), ("dlxv", C.c_void_p),
+                ("dlyv", C.c_void_p), ("zo", C.c_void_p), ("stream", C.c_void_p)]
+
+
 EXPORTS = (
     "orctm_abi_version", "orctm_status_string", "orctm_last_error", "orctm_create",
     "orctm_destroy", "orctm_field_size", "orctm_upload", "orctm_download", "orctm_ocuad",
@@ -83,7 +105,9 @@ EXPORTS = (
     "orctm_upload_async", "orctm_download_async", "orctm_set_step_outputs", "orctm_wait_copies",
     "orctm_write_extra", "orctm_write_extra_host", "orctm_read_extra", "orctm_read_extra_host",
     "orctm_set_obc", "orctm_obc_eta", "orctm_obc_uv", "orctm_write_gridinfo",
-    "orctm_set_obc_ts", "orctm_obc_ts",
+    "orctm_set_obc_ts", "orctm_obc_ts", "orctm_octdiff_noalloc",
+    "orctm_set_barotropic", "orctm_troneu", "orctm_ocvtro", "orctm_ocvtot",
+    "orctm_download_barotropic",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -149,6 +173,12 @@ def load(build_if_missing: bool = True):
     lib.orctm_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.orctm_check_division.argtypes = [C.c_int, _D, _D, _D, C.c_size_t]
     lib.orctm_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.orctm_octdiff_noalloc.argtypes = [C.POINTER(NoAllocArgs)]
+    lib.orctm_set_barotropic.argtypes = [C.c_void_p, C.POINTER(Barotropic)]
+    lib.orctm_troneu.argtypes = [C.c_void_p, _D, _D, _D, _D]
+    lib.orctm_ocvtro.argtypes = [C.c_void_p]
+    lib.orctm_ocvtot.argtypes = [C.c_void_p]
+    lib.orctm_download_barotropic.argtypes = [C.c_void_p, C.c_int, _D, C.c_size_t]
     _lib = lib
     return lib
 

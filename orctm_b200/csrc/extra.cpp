@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "../../include/orctm_gpu.h"
@@ -58,11 +59,19 @@ extern "C" int orctm_write_extra_host(const char* path, int append, int idate, i
 
 namespace {
 
-bool get_record(FILE* f, std::vector<unsigned char>& payload) {
+// One Fortran sequential record whose length must be `expected` bytes: the
+// marker is checked before anything is allocated, so a corrupt or
+// wrong-endian file cannot ask for a huge buffer.
+bool get_record(FILE* f, std::vector<unsigned char>& payload, uint64_t expected) {
   uint32_t m0, m1;
   if (fread(&m0, 4, 1, f) != 1) return false;
   const uint32_t n = be32(m0);
-  payload.resize(n);
+  if (n != expected) return false;
+  try {
+    payload.resize(n);
+  } catch (const std::bad_alloc&) {
+    return false;
+  }
   if (n && fread(payload.data(), 1, n, f) != n) return false;
   if (fread(&m1, 4, 1, f) != 1 || m1 != m0) return false;
   return true;
@@ -82,11 +91,7 @@ extern "C" int orctm_read_extra_host(const char* path, int code, int nlev, int i
   std::vector<unsigned char> hdr, vals;
   int found = 0;
   bool ok = true;
-  while (found < nlev && (ok = get_record(f, hdr))) {
-    if (hdr.size() != 16 || !(ok = get_record(f, vals))) {
-      ok = false;
-      break;
-    }
+  while (found < nlev && (ok = get_record(f, hdr, 16))) {
     int32_t h[4];
     for (int k = 0; k < 4; ++k) {
       uint32_t u;
@@ -94,7 +99,14 @@ extern "C" int orctm_read_extra_host(const char* path, int code, int nlev, int i
       u = be32(u);
       std::memcpy(&h[k], &u, 4);
     }
-    if (h[1] != code || h[3] != iedim || vals.size() != (size_t)4 * iedim) continue;
+    // IEDIM of the header sizes the data record (4-byte reals; a record
+    // length is a 32-bit marker)
+    if (h[3] < 1 || (uint64_t)h[3] * 4 > 0xFFFFFFFFull ||
+        !(ok = get_record(f, vals, (uint64_t)h[3] * 4))) {
+      ok = false;
+      break;
+    }
+    if (h[1] != code || h[3] != iedim) continue;
     double* dst = out + (size_t)found * iedim;
     for (int n = 0; n < iedim; ++n) {
       uint32_t u;

@@ -42,7 +42,6 @@ static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxCells];
 
 std::mutex g_na_mutex;
 double* g_na_ptr[kNoAllocMaxDevices] = {};
-thread_local std::string g_na_error;
 
 struct NaArgs {
   int IE, JE, KE;
@@ -162,23 +161,37 @@ __global__ void k_na_bih(NaArgs a, const double* __restrict__ T, const double* _
   O[p3(a, i, j, K)] = r;
 }
 
-// Device address of the scratch array on the current device; looked up once
-// per device (cudaGetSymbolAddress), then cached.
-int scratch_for_current_device(double** out) {
+// Device address of the scratch array on the current device.  The first call
+// on a device looks it up (cudaGetSymbolAddress, with that device current).
+// Later calls look it up again when their stream is not being captured, so
+// an address cached before a cudaDeviceReset (which unloads the module and
+// may place the array elsewhere) is not reused; a call on a capturing stream
+// uses the cached address, so the first call on a device must come before
+// any capture, and a device reset must be followed by one call outside a
+// capture before the next capture.
+int scratch_for_current_device(cudaStream_t s, double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_status(e);
   if (dev < 0 || dev >= kNoAllocMaxDevices) {
-    g_na_error = "device ordinal beyond the no-allocation table";
+    set_unbound_error("device ordinal beyond the no-allocation table");
     return ORCTM_E_ARG;
   }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool capturing = cudaStreamIsCapturing(s, &cs) != cudaSuccess ||
+                         cs != cudaStreamCaptureStatusNone;
   std::lock_guard<std::mutex> lk(g_na_mutex);
-  if (!g_na_ptr[dev]) {
+  if (!g_na_ptr[dev] || !capturing) {
+    if (capturing) {
+      set_unbound_error("the first call on a device must not be made under stream capture");
+      return ORCTM_E_ARG;
+    }
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) {
-      g_na_error = std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
-      return cuda_status(e);
+      const int st = cuda_status(e);
+      set_unbound_error((std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e)).c_str());
+      return st;
     }
     g_na_ptr[dev] = static_cast<double*>(p);
   }
@@ -192,15 +205,18 @@ int scratch_for_current_device(double** out) {
 using namespace orctm;
 
 extern "C" int orctm_octdiff_noalloc(const orctm_octdiff_noalloc_args* in) {
-  g_na_error.clear();
-  if (!in) return ORCTM_E_ARG;
+  clear_unbound_errors();
+  if (!in) {
+    set_unbound_error("null argument block");
+    return ORCTM_E_ARG;
+  }
   const long long cells = (long long)in->ie * in->je * in->ke;
   if (in->ie < 3 || in->je < 3 || in->ke < 2 || in->ke > kMaxKe) {
-    g_na_error = "grid size out of range";
+    set_unbound_error("grid size out of range");
     return ORCTM_E_ARG;
   }
   if (cells > kNoAllocMaxCells) {
-    g_na_error = "IE*JE*KE exceeds the no-allocation limit of 2097152 cells";
+    set_unbound_error("IE*JE*KE exceeds the no-allocation limit of 2097152 cells");
     return ORCTM_E_TOO_LARGE;
   }
   const void* req[] = {in->tracer_in, in->tracer_out, in->dvo, in->ddpo, in->weto, in->di,
@@ -208,25 +224,25 @@ extern "C" int orctm_octdiff_noalloc(const orctm_octdiff_noalloc_args* in) {
                        in->zo};
   for (const void* p : req)
     if (!p) {
-      g_na_error = "missing device pointer";
+      set_unbound_error("missing device pointer");
       return ORCTM_E_ARG;
     }
   if (in->tracer_in == in->tracer_out) {
-    g_na_error = "tracer_in and tracer_out must be different buffers";
+    set_unbound_error("tracer_in and tracer_out must be different buffers");
     return ORCTM_E_ARG;
   }
   if (in->ah00 > in->almzer) {
-    g_na_error = "harmonic tracer diffusion (AH00 > ALMZER) is not implemented";
+    set_unbound_error("harmonic tracer diffusion (AH00 > ALMZER) is not implemented");
     return ORCTM_E_UNSUPPORTED;
   }
+  cudaStream_t s = static_cast<cudaStream_t>(in->stream);
   double* scratch = nullptr;
-  int st = scratch_for_current_device(&scratch);
+  int st = scratch_for_current_device(s, &scratch);
   if (st != ORCTM_OK) return st;
   double* vdiff = scratch;                     // vertically diffused tracer
   double* lap = scratch + kNoAllocMaxCells;    // first Laplacian T1O
   NaArgs a{in->ie, in->je, in->ke, in->dt, in->almzer, in->aulapts, in->dvo, in->ddpo, in->weto,
            in->di, in->dzw, in->dlxp, in->dlyp, in->dlxu, in->dlyu, in->dlxv, in->dlyv, in->zo};
-  cudaStream_t s = static_cast<cudaStream_t>(in->stream);
   const dim3 bc(32, 2), b3(32, 4);
   const dim3 gc((in->ie + 31) / 32, (in->je + 1) / 2, 1);
   const dim3 g3((in->ie + 31) / 32, (in->je + 3) / 4, in->ke);
@@ -240,9 +256,6 @@ extern "C" int orctm_octdiff_noalloc(const orctm_octdiff_noalloc_args* in) {
     count_launch();
   }
   const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    g_na_error = cudaGetErrorString(e);
-    return cuda_status(e);
-  }
+  if (e != cudaSuccess) return cuda_status(e);
   return ORCTM_OK;
 }

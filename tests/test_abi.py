@@ -148,5 +148,71 @@ def test_fortran_module_binds_exported_symbols_and_matching_types():
         assert hasattr(lib, n), n
         assert n in declared_functions(), n
     hdr = open(HEADER).read()
-    for t in ("orctm_desc", "orctm_solve_stats", "orctm_obc", "orctm_gridinfo"):
+    for t in ("orctm_desc", "orctm_solve_stats", "orctm_obc", "orctm_gridinfo", "orctm_barotropic"):
         assert _fortran_type_fields(src, t) == _c_struct_fields(hdr, t), t
+
+
+_NOALLOC_PTRS = ("tracer_in", "tracer_out", "dvo", "ddpo", "weto", "di", "dzw", "dlxp", "dlyp",
+                 "dlxu", "dlyu", "dlxv", "dlyv", "zo")
+
+
+def _noalloc_args():
+    a = _lib.NoAllocArgs()
+    a.ie, a.je, a.ke = 10, 9, 5
+    a.dt, a.almzer, a.aulapts, a.ah00 = 10.0, 1e-19, 1e3, 0.0
+    # distinct non-null placeholders: every refusal below happens before the
+    # entry point touches a device, so they are never dereferenced
+    for n, k in enumerate(_NOALLOC_PTRS):
+        setattr(a, k, 0x100000 + 0x1000 * n)
+    return a
+
+
+@pytest.mark.parametrize("change,status,words", [
+    (dict(ke=1), -1, b"grid size"),
+    (dict(ke=321), -1, b"grid size"),
+    (dict(ie=2), -1, b"grid size"),
+    (dict(ie=2050, je=2050, ke=10), -8, b"no-allocation limit"),
+    (dict(zo=None), -1, b"missing device pointer"),
+    (dict(dvo=None), -1, b"missing device pointer"),
+    (dict(tracer_out=0x100000), -1, b"different buffers"),
+    (dict(ah00=1.0), -6, b"harmonic"),
+])
+def test_noalloc_refusals_carry_a_message(change, status, words):
+    """orctm_octdiff_noalloc refuses bad sizes, missing or aliased arrays and
+    harmonic diffusion before any device work, and orctm_last_error(NULL)
+    then says why."""
+    lib = _lib.load()
+    a = _noalloc_args()
+    for k, v in change.items():
+        setattr(a, k, v)
+    assert lib.orctm_octdiff_noalloc(C.byref(a)) == status
+    assert words in lib.orctm_last_error(None)
+    assert lib.orctm_octdiff_noalloc(None) == -1
+    assert b"null argument" in lib.orctm_last_error(None)
+
+
+def test_extra_reader_rejects_corrupt_record_markers(tmp_path):
+    """A record marker that does not match the header's size (a corrupt or
+    wrong-endian file) is refused before a buffer is sized from it."""
+    lib = _lib.load()
+    good = tmp_path / "good.ext"
+    O.write_extra(str(good), [(1, 2, 3, np.arange(6.0))])
+    out = np.zeros(6)
+    assert lib.orctm_read_extra_host(str(good).encode(), 2, 1, 6, _lib_ptr(out), None) == 0
+    assert np.array_equal(out, np.arange(6.0))
+    raw = bytearray(good.read_bytes())
+    for bad in (b"\xff\xff\xff\xf0", raw[0:4][::-1]):      # huge marker; little-endian marker
+        b = bytearray(raw)
+        b[0:4] = bad
+        p = tmp_path / "bad.ext"
+        p.write_bytes(bytes(b))
+        assert lib.orctm_read_extra_host(str(p).encode(), 2, 1, 6, _lib_ptr(out), None) == -1
+    b = bytearray(raw)
+    b[24:28] = b"\x7f\xff\xff\xff"                          # data marker disagrees with IEDIM
+    p = tmp_path / "bad2.ext"
+    p.write_bytes(bytes(b))
+    assert lib.orctm_read_extra_host(str(p).encode(), 2, 1, 6, _lib_ptr(out), None) == -1
+
+
+def _lib_ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
