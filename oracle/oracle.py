@@ -119,6 +119,24 @@ def build_grid(ie, je, ke, dt, dzw, depto, dlxp, dlyp, dlxu, dlyu, dlxv, dlyv):
     return depto, g
 
 
+class _Baro(C.Structure):
+    _fields_ = [("grav", C.c_double), ("stabn", C.c_double), ("conn", C.c_double),
+                ("rlsa1", C.c_double), ("sorpar", C.c_double), ("niter", C.c_int),
+                ("eta_forc", C.c_int)]
+
+
+# the reference driver's constants (orctm.f90:352-353, 657-661, 680) and the
+# SOR sweeps of troneu.f90:104; SORPAR is TROTEST's choice at run time
+BARO_DEFAULTS = {"grav": 9.806, "stabn": 0.6, "conn": 0.5, "rlsa1": 1.0 - 0.085,
+                 "sorpar": 1.75, "niter": 250, "eta_forc": 0}
+
+
+def baro_struct(b: dict):
+    v = dict(BARO_DEFAULTS, **b)
+    return _Baro(v["grav"], v["stabn"], v["conn"], v["rlsa1"], v["sorpar"], int(v["niter"]),
+                 int(v["eta_forc"]))
+
+
 class Oracle:
     """Holds one instance's geometry and exposes the restated routines."""
 
@@ -183,6 +201,42 @@ class Oracle:
     def octimf(self, uoo, voe, uko, vke):
         lib().og_octimf(C.byref(self.g), _p(uoo), _p(voe), _p(uko), _p(vke))
 
+    # -- barotropic solve (boden.f90, itprep.f90, troneu.f90, ocvtro.f90, ocvtot.f90)
+    def _f2(self, kind):
+        ie, je = self.ie, self.je
+        return np.zeros({"p": (ie, je), "u": (ie + 1, je), "v": (ie, je + 1)}[kind], order="F")
+
+    def deut(self, depto, minvalue):
+        """(DEUTO, DEUTE, DEUTIO, DEUTIE) from the BODEN-adjusted DEPTO."""
+        out = [self._f2("u"), self._f2("v"), self._f2("u"), self._f2("v")]
+        lib().og_deut(C.byref(self.g), _p(np.asfortranarray(depto, dtype=np.float64)),
+                      C.c_double(minvalue), *[_p(a) for a in out])
+        return tuple(out)
+
+    def itprep(self, b, deuto, deute):
+        out = [self._f2("p"), self._f2("u"), self._f2("v"), self._f2("p")]
+        lib().og_itprep(C.byref(self.g), C.byref(baro_struct(b)), _p(deuto), _p(deute),
+                        *[_p(a) for a in out])
+        return tuple(out)  # xx, uf, vf, ff
+
+    def troneu(self, b, xx, uf, vf, ff, u1o, v1e, uzo, vze):
+        b1o, z1o = self._f2("p"), self._f2("p")
+        lib().og_troneu(C.byref(self.g), C.byref(baro_struct(b)), _p(xx), _p(uf), _p(vf), _p(ff),
+                        _p(u1o), _p(v1e), _p(uzo), _p(vze), _p(b1o), _p(z1o))
+        return b1o, z1o
+
+    def ocvtro(self, b, deutio, deutie, z1o, uzo, vze, zo):
+        """In place on uzo, vze, zo; returns (uso, vse)."""
+        uso, vse = self._f2("u"), self._f2("v")
+        lib().og_ocvtro(C.byref(self.g), C.byref(baro_struct(b)), _p(deutio), _p(deutie),
+                        _p(z1o), _p(uzo), _p(vze), _p(uso), _p(vse), _p(zo))
+        return uso, vse
+
+    def ocvtot(self, b, uso, vse, uoo, voe, uko, vke, wo):
+        """In place on uoo, voe, uko, vke, wo."""
+        lib().og_ocvtot(C.byref(self.g), C.byref(baro_struct(b)), _p(uso), _p(vse), _p(uoo),
+                        _p(voe), _p(uko), _p(vke), _p(wo))
+
     # -- OCVTOT_NH ----------------------------------------------------------
     @property
     def nunk(self):
@@ -229,9 +283,18 @@ class Oracle:
         lib().og_nh_post(C.byref(self.g), _p(np.ascontiguousarray(x)), _p(pnh), _p(uoo), _p(voe),
                          _p(wno), _p(uoo1), _p(voe1), _p(wno1), _p(wo))
 
-    def ocvtot_nh(self, st, solver="direct", rtol=1e-13):
-        """Whole OCVTOT_NH on a state dict (in place).  Returns solve info."""
+    def ocvtot_nh(self, st, solver="direct", rtol=1e-13, pnh=None):
+        """Whole OCVTOT_NH on a state dict (in place).  Returns solve info.
+
+        ``pnh`` (a p-point array, e.g. the pressure another implementation
+        found) replaces the solve: its interior is used as the solution, so
+        that the post-solve update can be checked apart from the solver."""
         b = self.nh_rhs(st["uoo"], st["uoo1"], st["voe"], st["voe1"], st["wno"], st["wno1"], st["zo"])
+        if pnh is not None:
+            x = np.asarray(pnh)[1:-1, 1:-1, :].reshape(-1, order="F").copy()
+            self.nh_post(x, st["pnh"], st["uoo"], st["voe"], st["wno"], st["uoo1"], st["voe1"],
+                         st["wno1"], st["wo"])
+            return {"its": 0, "relres": None, "b": b, "x": x}
         A = self.matrix()
         x0 = st["pnh"][1:-1, 1:-1, :].reshape(-1, order="F").copy()
         if solver == "direct":
@@ -243,8 +306,9 @@ class Oracle:
                      st["wno1"], st["wo"])
         return {"its": its, "relres": rel, "b": b, "x": x}
 
-    def step_hotpath(self, st, solver="direct", rtol=1e-13):
-        """One pass of the hot path in the driver's order (orctm.f90:1454-1562)."""
+    def step_hotpath(self, st, solver="direct", rtol=1e-13, pnh=None):
+        """One pass of the hot path in the driver's order (orctm.f90:1454-1562);
+        ``pnh`` as in ocvtot_nh."""
         self.ocuad(st["uoo"], st["uko"], st["vke"], st["wo"])
         self.ocvad(st["voe"], st["uko"], st["vke"], st["wo"])
         self.ocwad(st["wno"], st["uko"], st["vke"], st["wo"], st["zo"])
@@ -253,7 +317,7 @@ class Oracle:
         self.octdiff(st["tracers"], st["dvo"], st["zo"])
         self.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
         self.ocvisc(st["uoo"], st["voe"], st["wno"], st["uko"], st["vke"], st["avo"])
-        info = self.ocvtot_nh(st, solver=solver, rtol=rtol)
+        info = self.ocvtot_nh(st, solver=solver, rtol=rtol, pnh=pnh)
         self.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
         return info
 

@@ -2013,3 +2013,185 @@ void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], do
   free(bw); free(be); free(bn); free(bs);
   free(tt); free(fo); free(fw); free(fe); free(fn); free(fs);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Barotropic solve: DEUTO/DEUTE (boden.f90), ITPREP, TRONEU, OCVTRO, OCVTOT */
+/* ------------------------------------------------------------------------ */
+void og_deut(const og_grid *g, const double *depto, double minvalue, double *deuto,
+             double *deute, double *deutio, double *deutie) {
+  DIMS;
+  /* boden.f90:117-128 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE1; ++i) U2(deuto, i, j) = fmn(P2(depto, i, j), P2(depto, i + 1, j));
+  for (int j = 1; j <= JE; ++j) {
+    U2(deuto, 0, j) = U2(deuto, 1, j);
+    U2(deuto, IE, j) = U2(deuto, IE1, j);
+  }
+  for (int j = 1; j <= JE1; ++j)
+    for (int i = 1; i <= IE; ++i) V2(deute, i, j) = fmn(P2(depto, i, j), P2(depto, i, j + 1));
+  for (int i = 1; i <= IE; ++i) {
+    V2(deute, i, 0) = V2(deute, i, 1);
+    V2(deute, i, JE) = V2(deute, i, JE1);
+  }
+  /* boden.f90:264-274 (zero elsewhere, beleg_zero.f90:59,69) */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i)
+      U2(deutio, i, j) = U2(deuto, i, j) > minvalue ? 1. / U2(deuto, i, j) : 0.0;
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i)
+      V2(deutie, i, j) = V2(deute, i, j) > minvalue ? 1. / V2(deute, i, j) : 0.0;
+}
+
+void og_itprep(const og_grid *g, const og_baro *b, const double *deuto, const double *deute,
+               double *xx, double *uf, double *vf, double *ff) {
+  DIMS;
+  const double dt = g->dt;
+  /* itprep.f90:17-21 */
+  for (int i = 1; i <= IE; ++i)
+    for (int j = 1; j <= JE; ++j) P2(xx, i, j) = P2(g->dlxp, i, j) * P2(g->dlyp, i, j);
+  /* itprep.f90:23-27: DEUTO*DLYU/DLXU*G*CONN*STABN*DT**2, left to right */
+  for (int i = 0; i <= IE; ++i)
+    for (int j = 1; j <= JE; ++j)
+      U2(uf, i, j) = U2(deuto, i, j) * U2(g->dlyu, i, j) / U2(g->dlxu, i, j) * b->grav * b->conn *
+                     b->stabn * (dt * dt);
+  /* itprep.f90:29-33 */
+  for (int i = 1; i <= IE; ++i)
+    for (int j = 0; j <= JE; ++j)
+      V2(vf, i, j) = V2(deute, i, j) * V2(g->dlxv, i, j) / V2(g->dlyv, i, j) * b->grav * b->conn *
+                     b->stabn * (dt * dt);
+  /* itprep.f90:35-40 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i)
+      P2(ff, i, j) = 1. / (P2(xx, i, j) + U2(uf, i, j) + U2(uf, i - 1, j) + V2(vf, i, j) +
+                           V2(vf, i, j - 1));
+}
+
+/* one SOR colour of troneu.f90:108-127: J = 2..JE-1, I = IS..IE-1 step 2 */
+static void sor_colour(const og_grid *g, const og_baro *b, int parity, const double *uf,
+                       const double *vf, const double *ff, const double *b1o, double *z1o) {
+  DIMS;
+  const double sorpai = 1. - b->sorpar;
+#pragma omp parallel for schedule(static)
+  for (int j = 2; j <= JE1; ++j) {
+    const int is = (j + parity) % 2 + 2;  /* MOD(p_ioff+p_joff+j(+1),2)+2 on one rank */
+    for (int i = is; i <= IE1; i += 2)
+      P2(z1o, i, j) = b->sorpar * P2(ff, i, j) *
+                          (P2(b1o, i, j) + U2(uf, i, j) * P2(z1o, i + 1, j) +
+                           U2(uf, i - 1, j) * P2(z1o, i - 1, j) + V2(vf, i, j) * P2(z1o, i, j + 1) +
+                           V2(vf, i, j - 1) * P2(z1o, i, j - 1)) +
+                      sorpai * P2(z1o, i, j);
+  }
+}
+
+void og_troneu(const og_grid *g, const og_baro *b, const double *xx, const double *uf,
+               const double *vf, const double *ff, const double *u1o, const double *v1e,
+               const double *uzo, const double *vze, double *b1o, double *z1o) {
+  DIMS;
+  const double conn = b->conn, cono = 1. - b->conn;
+  /* troneu.f90:48-60 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      double v = P3(g->weto, i, j, 1) *
+                 (P2(g->dtdxpo, i, j) *
+                      ((cono * U2(u1o, i - 1, j) + U2(uzo, i - 1, j) * conn) * U2(g->dlyu, i - 1, j) -
+                       (U2(u1o, i, j) * cono + U2(uzo, i, j) * conn) * U2(g->dlyu, i, j)) /
+                      P2(g->dlyp, i, j) +
+                  P2(g->dtdyo, i, j) *
+                      ((V2(v1e, i, j) * cono + conn * V2(vze, i, j)) * V2(g->dlxv, i, j) -
+                       (V2(v1e, i, j - 1) * cono + conn * V2(vze, i, j - 1)) * V2(g->dlxv, i, j - 1)) /
+                      P2(g->dlxp, i, j));
+      P2(b1o, i, j) = v * P2(xx, i, j);
+    }
+  memset(z1o, 0, sizeof(double) * (size_t)IE * JE);
+  if (!b->eta_forc) {  /* troneu.f90:67-102 (one rank holds every edge) */
+    for (int j = 1; j <= JE; ++j) P2(z1o, 1, j) = P2(b1o, 1, j) / P2(xx, 1, j);
+    for (int j = 1; j <= JE; ++j) P2(z1o, IE, j) = P2(b1o, IE, j) / P2(xx, IE, j);
+    for (int i = 1; i <= IE; ++i) P2(z1o, i, 1) = P2(b1o, i, 1) / P2(xx, i, 1);
+    for (int i = 1; i <= IE; ++i) P2(z1o, i, JE) = P2(b1o, i, JE) / P2(xx, i, JE);
+  }
+  /* troneu.f90:104-134 */
+  for (int it = 0; it < b->niter; ++it) {
+    sor_colour(g, b, 0, uf, vf, ff, b1o, z1o);
+    sor_colour(g, b, 1, uf, vf, ff, b1o, z1o);
+  }
+}
+
+void og_ocvtro(const og_grid *g, const og_baro *b, const double *deutio, const double *deutie,
+               const double *z1o, double *uzo, double *vze, double *uso, double *vse, double *zo) {
+  DIMS;
+  const double c = b->rlsa1 * b->grav * b->stabn;
+  /* ocvtro.f90:11-23 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i) {
+      U2(uzo, i, j) = U2(uzo, i, j) * U2(deutio, i, j);
+      U2(uso, i, j) = U2(uzo, i, j);
+    }
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      V2(vze, i, j) = V2(vze, i, j) * V2(deutie, i, j);
+      V2(vse, i, j) = V2(vze, i, j);
+    }
+  /* ocvtro.f90:34-48: rlsa1*G*STABN*DTDXUO*(Z1O(I)-Z1O(I+1))*AMSUO(I,J,1) */
+  for (int j = 2; j <= JE1; ++j)
+    for (int i = 1; i <= IE1; ++i)
+      U2(uso, i, j) = U2(uzo, i, j) + c * U2(g->dtdxuo, i, j) * (P2(z1o, i, j) - P2(z1o, i + 1, j)) *
+                                          U3(g->amsuo, i, j, 1);
+  for (int j = 1; j <= JE1; ++j)
+    for (int i = 2; i <= IE1; ++i)
+      V2(vse, i, j) = V2(vze, i, j) + c * V2(g->dpye, i, j) * (P2(z1o, i, j + 1) - P2(z1o, i, j)) *
+                                          V3(g->amsue, i, j, 1);
+  /* ocvtro.f90:53-57 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) P2(zo, i, j) = P2(zo, i, j) + P2(z1o, i, j);
+}
+
+void og_ocvtot(const og_grid *g, const og_baro *b, const double *uso, const double *vse,
+               double *uoo, double *voe, double *uko, double *vke, double *wo) {
+  DIMS;
+  const double conn = b->conn, cono = 1. - b->conn, dti = 1. / g->dt;
+  /* ocvtot.f90:13-29 (T1O/S1O, copies of UOO/VOE, are not kept) */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i)
+        U3(uko, i, j, k) = U3(g->amsuo, i, j, k) * (U2(uso, i, j) + U3(uko, i, j, k));
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i)
+        V3(vke, i, j, k) = V3(g->amsue, i, j, k) * (V2(vse, i, j) + V3(vke, i, j, k));
+  }
+  /* ocvtot.f90:43-61 */
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        const double uako = U3(uko, i, j, k);
+        U3(uko, i, j, k) = conn * U3(uko, i, j, k) + U3(uoo, i, j, k) * cono;
+        U3(uoo, i, j, k) = uako;
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        const double vake = V3(vke, i, j, k);
+        V3(vke, i, j, k) = conn * V3(vke, i, j, k) + V3(voe, i, j, k) * cono;
+        V3(voe, i, j, k) = vake;
+      }
+  }
+  /* ocvtot.f90:73-93, WO(KEP) = 0 */
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      P3(wo, i, j, KE + 1) = 0.0;
+      for (int k = KE; k >= 1; --k)
+        P3(wo, i, j, k) =
+            P3(wo, i, j, k + 1) +
+            dti * P3(g->weto, i, j, k) *
+                (P2(g->dtdxpo, i, j) *
+                 (U3(uko, i - 1, j, k) * U3(g->dduo, i - 1, j, k) * U2(g->dlyu, i - 1, j) -
+                  U3(uko, i, j, k) * U3(g->dduo, i, j, k) * U2(g->dlyu, i, j)) /
+                 P2(g->dlyp, i, j)) +
+            dti * P3(g->weto, i, j, k) *
+                (+P2(g->dtdyo, i, j) *
+                 (V3(vke, i, j, k) * V3(g->ddue, i, j, k) * V2(g->dlxv, i, j) -
+                  V3(vke, i, j - 1, k) * V3(g->ddue, i, j - 1, k) * V2(g->dlxv, i, j - 1)) /
+                 P2(g->dlxp, i, j));
+    }
+}

@@ -127,6 +127,38 @@ void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], do
 void og_octimf(const og_grid *g, const double *uoo, const double *voe,
                double *uko, double *vke);
 
+/* ---- Barotropic (free-surface) solve and total velocities ------------------
+ * Constants of the reference's driver (orctm.f90:352-353, 657-661, 680):
+ * G = 9.806, STABN = 0.6, CONN = 0.5, CONO = 1 - CONN, RLSA1 = 1 - 0.085.
+ * 2D layouts: p (IE, JE), u (IE+1, JE) from I = 0, v (IE, JE+1) from J = 0. */
+typedef struct og_baro {
+  double grav, stabn, conn, rlsa1, sorpar;
+  int niter;      /* SOR sweeps (250, troneu.f90:104) */
+  int eta_forc;   /* OBC_ETA_FORC set: the boundary Z1O stays 0 (troneu.f90:67-102) */
+} og_baro;
+
+/* DEUTO / DEUTE and their inverses DEUTIO / DEUTIE from the BODEN-adjusted
+ * DEPTO (boden.f90:117-128, 264-274); minvalue is the reference's small
+ * threshold. */
+void og_deut(const og_grid *g, const double *depto, double minvalue, double *deuto,
+             double *deute, double *deutio, double *deutie);
+/* ITPREP (itprep.f90:15-40): XX, FF (p), UF (u), VF (v). */
+void og_itprep(const og_grid *g, const og_baro *b, const double *deuto, const double *deute,
+               double *xx, double *uf, double *vf, double *ff);
+/* TRONEU (troneu.f90:48-134): B1O and the red-black SOR for Z1O. */
+void og_troneu(const og_grid *g, const og_baro *b, const double *xx, const double *uf,
+               const double *vf, const double *ff, const double *u1o, const double *v1e,
+               const double *uzo, const double *vze, double *b1o, double *z1o);
+/* OCVTRO (ocvtro.f90:1-62): UZO, VZE scaled by the inverse depths, the
+ * barotropic velocities USO, VSE, and ZO += Z1O. */
+void og_ocvtro(const og_grid *g, const og_baro *b, const double *deutio, const double *deutie,
+               const double *z1o, double *uzo, double *vze, double *uso, double *vse, double *zo);
+/* OCVTOT (ocvtot.f90:13-96): UKO, VKE with the barotropic part, the time
+ * filter UKO <- CONN UKO + CONO UOO with UOO <- the unfiltered value, and WO
+ * from the divergence, bottom up. */
+void og_ocvtot(const og_grid *g, const og_baro *b, const double *uso, const double *vse,
+               double *uoo, double *voe, double *uko, double *vke, double *wo);
+
 #ifdef __cplusplus
 }
 #endif
