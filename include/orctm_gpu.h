@@ -28,6 +28,11 @@
  *                                            mo_obcs.f90:1881-2032, 2295-2582
  *   orctm_set_obc_ts / orctm_obc_ts  FORC_OBCS_TS + SPONGE_OBCS_TS(THO,SAO)
  *                       octher.f90:114-119, mo_obcs.f90:932-1272
+ *   orctm_set_barotropic  SUBROUTINE ITPREP  itprep.f90:15-40 (with BODEN's
+ *                       inverse u/v depths, boden.f90:264-274)
+ *   orctm_troneu        SUBROUTINE TRONEU    troneu.f90:48-134
+ *   orctm_ocvtro        SUBROUTINE OCVTRO    ocvtro.f90:1-62
+ *   orctm_ocvtot        SUBROUTINE OCVTOT    ocvtot.f90:13-96
  *   orctm_upload / orctm_download   the module arrays of MO_COMMO1
  *                                   (mo_commo1.f90:32-146) that the path reads
  *                                   and writes, moved between host and device
@@ -269,6 +274,50 @@ int orctm_obc_uv(orctm_handle* h, int ldtrun);
 int orctm_set_obc_ts(orctm_handle* h, int tracer, const double* const* cli);
 int orctm_obc_ts(orctm_handle* h);
 
+/* ---- Barotropic (free-surface) solve and total velocities --------------
+ * The part of the reference step that runs just before the hot path
+ * (orctm.f90:1411-1431): TRONEU, OCVTRO, OCVTOT.  2D host arrays use the
+ * layouts above: p (IE, JE), u (IE+1, JE) from I = 0, v (IE, JE+1) from J = 0.
+ *
+ * orctm_set_barotropic replaces ITPREP (itprep.f90:15-40, called once at
+ * start-up, orctm.f90:872) and BODEN's inverse u/v depths
+ * (boden.f90:264-274): XX, UF, VF, FF and DEUTIO, DEUTIE on the device, from
+ * DEUTO / DEUTE (boden.f90:117-128) and the run's constants. */
+typedef struct orctm_barotropic {
+  const double* deuto;  /* host, u-points: MIN of the neighbouring DEPTO */
+  const double* deute;  /* host, v-points */
+  double minvalue;      /* BODEN's threshold MIN(1, DZW(1)/10): DEUTIO = 0 at or below it */
+  double grav;          /* G (9.806, orctm.f90:680) */
+  double stabn;         /* STABN (0.6, orctm.f90:657) */
+  double conn;          /* CONN (0.5, orctm.f90:660); CONO = 1 - CONN */
+  double rlsa1;         /* 1 - rlsa (0.915, orctm.f90:352-353) */
+  double sorpar;        /* SORPAR (TROTEST's choice, trotest.f90) */
+  int niter;            /* SOR sweeps (250, troneu.f90:104) */
+  int eta_forc;         /* OBC_ETA_FORC: the boundary Z1O stays 0 (troneu.f90:67) */
+} orctm_barotropic;
+int orctm_set_barotropic(orctm_handle* h, const orctm_barotropic* b);
+/* TRONEU (troneu.f90:48-134): uploads U1O, UZO (u-points) and V1E, VZE
+ * (v-points), forms B1O and runs the red-black SOR for Z1O on the device. */
+int orctm_troneu(orctm_handle* h, const double* u1o, const double* v1e, const double* uzo,
+                 const double* vze);
+/* OCVTRO (ocvtro.f90:1-62): UZO, VZE scaled by the inverse depths, the
+ * barotropic velocities USO, VSE, and ZO += Z1O (device, in place). */
+int orctm_ocvtro(orctm_handle* h);
+/* OCVTOT (ocvtot.f90:13-96): UKO, VKE with USO, VSE added and the time filter
+ * UKO <- CONN UKO + CONO UOO, UOO <- the unfiltered value (the same for v),
+ * and WO from the divergence of the filtered velocities, bottom up. */
+int orctm_ocvtot(orctm_handle* h);
+/* 2D barotropic fields to the host: which = ORCTM_B_* below. */
+enum {
+  ORCTM_B_Z1O = 0,  /* p-points */
+  ORCTM_B_B1O = 1,  /* p-points */
+  ORCTM_B_USO = 2,  /* u-points */
+  ORCTM_B_VSE = 3,  /* v-points */
+  ORCTM_B_UZO = 4,  /* u-points */
+  ORCTM_B_VZE = 5   /* v-points */
+};
+int orctm_download_barotropic(orctm_handle* h, int which, double* host, size_t n);
+
 /* solver mode and relative-residual target (default FP64, 1e-10, 5000) */
 int orctm_set_solver(orctm_handle* h, int mode, double rtol, int maxit);
 int orctm_synchronize(orctm_handle* h);
@@ -429,7 +478,11 @@ int orctm_build_grid(int ie, int je, int ke, double dt, const double* dzw, doubl
  * exits), which limits IE*JE*KE to 2,097,152 cells; larger grids return
  * ORCTM_E_TOO_LARGE.  The first call on each device looks up that array's
  * device address (cudaGetSymbolAddress) with the device current: make that
- * first call before any stream capture.  All calls share the array and it
+ * first call before any stream capture (a first call on a capturing stream
+ * returns ORCTM_E_ARG).  Calls on a stream that is not capturing look the
+ * address up again, so after a cudaDeviceReset one such call must precede
+ * the next capture.  A refused call's message is orctm_last_error(NULL).
+ * All calls share the array and it
  * keeps the last call's contents; every value a call reads is written earlier
  * in the same call.  Calls that overlap on the GPU race on the array: order
  * them on one stream.  The kernels are enqueued on args->stream and the call

@@ -362,3 +362,34 @@ def copy_state(inst: dict) -> dict:
     st = {k: np.array(inst[k], order="F", copy=True) for k in STATE_KEYS}
     st["tracers"] = [np.array(t, order="F", copy=True) for t in inst["tracers"]]
     return st
+
+
+def barotropic_minvalue(inst: dict) -> float:
+    """BODEN's small thickness threshold MIN(1, DZW(1)/10) (boden.f90)."""
+    return min(1.0, float(inst["dzw"][0]) / 10.0)
+
+
+def make_barotropic(inst: dict, seed: int | None = None) -> dict:
+    """Seeded inputs of the barotropic solve (TRONEU, OCVTRO, OCVTOT): the
+    previous and the new vertically integrated transports U1O/UZO (u-points,
+    (IE+1, JE), m^2/s) and V1E/VZE (v-points, (IE, JE+1)), smooth, of the
+    size of the instance's velocities times its depths, zero where the
+    column is dry."""
+    ie, je = inst["ie"], inst["je"]
+    g = rng((inst["seed"] if seed is None else seed) + 31337)
+    depth = np.asarray(inst["depto"], dtype=np.float64)
+    du = np.zeros((ie + 1, je))
+    du[1:ie, :] = np.minimum(depth[:-1, :], depth[1:, :])
+    dv = np.zeros((ie, je + 1))
+    dv[:, 1:je] = np.minimum(depth[:, :-1], depth[:, 1:])
+
+    def smooth(shape, amp):
+        a = g.standard_normal(shape)
+        a = _gauss_filter2d(a, 3.0) if min(shape) > 8 else a
+        return np.asfortranarray(amp * a / max(np.abs(a).max(), 1e-30))
+
+    out = {}
+    for k, shp, d in (("u1o", (ie + 1, je), du), ("uzo", (ie + 1, je), du),
+                      ("v1e", (ie, je + 1), dv), ("vze", (ie, je + 1), dv)):
+        out[k] = np.asfortranarray(smooth(shp, 0.1) * d)
+    return out

@@ -45,6 +45,13 @@ module orctm_gpu_mod
      type(c_ptr) :: amp(3, 4), pha(3, 4)
   end type orctm_obc
 
+  ! barotropic solve (ITPREP's inputs and the run's constants)
+  type, bind(c) :: orctm_barotropic
+     type(c_ptr) :: deuto, deute
+     real(c_double) :: minvalue, grav, stabn, conn, rlsa1, sorpar
+     integer(c_int) :: niter, eta_forc
+  end type orctm_barotropic
+
   interface
      integer(c_int) function orctm_create(desc, h) bind(c, name="orctm_create")
        import :: c_int, c_ptr, orctm_desc
@@ -119,6 +126,30 @@ module orctm_gpu_mod
      integer(c_int) function orctm_obc_ts(h) bind(c, name="orctm_obc_ts")
        import :: c_int, c_ptr
        type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_set_barotropic(h, b) bind(c, name="orctm_set_barotropic")
+       import :: c_int, c_ptr, orctm_barotropic
+       type(c_ptr), value :: h
+       type(orctm_barotropic), intent(in) :: b
+     end function
+     integer(c_int) function orctm_troneu(h, u1o, v1e, uzo, vze) bind(c, name="orctm_troneu")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, u1o, v1e, uzo, vze
+     end function
+     integer(c_int) function orctm_ocvtro(h) bind(c, name="orctm_ocvtro")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocvtot(h) bind(c, name="orctm_ocvtot")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_download_barotropic(h, which, host, n) &
+         bind(c, name="orctm_download_barotropic")
+       import :: c_int, c_ptr, c_size_t
+       type(c_ptr), value :: h, host
+       integer(c_int), value :: which
+       integer(c_size_t), value :: n
      end function
      integer(c_int) function orctm_ocvisc(h) bind(c, name="orctm_ocvisc")
        import :: c_int, c_ptr

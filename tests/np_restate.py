@@ -986,3 +986,111 @@ def ocvisc(g, uoo, voe, wno, uko, vke, avo):
         wno[r, c, k] = (E[r, c] / vol) * (dlxp[r, c] * dlyp[r, c] * dzp[r, c, k] * wno[r, c, k] - t)
     # OCTIMF (ocvisc.f90:767)
     return uoo, voe, wno, uoo.copy(), voe.copy()
+
+
+# --------------------------------------------------------------- barotropic ---
+# Written from boden.f90:117-128, 264-274, itprep.f90:15-40, troneu.f90:48-134,
+# ocvtro.f90:1-62 and ocvtot.f90:13-96.  2D arrays: p (IE, JE), u (IE+1, JE)
+# with index i <-> I, v (IE, JE+1) with index j <-> J.
+
+def deut(g, depto, minvalue):
+    ie, je = g["ie"], g["je"]
+    deuto = np.zeros((ie + 1, je))
+    deuto[1:ie, :] = np.minimum(depto[:-1, :], depto[1:, :])
+    deuto[0, :] = deuto[1, :]
+    deuto[ie, :] = deuto[ie - 1, :]
+    deute = np.zeros((ie, je + 1))
+    deute[:, 1:je] = np.minimum(depto[:, :-1], depto[:, 1:])
+    deute[:, 0] = deute[:, 1]
+    deute[:, je] = deute[:, je - 1]
+    with np.errstate(divide="ignore"):
+        deutio = np.where(deuto > minvalue, 1.0 / np.where(deuto > minvalue, deuto, 1.0), 0.0)
+        deutie = np.where(deute > minvalue, 1.0 / np.where(deute > minvalue, deute, 1.0), 0.0)
+    return deuto, deute, deutio, deutie
+
+
+def itprep(g, b, deuto, deute):
+    dt = g["dt"]
+    xx = g["dlxp"] * g["dlyp"]
+    uf = deuto * g["dlyu"] / g["dlxu"] * b["grav"] * b["conn"] * b["stabn"] * (dt * dt)
+    vf = deute * g["dlxv"] / g["dlyv"] * b["grav"] * b["conn"] * b["stabn"] * (dt * dt)
+    ff = 1.0 / (xx + uf[1:, :] + uf[:-1, :] + vf[:, 1:] + vf[:, :-1])
+    return xx, uf, vf, ff
+
+
+def troneu(g, b, xx, uf, vf, ff, u1o, v1e, uzo, vze):
+    ie, je = g["ie"], g["je"]
+    conn = b["conn"]
+    cono = 1.0 - conn
+    fu = (cono * u1o + uzo * conn) * g["dlyu"]           # the west face term at I-1 ...
+    fu2 = (u1o * cono + uzo * conn) * g["dlyu"]          # ... and the east face term at I
+    fv = (v1e * cono + conn * vze) * g["dlxv"]
+    b1o = g["weto"][:, :, 0] * (g["dtdxpo"] * (fu[:-1, :] - fu2[1:, :]) / g["dlyp"]
+                                + g["dtdyo"] * (fv[:, 1:] - fv[:, :-1]) / g["dlxp"])
+    b1o = b1o * xx
+    z = np.zeros((ie, je))
+    if not b["eta_forc"]:
+        z[0, :] = b1o[0, :] / xx[0, :]
+        z[ie - 1, :] = b1o[ie - 1, :] / xx[ie - 1, :]
+        z[:, 0] = b1o[:, 0] / xx[:, 0]
+        z[:, je - 1] = b1o[:, je - 1] / xx[:, je - 1]
+    # red-black masks over the interior I = 2..IE-1, J = 2..JE-1 (0-based 1..)
+    I, J = np.meshgrid(np.arange(1, ie + 1), np.arange(1, je + 1), indexing="ij")
+    inner = (I >= 2) & (I <= ie - 1) & (J >= 2) & (J <= je - 1)
+    colour = [inner & ((I + J) % 2 == 0), inner & ((I + J) % 2 == 1)]
+    sorpar = b["sorpar"]
+    sorpai = 1.0 - sorpar
+    ufe = np.zeros((ie, je)); ufw = np.zeros((ie, je))
+    vfs = np.zeros((ie, je)); vfn = np.zeros((ie, je))
+    ufe[:, :] = uf[1:, :]       # UF(I,J)
+    ufw[:, :] = uf[:-1, :]      # UF(I-1,J)
+    vfs[:, :] = vf[:, 1:]       # VF(I,J)
+    vfn[:, :] = vf[:, :-1]      # VF(I,J-1)
+    for _ in range(b["niter"]):
+        for m in colour:
+            ze = np.zeros_like(z); zw = np.zeros_like(z); zs = np.zeros_like(z); zn = np.zeros_like(z)
+            ze[:-1, :] = z[1:, :]
+            zw[1:, :] = z[:-1, :]
+            zs[:, :-1] = z[:, 1:]
+            zn[:, 1:] = z[:, :-1]
+            new = sorpar * ff * (b1o + ufe * ze + ufw * zw + vfs * zs + vfn * zn) + sorpai * z
+            z = np.where(m, new, z)
+    return b1o, z
+
+
+def ocvtro(g, b, deutio, deutie, z1o, uzo, vze, zo):
+    ie, je = g["ie"], g["je"]
+    c = b["rlsa1"] * b["grav"] * b["stabn"]
+    uzo = uzo * deutio
+    vze = vze * deutie
+    uso = uzo.copy()
+    vse = vze.copy()
+    # USO: I = 1..IE-1, J = 2..JE-1
+    uso[1:ie, 1:je - 1] = (uzo[1:ie, 1:je - 1] + c * g["dtdxuo"][1:ie, 1:je - 1]
+                           * (z1o[0:ie - 1, 1:je - 1] - z1o[1:ie, 1:je - 1])
+                           * g["amsuo"][1:ie, 1:je - 1, 0])
+    # VSE: I = 2..IE-1, J = 1..JE-1
+    vse[1:ie - 1, 1:je] = (vze[1:ie - 1, 1:je] + c * g["dpye"][1:ie - 1, 1:je]
+                           * (z1o[1:ie - 1, 1:je] - z1o[1:ie - 1, 0:je - 1])
+                           * g["amsue"][1:ie - 1, 1:je, 0])
+    return uzo, vze, uso, vse, zo + z1o
+
+
+def ocvtot(g, b, uso, vse, uoo, voe, uko, vke):
+    conn = b["conn"]
+    cono = 1.0 - conn
+    dti = 1.0 / g["dt"]
+    uk = g["amsuo"] * (uso[:, :, None] + uko)
+    vk = g["amsue"] * (vse[:, :, None] + vke)
+    uko_n = conn * uk + uoo * cono
+    vke_n = conn * vk + voe * cono
+    uoo_n, voe_n = uk, vk
+    fu = uko_n * g["dduo"] * g["dlyu"][:, :, None]
+    fv = vke_n * g["ddue"] * g["dlxv"][:, :, None]
+    tx = dti * g["weto"] * (g["dtdxpo"][:, :, None] * (fu[:-1] - fu[1:]) / g["dlyp"][:, :, None])
+    ty = dti * g["weto"] * (g["dtdyo"][:, :, None] * (fv[:, 1:] - fv[:, :-1]) / g["dlxp"][:, :, None])
+    ke = g["ke"]
+    wo = np.zeros(g["weto"].shape[:2] + (ke + 1,))
+    for k in range(ke - 1, -1, -1):
+        wo[:, :, k] = wo[:, :, k + 1] + tx[:, :, k] + ty[:, :, k]
+    return uoo_n, voe_n, uko_n, vke_n, wo
