@@ -220,7 +220,8 @@ def run_reference(args, ws, rank, pg):
     """The reference arm: the reference's Fortran/PETSc path cannot be built on
     this image, so its CPU restatement (the oracle, OpenMP on every host core)
     runs the same workload's generators on a bounded sub-domain, one hot-path
-    step per bench step (W untimed, K timed).  Rank 0 only."""
+    step per bench step (W untimed, K timed).  Rank 0 only.  The line's
+    config names the sub-domain it timed, and the full workload it samples."""
     if rank != 0:
         return 0
     from orctm_b200 import configs
@@ -229,18 +230,62 @@ def run_reference(args, ws, rank, pg):
     if args.size:
         nx, ny, nz = (int(v) for v in args.size.split("x"))
         over = {"nx": nx, "ny": ny, "nz": nz}
-    inst = configs.raw_instance(args.config, index=0, **over)
+    full = configs.raw_instance(args.config, index=0, **over)
+    nx, ny, nz = args.cpu_sample
+    inst = configs.raw_instance(args.config, index=0, nx=nx, ny=ny, nz=nz)
     cb = cpu_sample(args, steps=args.steps, warmup=args.warmup)
+    cfg = workload_config(inst)
+    if (nx, ny, nz) != (full["nx"], full["ny"], full["nz"]):
+        cfg["workload"] = (f"{inst['name']} {nx}x{ny}x{nz} sub-domain sample of the "
+                           f"{full['nx']}x{full['ny']}x{full['nz']} workload (same generators, "
+                           f"dx, dz, dt={inst['dt']:g}s)")
+        cfg["sampled_workload"] = workload_config(full)["workload"]
+    cfg["solver"] = "FGMRES(30) + column (line) preconditioner, FP64, C restatement"
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"],
             "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
-            "config": workload_config(inst),
+            "config": cfg,
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def tracer_content(inst, t) -> float:
+    """Sum of T * V over the wet interior cells, V = DLXP DLYP (DDPO + ZO at
+    the surface level): the tracer content the advection and diffusion
+    conserve apart from the fluxes through open boundaries."""
+    area = (inst["dlxp"] * inst["dlyp"])[1:-1, 1:-1]
+    tot = 0.0
+    for k in range(inst["ke"]):
+        th = inst["ddpo"][1:-1, 1:-1, k] + (inst["zo"][1:-1, 1:-1] if k == 0 else 0.0)
+        tot += float(np.sum(t[1:-1, 1:-1, k] * inst["weto"][1:-1, 1:-1, k] * th * area))
+    return tot
+
+
+def compare_forms(inst, a, b, nsteps) -> dict:
+    """Fields of the FP32-refined form (b) against the FP64 form (a) after the
+    same steps from the same state: relative max-norm differences, and each
+    form's tracer-content drift from the initial state."""
+    def rel(x, y):
+        return float(np.abs(x - y).max() / max(np.abs(y).max(), 1e-300))
+
+    out = {"steps": nsteps, "rel_maxnorm": {}, "tracer_content_drift": {}}
+    for k in ("pnh", "uoo", "voe", "wno"):
+        out["rel_maxnorm"][k] = rel(b.download(k), a.download(k))
+    for n in range(a.ntr):
+        ta, tb = a.download(f"tracer{n}"), b.download(f"tracer{n}")
+        out["rel_maxnorm"][f"tracer{n}"] = rel(tb, ta)
+        c0 = tracer_content(inst, inst["tracers"][n])
+        ca, cb = tracer_content(inst, ta), tracer_content(inst, tb)
+        out["tracer_content_drift"][f"tracer{n}"] = {
+            "fp64": (ca - c0) / abs(c0), "fp32_refined": (cb - c0) / abs(c0),
+            "forms_differ_by": (cb - ca) / abs(c0)}
+    out["note"] = ("open W and S boundaries: the content changes through boundary fluxes; "
+                   "the two forms' drifts differ by forms_differ_by")
+    return out
 
 
 def timed_steps(gpu, k, pg):
@@ -279,9 +324,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-sample", type=lambda s: tuple(int(v) for v in s.split("x")),
-                    default=(128, 128, 80))
+                    default=None, help="sub-domain the CPU restatement times (default: the "
+                    "whole c1 slice; 128x128xNZ for the 3D configurations)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.cpu_sample is None:
+        args.cpu_sample = {"c1": (512, 1, 60), "c2": (128, 128, 60)}.get(args.config, (128, 128, 80))
     ws, rank, local, pg = dist_setup()
     if args.impl == "reference":
         return run_reference(args, ws, rank, pg)
@@ -318,10 +366,16 @@ def main():
     relres = max(s["relres"] for s in stats2)
 
     # ---- FP32-refined solver form ------------------------------------------
-    gpu.set_solver("fp32_refined", rtol=1e-10, maxit=5000)
-    for _ in range(2):
-        gpu.step_hotpath()
-    ms_m, stats_m, _ = timed_steps(gpu, args.steps, pg)
+    # a second instance from the same initial state, stepped as often as the
+    # FP64 one (W warm-up, K untimed, K timed), so that the two forms' fields
+    # can be compared after the same number of steps
+    nsteps = args.warmup + 2 * args.steps
+    gpu2 = Instance(inst, device=local)
+    gpu2.upload_state(configs.copy_state(inst))
+    gpu2.set_solver("fp32_refined", rtol=1e-10, maxit=5000)
+    for _ in range(args.warmup + args.steps):
+        gpu2.step_hotpath()
+    ms_m, stats_m, _ = timed_steps(gpu2, args.steps, pg)
     ms_m = max_over_ranks(pg, ms_m)
     mixed = {"value": ws * cells * args.steps / (ms_m / 1e3), "unit": "cell-steps/s",
              "ms_per_step": ms_m / args.steps,
@@ -331,9 +385,10 @@ def main():
              "relres_max": max(s["relres"] for s in stats_m)}
     mixed["speedup_vs_fp64"] = mixed["value"] / value
     mixed["solver_speedup_vs_fp64"] = poisson_ms / mixed["poisson_ms"]
-    tuning = {"fp64": list(gpu.tuning("fp64")), "fp32_refined": list(gpu.tuning("fp32_refined")),
+    mixed["vs_fp64"] = compare_forms(inst, gpu, gpu2, nsteps)
+    tuning = {"fp64": list(gpu.tuning("fp64")), "fp32_refined": list(gpu2.tuning("fp32_refined")),
               "meaning": "(column-kernel variant, stencil-kernel variant) picked by the autotuner"}
-    gpu.set_solver("fp64", rtol=1e-10, maxit=5000)
+    gpu2.close()
 
     # ---- roofline of the dominant kernel --------------------------------
     hbm, peak_kind = peaks()

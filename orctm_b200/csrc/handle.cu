@@ -49,6 +49,8 @@ int cuda_status(cudaError_t e) {
 
 namespace {
 
+// text of the calling thread's last failure of a call made without a handle
+// (orctm_create, orctm_octdiff_noalloc), returned by orctm_last_error(NULL)
 thread_local std::string g_create_error;
 
 // One stream-ordered memory pool per device, owned by the library.  Freed
@@ -116,6 +118,13 @@ Kind field_kind(int f) {
 }
 
 }  // namespace
+
+void set_unbound_error(const char* msg) { g_create_error = msg ? msg : ""; }
+void clear_unbound_errors() {
+  g_create_error.clear();
+  g_cuda_error.clear();
+}
+
 }  // namespace orctm
 
 using namespace orctm;
@@ -178,6 +187,12 @@ struct orctm_handle {
   ObcArgs obc_ts[2] = {};
   double* obc_ts_buf[2] = {nullptr, nullptr};
   size_t obc_ts_cap[2] = {0, 0};
+  // barotropic solve (orctm_set_barotropic): its constants, its 2D device
+  // fields and TRONEU's SOR sweeps captured once as a graph
+  bool baro_ready = false;
+  BaroArgs baro{};
+  BaroFields bf{};
+  cudaGraphExec_t sor_graph = nullptr;
   // replayed chunk of PCG iterations per precision and the variants it holds
   cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
   int pcg_graph_key[2][2] = {{-1, -1}, {-1, -1}};
@@ -742,14 +757,20 @@ int pcg_chunk_graph(orctm_handle* h, const T* b, TX* x, T* r, T* z, T* pa, T* pb
   }
   const unsigned long long before = launch_count();
   ORCTM_CUDA_OK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e0 = cudaSuccess;
   T *pc = pa, *pn = pb;
   for (int k = 0; k < kPcgChunk; ++k) {
-    launch_pcg_spmv<T>(h->G, h->P, h->S, z, pc, pn, q, 0, sv, h->stream);
+    if (e0 == cudaSuccess) e0 = launch_pcg_spmv<T>(h->G, h->P, h->S, z, pc, pn, q, 0, sv, h->stream);
     launch_pcg_col<T, TX>(h->G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream);
     std::swap(pc, pn);
   }
   cudaGraph_t g = nullptr;
   const cudaError_t e1 = cudaStreamEndCapture(h->stream, &g);
+  if (e0 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    add_launches(-(long long)(launch_count() - before));
+    return cuda_status(e0);
+  }
   // launches are counted when the graph runs, not when it is recorded
   add_launches(-(long long)(launch_count() - before));
   ORCTM_CUDA_OK(e1);
@@ -784,7 +805,8 @@ int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* p
       add_launches(2 * kPcgChunk);
       it += kPcgChunk;  // pc, pn end where they started
     } else {
-      PROF(h, ORCTM_PROF_PCG_SPMV, (launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, sv, h->stream)));
+      PROF(h, ORCTM_PROF_PCG_SPMV,
+           ORCTM_CUDA_OK(launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, sv, h->stream)));
       PROF(h, ORCTM_PROF_PCG_COL, (launch_pcg_col<T, TX>(G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream)));
       ORCTM_CUDA_OK(cudaGetLastError());  // a rejected launch is reported at once
       std::swap(pc, pn);
@@ -873,10 +895,13 @@ int autotune(orctm_handle* h, T* x, T* r, T* z, T* pa, T* pb, T* q) {
     if (ms < bc) { bc = ms; best_c = v; }
   }
   for (int v = 0; v < pcg_spmv_variants(); ++v) {
+    if (!pcg_spmv_variant_ok(v)) continue;
     float ms;
-    if ((st = timed([&] { launch_pcg_spmv<T>(G, h->P, h->S_tune, z, pa, pb, q, 0, v, h->stream); },
+    cudaError_t le = cudaSuccess;
+    if ((st = timed([&] { le = launch_pcg_spmv<T>(G, h->P, h->S_tune, z, pa, pb, q, 0, v, h->stream); },
                     &ms)))
       return st;
+    if (le != cudaSuccess) continue;
     if (ms < bs) { bs = ms; best_s = v; }
   }
   {
@@ -898,6 +923,14 @@ int ensure_tuned(orctm_handle* h, bool f32) {
   }
   if (f32) return autotune<float>(h, h->d32, h->r32, h->z32, h->p32a, h->p32b, h->q32);
   return autotune<double>(h, h->d, h->rw, h->z, h->p0, h->p1, h->q);
+}
+
+// converged = 4: a bounded wait inside a kernel (a TMA stage that never
+// arrived) gave up; the solve stops and reports it as a device error.
+int check_device_wait(orctm_handle* h, int conv) {
+  if (conv != 4) return ORCTM_OK;
+  h->err = "a device-side wait for a staged copy timed out in the Poisson stencil kernel";
+  return ORCTM_E_CUDA;
 }
 
 // Solves A x = b (b in h->b, x in h->xs holding the warm start) by iterative
@@ -940,6 +973,7 @@ int poisson_solve(orctm_handle* h, orctm_solve_stats* stats) {
       if ((st = pcg_loop<float, float>(h, 1, h->r32b, h->d32, h->r32, h->z32, h->p32a, h->p32b,
                                        h->q32, h->maxit - total, &its, &conv)))
         return st;
+      if ((st = check_device_wait(h, conv))) return st;
       launch_axpy_f32(G, h->d32, h->S, h->xs, h->stream);
     } else {
       ORCTM_CUDA_OK(cudaMemsetAsync(h->d, 0, sizeof(double) * n3, h->stream));
@@ -947,6 +981,7 @@ int poisson_solve(orctm_handle* h, orctm_solve_stats* stats) {
       if ((st = pcg_loop<double, double>(h, 1, h->r, h->d, h->rw, h->z, h->p0, h->p1, h->q,
                                          h->maxit - total, &its, &conv)))
         return st;
+      if ((st = check_device_wait(h, conv))) return st;
       launch_axpy_f64(G, h->d, h->xs, h->stream);
     }
     ORCTM_CUDA_OK(cudaGetLastError());
@@ -1119,16 +1154,16 @@ int r_octdiff(orctm_handle* h) {
   ORCTM_CUDA_OK(cudaGetLastError());
   for (int n = 0; n < ntr; ++n) h->bind(ORCTM_F_THO + n, outv[n]);
   if (h->G.aulapts > h->G.almzer) {
-    double* lap;
-    if ((st = h->alloc(&lap))) return st;
+    // Laplacian and biharmonic update of every tracer in one fused launch
+    const double* vin[kMaxTracers];
+    double* bout[kMaxTracers];
     for (int n = 0; n < ntr; ++n) {
-      double* out;
-      if ((st = h->alloc(&out))) return st;
-      PROF(h, ORCTM_PROF_OCTDIFF, launch_octdiff_bih(h->G, h->slot[ORCTM_F_THO + n], h->zo, lap, out, h->stream));
-      h->bind(ORCTM_F_THO + n, out);
+      vin[n] = h->slot[ORCTM_F_THO + n];
+      if ((st = h->alloc(&bout[n]))) return st;
     }
+    PROF(h, ORCTM_PROF_OCTDIFF, launch_octdiff_hbih(h->G, ntr, vin, bout, h->zo, h->stream));
     ORCTM_CUDA_OK(cudaGetLastError());
-    h->unref(lap);
+    for (int n = 0; n < ntr; ++n) h->bind(ORCTM_F_THO + n, bout[n]);
   }
   return ORCTM_OK;
 }
@@ -1149,22 +1184,20 @@ int r_ocvisc(orctm_handle* h) {
     if (st0) return st0;
   }
   int st;
-  double *sp, *ukv, *vkv, *wnv, *u1, *v1, *w1, *uo, *vo, *wo;
+  double *sp, *ukv, *vkv, *wnv, *uo, *vo, *wo;
   if ((st = h->alloc(&sp)) || (st = h->alloc(&ukv)) || (st = h->alloc(&vkv)) ||
-      (st = h->alloc(&wnv)) || (st = h->alloc(&u1)) || (st = h->alloc(&v1)) ||
-      (st = h->alloc(&w1)) || (st = h->alloc(&uo)) || (st = h->alloc(&vo)) || (st = h->alloc(&wo)))
+      (st = h->alloc(&wnv)) || (st = h->alloc(&uo)) || (st = h->alloc(&vo)) || (st = h->alloc(&wo)))
     return st;
   // the two 2D speed fields live in the first two planes of one scratch buffer
   PROF(h, ORCTM_PROF_OCVISC,
        launch_ocvisc(h->G, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE], h->slot[ORCTM_F_WNO],
                      h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], h->slot[ORCTM_F_AVO], sp,
-                     sp + h->L.plane, ukv, vkv, wnv, u1, v1, w1, uo, vo, wo, h->stream));
+                     sp + h->L.plane, ukv, vkv, wnv, uo, vo, wo, h->stream));
   ORCTM_CUDA_OK(cudaGetLastError());
   h->bind(ORCTM_F_UOO, uo);
   h->bind(ORCTM_F_VOE, vo);
   h->bind(ORCTM_F_WNO, wo);
   h->unref(sp); h->unref(ukv); h->unref(vkv); h->unref(wnv);
-  h->unref(u1); h->unref(v1); h->unref(w1);
   return r_octimf(h);  // ocvisc.f90:767
 }
 
@@ -1276,6 +1309,7 @@ int orctm_destroy(orctm_handle* h) {
   }
   for (int pr = 0; pr < 2; ++pr)
     if (h->pcg_graph[pr]) cudaGraphExecDestroy(h->pcg_graph[pr]);
+  if (h->sor_graph) cudaGraphExecDestroy(h->sor_graph);
   if (h->hS) pinned_state_put(h->hS);
   for (int k = 0; k < ORCTM_PROF_KINDS; ++k)
     for (auto& pr : h->prof_pairs[k]) {
@@ -1715,6 +1749,152 @@ int orctm_obc_uv(orctm_handle* h, int ldtrun) {
   au.t = av.t = (double)ldtrun * h->G.dt;
   launch_obc_uv(h->G, au, av, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE], h->stream);
   ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+// ------------------------------------------------------------ barotropic
+int orctm_set_barotropic(orctm_handle* h, const orctm_barotropic* b) {
+  ORCTM_ENTER(h);
+  if (!b || !b->deuto || !b->deute)
+    return h->fail(ORCTM_E_ARG, "orctm_set_barotropic: missing DEUTO or DEUTE");
+  if (b->niter < 0 || !(b->sorpar > 0.0 && b->sorpar < 2.0) || !(b->grav > 0.0))
+    return h->fail(ORCTM_E_ARG, "orctm_set_barotropic: niter >= 0, 0 < SORPAR < 2 and G > 0");
+  const int IE = h->L.ie, JE = h->L.je;
+  const size_t n2 = (size_t)h->L.plane;
+  int st;
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
+  if (!h->bf.xx) {
+    double** all[] = {&h->bf.xx,  &h->bf.ff,     &h->bf.b1o, &h->bf.z1o, &h->bf.uf,
+                      &h->bf.deutio, &h->bf.u1o, &h->bf.uzo, &h->bf.uso, &h->bf.vf,
+                      &h->bf.deutie, &h->bf.v1e, &h->bf.vze, &h->bf.vse};
+    for (double** p : all)
+      if ((st = h->dev_alloc(p, n2))) return st;
+  }
+  // the depths pass through the two scratch slots of the transports
+  if ((st = upload_2d(h, h->bf.u1o, b->deuto, 0, IE + 1, 1, JE)) ||
+      (st = upload_2d(h, h->bf.v1e, b->deute, 1, IE, 0, JE + 1)))
+    return st;
+  BaroArgs a{b->grav, b->stabn, b->conn, b->rlsa1, b->sorpar, b->minvalue, b->niter, b->eta_forc ? 1 : 0};
+  launch_itprep(h->G, a, h->bf.u1o, h->bf.v1e, h->bf, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  // the new constants change the SOR launches: capture them again
+  if (h->sor_graph) {
+    ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+    cudaGraphExecDestroy(h->sor_graph);
+    h->sor_graph = nullptr;
+  }
+  h->baro = a;
+  h->baro_ready = true;
+  return ORCTM_OK;
+}
+
+namespace {
+int sor_graph(orctm_handle* h, cudaGraphExec_t* out) {
+  if (h->sor_graph) {
+    *out = h->sor_graph;
+    return ORCTM_OK;
+  }
+  const unsigned long long before = launch_count();
+  ORCTM_CUDA_OK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  for (int it = 0; it < h->baro.niter; ++it) {
+    launch_sor(h->G, h->baro, h->bf, 0, h->stream);
+    launch_sor(h->G, h->baro, h->bf, 1, h->stream);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e1 = cudaStreamEndCapture(h->stream, &g);
+  add_launches(-(long long)(launch_count() - before));  // counted when the graph runs
+  ORCTM_CUDA_OK(e1);
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0ULL);
+  cudaGraphDestroy(g);
+  ORCTM_CUDA_OK(e2);
+  h->sor_graph = *out = ex;
+  return ORCTM_OK;
+}
+}  // namespace
+
+int orctm_troneu(orctm_handle* h, const double* u1o, const double* v1e, const double* uzo,
+                 const double* vze) {
+  ORCTM_ENTER(h);
+  if (!h->baro_ready) return h->fail(ORCTM_E_ARG, "orctm_troneu: orctm_set_barotropic not called");
+  if (!u1o || !v1e || !uzo || !vze) return h->fail(ORCTM_E_ARG, "orctm_troneu: missing array");
+  const int IE = h->L.ie, JE = h->L.je;
+  int st;
+  if ((st = compute_after_copies(h))) return st;
+  if ((st = upload_2d(h, h->bf.u1o, u1o, 0, IE + 1, 1, JE)) ||
+      (st = upload_2d(h, h->bf.uzo, uzo, 0, IE + 1, 1, JE)) ||
+      (st = upload_2d(h, h->bf.v1e, v1e, 1, IE, 0, JE + 1)) ||
+      (st = upload_2d(h, h->bf.vze, vze, 1, IE, 0, JE + 1)))
+    return st;
+  ORCTM_CUDA_OK(cudaMemsetAsync(h->bf.z1o, 0, sizeof(double) * (size_t)h->L.plane, h->stream));
+  launch_troneu_rhs(h->G, h->baro, h->bf, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  if (h->baro.niter > 0) {
+    cudaGraphExec_t ex;
+    if ((st = sor_graph(h, &ex))) return st;
+    ORCTM_CUDA_OK(cudaGraphLaunch(ex, h->stream));
+    add_launches(2LL * h->baro.niter);
+  }
+  return ORCTM_OK;
+}
+
+int orctm_ocvtro(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  if (!h->baro_ready) return h->fail(ORCTM_E_ARG, "orctm_ocvtro: orctm_set_barotropic not called");
+  int st;
+  // ZO is updated in place: after its uploads, and after downloads queued before
+  if ((st = wait_uploads(h, {ORCTM_F_ZO})) || (st = compute_after_copies(h))) return st;
+  launch_ocvtro(h->G, h->baro, h->bf, h->zo, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+int orctm_ocvtot(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  if (!h->baro_ready) return h->fail(ORCTM_E_ARG, "orctm_ocvtot: orctm_set_barotropic not called");
+  {
+    const int st0 = wait_all_uploads(h);  // rebinds slots
+    if (st0) return st0;
+  }
+  int st;
+  double *uo, *vo, *uk, *vk, *wo;
+  if ((st = h->alloc(&uo)) || (st = h->alloc(&vo)) || (st = h->alloc(&uk)) ||
+      (st = h->alloc(&vk)) || (st = h->alloc(&wo)))
+    return st;
+  launch_ocvtot(h->G, h->baro, h->bf.uso, h->bf.vse, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE],
+                h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], uo, vo, uk, vk, wo, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  h->bind(ORCTM_F_UOO, uo);
+  h->bind(ORCTM_F_VOE, vo);
+  h->bind(ORCTM_F_UKO, uk);
+  h->bind(ORCTM_F_VKE, vk);
+  h->bind(ORCTM_F_WO, wo);
+  return ORCTM_OK;
+}
+
+int orctm_download_barotropic(orctm_handle* h, int which, double* host, size_t n) {
+  ORCTM_ENTER(h);
+  if (!h->baro_ready) return h->fail(ORCTM_E_ARG, "orctm_download_barotropic: not set up");
+  const int IE = h->L.ie, JE = h->L.je;
+  const double* src;
+  int i0 = 1, ni = IE, j0 = 1, nj = JE;
+  switch (which) {
+    case ORCTM_B_Z1O: src = h->bf.z1o; break;
+    case ORCTM_B_B1O: src = h->bf.b1o; break;
+    case ORCTM_B_USO: src = h->bf.uso; i0 = 0; ni = IE + 1; break;
+    case ORCTM_B_UZO: src = h->bf.uzo; i0 = 0; ni = IE + 1; break;
+    case ORCTM_B_VSE: src = h->bf.vse; j0 = 0; nj = JE + 1; break;
+    case ORCTM_B_VZE: src = h->bf.vze; j0 = 0; nj = JE + 1; break;
+    default: return h->fail(ORCTM_E_ARG, "orctm_download_barotropic: unknown field");
+  }
+  if (!host || n != (size_t)ni * nj) return h->fail(ORCTM_E_ARG, "orctm_download_barotropic: size");
+  ORCTM_CUDA_OK(cudaMemcpy2DAsync(host, sizeof(double) * ni, src + h->L.at2(i0, j0),
+                                  sizeof(double) * h->L.P, sizeof(double) * ni, nj,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
   return ORCTM_OK;
 }
 

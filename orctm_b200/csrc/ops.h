@@ -47,6 +47,28 @@ struct ObcArgs {
   ObcSide side[4];
 };
 
+// barotropic.cu: constants of the barotropic solve and its 2D device fields
+// (padded plane layout)
+struct BaroArgs {
+  double grav, stabn, conn, rlsa1, sorpar, minvalue;
+  int niter, eta_forc;
+};
+struct BaroFields {
+  double *xx, *ff, *b1o, *z1o;            // p-points
+  double *uf, *deutio, *u1o, *uzo, *uso;  // u-points
+  double *vf, *deutie, *v1e, *vze, *vse;  // v-points
+};
+void launch_itprep(const Geo& G, const BaroArgs& a, const double* deuto, const double* deute,
+                   const BaroFields& f, cudaStream_t st);
+void launch_troneu_rhs(const Geo& G, const BaroArgs& a, const BaroFields& f, cudaStream_t st);
+void launch_sor(const Geo& G, const BaroArgs& a, const BaroFields& f, int parity, cudaStream_t st);
+void launch_ocvtro(const Geo& G, const BaroArgs& a, const BaroFields& f, double* zo,
+                   cudaStream_t st);
+void launch_ocvtot(const Geo& G, const BaroArgs& a, const double* uso, const double* vse,
+                   const double* uoo, const double* voe, const double* uko, const double* vke,
+                   double* uoo_o, double* voe_o, double* uko_o, double* vke_o, double* wo_o,
+                   cudaStream_t st);
+
 // advect.cu
 void launch_ocadpo(const Geo& G, const double* T, const double* uko, const double* vke,
                    const double* wo, const double* zo, double* out, double* tA, double* vA,
@@ -71,12 +93,13 @@ void launch_ocwad(const Geo& G, const double* T, const double* uko, const double
 // diffuse.cu
 void launch_octdiff_vert(const Geo& G, int ntr, const double* const* in, double* const* out,
                          const double* dvo, const double* zo, cudaStream_t st);
-void launch_octdiff_bih(const Geo& G, const double* T, const double* zo, double* lap, double* out,
-                        cudaStream_t st);
+// Laplacian + biharmonic of OCTDIFF_TS for every tracer, fused (no scratch field)
+void launch_octdiff_hbih(const Geo& G, int ntr, const double* const* in, double* const* out,
+                         const double* zo, cudaStream_t st);
 void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const double* wno,
                    const double* uko, const double* vke, const double* avo, double* spu,
-                   double* spv, double* ukv, double* vkv, double* wnv, double* u1, double* v1,
-                   double* w1, double* uo, double* vo, double* wo, cudaStream_t st);
+                   double* spv, double* ukv, double* vkv, double* wnv, double* uo, double* vo,
+                   double* wo, cudaStream_t st);
 
 // obc.cu: FORC_OBCS_ETA + SPONGE_OBCS_ETA on ZO, and FORC_OBCS_UV +
 // UPGRADE_OBCS_UV + SPONGE_OBCS_UV on UOO / VOE, in place
@@ -99,8 +122,9 @@ template <typename T, typename TX>
 void launch_pcg_col(const Geo& G, const PoissonGeo& P, SolverState* S, int mode, const T* b, TX* x,
                     T* r, const T* p, const T* q, T* z, int variant, cudaStream_t st);
 template <typename T>
-void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
-                     T* pnew, T* q, int first, int variant, cudaStream_t st);
+cudaError_t launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z,
+                            const T* pold, T* pnew, T* q, int first, int variant,
+                            cudaStream_t st);
 // kernel variants the autotuner chooses between (a variant a grid cannot use
 // falls back to variant 0)
 int pcg_col_variants();
@@ -110,6 +134,7 @@ cudaError_t pcg_prepare_device();
 template <typename T>
 bool pcg_col_variant_ok(const Geo& G, int variant);
 int pcg_spmv_variants();
+bool pcg_spmv_variant_ok(int variant);
 void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b,
                   const double* x, double* r, cudaStream_t st);
 void launch_axpy_f64(const Geo& G, const double* d, double* x, cudaStream_t st);
@@ -123,6 +148,10 @@ void launch_nh_post(const Geo& G, const double* x, const double* pold, double* p
                     cudaStream_t st);
 
 int cuda_status(cudaError_t e);
+// message of the calling thread's last failed call made without a handle,
+// returned by orctm_last_error(NULL); cleared at the start of such calls
+void set_unbound_error(const char* msg);
+void clear_unbound_errors();
 
 // number of kernels launched by this library (all handles, this process)
 void count_launch();

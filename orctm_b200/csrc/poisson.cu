@@ -31,6 +31,7 @@
 
 #include "common.cuh"
 #include "ops.h"
+#include "tma.cuh"
 
 namespace orctm {
 
@@ -180,6 +181,55 @@ __device__ bool grid_sum(double (&v)[NV], SolverState* S) {
     double x = v[q];
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
     if (lane == 0 && row < nrow) S->partials[(size_t)q * S->max_blocks + row * nchunk + blockIdx.x] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  const unsigned nb = gridDim.x * gridDim.y;
+  if (tid == 0) {
+    const unsigned t = atomicAdd(&S->ticket, 1u);
+    last = (t == nb - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  const unsigned n = nrow * nchunk;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double x = 0.0;
+    if (tid < 64)
+      for (unsigned b = tid; b < n; b += 64)
+        x += ((volatile double*)S->partials)[(size_t)q * S->max_blocks + b];
+    if (tid < 64) {
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[q * 2 + (tid >> 5)] = x;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = sh[q * 2] + sh[q * 2 + 1];
+    S->ticket = 0;
+  }
+  return tid == 0;
+}
+
+// The same reduction for blocks whose warps are identified by (row, chunk)
+// directly (blocks wider than 32 columns, or with a warp that owns no
+// columns: writes = false).  The partial index and the summation order are
+// those of grid_sum, so every form's totals agree bit for bit.
+template <int NV>
+__device__ bool grid_sum_rows(double (&v)[NV], SolverState* S, unsigned row, unsigned chunk,
+                              unsigned nchunk, bool writes) {
+  __shared__ double sh[NV * 2];
+  __shared__ bool last;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y, lane = tid & 31;
+  const unsigned nrow = (unsigned)S->rows;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double x = v[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (writes && lane == 0 && row < nrow && chunk < nchunk)
+      S->partials[(size_t)q * S->max_blocks + row * nchunk + chunk] = x;
   }
   __threadfence();
   __syncthreads();
@@ -706,6 +756,234 @@ __global__ void __launch_bounds__(32 * BY) k_pcg_spmv_wr(Geo G, PoissonGeo P, So
   }
 }
 
+// TMA-staged form.  A block of TX x TY consumer threads (one column each)
+// and one producer warp marches down the levels.  The producer's first lane
+// issues, for every level, tiled bulk-tensor loads of the (TX+4) x (TY+2)
+// halo tiles of z and p_old into an NS-stage shared-memory ring (the tile
+// starts two columns west of the block so that its first element is 16-byte
+// aligned); a stage is refilled once every consumer warp has released it, so
+// up to NS-2 levels are in flight ahead of the two the consumers read.
+// Consumers form p = z + beta p_old for their column and its four horizontal
+// neighbours from the tile, keep p of the level above in a register and read
+// the level below from the next stage.  No block-wide barrier in the level
+// loop; waits on the stage barriers are bounded (a timeout stops the solve
+// with converged = 4).  Positions outside the unknowns hold zeros (the solver
+// vectors are zeroed at allocation and only unknowns are written; loads past
+// the field's extent are zero-filled) and meet zero coefficients, and the
+// arithmetic and dot order equal the other forms', so the results are the
+// same bit for bit.
+template <typename T, int TX, int TY, int NS>
+struct SpmvTma {
+  static constexpr int HX = TX + 4, HY = TY + 2;
+  static constexpr int kArrBytes = HX * HY * (int)sizeof(T);
+  static constexpr int kArrPitch = (kArrBytes + 127) / 128 * 128;
+  static constexpr int kStage = 2 * kArrPitch;
+  static constexpr int kSmem = NS * kStage + 128;  // + alignment slack
+  static constexpr int kConsumers = TX * TY;
+  static constexpr int kThreads = kConsumers + 32;
+  static_assert(TX % 32 == 0, "a warp covers 32 columns of one row");
+  static_assert((HX * sizeof(T)) % 16 == 0, "TMA box rows are whole 16-byte units");
+  static_assert(NS >= 3, "two stages are read while at least one loads");
+};
+
+// Partial of one warp row (row j, 32-column chunk) at its canonical index,
+// summed with the shuffle pattern of grid_sum (a warp's lanes are 32
+// consecutive columns).
+__device__ __forceinline__ void warp_partial(double x, SolverState* S, unsigned row,
+                                             unsigned chunk, unsigned nchunk, int lane) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  if (lane == 0 && row < (unsigned)S->rows && chunk < nchunk)
+    S->partials[row * nchunk + chunk] = x;
+}
+
+// Totals over all partials by the last block to finish (grid_sum's second
+// half): the same index order and 64-thread pattern.
+__device__ bool grid_total1(double& v, SolverState* S) {
+  __shared__ double sh[2];
+  __shared__ bool last;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y, lane = tid & 31;
+  __threadfence();
+  __syncthreads();
+  const unsigned nb = gridDim.x * gridDim.y;
+  if (tid == 0) last = (atomicAdd(&S->ticket, 1u) == nb - 1);
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  const unsigned n = (unsigned)S->rows * (unsigned)((S->max_blocks) / S->rows);
+  double x = 0.0;
+  if (tid < 64)
+    for (unsigned b = tid; b < n; b += 64) x += ((volatile double*)S->partials)[b];
+  if (tid < 64) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[tid >> 5] = x;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    v = sh[0] + sh[1];
+    S->ticket = 0;
+  }
+  return tid == 0;
+}
+
+// The block walks tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (one
+// tile per block when the grid has a block per tile; a persistent grid of a
+// block or two per SM otherwise, so that the producer streams the next
+// tile's first levels while the consumers finish the current one and the
+// block's set-up is paid once).
+template <typename T, int TX, int TY, int NS>
+__global__ void __launch_bounds__(TX * TY + 32, 1)
+    k_pcg_spmv_tma(Geo G, PoissonGeo P, SolverState* S, const __grid_constant__ CUtensorMap mz,
+                   const __grid_constant__ CUtensorMap mpo, T* __restrict__ pnew,
+                   T* __restrict__ q, int first) {
+  using C = SpmvTma<T, TX, TY, NS>;
+  extern __shared__ unsigned char spmv_dsm[];
+  __shared__ __align__(8) uint64_t full[NS], empty[NS];
+  __shared__ T szw[kMaxKe + 1], siz[kMaxKe];
+  if (S->converged) return;
+  const int KE = G.L.ke, IE = G.L.ie, JE = G.L.je;
+  const unsigned plane = (unsigned)G.L.plane;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntx = (IE - 2 + TX - 1) / TX, nty = (JE - 2 + TY - 1) / TY, ntiles = ntx * nty;
+  const unsigned nchunk = (unsigned)((IE - 2 + 31) / 32);
+  unsigned char* ring = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(spmv_dsm) + 127) & ~uintptr_t(127));
+  auto zt = [&](int s) { return reinterpret_cast<T*>(ring + s * C::kStage); };
+  auto pt = [&](int s) { return reinterpret_cast<T*>(ring + s * C::kStage + C::kArrPitch); };
+  for (int e = tid; e <= KE; e += C::kThreads) {
+    szw[e] = (T)P.zwn[e];
+    if (e < KE) siz[e] = (T)P.izn[e];
+  }
+  if (tid == 0) {
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], C::kConsumers / 32);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  bool ok = true;
+  if (warp == C::kConsumers / 32) {
+    // ---- producer: the whole warp walks the (tile, level) steps so that it
+    // reaches the block's later barriers together; its first lane issues
+    const uint32_t bytes = (first ? 1u : 2u) * (uint32_t)C::kArrBytes;
+    if (lane == 0) {
+      tma_prefetch_desc(&mz);
+      if (!first) tma_prefetch_desc(&mpo);
+    }
+    long long g = 0;  // steps issued
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+      const int i0 = (t % ntx) * TX + 2, j0 = (t / ntx) * TY + 2;
+      for (int K = 1; K <= KE; ++K, ++g) {
+        const int s = (int)(g % NS);
+        const long long n = g / NS;
+        if (n > 0 && !__all_sync(0xffffffffu, mbar_wait(&empty[s], (unsigned)((n - 1) & 1)))) {
+          ok = false;
+          break;
+        }
+        if (lane == 0) {
+          mbar_arrive_expect_tx(&full[s], bytes);
+          tma_load_3d(zt(s), &mz, i0 - 2, j0 - 1, K - 1, &full[s]);
+          if (!first) tma_load_3d(pt(s), &mpo, i0 - 2, j0 - 1, K - 1, &full[s]);
+        }
+        __syncwarp();
+      }
+    }
+    // the block does not exit with copies in flight into its shared memory
+    for (long long h = g - NS > 0 ? g - NS : 0; h < g; ++h)
+      ok = __all_sync(0xffffffffu, mbar_wait(&full[h % NS], (unsigned)((h / NS) & 1))) && ok;
+  } else {
+    // ---- consumers
+    const int tx = tid % TX, ty = tid / TX;
+    const T beta = first ? T(0) : (T)S->beta;
+    const int me = (ty + 1) * C::HX + (tx + 2);
+    auto pv = [&](int s, int e) -> T {
+      return first ? zt(s)[e] : fma(beta, pt(s)[e], zt(s)[e]);
+    };
+    long long g = 0;  // steps consumed
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+      const int i0 = (t % ntx) * TX + 2, j0 = (t / ntx) * TY + 2;
+      const int i = i0 + tx, j = j0 + ty;
+      const bool act = i <= IE - 1 && j <= JE - 1;
+      ColC c;
+      T cw = 0, ce = 0, cn = 0, cs = 0, xyc = 0;
+      int kreg = 0;
+      if (act) {
+        c = load_col(G, P, i, j);
+        cw = c.iw ? (T)c.cw : T(0);
+        ce = c.ie ? (T)c.ce : T(0);
+        cn = c.in ? (T)c.cn : T(0);
+        cs = c.is ? (T)c.cs : T(0);
+        xyc = (T)(c.xcf + c.ycf);
+        kreg = c.kreg;
+      }
+      const unsigned own = act ? (unsigned)G.L.at(i, j, 0) : 0u;
+      double pq = 0.0;
+      ok = __all_sync(0xffffffffu, mbar_wait(&full[g % NS], (unsigned)((g / NS) & 1)));
+      T pu = T(0), p0 = ok ? pv((int)(g % NS), me) : T(0);
+      T pqt = T(0);
+      for (int K = 1; K <= KE && ok; ++K, ++g) {
+        const int s = (int)(g % NS);
+        T pd = T(0);
+        if (K < KE) {
+          const int s1 = (int)((g + 1) % NS);
+          if (!__all_sync(0xffffffffu, mbar_wait(&full[s1], (unsigned)(((g + 1) / NS) & 1)))) {
+            ok = false;
+            break;
+          }
+          pd = pv(s1, me);
+        }
+        if (act) {
+          const T pw = pv(s, me - 1), pe = pv(s, me + 1);
+          const T pn = pv(s, me - C::HX), ps = pv(s, me + C::HX);
+          T sv;
+          if (K >= 2 && K <= kreg) {
+            const T zw0 = szw[K - 1], zw1 = szw[K], hs = siz[K - 1];
+            T h = cw * pw;
+            h = fma(ce, pe, h);
+            h = fma(cn, pn, h);
+            h = fma(cs, ps, h);
+            h = fma(-xyc, p0, h);
+            sv = zw0 * (pu - p0);
+            sv = fma(zw1, pd - p0, sv);
+            sv = fma(hs, h, sv);
+          } else {
+            const Coef rw = row<true>(c, P, K, KE);
+            sv = (T)rw.dc * p0;
+            sv = fma((T)rw.u, pu, sv);
+            sv = fma((T)rw.n, pn, sv);
+            sv = fma((T)rw.w, pw, sv);
+            sv = fma((T)rw.e, pe, sv);
+            sv = fma((T)rw.s, ps, sv);
+            sv = fma((T)rw.d, pd, sv);
+          }
+          const unsigned o = own + plane * (unsigned)(K - 1);
+          pnew[o] = p0;
+          q[o] = sv;
+          pqt = fma(p0, sv, pqt);
+          if ((K & 7) == 0) {
+            pq += (double)pqt;
+            pqt = T(0);
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        pu = p0;
+        p0 = pd;
+      }
+      pq += (double)pqt;
+      // this tile's warp-row partial (a warp is 32 columns of one row)
+      warp_partial(pq, S, (unsigned)(j0 - 2 + ty), (unsigned)((i0 - 2 + tx) / 32), nchunk, lane);
+    }
+  }
+  if (!ok) atomicExch(&S->converged, 4);  // a stage wait timed out: stop the solve
+  double v = 0.0;
+  if (grid_total1(v, S)) {
+    S->pq = v;
+    S->alpha = S->rho / v;
+    if (S->converged == 0 && !(v > 0.0) && !(v < 0.0)) S->converged = 3;  // breakdown
+  }
+}
+
 // r = b - A x with the exact FP64 entries of compute_matrix, accumulated in
 // double-double (products split exactly with an FMA), then rounded once; and
 // ||r||^2, ||b||^2.  This is the outer residual of the refinement loop and
@@ -811,6 +1089,83 @@ void launch_factor(const Geo& G, const PoissonGeo& P, double* dinv64, float* din
   count_launch();
 }
 
+// ---------------------------------------------------------- tensor maps
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (the library does not link libcuda)
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+constexpr int kTmaTx = 64, kTmaTy = 8, kTmaNs = 6;      // variant 6
+constexpr int kTmaTx2 = 32, kTmaTy2 = 8, kTmaNs2 = 8;   // variant 7
+
+template <typename T, int TX, int TY, int NS>
+cudaError_t tma_optin() {
+  return cudaFuncSetAttribute(k_pcg_spmv_tma<T, TX, TY, NS>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              SpmvTma<T, TX, TY, NS>::kSmem);
+}
+
+// persistent: a grid of one block per SM (the kernels fit one block per SM),
+// otherwise a block per tile
+template <typename T, int TX, int TY, int NS>
+int tma_launch(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
+               T* pnew, T* q, int first, bool persistent, cudaStream_t st) {
+  using C = SpmvTma<T, TX, TY, NS>;
+  CUtensorMap mz, mp;
+  const int e1 = encode_field_map(&mz, z, (int)sizeof(T), G.L.P, G.L.JN, G.L.ke, C::HX, C::HY);
+  const int e2 = encode_field_map(&mp, first ? z : pold, (int)sizeof(T), G.L.P, G.L.JN, G.L.ke,
+                                  C::HX, C::HY);
+  if (e1 || e2) return e1 ? e1 : e2;
+  const int ntiles = ((G.L.ie - 2 + TX - 1) / TX) * ((G.L.je - 2 + TY - 1) / TY);
+  int nblk = ntiles;
+  if (persistent) {
+    static int nsm = 0;
+    if (!nsm) {
+      int dev = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        nsm = 148;
+    }
+    nblk = ntiles < nsm ? ntiles : nsm;
+  }
+  k_pcg_spmv_tma<T, TX, TY, NS><<<nblk, C::kThreads, C::kSmem, st>>>(G, P, S, mz, mp, pnew, q,
+                                                                      first);
+  return 0;
+}
+
+}  // namespace
+
+int encode_field_map(CUtensorMap* map, const void* base, int elem_bytes, int P, int JN, int nlev,
+                     int bx, int by) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return (int)CUDA_ERROR_NOT_FOUND;
+  const cuuint64_t dims[3] = {(cuuint64_t)P, (cuuint64_t)JN, (cuuint64_t)nlev};
+  const cuuint64_t strides[2] = {(cuuint64_t)P * elem_bytes, (cuuint64_t)P * JN * elem_bytes};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return (int)fn(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+
 namespace {
 
 // Variants of the column kernel (chosen per handle by the autotuner):
@@ -870,7 +1225,11 @@ cudaError_t pcg_prepare_device() {
   const cudaError_t e[] = {col_optin<double, 1, 4>(), col_optin<double, 2, 4>(),
                            col_optin<double, 1, 8>(), col_optin<double, 2, 8>(),
                            col_optin<float, 1, 4>(),  col_optin<float, 2, 4>(),
-                           col_optin<float, 1, 8>(),  col_optin<float, 2, 8>()};
+                           col_optin<float, 1, 8>(),  col_optin<float, 2, 8>(),
+                           tma_optin<double, kTmaTx, kTmaTy, kTmaNs>(),
+                           tma_optin<float, kTmaTx, kTmaTy, kTmaNs>(),
+                           tma_optin<double, kTmaTx2, kTmaTy2, kTmaNs2>(),
+                           tma_optin<float, kTmaTx2, kTmaTy2, kTmaNs2>()};
   for (cudaError_t x : e)
     if (x != cudaSuccess) return x;
   return cudaSuccess;
@@ -899,14 +1258,36 @@ template void launch_pcg_col<float, float>(const Geo&, const PoissonGeo&, Solver
 
 // Variants of the stencil kernel: shared-memory ring with 32 x 8 or 32 x 4
 // tiles, the barrier-free L1 form, or the warp-row form, each with 32 x 8 or
-// 32 x 4 blocks.
-int pcg_spmv_variants() { return 6; }
+// 32 x 4 blocks; and the TMA-staged form with 64 x 8 (6 stages) or 32 x 8
+// (8 stages) columns per block, a block per tile, and the 64 x 8 form with a
+// persistent grid of one block per SM.
+int pcg_spmv_variants() { return 9; }
 
+bool pcg_spmv_variant_ok(int variant) {
+  if (variant < 0 || variant >= pcg_spmv_variants()) return false;
+  return variant < 6 || encode_tiled() != nullptr;
+}
+
+// Returns cudaErrorInvalidValue (nothing launched) when a TMA variant's
+// tensor maps cannot be encoded.
 template <typename T>
-void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z, const T* pold,
-                     T* pnew, T* q, int first, int variant, cudaStream_t st) {
+cudaError_t launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T* z,
+                            const T* pold, T* pnew, T* q, int first, int variant,
+                            cudaStream_t st) {
   const int nx = G.L.ie - 2, ny = G.L.je - 2;
   switch (variant) {
+    case 6:
+      if (tma_launch<T, kTmaTx, kTmaTy, kTmaNs>(G, P, S, z, pold, pnew, q, first, false, st))
+        return cudaErrorInvalidValue;
+      break;
+    case 7:
+      if (tma_launch<T, kTmaTx2, kTmaTy2, kTmaNs2>(G, P, S, z, pold, pnew, q, first, false, st))
+        return cudaErrorInvalidValue;
+      break;
+    case 8:
+      if (tma_launch<T, kTmaTx, kTmaTy, kTmaNs>(G, P, S, z, pold, pnew, q, first, true, st))
+        return cudaErrorInvalidValue;
+      break;
     case 1:
       k_pcg_spmv<T, 4><<<grid2(nx, ny, dim3(kTx, 4)), dim3(kTx, 4), 0, st>>>(G, P, S, z, pold,
                                                                               pnew, q, first);
@@ -933,11 +1314,14 @@ void launch_pcg_spmv(const Geo& G, const PoissonGeo& P, SolverState* S, const T*
       break;
   }
   count_launch();
+  return cudaSuccess;
 }
-template void launch_pcg_spmv<double>(const Geo&, const PoissonGeo&, SolverState*, const double*,
-                                      const double*, double*, double*, int, int, cudaStream_t);
-template void launch_pcg_spmv<float>(const Geo&, const PoissonGeo&, SolverState*, const float*,
-                                     const float*, float*, float*, int, int, cudaStream_t);
+template cudaError_t launch_pcg_spmv<double>(const Geo&, const PoissonGeo&, SolverState*,
+                                             const double*, const double*, double*, double*, int,
+                                             int, cudaStream_t);
+template cudaError_t launch_pcg_spmv<float>(const Geo&, const PoissonGeo&, SolverState*,
+                                            const float*, const float*, float*, float*, int, int,
+                                            cudaStream_t);
 
 void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b,
                   const double* x, double* r, cudaStream_t st) {
