@@ -125,17 +125,22 @@ __global__ void __launch_bounds__(kHbN) k_tdiff_hbih(Geo G, TrPtrs tp, int ntr,
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kHbX * ty;
   const int i0 = blockIdx.x * kHbX + 1, j0 = blockIdx.y * kHbY + 1;
   const int K = blockIdx.z + 1;
-  const unsigned lev = (unsigned)G.L.plane * (unsigned)(K - 1);
+  // int: tile offsets west/north of the array start are negative (guard zone)
+  const int lev = G.L.plane * (K - 1);
   auto wet_at = [K](int kb) { return K <= kb ? 1.0 : 0.0; };
-  // tracer-tile entries this thread loads (element (i0-2+hx, j0-2+hy))
+  // tracer-tile entries this thread loads (element (i0-2+hx, j0-2+hy));
+  // entries outside the field's plane [0, IE] x [0, JE] are not loaded and
+  // hold 0 (no Laplacian or update that is formed reads them)
   int toff[kHbTf];
-  bool tval[kHbTf];
+  bool tval[kHbTf], tin[kHbTf];
 #pragma unroll
   for (int f = 0; f < kHbTf; ++f) {
     const int e = tid + f * kHbN;
     const int hy = e / kHbTx, hx = e - hy * kHbTx;
+    const int ii = i0 - 2 + hx, jj = j0 - 2 + hy;
     tval[f] = e < kHbT;
-    toff[f] = G.L.at2(i0 - 2 + hx, j0 - 2 + hy);
+    tin[f] = tval[f] && ii >= 0 && ii <= IE && jj >= 0 && jj <= JE;
+    toff[f] = tin[f] ? G.L.at2(ii, jj) : 0;
   }
   // Laplacian positions this thread forms: masks of the level and metrics
   struct LapPos {
@@ -190,7 +195,7 @@ __global__ void __launch_bounds__(kHbN) k_tdiff_hbih(Geo G, TrPtrs tp, int ntr,
     if (n > 0) __syncthreads();  // the previous tracer's tiles are no longer read
 #pragma unroll
     for (int f = 0; f < kHbTf; ++f)
-      if (tval[f]) ts[tid + f * kHbN] = T[toff[f] + lev];
+      if (tval[f]) ts[tid + f * kHbN] = tin[f] ? T[toff[f] + lev] : 0.0;
     __syncthreads();
 #pragma unroll
     for (int f = 0; f < kHbLf; ++f) {
@@ -520,14 +525,18 @@ __global__ void __launch_bounds__(kVhN) k_visc_hbih(Geo G, const double* __restr
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kVhX * ty;
   const int i0 = blockIdx.x * kVhX, j0 = blockIdx.y * kVhY;
   const int K = blockIdx.z + 1;
-  const unsigned lev = (unsigned)G.L.plane * (unsigned)(K - 1);
+  // int: tile offsets west/north of the array start are negative (guard zone)
+  const int lev = G.L.plane * (K - 1);
   const double mv = G.minvalue;
+  // entries outside the field's plane [0, IE] x [0, JE] are not loaded and
+  // hold 0 (no Laplacian or update that is formed reads them)
 #pragma unroll
   for (int f = 0; f < kVhTf; ++f) {
     const int e = tid + f * kVhN;
     if (e < kVhT) {
       const int hy = e / kVhTx, hx = e - hy * kVhTx;
-      ts[e] = X[G.L.at2(i0 - 2 + hx, j0 - 2 + hy) + lev];
+      const int ii = i0 - 2 + hx, jj = j0 - 2 + hy;
+      ts[e] = (ii >= 0 && ii <= IE && jj >= 0 && jj <= JE) ? X[G.L.at2(ii, jj) + lev] : 0.0;
     }
   }
   __syncthreads();
