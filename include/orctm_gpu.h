@@ -33,6 +33,8 @@
  *   orctm_troneu        SUBROUTINE TRONEU    troneu.f90:48-134
  *   orctm_ocvtro        SUBROUTINE OCVTRO    ocvtro.f90:1-62
  *   orctm_ocvtot        SUBROUTINE OCVTOT    ocvtot.f90:13-96
+ *   orctm_ocbarp        SUBROUTINE OCBARP    ocbarp.f90:1-48
+ *   orctm_ocwind        SUBROUTINE OCWIND    ocwind.f90:1-42
  *   orctm_upload / orctm_download   the module arrays of MO_COMMO1
  *                                   (mo_commo1.f90:32-146) that the path reads
  *                                   and writes, moved between host and device
@@ -303,6 +305,15 @@ int orctm_troneu(orctm_handle* h, const double* u1o, const double* v1e, const do
 /* OCVTRO (ocvtro.f90:1-62): UZO, VZE scaled by the inverse depths, the
  * barotropic velocities USO, VSE, and ZO += Z1O (device, in place). */
 int orctm_ocvtro(orctm_handle* h);
+/* OCBARP (ocbarp.f90:1-48): UZO = USO, VZE = VSE, all four times the
+ * surface masks (device, in place; USO / VSE as OCVTRO left them). */
+int orctm_ocbarp(orctm_handle* h);
+/* OCWIND (ocwind.f90:1-42): the surface stress added to UOO and VOE at level
+ * 1, in place.  Host arrays: TXO u-points (IE+1)*JE, TYE v-points IE*(JE+1),
+ * SICOMU, SICOMV, TAUWATU, TAUWATV IE*JE (as mo_commo1.f90:160-167 declares
+ * them). */
+int orctm_ocwind(orctm_handle* h, const double* txo, const double* tye, const double* sicomu,
+                 const double* sicomv, const double* tauwatu, const double* tauwatv);
 /* OCVTOT (ocvtot.f90:13-96): UKO, VKE with USO, VSE added and the time filter
  * UKO <- CONN UKO + CONO UOO, UOO <- the unfiltered value (the same for v),
  * and WO from the divergence of the filtered velocities, bottom up. */

@@ -232,6 +232,16 @@ class Oracle:
                         _p(z1o), _p(uzo), _p(vze), _p(uso), _p(vse), _p(zo))
         return uso, vse
 
+    def ocbarp(self, uso, vse, uzo, vze):
+        """In place on uso, vse, uzo, vze."""
+        lib().og_ocbarp(C.byref(self.g), _p(uso), _p(vse), _p(uzo), _p(vze))
+
+    def ocwind(self, txo, tye, sicomu, sicomv, tauwatu, tauwatv, uoo, voe):
+        """In place on uoo, voe (level 1)."""
+        arrs = [np.asfortranarray(a, dtype=np.float64)
+                for a in (txo, tye, sicomu, sicomv, tauwatu, tauwatv)]
+        lib().og_ocwind(C.byref(self.g), *[_p(a) for a in arrs], _p(uoo), _p(voe))
+
     def ocvtot(self, b, uso, vse, uoo, voe, uko, vke, wo):
         """In place on uoo, voe, uko, vke, wo."""
         lib().og_ocvtot(C.byref(self.g), C.byref(baro_struct(b)), _p(uso), _p(vse), _p(uoo),

@@ -2195,3 +2195,44 @@ void og_ocvtot(const og_grid *g, const og_baro *b, const double *uso, const doub
                  P2(g->dlxp, i, j));
     }
 }
+
+/* ocbarp.f90:10-45 */
+void og_ocbarp(const og_grid *g, double *uso, double *vse, double *uzo, double *vze) {
+  DIMS;
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i) U2(uzo, i, j) = U2(uso, i, j);
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) V2(vze, i, j) = V2(vse, i, j);
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i) {
+      U2(uso, i, j) = U2(uso, i, j) * U3(g->amsuo, i, j, 1);
+      U2(uzo, i, j) = U2(uzo, i, j) * U3(g->amsuo, i, j, 1);
+    }
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      V2(vse, i, j) = V2(vse, i, j) * V3(g->amsue, i, j, 1);
+      V2(vze, i, j) = V2(vze, i, j) * V3(g->amsue, i, j, 1);
+    }
+}
+
+/* ocwind.f90:20-38 */
+void og_ocwind(const og_grid *g, const double *txo, const double *tye, const double *sicomu,
+               const double *sicomv, const double *tauwatu, const double *tauwatv, double *uoo,
+               double *voe) {
+  DIMS;
+  const double dtdect = g->dt / K1(g->dzw, 1);
+  for (int j = 2; j <= JE1; ++j)
+    for (int i = 1; i <= IE1; ++i) {
+      const double ur = P2(sicomu, i, j);
+      U3(uoo, i, j, 1) = U3(uoo, i, j, 1) +
+                         dtdect * U3(g->amsuo, i, j, 1) *
+                             (U2(txo, i, j) * ur + (1. - ur) * U3(g->amsuo, i, j, 1) * P2(tauwatu, i, j));
+    }
+  for (int j = 1; j <= JE1; ++j)
+    for (int i = 2; i <= IE1; ++i) {
+      const double vr = P2(sicomv, i, j);
+      V3(voe, i, j, 1) = V3(voe, i, j, 1) +
+                         dtdect * V3(g->amsue, i, j, 1) *
+                             (V2(tye, i, j) * vr + (1. - vr) * V3(g->amsue, i, j, 1) * P2(tauwatv, i, j));
+    }
+}

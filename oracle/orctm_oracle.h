@@ -153,6 +153,14 @@ void og_troneu(const og_grid *g, const og_baro *b, const double *xx, const doubl
  * barotropic velocities USO, VSE, and ZO += Z1O. */
 void og_ocvtro(const og_grid *g, const og_baro *b, const double *deutio, const double *deutie,
                const double *z1o, double *uzo, double *vze, double *uso, double *vse, double *zo);
+/* OCBARP (ocbarp.f90:1-48): UZO = USO, VZE = VSE, then all four times the
+ * surface masks AMSUO(.,.,1) / AMSUE(.,.,1). */
+void og_ocbarp(const og_grid *g, double *uso, double *vse, double *uzo, double *vze);
+/* OCWIND (ocwind.f90:1-42): the surface stress on UOO(.,.,1), VOE(.,.,1).
+ * txo u-points, tye v-points; sicomu, sicomv, tauwatu, tauwatv (IE, JE). */
+void og_ocwind(const og_grid *g, const double *txo, const double *tye, const double *sicomu,
+               const double *sicomv, const double *tauwatu, const double *tauwatv, double *uoo,
+               double *voe);
 /* OCVTOT (ocvtot.f90:13-96): UKO, VKE with the barotropic part, the time
  * filter UKO <- CONN UKO + CONO UOO with UOO <- the unfiltered value, and WO
  * from the divergence, bottom up. */

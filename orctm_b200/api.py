@@ -396,6 +396,20 @@ class Instance:
     def ocvtot(self):
         _lib.check(self.lib.orctm_ocvtot(self.h), self.h)
 
+    def ocbarp(self):
+        _lib.check(self.lib.orctm_ocbarp(self.h), self.h)
+
+    def ocwind(self, txo, tye, sicomu, sicomv, tauwatu, tauwatv):
+        """OCWIND: TXO (IE+1, JE), TYE (IE, JE+1), the rest (IE, JE)."""
+        ie, je = self.ie, self.je
+        want = [(ie + 1, je), (ie, je + 1)] + [(ie, je)] * 4
+        arrs = [np.asfortranarray(a, dtype=np.float64)
+                for a in (txo, tye, sicomu, sicomv, tauwatu, tauwatv)]
+        for a, w in zip(arrs, want):
+            if a.shape != w:
+                raise ValueError(f"OCWIND forcing shape {a.shape}, expected {w}")
+        _lib.check(self.lib.orctm_ocwind(self.h, *[_p(a) for a in arrs]), self.h)
+
     def download_barotropic(self, name: str) -> np.ndarray:
         kind, which = self.BARO_FIELDS[name]
         shp = {"p": (self.ie, self.je), "u": (self.ie + 1, self.je),

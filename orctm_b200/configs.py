@@ -393,3 +393,19 @@ def make_barotropic(inst: dict, seed: int | None = None) -> dict:
                       ("v1e", (ie, je + 1), dv), ("vze", (ie, je + 1), dv)):
         out[k] = np.asfortranarray(smooth(shp, 0.1) * d)
     return out
+
+
+def make_wind(inst: dict, seed: int | None = None) -> dict:
+    """Seeded surface forcing of OCWIND: wind stress TXO (u-points, (IE+1,
+    JE)) and TYE (v-points, (IE, JE+1)) in N/m^2 / (rho) units of m^2/s^2,
+    the open-water fractions SICOMU / SICOMV in [0, 1] and the ice-ocean
+    stresses TAUWATU / TAUWATV, both (IE, JE) as the reference declares them
+    (mo_commo1.f90:160-167)."""
+    ie, je = inst["ie"], inst["je"]
+    g = rng((inst["seed"] if seed is None else seed) + 4242)
+    return {"txo": np.asfortranarray(1e-4 * g.standard_normal((ie + 1, je))),
+            "tye": np.asfortranarray(1e-4 * g.standard_normal((ie, je + 1))),
+            "sicomu": np.asfortranarray(g.uniform(0.0, 1.0, (ie, je))),
+            "sicomv": np.asfortranarray(g.uniform(0.0, 1.0, (ie, je))),
+            "tauwatu": np.asfortranarray(1e-4 * g.standard_normal((ie, je))),
+            "tauwatv": np.asfortranarray(1e-4 * g.standard_normal((ie, je)))}

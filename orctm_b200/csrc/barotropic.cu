@@ -1,5 +1,7 @@
 // Barotropic (free-surface) solve and total velocities, the part of the
-// reference step that runs just before the hot path (orctm.f90:1411-1431):
+// reference step that runs just before the hot path (orctm.f90:1342-1431):
+// OCWIND's surface stress (ocwind.f90:1-42), OCBARP's barotropic transports
+// (ocbarp.f90:1-48),
 // ITPREP's SOR coefficients (itprep.f90:15-40) with the inverse u/v depths
 // (boden.f90:264-274), TRONEU's right-hand side and red-black SOR for the
 // elevation change Z1O (troneu.f90:48-134), OCVTRO's barotropic velocities
@@ -183,9 +185,56 @@ __global__ void k_ocvtot(Geo G, BaroArgs a, const double* __restrict__ uso,
   }
 }
 
+// OCBARP (ocbarp.f90:10-45); one thread per (i, j) in [0, IE] x [0, JE]
+__global__ void k_ocbarp(Geo G, BaroFields f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  const int ij = G.L.at2(i, j);
+  if (j >= 1) {
+    const double u = f.uso[ij], a = wet(G.gu, ij, 1);
+    f.uzo[ij] = u * a;
+    f.uso[ij] = u * a;
+  }
+  if (i >= 1) {
+    const double v = f.vse[ij], a = wet(G.gv, ij, 1);
+    f.vze[ij] = v * a;
+    f.vse[ij] = v * a;
+  }
+}
+
+// OCWIND (ocwind.f90:20-38): the surface stress on level 1 of UOO and VOE
+__global__ void k_ocwind(Geo G, WindFields w, double* __restrict__ uoo, double* __restrict__ voe) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  const int ij = G.L.at2(i, j);
+  const double dtdect = G.dt / G.dzw[0];
+  if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
+    const double ur = w.sicomu[ij], a = wet(G.gu, ij, 1);
+    uoo[ij] = uoo[ij] + dtdect * a * (w.txo[ij] * ur + (1. - ur) * a * w.tauwatu[ij]);
+  }
+  if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
+    const double vr = w.sicomv[ij], a = wet(G.gv, ij, 1);
+    voe[ij] = voe[ij] + dtdect * a * (w.tye[ij] * vr + (1. - vr) * a * w.tauwatv[ij]);
+  }
+}
+
 const dim3 kB2(32, 8);
 
 }  // namespace
+
+void launch_ocbarp(const Geo& G, const BaroFields& f, cudaStream_t st) {
+  k_ocbarp<<<grid2(G.L.ie + 1, G.L.je + 1, kB2), kB2, 0, st>>>(G, f);
+  count_launch();
+}
+
+void launch_ocwind(const Geo& G, const WindFields& w, double* uoo, double* voe, cudaStream_t st) {
+  k_ocwind<<<grid2(G.L.ie + 1, G.L.je + 1, kB2), kB2, 0, st>>>(G, w, uoo, voe);
+  count_launch();
+}
 
 void launch_itprep(const Geo& G, const BaroArgs& a, const double* deuto, const double* deute,
                    const BaroFields& f, cudaStream_t st) {

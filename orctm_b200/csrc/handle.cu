@@ -193,6 +193,7 @@ struct orctm_handle {
   BaroArgs baro{};
   BaroFields bf{};
   cudaGraphExec_t sor_graph = nullptr;
+  WindFields wind{};  // OCWIND's forcing (orctm_ocwind), allocated on first use
   // replayed chunk of PCG iterations per precision and the variants it holds
   cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
   int pcg_graph_key[2][2] = {{-1, -1}, {-1, -1}};
@@ -1848,6 +1849,45 @@ int orctm_ocvtro(orctm_handle* h) {
   // ZO is updated in place: after its uploads, and after downloads queued before
   if ((st = wait_uploads(h, {ORCTM_F_ZO})) || (st = compute_after_copies(h))) return st;
   launch_ocvtro(h->G, h->baro, h->bf, h->zo, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+int orctm_ocbarp(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  if (!h->baro_ready) return h->fail(ORCTM_E_ARG, "orctm_ocbarp: orctm_set_barotropic not called");
+  launch_ocbarp(h->G, h->bf, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+int orctm_ocwind(orctm_handle* h, const double* txo, const double* tye, const double* sicomu,
+                 const double* sicomv, const double* tauwatu, const double* tauwatv) {
+  ORCTM_ENTER(h);
+  if (!txo || !tye || !sicomu || !sicomv || !tauwatu || !tauwatv)
+    return h->fail(ORCTM_E_ARG, "orctm_ocwind: missing array");
+  const int IE = h->L.ie, JE = h->L.je;
+  int st;
+  if (!h->wind.txo) {
+    double** all[] = {&h->wind.txo, &h->wind.tye, &h->wind.sicomu, &h->wind.sicomv,
+                      &h->wind.tauwatu, &h->wind.tauwatv};
+    for (double** p : all)
+      if ((st = h->dev_alloc(p, (size_t)h->L.plane))) return st;
+  }
+  // the forcing of the previous call may still be read by queued launches
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  if ((st = upload_2d(h, h->wind.txo, txo, 0, IE + 1, 1, JE)) ||
+      (st = upload_2d(h, h->wind.tye, tye, 1, IE, 0, JE + 1)) ||
+      (st = upload_2d(h, h->wind.sicomu, sicomu, 1, IE, 1, JE)) ||
+      (st = upload_2d(h, h->wind.sicomv, sicomv, 1, IE, 1, JE)) ||
+      (st = upload_2d(h, h->wind.tauwatu, tauwatu, 1, IE, 1, JE)) ||
+      (st = upload_2d(h, h->wind.tauwatv, tauwatv, 1, IE, 1, JE)))
+    return st;
+  // UOO and VOE are updated in place (level 1)
+  if ((st = wait_uploads(h, {ORCTM_F_UOO, ORCTM_F_VOE})) || (st = own_buffer(h, ORCTM_F_UOO)) ||
+      (st = own_buffer(h, ORCTM_F_VOE)))
+    return st;
+  launch_ocwind(h->G, h->wind, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE], h->stream);
   ORCTM_CUDA_OK(cudaGetLastError());
   return ORCTM_OK;
 }

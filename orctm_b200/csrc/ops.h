@@ -58,6 +58,12 @@ struct BaroFields {
   double *uf, *deutio, *u1o, *uzo, *uso;  // u-points
   double *vf, *deutie, *v1e, *vze, *vse;  // v-points
 };
+// surface forcing of OCWIND (2D, padded plane layout)
+struct WindFields {
+  double *txo, *tye, *sicomu, *sicomv, *tauwatu, *tauwatv;
+};
+void launch_ocbarp(const Geo& G, const BaroFields& f, cudaStream_t st);
+void launch_ocwind(const Geo& G, const WindFields& w, double* uoo, double* voe, cudaStream_t st);
 void launch_itprep(const Geo& G, const BaroArgs& a, const double* deuto, const double* deute,
                    const BaroFields& f, cudaStream_t st);
 void launch_troneu_rhs(const Geo& G, const BaroArgs& a, const BaroFields& f, cudaStream_t st);

@@ -144,6 +144,15 @@ module orctm_gpu_mod
        import :: c_int, c_ptr
        type(c_ptr), value :: h
      end function
+     integer(c_int) function orctm_ocbarp(h) bind(c, name="orctm_ocbarp")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocwind(h, txo, tye, sicomu, sicomv, tauwatu, tauwatv) &
+         bind(c, name="orctm_ocwind")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, txo, tye, sicomu, sicomv, tauwatu, tauwatv
+     end function
      integer(c_int) function orctm_download_barotropic(h, which, host, n) &
          bind(c, name="orctm_download_barotropic")
        import :: c_int, c_ptr, c_size_t

@@ -1094,3 +1094,27 @@ def ocvtot(g, b, uso, vse, uoo, voe, uko, vke):
     for k in range(ke - 1, -1, -1):
         wo[:, :, k] = wo[:, :, k + 1] + tx[:, :, k] + ty[:, :, k]
     return uoo_n, voe_n, uko_n, vke_n, wo
+
+
+def ocbarp(g, uso, vse):
+    """ocbarp.f90:10-45: returns (uso, vse, uzo, vze)."""
+    uzo = uso * g["amsuo"][:, :, 0]
+    vze = vse * g["amsue"][:, :, 0]
+    return uso * g["amsuo"][:, :, 0], vse * g["amsue"][:, :, 0], uzo, vze
+
+
+def ocwind(g, txo, tye, sicomu, sicomv, tauwatu, tauwatv, uoo, voe):
+    """ocwind.f90:20-38 on copies of uoo, voe.  p-shaped ice fields are
+    indexed [I-1, J-1]; u arrays [I, J-1]; v arrays [I-1, J]."""
+    ie, je = g["ie"], g["je"]
+    dtdect = g["dt"] / g["dzw"][0]
+    uoo, voe = uoo.copy(), voe.copy()
+    a = g["amsuo"][1:ie, 1:je - 1, 0]                      # I = 1..IE-1, J = 2..JE-1
+    ur = sicomu[0:ie - 1, 1:je - 1]
+    uoo[1:ie, 1:je - 1, 0] = uoo[1:ie, 1:je - 1, 0] + dtdect * a * (
+        txo[1:ie, 1:je - 1] * ur + (1. - ur) * a * tauwatu[0:ie - 1, 1:je - 1])
+    b = g["amsue"][1:ie - 1, 1:je, 0]                      # I = 2..IE-1, J = 1..JE-1
+    vr = sicomv[1:ie - 1, 0:je - 1]
+    voe[1:ie - 1, 1:je, 0] = voe[1:ie - 1, 1:je, 0] + dtdect * b * (
+        tye[1:ie - 1, 1:je] * vr + (1. - vr) * b * tauwatv[1:ie - 1, 0:je - 1])
+    return uoo, voe

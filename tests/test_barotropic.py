@@ -85,3 +85,26 @@ def test_ocvtro_and_ocvtot(case):
     orc.ocvtot(B, uso, vse, st["uoo"], st["voe"], st["uko"], st["vke"], st["wo"])
     for k, b in zip(("uoo", "voe", "uko", "vke", "wo"), ref):
         assert np.array_equal(st[k], b), k
+
+
+def test_ocbarp_and_ocwind(case):
+    inst, orc, _ = case
+    st = C.copy_state(inst)
+    g = _g(inst)
+    g["dzw"] = inst["dzw"]
+    rng = np.random.default_rng(5)
+    uso = np.asfortranarray(rng.standard_normal((inst["ie"] + 1, inst["je"])))
+    vse = np.asfortranarray(rng.standard_normal((inst["ie"], inst["je"] + 1)))
+    want = R.ocbarp(g, uso, vse)
+    uzo, vze = np.zeros_like(uso), np.zeros_like(vse)
+    u, v = uso.copy(order="F"), vse.copy(order="F")
+    orc.ocbarp(u, v, uzo, vze)
+    for a, b in zip((u, v, uzo, vze), want):
+        assert np.array_equal(a, b)
+    w = C.make_wind(inst)
+    wu, wv = R.ocwind(g, w["txo"], w["tye"], w["sicomu"], w["sicomv"], w["tauwatu"],
+                      w["tauwatv"], st["uoo"], st["voe"])
+    orc.ocwind(w["txo"], w["tye"], w["sicomu"], w["sicomv"], w["tauwatu"], w["tauwatv"],
+               st["uoo"], st["voe"])
+    assert np.array_equal(st["uoo"], wu) and np.array_equal(st["voe"], wv)
+    assert not np.array_equal(wu, C.copy_state(inst)["uoo"])

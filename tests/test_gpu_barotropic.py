@@ -1,7 +1,8 @@
 """The barotropic solve on the GPU against the oracle, bit for bit (the
 kernels evaluate the reference's expressions in IEEE binary64 without
 contraction, as the oracle does): ITPREP + TRONEU's SOR (Z1O, B1O), OCVTRO
-(USO, VSE, UZO, VZE, ZO) and OCVTOT (UOO, VOE, UKO, VKE, WO), on a c1 slice,
+(USO, VSE, UZO, VZE, ZO), OCVTOT (UOO, VOE, UKO, VKE, WO), OCBARP and OCWIND,
+on a c1 slice,
 c2 boxes (with and without OBC_ETA_FORC) and a c4 member; then c2 at its own
 size, 256x256x60, with the reference's 250 sweeps."""
 import numpy as np
@@ -48,6 +49,23 @@ def test_barotropic_solve_bit_identical(name, over, eta_forc):
     orc.ocvtot(b, uso, vse, st["uoo"], st["voe"], st["uko"], st["vke"], st["wo"])
     for k in ("uoo", "voe", "uko", "vke", "wo"):
         assert np.array_equal(gpu.download(k), st[k]), k
+    # OCBARP on the USO / VSE that OCVTRO left, then OCWIND after OCTIMF
+    # (UKO shares UOO's buffer there: the in-place update must not touch UKO)
+    gpu.ocbarp()
+    uzo2, vze2 = np.zeros_like(uso), np.zeros_like(vse)
+    orc.ocbarp(uso, vse, uzo2, vze2)
+    for k, want in (("uso", uso), ("vse", vse), ("uzo", uzo2), ("vze", vze2)):
+        assert np.array_equal(gpu.download_barotropic(k), want), k
+    gpu.octimf()
+    orc.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
+    w = C.make_wind(inst)
+    gpu.ocwind(w["txo"], w["tye"], w["sicomu"], w["sicomv"], w["tauwatu"], w["tauwatv"])
+    uko_before = st["uko"].copy()
+    orc.ocwind(w["txo"], w["tye"], w["sicomu"], w["sicomv"], w["tauwatu"], w["tauwatv"],
+               st["uoo"], st["voe"])
+    for k in ("uoo", "voe"):
+        assert np.array_equal(gpu.download(k), st[k]), k
+    assert np.array_equal(gpu.download("uko"), uko_before)
     gpu.close()
 
 
