@@ -30,6 +30,7 @@
  *                       octher.f90:114-119, mo_obcs.f90:932-1272
  *   orctm_set_barotropic  SUBROUTINE ITPREP  itprep.f90:15-40 (with BODEN's
  *                       inverse u/v depths, boden.f90:264-274)
+ *   orctm_trotest       SUBROUTINE TROTEST   trotest.f90:1-118
  *   orctm_troneu        SUBROUTINE TRONEU    troneu.f90:48-134
  *   orctm_ocvtro        SUBROUTINE OCVTRO    ocvtro.f90:1-62
  *   orctm_ocvtot        SUBROUTINE OCVTOT    ocvtot.f90:13-96
@@ -302,6 +303,13 @@ int orctm_set_barotropic(orctm_handle* h, const orctm_barotropic* b);
  * (v-points), forms B1O and runs the red-black SOR for Z1O on the device. */
 int orctm_troneu(orctm_handle* h, const double* u1o, const double* v1e, const double* uzo,
                  const double* vze);
+/* TROTEST (trotest.f90:1-118, called once at start-up, orctm.f90:873): tries
+ * SORPAR = 1.751, 1.752, ... (ntry values; 200 in the reference) for niter
+ * SOR sweeps each (200) on SQRTRND's pseudo-random right-hand side and keeps
+ * the one whose squared changes shrink most from the first sweep to the last;
+ * TRONEU uses it from then on and *sorpar receives it.  Needs
+ * orctm_set_barotropic. */
+int orctm_trotest(orctm_handle* h, int ntry, int niter, double* sorpar);
 /* OCVTRO (ocvtro.f90:1-62): UZO, VZE scaled by the inverse depths, the
  * barotropic velocities USO, VSE, and ZO += Z1O (device, in place). */
 int orctm_ocvtro(orctm_handle* h);

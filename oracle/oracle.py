@@ -219,6 +219,12 @@ class Oracle:
                         *[_p(a) for a in out])
         return tuple(out)  # xx, uf, vf, ff
 
+    def trotest(self, b, xx, uf, vf, ff, ntry=200, niter=200):
+        """TROTEST's choice of SORPAR."""
+        lib().og_trotest.restype = C.c_double
+        return lib().og_trotest(C.byref(self.g), C.byref(baro_struct(b)), _p(xx), _p(uf), _p(vf),
+                                _p(ff), int(ntry), int(niter))
+
     def troneu(self, b, xx, uf, vf, ff, u1o, v1e, uzo, vze):
         b1o, z1o = self._f2("p"), self._f2("p")
         lib().og_troneu(C.byref(self.g), C.byref(baro_struct(b)), _p(xx), _p(uf), _p(vf), _p(ff),

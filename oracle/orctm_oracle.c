@@ -2236,3 +2236,59 @@ void og_ocwind(const og_grid *g, const double *txo, const double *tye, const dou
                              (V2(tye, i, j) * vr + (1. - vr) * V3(g->amsue, i, j, 1) * P2(tauwatv, i, j));
     }
 }
+
+/* sqrtrnd.f90:1-8: C = SQRT(B*D); D = C - INT(C); the state D persists */
+static double sqrtrnd(double *d) {
+  const double b = 34251.;
+  const double c = sqrt(b * *d);
+  const int m = (int)c;
+  *d = c - m;
+  return *d;
+}
+
+/* trotest.f90:24-115 on one rank (p_ioff = p_joff = 0, IE_G = IE, JE_G = JE) */
+double og_trotest(const og_grid *g, const og_baro *b, const double *xx, const double *uf,
+                  const double *vf, const double *ff, int ntry, int niter) {
+  DIMS;
+  double *b1o = zalloc((size_t)IE * JE), *z = zalloc((size_t)IE * JE);
+  double d = 0.34679201245;  /* DATA D of SQRTRND */
+  for (int jj = 1; jj <= JE; ++jj)
+    for (int ii = 1; ii <= IE; ++ii) {
+      const double rnd = sqrtrnd(&d);
+      P2(b1o, ii, jj) = (rnd - 0.5) * P3(g->weto, ii, jj, 1) * P2(xx, ii, jj);
+    }
+  double sorpar = 1.75, convmin = 9.E99, sorpmin = sorpar;
+  for (int isor = 1; isor <= ntry; ++isor) {
+    sorpar = sorpar + 0.001;
+    memset(z, 0, sizeof(double) * (size_t)IE * JE);
+    const double sorpai = 1. - sorpar;
+    double chabas = 0.0, sumcha = 0.0;
+    for (int kiter = 1; kiter <= niter; ++kiter) {
+      sumcha = 0.;
+      for (int parity = 0; parity < 2; ++parity)
+        for (int j = 2; j <= JE1; ++j) {
+          const int is = (j + parity) % 2 + 2;
+          for (int i = is; i <= IE1; i += 2) {
+            const double zalt = P2(z, i, j);
+            P2(z, i, j) = sorpar * P2(ff, i, j) *
+                              (P2(b1o, i, j) + U2(uf, i, j) * P2(z, i + 1, j) +
+                               U2(uf, i - 1, j) * P2(z, i - 1, j) + V2(vf, i, j) * P2(z, i, j + 1) +
+                               V2(vf, i, j - 1) * P2(z, i, j - 1)) +
+                          sorpai * P2(z, i, j);
+            const double dz = zalt - P2(z, i, j);
+            sumcha = sumcha + dz * dz;
+          }
+        }
+      if (kiter == 1) chabas = sumcha;
+    }
+    const double contric = sumcha / chabas;
+    if (contric < convmin) {
+      sorpmin = sorpar;
+      convmin = contric;
+    }
+  }
+  free(b1o);
+  free(z);
+  (void)b;
+  return sorpmin;
+}

@@ -149,6 +149,13 @@ void og_itprep(const og_grid *g, const og_baro *b, const double *deuto, const do
 void og_troneu(const og_grid *g, const og_baro *b, const double *xx, const double *uf,
                const double *vf, const double *ff, const double *u1o, const double *v1e,
                const double *uzo, const double *vze, double *b1o, double *z1o);
+/* TROTEST (trotest.f90:1-118) with SQRTRND (sqrtrnd.f90:1-8): SORPAR from
+ * 1.751 to 1.950 in steps of 0.001 (accumulated), each tried for `niter`
+ * SOR sweeps from Z1O = 0 on a pseudo-random right-hand side; returns the
+ * SORPAR of the smallest ratio of the squared changes of the last sweep to
+ * those of the first.  ntry and niter are 200 in the reference. */
+double og_trotest(const og_grid *g, const og_baro *b, const double *xx, const double *uf,
+                  const double *vf, const double *ff, int ntry, int niter);
 /* OCVTRO (ocvtro.f90:1-62): UZO, VZE scaled by the inverse depths, the
  * barotropic velocities USO, VSE, and ZO += Z1O. */
 void og_ocvtro(const og_grid *g, const og_baro *b, const double *deutio, const double *deutie,

@@ -107,7 +107,7 @@ EXPORTS = (
     "orctm_set_obc", "orctm_obc_eta", "orctm_obc_uv", "orctm_write_gridinfo",
     "orctm_set_obc_ts", "orctm_obc_ts", "orctm_octdiff_noalloc",
     "orctm_set_barotropic", "orctm_troneu", "orctm_ocvtro", "orctm_ocvtot",
-    "orctm_download_barotropic", "orctm_ocbarp", "orctm_ocwind",
+    "orctm_download_barotropic", "orctm_ocbarp", "orctm_ocwind", "orctm_trotest",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -180,6 +180,7 @@ def load(build_if_missing: bool = True):
     lib.orctm_ocvtot.argtypes = [C.c_void_p]
     lib.orctm_download_barotropic.argtypes = [C.c_void_p, C.c_int, _D, C.c_size_t]
     lib.orctm_ocbarp.argtypes = [C.c_void_p]
+    lib.orctm_trotest.argtypes = [C.c_void_p, C.c_int, C.c_int, _D]
     lib.orctm_ocwind.argtypes = [C.c_void_p, _D, _D, _D, _D, _D, _D]
     _lib = lib
     return lib

@@ -381,6 +381,12 @@ class Instance:
                             int(niter), int(bool(eta_forc)))
         _lib.check(self.lib.orctm_set_barotropic(self.h, C.byref(b)), self.h)
 
+    def trotest(self, ntry: int = 200, niter: int = 200) -> float:
+        """TROTEST: chooses SORPAR (kept for TRONEU) and returns it."""
+        v = C.c_double()
+        _lib.check(self.lib.orctm_trotest(self.h, int(ntry), int(niter), C.byref(v)), self.h)
+        return v.value
+
     def troneu(self, u1o, v1e, uzo, vze):
         """TRONEU: B1O and Z1O from the transports (u: (IE+1, JE), v: (IE, JE+1))."""
         arrs = [np.asfortranarray(a, dtype=np.float64) for a in (u1o, v1e, uzo, vze)]

@@ -1,8 +1,8 @@
 // Barotropic (free-surface) solve and total velocities, the part of the
 // reference step that runs just before the hot path (orctm.f90:1342-1431):
 // OCWIND's surface stress (ocwind.f90:1-42), OCBARP's barotropic transports
-// (ocbarp.f90:1-48),
-// ITPREP's SOR coefficients (itprep.f90:15-40) with the inverse u/v depths
+// (ocbarp.f90:1-48), ITPREP's SOR coefficients (itprep.f90:15-40) and
+// TROTEST's choice of the SOR parameter (trotest.f90:1-118), with the inverse u/v depths
 // (boden.f90:264-274), TRONEU's right-hand side and red-black SOR for the
 // elevation change Z1O (troneu.f90:48-134), OCVTRO's barotropic velocities
 // and ZO update (ocvtro.f90:1-62), and OCVTOT's total velocities, time
@@ -94,6 +94,41 @@ __global__ void k_sor(Geo G, BaroArgs a, BaroFields f, int parity) {
               (f.b1o[ij] + f.uf[ij] * z[G.L.at2(i + 1, j)] + f.uf[G.L.at2(i - 1, j)] * z[G.L.at2(i - 1, j)] +
                f.vf[ij] * z[G.L.at2(i, j + 1)] + f.vf[G.L.at2(i, j - 1)] * z[G.L.at2(i, j - 1)]) +
           sorpai * z[ij];
+}
+
+// TROTEST's right-hand side B1O = (RND - 0.5) WETO(.,.,1) XX from the
+// pseudo-random values the host drew (trotest.f90:43-55), in place on b1o
+__global__ void k_trotest_rhs(Geo G, BaroFields f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (i > G.L.ie || j > G.L.je) return;
+  const int ij = G.L.at2(i, j);
+  f.b1o[ij] = (f.b1o[ij] - 0.5) * wet(G.gp, ij, 1) * f.xx[ij];
+}
+
+// one SOR colour of TROTEST (trotest.f90:62-91): SORPAR from device memory
+// (the trials replay one captured graph); the squared change of each point,
+// ZALT - Z1O, goes to d2 when d2 is not null
+__global__ void k_sor_trial(Geo G, BaroFields f, const double* __restrict__ sorpar, double* d2,
+                            int parity) {
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int IE = G.L.ie, JE = G.L.je;
+  if (j > JE - 1) return;
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + (j + parity) % 2 + 2;
+  if (i > IE - 1) return;
+  const int ij = G.L.at2(i, j);
+  const double sp = *sorpar, sorpai = 1. - sp;
+  double* z = f.z1o;
+  const double zalt = z[ij];
+  const double zn = sp * f.ff[ij] *
+                        (f.b1o[ij] + f.uf[ij] * z[G.L.at2(i + 1, j)] + f.uf[G.L.at2(i - 1, j)] * z[G.L.at2(i - 1, j)] +
+                         f.vf[ij] * z[G.L.at2(i, j + 1)] + f.vf[G.L.at2(i, j - 1)] * z[G.L.at2(i, j - 1)]) +
+                    sorpai * zalt;
+  z[ij] = zn;
+  if (d2) {
+    const double dz = zalt - zn;
+    d2[ij] = dz * dz;
+  }
 }
 
 // OCVTRO; one thread per (i, j) in [0, IE] x [0, JE]
@@ -225,6 +260,19 @@ __global__ void k_ocwind(Geo G, WindFields w, double* __restrict__ uoo, double* 
 const dim3 kB2(32, 8);
 
 }  // namespace
+
+void launch_trotest_rhs(const Geo& G, const BaroFields& f, cudaStream_t st) {
+  k_trotest_rhs<<<grid2(G.L.ie, G.L.je, kB2), kB2, 0, st>>>(G, f);
+  count_launch();
+}
+
+void launch_sor_trial(const Geo& G, const BaroFields& f, const double* sorpar, double* d2,
+                      int parity, cudaStream_t st) {
+  const int nx = (G.L.ie - 2 + 1) / 2, ny = G.L.je - 2;
+  if (nx < 1 || ny < 1) return;
+  k_sor_trial<<<grid2(nx, ny, kB2), kB2, 0, st>>>(G, f, sorpar, d2, parity);
+  count_launch();
+}
 
 void launch_ocbarp(const Geo& G, const BaroFields& f, cudaStream_t st) {
   k_ocbarp<<<grid2(G.L.ie + 1, G.L.je + 1, kB2), kB2, 0, st>>>(G, f);

@@ -194,6 +194,7 @@ struct orctm_handle {
   BaroFields bf{};
   cudaGraphExec_t sor_graph = nullptr;
   WindFields wind{};  // OCWIND's forcing (orctm_ocwind), allocated on first use
+  double* trotest_buf = nullptr;  // orctm_trotest's scratch, allocated on first use
   // replayed chunk of PCG iterations per precision and the variants it holds
   cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
   int pcg_graph_key[2][2] = {{-1, -1}, {-1, -1}};
@@ -1850,6 +1851,94 @@ int orctm_ocvtro(orctm_handle* h) {
   if ((st = wait_uploads(h, {ORCTM_F_ZO})) || (st = compute_after_copies(h))) return st;
   launch_ocvtro(h->G, h->baro, h->bf, h->zo, h->stream);
   ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+// TROTEST: the device runs the SOR trials; the host draws SQRTRND's
+// sequence and sums the squared changes of the first and the last sweep of
+// each trial in the reference's loop order, so SORPAR is the reference's
+// choice bit for bit.
+int orctm_trotest(orctm_handle* h, int ntry, int niter, double* sorpar_out) {
+  ORCTM_ENTER(h);
+  if (!h->baro_ready) return h->fail(ORCTM_E_ARG, "orctm_trotest: orctm_set_barotropic not called");
+  if (ntry < 1 || niter < 1 || !sorpar_out) return h->fail(ORCTM_E_ARG, "orctm_trotest: arguments");
+  const int IE = h->L.ie, JE = h->L.je;
+  const size_t n2 = (size_t)h->L.plane;
+  int st;
+  if ((st = compute_after_copies(h))) return st;
+  if (!h->trotest_buf && (st = h->dev_alloc(&h->trotest_buf, 4 * n2 + 1))) return st;
+  double* d2 = h->trotest_buf;  // squared changes: first sweep, last sweep (2 colours each)
+  double* sp = h->trotest_buf + 4 * n2;  // SORPAR of the trial
+  // sqrtrnd.f90:1-8 in trotest.f90:43-55's order (II fastest)
+  std::vector<double> rnd((size_t)IE * JE);
+  double d = 0.34679201245;
+  for (size_t k = 0; k < rnd.size(); ++k) {
+    const double c = std::sqrt(34251. * d);
+    d = c - (int)c;
+    rnd[k] = d;
+  }
+  if ((st = upload_2d(h, h->bf.b1o, rnd.data(), 1, IE, 1, JE))) return st;
+  launch_trotest_rhs(h->G, h->bf, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  // one trial as a graph: niter sweeps, the first and last recording their changes
+  const unsigned long long before = launch_count();
+  ORCTM_CUDA_OK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  for (int k = 1; k <= niter; ++k)
+    for (int c = 0; c < 2; ++c) {
+      double* out = k == niter ? d2 + (2 + c) * n2 : (k == 1 ? d2 + c * n2 : nullptr);
+      launch_sor_trial(h->G, h->bf, sp, out, c, h->stream);
+    }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e1 = cudaStreamEndCapture(h->stream, &g);
+  const long long per_trial = (long long)(launch_count() - before);
+  add_launches(-per_trial);
+  ORCTM_CUDA_OK(e1);
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0ULL);
+  cudaGraphDestroy(g);
+  ORCTM_CUDA_OK(e2);
+  std::vector<double> first(2 * n2), last(2 * n2);
+  auto serial = [&](const std::vector<double>& a) {  // trotest.f90:69-91 order
+    double s = 0.;
+    for (int c = 0; c < 2; ++c)
+      for (int j = 2; j <= JE - 1; ++j)
+        for (int i = (j + c) % 2 + 2; i <= IE - 1; i += 2) s = s + a[c * n2 + h->L.at2(i, j)];
+    return s;
+  };
+  double sorpar = 1.75, convmin = 9.E99, sorpmin = sorpar;
+  int rc = ORCTM_OK;
+  for (int isor = 1; isor <= ntry && rc == ORCTM_OK; ++isor) {
+    sorpar = sorpar + 0.001;
+    cudaError_t e = cudaMemcpyAsync(sp, &sorpar, sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->bf.z1o, 0, sizeof(double) * n2, h->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ex, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(first.data(), d2, sizeof(double) * 2 * n2, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(last.data(), d2 + 2 * n2, sizeof(double) * 2 * n2, cudaMemcpyDeviceToHost,
+                          h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      rc = cuda_status(e);
+      break;
+    }
+    add_launches(per_trial);
+    const double chabas = serial(first), sumcha = niter == 1 ? chabas : serial(last);
+    const double contric = sumcha / chabas;
+    if (contric < convmin) {
+      sorpmin = sorpar;
+      convmin = contric;
+    }
+  }
+  cudaGraphExecDestroy(ex);
+  if (rc != ORCTM_OK) return rc;
+  *sorpar_out = sorpmin;
+  // TRONEU uses the chosen value from now on
+  if (h->sor_graph) {
+    cudaGraphExecDestroy(h->sor_graph);
+    h->sor_graph = nullptr;
+  }
+  h->baro.sorpar = sorpmin;
   return ORCTM_OK;
 }
 

@@ -63,6 +63,9 @@ struct WindFields {
   double *txo, *tye, *sicomu, *sicomv, *tauwatu, *tauwatv;
 };
 void launch_ocbarp(const Geo& G, const BaroFields& f, cudaStream_t st);
+void launch_trotest_rhs(const Geo& G, const BaroFields& f, cudaStream_t st);
+void launch_sor_trial(const Geo& G, const BaroFields& f, const double* sorpar, double* d2,
+                      int parity, cudaStream_t st);
 void launch_ocwind(const Geo& G, const WindFields& w, double* uoo, double* voe, cudaStream_t st);
 void launch_itprep(const Geo& G, const BaroArgs& a, const double* deuto, const double* deute,
                    const BaroFields& f, cudaStream_t st);

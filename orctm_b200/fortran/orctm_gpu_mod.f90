@@ -144,6 +144,12 @@ module orctm_gpu_mod
        import :: c_int, c_ptr
        type(c_ptr), value :: h
      end function
+     integer(c_int) function orctm_trotest(h, ntry, niter, sorpar) bind(c, name="orctm_trotest")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: ntry, niter
+       real(c_double), intent(out) :: sorpar
+     end function
      integer(c_int) function orctm_ocbarp(h) bind(c, name="orctm_ocbarp")
        import :: c_int, c_ptr
        type(c_ptr), value :: h

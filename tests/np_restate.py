@@ -1118,3 +1118,51 @@ def ocwind(g, txo, tye, sicomu, sicomv, tauwatu, tauwatv, uoo, voe):
     voe[1:ie - 1, 1:je, 0] = voe[1:ie - 1, 1:je, 0] + dtdect * b * (
         tye[1:ie - 1, 1:je] * vr + (1. - vr) * b * tauwatv[1:ie - 1, 0:je - 1])
     return uoo, voe
+
+
+def trotest(g, b, xx, uf, vf, ff, ntry=200, niter=200):
+    """trotest.f90:24-115 with SQRTRND (sqrtrnd.f90:1-8), one rank.  The SOR
+    colours are vectorised (updates within a colour are independent); the sum
+    of squared changes is accumulated serially in the reference's loop order
+    (colour 1 then colour 2, J outer, I inner) with a cumulative sum."""
+    import math
+    ie, je = g["ie"], g["je"]
+    d = 0.34679201245
+    rnd = np.zeros((ie, je))
+    for jj in range(je):
+        for ii in range(ie):
+            c = math.sqrt(34251. * d)
+            d = c - int(c)
+            rnd[ii, jj] = d
+    b1o = (rnd - 0.5) * g["weto"][:, :, 0] * xx
+    I, J = np.meshgrid(np.arange(1, ie + 1), np.arange(1, je + 1), indexing="ij")
+    inner = (I >= 2) & (I <= ie - 1) & (J >= 2) & (J <= je - 1)
+    colours = [inner & ((I + J) % 2 == 0), inner & ((I + J) % 2 == 1)]
+    order = []  # (J, I)-ordered flat positions of each colour, Fortran order
+    for m in colours:
+        jj, ii = np.nonzero(m.T)
+        order.append(ii + ie * jj)
+    ufe, ufw, vfs, vfn = uf[1:, :], uf[:-1, :], vf[:, 1:], vf[:, :-1]
+    sorpar, convmin, sorpmin = 1.75, 9e99, 1.75
+    for _ in range(ntry):
+        sorpar = sorpar + 0.001
+        sorpai = 1. - sorpar
+        z = np.zeros((ie, je))
+        chabas = sumcha = 0.0
+        for kiter in range(1, niter + 1):
+            parts = []
+            for m, pos in zip(colours, order):
+                ze = np.zeros_like(z); zw = np.zeros_like(z); zs = np.zeros_like(z); zn = np.zeros_like(z)
+                ze[:-1, :] = z[1:, :]; zw[1:, :] = z[:-1, :]; zs[:, :-1] = z[:, 1:]; zn[:, 1:] = z[:, :-1]
+                new = sorpar * ff * (b1o + ufe * ze + ufw * zw + vfs * zs + vfn * zn) + sorpai * z
+                dz = (z - new).ravel(order="F")[pos]
+                parts.append(dz * dz)
+                z = np.where(m, new, z)
+            s = np.concatenate(parts)
+            sumcha = float(np.cumsum(s)[-1]) if s.size else 0.0
+            if kiter == 1:
+                chabas = sumcha
+        contric = sumcha / chabas
+        if contric < convmin:
+            sorpmin, convmin = sorpar, contric
+    return sorpmin

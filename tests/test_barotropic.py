@@ -108,3 +108,15 @@ def test_ocbarp_and_ocwind(case):
                st["uoo"], st["voe"])
     assert np.array_equal(st["uoo"], wu) and np.array_equal(st["voe"], wv)
     assert not np.array_equal(wu, C.copy_state(inst)["uoo"])
+
+
+def test_trotest(case):
+    """TROTEST's SORPAR: the oracle and the numpy restatement agree exactly
+    (fewer tries and sweeps than the reference's 200 x 200, to stay fast)."""
+    inst, orc, _ = case
+    deuto, deute, _, _ = orc.deut(inst["depto"], C.barotropic_minvalue(inst))
+    tab = orc.itprep(B, deuto, deute)
+    got = orc.trotest(B, *tab, ntry=25, niter=30)
+    want = R.trotest(_g(inst), B, *tab, ntry=25, niter=30)
+    assert got == want
+    assert 1.75 < got <= 1.775 + 1e-12

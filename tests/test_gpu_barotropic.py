@@ -86,3 +86,27 @@ def test_barotropic_requires_setup_and_checks_arguments():
     gpu.set_barotropic(d[0], d[1], 0.2)
     with pytest.raises(ValueError):
         gpu.troneu(bt["v1e"], bt["u1o"], bt["uzo"], bt["vze"])
+
+
+@pytest.mark.parametrize("name,over,ntry,niter", [("c2", dict(nx=40, ny=33, nz=8), 200, 200),
+                                                   ("c1", dict(nx=96), 60, 80),
+                                                   ("c4", dict(nx=50, ny=41, nz=9), 40, 50)])
+def test_trotest_chooses_the_oracles_sorpar(name, over, ntry, niter):
+    """TROTEST on the device (the reference's 200 x 200 on a c2 box): the same
+    SORPAR as the oracle, bit for bit, and TRONEU then uses it."""
+    inst = C.make_instance(name, builder=grid.build_grid, **over)
+    orc = O.Oracle(inst)
+    mv = C.barotropic_minvalue(inst)
+    deuto, deute, _, _ = orc.deut(inst["depto"], mv)
+    tab = orc.itprep(O.BARO_DEFAULTS, deuto, deute)
+    want = orc.trotest(O.BARO_DEFAULTS, *tab, ntry=ntry, niter=niter)
+    gpu = Instance(inst)
+    gpu.upload_state(C.copy_state(inst))
+    gpu.set_barotropic(deuto, deute, mv)
+    got = gpu.trotest(ntry, niter)
+    assert got == want, (got, want)
+    bt = C.make_barotropic(inst)
+    gpu.troneu(bt["u1o"], bt["v1e"], bt["uzo"], bt["vze"])
+    _, z1o = orc.troneu(dict(O.BARO_DEFAULTS, sorpar=want), *tab, bt["u1o"], bt["v1e"], bt["uzo"],
+                        bt["vze"])
+    assert np.array_equal(gpu.download_barotropic("z1o"), z1o)
