@@ -3,9 +3,10 @@
 // bottom drag (OCVISC, FREESLIP branch: ocvisc.f90:37-478, 615-688).
 //
 // Implicit vertical diffusion is one Thomas solve per water column, one
-// thread per column.  The horizontal biharmonic operator is one fused pass
-// per field (the first Laplacian formed per level in shared memory, never
-// stored).  Arithmetic follows the reference's operation order in IEEE binary64,
+// thread per column.  The tracers' horizontal biharmonic operator is one
+// fused pass (the first Laplacian formed per level in shared memory, never
+// stored); the momentum one is two passes (a Laplacian into a scratch field,
+// then the flux-form update).  Arithmetic follows the reference's operation order in IEEE binary64,
 // with two changes that stay within a few ulp: the stencils multiply by
 // reciprocal metrics and per-face coefficients computed once at set-up
 // instead of dividing by the metrics, and the remaining divisions (by
@@ -101,16 +102,19 @@ __global__ void __launch_bounds__(kVertBlock) k_tdiff_vert(Geo G, TrPtrs tp, int
 }
 
 // Laplacian and biharmonic update fused (octdiff_ts.f90:342-399), all
-// tracers in one launch.  A block of 32 x 8 cells of one level stages the
-// 36 x 12 tile of the vertically diffused tracer in shared memory, forms the
-// masked Laplacian T1O on the 34 x 10 positions its cells need, and applies
-// the biharmonic update, so the Laplacian never goes to HBM; the geometry a
-// thread needs is loaded once for all tracers.  The Laplacian (0 outside the
-// interior) and the biharmonic factor W / ((DDPO + ALMZER + ZZSURF ZO) DLXP
-// DLYP) DZW use 1/(DLXP DLYP), reciprocal metrics and the face terms AULX
-// DLYU / DLXU and AULY DLXV / DLYV precomputed, multiplied in the reference's
-// order.  The blocks cover i in [1, IE], j in [1, JE] (cells outside the
-// interior are copied); blockIdx.z is the level.
+// tracers in one launch.  A block of 32 x 8 cells marches down the levels;
+// per level it stages the 36 x 12 tile of the vertically diffused tracer in
+// shared memory, forms the masked Laplacian T1O on the 34 x 10 positions its
+// cells need, and applies the biharmonic update, so the Laplacian never goes
+// to HBM.  The geometry a thread needs (wet-level counts, reciprocal metrics,
+// face terms) is loaded once for all levels and tracers, and the loads of the
+// next level are issued before the current one is computed.  The Laplacian
+// (0 outside the interior) and the biharmonic factor W / ((DDPO + ALMZER +
+// ZZSURF ZO) DLXP DLYP) DZW use 1/(DLXP DLYP), reciprocal metrics and the
+// face terms AULX DLYU / DLXU and AULY DLXV / DLYV precomputed, multiplied in
+// the reference's order.  The blocks cover i in [1, IE], j in [1, JE]: cells
+// outside the interior are copied.  (Measured on c3: one launch per level,
+// reloading the geometry each time, was 2.1x slower than this form.)
 constexpr int kHbX = 32, kHbY = 8;
 constexpr int kHbTx = kHbX + 4, kHbTy = kHbY + 4;   // tracer tile
 constexpr int kHbLx = kHbX + 2, kHbLy = kHbY + 2;   // Laplacian tile
@@ -121,13 +125,10 @@ __global__ void __launch_bounds__(kHbN) k_tdiff_hbih(Geo G, TrPtrs tp, int ntr,
                                                      const double* __restrict__ zo) {
   __shared__ double ts[kHbT];
   __shared__ double ls[kHbL];
-  const int IE = G.L.ie, JE = G.L.je;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kHbX * ty;
   const int i0 = blockIdx.x * kHbX + 1, j0 = blockIdx.y * kHbY + 1;
-  const int K = blockIdx.z + 1;
-  // int: tile offsets west/north of the array start are negative (guard zone)
-  const int lev = G.L.plane * (K - 1);
-  auto wet_at = [K](int kb) { return K <= kb ? 1.0 : 0.0; };
+  const int plane = G.L.plane;
   // tracer-tile entries this thread loads (element (i0-2+hx, j0-2+hy));
   // entries outside the field's plane [0, IE] x [0, JE] are not loaded and
   // hold 0 (no Laplacian or update that is formed reads them)
@@ -142,11 +143,11 @@ __global__ void __launch_bounds__(kHbN) k_tdiff_hbih(Geo G, TrPtrs tp, int ntr,
     tin[f] = tval[f] && ii >= 0 && ii <= IE && jj >= 0 && jj <= JE;
     toff[f] = tin[f] ? G.L.at2(ii, jj) : 0;
   }
-  // Laplacian positions this thread forms: masks of the level and metrics
+  // Laplacian positions this thread forms, with their level-independent data
   struct LapPos {
-    int e, c;
+    int e, c, kb, w, ea, n, s;
     bool in;
-    double w0, ww, we, wn, ws, rxw, rxe, rxp, ryn, rys, ryp;
+    double rxw, rxe, rxp, ryn, rys, ryp;
   };
   LapPos lp[kHbLf];
 #pragma unroll
@@ -159,11 +160,11 @@ __global__ void __launch_bounds__(kHbN) k_tdiff_hbih(Geo G, TrPtrs tp, int ntr,
     L.c = (hy + 1) * kHbTx + (hx + 1);
     if (L.in) {
       const int ij = G.L.at2(i, j);
-      L.w0 = wet_at(G.gp.kb[ij]);
-      L.ww = wet_at(G.gp.kb[G.L.at2(i - 1, j)]);
-      L.we = wet_at(G.gp.kb[G.L.at2(i + 1, j)]);
-      L.wn = wet_at(G.gp.kb[G.L.at2(i, j - 1)]);
-      L.ws = wet_at(G.gp.kb[G.L.at2(i, j + 1)]);
+      L.kb = G.gp.kb[ij];
+      L.w = G.gp.kb[G.L.at2(i - 1, j)];
+      L.ea = G.gp.kb[G.L.at2(i + 1, j)];
+      L.n = G.gp.kb[G.L.at2(i, j - 1)];
+      L.s = G.gp.kb[G.L.at2(i, j + 1)];
       L.rxw = G.rdlxu[G.L.at2(i - 1, j)];
       L.rxe = G.rdlxu[ij];
       L.rxp = G.rdlxp[ij];
@@ -176,50 +177,77 @@ __global__ void __launch_bounds__(kHbN) k_tdiff_hbih(Geo G, TrPtrs tp, int ntr,
   const int i = i0 + tx, j = j0 + ty;
   const bool cell = i <= IE && j <= JE;
   const bool inner = cell && i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1;
-  double fw = 0, fe = 0, fn = 0, fs = 0, fac = 0;
+  int kbc = 0, kbw = 0, kbe = 0, kbn = 0, kbs = 0;
+  double tfw = 0, tfe = 0, tfn = 0, tfs = 0, rar = 0, bot = 0, zc = 0;
   if (inner) {
-    const int ij = G.L.at2(i, j);
-    const int kbc = G.gp.kb[ij];
-    fw = wet_at(G.gp.kb[G.L.at2(i - 1, j)]) * G.tfx[G.L.at2(i - 1, j)];
-    fe = wet_at(G.gp.kb[G.L.at2(i + 1, j)]) * G.tfx[ij];
-    fn = wet_at(G.gp.kb[G.L.at2(i, j - 1)]) * G.tfy[G.L.at2(i, j - 1)];
-    fs = wet_at(G.gp.kb[G.L.at2(i, j + 1)]) * G.tfy[ij];
-    const double zzsurf = K == 1 ? 1. : 0.;
-    const double th = K < kbc ? G.dzw[K - 1] : (K == kbc ? G.gp.bot[ij] : 0.0);
-    fac = div_nr(wet_at(kbc) * G.rareap[ij], th + G.almzer + zzsurf * (zo[ij])) * G.dzw[K - 1];
+    const int ijc = G.L.at2(i, j);
+    kbc = G.gp.kb[ijc];
+    kbw = G.gp.kb[G.L.at2(i - 1, j)];
+    kbe = G.gp.kb[G.L.at2(i + 1, j)];
+    kbn = G.gp.kb[G.L.at2(i, j - 1)];
+    kbs = G.gp.kb[G.L.at2(i, j + 1)];
+    tfw = G.tfx[G.L.at2(i - 1, j)];
+    tfe = G.tfx[ijc];
+    tfn = G.tfy[G.L.at2(i, j - 1)];
+    tfs = G.tfy[ijc];
+    rar = G.rareap[ijc];
+    bot = G.gp.bot[ijc];
+    zc = zo[ijc];
   }
   const int me_t = (ty + 2) * kHbTx + (tx + 2), me_l = (ty + 1) * kHbLx + (tx + 1);
-  const unsigned own = cell ? (unsigned)G.L.at(i, j, K - 1) : 0u;
+  const int own = cell ? G.L.at(i, j, 0) : 0;
+  auto wet_at = [](int kb, int K) { return K <= kb ? 1.0 : 0.0; };
   for (int n = 0; n < ntr; ++n) {
     const double* __restrict__ T = tp.in[n];
-    if (n > 0) __syncthreads();  // the previous tracer's tiles are no longer read
+    double* __restrict__ O = tp.out[n];
+    double nx[kHbTf];
 #pragma unroll
-    for (int f = 0; f < kHbTf; ++f)
-      if (tval[f]) ts[tid + f * kHbN] = tin[f] ? T[toff[f] + lev] : 0.0;
-    __syncthreads();
+    for (int f = 0; f < kHbTf; ++f) nx[f] = tin[f] ? T[toff[f]] : 0.0;
+    for (int K = 1; K <= KE; ++K) {
+      __syncthreads();  // the previous level's tiles are no longer read
 #pragma unroll
-    for (int f = 0; f < kHbLf; ++f) {
-      const LapPos& L = lp[f];
-      if (L.e >= kHbL) continue;
-      double r = 0.0;
-      if (L.in) {
-        const double c = ts[L.c];
-        r = L.w0 * ((L.ww * (ts[L.c - 1] - c) * L.rxw + L.we * (ts[L.c + 1] - c) * L.rxe) * L.rxp +
-                    (L.wn * (ts[L.c - kHbTx] - c) * L.ryn + L.ws * (ts[L.c + kHbTx] - c) * L.rys) *
-                        L.ryp);
+      for (int f = 0; f < kHbTf; ++f)
+        if (tval[f]) ts[tid + f * kHbN] = nx[f];
+      if (K < KE) {
+#pragma unroll
+        for (int f = 0; f < kHbTf; ++f)
+          if (tin[f]) nx[f] = T[toff[f] + plane * K];
       }
-      ls[L.e] = r;
-    }
-    __syncthreads();
-    if (cell) {
-      const double t = ts[me_t];
-      double r = t;
-      if (inner) {
-        const double c = ls[me_l];
-        r = t - fac * (fw * (ls[me_l - 1] - c) + fe * (ls[me_l + 1] - c) +
-                       fn * (ls[me_l - kHbLx] - c) + fs * (ls[me_l + kHbLx] - c));
+      __syncthreads();
+#pragma unroll
+      for (int f = 0; f < kHbLf; ++f) {
+        const LapPos& L = lp[f];
+        if (L.e >= kHbL) continue;
+        double r = 0.0;
+        if (L.in) {
+          const double c = ts[L.c];
+          r = wet_at(L.kb, K) *
+              ((wet_at(L.w, K) * (ts[L.c - 1] - c) * L.rxw +
+                wet_at(L.ea, K) * (ts[L.c + 1] - c) * L.rxe) *
+                   L.rxp +
+               (wet_at(L.n, K) * (ts[L.c - kHbTx] - c) * L.ryn +
+                wet_at(L.s, K) * (ts[L.c + kHbTx] - c) * L.rys) *
+                   L.ryp);
+        }
+        ls[L.e] = r;
       }
-      tp.out[n][own] = r;
+      __syncthreads();
+      if (cell) {
+        const double t = ts[me_t];
+        double r = t;
+        if (inner) {
+          const double zzsurf = K == 1 ? 1. : 0.;
+          const double c = ls[me_l];
+          const double th = K < kbc ? G.dzw[K - 1] : (K == kbc ? bot : 0.0);
+          const double fac = div_nr(wet_at(kbc, K) * rar, th + G.almzer + zzsurf * (zc));
+          r = t - fac * G.dzw[K - 1] *
+                      (wet_at(kbw, K) * tfw * (ls[me_l - 1] - c) +
+                       wet_at(kbe, K) * tfe * (ls[me_l + 1] - c) +
+                       wet_at(kbn, K) * tfn * (ls[me_l - kHbLx] - c) +
+                       wet_at(kbs, K) * tfs * (ls[me_l + kHbLx] - c));
+        }
+        O[own + plane * (K - 1)] = r;
+      }
     }
   }
 }
@@ -393,207 +421,195 @@ __global__ void __launch_bounds__(kVertBlock) k_visc_w(Geo G, const double* __re
 __device__ __forceinline__ double rdlypsi(const Geo& G, int i, int j) { return G.rdlypsi[G.L.at2(i, j)]; }
 __device__ __forceinline__ double rdlxpsi(const Geo& G, int i, int j) { return G.rdlxpsi[G.L.at2(i, j)]; }
 
-// ---- OCVISC horizontal part, fused -------------------------------------
-// The first Laplacians UK1O / VK1E / WN1O (ocvisc.f90:350-438, 617-669) at one
-// position, from a field accessor F(ii, jj) of the vertically diffused
-// component at level K; 0 where the reference leaves them unset.
-template <class F>
-__device__ __forceinline__ double lap_u(const Geo& G, int i, int j, int K, F UK) {
-  const int IE = G.L.ie, JE = G.L.je;
-  if (i < 0 || i > IE || j < 1 || j > JE) return 0.0;
-  auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
-  const bool jin = j >= 2 && j <= JE - 1, iin = i >= 1 && i <= IE - 1;
-  auto ypart = [&]() {
-    return (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) * rdlypsi(G, i, j - 1) -
-            AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) * rdlypsi(G, i, j)) *
-           G.rdlyu[G.L.at2(i, j)];
-  };
-  auto xpart = [&]() {
-    return (AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) * G.rdlxp[G.L.at2(i + 1, j)] -
-            AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) * G.rdlxp[G.L.at2(i, j)]) *
-           G.rdlxu[G.L.at2(i, j)];
-  };
-  if (jin && iin) return AO(i, j) * (xpart() + ypart());
-  if (jin && i == 0)
-    return AO(i, j) * ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) * G.rdlxp[G.L.at2(i + 1, j)]) *
-                           G.rdlxu[G.L.at2(i, j)] +
-                       ypart());
-  if (jin && i == IE)
-    return AO(i, j) * ((-AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) * G.rdlxp[G.L.at2(i, j)]) *
-                           G.rdlxu[G.L.at2(i, j)] +
-                       ypart());
-  if (iin && j == 1)
-    return AO(i, j) * (xpart() + (-AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) * rdlypsi(G, i, j)) *
-                                     G.rdlyu[G.L.at2(i, j)]);
-  if (iin && j == JE)
-    return AO(i, j) * (xpart() + (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) * rdlypsi(G, i, j - 1)) *
-                                     G.rdlyu[G.L.at2(i, j)]);
-  return 0.0;
-}
-
-template <class F>
-__device__ __forceinline__ double lap_v(const Geo& G, int i, int j, int K, F VK) {
-  const int IE = G.L.ie, JE = G.L.je;
-  if (i < 1 || i > IE || j < 0 || j > JE) return 0.0;
-  auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
-  const bool jin = j >= 1 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
-  auto xpart = [&]() {
-    return (AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) * rdlxpsi(G, i, j) -
-            AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) * rdlxpsi(G, i - 1, j)) *
-           G.rdlxv[G.L.at2(i, j)];
-  };
-  auto ypart = [&]() {
-    return (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) * G.rdlyp[G.L.at2(i, j)] -
-            AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) * G.rdlyp[G.L.at2(i, j + 1)]) *
-           G.rdlyv[G.L.at2(i, j)];
-  };
-  if (jin && iin) return AE(i, j) * (xpart() + ypart());
-  if (jin && i == 1)
-    return AE(i, j) * ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) * rdlxpsi(G, i, j)) *
-                           G.rdlxv[G.L.at2(i, j)] +
-                       ypart());
-  if (jin && i == IE)
-    return AE(i, j) * ((-AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) * rdlxpsi(G, i - 1, j)) *
-                           G.rdlxv[G.L.at2(i, j)] +
-                       ypart());
-  if (iin && j == 0)
-    return AE(i, j) * (xpart() + (-AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) * G.rdlyp[G.L.at2(i, j + 1)]) *
-                                     G.rdlyv[G.L.at2(i, j)]);
-  if (iin && j == JE)
-    return AE(i, j) * (xpart() + (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) * G.rdlyp[G.L.at2(i, j)]) *
-                                     G.rdlyv[G.L.at2(i, j)]);
-  return 0.0;
-}
-
-template <class F>
-__device__ __forceinline__ double lap_w(const Geo& G, int i, int j, int K, F WN) {
-  const int IE = G.L.ie, JE = G.L.je;
-  if (i < 1 || i > IE || j < 1 || j > JE) return 0.0;
-  auto WE = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
-  const bool jin = j >= 2 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
-  auto xpart = [&]() {
-    return (WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) * G.rdlxu[G.L.at2(i, j)] -
-            WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) * G.rdlxu[G.L.at2(i - 1, j)]) *
-           G.rdlxp[G.L.at2(i, j)];
-  };
-  auto ypart = [&]() {
-    return (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) * G.rdlyv[G.L.at2(i, j - 1)] -
-            WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) * G.rdlyv[G.L.at2(i, j)]) *
-           G.rdlyp[G.L.at2(i, j)];
-  };
-  if (jin && iin) return WE(i, j) * (xpart() + ypart());
-  if (jin && i == 1)
-    return WE(i, j) * ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) * G.rdlxu[G.L.at2(i, j)]) *
-                           G.rdlxp[G.L.at2(i, j)] +
-                       ypart());
-  if (jin && i == IE)
-    return WE(i, j) * ((-WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) * G.rdlxu[G.L.at2(i - 1, j)]) *
-                           G.rdlxp[G.L.at2(i, j)] +
-                       ypart());
-  if (iin && j == 1)
-    return WE(i, j) * (xpart() + (-WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) * G.rdlyv[G.L.at2(i, j)]) *
-                                     G.rdlyp[G.L.at2(i, j)]);
-  if (iin && j == JE)
-    return WE(i, j) * (xpart() + (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) * G.rdlyv[G.L.at2(i, j - 1)]) *
-                                     G.rdlyp[G.L.at2(i, j)]);
-  return 0.0;
-}
-
-// Laplacian and biharmonic update of one momentum component fused
-// (COMP 0 u, 1 v, 2 w; ocvisc.f90:346-478, 615-688).  A block of 32 x 8
-// positions of one level (blockIdx.z; origin i = j = 0, covering
-// [0, IE] x [0, JE]) stages the 36 x 12 tile of the vertically diffused
-// component (X) in shared memory, forms the first Laplacian on the 34 x 10
-// positions its cells need, and applies the flux-form update; the Laplacian
-// never goes to HBM.  Cells outside the interior keep the undiffused value
-// (KEEP: UOO, VOE; for w the vertically diffused WNO, which also carries
-// level KE+1).  The per-position arithmetic is the reference's, with the
-// face terms AUL.. * width / length and the cells' reciprocal areas formed
-// once at set-up.
-constexpr int kVhX = 32, kVhY = 8;
-constexpr int kVhTx = kVhX + 4, kVhTy = kVhY + 4, kVhLx = kVhX + 2, kVhLy = kVhY + 2;
-constexpr int kVhT = kVhTx * kVhTy, kVhL = kVhLx * kVhLy, kVhN = kVhX * kVhY;
-constexpr int kVhTf = (kVhT + kVhN - 1) / kVhN;
-
-template <int COMP>
-__global__ void __launch_bounds__(kVhN) k_visc_hbih(Geo G, const double* __restrict__ X,
-                                                    const double* __restrict__ keep,
-                                                    double* __restrict__ O) {
-  __shared__ double ts[kVhT];
-  __shared__ double ls[kVhL];
-  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kVhX * ty;
-  const int i0 = blockIdx.x * kVhX, j0 = blockIdx.y * kVhY;
+// first Laplacians UK1O (u), VK1E (v), WN1O (w), ocvisc.f90:350-438, 617-669.
+// (Fusing this pass with the next through shared-memory tiles, as the tracer
+// kernel above does, was measured on c3 and not kept: with the geometry of
+// the edge cases reloaded every level the fused form was 5% slower, and one
+// launch per level 1.7x slower, than these two level-parallel passes.)
+__global__ void k_visc_lap(Geo G, const double* __restrict__ uk, const double* __restrict__ vk,
+                           const double* __restrict__ wn, double* __restrict__ u1,
+                           double* __restrict__ v1, double* __restrict__ w1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int K = blockIdx.z + 1;
-  // int: tile offsets west/north of the array start are negative (guard zone)
-  const int lev = G.L.plane * (K - 1);
+  const int IE = G.L.ie, JE = G.L.je;
+  if (i > IE || j > JE) return;
+  // ---- u-points
+  if (j >= 1) {
+    auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
+    auto UK = [&](int ii, int jj) { return AT(uk, ii, jj, K); };
+    const bool jin = j >= 2 && j <= JE - 1, iin = i >= 1 && i <= IE - 1;
+    double r = 0.0;
+    auto ypart = [&]() {
+      return (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) * rdlypsi(G, i, j - 1) -
+              AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) * rdlypsi(G, i, j)) *
+             G.rdlyu[G.L.at2(i, j)];
+    };
+    auto xpart = [&]() {
+      return (AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) * G.rdlxp[G.L.at2(i + 1, j)] -
+              AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) * G.rdlxp[G.L.at2(i, j)]) *
+             G.rdlxu[G.L.at2(i, j)];
+    };
+    if (jin && iin) {
+      r = AO(i, j) * (xpart() + ypart());
+    } else if (jin && i == 0) {
+      r = AO(i, j) * ((AO(i + 1, j) * (UK(i + 1, j) - UK(i, j)) * G.rdlxp[G.L.at2(i + 1, j)]) *
+                          G.rdlxu[G.L.at2(i, j)] +
+                      ypart());
+    } else if (jin && i == IE) {
+      r = AO(i, j) * ((-AO(i - 1, j) * (UK(i, j) - UK(i - 1, j)) * G.rdlxp[G.L.at2(i, j)]) *
+                          G.rdlxu[G.L.at2(i, j)] +
+                      ypart());
+    } else if (iin && j == 1) {
+      r = AO(i, j) * (xpart() + (-AO(i, j + 1) * (UK(i, j) - UK(i, j + 1)) * rdlypsi(G, i, j)) *
+                                    G.rdlyu[G.L.at2(i, j)]);
+    } else if (iin && j == JE) {
+      r = AO(i, j) * (xpart() + (AO(i, j - 1) * (UK(i, j - 1) - UK(i, j)) * rdlypsi(G, i, j - 1)) *
+                                    G.rdlyu[G.L.at2(i, j)]);
+    }
+    AT(u1, i, j, K) = r;
+  }
+  // ---- v-points
+  if (i >= 1) {
+    auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
+    auto VK = [&](int ii, int jj) { return AT(vk, ii, jj, K); };
+    const bool jin = j >= 1 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
+    double r = 0.0;
+    auto xpart = [&]() {
+      return (AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) * rdlxpsi(G, i, j) -
+              AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) * rdlxpsi(G, i - 1, j)) *
+             G.rdlxv[G.L.at2(i, j)];
+    };
+    auto ypart = [&]() {
+      return (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) * G.rdlyp[G.L.at2(i, j)] -
+              AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) * G.rdlyp[G.L.at2(i, j + 1)]) *
+             G.rdlyv[G.L.at2(i, j)];
+    };
+    if (jin && iin) {
+      r = AE(i, j) * (xpart() + ypart());
+    } else if (jin && i == 1) {
+      r = AE(i, j) * ((AE(i + 1, j) * (VK(i + 1, j) - VK(i, j)) * rdlxpsi(G, i, j)) *
+                          G.rdlxv[G.L.at2(i, j)] +
+                      ypart());
+    } else if (jin && i == IE) {
+      r = AE(i, j) * ((-AE(i - 1, j) * (VK(i, j) - VK(i - 1, j)) * rdlxpsi(G, i - 1, j)) *
+                          G.rdlxv[G.L.at2(i, j)] +
+                      ypart());
+    } else if (iin && j == 0) {
+      r = AE(i, j) * (xpart() + (-AE(i, j + 1) * (VK(i, j) - VK(i, j + 1)) * G.rdlyp[G.L.at2(i, j + 1)]) *
+                                    G.rdlyv[G.L.at2(i, j)]);
+    } else if (iin && j == JE) {
+      r = AE(i, j) * (xpart() + (AE(i, j - 1) * (VK(i, j - 1) - VK(i, j)) * G.rdlyp[G.L.at2(i, j)]) *
+                                    G.rdlyv[G.L.at2(i, j)]);
+    }
+    AT(v1, i, j, K) = r;
+  }
+  // ---- w-points (levels 1..KE)
+  if (i >= 1 && j >= 1) {
+    auto WE = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
+    auto WN = [&](int ii, int jj) { return AT(wn, ii, jj, K); };
+    const bool jin = j >= 2 && j <= JE - 1, iin = i >= 2 && i <= IE - 1;
+    double r = 0.0;
+    auto xpart = [&]() {
+      return (WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) * G.rdlxu[G.L.at2(i, j)] -
+              WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) * G.rdlxu[G.L.at2(i - 1, j)]) *
+             G.rdlxp[G.L.at2(i, j)];
+    };
+    auto ypart = [&]() {
+      return (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) * G.rdlyv[G.L.at2(i, j - 1)] -
+              WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) * G.rdlyv[G.L.at2(i, j)]) *
+             G.rdlyp[G.L.at2(i, j)];
+    };
+    if (jin && iin) {
+      r = WE(i, j) * (xpart() + ypart());
+    } else if (jin && i == 1) {
+      r = WE(i, j) * ((WE(i + 1, j) * (WN(i + 1, j) - WN(i, j)) * G.rdlxu[G.L.at2(i, j)]) *
+                          G.rdlxp[G.L.at2(i, j)] +
+                      ypart());
+    } else if (jin && i == IE) {
+      r = WE(i, j) * ((-WE(i - 1, j) * (WN(i, j) - WN(i - 1, j)) * G.rdlxu[G.L.at2(i - 1, j)]) *
+                          G.rdlxp[G.L.at2(i, j)] +
+                      ypart());
+    } else if (iin && j == 1) {
+      r = WE(i, j) * (xpart() + (-WE(i, j + 1) * (WN(i, j) - WN(i, j + 1)) * G.rdlyv[G.L.at2(i, j)]) *
+                                    G.rdlyp[G.L.at2(i, j)]);
+    } else if (iin && j == JE) {
+      r = WE(i, j) * (xpart() + (WE(i, j - 1) * (WN(i, j - 1) - WN(i, j)) * G.rdlyv[G.L.at2(i, j - 1)]) *
+                                    G.rdlyp[G.L.at2(i, j)]);
+    }
+    AT(w1, i, j, K) = r;
+  }
+}
+
+// second passes, ocvisc.f90:445-477 (u, v) and 673-688 (w)
+__global__ void k_visc_bih(Geo G, const double* __restrict__ uoo, const double* __restrict__ voe,
+                           const double* __restrict__ uk, const double* __restrict__ vk,
+                           const double* __restrict__ wn, const double* __restrict__ u1,
+                           const double* __restrict__ v1, const double* __restrict__ w1,
+                           double* __restrict__ uo, double* __restrict__ vo,
+                           double* __restrict__ wo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int K = blockIdx.z + 1;  // 1..KE+1
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
   const double mv = G.minvalue;
-  // entries outside the field's plane [0, IE] x [0, JE] are not loaded and
-  // hold 0 (no Laplacian or update that is formed reads them)
-#pragma unroll
-  for (int f = 0; f < kVhTf; ++f) {
-    const int e = tid + f * kVhN;
-    if (e < kVhT) {
-      const int hy = e / kVhTx, hx = e - hy * kVhTx;
-      const int ii = i0 - 2 + hx, jj = j0 - 2 + hy;
-      ts[e] = (ii >= 0 && ii <= IE && jj >= 0 && jj <= JE) ? X[G.L.at2(ii, jj) + lev] : 0.0;
+  // The face terms AUL.. * width / length of ocvisc.f90:445-477, 673-688 are
+  // precomputed per face (G.ugx .. G.wgy) and the cell areas' reciprocals per
+  // cell, so a cell needs no division except by its thickness (w).
+  if (K <= KE) {
+    // ---- u
+    if (j >= 1) {
+      double r = AT(uoo, i, j, K);
+      if (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
+        auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
+        auto U1 = [&](int ii, int jj) { return AT(u1, ii, jj, K); };
+        const int ij = G.L.at2(i, j);
+        r = (AO(i, j) * G.rareau[ij]) *
+            (G.dlxu[ij] * G.dlyu[ij] * AT(uk, i, j, K) -
+             (G.ugx[G.L.at2(i + 1, j)] * AO(i + 1, j) * (U1(i + 1, j) - U1(i, j)) -
+              G.ugx[ij] * AO(i - 1, j) * (U1(i, j) - U1(i - 1, j)) +
+              G.ugy[G.L.at2(i, j - 1)] * AO(i, j - 1) * (U1(i, j - 1) - U1(i, j)) -
+              G.ugy[ij] * AO(i, j + 1) * (U1(i, j) - U1(i, j + 1))));
+      }
+      AT(uo, i, j, K) = r;
+    }
+    // ---- v
+    if (i >= 1) {
+      double r = AT(voe, i, j, K);
+      if (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1) {
+        auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
+        auto V1 = [&](int ii, int jj) { return AT(v1, ii, jj, K); };
+        const int ij = G.L.at2(i, j);
+        r = (AE(i, j) * G.rareav[ij]) *
+            (G.dlxv[ij] * G.dlyv[ij] * AT(vk, i, j, K) -
+             (G.vgx[ij] * AE(i + 1, j) * (V1(i + 1, j) - V1(i, j)) -
+              G.vgx[G.L.at2(i - 1, j)] * AE(i - 1, j) * (V1(i, j) - V1(i - 1, j)) +
+              G.vgy[ij] * AE(i, j - 1) * (V1(i, j - 1) - V1(i, j)) -
+              G.vgy[G.L.at2(i, j + 1)] * AE(i, j + 1) * (V1(i, j) - V1(i, j + 1))));
+      }
+      AT(vo, i, j, K) = r;
     }
   }
-  __syncthreads();
-  const bool klev = K <= KE;  // w's level KE+1 is carried unchanged
-  if (klev) {
-    for (int e = tid; e < kVhL; e += kVhN) {
-      const int hy = e / kVhLx, hx = e - hy * kVhLx;
-      const int pi = i0 - 1 + hx, pj = j0 - 1 + hy;
-      auto acc = [&](int ii, int jj) { return ts[(jj - j0 + 2) * kVhTx + (ii - i0 + 2)]; };
-      ls[e] = COMP == 0 ? lap_u(G, pi, pj, K, acc)
-              : COMP == 1 ? lap_v(G, pi, pj, K, acc)
-                          : lap_w(G, pi, pj, K, acc);
-    }
-  }
-  __syncthreads();
-  const int i = i0 + tx, j = j0 + ty;
-  const bool cell = i <= IE && j <= JE && (COMP == 0 ? j >= 1 : COMP == 1 ? i >= 1 : (i >= 1 && j >= 1));
-  if (!cell) return;
-  const bool inner = COMP == 0 ? (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1)
-                     : COMP == 1 ? (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1)
-                                 : (i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1);
-  const int me_t = (ty + 2) * kVhTx + (tx + 2), me_l = (ty + 1) * kVhLx + (tx + 1);
-  const unsigned o = (unsigned)G.L.at(i, j, K - 1);
-  double r = COMP == 2 ? ts[me_t] : keep[o];
-  if (inner && klev) {
-    const int ij = G.L.at2(i, j);
-    auto L1 = [&](int di, int dj) { return ls[me_l + di + kVhLx * dj]; };
-    if (COMP == 0) {
-      auto AO = [&](int ii, int jj) { return wet(G.gu, G.L.at2(ii, jj), K); };
-      r = (AO(i, j) * G.rareau[ij]) *
-          (G.dlxu[ij] * G.dlyu[ij] * ts[me_t] -
-           (G.ugx[G.L.at2(i + 1, j)] * AO(i + 1, j) * (L1(1, 0) - L1(0, 0)) -
-            G.ugx[ij] * AO(i - 1, j) * (L1(0, 0) - L1(-1, 0)) +
-            G.ugy[G.L.at2(i, j - 1)] * AO(i, j - 1) * (L1(0, -1) - L1(0, 0)) -
-            G.ugy[ij] * AO(i, j + 1) * (L1(0, 0) - L1(0, 1))));
-    } else if (COMP == 1) {
-      auto AE = [&](int ii, int jj) { return wet(G.gv, G.L.at2(ii, jj), K); };
-      r = (AE(i, j) * G.rareav[ij]) *
-          (G.dlxv[ij] * G.dlyv[ij] * ts[me_t] -
-           (G.vgx[ij] * AE(i + 1, j) * (L1(1, 0) - L1(0, 0)) -
-            G.vgx[G.L.at2(i - 1, j)] * AE(i - 1, j) * (L1(0, 0) - L1(-1, 0)) +
-            G.vgy[ij] * AE(i, j - 1) * (L1(0, -1) - L1(0, 0)) -
-            G.vgy[G.L.at2(i, j + 1)] * AE(i, j + 1) * (L1(0, 0) - L1(0, 1))));
-    } else {
+  // ---- w (levels 1..KE updated, KEP carried)
+  if (i >= 1 && j >= 1) {
+    double r = AT(wn, i, j, K);
+    if (K <= KE && i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1) {
       auto WE = [&](int ii, int jj) { return wet(G.gp, G.L.at2(ii, jj), K); };
+      auto W1 = [&](int ii, int jj) { return AT(w1, ii, jj, K); };
       auto dzu = [&](int ii, int jj) { return fmx(thick(G.gu, G.dzw, G.L.at2(ii, jj), K), mv); };
       auto dzv = [&](int ii, int jj) { return fmx(thick(G.gv, G.dzw, G.L.at2(ii, jj), K), mv); };
+      const int ij = G.L.at2(i, j);
       const double dzp = fmx(thick(G.gp, G.dzw, ij, K), mv);
       r = div_nr(WE(i, j) * G.rareap[ij], dzp) *
-          (G.dlxp[ij] * G.dlyp[ij] * dzp * ts[me_t] -
-           (G.wgx[ij] * dzu(i, j) * WE(i + 1, j) * (L1(1, 0) - L1(0, 0)) -
-            G.wgx[G.L.at2(i - 1, j)] * dzu(i - 1, j) * WE(i - 1, j) * (L1(0, 0) - L1(-1, 0)) +
-            G.wgy[G.L.at2(i, j - 1)] * dzv(i, j - 1) * WE(i, j - 1) * (L1(0, -1) - L1(0, 0)) -
-            G.wgy[ij] * dzv(i, j) * WE(i, j + 1) * (L1(0, 0) - L1(0, 1))));
+          (G.dlxp[ij] * G.dlyp[ij] * dzp * AT(wn, i, j, K) -
+           (G.wgx[ij] * dzu(i, j) * WE(i + 1, j) * (W1(i + 1, j) - W1(i, j)) -
+            G.wgx[G.L.at2(i - 1, j)] * dzu(i - 1, j) * WE(i - 1, j) * (W1(i, j) - W1(i - 1, j)) +
+            G.wgy[G.L.at2(i, j - 1)] * dzv(i, j - 1) * WE(i, j - 1) * (W1(i, j - 1) - W1(i, j)) -
+            G.wgy[ij] * dzv(i, j) * WE(i, j + 1) * (W1(i, j) - W1(i, j + 1))));
     }
+    AT(wo, i, j, K) = r;
   }
-  O[o] = r;
 }
 
 }  // namespace
@@ -618,18 +634,16 @@ void launch_octdiff_hbih(const Geo& G, int ntr, const double* const* in, double*
     tp.out[n] = out[n];
   }
   const dim3 b(kHbX, kHbY);
-  dim3 g = grid2(G.L.ie, G.L.je, b);
-  g.z = G.L.ke;
-  k_tdiff_hbih<<<g, b, 0, st>>>(G, tp, ntr, zo);
+  k_tdiff_hbih<<<grid2(G.L.ie, G.L.je, b), b, 0, st>>>(G, tp, ntr, zo);
   count_launch();
 }
 
 void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const double* wno,
                    const double* uko, const double* vke, const double* avo, double* spu,
-                   double* spv, double* ukv, double* vkv, double* wnv, double* uo, double* vo,
-                   double* wo, cudaStream_t st) {
-  const int IE = G.L.ie, JE = G.L.je;
-  const dim3 b2(32, 4), bc(32, kVertBlock / 32);
+                   double* spv, double* ukv, double* vkv, double* wnv, double* u1, double* v1,
+                   double* w1, double* uo, double* vo, double* wo, cudaStream_t st) {
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const dim3 b2(32, 4), bc(32, kVertBlock / 32), b3(32, 4);
   k_visc_speed<<<grid2(IE + 1, JE + 1, b2), b2, 0, st>>>(G, uoo, voe, spu, spv);
   count_launch();
   k_visc_uv<0><<<grid2(IE + 1, JE + 1, bc), bc, 0, st>>>(G, uoo, uko, avo, spu, ukv);
@@ -638,15 +652,12 @@ void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const dou
   count_launch();
   k_visc_w<<<grid2(IE, JE, bc), bc, 0, st>>>(G, wno, avo, wnv);
   count_launch();
-  const dim3 bh(kVhX, kVhY);
-  dim3 gh = grid2(IE + 1, JE + 1, bh);
-  gh.z = G.L.ke;
-  k_visc_hbih<0><<<gh, bh, 0, st>>>(G, ukv, uoo, uo);
+  dim3 gl = grid2(IE + 1, JE + 1, b3);
+  gl.z = KE;
+  k_visc_lap<<<gl, b3, 0, st>>>(G, ukv, vkv, wnv, u1, v1, w1);
   count_launch();
-  k_visc_hbih<1><<<gh, bh, 0, st>>>(G, vkv, voe, vo);
-  count_launch();
-  gh.z = G.L.ke + 1;
-  k_visc_hbih<2><<<gh, bh, 0, st>>>(G, wnv, wnv, wo);
+  gl.z = KE + 1;
+  k_visc_bih<<<gl, b3, 0, st>>>(G, uoo, voe, ukv, vkv, wnv, u1, v1, w1, uo, vo, wo);
   count_launch();
 }
 

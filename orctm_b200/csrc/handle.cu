@@ -1186,20 +1186,22 @@ int r_ocvisc(orctm_handle* h) {
     if (st0) return st0;
   }
   int st;
-  double *sp, *ukv, *vkv, *wnv, *uo, *vo, *wo;
+  double *sp, *ukv, *vkv, *wnv, *u1, *v1, *w1, *uo, *vo, *wo;
   if ((st = h->alloc(&sp)) || (st = h->alloc(&ukv)) || (st = h->alloc(&vkv)) ||
-      (st = h->alloc(&wnv)) || (st = h->alloc(&uo)) || (st = h->alloc(&vo)) || (st = h->alloc(&wo)))
+      (st = h->alloc(&wnv)) || (st = h->alloc(&u1)) || (st = h->alloc(&v1)) ||
+      (st = h->alloc(&w1)) || (st = h->alloc(&uo)) || (st = h->alloc(&vo)) || (st = h->alloc(&wo)))
     return st;
   // the two 2D speed fields live in the first two planes of one scratch buffer
   PROF(h, ORCTM_PROF_OCVISC,
        launch_ocvisc(h->G, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE], h->slot[ORCTM_F_WNO],
                      h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], h->slot[ORCTM_F_AVO], sp,
-                     sp + h->L.plane, ukv, vkv, wnv, uo, vo, wo, h->stream));
+                     sp + h->L.plane, ukv, vkv, wnv, u1, v1, w1, uo, vo, wo, h->stream));
   ORCTM_CUDA_OK(cudaGetLastError());
   h->bind(ORCTM_F_UOO, uo);
   h->bind(ORCTM_F_VOE, vo);
   h->bind(ORCTM_F_WNO, wo);
   h->unref(sp); h->unref(ukv); h->unref(vkv); h->unref(wnv);
+  h->unref(u1); h->unref(v1); h->unref(w1);
   return r_octimf(h);  // ocvisc.f90:767
 }
 

@@ -107,8 +107,8 @@ void launch_octdiff_hbih(const Geo& G, int ntr, const double* const* in, double*
                          const double* zo, cudaStream_t st);
 void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const double* wno,
                    const double* uko, const double* vke, const double* avo, double* spu,
-                   double* spv, double* ukv, double* vkv, double* wnv, double* uo, double* vo,
-                   double* wo, cudaStream_t st);
+                   double* spv, double* ukv, double* vkv, double* wnv, double* u1, double* v1,
+                   double* w1, double* uo, double* vo, double* wo, cudaStream_t st);
 
 // obc.cu: FORC_OBCS_ETA + SPONGE_OBCS_ETA on ZO, and FORC_OBCS_UV +
 // UPGRADE_OBCS_UV + SPONGE_OBCS_UV on UOO / VOE, in place
