@@ -406,7 +406,10 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
     }
   }
   double v[3] = {rz, rr, bb};
-  if (grid_sum<3>(v, S)) {
+  // warp (row, 32-column chunk) of this thread, for blocks of any width
+  const unsigned row = blockIdx.y * blockDim.y + threadIdx.y;
+  const unsigned chunk = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  if (grid_sum_rows<3>(v, S, row, chunk, (unsigned)((IE - 2 + 31) / 32), true)) {
     if (MODE == 2) {
       S->beta = v[0] / S->rho;
     } else {
@@ -1169,16 +1172,19 @@ int encode_field_map(CUtensorMap* map, const void* base, int elem_bytes, int P, 
 namespace {
 
 // Variants of the column kernel (chosen per handle by the autotuner):
-// forward values through the output vector or in shared memory, and the
-// number of levels whose loads are issued together.
+// forward values through the output vector or in shared memory, the number
+// of levels whose loads are issued together, and blocks of 32 x 4 columns or
+// of 128 consecutive columns of one row (each warp's segment then adjoins its
+// neighbours', the same DRAM pages).
 struct ColVariant {
   bool sm;
   int u;
   dim3 blk;
 };
-constexpr int kNumColVariants = 4;
+constexpr int kNumColVariants = 6;
 const ColVariant kColVariants[kNumColVariants] = {
-    {false, 4, dim3(32, 4)}, {false, 8, dim3(32, 4)}, {true, 4, dim3(32, 2)}, {true, 8, dim3(32, 2)}};
+    {false, 4, dim3(32, 4)}, {false, 8, dim3(32, 4)}, {true, 4, dim3(32, 2)}, {true, 8, dim3(32, 2)},
+    {false, 4, dim3(128, 1)}, {false, 8, dim3(128, 1)}};
 // a shared-memory variant is usable while its block's forward values fit here
 constexpr size_t kColSmemMax = 96 * 1024;
 
@@ -1242,8 +1248,8 @@ void launch_pcg_col(const Geo& G, const PoissonGeo& P, SolverState* S, int mode,
   const ColVariant& v = kColVariants[variant];
   const size_t smem = v.sm ? (size_t)v.blk.x * v.blk.y * G.L.ke * sizeof(T) : 0;
   switch (variant) {
-    case 0: col_mode<T, false, 4>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
-    case 1: col_mode<T, false, 8>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
+    case 0: case 4: col_mode<T, false, 4>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
+    case 1: case 5: col_mode<T, false, 8>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
     case 2: col_mode<T, true, 4>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
     default: col_mode<T, true, 8>(mode, v.blk, smem, G, P, S, b, x, r, p, q, z, st); break;
   }

@@ -184,7 +184,7 @@ def test_solver_variants_bit_identical(case_name, mode):
     between gives the same pressure bit for bit, with the same iteration
     count, as the autotuned solve."""
     inst = instance(case_name)
-    combos = [(-1, -1)] + [(c, 0) for c in range(4)] + [(0, s) for s in range(1, 8)]
+    combos = [(-1, -1)] + [(c, 0) for c in range(6)] + [(0, s) for s in range(1, 9)]
     ref = None
     for c, s in combos:
         gpu = Instance(inst)
