@@ -401,11 +401,10 @@ def main():
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
         if top in tj:
-            per = tj[top]["dram_bytes_per_cell"]
-            # the column kernel's traffic depends on the variant the tuner picked
-            var = str(tuning["fp64"][0]) if top == "pcg_col" else None
-            per = tj[top].get("by_variant", {}).get(var, per)
-            traffic = per * cells
+            # measured per variant: reported only for the variant the tuner picked
+            var = str(tuning["fp64"][0] if top == "pcg_col" else tuning["fp64"][1])
+            per = tj[top].get("by_variant", {}).get(var)
+            traffic = per * cells if per is not None else None
     except Exception:
         pass
     roofline = {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": hbm,
