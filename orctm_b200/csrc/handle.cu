@@ -745,8 +745,8 @@ int read_state(orctm_handle* h) {
 constexpr int kPcgChunk = 8;
 
 template <typename T, typename TX>
-int pcg_chunk_graph(orctm_handle* h, const T* b, TX* x, T* r, T* z, T* pa, T* pb, T* q,
-                    cudaGraphExec_t* out) {
+int pcg_loop_graph(orctm_handle* h, const T* b, TX* x, T* r, T* z, T* pa, T* pb, T* q,
+                   cudaGraphExec_t* out) {
   const int pr = sizeof(T) == 4;
   const int cv = h->col_var[pr], sv = h->spmv_var[pr];
   if (h->pcg_graph[pr] && h->pcg_graph_key[pr][0] == cv && h->pcg_graph_key[pr][1] == sv) {
@@ -757,8 +757,31 @@ int pcg_chunk_graph(orctm_handle* h, const T* b, TX* x, T* r, T* z, T* pa, T* pb
     cudaGraphExecDestroy(h->pcg_graph[pr]);
     h->pcg_graph[pr] = nullptr;
   }
+  // a graph holding one conditional while node; its body is a chunk of
+  // kPcgChunk iterations ended by the kernel that sets the loop condition
+  cudaGraph_t g = nullptr;
+  ORCTM_CUDA_OK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hc;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hc;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_status(e);
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
   const unsigned long long before = launch_count();
-  ORCTM_CUDA_OK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_status(e);
+  }
   cudaError_t e0 = cudaSuccess;
   T *pc = pa, *pn = pb;
   for (int k = 0; k < kPcgChunk; ++k) {
@@ -766,16 +789,14 @@ int pcg_chunk_graph(orctm_handle* h, const T* b, TX* x, T* r, T* z, T* pa, T* pb
     launch_pcg_col<T, TX>(h->G, h->P, h->S, 2, b, x, r, pn, q, z, cv, h->stream);
     std::swap(pc, pn);
   }
-  cudaGraph_t g = nullptr;
-  const cudaError_t e1 = cudaStreamEndCapture(h->stream, &g);
-  if (e0 != cudaSuccess) {
-    if (g) cudaGraphDestroy(g);
-    add_launches(-(long long)(launch_count() - before));
-    return cuda_status(e0);
-  }
-  // launches are counted when the graph runs, not when it is recorded
+  launch_pcg_continue(hc, h->S, kPcgChunk, h->stream);
+  const cudaError_t e1 = cudaStreamEndCapture(h->stream, &body);
+  // launches are counted from the iterations the solve reports, not here
   add_launches(-(long long)(launch_count() - before));
-  ORCTM_CUDA_OK(e1);
+  if (e0 != cudaSuccess || e1 != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_status(e0 != cudaSuccess ? e0 : e1);
+  }
   cudaGraphExec_t ex = nullptr;
   const cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0ULL);
   cudaGraphDestroy(g);
@@ -795,17 +816,31 @@ int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* p
   const int cv = h->col_var[pr], sv = h->spmv_var[pr];
   launch_pcg_col<T, TX>(G, h->P, h->S, init_mode, b, x, r, nullptr, nullptr, z, cv, h->stream);
   ORCTM_CUDA_OK(cudaGetLastError());
-  const int check = kPcgChunk;
   int it = 0;
   T *pc = pa, *pn = pb;
+  // the first chunk one by one (its first stencil launch forms p = z), then,
+  // unless profiling, the device-side loop: chunks of kPcgChunk iterations
+  // replayed by a conditional while node until the solve converges or another
+  // chunk would pass maxit; no host round trip in between.  The p buffers are
+  // back in their roles after every (even) chunk.
   while (it < maxit) {
     if (it > 0 && it % kPcgChunk == 0 && it + kPcgChunk <= maxit && !h->prof) {
       cudaGraphExec_t ex;
       int st;
-      if ((st = pcg_chunk_graph<T, TX>(h, b, x, r, z, pa, pb, q, &ex))) return st;
+      if ((st = pcg_loop_graph<T, TX>(h, b, x, r, z, pa, pb, q, &ex))) return st;
+      launch_set_limit(h->S, maxit, h->stream);
       ORCTM_CUDA_OK(cudaGraphLaunch(ex, h->stream));
-      add_launches(2 * kPcgChunk);
-      it += kPcgChunk;  // pc, pn end where they started
+      ORCTM_CUDA_OK(cudaGetLastError());
+      if ((st = read_state(h))) return st;
+      // every body run launches the whole chunk and the condition kernel;
+      // after convergence the chunk's remaining kernels return at once
+      const int done = h->hS->iter;
+      add_launches((long long)((done - it + kPcgChunk - 1) / kPcgChunk) * (2 * kPcgChunk + 1));
+      if (h->hS->converged) break;
+      // not converged: the loop stopped because one more chunk would pass
+      // maxit, after whole chunks, so the p buffers are in their roles
+      it = done;
+      continue;
     } else {
       PROF(h, ORCTM_PROF_PCG_SPMV,
            ORCTM_CUDA_OK(launch_pcg_spmv<T>(G, h->P, h->S, z, pc, pn, q, it == 0, sv, h->stream)));
@@ -814,7 +849,7 @@ int pcg_loop(orctm_handle* h, int init_mode, const T* b, TX* x, T* r, T* z, T* p
       std::swap(pc, pn);
       ++it;
     }
-    if (it % check == 0 || it == maxit) {
+    if (it % kPcgChunk == 0 || it == maxit) {
       int st;
       ORCTM_CUDA_OK(cudaGetLastError());
       if ((st = read_state(h))) return st;

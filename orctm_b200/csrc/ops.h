@@ -21,8 +21,9 @@ struct PoissonGeo {
 // Device-resident scalars of one Krylov solve.
 struct SolverState {
   double rho, beta, alpha, pq, rr, bb, tol, res_rr, res_bb;
-  int converged;  // 0 running, 1 converged, 2 NaN, 3 breakdown
+  int converged;  // 0 running, 1 converged, 2 NaN, 3 breakdown, 4 a stage wait timed out
   int iter;
+  int limit;      // iteration limit of the device-side loop (orctm handle's maxit)
   unsigned ticket;
   int rows;          // JE - 2: rows of unknowns, the reduction's row count
   int max_blocks;    // partial sums per quantity: 32-column chunks x rows
@@ -152,6 +153,12 @@ void launch_scale_to_f32(const Geo& G, const double* r, const SolverState* S, fl
 void launch_axpy_f32(const Geo& G, const float* d, const SolverState* S, double* x,
                      cudaStream_t st);
 void launch_solver_reset(SolverState* S, double tol, int keep_bb, cudaStream_t st);
+// device-side PCG loop: the limit of iterations, and the kernel that ends a
+// while-node body (keep looping while not converged and a further chunk of
+// `chunk` iterations stays within the limit)
+void launch_set_limit(SolverState* S, int limit, cudaStream_t st);
+void launch_pcg_continue(cudaGraphConditionalHandle hc, const SolverState* S, int chunk,
+                         cudaStream_t st);
 void launch_nh_post(const Geo& G, const double* x, const double* pold, double* pnh,
                     const double* uoo, const double* voe, double* uo, double* vo, double* wno,
                     cudaStream_t st);

@@ -1073,6 +1073,13 @@ __global__ void k_axpy_f64(Geo G, const double* __restrict__ d, double* __restri
   AT(x, i, j, K) = AT(x, i, j, K) + AT(d, i, j, K);
 }
 
+__global__ void k_set_limit(SolverState* S, int limit) { S->limit = limit; }
+
+// the last node of the device-side PCG loop's body
+__global__ void k_pcg_continue(cudaGraphConditionalHandle hc, const SolverState* S, int chunk) {
+  cudaGraphSetConditional(hc, (S->converged == 0 && S->iter + chunk <= S->limit) ? 1u : 0u);
+}
+
 __global__ void k_reset(SolverState* S, double tol, int keep_bb) {
   S->converged = 0;
   S->iter = 0;
@@ -1357,6 +1364,17 @@ void launch_axpy_f64(const Geo& G, const double* d, double* x, cudaStream_t st) 
 
 void launch_solver_reset(SolverState* S, double tol, int keep_bb, cudaStream_t st) {
   k_reset<<<1, 1, 0, st>>>(S, tol, keep_bb);
+  count_launch();
+}
+
+void launch_set_limit(SolverState* S, int limit, cudaStream_t st) {
+  k_set_limit<<<1, 1, 0, st>>>(S, limit);
+  count_launch();
+}
+
+void launch_pcg_continue(cudaGraphConditionalHandle hc, const SolverState* S, int chunk,
+                         cudaStream_t st) {
+  k_pcg_continue<<<1, 1, 0, st>>>(hc, S, chunk);
   count_launch();
 }
 
