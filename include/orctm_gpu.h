@@ -83,6 +83,8 @@ extern "C" {
 #define ORCTM_E_UNSUPPORTED (-6)   /* option outside the restated path */
 #define ORCTM_E_NODEVICE (-7)      /* no usable CUDA device */
 #define ORCTM_E_TOO_LARGE (-8)     /* size beyond orctm_octdiff_noalloc's fixed scratch */
+#define ORCTM_E_UNSTABLE (-9)      /* OCCLIT's CONTRA above 1e-3, where the reference aborts
+                                      (occlit.f90:321-326); the state is still updated */
 
 /* field ids for orctm_upload / orctm_download (MO_COMMO1 array names) */
 enum {
@@ -300,7 +302,9 @@ typedef struct orctm_barotropic {
 } orctm_barotropic;
 int orctm_set_barotropic(orctm_handle* h, const orctm_barotropic* b);
 /* TRONEU (troneu.f90:48-134): uploads U1O, UZO (u-points) and V1E, VZE
- * (v-points), forms B1O and runs the red-black SOR for Z1O on the device. */
+ * (v-points), forms B1O and runs the red-black SOR for Z1O on the device.
+ * With all four NULL it uses the device's U1O, V1E (orctm_ocmodmom) and UZO,
+ * VZE (orctm_ocbarp). */
 int orctm_troneu(orctm_handle* h, const double* u1o, const double* v1e, const double* uzo,
                  const double* vze);
 /* TROTEST (trotest.f90:1-118, called once at start-up, orctm.f90:873): tries
@@ -319,7 +323,7 @@ int orctm_ocbarp(orctm_handle* h);
 /* OCWIND (ocwind.f90:1-42): the surface stress added to UOO and VOE at level
  * 1, in place.  Host arrays: TXO u-points (IE+1)*JE, TYE v-points IE*(JE+1),
  * SICOMU, SICOMV, TAUWATU, TAUWATV IE*JE (as mo_commo1.f90:160-167 declares
- * them). */
+ * them); all six NULL reuses the forcing of the previous call. */
 int orctm_ocwind(orctm_handle* h, const double* txo, const double* tye, const double* sicomu,
                  const double* sicomv, const double* tauwatu, const double* tauwatv);
 /* OCVTOT (ocvtot.f90:13-96): UKO, VKE with USO, VSE added and the time filter
@@ -333,9 +337,79 @@ enum {
   ORCTM_B_USO = 2,  /* u-points */
   ORCTM_B_VSE = 3,  /* v-points */
   ORCTM_B_UZO = 4,  /* u-points */
-  ORCTM_B_VZE = 5   /* v-points */
+  ORCTM_B_VZE = 5,  /* v-points */
+  ORCTM_B_U1O = 6,  /* u-points: OCMODMOM's sum of DDUO UOO, TRONEU's input */
+  ORCTM_B_V1E = 7   /* v-points */
 };
 int orctm_download_barotropic(orctm_handle* h, int which, double* host, size_t n);
+
+/* ---- OCTHER, OCMODMOM, OCCLIT and the whole step -------------------------
+ * The rest of the reference step before the hot path, on the device, as the
+ * reference is built (Makefile:42-51: EISREST, REDWMICE, NURDIF,
+ * NON_HYDROSTATIC; no PLUME, UMKLAP).  Host 2D arrays are (IE, JE)
+ * p-points; NULL reads as zero. */
+#define ORCTM_EOS_UNESCO 0 /* ADISITJ + RHO1J (adisitj.f90, rho1j.f90) */
+#define ORCTM_EOS_LINEAR 1 /* RHO = rho0 + drdt (T - t0) + drds (S - s0); not in the reference */
+typedef struct orctm_thermo {
+  int eos;                      /* ORCTM_EOS_* */
+  double rho0, drdt, drds, t0, s0; /* linear EOS */
+  double grav;                  /* G (9.806) */
+  double relsal, reltem;        /* RELSAL = CRELSAL 20/DZW(1), RELTEM (orctm.f90:561, 569), 1/s */
+  double rhoicwa, rhosnwa;      /* RHOICE/RHOWAT, RHOSNO/RHOWAT (orctm.f90:739-743) */
+  double wt;                    /* WT = CWT / 6**3 (orctm.f90:503) */
+  double cstabeps, dv0, av0, cavocon, cdvocon; /* orctm.f90:311-318 */
+  const double* preff;          /* KE reference pressures; NULL = 0.1026 TIESTU (beleg.f90:127) */
+  const double* dbackv;         /* KE+1 background diffusivity DBACKV */
+  const double* abackv;         /* KE+1 background viscosity ABACKV */
+  const double *sicomo, *sictho, *sicsno; /* sea-ice fraction, thickness, snow */
+  const double *relsao, *reltho;          /* surface restoring targets */
+  const double *giriv;                    /* river inflow (m/s) */
+  const double *fu10;                     /* 10 m wind speed */
+} orctm_thermo;
+/* Sets OCTHER's constants and forcing; may be called again (daily forcing).
+ * The first call sets KCONDEP as BODEN does (boden.f90:261). */
+int orctm_set_thermo(orctm_handle* h, const orctm_thermo* t);
+/* OCMODMOM's Coriolis inputs: FTWOU (IE+1)*JE, FTWOV IE*(JE+1) (the grid
+ * file's, orctm.f90:811), GILA / GIPH (2 IE)*(2 JE) (coriol.f90:46-47),
+ * OMEGA (7.292e-5, orctm.f90:678).  The grid-angle factors are formed here
+ * on the host. */
+typedef struct orctm_coriolis {
+  const double *ftwou, *ftwov, *gila, *giph;
+  double omega;
+} orctm_coriolis;
+int orctm_set_coriolis(orctm_handle* h, const orctm_coriolis* c);
+/* OCTHER (octher.f90:1-455): restoring, fresh water and rivers into THO,
+ * SAO, ZO; the T/S boundary forcing when orctm_set_obc_ts was called; PO,
+ * STABIO, KCONDEP, AVO, DVO, RHOO; tracers copied down into land. */
+int orctm_octher(orctm_handle* h);
+/* OCMODMOM (ocmodmom.f90:1-243): 12 Coriolis iterations on UK1O, VK1E,
+ * WNO; U1O, USO, V1E, VSE; baroclinic UKO, VKE, UK1O, VK1E.  Needs
+ * orctm_set_thermo, orctm_set_coriolis and orctm_set_barotropic. */
+int orctm_ocmodmom(orctm_handle* h);
+/* OCCLIT (occlit.f90:1-332): the baroclinic iteration with WO; *contra
+ * (may be NULL) receives CONTRA, summed in a fixed order of its own;
+ * ORCTM_E_UNSTABLE above 1e-3. */
+int orctm_occlit(orctm_handle* h, double* contra);
+/* Baroclinic arrays to and from the host: which = ORCTM_C_* below. */
+enum {
+  ORCTM_C_PO = 0,      /* p-points (IE, JE, KE) */
+  ORCTM_C_STABIO = 1,  /* p-points */
+  ORCTM_C_RHOO = 2,    /* p-points */
+  ORCTM_C_UK1O = 3,    /* u-points (IE+1, JE, KE) */
+  ORCTM_C_VK1E = 4,    /* v-points (IE, JE+1, KE) */
+  ORCTM_C_EMINPO = 5,  /* 2D p-points */
+  ORCTM_C_RIVRUN = 6,  /* 2D p-points */
+  ORCTM_C_KCONDEP = 7  /* 2D p-points, integral values */
+};
+int orctm_upload_baroclinic(orctm_handle* h, int which, const double* host, size_t n);
+int orctm_download_baroclinic(orctm_handle* h, int which, double* host, size_t n);
+/* One whole time step in the driver's order (orctm.f90:1327-1562): OCTHER,
+ * OCWIND (with the forcing of the last orctm_ocwind call, if any), the open-
+ * boundary forcing (when orctm_set_obc was called; the elevation only with
+ * eta_forc), OCTIMF, OCMODMOM, OCBARP, OCCLIT, TRONEU, OCVTRO, OCVTOT, STABIO
+ * times 1000/DZ, and orctm_step_hotpath.  ldtrun is the step number the
+ * tides are evaluated at.  Returns the hot path's status, else OCCLIT's. */
+int orctm_step_full(orctm_handle* h, int ldtrun, orctm_solve_stats* s, double* contra);
 
 /* solver mode and relative-residual target (default FP64, 1e-10, 5000) */
 int orctm_set_solver(orctm_handle* h, int mode, double rtol, int maxit);

@@ -137,6 +137,73 @@ def baro_struct(b: dict):
                  int(v["eta_forc"]))
 
 
+class _Thermo(C.Structure):
+    _fields_ = [("eos", C.c_int), ("rho0", C.c_double), ("drdt", C.c_double),
+                ("drds", C.c_double), ("t0", C.c_double), ("s0", C.c_double),
+                ("grav", C.c_double), ("relsal", C.c_double), ("reltem", C.c_double),
+                ("rhoicwa", C.c_double), ("rhosnwa", C.c_double), ("wt", C.c_double),
+                ("cstabeps", C.c_double), ("dv0", C.c_double), ("av0", C.c_double),
+                ("cavocon", C.c_double), ("cdvocon", C.c_double),
+                ("preff", _D), ("dbackv", _D), ("abackv", _D),
+                ("sicomo", _D), ("sictho", _D), ("sicsno", _D), ("relsao", _D), ("reltho", _D),
+                ("giriv", _D), ("fu10", _D)]
+
+
+# the reference driver's OCTHER constants (orctm.f90:311-330, 503, 561-569,
+# 739-743); eos 0 = ADISITJ + RHO1J, 1 = linear (rho0 + drdt (T - t0) + drds (S - s0))
+THERMO_DEFAULTS = {"eos": 0, "rho0": 1025.0, "drdt": -0.2, "drds": 0.78, "t0": 10.0, "s0": 35.0,
+                   "grav": 9.806, "crelsal": 3.E-7, "creltem": 0.0,
+                   "rhoicwa": 0.91E+03 / 1.025E+03, "rhosnwa": 0.33E+03 / 1.025E+03,
+                   "wt": 0.5E-3 / (6.0 ** 3), "cstabeps": 0.05, "dv0": 0.5E-2, "av0": 0.5E-2,
+                   "cavocon": 0.0, "cdvocon": 20.0, "aback": 5.E-5, "dback": 5.E-5}
+THERMO_2D = ("sicomo", "sictho", "sicsno", "relsao", "reltho", "giriv", "fu10")
+
+
+def thermo_values(inst: dict, t: dict) -> dict:
+    """The full OCTHER parameter set of an instance: THERMO_DEFAULTS updated by
+    ``t``; RELSAL / RELTEM from CRELSAL / CRELTEM (orctm.f90:561, 569), PREFF
+    = 0.1026 TIESTU (beleg.f90:127), DBACKV / ABACKV constant (orctm.f90:515-519)."""
+    v = dict(THERMO_DEFAULTS, **t)
+    ke = inst["ke"]
+    dzw1 = float(np.asarray(inst["dzw"])[0])
+    v.setdefault("relsal", v["crelsal"] * 20. / dzw1)
+    v.setdefault("reltem", v["creltem"] * 20. / dzw1)
+    if "preff" not in v:
+        v["preff"] = 0.1026 * np.asarray(inst["tiestu"], dtype=np.float64)[:ke]
+    if "dbackv" not in v:
+        v["dbackv"] = np.full(ke + 1, v["dback"])
+    if "abackv" not in v:
+        v["abackv"] = np.full(ke + 1, v["aback"])
+    return v
+
+
+def thermo_struct(inst: dict, t: dict):
+    v = thermo_values(inst, t)
+    keep = []
+
+    def arr(a):
+        if a is None:
+            return _D()
+        a = np.asfortranarray(a, dtype=np.float64)
+        keep.append(a)
+        return _p(a)
+
+    s = _Thermo(int(v["eos"]), v["rho0"], v["drdt"], v["drds"], v["t0"], v["s0"], v["grav"],
+                v["relsal"], v["reltem"], v["rhoicwa"], v["rhosnwa"], v["wt"], v["cstabeps"],
+                v["dv0"], v["av0"], v["cavocon"], v["cdvocon"], arr(v["preff"]), arr(v["dbackv"]),
+                arr(v["abackv"]), *[arr(v.get(k)) for k in THERMO_2D])
+    return s, keep
+
+
+class _Coriolis(C.Structure):
+    _fields_ = [("ftwou", _D), ("ftwov", _D), ("gila", _D), ("giph", _D), ("omega", C.c_double)]
+
+
+def coriolis_struct(c: dict):
+    keep = [np.asfortranarray(c[k], dtype=np.float64) for k in ("ftwou", "ftwov", "gila", "giph")]
+    return _Coriolis(*[_p(a) for a in keep], float(c.get("omega", 7.292E-5))), keep
+
+
 class Oracle:
     """Holds one instance's geometry and exposes the restated routines."""
 
@@ -252,6 +319,98 @@ class Oracle:
         """In place on uoo, voe, uko, vke, wo."""
         lib().og_ocvtot(C.byref(self.g), C.byref(baro_struct(b)), _p(uso), _p(vse), _p(uoo),
                         _p(voe), _p(uko), _p(vke), _p(wo))
+
+    # -- OCTHER, OCMODMOM, OCCLIT --------------------------------------------
+    def octher_surface(self, t, tho, sao, zo):
+        """OCTHER part A in place on tho, sao, zo; returns (eminpo, rivrun)."""
+        ts, keep = thermo_struct(self.inst, t)
+        eminpo, rivrun = self._f2("p"), self._f2("p")
+        lib().og_octher_surface(C.byref(self.g), C.byref(ts), _p(tho), _p(sao), _p(zo),
+                                _p(eminpo), _p(rivrun))
+        return eminpo, rivrun
+
+    def octher_column(self, t, tho, sao, zo, uko, vke, avo, dvo, kcondep):
+        """OCTHER parts C, D in place on tho, sao, avo, dvo, kcondep (int32,
+        (IE, JE)); returns (po, stabio, rhoo)."""
+        ts, keep = thermo_struct(self.inst, t)
+        shp = (self.ie, self.je, self.ke)
+        po, stabio, rhoo = (np.zeros(shp, order="F") for _ in range(3))
+        assert kcondep.dtype == np.int32 and kcondep.flags.f_contiguous
+        lib().og_octher_column(C.byref(self.g), C.byref(ts), _p(tho), _p(sao), _p(zo), _p(uko),
+                               _p(vke), _p(po), _p(stabio), _p(rhoo), _p(avo), _p(dvo),
+                               kcondep.ctypes.data_as(_I))
+        return po, stabio, rhoo
+
+    def octher(self, t, st, obc=None, cli=None):
+        """Whole OCTHER (octher.f90:1-455) on a state dict: part A, the T/S
+        boundary forcing of tracers 0 and 1 when ``obc`` and ``cli`` (cli[n]
+        the four side records of tracer n) are given, parts C and D.  Sets
+        st's eminpo, rivrun, po, stabio, rhoo."""
+        tho, sao = st["tracers"][0], st["tracers"][1]
+        st["eminpo"], st["rivrun"] = self.octher_surface(t, tho, sao, st["zo"])
+        if obc is not None and cli is not None:
+            for n in (0, 1):
+                if cli[n] is not None:
+                    self.obc_ts(obc, cli[n], st["tracers"][n])
+        st["po"], st["stabio"], st["rhoo"] = self.octher_column(
+            t, tho, sao, st["zo"], st["uko"], st["vke"], st["avo"], st["dvo"], st["kcondep"])
+
+    def ocmodmom(self, b, c, deutio, deutie, st):
+        """OCMODMOM on a state dict (in place on uko, vke, wno, po, stabio; sets
+        uk1o, vk1e, wn1o, u1o, uso, v1e, vse)."""
+        cs, keep = coriolis_struct(c)
+        ie, je, ke = self.ie, self.je, self.ke
+        st["uk1o"] = np.zeros((ie + 1, je, ke), order="F")
+        st["vk1e"] = np.zeros((ie, je + 1, ke), order="F")
+        st["wn1o"] = np.zeros((ie, je, ke + 1), order="F")
+        for k in ("u1o", "uso"):
+            st[k] = self._f2("u")
+        for k in ("v1e", "vse"):
+            st[k] = self._f2("v")
+        lib().og_ocmodmom(C.byref(self.g), C.byref(baro_struct(b)), C.byref(cs), _p(deutio),
+                          _p(deutie), _p(st["zo"]), _p(st["uoo"]), _p(st["voe"]), _p(st["uko"]),
+                          _p(st["vke"]), _p(st["uk1o"]), _p(st["vk1e"]), _p(st["wno"]),
+                          _p(st["wn1o"]), _p(st["po"]), _p(st["stabio"]), _p(st["u1o"]),
+                          _p(st["uso"]), _p(st["v1e"]), _p(st["vse"]))
+
+    def occlit(self, b, deutio, deutie, st):
+        """OCCLIT on a state dict (in place on uko, vke, uk1o, vk1e, wo,
+        stabio); returns CONTRA."""
+        lib().og_occlit.restype = C.c_double
+        return lib().og_occlit(C.byref(self.g), C.byref(baro_struct(b)), _p(deutio), _p(deutie),
+                               _p(st["uko"]), _p(st["vke"]), _p(st["uk1o"]), _p(st["vk1e"]),
+                               _p(st["wo"]), _p(st["stabio"]))
+
+    def step_full(self, st, t, b, c, deut, tables, ldtrun, wind=None, obc=None, cli=None,
+                  solver="direct", rtol=1e-13, pnh=None):
+        """One whole step in the driver's order (orctm.f90:1327-1562) on a state
+        dict: OCTHER, OCWIND, the open-boundary forcing, OCTIMF, OCMODMOM,
+        OCBARP, OCCLIT, TRONEU, OCVTRO, OCVTOT, STABIO times 1000/DZ, the hot
+        path.  deut = (DEUTIO, DEUTIE), tables = ITPREP's (XX, UF, VF, FF).
+        Returns the hot path's solve info with "contra"."""
+        deutio, deutie = deut
+        self.octher(t, st, obc=obc, cli=cli)
+        if wind is not None:
+            self.ocwind(wind["txo"], wind["tye"], wind["sicomu"], wind["sicomv"],
+                        wind["tauwatu"], wind["tauwatv"], st["uoo"], st["voe"])
+        if obc is not None:
+            if dict(BARO_DEFAULTS, **b)["eta_forc"]:
+                self.obc_eta(obc, ldtrun, st["zo"])
+            self.obc_uv(obc, ldtrun, st["uoo"], st["voe"])
+        self.octimf(st["uoo"], st["voe"], st["uko"], st["vke"])
+        self.ocmodmom(b, c, deutio, deutie, st)
+        st["uzo"], st["vze"] = self._f2("u"), self._f2("v")
+        self.ocbarp(st["uso"], st["vse"], st["uzo"], st["vze"])
+        contra = self.occlit(b, deutio, deutie, st)
+        st["b1o"], st["z1o"] = self.troneu(b, *tables, st["u1o"], st["v1e"], st["uzo"], st["vze"])
+        st["uso"], st["vse"] = self.ocvtro(b, deutio, deutie, st["z1o"], st["uzo"], st["vze"], st["zo"])
+        self.ocvtot(b, st["uso"], st["vse"], st["uoo"], st["voe"], st["uko"], st["vke"], st["wo"])
+        dz = np.asarray(self.inst["dz"], dtype=np.float64)
+        for k in range(self.ke):
+            st["stabio"][:, :, k] = (1000. / dz[k]) * st["stabio"][:, :, k]
+        info = self.step_hotpath(st, solver=solver, rtol=rtol, pnh=pnh)
+        info["contra"] = contra
+        return info
 
     # -- OCVTOT_NH ----------------------------------------------------------
     @property

@@ -2292,3 +2292,534 @@ double og_trotest(const og_grid *g, const og_baro *b, const double *xx, const do
   (void)b;
   return sorpmin;
 }
+
+/* ------------------------------------------------------------------------ */
+/* OCTHER (octher.f90) with ADISITJ / RHO1J                                  */
+/* ------------------------------------------------------------------------ */
+
+/* adisitj.f90:46-69 with MO_PARAM3's coefficients (mo_param3.f90:11-13) */
+double og_adisit(double th, double sh, double pa) {
+  const double a1 = 3.6504E-4, a2 = 8.3198E-5, a3 = 5.4065E-7, a4 = 4.0274E-9;
+  const double b1 = 1.7439E-5, b2 = 2.9778E-7, c1 = 8.9309E-7, c2 = 3.1628E-8;
+  const double c3 = 2.1987E-10, d = 4.1057E-9, e1 = 1.6056E-10, e2 = 5.0484E-12;
+  const double pr = pa;
+  const double qc = pr * (a1 + pr * (c1 - e1 * pr));
+  const double qv = pr * (b1 - d * pr);
+  const double dc = 1. + pr * (-a2 + pr * (c2 - e2 * pr));
+  const double dv = b2 * pr;
+  const double qnq = -pr * (-a3 + pr * c3);
+  const double qn3 = -pr * a4;
+  const double qvs = qv * (sh - 35.) + qc;
+  const double dvs = dv * (sh - 35.) + dc;
+  const double tpo = th;
+  th = (th + qvs) / dvs;
+  const double t = th;
+  const double fne = -qvs + t * (dvs + t * (qnq + t * qn3)) - tpo;
+  const double fst = dvs + t * (2 * qnq + 3 * qn3 * t);
+  return th - fne / fst;
+}
+
+/* rho1j.f90:82-115 */
+double og_rho1(double t, double s, double p) {
+  const double b0 = 8.24493E-1, b1 = -4.0899E-3, b2 = 7.6438E-5, b3 = -8.2467E-7, b4 = 5.3875E-9;
+  const double c0 = -5.72466E-3, c1 = 1.0227E-4, c2 = -1.6546E-6, d0 = 4.8314E-4;
+  const double a0 = 999.8426, a1 = 6.793952E-2, a2 = -9.095290E-3, a3 = 1.001685E-4,
+               a4 = -1.120083E-6, a5 = 6.536332E-9;
+  const double f0 = 54.6746, f1 = -0.603459, f2 = 1.09987E-2, f3 = -6.1670E-5;
+  const double g0 = 7.944E-2, g1 = 1.6483E-2, g2 = -5.3009E-4;
+  const double ai0 = 2.2838E-3, ai1 = -1.0981E-5, ai2 = -1.6078E-6, aj0 = 1.91075E-4;
+  const double am0 = -9.9348E-7, am1 = 2.0816E-8, am2 = 9.1697E-10;
+  const double e0 = 19652.21, e1 = 148.4206, e2 = -2.327105, e3 = 1.360477E-2, e4 = -5.155288E-5;
+  const double h0 = 3.239908, h1 = 1.43713E-3, h2 = 1.16092E-4, h3 = -5.77905E-7;
+  const double ak0 = 8.50935E-5, ak1 = -6.12293E-6, ak2 = 5.2787E-8;
+  s = fmx(s, 28.);
+  const double s3h = sqrt(s * s * s);
+  const double num = a0 + t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5)))) +
+                     s * (b0 + t * (b1 + t * (b2 + t * (b3 + t * b4)))) + d0 * (s * s) +
+                     s3h * (c0 + t * (c1 + c2 * t));
+  const double kk = p * (h0 + t * (h1 + t * (h2 + t * h3)) + s * (ai0 + t * (ai1 + ai2 * t)) +
+                         aj0 * s3h + (ak0 + t * (ak1 + t * ak2) + s * (am0 + t * (am1 + t * am2))) * p) +
+                    e0 + t * (e1 + t * (e2 + t * (e3 + t * e4))) +
+                    s * (f0 + t * (f1 + t * (f2 + t * f3))) + s3h * (g0 + t * (g1 + g2 * t));
+  return num / (1. - p / kk);
+}
+
+/* density of potential temperature th, salinity s at reference pressure p
+ * (ADISITJ then RHO1J, octher.f90:147-148), or the linear option */
+static double og_density(const og_thermo *t, double th, double s, double p) {
+  if (t->eos == 1) return t->rho0 + t->drdt * (th - t->t0) + t->drds * (s - t->s0);
+  return og_rho1(og_adisit(th, s, p), s, p);
+}
+
+#define OPT2(a, i, j) ((a) ? P2((a), i, j) : 0.0)
+
+/* octher.f90:43-107 */
+void og_octher_surface(const og_grid *g, const og_thermo *t, double *tho, double *sao,
+                       double *zo, double *eminpo, double *rivrun) {
+  DIMS;
+  const double dt = g->dt;
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      P2(eminpo, i, j) = 0.;
+      const double reiscon = 1. - OPT2(t->sicomo, i, j); /* EISREST */
+      const double oldso = P3(sao, i, j, 1);
+      P3(sao, i, j, 1) = P3(sao, i, j, 1) + dt * t->relsal * reiscon *
+                                                (OPT2(t->relsao, i, j) - P3(sao, i, j, 1));
+      P3(tho, i, j, 1) =
+          P3(tho, i, j, 1) + dt * t->reltem * (OPT2(t->reltho, i, j) - P3(tho, i, j, 1));
+      P2(eminpo, i, j) = (P3(g->ddpo, i, j, 1) + P2(zo, i, j) - OPT2(t->sictho, i, j) * t->rhoicwa -
+                          OPT2(t->sicsno, i, j) * t->rhosnwa) *
+                         (fmx(oldso, 1.E-3) / fmx(P3(sao, i, j, 1), 1.E-3) - 1.);
+    }
+  const double dti = 1. / dt;
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      P2(zo, i, j) = (P2(zo, i, j) + P2(eminpo, i, j)) * P3(g->weto, i, j, 1);
+      P2(eminpo, i, j) = P2(eminpo, i, j) * dti;
+    }
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      const double zzzdz = fmx(g->almzer, P3(g->ddpo, i, j, 1) + P2(zo, i, j) -
+                                              OPT2(t->sictho, i, j) * t->rhoicwa -
+                                              OPT2(t->sicsno, i, j) * t->rhosnwa);
+      const double driv = OPT2(t->giriv, i, j) * dt;
+      P3(sao, i, j, 1) = P3(sao, i, j, 1) * zzzdz / (zzzdz + driv);
+      P2(zo, i, j) = P2(zo, i, j) + driv;
+      P2(rivrun, i, j) = driv / dt;
+    }
+}
+
+/* octher.f90:139-451 */
+void og_octher_column(const og_grid *g, const og_thermo *t, double *tho, double *sao,
+                      const double *zo, const double *uko, const double *vke, double *po,
+                      double *stabio, double *rhoo, double *avo, double *dvo, int *kcondep) {
+  DIMS;
+  const double G = t->grav;
+  const double one = 1.;
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      /* C.1 upper layer (octher.f90:142-154) */
+      const double rh1 = og_density(t, P3(tho, i, j, 1), P3(sao, i, j, 1), K1(t->preff, 1));
+      P3(stabio, i, j, 1) = 0.;
+      P3(po, i, j, 1) = G * K1(g->tiestu, 1) * 0.00097 * rh1;
+      /* C.2 levels 2..KE (octher.f90:164-259); ZSURF(K-1) = 1 only for K = 2 */
+      for (int k = 2; k <= KE; ++k) {
+        const double disti = 1. / K1(g->dz, k);
+        const double rh = og_density(t, P3(tho, i, j, k), P3(sao, i, j, k), K1(t->preff, k));
+        const double rup = og_density(t, P3(tho, i, j, k - 1), P3(sao, i, j, k - 1), K1(t->preff, k));
+        P3(stabio, i, j, k) = disti * (rh - rup);
+        P3(po, i, j, k) = P3(po, i, j, k - 1) + G * K1(g->dz, k) * 0.00049 * (rh + rup);
+        const double zs = k - 1 == 1 ? 1. : 0.;
+        const double surf =
+            zs * (P2(zo, i, j) - OPT2(t->sictho, i, j) * t->rhoicwa - OPT2(t->sicsno, i, j) * t->rhosnwa);
+        const double tq = ((P3(g->ddpo, i, j, k - 1) + surf) * P3(tho, i, j, k - 1) +
+                           P3(g->ddpo, i, j, k) * P3(tho, i, j, k)) /
+                          (P3(g->ddpo, i, j, k) + P3(g->ddpo, i, j, k - 1) + surf +
+                           (1. - P3(g->weto, i, j, k)));
+        const double sq = ((P3(g->ddpo, i, j, k - 1) + surf) * P3(sao, i, j, k - 1) +
+                           P3(g->ddpo, i, j, k) * P3(sao, i, j, k)) /
+                          (P3(g->ddpo, i, j, k) + P3(g->ddpo, i, j, k - 1) + surf +
+                           (1. - P3(g->weto, i, j, k)));
+        const double st = P3(stabio, i, j, k);
+        double switc = fmx(0., -st / (1.E-11 + fabs(st))) * P3(g->weto, i, j, k);
+        const double helpswi = switc; /* NURDIF */
+        switc = 0.;
+        P3(tho, i, j, k - 1) = tq * switc + (one - switc) * P3(tho, i, j, k - 1);
+        P3(tho, i, j, k) = tq * switc + (one - switc) * P3(tho, i, j, k);
+        P3(sao, i, j, k - 1) = sq * switc + (one - switc) * P3(sao, i, j, k - 1);
+        P3(sao, i, j, k) = sq * switc + (one - switc) * P3(sao, i, j, k);
+        P3(stabio, i, j, k) = (one - switc) * P3(stabio, i, j, k);
+        P3(stabio, i, j, k) = fmx(P3(stabio, i, j, k), 0.);
+        switc = helpswi;
+        if (P2(kcondep, i, j) == k - 1) P2(kcondep, i, j) += switc >= 0.5 ? 1 : 0; /* NINT */
+      }
+    }
+  /* D: Richardson-number mixing (octher.f90:294-403) */
+  const double relne = 0.4, relax = 1. - relne, gor = G / 1025.;
+  const double cra = 5., crd = 5., wpendep = 40.;
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= JE1; ++j)
+    for (int i = 1; i <= IE1; ++i) {
+      const double ice = 1. - OPT2(t->sicomo, i, j);
+      const double f = OPT2(t->fu10, i, j);
+      double t1 = t->wt * (ice * ice) * (f * f * f); /* REDWMICE */
+      double s1 = t->wt * (ice * ice) * (f * f * f);
+      for (int k = 2; k <= KE; ++k) {
+        const int ko = k - 1;
+        const double stabeps = t->cstabeps / K1(g->dzw, ko);
+        const double wtdecay = exp(-K1(g->dzw, ko) / wpendep);
+        const double topnah = 0.0;
+        const double zs = ko == 1 ? 1. : 0.;
+        t1 = t1 * wtdecay * stabeps /
+             (stabeps + 0.5 * (P3(stabio, i, j, k) + (1. - zs) * P3(stabio, i, j, ko)));
+        s1 = s1 * wtdecay * stabeps /
+             (stabeps + 0.5 * (P3(stabio, i, j, k) + (1. - zs) * P3(stabio, i, j, ko)));
+        const double du1 = U3(uko, i - 1, j, k) - U3(uko, i - 1, j, ko);
+        const double du2 = U3(uko, i, j, k) - U3(uko, i, j, ko);
+        const double dv1 = V3(vke, i, j - 1, k) - V3(vke, i, j - 1, ko);
+        const double dv2 = V3(vke, i, j, k) - V3(vke, i, j, ko);
+        const double w = P3(g->weto, i, j, k);
+        const double dik = K1(g->di, k);
+        const double dudo =
+            g->almzer + w * (dik * dik) * (du1 * du1 + du2 * du2 + dv1 * dv1 + dv2 * dv2) * 0.5;
+        const double hho = w * (U3(g->amsuo, i, j, k) + U3(g->amsuo, i - 1, j, k) +
+                                V3(g->amsue, i, j - 1, k) + V3(g->amsue, i, j, k)) *
+                           0.25;
+        const double rinumo = hho * fmx(gor * P3(stabio, i, j, k) / dudo, 0.);
+        const double xd = 1. + crd * rinumo, xa = 1. + cra * rinumo;
+        double *dv = &P3(dvo, i, j, k), *av = &P3(avo, i, j, k);
+        *dv = (relax * fmn(*dv, t->dv0 + s1) +
+               relne * (s1 + t->dv0 / (xd * xd * xd) + K1(t->dbackv, k) + topnah)) * w;
+        *av = (relax * fmn(*av, t->av0 + K1(t->abackv, k)) +
+               relne * (t1 + t->av0 / (xa * xa) + K1(t->abackv, k) + topnah)) * w;
+        const double st = P3(stabio, i, j, k);
+        *av = w * fmx(t->cavocon * (1.E-11 - st) / (1.E-11 + fabs(st)), *av);
+        *dv = w * fmx(t->cdvocon * (1.E-11 - st) / (1.E-11 + fabs(st)), *dv);
+        P3(stabio, i, j, k) = fmx(P3(stabio, i, j, k), 0.);
+      }
+    }
+  /* octher.f90:415-451 */
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      P3(avo, i, j, KEP) = 0.;
+      P3(dvo, i, j, KEP) = 0.;
+      for (int k = 2; k <= KE; ++k)
+        if (P3(g->weto, i, j, k) < 0.5) {
+          P3(tho, i, j, k) = P3(tho, i, j, k - 1);
+          P3(sao, i, j, k) = P3(sao, i, j, k - 1);
+        }
+      for (int k = 1; k <= KE; ++k)
+        P3(rhoo, i, j, k) = og_density(t, P3(tho, i, j, k), P3(sao, i, j, k), K1(t->preff, k));
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCMODMOM (ocmodmom.f90), NON_HYDROSTATIC                                  */
+/* ------------------------------------------------------------------------ */
+/* GILA / GIPH are (ITO, JTO) = (2 IE, 2 JE), 1-based */
+#define GI(a, ii, jj) (a)[(size_t)((jj)-1) * (2 * IE) + (size_t)((ii)-1)]
+#define W3(a, i, j, k) P3(a, i, j, k)
+
+void og_ocmodmom(const og_grid *g, const og_baro *b, const og_coriolis *c,
+                 const double *deutio, const double *deutie, const double *zo,
+                 const double *uoo, const double *voe, double *uko, double *vke, double *uk1o,
+                 double *vk1e, double *wno, double *wn1o, double *po, double *stabio,
+                 double *u1o, double *uso, double *v1e, double *vse) {
+  DIMS;
+  const double G = b->grav, stabn = b->stabn, stabo = 1. - b->stabn, dt = g->dt;
+  const double almzer = g->almzer, omega = c->omega;
+  const size_t nu = (size_t)(IE + 1) * JE * KE, nv = (size_t)IE * (JE + 1) * KE;
+  const size_t nw = (size_t)IE * JE * KEP;
+  double *ucor = zalloc(nu), *vcor = zalloc(nv), *wcor = zalloc(nw);
+  /* ocmodmom.f90:24-36 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i) U2(u1o, i, j) = U2(uso, i, j) = 0.;
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) V2(v1e, i, j) = V2(vse, i, j) = 0.;
+  /* ocmodmom.f90:39-62 */
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        P3(stabio, i, j, k) = 0.001 * K1(g->dz, k) * P3(stabio, i, j, k) * P3(g->weto, i, j, k);
+        P3(po, i, j, k) = P3(po, i, j, k) + G * P2(zo, i, j) * b->rlsa1;
+      }
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        U3(uko, i, j, k) = U3(uko, i, j, k) * U3(g->dduo, i, j, k);
+        U3(uk1o, i, j, k) = U3(uko, i, j, k);
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        V3(vke, i, j, k) = V3(vke, i, j, k) * V3(g->ddue, i, j, k);
+        V3(vk1e, i, j, k) = V3(vke, i, j, k);
+      }
+  }
+  memcpy(wn1o, wno, sizeof(double) * nw);
+  for (int iter = 1; iter <= 12; ++iter) {
+    /* ocmodmom.f90:76-96 */
+    for (int k = 1; k <= KE; ++k) {
+      for (int j = 1; j <= JE; ++j)
+        for (int i = 0; i <= IE; ++i)
+          U3(ucor, i, j, k) = stabn * U3(uk1o, i, j, k) + stabo * U3(uko, i, j, k);
+      for (int j = 0; j <= JE; ++j)
+        for (int i = 1; i <= IE; ++i)
+          V3(vcor, i, j, k) = stabn * V3(vk1e, i, j, k) + stabo * V3(vke, i, j, k);
+    }
+    for (int k = 1; k <= KEP; ++k)
+      for (int j = 1; j <= JE; ++j)
+        for (int i = 1; i <= IE; ++i)
+          W3(wcor, i, j, k) = stabn * W3(wn1o, i, j, k) + stabo * W3(wno, i, j, k);
+    /* ocmodmom.f90:99-170 */
+    for (int k = 1; k <= KE; ++k) {
+      for (int j = 2; j <= JE1; ++j)
+        for (int i = 1; i <= IE1; ++i) {
+          const double vcor_u = 0.25 * (V3(vcor, i, j, k) + V3(vcor, i + 1, j, k) +
+                                        V3(vcor, i, j - 1, k) + V3(vcor, i + 1, j - 1, k));
+          U3(uk1o, i, j, k) = U3(uko, i, j, k) +
+                              U2(g->dtdxuo, i, j) * (P3(po, i, j, k) - P3(po, i + 1, j, k)) *
+                                  U3(g->dduo, i, j, k) +
+                              dt * U2(c->ftwou, i, j) * vcor_u * U3(g->amsuo, i, j, k);
+        }
+      for (int j = 1; j <= JE1; ++j)
+        for (int i = 2; i <= IE1; ++i) {
+          const double ucor_v = 0.25 * (U3(ucor, i, j, k) + U3(ucor, i - 1, j, k) +
+                                        U3(ucor, i, j + 1, k) + U3(ucor, i - 1, j + 1, k));
+          V3(vk1e, i, j, k) = V3(vke, i, j, k) +
+                              V2(g->dpye, i, j) * (P3(po, i, j + 1, k) - P3(po, i, j, k)) *
+                                  V3(g->ddue, i, j, k) -
+                              dt * V2(c->ftwov, i, j) * ucor_v * V3(g->amsue, i, j, k);
+        }
+      for (int j = 2; j <= JE1; ++j)
+        for (int i = 1; i <= IE1; ++i) {
+          const double dlon = (GI(c->gila, 2 * i + 2, 2 * j) - GI(c->gila, 2 * i + 1, 2 * j)) *
+                              cos(GI(c->gila, 2 * i + 1, 2 * j));
+          const double dlat = GI(c->giph, 2 * i + 2, 2 * j) - GI(c->giph, 2 * i + 1, 2 * j);
+          const double dist = sqrt(dlon * dlon + dlat * dlat) + almzer;
+          const double ftwou1 = 2 * omega * cos(GI(c->giph, 2 * i + 1, 2 * j));
+          const double wcor_u = 0.25 *
+                                ((W3(wcor, i, j, k) + W3(wcor, i, j, k + 1)) * P2(g->dlxp, i, j) +
+                                 (W3(wcor, i + 1, j, k) + W3(wcor, i + 1, j, k + 1)) * P2(g->dlxp, i + 1, j)) /
+                                U2(g->dlxu, i, j);
+          U3(uk1o, i, j, k) =
+              U3(uk1o, i, j, k) - dt * ftwou1 * wcor_u * U3(g->dduo, i, j, k) * dlon / dist;
+        }
+      for (int j = 1; j <= JE1; ++j)
+        for (int i = 2; i <= IE1; ++i) {
+          const double dlon = (GI(c->gila, 2 * i, 2 * j) - GI(c->gila, 2 * i, 2 * j + 1)) *
+                              cos(GI(c->gila, 2 * i, 2 * j + 1));
+          const double dlat = GI(c->giph, 2 * i, 2 * j) - GI(c->giph, 2 * i, 2 * j + 1);
+          const double dist = sqrt(dlon * dlon + dlat * dlat) + almzer;
+          const double ftwov1 = 2 * omega * cos(GI(c->giph, 2 * i, 2 * j + 1));
+          const double wcor_v = 0.25 *
+                                ((W3(wcor, i, j, k) + W3(wcor, i, j, k + 1)) * P2(g->dlyp, i, j) +
+                                 (W3(wcor, i, j + 1, k) + W3(wcor, i, j + 1, k + 1)) * P2(g->dlyp, i, j + 1)) /
+                                V2(g->dlyv, i, j);
+          V3(vk1e, i, j, k) =
+              V3(vk1e, i, j, k) - dt * ftwov1 * wcor_v * V3(g->ddue, i, j, k) * dlon / dist;
+        }
+      if (k > 1)
+        for (int j = 2; j <= JE1; ++j)
+          for (int i = 2; i <= IE1; ++i) {
+            const double dlon = (GI(c->gila, 2 * i + 1, 2 * j) - GI(c->gila, 2 * i, 2 * j)) *
+                                cos(GI(c->gila, 2 * i, 2 * j));
+            const double dlat = GI(c->giph, 2 * i, 2 * j - 1) - GI(c->giph, 2 * i, 2 * j);
+            const double dist = sqrt(dlon * dlon + dlat * dlat) + almzer;
+            const double ftwow1 = 2 * omega * cos(GI(c->giph, 2 * i, 2 * j));
+            const double ucor_w =
+                0.25 * ((U3(uko, i, j, k) + U3(uko, i - 1, j, k)) / (P3(g->ddpo, i, j, k) + almzer) +
+                        (U3(uko, i, j, k - 1) + U3(uko, i - 1, j, k - 1)) /
+                            (P3(g->ddpo, i, j, k - 1) + almzer));
+            const double vcor_w =
+                0.25 * ((V3(vke, i, j, k) + V3(vke, i, j - 1, k)) / (P3(g->ddpo, i, j, k) + almzer) +
+                        (V3(vke, i, j, k - 1) + V3(vke, i, j - 1, k - 1)) /
+                            (P3(g->ddpo, i, j, k - 1) + almzer));
+            W3(wn1o, i, j, k) = W3(wno, i, j, k) +
+                                dt * P3(g->weto, i, j, k) *
+                                    (ftwow1 * dlon / dist * ucor_w - ftwow1 * dlat / dist * vcor_w);
+          }
+    }
+    /* ocmodmom.f90:177-183 */
+    memcpy(wno, wn1o, sizeof(double) * nw);
+  }
+  /* ocmodmom.f90:193-215 */
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) P3(po, i, j, k) = P3(po, i, j, k) - G * P2(zo, i, j) * b->rlsa1;
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        U2(u1o, i, j) = U2(u1o, i, j) + U3(g->dduo, i, j, k) * U3(uoo, i, j, k);
+        U2(uso, i, j) = U2(uso, i, j) + U3(uk1o, i, j, k);
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        V2(v1e, i, j) = V2(v1e, i, j) + V3(g->ddue, i, j, k) * V3(voe, i, j, k);
+        V2(vse, i, j) = V2(vse, i, j) + V3(vk1e, i, j, k);
+      }
+  }
+  /* ocmodmom.f90:219-237 */
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        U3(uko, i, j, k) = U3(uoo, i, j, k) - U3(g->amsuo, i, j, k) * U2(deutio, i, j) * U2(u1o, i, j);
+        U3(uk1o, i, j, k) = U3(uk1o, i, j, k) * (U3(g->amsuo, i, j, k) / (almzer + U3(g->dduo, i, j, k))) -
+                            U3(g->amsuo, i, j, k) * U2(deutio, i, j) * U2(uso, i, j);
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        V3(vke, i, j, k) = V3(voe, i, j, k) - V3(g->amsue, i, j, k) * V2(deutie, i, j) * V2(v1e, i, j);
+        V3(vk1e, i, j, k) = V3(vk1e, i, j, k) * (V3(g->amsue, i, j, k) / (almzer + V3(g->ddue, i, j, k))) -
+                            V3(g->amsue, i, j, k) * V2(deutie, i, j) * V2(vse, i, j);
+      }
+  }
+  free(ucor);
+  free(vcor);
+  free(wcor);
+}
+
+/* ------------------------------------------------------------------------ */
+/* OCCLIT (occlit.f90)                                                       */
+/* ------------------------------------------------------------------------ */
+/* vertical velocity from the divergence of transports uko / vke (already
+ * multiplied by the thicknesses), bottom up from `bottom` (occlit.f90:108-112,
+ * 250-254): out(k) = below + DTI WETO (...) */
+static double og_occlit_div(const og_grid *g, const double *uko, const double *vke, int i, int j,
+                            int k, double below) {
+  const int IE = g->ie, JE = g->je;
+  const double dti = 1. / g->dt;
+  return below + dti * P3(g->weto, i, j, k) *
+                     (P2(g->dtdxpo, i, j) *
+                          (U3(uko, i - 1, j, k) * U2(g->dlyu, i - 1, j) - U3(uko, i, j, k) * U2(g->dlyu, i, j)) /
+                          P2(g->dlyp, i, j) +
+                      P2(g->dtdyo, i, j) *
+                          (V3(vke, i, j, k) * V2(g->dlxv, i, j) - V3(vke, i, j - 1, k) * V2(g->dlxv, i, j - 1)) /
+                          P2(g->dlxp, i, j));
+}
+
+double og_occlit(const og_grid *g, const og_baro *b, const double *deutio,
+                 const double *deutie, double *uko, double *vke, double *uk1o, double *vk1e,
+                 double *wo, double *stabio) {
+  DIMS;
+  const double G = b->grav, stabn = b->stabn, conn = b->conn, dt = g->dt, almzer = g->almzer;
+  const size_t n2 = (size_t)IE * JE, n3 = n2 * KE;
+  double *bruva = zalloc(n2), *slow = zalloc(n2), *tlow = zalloc(n2), *contrij = zalloc(n2);
+  double *pxoin = zalloc((size_t)(IE + 1) * JE), *ucos = zalloc((size_t)(IE + 1) * JE);
+  double *pyein = zalloc((size_t)IE * (JE + 1)), *vcos = zalloc((size_t)IE * (JE + 1));
+  double *t1o = zalloc(n3), *wpo = zalloc(n3);
+  /* occlit.f90:20-63 (PXOIN / PYEIN of this first pass are reset before use) */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) P3(stabio, i, j, 1) = 0.;
+  for (int k = 1; k <= KE; ++k)
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i)
+        P2(bruva, i, j) = P2(bruva, i, j) + K1(g->tiestw, k + 1) * P3(stabio, i, j, k);
+  /* occlit.f90:85-101 */
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        U3(uko, i, j, k) = U3(uko, i, j, k) * U3(g->dduo, i, j, k);
+        U3(uk1o, i, j, k) = U3(uk1o, i, j, k) * U3(g->dduo, i, j, k);
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        V3(vke, i, j, k) = V3(vke, i, j, k) * V3(g->ddue, i, j, k);
+        V3(vk1e, i, j, k) = V3(vk1e, i, j, k) * V3(g->ddue, i, j, k);
+      }
+  }
+  /* occlit.f90:104-127 */
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i)
+      for (int k = KE; k >= 1; --k) P3(wo, i, j, k) = og_occlit_div(g, uko, vke, i, j, k, P3(wo, i, j, k + 1));
+  for (int j = 1; j <= JE; ++j)
+    for (int k = 1; k <= KE; ++k)
+      for (int i = 1; i <= IE; ++i) {
+        P3(t1o, i, j, k) = P3(wo, i, j, k);
+        P2(slow, i, j) = P2(slow, i, j) + P3(stabio, i, j, k) * dt * P3(wo, i, j, k);
+        P3(wpo, i, j, k) = P2(slow, i, j);
+      }
+  double under = 0.;
+  const int itermax = 8;
+  for (int iter = 1; iter <= itermax; ++iter) {
+    /* occlit.f90:139-183 */
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) U2(ucos, i, j) = U2(pxoin, i, j) = 0.;
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) V2(vcos, i, j) = V2(pyein, i, j) = 0.;
+    for (int k = 1; k <= KE; ++k) {
+      for (int j = 1; j <= JE; ++j)
+        for (int i = 1; i <= IE1; ++i)
+          U2(pxoin, i, j) = U2(pxoin, i, j) + U3(g->dduo, i, j, k) * U2(g->dtdxuo, i, j) *
+                                                  (P3(wpo, i + 1, j, k) - P3(wpo, i, j, k)) *
+                                                  U3(g->amsuo, i, j, k);
+      for (int j = 1; j <= JE1; ++j)
+        for (int i = 1; i <= IE; ++i)
+          V2(pyein, i, j) = V2(pyein, i, j) + V3(g->ddue, i, j, k) * V2(g->dpye, i, j) *
+                                                  (P3(wpo, i, j, k) - P3(wpo, i, j + 1, k)) *
+                                                  V3(g->amsue, i, j, k);
+    }
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE1; ++i) U2(pxoin, i, j) = U2(pxoin, i, j) * U2(deutio, i, j);
+    for (int j = 1; j <= JE1; ++j)
+      for (int i = 1; i <= IE; ++i) V2(pyein, i, j) = V2(pyein, i, j) * V2(deutie, i, j);
+    /* occlit.f90:191-228 */
+    for (int k = 1; k <= KE; ++k) {
+      for (int j = 2; j <= JE1; ++j)
+        for (int i = 1; i <= IE1; ++i) {
+          U3(uko, i, j, k) = U3(uk1o, i, j, k) +
+                             stabn * (U2(pxoin, i, j) - U2(g->dtdxuo, i, j) * (P3(wpo, i + 1, j, k) - P3(wpo, i, j, k))) *
+                                 U3(g->dduo, i, j, k);
+          U2(ucos, i, j) = U2(ucos, i, j) + U3(uko, i, j, k);
+          U3(uko, i, j, k) = U3(uko, i, j, k) * U3(g->amsuo, i, j, k);
+        }
+      for (int j = 1; j <= JE1; ++j)
+        for (int i = 2; i <= IE1; ++i) {
+          V3(vke, i, j, k) = V3(vk1e, i, j, k) +
+                             stabn * (V2(pyein, i, j) - V2(g->dpye, i, j) * (P3(wpo, i, j, k) - P3(wpo, i, j + 1, k))) *
+                                 V3(g->ddue, i, j, k);
+          V2(vcos, i, j) = V2(vcos, i, j) + V3(vke, i, j, k);
+          V3(vke, i, j, k) = V3(vke, i, j, k) * V3(g->amsue, i, j, k);
+        }
+    }
+    for (int k = 1; k <= KE; ++k) {
+      for (int j = 2; j <= JE1; ++j)
+        for (int i = 1; i <= IE1; ++i)
+          U3(uko, i, j, k) = U3(uko, i, j, k) - U2(ucos, i, j) * U2(deutio, i, j) * U3(g->dduo, i, j, k);
+      for (int j = 1; j <= JE1; ++j)
+        for (int i = 2; i <= IE1; ++i)
+          V3(vke, i, j, k) = V3(vke, i, j, k) - V2(vcos, i, j) * V2(deutie, i, j) * V3(g->ddue, i, j, k);
+    }
+    if (iter == itermax) break;
+    /* occlit.f90:238-284 */
+    for (size_t q = 0; q < n2; ++q) tlow[q] = slow[q] = contrij[q] = 0.;
+    for (int k = KE; k >= 1; --k)
+      for (int j = 1; j <= JE; ++j)
+        for (int i = 1; i <= IE; ++i) {
+          P3(t1o, i, j, k) = og_occlit_div(g, uko, vke, i, j, k, P2(slow, i, j));
+          P2(slow, i, j) = P3(t1o, i, j, k);
+        }
+    for (int k = 2; k <= KE; ++k)
+      for (int j = 1; j <= JE; ++j)
+        for (int i = 1; i <= IE; ++i) {
+          const double ove = P3(wpo, i, j, k);
+          P2(tlow, i, j) = P2(tlow, i, j) + G * P3(stabio, i, j, k) * dt *
+                                                (conn * P3(t1o, i, j, k) + P3(wo, i, j, k));
+          const double speed = 2. * G * P2(bruva, i, j) *
+                               (U2(g->dtdxuo, i, j) * U2(g->dtdxuo, i, j) + P2(g->dtdyo, i, j) * P2(g->dtdyo, i, j));
+          const double brems = under * speed * conn * stabn / (1. + speed);
+          const double vorw = 1. - brems;
+          P3(wpo, i, j, k) = vorw * P2(tlow, i, j) + brems * P3(wpo, i, j, k);
+          const double d = ove - P3(wpo, i, j, k);
+          P2(contrij, i, j) = P2(contrij, i, j) + d * d;
+        }
+    under = 1.;
+  }
+  /* occlit.f90:289-305 */
+  for (int k = 1; k <= KE; ++k) {
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 0; i <= IE; ++i) {
+        U3(uko, i, j, k) = U3(uko, i, j, k) * U3(g->amsuo, i, j, k) / (almzer + U3(g->dduo, i, j, k));
+        U3(uk1o, i, j, k) = U3(uk1o, i, j, k) * U3(g->amsuo, i, j, k) / (almzer + U3(g->dduo, i, j, k));
+      }
+    for (int j = 0; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i) {
+        V3(vke, i, j, k) = V3(vke, i, j, k) * V3(g->amsue, i, j, k) / (almzer + V3(g->ddue, i, j, k));
+        V3(vk1e, i, j, k) = V3(vk1e, i, j, k) * V3(g->amsue, i, j, k) / (almzer + V3(g->ddue, i, j, k));
+      }
+  }
+  /* occlit.f90:309-317, global (J, I) order */
+  double contra = 0.;
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) contra = contra + P2(contrij, i, j);
+  free(bruva);
+  free(slow);
+  free(tlow);
+  free(contrij);
+  free(pxoin);
+  free(ucos);
+  free(pyein);
+  free(vcos);
+  free(t1o);
+  free(wpo);
+  return contra;
+}

@@ -174,6 +174,69 @@ void og_ocwind(const og_grid *g, const double *txo, const double *tye, const dou
 void og_ocvtot(const og_grid *g, const og_baro *b, const double *uso, const double *vse,
                double *uoo, double *voe, double *uko, double *vke, double *wo);
 
+/* ---- Thermodynamics, baroclinic pressure and mixing (OCTHER) ---------------
+ * As built by the reference's Makefile:42-51: EISREST (REISCON = 1 - SICOMO),
+ * REDWMICE (wind mixing (1 - SICOMO)**2), NURDIF (the convective switch
+ * counts KCONDEP but mixes no tracer), no PLUME, no UMKLAP.  eos 0 is the
+ * reference's ADISITJ + RHO1J (adisitj.f90, rho1j.f90); eos 1 is a linear
+ * equation of state, RHO = rho0 + drdt (T - t0) + drds (S - s0), which the
+ * reference lacks. */
+typedef struct og_thermo {
+  int eos;
+  double rho0, drdt, drds, t0, s0;    /* linear EOS */
+  double grav;                        /* G */
+  double relsal, reltem;              /* RELSAL, RELTEM (orctm.f90:561, 569) */
+  double rhoicwa, rhosnwa;            /* RHOICE/RHOWAT, RHOSNO/RHOWAT (orctm.f90:742-743) */
+  double wt;                          /* WT = CWT / 6**3 (orctm.f90:503) */
+  double cstabeps, dv0, av0, cavocon, cdvocon; /* orctm.f90:311-318 */
+  const double *preff;                /* PREFF(KE) = 0.1026 TIESTU (beleg.f90:127) */
+  const double *dbackv, *abackv;      /* DBACKV, ABACKV (KE+1) */
+  /* 2D (IE, JE); NULL reads as 0 */
+  const double *sicomo, *sictho, *sicsno, *relsao, *reltho, *giriv, *fu10;
+} og_thermo;
+/* ADISITJ on one value: potential to in-situ temperature at pressure pa. */
+double og_adisit(double th, double sh, double pa);
+/* RHO1J on one value (in-situ temperature t). */
+double og_rho1(double t, double s, double p);
+/* OCTHER part A (octher.f90:37-107): salinity / temperature restoring at the
+ * surface, the fresh-water flux EMINPO into ZO, river input.  rivrun (IE, JE)
+ * receives RIVRUN; PRECO / PRECH (flux diagnostics) are not kept. */
+void og_octher_surface(const og_grid *g, const og_thermo *t, double *tho, double *sao,
+                       double *zo, double *eminpo, double *rivrun);
+/* OCTHER parts C and D (octher.f90:123-451): density, baroclinic pressure PO,
+ * stability STABIO, the convection counter KCONDEP, the Richardson-number
+ * mixing coefficients AVO / DVO (w-points, KE+1 levels), the tracers copied
+ * down into land, and RHOO.  Part B, the T/S boundary forcing, runs between
+ * og_octher_surface and this (og_obc_ts). */
+void og_octher_column(const og_grid *g, const og_thermo *t, double *tho, double *sao,
+                      const double *zo, const double *uko, const double *vke, double *po,
+                      double *stabio, double *rhoo, double *avo, double *dvo, int *kcondep);
+
+/* ---- Barotropic / baroclinic decomposition (OCMODMOM) ----------------------
+ * Coriolis inputs: ftwou u-points, ftwov v-points (the grid file's FTWOU,
+ * FTWOV), gila / giph (2 IE, 2 JE) the double-resolution longitudes and
+ * latitudes (coriol.f90:46-47), omega (orctm.f90:678). */
+typedef struct og_coriolis {
+  const double *ftwou, *ftwov, *gila, *giph;
+  double omega;
+} og_coriolis;
+/* OCMODMOM (ocmodmom.f90:1-243), NON_HYDROSTATIC: 12 Coriolis iterations on
+ * UK1O, VK1E and WN1O (WNO follows WN1O), PO shifted by G ZO RLSA1 meanwhile,
+ * STABIO scaled to a density step, the vertical sums U1O, USO (u) and V1E,
+ * VSE (v), and UKO, VKE, UK1O, VK1E made baroclinic. */
+void og_ocmodmom(const og_grid *g, const og_baro *b, const og_coriolis *c,
+                 const double *deutio, const double *deutie, const double *zo,
+                 const double *uoo, const double *voe, double *uko, double *vke, double *uk1o,
+                 double *vk1e, double *wno, double *wn1o, double *po, double *stabio,
+                 double *u1o, double *uso, double *v1e, double *vse);
+/* OCCLIT (occlit.f90:1-332): 8 iterations of the baroclinic system in UKO,
+ * VKE with the vertical velocity WO; returns CONTRA, the sum of the squared
+ * WPO changes of the last completed update (the reference aborts above
+ * 1e-3). */
+double og_occlit(const og_grid *g, const og_baro *b, const double *deutio,
+                 const double *deutie, double *uko, double *vke, double *uk1o, double *vk1e,
+                 double *wo, double *stabio);
+
 #ifdef __cplusplus
 }
 #endif

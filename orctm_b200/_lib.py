@@ -76,7 +76,30 @@ class Barotropic(C.Structure):
                 ("sorpar", C.c_double), ("niter", C.c_int), ("eta_forc", C.c_int)]
 
 
-B_Z1O, B_B1O, B_USO, B_VSE, B_UZO, B_VZE = range(6)
+B_Z1O, B_B1O, B_USO, B_VSE, B_UZO, B_VZE, B_U1O, B_V1E = range(8)
+
+
+class Thermo(C.Structure):
+    """orctm_thermo: OCTHER's constants and surface forcing."""
+    _fields_ = [("eos", C.c_int), ("rho0", C.c_double), ("drdt", C.c_double),
+                ("drds", C.c_double), ("t0", C.c_double), ("s0", C.c_double),
+                ("grav", C.c_double), ("relsal", C.c_double), ("reltem", C.c_double),
+                ("rhoicwa", C.c_double), ("rhosnwa", C.c_double), ("wt", C.c_double),
+                ("cstabeps", C.c_double), ("dv0", C.c_double), ("av0", C.c_double),
+                ("cavocon", C.c_double), ("cdvocon", C.c_double),
+                ("preff", _D), ("dbackv", _D), ("abackv", _D),
+                ("sicomo", _D), ("sictho", _D), ("sicsno", _D), ("relsao", _D), ("reltho", _D),
+                ("giriv", _D), ("fu10", _D)]
+
+
+class Coriolis(C.Structure):
+    """orctm_coriolis: OCMODMOM's Coriolis inputs."""
+    _fields_ = [("ftwou", _D), ("ftwov", _D), ("gila", _D), ("giph", _D), ("omega", C.c_double)]
+
+
+EOS_UNESCO, EOS_LINEAR = 0, 1
+(C_PO, C_STABIO, C_RHOO, C_UK1O, C_VK1E, C_EMINPO, C_RIVRUN, C_KCONDEP) = range(8)
+E_UNSTABLE = -9
 
 
 class NoAllocArgs(C.Structure):
@@ -108,6 +131,8 @@ EXPORTS = (
     "orctm_set_obc_ts", "orctm_obc_ts", "orctm_octdiff_noalloc",
     "orctm_set_barotropic", "orctm_troneu", "orctm_ocvtro", "orctm_ocvtot",
     "orctm_download_barotropic", "orctm_ocbarp", "orctm_ocwind", "orctm_trotest",
+    "orctm_set_thermo", "orctm_set_coriolis", "orctm_octher", "orctm_ocmodmom", "orctm_occlit",
+    "orctm_upload_baroclinic", "orctm_download_baroclinic", "orctm_step_full",
 )
 
 PROF_KINDS = ("ocuad", "ocvad", "ocwad", "ocadpo", "octdiff", "ocvisc", "nh_rhs", "pcg_spmv",
@@ -182,6 +207,14 @@ def load(build_if_missing: bool = True):
     lib.orctm_ocbarp.argtypes = [C.c_void_p]
     lib.orctm_trotest.argtypes = [C.c_void_p, C.c_int, C.c_int, _D]
     lib.orctm_ocwind.argtypes = [C.c_void_p, _D, _D, _D, _D, _D, _D]
+    lib.orctm_set_thermo.argtypes = [C.c_void_p, C.POINTER(Thermo)]
+    lib.orctm_set_coriolis.argtypes = [C.c_void_p, C.POINTER(Coriolis)]
+    lib.orctm_octher.argtypes = [C.c_void_p]
+    lib.orctm_ocmodmom.argtypes = [C.c_void_p]
+    lib.orctm_occlit.argtypes = [C.c_void_p, _D]
+    lib.orctm_upload_baroclinic.argtypes = [C.c_void_p, C.c_int, _D, C.c_size_t]
+    lib.orctm_download_baroclinic.argtypes = [C.c_void_p, C.c_int, _D, C.c_size_t]
+    lib.orctm_step_full.argtypes = [C.c_void_p, C.c_int, C.POINTER(SolveStats), _D]
     _lib = lib
     return lib
 

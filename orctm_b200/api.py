@@ -205,6 +205,7 @@ class Instance:
     def __init__(self, inst: dict, device: int = 0):
         self.lib = _lib.load()
         self.ie, self.je, self.ke = inst["ie"], inst["je"], inst["ke"]
+        self.dzw1 = float(np.asarray(inst["dzw"])[0])
         self.ntr = int(inst.get("ntracers", len(inst.get("tracers", [])) or 2))
         d, keep = make_desc(inst, device)
         h = C.c_void_p()
@@ -367,7 +368,105 @@ class Instance:
 
     # -- barotropic solve (itprep.f90, troneu.f90, ocvtro.f90, ocvtot.f90) -------
     BARO_FIELDS = {"z1o": ("p", _lib.B_Z1O), "b1o": ("p", _lib.B_B1O), "uso": ("u", _lib.B_USO),
-                   "vse": ("v", _lib.B_VSE), "uzo": ("u", _lib.B_UZO), "vze": ("v", _lib.B_VZE)}
+                   "vse": ("v", _lib.B_VSE), "uzo": ("u", _lib.B_UZO), "vze": ("v", _lib.B_VZE),
+                   "u1o": ("u", _lib.B_U1O), "v1e": ("v", _lib.B_V1E)}
+
+    # OCTHER's constants as the reference driver sets them (orctm.f90:311-330,
+    # 503, 561-569, 739-743); eos "unesco" = ADISITJ + RHO1J, "linear" =
+    # rho0 + drdt (T - t0) + drds (S - s0)
+    THERMO_DEFAULTS = {"eos": "unesco", "rho0": 1025.0, "drdt": -0.2, "drds": 0.78, "t0": 10.0,
+                       "s0": 35.0, "grav": 9.806, "crelsal": 3.E-7, "creltem": 0.0,
+                       "rhoicwa": 0.91E+03 / 1.025E+03, "rhosnwa": 0.33E+03 / 1.025E+03,
+                       "wt": 0.5E-3 / (6.0 ** 3), "cstabeps": 0.05, "dv0": 0.5E-2, "av0": 0.5E-2,
+                       "cavocon": 0.0, "cdvocon": 20.0, "aback": 5.E-5, "dback": 5.E-5}
+    THERMO_2D = ("sicomo", "sictho", "sicsno", "relsao", "reltho", "giriv", "fu10")
+    BAROCLINIC = {"po": ("p3", _lib.C_PO), "stabio": ("p3", _lib.C_STABIO),
+                  "rhoo": ("p3", _lib.C_RHOO), "uk1o": ("u3", _lib.C_UK1O),
+                  "vk1e": ("v3", _lib.C_VK1E), "eminpo": ("p", _lib.C_EMINPO),
+                  "rivrun": ("p", _lib.C_RIVRUN), "kcondep": ("p", _lib.C_KCONDEP)}
+
+    def set_thermo(self, **kw):
+        """OCTHER's constants and forcing (orctm_set_thermo).  Keys as
+        THERMO_DEFAULTS plus relsal / reltem (default CRELSAL 20 / DZW(1)),
+        preff (KE), dbackv / abackv (KE+1) and the (IE, JE) forcing arrays
+        THERMO_2D (absent = 0); ``eos`` is "unesco", "linear" or 0 / 1."""
+        v = dict(self.THERMO_DEFAULTS, **kw)
+        eos = {"unesco": _lib.EOS_UNESCO, "linear": _lib.EOS_LINEAR}.get(v["eos"], v["eos"])
+        dzw1 = self.dzw1
+        relsal = v.get("relsal", v["crelsal"] * 20. / dzw1)
+        reltem = v.get("reltem", v["creltem"] * 20. / dzw1)
+        ke = self.ke
+        keep = []
+
+        def arr(a, shape=None):
+            if a is None:
+                return None
+            a = np.asfortranarray(a, dtype=np.float64)
+            if shape is not None and a.shape != shape:
+                raise ValueError(f"OCTHER input shape {a.shape}, expected {shape}")
+            keep.append(a)
+            return _p(a)
+
+        dbackv = arr(v.get("dbackv", np.full(ke + 1, v["dback"])), (ke + 1,))
+        abackv = arr(v.get("abackv", np.full(ke + 1, v["aback"])), (ke + 1,))
+        preff = arr(v.get("preff"), (ke,))
+        t = _lib.Thermo(int(eos), v["rho0"], v["drdt"], v["drds"], v["t0"], v["s0"], v["grav"],
+                        relsal, reltem, v["rhoicwa"], v["rhosnwa"], v["wt"], v["cstabeps"],
+                        v["dv0"], v["av0"], v["cavocon"], v["cdvocon"], preff, dbackv, abackv,
+                        *[arr(v.get(k), (self.ie, self.je)) for k in self.THERMO_2D])
+        _lib.check(self.lib.orctm_set_thermo(self.h, C.byref(t)), self.h)
+
+    def set_coriolis(self, ftwou, ftwov, gila, giph, omega: float = 7.292E-5):
+        """OCMODMOM's Coriolis inputs: FTWOU (IE+1, JE), FTWOV (IE, JE+1),
+        GILA / GIPH (2 IE, 2 JE)."""
+        ie, je = self.ie, self.je
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (ftwou, ftwov, gila, giph)]
+        for a, w in zip(arrs, [(ie + 1, je), (ie, je + 1), (2 * ie, 2 * je), (2 * ie, 2 * je)]):
+            if a.shape != w:
+                raise ValueError(f"Coriolis input shape {a.shape}, expected {w}")
+        c = _lib.Coriolis(*[_p(a) for a in arrs], float(omega))
+        _lib.check(self.lib.orctm_set_coriolis(self.h, C.byref(c)), self.h)
+
+    def octher(self):
+        _lib.check(self.lib.orctm_octher(self.h), self.h)
+
+    def ocmodmom(self):
+        _lib.check(self.lib.orctm_ocmodmom(self.h), self.h)
+
+    def occlit(self) -> float:
+        """OCCLIT; returns CONTRA (raises above 1e-3, as the reference aborts)."""
+        v = C.c_double()
+        _lib.check(self.lib.orctm_occlit(self.h, C.byref(v)), self.h)
+        return v.value
+
+    def _baroclinic_shape(self, name):
+        kind, which = self.BAROCLINIC[name]
+        ie, je, ke = self.ie, self.je, self.ke
+        return {"p3": (ie, je, ke), "u3": (ie + 1, je, ke), "v3": (ie, je + 1, ke),
+                "p": (ie, je)}[kind], which
+
+    def download_baroclinic(self, name: str) -> np.ndarray:
+        shp, which = self._baroclinic_shape(name)
+        a = np.zeros(shp, dtype=np.float64, order="F")
+        _lib.check(self.lib.orctm_download_baroclinic(self.h, which, _p(a), a.size), self.h)
+        return a
+
+    def upload_baroclinic(self, name: str, a):
+        shp, which = self._baroclinic_shape(name)
+        a = np.asfortranarray(a, dtype=np.float64)
+        if a.shape != shp:
+            raise ValueError(f"{name} shape {a.shape}, expected {shp}")
+        _lib.check(self.lib.orctm_upload_baroclinic(self.h, which, _p(a), a.size), self.h)
+
+    def step_full(self, ldtrun: int) -> dict:
+        """One whole step (orctm_step_full); the solve's statistics and CONTRA."""
+        s = SolveStats()
+        v = C.c_double()
+        _lib.check(self.lib.orctm_step_full(self.h, int(ldtrun), C.byref(s), C.byref(v)), self.h,
+                   allow=(_lib.ORCTM_E_NOT_CONVERGED,))
+        d = s.as_dict()
+        d["contra"] = v.value
+        return d
 
     def set_barotropic(self, deuto, deute, minvalue: float, grav=9.806, stabn=0.6, conn=0.5,
                        rlsa1=1.0 - 0.085, sorpar=1.75, niter=250, eta_forc=False):
@@ -387,8 +486,12 @@ class Instance:
         _lib.check(self.lib.orctm_trotest(self.h, int(ntry), int(niter), C.byref(v)), self.h)
         return v.value
 
-    def troneu(self, u1o, v1e, uzo, vze):
-        """TRONEU: B1O and Z1O from the transports (u: (IE+1, JE), v: (IE, JE+1))."""
+    def troneu(self, u1o=None, v1e=None, uzo=None, vze=None):
+        """TRONEU: B1O and Z1O from the transports (u: (IE+1, JE), v: (IE, JE+1));
+        with none given, from the device's (OCMODMOM's U1O, V1E, OCBARP's UZO, VZE)."""
+        if u1o is None and v1e is None and uzo is None and vze is None:
+            _lib.check(self.lib.orctm_troneu(self.h, None, None, None, None), self.h)
+            return
         arrs = [np.asfortranarray(a, dtype=np.float64) for a in (u1o, v1e, uzo, vze)]
         for a, k in zip(arrs, "uvuv"):
             want = (self.ie + 1, self.je) if k == "u" else (self.ie, self.je + 1)
@@ -405,8 +508,12 @@ class Instance:
     def ocbarp(self):
         _lib.check(self.lib.orctm_ocbarp(self.h), self.h)
 
-    def ocwind(self, txo, tye, sicomu, sicomv, tauwatu, tauwatv):
-        """OCWIND: TXO (IE+1, JE), TYE (IE, JE+1), the rest (IE, JE)."""
+    def ocwind(self, txo=None, tye=None, sicomu=None, sicomv=None, tauwatu=None, tauwatv=None):
+        """OCWIND: TXO (IE+1, JE), TYE (IE, JE+1), the rest (IE, JE); with none
+        given, the forcing of the previous call."""
+        if all(a is None for a in (txo, tye, sicomu, sicomv, tauwatu, tauwatv)):
+            _lib.check(self.lib.orctm_ocwind(self.h, None, None, None, None, None, None), self.h)
+            return
         ie, je = self.ie, self.je
         want = [(ie + 1, je), (ie, je + 1)] + [(ie, je)] * 4
         arrs = [np.asfortranarray(a, dtype=np.float64)

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 SO = os.path.join(HERE, "liborctm_gpu.so")
 SOURCES = ["advect.cu", "diffuse.cu", "nh.cu", "poisson.cu", "handle.cu", "grid.cpp", "serve.cpp", "extra.cpp",
-           "noalloc.cu", "obc.cu", "barotropic.cu"]
+           "noalloc.cu", "obc.cu", "barotropic.cu", "baroclinic.cu"]
 HEADERS = ["common.cuh", "ops.h", "tma.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

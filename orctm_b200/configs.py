@@ -409,3 +409,60 @@ def make_wind(inst: dict, seed: int | None = None) -> dict:
             "sicomv": np.asfortranarray(g.uniform(0.0, 1.0, (ie, je))),
             "tauwatu": np.asfortranarray(1e-4 * g.standard_normal((ie, je))),
             "tauwatv": np.asfortranarray(1e-4 * g.standard_normal((ie, je)))}
+
+
+def make_thermo(inst: dict, seed: int | None = None, eos: int | None = None) -> dict:
+    """Seeded surface forcing and switches of OCTHER: restoring targets RELSAO
+    / RELTHO near the surface tracers, 10 m wind speed FU10 (m/s), a few river
+    inflow points GIRIV (m/s), and no sea ice.  The vertical slice c1 uses the
+    linear equation of state its description asks for; the other workloads
+    the reference's UNESCO EOS.  Constants not given default to the
+    reference driver's (oracle.THERMO_DEFAULTS, also in orctm_b200.api)."""
+    ie, je = inst["ie"], inst["je"]
+    g = rng((inst["seed"] if seed is None else seed) + 2718)
+    tr = inst["tracers"]
+    w1 = inst["weto"][:, :, 0]
+    giriv = np.zeros((ie, je))
+    wet = np.argwhere(w1 > 0.5)
+    if len(wet):
+        for q in g.choice(len(wet), size=min(3, len(wet)), replace=False):
+            i, j = wet[q]
+            giriv[i, j] = 1e-4 * g.uniform(0.5, 1.5)
+    return {"eos": (1 if inst["name"] == "c1" else 0) if eos is None else eos,
+            "relsao": np.asfortranarray(tr[1][:, :, 0] + 0.1 * g.standard_normal((ie, je))),
+            "reltho": np.asfortranarray(tr[0][:, :, 0] + 0.5 * g.standard_normal((ie, je))),
+            "creltem": 1e-7,
+            "fu10": np.asfortranarray(g.uniform(2.0, 12.0, (ie, je))),
+            "giriv": np.asfortranarray(giriv)}
+
+
+def make_coriolis(inst: dict, lat0: float = 20.5, seed: int | None = None) -> dict:
+    """Coriolis inputs of OCMODMOM for a plane grid near latitude lat0 (deg):
+    FTWOU / FTWOV = 2 OMEGA sin(lat) at u- / v-points and the double-resolution
+    longitudes / latitudes GILA / GIPH (2 IE, 2 JE), radians, with a slight
+    seeded rotation so that both of their differences are non-zero."""
+    ie, je = inst["ie"], inst["je"]
+    g = rng((inst["seed"] if seed is None else seed) + 1618)
+    omega, radius = 7.292E-5, 6.371E6
+    dx = float(inst["dlxp"][0, 0])
+    rot = g.uniform(0.05, 0.15)
+    ii, jj = np.meshgrid(np.arange(1, 2 * ie + 1), np.arange(1, 2 * je + 1), indexing="ij")
+    x, y = 0.5 * dx * ii, 0.5 * dx * jj
+    xr, yr = x * math.cos(rot) - y * math.sin(rot), x * math.sin(rot) + y * math.cos(rot)
+    lat = math.radians(lat0) + yr / radius
+    lon = xr / (radius * math.cos(math.radians(lat0)))
+    # u-point (i, j) sits at the double-resolution index (2 i + 1, 2 j), v at (2 i, 2 j + 1)
+    ftwou = np.zeros((ie + 1, je))
+    ftwov = np.zeros((ie, je + 1))
+    for i in range(ie + 1):
+        ftwou[i, :] = 2.0 * omega * np.sin(lat[min(2 * i, 2 * ie - 1), 1::2])
+    for j in range(je + 1):
+        ftwov[:, j] = 2.0 * omega * np.sin(lat[1::2, min(2 * j, 2 * je - 1)])
+    return {"ftwou": np.asfortranarray(ftwou), "ftwov": np.asfortranarray(ftwov),
+            "gila": np.asfortranarray(lon), "giph": np.asfortranarray(lat), "omega": omega}
+
+
+def initial_kcondep(inst: dict) -> np.ndarray:
+    """KCONDEP as BODEN initialises it (boden.f90:261): 1 wet, -99 dry."""
+    w = inst["weto"][:, :, 0]
+    return np.asfortranarray(np.where(w > 0.5, 1, -99).astype(np.int32))

@@ -140,6 +140,7 @@ struct orctm_handle {
   int ntr = 2;
   std::string err;
   std::vector<double> tiestu, tiestw;  // level depths (BELEG), the EXTRA level codes
+  std::vector<double> dzw;             // layer thicknesses DZW
 
   // geometry / tables (device)
   std::vector<void*> owned;  // freed at destroy
@@ -194,6 +195,17 @@ struct orctm_handle {
   BaroFields bf{};
   cudaGraphExec_t sor_graph = nullptr;
   WindFields wind{};  // OCWIND's forcing (orctm_ocwind), allocated on first use
+  bool wind_ready = false;
+  // OCTHER (orctm_set_thermo), OCMODMOM's Coriolis factors
+  // (orctm_set_coriolis), UK1O / VK1E and the scratch of OCMODMOM and OCCLIT
+  bool thermo_ready = false, cor_ready = false;
+  ThermoArgs th{};
+  ThermoFields tf{};
+  CorFields cf{};
+  double *uk1o = nullptr, *vk1e = nullptr;
+  double *occ_wpo = nullptr, *occ_t1o = nullptr, *occ_bruva = nullptr, *occ_contrij = nullptr;
+  double* occ_contra = nullptr;  // device scalar
+  double* h_contra = nullptr;    // its page-locked mirror
   double* trotest_buf = nullptr;  // orctm_trotest's scratch, allocated on first use
   // replayed chunk of PCG iterations per precision and the variants it holds
   cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
@@ -415,6 +427,7 @@ int setup(orctm_handle* h, const orctm_desc* d) {
   h->tiestu[0] = 0.5 * d->dzw[0];
   for (int k = 2; k <= KE; ++k) h->tiestu[k - 1] = 0.5 * (h->tiestw[k] + h->tiestw[k - 1]);
   h->tiestu[KE] = 9000.;
+  h->dzw.assign(d->dzw, d->dzw + KE);
   Geo& G = h->G;
   G.L = L;
   G.dt = d->dt;
@@ -1318,6 +1331,7 @@ const char* orctm_status_string(int s) {
     case ORCTM_E_UNSUPPORTED: return "option outside the implemented path";
     case ORCTM_E_NODEVICE: return "no usable CUDA device";
     case ORCTM_E_TOO_LARGE: return "grid too large (2^31 elements per padded field, or the scratch-free entry point's limit)";
+    case ORCTM_E_UNSTABLE: return "OCCLIT's baroclinic iteration did not settle (CONTRA above 1e-3)";
     default: return "unknown status";
   }
 }
@@ -1350,6 +1364,7 @@ int orctm_destroy(orctm_handle* h) {
     if (h->pcg_graph[pr]) cudaGraphExecDestroy(h->pcg_graph[pr]);
   if (h->sor_graph) cudaGraphExecDestroy(h->sor_graph);
   if (h->hS) pinned_state_put(h->hS);
+  if (h->h_contra) cudaFreeHost(h->h_contra);
   for (int k = 0; k < ORCTM_PROF_KINDS; ++k)
     for (auto& pr : h->prof_pairs[k]) {
       h->ev_pool.push_back(pr.first);
@@ -1859,14 +1874,16 @@ int orctm_troneu(orctm_handle* h, const double* u1o, const double* v1e, const do
                  const double* vze) {
   ORCTM_ENTER(h);
   if (!h->baro_ready) return h->fail(ORCTM_E_ARG, "orctm_troneu: orctm_set_barotropic not called");
-  if (!u1o || !v1e || !uzo || !vze) return h->fail(ORCTM_E_ARG, "orctm_troneu: missing array");
+  const bool host = u1o || v1e || uzo || vze;
+  if (host && !(u1o && v1e && uzo && vze))
+    return h->fail(ORCTM_E_ARG, "orctm_troneu: give all four arrays or none");
   const int IE = h->L.ie, JE = h->L.je;
   int st;
   if ((st = compute_after_copies(h))) return st;
-  if ((st = upload_2d(h, h->bf.u1o, u1o, 0, IE + 1, 1, JE)) ||
-      (st = upload_2d(h, h->bf.uzo, uzo, 0, IE + 1, 1, JE)) ||
-      (st = upload_2d(h, h->bf.v1e, v1e, 1, IE, 0, JE + 1)) ||
-      (st = upload_2d(h, h->bf.vze, vze, 1, IE, 0, JE + 1)))
+  if (host && ((st = upload_2d(h, h->bf.u1o, u1o, 0, IE + 1, 1, JE)) ||
+               (st = upload_2d(h, h->bf.uzo, uzo, 0, IE + 1, 1, JE)) ||
+               (st = upload_2d(h, h->bf.v1e, v1e, 1, IE, 0, JE + 1)) ||
+               (st = upload_2d(h, h->bf.vze, vze, 1, IE, 0, JE + 1))))
     return st;
   ORCTM_CUDA_OK(cudaMemsetAsync(h->bf.z1o, 0, sizeof(double) * (size_t)h->L.plane, h->stream));
   launch_troneu_rhs(h->G, h->baro, h->bf, h->stream);
@@ -1990,8 +2007,11 @@ int orctm_ocbarp(orctm_handle* h) {
 int orctm_ocwind(orctm_handle* h, const double* txo, const double* tye, const double* sicomu,
                  const double* sicomv, const double* tauwatu, const double* tauwatv) {
   ORCTM_ENTER(h);
-  if (!txo || !tye || !sicomu || !sicomv || !tauwatu || !tauwatv)
-    return h->fail(ORCTM_E_ARG, "orctm_ocwind: missing array");
+  const bool host = txo || tye || sicomu || sicomv || tauwatu || tauwatv;
+  if (host && !(txo && tye && sicomu && sicomv && tauwatu && tauwatv))
+    return h->fail(ORCTM_E_ARG, "orctm_ocwind: give all six arrays or none");
+  if (!host && !h->wind_ready)
+    return h->fail(ORCTM_E_ARG, "orctm_ocwind: no forcing given yet");
   const int IE = h->L.ie, JE = h->L.je;
   int st;
   if (!h->wind.txo) {
@@ -2000,15 +2020,18 @@ int orctm_ocwind(orctm_handle* h, const double* txo, const double* tye, const do
     for (double** p : all)
       if ((st = h->dev_alloc(p, (size_t)h->L.plane))) return st;
   }
-  // the forcing of the previous call may still be read by queued launches
-  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
-  if ((st = upload_2d(h, h->wind.txo, txo, 0, IE + 1, 1, JE)) ||
-      (st = upload_2d(h, h->wind.tye, tye, 1, IE, 0, JE + 1)) ||
-      (st = upload_2d(h, h->wind.sicomu, sicomu, 1, IE, 1, JE)) ||
-      (st = upload_2d(h, h->wind.sicomv, sicomv, 1, IE, 1, JE)) ||
-      (st = upload_2d(h, h->wind.tauwatu, tauwatu, 1, IE, 1, JE)) ||
-      (st = upload_2d(h, h->wind.tauwatv, tauwatv, 1, IE, 1, JE)))
-    return st;
+  if (host) {
+    // the forcing of the previous call may still be read by queued launches
+    ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+    if ((st = upload_2d(h, h->wind.txo, txo, 0, IE + 1, 1, JE)) ||
+        (st = upload_2d(h, h->wind.tye, tye, 1, IE, 0, JE + 1)) ||
+        (st = upload_2d(h, h->wind.sicomu, sicomu, 1, IE, 1, JE)) ||
+        (st = upload_2d(h, h->wind.sicomv, sicomv, 1, IE, 1, JE)) ||
+        (st = upload_2d(h, h->wind.tauwatu, tauwatu, 1, IE, 1, JE)) ||
+        (st = upload_2d(h, h->wind.tauwatv, tauwatv, 1, IE, 1, JE)))
+      return st;
+    h->wind_ready = true;
+  }
   // UOO and VOE are updated in place (level 1)
   if ((st = wait_uploads(h, {ORCTM_F_UOO, ORCTM_F_VOE})) || (st = own_buffer(h, ORCTM_F_UOO)) ||
       (st = own_buffer(h, ORCTM_F_VOE)))
@@ -2054,12 +2077,320 @@ int orctm_download_barotropic(orctm_handle* h, int which, double* host, size_t n
     case ORCTM_B_UZO: src = h->bf.uzo; i0 = 0; ni = IE + 1; break;
     case ORCTM_B_VSE: src = h->bf.vse; j0 = 0; nj = JE + 1; break;
     case ORCTM_B_VZE: src = h->bf.vze; j0 = 0; nj = JE + 1; break;
+    case ORCTM_B_U1O: src = h->bf.u1o; i0 = 0; ni = IE + 1; break;
+    case ORCTM_B_V1E: src = h->bf.v1e; j0 = 0; nj = JE + 1; break;
     default: return h->fail(ORCTM_E_ARG, "orctm_download_barotropic: unknown field");
   }
   if (!host || n != (size_t)ni * nj) return h->fail(ORCTM_E_ARG, "orctm_download_barotropic: size");
   ORCTM_CUDA_OK(cudaMemcpy2DAsync(host, sizeof(double) * ni, src + h->L.at2(i0, j0),
                                   sizeof(double) * h->L.P, sizeof(double) * ni, nj,
                                   cudaMemcpyDeviceToHost, h->stream));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return ORCTM_OK;
+}
+
+// ------------------------------------------- OCTHER, OCMODMOM, OCCLIT
+int orctm_set_thermo(orctm_handle* h, const orctm_thermo* t) {
+  ORCTM_ENTER(h);
+  if (!t || !t->dbackv || !t->abackv)
+    return h->fail(ORCTM_E_ARG, "orctm_set_thermo: missing DBACKV or ABACKV");
+  if (t->eos != ORCTM_EOS_UNESCO && t->eos != ORCTM_EOS_LINEAR)
+    return h->fail(ORCTM_E_ARG, "orctm_set_thermo: unknown equation of state");
+  if (!(t->grav > 0.0)) return h->fail(ORCTM_E_ARG, "orctm_set_thermo: G must be positive");
+  const int IE = h->L.ie, JE = h->L.je, KE = h->L.ke;
+  const size_t n2 = (size_t)h->L.plane;
+  int st;
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
+  ThermoFields& f = h->tf;
+  if (!f.po) {
+    double *preff, *dbackv, *abackv, *wtd, *tiu, *tiw, *dz;
+    if ((st = h->dev_alloc(&preff, KE)) || (st = h->dev_alloc(&dbackv, KE + 1)) ||
+        (st = h->dev_alloc(&abackv, KE + 1)) || (st = h->dev_alloc(&wtd, KE)) ||
+        (st = h->dev_alloc(&tiu, KE + 1)) || (st = h->dev_alloc(&tiw, KE + 1)) ||
+        (st = h->dev_alloc(&dz, KE + 1)))
+      return st;
+    f.preff = preff; f.dbackv = dbackv; f.abackv = abackv; f.wtdecay = wtd;
+    f.tiestu = tiu; f.tiestw = tiw; f.dz = dz;
+    double* d2[10];
+    for (double*& p : d2)
+      if ((st = h->dev_alloc(&p, n2))) return st;
+    f.sicomo = d2[0]; f.sictho = d2[1]; f.sicsno = d2[2]; f.relsao = d2[3]; f.reltho = d2[4];
+    f.giriv = d2[5]; f.fu10 = d2[6]; f.eminpo = d2[7]; f.rivrun = d2[8]; f.kcondep = d2[9];
+    const size_t n3 = (size_t)h->L.n3();
+    if ((st = h->dev_alloc(&f.po, n3)) || (st = h->dev_alloc(&f.stabio, n3)) ||
+        (st = h->dev_alloc(&f.rhoo, n3)) || (st = h->dev_alloc(&h->uk1o, n3)) ||
+        (st = h->dev_alloc(&h->vk1e, n3)))
+      return st;
+    ORCTM_CUDA_OK(cudaHostAlloc((void**)&h->h_contra, sizeof(double), cudaHostAllocDefault));
+  } else {
+    // the tables of the previous call may still be read by queued launches
+    ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  }
+  // vertical tables: PREFF (0.1026 TIESTU unless given), DBACKV, ABACKV, the
+  // wind-mixing decay EXP(-DZW(K)/WPENDEP) with WPENDEP = 40 (octher.f90:321,
+  // 349), TIESTU, TIESTW and DZ (beleg.f90:87-105)
+  std::vector<double> preff(KE), wtd(KE), dz(KE + 1);
+  for (int k = 0; k < KE; ++k) preff[k] = t->preff ? t->preff[k] : 0.1026 * h->tiestu[k];
+  for (int k = 0; k < KE; ++k) wtd[k] = std::exp(-h->dzw[k] / 40.);
+  dz[0] = h->tiestu[0];
+  for (int k = 1; k <= KE; ++k) dz[k] = h->tiestu[k] - h->tiestu[k - 1];
+  auto up1 = [&](const double* dst, const double* src, int n) {
+    return cudaMemcpyAsync((void*)dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+  };
+  ORCTM_CUDA_OK(up1(f.preff, preff.data(), KE));
+  ORCTM_CUDA_OK(up1(f.dbackv, t->dbackv, KE + 1));
+  ORCTM_CUDA_OK(up1(f.abackv, t->abackv, KE + 1));
+  ORCTM_CUDA_OK(up1(f.wtdecay, wtd.data(), KE));
+  ORCTM_CUDA_OK(up1(f.tiestu, h->tiestu.data(), KE + 1));
+  ORCTM_CUDA_OK(up1(f.tiestw, h->tiestw.data(), KE + 1));
+  ORCTM_CUDA_OK(up1(f.dz, dz.data(), KE + 1));
+  const double* src2[7] = {t->sicomo, t->sictho, t->sicsno, t->relsao, t->reltho, t->giriv, t->fu10};
+  const double* dst2[7] = {f.sicomo, f.sictho, f.sicsno, f.relsao, f.reltho, f.giriv, f.fu10};
+  for (int q = 0; q < 7; ++q) {
+    if (src2[q]) {
+      if ((st = upload_2d(h, (double*)dst2[q], src2[q], 1, IE, 1, JE))) return st;
+    } else {
+      ORCTM_CUDA_OK(cudaMemsetAsync((void*)dst2[q], 0, sizeof(double) * n2, h->stream));
+    }
+  }
+  if (!h->thermo_ready) {  // KCONDEP as BODEN sets it (boden.f90:261): 1 wet, -99 land
+    std::vector<double> kc((size_t)IE * JE);
+    std::vector<int> kb((size_t)n2);
+    ORCTM_CUDA_OK(cudaMemcpyAsync(kb.data(), h->G.gp.kb, sizeof(int) * n2, cudaMemcpyDeviceToHost,
+                                  h->stream));
+    ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+    for (int j = 1; j <= JE; ++j)
+      for (int i = 1; i <= IE; ++i)
+        kc[(size_t)(j - 1) * IE + (i - 1)] = kb[(size_t)h->L.at2(i, j)] >= 1 ? 1.0 : -99.0;
+    if ((st = upload_2d(h, f.kcondep, kc.data(), 1, IE, 1, JE))) return st;
+  }
+  h->th = ThermoArgs{t->eos, t->rho0, t->drdt, t->drds, t->t0, t->s0, t->grav, t->relsal, t->reltem,
+                     t->rhoicwa, t->rhosnwa, t->wt, t->cstabeps, t->dv0, t->av0, t->cavocon,
+                     t->cdvocon};
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
+  h->thermo_ready = true;
+  return ORCTM_OK;
+}
+
+int orctm_set_coriolis(orctm_handle* h, const orctm_coriolis* c) {
+  ORCTM_ENTER(h);
+  if (!c || !c->ftwou || !c->ftwov || !c->gila || !c->giph)
+    return h->fail(ORCTM_E_ARG, "orctm_set_coriolis: missing array");
+  const int IE = h->L.ie, JE = h->L.je;
+  const size_t n2 = (size_t)h->L.plane;
+  int st;
+  if (!h->cf.dtfu) {
+    double* p[10];
+    for (double*& q : p)
+      if ((st = h->dev_alloc(&q, n2))) return st;
+    h->cf = CorFields{p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8], p[9]};
+  } else {
+    ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  }
+  // ocmodmom.f90:103-164 on the host (COS and SQRT of the host's library)
+  const double dt = h->G.dt, almzer = h->G.almzer, omega = c->omega;
+  auto gi = [&](const double* a, int ii, int jj) { return a[(size_t)(jj - 1) * (2 * IE) + (ii - 1)]; };
+  std::vector<std::vector<double>> t(10, std::vector<double>(n2, 0.0));
+  for (int j = 1; j <= JE; ++j)
+    for (int i = 0; i <= IE; ++i) {
+      const size_t ij = (size_t)h->L.at2(i, j);
+      t[0][ij] = dt * c->ftwou[(size_t)(j - 1) * (IE + 1) + i];
+      if (j >= 2 && j <= JE - 1 && i >= 1 && i <= IE - 1) {
+        const double dlon = (gi(c->gila, 2 * i + 2, 2 * j) - gi(c->gila, 2 * i + 1, 2 * j)) *
+                            std::cos(gi(c->gila, 2 * i + 1, 2 * j));
+        const double dlat = gi(c->giph, 2 * i + 2, 2 * j) - gi(c->giph, 2 * i + 1, 2 * j);
+        t[1][ij] = dt * (2 * omega * std::cos(gi(c->giph, 2 * i + 1, 2 * j)));
+        t[2][ij] = dlon;
+        t[3][ij] = std::sqrt(dlon * dlon + dlat * dlat) + almzer;
+      }
+    }
+  for (int j = 0; j <= JE; ++j)
+    for (int i = 1; i <= IE; ++i) {
+      const size_t ij = (size_t)h->L.at2(i, j);
+      t[4][ij] = dt * c->ftwov[(size_t)j * IE + (i - 1)];
+      if (j >= 1 && j <= JE - 1 && i >= 2 && i <= IE - 1) {
+        const double dlon = (gi(c->gila, 2 * i, 2 * j) - gi(c->gila, 2 * i, 2 * j + 1)) *
+                            std::cos(gi(c->gila, 2 * i, 2 * j + 1));
+        const double dlat = gi(c->giph, 2 * i, 2 * j) - gi(c->giph, 2 * i, 2 * j + 1);
+        t[5][ij] = dt * (2 * omega * std::cos(gi(c->giph, 2 * i, 2 * j + 1)));
+        t[6][ij] = dlon;
+        t[7][ij] = std::sqrt(dlon * dlon + dlat * dlat) + almzer;
+      }
+    }
+  for (int j = 2; j <= JE - 1; ++j)
+    for (int i = 2; i <= IE - 1; ++i) {
+      const size_t ij = (size_t)h->L.at2(i, j);
+      const double dlon = (gi(c->gila, 2 * i + 1, 2 * j) - gi(c->gila, 2 * i, 2 * j)) *
+                          std::cos(gi(c->gila, 2 * i, 2 * j));
+      const double dlat = gi(c->giph, 2 * i, 2 * j - 1) - gi(c->giph, 2 * i, 2 * j);
+      const double dist = std::sqrt(dlon * dlon + dlat * dlat) + almzer;
+      const double ftwow1 = 2 * omega * std::cos(gi(c->giph, 2 * i, 2 * j));
+      t[8][ij] = ftwow1 * dlon / dist;
+      t[9][ij] = ftwow1 * dlat / dist;
+    }
+  const double* dst[10] = {h->cf.dtfu, h->cf.cu, h->cf.dlonu, h->cf.distu, h->cf.dtfv,
+                           h->cf.cv,   h->cf.dlonv, h->cf.distv, h->cf.aw, h->cf.bw};
+  for (int q = 0; q < 10; ++q)
+    ORCTM_CUDA_OK(cudaMemcpyAsync((void*)dst[q], t[q].data(), sizeof(double) * n2,
+                                  cudaMemcpyHostToDevice, h->stream));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  h->cor_ready = true;
+  return ORCTM_OK;
+}
+
+namespace {
+int r_octher(orctm_handle* h) {
+  int st;
+  const int ft = ORCTM_F_THO, fs = ORCTM_F_THO + 1;
+  if ((st = wait_uploads(h, {ft, fs, ORCTM_F_ZO, ORCTM_F_UKO, ORCTM_F_VKE, ORCTM_F_AVO, ORCTM_F_DVO})) ||
+      (st = compute_after_copies(h)) || (st = own_buffer(h, ft)) || (st = own_buffer(h, fs)) ||
+      (st = own_buffer(h, ORCTM_F_AVO)) || (st = own_buffer(h, ORCTM_F_DVO)))
+    return st;
+  launch_octher_surface(h->G, h->th, h->tf, h->slot[ft], h->slot[fs], h->zo, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  // B: the T/S boundary forcing (octher.f90:113-121)
+  for (int n = 0; n < 2; ++n) {
+    if (!h->obc_ts_ready[n]) continue;
+    launch_obc_ts(h->G, h->obc_ts[n], h->slot[ORCTM_F_THO + n], h->stream);
+    ORCTM_CUDA_OK(cudaGetLastError());
+  }
+  launch_octher_column(h->G, h->th, h->tf, h->slot[ft], h->slot[fs], h->zo, h->slot[ORCTM_F_UKO],
+                       h->slot[ORCTM_F_VKE], h->slot[ORCTM_F_AVO], h->slot[ORCTM_F_DVO], h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+int r_ocmodmom(orctm_handle* h) {
+  int st;
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
+  if ((st = compute_after_copies(h)) || (st = own_buffer(h, ORCTM_F_UKO)) ||
+      (st = own_buffer(h, ORCTM_F_VKE)) || (st = own_buffer(h, ORCTM_F_WNO)))
+    return st;
+  double *ub, *vb, *wb;
+  if ((st = h->alloc(&ub)) || (st = h->alloc(&vb)) || (st = h->alloc(&wb))) return st;
+  launch_ocmodmom(h->G, h->baro, h->tf, h->cf, h->bf, h->zo, h->slot[ORCTM_F_UOO],
+                  h->slot[ORCTM_F_VOE], h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], h->uk1o,
+                  h->vk1e, h->slot[ORCTM_F_WNO], ub, vb, wb, h->stream);
+  const cudaError_t e = cudaGetLastError();
+  h->unref(ub);  // stream-ordered: a later user of the buffer runs after these launches
+  h->unref(vb);
+  h->unref(wb);
+  ORCTM_CUDA_OK(e);
+  return ORCTM_OK;
+}
+
+int r_occlit(orctm_handle* h) {
+  int st;
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
+  if ((st = compute_after_copies(h)) || (st = own_buffer(h, ORCTM_F_UKO)) ||
+      (st = own_buffer(h, ORCTM_F_VKE)) || (st = own_buffer(h, ORCTM_F_WO)))
+    return st;
+  if (!h->occ_wpo) {
+    const size_t n3 = (size_t)h->L.n3(), n2 = (size_t)h->L.plane;
+    if ((st = h->dev_alloc(&h->occ_wpo, n3)) || (st = h->dev_alloc(&h->occ_t1o, n3)) ||
+        (st = h->dev_alloc(&h->occ_bruva, n2)) || (st = h->dev_alloc(&h->occ_contrij, n2)) ||
+        (st = h->dev_alloc(&h->occ_contra, 1)))
+      return st;
+  }
+  launch_occlit(h->G, h->baro, h->tf, h->bf, h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], h->uk1o,
+                h->vk1e, h->slot[ORCTM_F_WO], h->occ_wpo, h->occ_t1o, h->occ_bruva,
+                h->occ_contrij, h->occ_contra, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  ORCTM_CUDA_OK(cudaMemcpyAsync(h->h_contra, h->occ_contra, sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream));
+  return ORCTM_OK;
+}
+
+// OCCLIT's check (occlit.f90:321-326), once the copy of CONTRA has landed
+int contra_status(orctm_handle* h, double* contra) {
+  const double c = *h->h_contra;
+  if (contra) *contra = c;
+  if (!(c <= 1.E-3)) return h->fail(ORCTM_E_UNSTABLE, "OCCLIT: CONTRA above 1e-3 (the reference aborts)");
+  return ORCTM_OK;
+}
+}  // namespace
+
+int orctm_octher(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  if (!h->thermo_ready) return h->fail(ORCTM_E_ARG, "orctm_octher: orctm_set_thermo not called");
+  return r_octher(h);
+}
+
+int orctm_ocmodmom(orctm_handle* h) {
+  ORCTM_ENTER(h);
+  if (!h->thermo_ready || !h->cor_ready || !h->baro_ready)
+    return h->fail(ORCTM_E_ARG,
+                   "orctm_ocmodmom: needs orctm_set_thermo, orctm_set_coriolis and orctm_set_barotropic");
+  return r_ocmodmom(h);
+}
+
+int orctm_occlit(orctm_handle* h, double* contra) {
+  ORCTM_ENTER(h);
+  if (!h->thermo_ready || !h->baro_ready)
+    return h->fail(ORCTM_E_ARG, "orctm_occlit: needs orctm_set_thermo and orctm_set_barotropic");
+  int st;
+  if ((st = r_occlit(h))) return st;
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return contra_status(h, contra);
+}
+
+namespace {
+// the baroclinic state arrays: device buffer, staggering and levels
+int baroclinic_array(orctm_handle* h, int which, double** p, int* i0, int* ni, int* j0, int* nj,
+                     int* nk) {
+  const int IE = h->L.ie, JE = h->L.je, KE = h->L.ke;
+  *i0 = 1; *ni = IE; *j0 = 1; *nj = JE; *nk = KE;
+  switch (which) {
+    case ORCTM_C_PO: *p = h->tf.po; break;
+    case ORCTM_C_STABIO: *p = h->tf.stabio; break;
+    case ORCTM_C_RHOO: *p = h->tf.rhoo; break;
+    case ORCTM_C_UK1O: *p = h->uk1o; *i0 = 0; *ni = IE + 1; break;
+    case ORCTM_C_VK1E: *p = h->vk1e; *j0 = 0; *nj = JE + 1; break;
+    case ORCTM_C_EMINPO: *p = h->tf.eminpo; *nk = 1; break;
+    case ORCTM_C_RIVRUN: *p = h->tf.rivrun; *nk = 1; break;
+    case ORCTM_C_KCONDEP: *p = h->tf.kcondep; *nk = 1; break;
+    default: return h->fail(ORCTM_E_ARG, "unknown baroclinic array");
+  }
+  return ORCTM_OK;
+}
+}  // namespace
+
+int orctm_upload_baroclinic(orctm_handle* h, int which, const double* host, size_t n) {
+  ORCTM_ENTER(h);
+  if (!h->thermo_ready) return h->fail(ORCTM_E_ARG, "orctm_upload_baroclinic: orctm_set_thermo not called");
+  double* p;
+  int i0, ni, j0, nj, nk, st;
+  if ((st = baroclinic_array(h, which, &p, &i0, &ni, &j0, &nj, &nk))) return st;
+  if (!host || n != (size_t)ni * nj * nk) return h->fail(ORCTM_E_ARG, "orctm_upload_baroclinic: size");
+  if ((st = compute_after_copies(h))) return st;
+  for (int k = 0; k < nk; ++k)
+    ORCTM_CUDA_OK(cudaMemcpy2DAsync(p + h->L.at(i0, j0, k), sizeof(double) * h->L.P,
+                                    host + (size_t)k * ni * nj, sizeof(double) * ni,
+                                    sizeof(double) * ni, nj, cudaMemcpyHostToDevice, h->stream));
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  return ORCTM_OK;
+}
+
+int orctm_download_baroclinic(orctm_handle* h, int which, double* host, size_t n) {
+  ORCTM_ENTER(h);
+  if (!h->thermo_ready) return h->fail(ORCTM_E_ARG, "orctm_download_baroclinic: orctm_set_thermo not called");
+  double* p;
+  int i0, ni, j0, nj, nk, st;
+  if ((st = baroclinic_array(h, which, &p, &i0, &ni, &j0, &nj, &nk))) return st;
+  if (!host || n != (size_t)ni * nj * nk) return h->fail(ORCTM_E_ARG, "orctm_download_baroclinic: size");
+  for (int k = 0; k < nk; ++k)
+    ORCTM_CUDA_OK(cudaMemcpy2DAsync(host + (size_t)k * ni * nj, sizeof(double) * ni,
+                                    p + h->L.at(i0, j0, k), sizeof(double) * h->L.P,
+                                    sizeof(double) * ni, nj, cudaMemcpyDeviceToHost, h->stream));
   ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
   return ORCTM_OK;
 }
@@ -2079,6 +2410,40 @@ int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* s) {
   r_octimf(h);
   if ((st = step_outputs(h, false))) return st;
   return ns;
+}
+
+// One whole time step in the reference driver's order (orctm.f90:1327-1562):
+// OCTHER, OCWIND, the open-boundary forcing, OCTIMF, OCMODMOM, OCBARP,
+// OCCLIT, TRONEU, OCVTRO, OCVTOT, the STABIO rescaling, then the hot path.
+// Nothing crosses to the host but the solve's scalars and OCCLIT's CONTRA.
+int orctm_step_full(orctm_handle* h, int ldtrun, orctm_solve_stats* s, double* contra) {
+  ORCTM_ENTER(h);
+  if (!h->thermo_ready || !h->cor_ready || !h->baro_ready)
+    return h->fail(ORCTM_E_ARG,
+                   "orctm_step_full: needs orctm_set_thermo, orctm_set_coriolis and orctm_set_barotropic");
+  int st;
+  if ((st = r_octher(h))) return st;
+  if (h->wind_ready && (st = orctm_ocwind(h, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr)))
+    return st;
+  if (h->obc_ready) {
+    if (h->baro.eta_forc && (st = orctm_obc_eta(h, ldtrun))) return st;
+    if ((st = orctm_obc_uv(h, ldtrun))) return st;
+  }
+  if ((st = r_octimf(h)) || (st = r_ocmodmom(h)) || (st = orctm_ocbarp(h)) || (st = r_occlit(h)))
+    return st;
+  cudaEvent_t contra_done = h->get_event();
+  ORCTM_CUDA_OK(cudaEventRecord(contra_done, h->stream));
+  if ((st = orctm_troneu(h, nullptr, nullptr, nullptr, nullptr)) || (st = orctm_ocvtro(h)) ||
+      (st = orctm_ocvtot(h)))
+    return st;
+  launch_stabio_rescale(h->G, h->tf, h->stream);
+  ORCTM_CUDA_OK(cudaGetLastError());
+  const int ns = orctm_step_hotpath(h, s);
+  if (ns != ORCTM_OK && ns != ORCTM_E_NOT_CONVERGED) return ns;
+  ORCTM_CUDA_OK(cudaEventSynchronize(contra_done));  // long done: the solve waited on the host
+  h->ev_pool.push_back(contra_done);
+  const int cs = contra_status(h, contra);
+  return ns != ORCTM_OK ? ns : cs;
 }
 
 int orctm_set_solver(orctm_handle* h, int mode, double rtol, int maxit) {

@@ -79,6 +79,46 @@ void launch_ocvtot(const Geo& G, const BaroArgs& a, const double* uso, const dou
                    double* uoo_o, double* voe_o, double* uko_o, double* vke_o, double* wo_o,
                    cudaStream_t st);
 
+// baroclinic.cu: OCTHER, OCMODMOM, OCCLIT
+struct ThermoArgs {
+  int eos;  // 0 ADISITJ + RHO1J, 1 linear
+  double rho0, drdt, drds, t0, s0;
+  double grav, relsal, reltem, rhoicwa, rhosnwa, wt, cstabeps, dv0, av0, cavocon, cdvocon;
+};
+struct ThermoFields {
+  // 1D (device): PREFF[KE], DBACKV / ABACKV [KE+1], WTDECAY[KE] (exp(-DZW/40)
+  // from the host's exp), TIESTU / TIESTW / DZ [KE+1]
+  const double *preff, *dbackv, *abackv, *wtdecay, *tiestu, *tiestw, *dz;
+  // 2D surface forcing (padded plane; zero where the caller gave none)
+  const double *sicomo, *sictho, *sicsno, *relsao, *reltho, *giriv, *fu10;
+  double *eminpo, *rivrun, *kcondep;  // 2D outputs (KCONDEP as integral doubles)
+  double *po, *stabio, *rhoo;         // 3D p-points
+};
+// Coriolis factors of OCMODMOM per point, formed on the host with its own
+// cos/sqrt exactly as the reference writes them (ocmodmom.f90:103-164):
+//   u: dtfu = DT FTWOU, cu = DT FTWOU1, dlonu, distu
+//   v: dtfv = DT FTWOV, cv = DT FTWOV1, dlonv, distv
+//   w: aw = FTWOW1 dlon / dist, bw = FTWOW1 dlat / dist
+struct CorFields {
+  const double *dtfu, *cu, *dlonu, *distu, *dtfv, *cv, *dlonv, *distv, *aw, *bw;
+};
+void launch_octher_surface(const Geo& G, const ThermoArgs& a, const ThermoFields& f, double* tho,
+                           double* sao, double* zo, cudaStream_t st);
+void launch_octher_column(const Geo& G, const ThermoArgs& a, const ThermoFields& f, double* tho,
+                          double* sao, const double* zo, const double* uko, const double* vke,
+                          double* avo, double* dvo, cudaStream_t st);
+// STABIO *= (1000 / DZ): orctm.f90:1443-1449, after OCVTOT
+void launch_stabio_rescale(const Geo& G, const ThermoFields& f, cudaStream_t st);
+void launch_ocmodmom(const Geo& G, const BaroArgs& b, const ThermoFields& f, const CorFields& c,
+                     const BaroFields& bf, const double* zo, const double* uoo, const double* voe,
+                     double* uko, double* vke, double* uk1o, double* vk1e, double* wno,
+                     double* ub, double* vb, double* wb, cudaStream_t st);
+// OCCLIT; scratch: wpo, t1o (3D), bruva, contrij (2D); *contra receives the
+// sum of CONTRIJ (device scalar)
+void launch_occlit(const Geo& G, const BaroArgs& b, const ThermoFields& f, const BaroFields& bf,
+                   double* uko, double* vke, double* uk1o, double* vk1e, double* wo, double* wpo,
+                   double* t1o, double* bruva, double* contrij, double* contra, cudaStream_t st);
+
 // advect.cu
 void launch_ocadpo(const Geo& G, const double* T, const double* uko, const double* vke,
                    const double* wo, const double* zo, double* out, double* tA, double* vA,

@@ -6,6 +6,8 @@ compute_matrix (mo_petsc.f90:543-782).  Test infrastructure only.
 Arrays are 0-based numpy views of the Fortran arrays: p-point index
 i-1 <-> Fortran I, u-point index i <-> Fortran I (I_start = 0).
 """
+import math
+
 import numpy as np
 import scipy.sparse as sp
 
@@ -1166,3 +1168,366 @@ def trotest(g, b, xx, uf, vf, ff, ntry=200, niter=200):
         if contric < convmin:
             sorpmin, convmin = sorpar, contric
     return sorpmin
+
+
+# --------------------------------------------------------------- OCTHER ---
+# Written from octher.f90, adisitj.f90 and rho1j.f90 as the reference is
+# built (EISREST, REDWMICE, NURDIF); vectorised over (i, j).
+def adisit(th, sh, pa):
+    a1, a2, a3, a4 = 3.6504E-4, 8.3198E-5, 5.4065E-7, 4.0274E-9
+    b1, b2, c1, c2 = 1.7439E-5, 2.9778E-7, 8.9309E-7, 3.1628E-8
+    c3, d, e1, e2 = 2.1987E-10, 4.1057E-9, 1.6056E-10, 5.0484E-12
+    pr = pa
+    qc = pr * (a1 + pr * (c1 - e1 * pr))
+    qv = pr * (b1 - d * pr)
+    dc = 1. + pr * (-a2 + pr * (c2 - e2 * pr))
+    dv = b2 * pr
+    qnq = -pr * (-a3 + pr * c3)
+    qn3 = -pr * a4
+    qvs = qv * (sh - 35.) + qc
+    dvs = dv * (sh - 35.) + dc
+    tpo = th
+    th = (th + qvs) / dvs
+    t = th
+    fne = -qvs + t * (dvs + t * (qnq + t * qn3)) - tpo
+    fst = dvs + t * (2 * qnq + 3 * qn3 * t)
+    return th - fne / fst
+
+
+def rho1(t, s, p):
+    B = (8.24493E-1, -4.0899E-3, 7.6438E-5, -8.2467E-7, 5.3875E-9)
+    Cc = (-5.72466E-3, 1.0227E-4, -1.6546E-6)
+    d0 = 4.8314E-4
+    A = (999.8426, 6.793952E-2, -9.095290E-3, 1.001685E-4, -1.120083E-6, 6.536332E-9)
+    F = (54.6746, -0.603459, 1.09987E-2, -6.1670E-5)
+    Gg = (7.944E-2, 1.6483E-2, -5.3009E-4)
+    AI = (2.2838E-3, -1.0981E-5, -1.6078E-6)
+    aj0 = 1.91075E-4
+    AM = (-9.9348E-7, 2.0816E-8, 9.1697E-10)
+    E = (19652.21, 148.4206, -2.327105, 1.360477E-2, -5.155288E-5)
+    H = (3.239908, 1.43713E-3, 1.16092E-4, -5.77905E-7)
+    AK = (8.50935E-5, -6.12293E-6, 5.2787E-8)
+    s = np.where(s > 28., s, 28.)
+    s3h = np.sqrt(s * s * s)
+    num = (A[0] + t * (A[1] + t * (A[2] + t * (A[3] + t * (A[4] + t * A[5]))))
+           + s * (B[0] + t * (B[1] + t * (B[2] + t * (B[3] + t * B[4])))) + d0 * (s * s)
+           + s3h * (Cc[0] + t * (Cc[1] + Cc[2] * t)))
+    kk = (p * (H[0] + t * (H[1] + t * (H[2] + t * H[3])) + s * (AI[0] + t * (AI[1] + AI[2] * t))
+               + aj0 * s3h + (AK[0] + t * (AK[1] + t * AK[2]) + s * (AM[0] + t * (AM[1] + t * AM[2]))) * p)
+          + E[0] + t * (E[1] + t * (E[2] + t * (E[3] + t * E[4])))
+          + s * (F[0] + t * (F[1] + t * (F[2] + t * F[3]))) + s3h * (Gg[0] + t * (Gg[1] + Gg[2] * t)))
+    return num / (1. - p / kk)
+
+
+def density(th_, t, s, p):
+    if th_["eos"] == 1:
+        return th_["rho0"] + th_["drdt"] * (t - th_["t0"]) + th_["drds"] * (s - th_["s0"])
+    return rho1(adisit(t, s, p), s, p)
+
+
+def _z2(th_, k, shape):
+    a = th_.get(k)
+    return np.zeros(shape) if a is None else np.asarray(a, dtype=np.float64)
+
+
+def octher_surface(g, th_, tho, sao, zo):
+    """octher.f90:43-107 in place on tho, sao, zo; returns (eminpo, rivrun)."""
+    shp = zo.shape
+    dt = g["dt"]
+    sicomo, sictho, sicsno = (_z2(th_, k, shp) for k in ("sicomo", "sictho", "sicsno"))
+    relsao, reltho, giriv = (_z2(th_, k, shp) for k in ("relsao", "reltho", "giriv"))
+    reiscon = 1. - sicomo
+    oldso = sao[:, :, 0].copy()
+    sao[:, :, 0] = sao[:, :, 0] + dt * th_["relsal"] * reiscon * (relsao - sao[:, :, 0])
+    tho[:, :, 0] = tho[:, :, 0] + dt * th_["reltem"] * (reltho - tho[:, :, 0])
+    ddpo1 = g["ddpo"][:, :, 0]
+    eminpo = ((ddpo1 + zo - sictho * th_["rhoicwa"] - sicsno * th_["rhosnwa"])
+              * (np.where(oldso > 1.E-3, oldso, 1.E-3) / np.where(sao[:, :, 0] > 1.E-3, sao[:, :, 0], 1.E-3) - 1.))
+    zo[:] = (zo + eminpo) * g["weto"][:, :, 0]
+    eminpo = eminpo * (1. / dt)
+    z = ddpo1 + zo - sictho * th_["rhoicwa"] - sicsno * th_["rhosnwa"]
+    zzzdz = np.where(g["almzer"] > z, g["almzer"], z)
+    driv = giriv * dt
+    sao[:, :, 0] = sao[:, :, 0] * zzzdz / (zzzdz + driv)
+    zo[:] = zo + driv
+    return eminpo, driv / dt
+
+
+def octher_column(g, th_, tho, sao, zo, uko, vke, avo, dvo, kcondep):
+    """octher.f90:139-451 in place on tho, sao, avo, dvo, kcondep; returns
+    (po, stabio, rhoo)."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    shp = (ie, je)
+    G = th_["grav"]
+    preff, dz, di, dzw = th_["preff"], g["dz"], g["di"], g["dzw"]
+    weto, ddpo = g["weto"], g["ddpo"]
+    sicomo, sictho, sicsno, fu10 = (_z2(th_, k, shp) for k in ("sicomo", "sictho", "sicsno", "fu10"))
+    po = np.zeros((ie, je, ke), order="F")
+    stab = np.zeros((ie, je, ke), order="F")
+    rhoo = np.zeros((ie, je, ke), order="F")
+    rh = density(th_, tho[:, :, 0], sao[:, :, 0], preff[0])
+    po[:, :, 0] = G * g["tiestu"][0] * 0.00097 * rh
+    for k in range(1, ke):                      # Fortran K = k + 1
+        disti = 1. / dz[k]
+        rh = density(th_, tho[:, :, k], sao[:, :, k], preff[k])
+        rup = density(th_, tho[:, :, k - 1], sao[:, :, k - 1], preff[k])
+        stab[:, :, k] = disti * (rh - rup)
+        po[:, :, k] = po[:, :, k - 1] + G * dz[k] * 0.00049 * (rh + rup)
+        zs = 1. if k == 1 else 0.
+        surf = zs * (zo - sictho * th_["rhoicwa"] - sicsno * th_["rhosnwa"])
+        den = ddpo[:, :, k] + ddpo[:, :, k - 1] + surf + (1. - weto[:, :, k])
+        tq = ((ddpo[:, :, k - 1] + surf) * tho[:, :, k - 1] + ddpo[:, :, k] * tho[:, :, k]) / den
+        sq = ((ddpo[:, :, k - 1] + surf) * sao[:, :, k - 1] + ddpo[:, :, k] * sao[:, :, k]) / den
+        st = stab[:, :, k]
+        q = -st / (1.E-11 + np.abs(st))
+        switc = np.where(0. > q, 0., q) * weto[:, :, k]
+        helpswi = switc
+        sw = 0.
+        tho[:, :, k - 1] = tq * sw + (1. - sw) * tho[:, :, k - 1]
+        tho[:, :, k] = tq * sw + (1. - sw) * tho[:, :, k]
+        sao[:, :, k - 1] = sq * sw + (1. - sw) * sao[:, :, k - 1]
+        sao[:, :, k] = sq * sw + (1. - sw) * sao[:, :, k]
+        st = (1. - sw) * st
+        stab[:, :, k] = np.where(st > 0., st, 0.)
+        kcondep += ((kcondep == k) & (helpswi >= 0.5)).astype(kcondep.dtype)
+    # D on I = 1..IE-1, J = 1..JE-1 (0-based p index 0..IE-2)
+    relne = 0.4
+    relax = 1. - relne
+    gor = G / 1025.
+    P = (slice(0, ie - 1), slice(0, je - 1))
+    Uw, Ue = (slice(0, ie - 1), slice(0, je - 1)), (slice(1, ie), slice(0, je - 1))
+    Vs, Vn = (slice(0, ie - 1), slice(0, je - 1)), (slice(0, ie - 1), slice(1, je))
+    ice = 1. - sicomo[P]
+    f = fu10[P]
+    t1 = th_["wt"] * (ice * ice) * (f * f * f)
+    s1 = th_["wt"] * (ice * ice) * (f * f * f)
+    amsuo, amsue = g["amsuo"], g["amsue"]
+    for k in range(1, ke):
+        ko = k - 1
+        stabeps = th_["cstabeps"] / dzw[ko]
+        wtdecay = math.exp(-float(dzw[ko]) / 40.)
+        zs = 1. if ko == 0 else 0.
+        sk, sko = stab[P + (k,)], stab[P + (ko,)]
+        t1 = t1 * wtdecay * stabeps / (stabeps + 0.5 * (sk + (1. - zs) * sko))
+        s1 = s1 * wtdecay * stabeps / (stabeps + 0.5 * (sk + (1. - zs) * sko))
+        du1 = uko[Uw + (k,)] - uko[Uw + (ko,)]
+        du2 = uko[Ue + (k,)] - uko[Ue + (ko,)]
+        dv1 = vke[Vs + (k,)] - vke[Vs + (ko,)]
+        dv2 = vke[Vn + (k,)] - vke[Vn + (ko,)]
+        w = weto[P + (k,)]
+        dudo = g["almzer"] + w * (di[k] * di[k]) * (du1 * du1 + du2 * du2 + dv1 * dv1 + dv2 * dv2) * 0.5
+        hho = w * (amsuo[Ue + (k,)] + amsuo[Uw + (k,)] + amsue[Vs + (k,)] + amsue[Vn + (k,)]) * 0.25
+        r = gor * sk / dudo
+        rinumo = hho * np.where(r > 0., r, 0.)
+        xd, xa = 1. + 5. * rinumo, 1. + 5. * rinumo
+        dv, av = dvo[P + (k,)], avo[P + (k,)]
+        m = th_["dv0"] + s1
+        dv = (relax * np.where(m < dv, m, dv) + relne * (s1 + th_["dv0"] / (xd * xd * xd) + th_["dbackv"][k] + 0.0)) * w
+        m = th_["av0"] + th_["abackv"][k]
+        av = (relax * np.where(m < av, m, av) + relne * (t1 + th_["av0"] / (xa * xa) + th_["abackv"][k] + 0.0)) * w
+        ca = th_["cavocon"] * (1.E-11 - sk) / (1.E-11 + np.abs(sk))
+        av = w * np.where(ca > av, ca, av)
+        cd = th_["cdvocon"] * (1.E-11 - sk) / (1.E-11 + np.abs(sk))
+        dv = w * np.where(cd > dv, cd, dv)
+        dvo[P + (k,)] = dv
+        avo[P + (k,)] = av
+    avo[:, :, ke] = 0.
+    dvo[:, :, ke] = 0.
+    for k in range(1, ke):
+        land = weto[:, :, k] < 0.5
+        tho[:, :, k] = np.where(land, tho[:, :, k - 1], tho[:, :, k])
+        sao[:, :, k] = np.where(land, sao[:, :, k - 1], sao[:, :, k])
+    for k in range(ke):
+        rhoo[:, :, k] = density(th_, tho[:, :, k], sao[:, :, k], preff[k])
+    return po, stab, rhoo
+
+
+# ------------------------------------------------------------- OCMODMOM ---
+# Written from ocmodmom.f90 (NON_HYDROSTATIC); vectorised over (i, j), with
+# the grid angles evaluated by math.cos / math.sqrt point by point.
+def ocmodmom(g, b, c, deutio, deutie, zo, uoo, voe, uko, vke, wno, po, stabio):
+    """In place on uko, vke, wno, po, stabio; returns (uk1o, vk1e, u1o, uso, v1e, vse)."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    G, stabn, dt, almzer = b["grav"], b["stabn"], g["dt"], g["almzer"]
+    stabo = 1. - stabn
+    dduo, ddue, amsuo, amsue = g["dduo"], g["ddue"], g["amsuo"], g["amsue"]
+    gila, giph, omega = c["gila"], c["giph"], c["omega"]
+    GI = lambda a, ii, jj: float(a[ii - 1, jj - 1])
+    for k in range(ke):
+        stabio[:, :, k] = 0.001 * g["dz"][k] * stabio[:, :, k] * g["weto"][:, :, k]
+        po[:, :, k] = po[:, :, k] + G * zo * b["rlsa1"]
+    for k in range(ke):
+        uko[:, :, k] = uko[:, :, k] * dduo[:, :, k]
+        vke[:, :, k] = vke[:, :, k] * ddue[:, :, k]
+    uk1o, vk1e = uko.copy(order="F"), vke.copy(order="F")
+    wn1o = wno.copy(order="F")
+    # grid-angle factors (Fortran I, J -> 0-based u index I, p index I-1)
+    fu = {}
+    for j in range(2, je):
+        for i in range(1, ie):
+            dlon = (GI(gila, 2 * i + 2, 2 * j) - GI(gila, 2 * i + 1, 2 * j)) * math.cos(GI(gila, 2 * i + 1, 2 * j))
+            dlat = GI(giph, 2 * i + 2, 2 * j) - GI(giph, 2 * i + 1, 2 * j)
+            fu[i, j] = (dlon, math.sqrt(dlon * dlon + dlat * dlat) + almzer,
+                        2 * omega * math.cos(GI(giph, 2 * i + 1, 2 * j)))
+    fv = {}
+    for j in range(1, je):
+        for i in range(2, ie):
+            dlon = (GI(gila, 2 * i, 2 * j) - GI(gila, 2 * i, 2 * j + 1)) * math.cos(GI(gila, 2 * i, 2 * j + 1))
+            dlat = GI(giph, 2 * i, 2 * j) - GI(giph, 2 * i, 2 * j + 1)
+            fv[i, j] = (dlon, math.sqrt(dlon * dlon + dlat * dlat) + almzer,
+                        2 * omega * math.cos(GI(giph, 2 * i, 2 * j + 1)))
+    fw = {}
+    for j in range(2, je):
+        for i in range(2, ie):
+            dlon = (GI(gila, 2 * i + 1, 2 * j) - GI(gila, 2 * i, 2 * j)) * math.cos(GI(gila, 2 * i, 2 * j))
+            dlat = GI(giph, 2 * i, 2 * j - 1) - GI(giph, 2 * i, 2 * j)
+            fw[i, j] = (dlon, dlat, math.sqrt(dlon * dlon + dlat * dlat) + almzer,
+                        2 * omega * math.cos(GI(giph, 2 * i, 2 * j)))
+
+    def tab(d, lo_i, hi_i, lo_j, hi_j, q):
+        return np.array([[d[i, j][q] for j in range(lo_j, hi_j + 1)] for i in range(lo_i, hi_i + 1)])
+
+    dlon_u, dist_u, f1_u = (tab(fu, 1, ie - 1, 2, je - 1, q) for q in range(3))
+    dlon_v, dist_v, f1_v = (tab(fv, 2, ie - 1, 1, je - 1, q) for q in range(3))
+    dlon_w, dlat_w, dist_w, f1_w = (tab(fw, 2, ie - 1, 2, je - 1, q) for q in range(4))
+    # index maps: u(I, J) -> [I, J-1]; v(I, J) -> [I-1, J]; p(I, J) -> [I-1, J-1]
+    Iu, Ju = slice(1, ie), slice(1, je - 1)            # u interior I 1..IE-1, J 2..JE-1
+    for _ in range(12):
+        ucor = stabn * uk1o + stabo * uko
+        vcor = stabn * vk1e + stabo * vke
+        wcor = stabn * wn1o + stabo * wno
+        for k in range(ke):
+            # u: VCOR(I,J), (I+1,J), (I,J-1), (I+1,J-1) -> v array [I-1, J], [I, J], [I-1, J-1], [I, J-1]
+            vc = vcor[:, :, k]
+            vcor_u = 0.25 * (vc[0:ie - 1, 2:je] + vc[1:ie, 2:je] + vc[0:ie - 1, 1:je - 1] + vc[1:ie, 1:je - 1])
+            pk = po[:, :, k]
+            new_u = (uko[Iu, Ju, k] + g["dtdxuo"][Iu, Ju] * (pk[0:ie - 1, 1:je - 1] - pk[1:ie, 1:je - 1]) * dduo[Iu, Ju, k]
+                     + dt * c["ftwou"][Iu, Ju] * vcor_u * amsuo[Iu, Ju, k])
+            # v: UCOR(I,J), (I-1,J), (I,J+1), (I-1,J+1) for I 2..IE-1, J 1..JE-1
+            uc = ucor[:, :, k]
+            ucor_v = 0.25 * (uc[2:ie, 0:je - 1] + uc[1:ie - 1, 0:je - 1] + uc[2:ie, 1:je] + uc[1:ie - 1, 1:je])
+            new_v = (vke[1:ie - 1, 1:je, k] + g["dpye"][1:ie - 1, 1:je] * (pk[1:ie - 1, 1:je] - pk[1:ie - 1, 0:je - 1])
+                     * ddue[1:ie - 1, 1:je, k] - dt * c["ftwov"][1:ie - 1, 1:je] * ucor_v * amsue[1:ie - 1, 1:je, k])
+            # NH u: WCOR at p (I, J) and (I+1, J), J 2..JE-1 -> p [I-1, J-1], [I, J-1]
+            wa, wb = wcor[:, :, k], wcor[:, :, k + 1]
+            dlxp, dlyp = g["dlxp"], g["dlyp"]
+            wcor_u = 0.25 * ((wa[0:ie - 1, 1:je - 1] + wb[0:ie - 1, 1:je - 1]) * dlxp[0:ie - 1, 1:je - 1]
+                             + (wa[1:ie, 1:je - 1] + wb[1:ie, 1:je - 1]) * dlxp[1:ie, 1:je - 1]) / g["dlxu"][Iu, Ju]
+            new_u = new_u - dt * f1_u * wcor_u * dduo[Iu, Ju, k] * dlon_u / dist_u
+            # NH v: p (I, J), (I, J+1) for I 2..IE-1, J 1..JE-1 -> p [I-1, J-1], [I-1, J]
+            wcor_v = 0.25 * ((wa[1:ie - 1, 0:je - 1] + wb[1:ie - 1, 0:je - 1]) * dlyp[1:ie - 1, 0:je - 1]
+                             + (wa[1:ie - 1, 1:je] + wb[1:ie - 1, 1:je]) * dlyp[1:ie - 1, 1:je]) / g["dlyv"][1:ie - 1, 1:je]
+            new_v = new_v - dt * f1_v * wcor_v * ddue[1:ie - 1, 1:je, k] * dlon_v / dist_v
+            uk1o[Iu, Ju, k] = new_u
+            vk1e[1:ie - 1, 1:je, k] = new_v
+            if k >= 1:
+                # p I, J 2..IE-1 / 2..JE-1 -> [1:ie-1, 1:je-1]; u(I), u(I-1) -> [I], [I-1]; v(J), v(J-1)
+                dd = g["ddpo"][1:ie - 1, 1:je - 1, k] + almzer
+                ddm = g["ddpo"][1:ie - 1, 1:je - 1, k - 1] + almzer
+                ucor_w = 0.25 * ((uko[2:ie, 1:je - 1, k] + uko[1:ie - 1, 1:je - 1, k]) / dd
+                                 + (uko[2:ie, 1:je - 1, k - 1] + uko[1:ie - 1, 1:je - 1, k - 1]) / ddm)
+                vcor_w = 0.25 * ((vke[1:ie - 1, 2:je, k] + vke[1:ie - 1, 1:je - 1, k]) / dd
+                                 + (vke[1:ie - 1, 2:je, k - 1] + vke[1:ie - 1, 1:je - 1, k - 1]) / ddm)
+                wn1o[1:ie - 1, 1:je - 1, k] = (wno[1:ie - 1, 1:je - 1, k] + dt * g["weto"][1:ie - 1, 1:je - 1, k]
+                                               * (f1_w * dlon_w / dist_w * ucor_w - f1_w * dlat_w / dist_w * vcor_w))
+        wno[:] = wn1o
+    u1o = np.zeros((ie + 1, je))
+    uso = np.zeros((ie + 1, je))
+    v1e = np.zeros((ie, je + 1))
+    vse = np.zeros((ie, je + 1))
+    for k in range(ke):
+        po[:, :, k] = po[:, :, k] - G * zo * b["rlsa1"]
+        u1o = u1o + dduo[:, :, k] * uoo[:, :, k]
+        uso = uso + uk1o[:, :, k]
+        v1e = v1e + ddue[:, :, k] * voe[:, :, k]
+        vse = vse + vk1e[:, :, k]
+    for k in range(ke):
+        uko[:, :, k] = uoo[:, :, k] - amsuo[:, :, k] * deutio * u1o
+        uk1o[:, :, k] = uk1o[:, :, k] * (amsuo[:, :, k] / (almzer + dduo[:, :, k])) - amsuo[:, :, k] * deutio * uso
+        vke[:, :, k] = voe[:, :, k] - amsue[:, :, k] * deutie * v1e
+        vk1e[:, :, k] = vk1e[:, :, k] * (amsue[:, :, k] / (almzer + ddue[:, :, k])) - amsue[:, :, k] * deutie * vse
+    return uk1o, vk1e, u1o, uso, v1e, vse
+
+
+# --------------------------------------------------------------- OCCLIT ---
+def _occlit_div(g, uko, vke, k, below):
+    """occlit.f90:108-112 / 250-254 over all p-points at level k."""
+    ie, je = g["ie"], g["je"]
+    dti = 1. / g["dt"]
+    return below + dti * g["weto"][:, :, k] * (
+        g["dtdxpo"] * (uko[0:ie, :, k] * g["dlyu"][0:ie, :] - uko[1:ie + 1, :, k] * g["dlyu"][1:ie + 1, :]) / g["dlyp"]
+        + g["dtdyo"] * (vke[:, 1:je + 1, k] * g["dlxv"][:, 1:je + 1] - vke[:, 0:je, k] * g["dlxv"][:, 0:je]) / g["dlxp"])
+
+
+def occlit(g, b, deutio, deutie, uko, vke, uk1o, vk1e, wo, stabio):
+    """In place on uko, vke, uk1o, vk1e, wo, stabio; returns CONTRA."""
+    ie, je, ke = g["ie"], g["je"], g["ke"]
+    G, stabn, conn, dt, almzer = b["grav"], b["stabn"], b["conn"], g["dt"], g["almzer"]
+    dduo, ddue, amsuo, amsue = g["dduo"], g["ddue"], g["amsuo"], g["amsue"]
+    stabio[:, :, 0] = 0.
+    bruva = np.zeros((ie, je))
+    for k in range(ke):
+        bruva = bruva + g["tiestw"][k + 1] * stabio[:, :, k]
+    uko *= dduo
+    uk1o *= dduo
+    vke *= ddue
+    vk1e *= ddue
+    for k in range(ke - 1, -1, -1):
+        wo[:, :, k] = _occlit_div(g, uko, vke, k, wo[:, :, k + 1])
+    wpo = np.zeros((ie, je, ke))
+    slow = np.zeros((ie, je))
+    for k in range(ke):
+        slow = slow + stabio[:, :, k] * dt * wo[:, :, k]
+        wpo[:, :, k] = slow
+    under = 0.
+    contrij = np.zeros((ie, je))
+    dtdxuo_p = g["dtdxuo"][1:ie + 1, :]          # DTDXUO(I, J) at p-index I
+    for it in range(1, 9):
+        px = np.zeros((ie + 1, je))
+        py = np.zeros((ie, je + 1))
+        for k in range(ke):
+            px[1:ie, :] = px[1:ie, :] + dduo[1:ie, :, k] * g["dtdxuo"][1:ie, :] * (wpo[1:ie, :, k] - wpo[0:ie - 1, :, k]) * amsuo[1:ie, :, k]
+            py[:, 1:je] = py[:, 1:je] + ddue[:, 1:je, k] * g["dpye"][:, 1:je] * (wpo[:, 0:je - 1, k] - wpo[:, 1:je, k]) * amsue[:, 1:je, k]
+        px[1:ie, :] = px[1:ie, :] * deutio[1:ie, :]
+        py[:, 1:je] = py[:, 1:je] * deutie[:, 1:je]
+        ucos = np.zeros((ie + 1, je))
+        vcos = np.zeros((ie, je + 1))
+        U = (slice(1, ie), slice(1, je - 1))          # I 1..IE-1, J 2..JE-1
+        V = (slice(1, ie - 1), slice(1, je))          # I 2..IE-1, J 1..JE-1
+        for k in range(ke):
+            dw = wpo[1:ie, 1:je - 1, k] - wpo[0:ie - 1, 1:je - 1, k]
+            u = uk1o[U + (k,)] + stabn * (px[U] - g["dtdxuo"][U] * dw) * dduo[U + (k,)]
+            ucos[U] = ucos[U] + u
+            uko[U + (k,)] = u * amsuo[U + (k,)]
+            dwv = wpo[1:ie - 1, 0:je - 1, k] - wpo[1:ie - 1, 1:je, k]
+            v = vk1e[V + (k,)] + stabn * (py[V] - g["dpye"][V] * dwv) * ddue[V + (k,)]
+            vcos[V] = vcos[V] + v
+            vke[V + (k,)] = v * amsue[V + (k,)]
+        for k in range(ke):
+            uko[U + (k,)] = uko[U + (k,)] - ucos[U] * deutio[U] * dduo[U + (k,)]
+            vke[V + (k,)] = vke[V + (k,)] - vcos[V] * deutie[V] * ddue[V + (k,)]
+        if it == 8:
+            break
+        t1o = np.zeros((ie, je, ke))
+        slow = np.zeros((ie, je))
+        for k in range(ke - 1, -1, -1):
+            t1o[:, :, k] = _occlit_div(g, uko, vke, k, slow)
+            slow = t1o[:, :, k]
+        tlow = np.zeros((ie, je))
+        contrij = np.zeros((ie, je))
+        for k in range(1, ke):
+            ove = wpo[:, :, k].copy()
+            tlow = tlow + G * stabio[:, :, k] * dt * (conn * t1o[:, :, k] + wo[:, :, k])
+            speed = 2. * G * bruva * (dtdxuo_p * dtdxuo_p + g["dtdyo"] * g["dtdyo"])
+            brems = under * speed * conn * stabn / (1. + speed)
+            vorw = 1. - brems
+            wpo[:, :, k] = vorw * tlow + brems * wpo[:, :, k]
+            d = ove - wpo[:, :, k]
+            contrij = contrij + d * d
+        under = 1.
+    for k in range(ke):
+        uko[:, :, k] = uko[:, :, k] * amsuo[:, :, k] / (almzer + dduo[:, :, k])
+        uk1o[:, :, k] = uk1o[:, :, k] * amsuo[:, :, k] / (almzer + dduo[:, :, k])
+        vke[:, :, k] = vke[:, :, k] * amsue[:, :, k] / (almzer + ddue[:, :, k])
+        vk1e[:, :, k] = vk1e[:, :, k] * amsue[:, :, k] / (almzer + ddue[:, :, k])
+    return float(np.add.accumulate(contrij.T.ravel())[-1])  # J outer, I inner, in order
