@@ -302,6 +302,47 @@ def timed_steps(gpu, k, pg):
     return ms, stats, launches
 
 
+def run_whole_step(inst, cells, args, ws, pg, local, hot_ms_per_step):
+    """The whole reference step on the device (orctm_step_full: OCTHER, OCWIND,
+    OCTIMF, OCMODMOM, OCBARP, OCCLIT, TRONEU's 250 SOR sweeps, OCVTRO, OCVTOT,
+    then the hot path) on a third instance of the same workload: only the
+    solve's scalars and OCCLIT's CONTRA reach the host per step."""
+    from orctm_b200 import configs, grid
+    from orctm_b200.api import Instance
+
+    gpu = Instance(inst, device=local)
+    gpu.upload_state(configs.copy_state(inst))
+    gpu.set_solver("fp64", rtol=1e-10, maxit=5000)
+    gpu.set_thermo(**configs.make_thermo(inst))
+    cor = configs.make_coriolis(inst)
+    gpu.set_coriolis(cor["ftwou"], cor["ftwov"], cor["gila"], cor["giph"], cor["omega"])
+    deuto, deute = grid.uv_depths(inst["depto"])
+    gpu.set_barotropic(deuto, deute, configs.barotropic_minvalue(inst))
+    gpu.ocwind(**configs.make_wind(inst))
+    for s in range(args.warmup):
+        gpu.step_full(s + 1)
+    barrier(pg)
+    gpu.synchronize()
+    n0 = Instance.kernel_launches()
+    gpu.timer_start()
+    stats = [gpu.step_full(args.warmup + s + 1) for s in range(args.steps)]
+    ms = gpu.timer_stop()
+    launches = Instance.kernel_launches() - n0
+    barrier(pg)
+    ms = max_over_ranks(pg, ms)
+    gpu.close()
+    per = ms / args.steps
+    return {"value": ws * cells * args.steps / (ms / 1e3), "unit": "cell-steps/s",
+            "ms_per_step": per, "hot_path_ms_per_step": hot_ms_per_step,
+            "before_hot_path_ms_per_step": per - hot_ms_per_step,
+            "poisson_iterations": statistics.mean(s["iterations"] for s in stats),
+            "contra_max": max(s["contra"] for s in stats),
+            "gpu_launches_per_step": launches / args.steps,
+            "note": "OCTHER (EOS " + ("linear" if inst["name"] == "c1" else "UNESCO") +
+                    "), OCWIND, OCTIMF, OCMODMOM, OCBARP, OCCLIT, TRONEU (250 SOR sweeps), OCVTRO, "
+                    "OCVTOT and the hot path, all on the device; state resident, no host copies"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -322,6 +363,8 @@ def main():
     ap.add_argument("--size", default=None, help="override nx x ny x nz (e.g. 256x256x60)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-whole-step", action="store_true",
+                    help="skip the whole-step (orctm_step_full) measurement")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-sample", type=lambda s: tuple(int(v) for v in s.split("x")),
                     default=None, help="sub-domain the CPU restatement times (default: the "
@@ -420,6 +463,10 @@ def main():
     if not args.no_e2e:
         e2e = run_e2e(gpu, inst, cells, args, ws, pg)
 
+    whole = None
+    if not args.no_whole_step:
+        whole = run_whole_step(inst, cells, args, ws, pg, local, ms_max / args.steps)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -436,7 +483,8 @@ def main():
             "data": DATA,
             "config": workload_config(inst),
             "poisson_ms": poisson_ms, "poisson_iterations": iters, "relres_max": relres,
-            "mixed": mixed, "solver_tuning": tuning, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "mixed": mixed, "whole_step": whole, "solver_tuning": tuning, "roofline": roofline,
+            "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": ck,
         }
         print(json.dumps(line), flush=True)

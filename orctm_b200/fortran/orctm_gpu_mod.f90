@@ -12,6 +12,11 @@ module orctm_gpu_mod
        ORCTM_F_UKO = 3, ORCTM_F_VKE = 4, ORCTM_F_WO = 5, ORCTM_F_UOO_1 = 6, &
        ORCTM_F_VOE_1 = 7, ORCTM_F_WNO_1 = 8, ORCTM_F_PNH = 9, ORCTM_F_ZO = 10, &
        ORCTM_F_DVO = 11, ORCTM_F_AVO = 12, ORCTM_F_THO = 13, ORCTM_F_SAO = 14
+  integer(c_int), parameter :: ORCTM_E_UNSTABLE = -9
+  integer(c_int), parameter :: ORCTM_EOS_UNESCO = 0, ORCTM_EOS_LINEAR = 1
+  integer(c_int), parameter :: ORCTM_C_PO = 0, ORCTM_C_STABIO = 1, ORCTM_C_RHOO = 2, &
+       ORCTM_C_UK1O = 3, ORCTM_C_VK1E = 4, ORCTM_C_EMINPO = 5, ORCTM_C_RIVRUN = 6, &
+       ORCTM_C_KCONDEP = 7
 
   type, bind(c) :: orctm_desc
      integer(c_int) :: ie, je, ke, i_start, j_start, ntracers
@@ -51,6 +56,30 @@ module orctm_gpu_mod
      real(c_double) :: minvalue, grav, stabn, conn, rlsa1, sorpar
      integer(c_int) :: niter, eta_forc
   end type orctm_barotropic
+
+  ! OCTHER's constants and surface forcing (orctm.f90:311-330, 503, 561-569, 739-743)
+  type, bind(c) :: orctm_thermo
+     integer(c_int) :: eos
+     real(c_double) :: rho0, drdt, drds, t0, s0
+     real(c_double) :: grav
+     real(c_double) :: relsal, reltem
+     real(c_double) :: rhoicwa, rhosnwa
+     real(c_double) :: wt
+     real(c_double) :: cstabeps, dv0, av0, cavocon, cdvocon
+     type(c_ptr) :: preff
+     type(c_ptr) :: dbackv
+     type(c_ptr) :: abackv
+     type(c_ptr) :: sicomo, sictho, sicsno
+     type(c_ptr) :: relsao, reltho
+     type(c_ptr) :: giriv
+     type(c_ptr) :: fu10
+  end type orctm_thermo
+
+  ! OCMODMOM's Coriolis inputs (the grid file's FTWOU, FTWOV; coriol.f90's GILA, GIPH)
+  type, bind(c) :: orctm_coriolis
+     type(c_ptr) :: ftwou, ftwov, gila, giph
+     real(c_double) :: omega
+  end type orctm_coriolis
 
   interface
      integer(c_int) function orctm_create(desc, h) bind(c, name="orctm_create")
@@ -158,6 +187,50 @@ module orctm_gpu_mod
          bind(c, name="orctm_ocwind")
        import :: c_int, c_ptr
        type(c_ptr), value :: h, txo, tye, sicomu, sicomv, tauwatu, tauwatv
+     end function
+     integer(c_int) function orctm_set_thermo(h, t) bind(c, name="orctm_set_thermo")
+       import :: c_int, c_ptr, orctm_thermo
+       type(c_ptr), value :: h
+       type(orctm_thermo), intent(in) :: t
+     end function
+     integer(c_int) function orctm_set_coriolis(h, c) bind(c, name="orctm_set_coriolis")
+       import :: c_int, c_ptr, orctm_coriolis
+       type(c_ptr), value :: h
+       type(orctm_coriolis), intent(in) :: c
+     end function
+     integer(c_int) function orctm_octher(h) bind(c, name="orctm_octher")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_ocmodmom(h) bind(c, name="orctm_ocmodmom")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function orctm_occlit(h, contra) bind(c, name="orctm_occlit")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: contra
+     end function
+     integer(c_int) function orctm_upload_baroclinic(h, which, host, n) &
+         bind(c, name="orctm_upload_baroclinic")
+       import :: c_int, c_ptr, c_size_t
+       type(c_ptr), value :: h, host
+       integer(c_int), value :: which
+       integer(c_size_t), value :: n
+     end function
+     integer(c_int) function orctm_download_baroclinic(h, which, host, n) &
+         bind(c, name="orctm_download_baroclinic")
+       import :: c_int, c_ptr, c_size_t
+       type(c_ptr), value :: h, host
+       integer(c_int), value :: which
+       integer(c_size_t), value :: n
+     end function
+     integer(c_int) function orctm_step_full(h, ldtrun, stats, contra) bind(c, name="orctm_step_full")
+       import :: c_int, c_ptr, c_double, orctm_solve_stats
+       type(c_ptr), value :: h
+       integer(c_int), value :: ldtrun
+       type(orctm_solve_stats), intent(out) :: stats
+       real(c_double), intent(out) :: contra
      end function
      integer(c_int) function orctm_download_barotropic(h, which, host, n) &
          bind(c, name="orctm_download_barotropic")

@@ -32,3 +32,21 @@ def build_grid(ie, je, ke, dt, dzw, depto, dlxp, dlyp, dlxu, dlyu, dlxv, dlyv):
                                       *[_p(a) for a in m], *[_p(g[k]) for k in GEOM_KEYS])
     _lib.check(st)
     return depto, g
+
+
+def uv_depths(depto):
+    """BODEN's u- and v-point depths (boden.f90:116-131): DEUTO (IE+1, JE) =
+    MIN of the two neighbouring DEPTO, the first and last column copied from
+    their neighbours; DEUTE (IE, JE+1) likewise in j.  ``depto`` is the
+    BODEN-adjusted (IE, JE) depth."""
+    d = np.asarray(depto, dtype=np.float64)
+    ie, je = d.shape
+    deuto = np.zeros((ie + 1, je), order="F")
+    deuto[1:ie, :] = np.where(d[1:, :] < d[:-1, :], d[1:, :], d[:-1, :])
+    deuto[0, :] = deuto[1, :]
+    deuto[ie, :] = deuto[ie - 1, :]
+    deute = np.zeros((ie, je + 1), order="F")
+    deute[:, 1:je] = np.where(d[:, 1:] < d[:, :-1], d[:, 1:], d[:, :-1])
+    deute[:, 0] = deute[:, 1]
+    deute[:, je] = deute[:, je - 1]
+    return deuto, deute

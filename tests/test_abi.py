@@ -148,7 +148,8 @@ def test_fortran_module_binds_exported_symbols_and_matching_types():
         assert hasattr(lib, n), n
         assert n in declared_functions(), n
     hdr = open(HEADER).read()
-    for t in ("orctm_desc", "orctm_solve_stats", "orctm_obc", "orctm_gridinfo", "orctm_barotropic"):
+    for t in ("orctm_desc", "orctm_solve_stats", "orctm_obc", "orctm_gridinfo", "orctm_barotropic",
+              "orctm_thermo", "orctm_coriolis"):
         assert _fortran_type_fields(src, t) == _c_struct_fields(hdr, t), t
 
 
