@@ -458,14 +458,18 @@ class Instance:
             raise ValueError(f"{name} shape {a.shape}, expected {shp}")
         _lib.check(self.lib.orctm_upload_baroclinic(self.h, which, _p(a), a.size), self.h)
 
-    def step_full(self, ldtrun: int) -> dict:
-        """One whole step (orctm_step_full); the solve's statistics and CONTRA."""
+    def step_full(self, ldtrun: int, check_contra: bool = True) -> dict:
+        """One whole step (orctm_step_full); the solve's statistics and CONTRA.
+        With check_contra False a CONTRA above 1e-3 (ORCTM_E_UNSTABLE, where
+        the reference aborts) is reported in the result instead of raised."""
         s = SolveStats()
         v = C.c_double()
-        _lib.check(self.lib.orctm_step_full(self.h, int(ldtrun), C.byref(s), C.byref(v)), self.h,
-                   allow=(_lib.ORCTM_E_NOT_CONVERGED,))
+        allow = (_lib.ORCTM_E_NOT_CONVERGED,) + (() if check_contra else (_lib.E_UNSTABLE,))
+        st = _lib.check(self.lib.orctm_step_full(self.h, int(ldtrun), C.byref(s), C.byref(v)),
+                        self.h, allow=allow)
         d = s.as_dict()
         d["contra"] = v.value
+        d["unstable"] = st == _lib.E_UNSTABLE
         return d
 
     def set_barotropic(self, deuto, deute, minvalue: float, grav=9.806, stabn=0.6, conn=0.5,

@@ -87,7 +87,10 @@ def _bathymetry_box(g: np.random.Generator, nx: int, ny: int, depth: float = 400
 
 
 def raw_instance(name: str, index: int = 0, seed: int | None = None, **over) -> dict:
-    """Model inputs before the grid builder runs (depth, metrics, dz, dt, ...)."""
+    """Model inputs before the grid builder runs (depth, metrics, dz, dt, ...).
+    ``closed=True`` makes every side land (whole steps of c2-c5: the
+    reference's open-boundary elevation row in TRONEU, Z1O = B1O / XX,
+    troneu.f90:67-102, is explicit and grows at these time steps)."""
     s = BASE_SEED + index if seed is None else seed
     g = rng(s)
     ob = {"west": False, "east": False, "north": False, "south": False}
@@ -129,6 +132,11 @@ def raw_instance(name: str, index: int = 0, seed: int | None = None, **over) -> 
                 "phase": 0.0 if name in ("c2", "c3") else float(g.uniform(0.0, 2 * math.pi))}
     else:
         raise ValueError(f"unknown configuration {name!r}")
+    if over.get("closed"):
+        # every side land: the open west and south of c2-c5 closed
+        depto[0, :] = depto[-1, :] = 0.0
+        depto[:, 0] = depto[:, -1] = 0.0
+        ob = {k: False for k in ob}
     dt = over.get("dt", dt)
     ie, je, ke = nx + 2, ny + 2, nz
     inst = {"name": name, "seed": s, "ie": ie, "je": je, "ke": ke, "nx": nx, "ny": ny, "nz": nz,
