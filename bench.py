@@ -302,7 +302,7 @@ def timed_steps(gpu, k, pg):
     return ms, stats, launches
 
 
-def run_whole_step(inst, cells, args, ws, pg, local, hot_ms_per_step):
+def run_whole_step(inst, cells, args, ws, rank, pg, local, hot_ms_per_step):
     """The whole reference step on the device (orctm_step_full: OCTHER, OCWIND,
     OCTIMF, OCMODMOM, OCBARP, OCCLIT, TRONEU's 250 SOR sweeps, OCVTRO, OCVTOT,
     then the hot path) on a third instance of the same workload: only the
@@ -473,7 +473,7 @@ def main():
 
     whole = None
     if not args.no_whole_step:
-        whole = run_whole_step(inst, cells, args, ws, pg, local, ms_max / args.steps)
+        whole = run_whole_step(inst, cells, args, ws, rank, pg, local, ms_max / args.steps)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -626,7 +626,9 @@ def run_e2e(gpu, inst, cells, args, ws, pg):
     from orctm_b200 import configs
 
     st = configs.copy_state(inst)
-    ins = ["uoo", "voe", "wno", "uko", "vke", "wo"]
+    # the transports first (all three momentum advection routines read them),
+    # then each routine's own field; the tracers last (read after the solve)
+    ins = ["uko", "vke", "wo", "uoo", "voe", "wno"]
     outs = ["uoo", "voe", "wno", "pnh"]
     pinned = {}
 
@@ -648,10 +650,10 @@ def run_e2e(gpu, inst, cells, args, ws, pg):
     d2h = sum(pinned[k][1].nbytes for k in pinned if k.startswith("out_"))
     k_steps = max(2, min(args.steps, 5))
 
-    # uploads go to the copy stream (velocities first: the momentum advection
+    # uploads go to the copy stream (velocities first: the momentum path
     # waits for them, the tracers land while it runs); the outputs are
     # registered so that each step downloads them as soon as they are final
-    # (the tracers while OCVISC and the Poisson solve run)
+    # (the momentum fields while the tracers are advected and diffused)
     outmap = {k: pinned["out_" + k][1] for k in outs}
     outmap.update({f"tracer{n}": pinned[f"out_tracer{n}"][1] for n in range(gpu.ntr)})
     gpu.set_step_outputs(outmap)

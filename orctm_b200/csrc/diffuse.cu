@@ -101,6 +101,115 @@ __global__ void __launch_bounds__(kVertBlock) k_tdiff_vert(Geo G, TrPtrs tp, int
   }
 }
 
+// The same solve with the tracer count known at compile time and the loads
+// of U levels issued together before they are used: the input and output
+// arrays may alias as far as the compiler knows, so the one-level form above
+// waits a full memory latency per level in each sweep.  Every value is
+// formed by the same expressions in the same order, so the results equal
+// k_tdiff_vert's bit for bit.
+template <int NTR, int U>
+__global__ void __launch_bounds__(kVertBlock) k_tdiff_vert_b(Geo G, TrPtrs tp,
+                                                             const double* __restrict__ dvo,
+                                                             const double* __restrict__ zo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const int pl = G.L.plane;
+  const int base = G.L.at(i, j, 0);
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1;
+  if (!interior) {
+    for (int K0 = 1; K0 <= KE; K0 += U) {
+      double v[NTR][U];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int n = 0; n < NTR; ++n)
+          v[n][u] = K0 + u <= KE ? tp.in[n][base + (K0 + u - 1) * pl] : 0.0;
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int n = 0; n < NTR; ++n)
+          if (K0 + u <= KE) tp.out[n][base + (K0 + u - 1) * pl] = v[n][u];
+    }
+    return;
+  }
+  const int ij = G.L.at2(i, j);
+  const double zij = zo[ij];
+  auto den = [&](int K) {
+    const double zzsurf = K == 1 ? 1. : 0.;
+    return thick(G.gp, G.dzw, ij, K) + zzsurf * (zij) + G.almzer;
+  };
+  double t2p[kMaxKe];
+  double ylast[NTR];
+  double t2prev = 1.0, t3prev = 0.0;
+  // forward elimination, U levels per batch: DVO(K..K+U) and the tracers of
+  // K..K+U-1 are loaded first
+  for (int K0 = 1; K0 <= KE; K0 += U) {
+    double lt[NTR][U], ld[U + 1];
+#pragma unroll
+    for (int u = 0; u <= U; ++u) ld[u] = K0 + u <= KE + 1 ? dvo[base + (K0 + u - 1) * pl] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int n = 0; n < NTR; ++n)
+        lt[n][u] = K0 + u <= KE ? tp.in[n][base + (K0 + u - 1) * pl] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 + u;
+      if (K > KE) break;
+      const double dn = den(K);
+      const double t1 = div_nr(-G.dt * ld[u] * wet(G.gp, ij, K) * G.di[K - 1], dn);
+      const double t3 = div_nr(-G.dt * ld[u + 1] * G.di[K], dn);
+      double t2 = 1. - t1 - t3;
+      double m = 0.0;
+      if (K >= 2) {
+        m = div_nr(t1, t2prev);
+        t2 = t2 - div_nr(t3prev * t1, t2prev);
+      }
+      t2p[K - 1] = t2;
+#pragma unroll
+      for (int n = 0; n < NTR; ++n) {
+        const double tk = lt[n][u];
+        const double y = K == 1 ? tk : tk - m * ylast[n];
+        tp.out[n][base + (K - 1) * pl] = y;
+        ylast[n] = y;
+      }
+      t2prev = t2;
+      t3prev = t3;
+    }
+  }
+  // back substitution, U levels per batch: the forward values and DVO of
+  // l-U+1..l loaded first
+  double nxt[NTR];
+#pragma unroll
+  for (int n = 0; n < NTR; ++n) {
+    nxt[n] = div_nr(ylast[n], t2p[KE - 1]);
+    tp.out[n][base + (KE - 1) * pl] = nxt[n];
+  }
+  for (int l0 = KE - 1; l0 >= 1; l0 -= U) {
+    double ly[NTR][U], ld[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int l = l0 - u;
+      ld[u] = l >= 1 ? dvo[base + l * pl] : 0.0;  // DVO(l+1)
+#pragma unroll
+      for (int n = 0; n < NTR; ++n) ly[n][u] = l >= 1 ? tp.out[n][base + (l - 1) * pl] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int l = l0 - u;
+      if (l < 1) break;
+      const double t3 = div_nr(-G.dt * ld[u] * G.di[l], den(l));
+#pragma unroll
+      for (int n = 0; n < NTR; ++n) {
+        nxt[n] = div_nr(ly[n][u] - t3 * nxt[n], t2p[l - 1]);
+        tp.out[n][base + (l - 1) * pl] = nxt[n];
+      }
+    }
+  }
+}
+
 // Laplacian and biharmonic update fused (octdiff_ts.f90:342-399), all
 // tracers in one launch.  A block of 32 x 8 cells marches down the levels;
 // per level it stages the 36 x 12 tile of the vertically diffused tracer in
@@ -356,6 +465,196 @@ __global__ void __launch_bounds__(kVertBlock) k_visc_uv(Geo G, const double* __r
     t3 = t3 * wet(cg, ij, l + 1);
     nxt = div_nr((AT(O, i, j, l) - t3 * nxt) * wet(cg, ij, l), t2p[l - 1]);
     AT(O, i, j, l) = nxt;
+  }
+}
+
+// k_visc_uv with the loads of U levels issued together before they are used
+// (X and AVO of both columns in the forward sweep, the forward values and AVO
+// in the backward one); the same expressions in the same order, so the
+// results equal k_visc_uv's bit for bit.
+template <int DIR, int U>
+__global__ void __launch_bounds__(kVertBlock) k_visc_uv_b(Geo G, const double* __restrict__ X,
+                                                          const double* __restrict__ keep,
+                                                          const double* __restrict__ avo,
+                                                          const double* __restrict__ speed,
+                                                          double* __restrict__ O) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const bool interior = DIR == 0 ? (i >= 1 && i <= IE - 1 && j >= 2 && j <= JE - 1)
+                                 : (i >= 2 && i <= IE - 1 && j >= 1 && j <= JE - 1);
+  const bool valid = DIR == 0 ? (j >= 1) : (i >= 1);
+  if (!valid) return;
+  const int pl = G.L.plane;
+  const int base = G.L.at(i, j, 0);
+  if (!interior) {
+    for (int K = 1; K <= KE; ++K) O[base + (K - 1) * pl] = keep[base + (K - 1) * pl];
+    return;
+  }
+  const ColGeo& cg = DIR == 0 ? G.gu : G.gv;
+  const int ij = G.L.at2(i, j);
+  const int ij2 = DIR == 0 ? G.L.at2(i + 1, j) : G.L.at2(i, j + 1);
+  const double BOFRIC = 3.E-3, RAYFRIC = 3.E-3;
+  const double sp = speed[ij];
+  // TRIDSY(K,1) and TRIDSY(K,3) from AVO of levels K (a0, b0) and K+1 (a1, b1)
+  // of the two columns, as k_visc_uv's tri
+  auto tri = [&](int K, double a0, double b0, double a1, double b1, double& t1, double& t3) {
+    const double am = wet(cg, ij, K), dd = thick(cg, G.dzw, ij, K);
+    const double avup = 0.5 * (a0 + b0) * am;
+    if (K < KE) {
+      const double am1 = wet(cg, ij, K + 1);
+      const double avlo = 0.5 * (a1 + b1) * am1 + (BOFRIC + RAYFRIC * dd * sp) * (am - am1);
+      t1 = div_nr(-G.dt * avup * am * G.di[K - 1], G.almzer + dd);
+      t3 = div_nr(-G.dt * avlo * am * G.di[K], G.almzer + dd);
+    } else {
+      const double avlo = (BOFRIC + RAYFRIC * dd * sp) * am;
+      t1 = div_nr(-G.dt * avup * am * G.di[K - 1], G.almzer + dd);
+      t3 = div_nr(-G.dt * avlo * am * G.di[K], G.almzer + dd);
+    }
+  };
+  double t2p[kMaxKe];
+  double t2prev = 1.0, t3prev = 0.0, yprev = 0.0;
+  for (int K0 = 1; K0 <= KE; K0 += U) {
+    double la[U + 1], lb[U + 1], lx[U];
+#pragma unroll
+    for (int u = 0; u <= U; ++u) {
+      const bool ok = K0 + u <= KE;
+      la[u] = ok ? avo[ij + (K0 + u - 1) * pl] : 0.0;
+      lb[u] = ok ? avo[ij2 + (K0 + u - 1) * pl] : 0.0;
+      if (u < U) lx[u] = ok ? X[base + (K0 + u - 1) * pl] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 + u;
+      if (K > KE) break;
+      double t1, t3;
+      tri(K, la[u], lb[u], la[u + 1], lb[u + 1], t1, t3);
+      double t2 = 1. - t1 - t3;
+      t3 = K < KE ? t3 * wet(cg, ij, K + 1) : 0.;
+      const double xk = lx[u];
+      double y = xk;
+      if (K >= 2) {
+        const double m = div_nr(t1, t2prev);
+        t2 = t2 - div_nr(t3prev * t1, t2prev);
+        y = xk - m * yprev;
+      }
+      t2p[K - 1] = t2;
+      O[base + (K - 1) * pl] = y;
+      yprev = y;
+      t2prev = t2;
+      t3prev = t3;
+    }
+  }
+  double nxt = div_nr(wet(cg, ij, KE) * yprev, t2p[KE - 1]);
+  O[base + (KE - 1) * pl] = nxt;
+  for (int l0 = KE - 1; l0 >= 1; l0 -= U) {
+    double la[U], lb[U], la1[U], lb1[U], ly[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int l = l0 - u;
+      const bool ok = l >= 1;
+      la[u] = ok ? avo[ij + (l - 1) * pl] : 0.0;
+      lb[u] = ok ? avo[ij2 + (l - 1) * pl] : 0.0;
+      la1[u] = ok ? avo[ij + l * pl] : 0.0;
+      lb1[u] = ok ? avo[ij2 + l * pl] : 0.0;
+      ly[u] = ok ? O[base + (l - 1) * pl] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int l = l0 - u;
+      if (l < 1) break;
+      double t1, t3;
+      tri(l, la[u], lb[u], la1[u], lb1[u], t1, t3);
+      t3 = t3 * wet(cg, ij, l + 1);
+      nxt = div_nr((ly[u] - t3 * nxt) * wet(cg, ij, l), t2p[l - 1]);
+      O[base + (l - 1) * pl] = nxt;
+    }
+  }
+}
+
+// k_visc_w with the loads of U levels issued together (bit for bit the same)
+template <int U>
+__global__ void __launch_bounds__(kVertBlock) k_visc_w_b(Geo G, const double* __restrict__ W,
+                                                         const double* __restrict__ avo,
+                                                         double* __restrict__ O) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE || j > JE) return;
+  const int pl = G.L.plane;
+  const int base = G.L.at(i, j, 0);
+  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1 && KE >= 2;
+  if (!interior) {
+    for (int K = 1; K <= KE + 1; ++K) O[base + (K - 1) * pl] = W[base + (K - 1) * pl];
+    return;
+  }
+  const int ij = G.L.at2(i, j);
+  auto den = [&](int K) {
+    return 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
+  };
+  // AVO of levels K-1 (am), K (a0), K+1 (a1)
+  auto tri1 = [&](int K, double dn, double am, double a0) {
+    const double avup = 0.5 * (am + a0) * wet(G.gp, ij, K - 1);
+    return div_nr(-2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2], dn);
+  };
+  auto tri3 = [&](int K, double dn, double a0, double a1) {
+    const double avlo = K < KE ? 0.5 * (a1 + a0) * wet(G.gp, ij, K) : 0.0;
+    return div_nr(-2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1], dn);
+  };
+  double t2p[kMaxKe];
+  O[base] = W[base];
+  O[base + KE * pl] = W[base + KE * pl];
+  double prev = 0.0, t2prev = 1.0, t3prev = 0.0;
+  for (int K0 = 2; K0 <= KE; K0 += U) {
+    double la[U + 2], lw[U];
+#pragma unroll
+    for (int u = 0; u < U + 2; ++u) {
+      const int K = K0 - 1 + u;  // K0-1 .. K0+U
+      la[u] = K <= KE ? avo[base + (K - 1) * pl] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) lw[u] = K0 + u <= KE ? W[base + (K0 + u - 1) * pl] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 + u;
+      if (K > KE) break;
+      const double dn = den(K);
+      const double t1 = tri1(K, dn, la[u], la[u + 1]), t3 = tri3(K, dn, la[u + 1], la[u + 2]);
+      double t2 = 1. - t1 - t3;
+      double y = lw[u];
+      if (K >= 3) {
+        const double m = div_nr(t1, t2prev);
+        t2 = t2 - div_nr(t3prev * t1, t2prev);
+        y = y - m * prev;
+      }
+      t2p[K - 1] = t2;
+      O[base + (K - 1) * pl] = y;
+      prev = y;
+      t2prev = t2;
+      t3prev = K < KE ? t3 : 0.;
+    }
+  }
+  double nxt = div_nr(wet(G.gp, ij, KE) * prev, t2p[KE - 1]);
+  O[base + (KE - 1) * pl] = nxt;
+  for (int K0 = KE - 1; K0 >= 2; K0 -= U) {
+    double la[U], la1[U], ly[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 - u;
+      const bool ok = K >= 2;
+      la[u] = ok ? avo[base + (K - 1) * pl] : 0.0;
+      la1[u] = ok ? avo[base + K * pl] : 0.0;
+      ly[u] = ok ? O[base + (K - 1) * pl] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 - u;
+      if (K < 2) break;
+      const double t3 = tri3(K, den(K), la[u], la1[u]);
+      nxt = div_nr((ly[u] - t3 * nxt) * wet(G.gp, ij, K), t2p[K - 1]);
+      O[base + (K - 1) * pl] = nxt;
+    }
   }
 }
 
@@ -622,7 +921,14 @@ void launch_octdiff_vert(const Geo& G, int ntr, const double* const* in, double*
     tp.out[n] = out[n];
   }
   const dim3 b(32, kVertBlock / 32);
-  k_tdiff_vert<<<grid2(G.L.ie, G.L.je, b), b, 0, st>>>(G, tp, ntr, dvo, zo);
+  const dim3 gr = grid2(G.L.ie, G.L.je, b);
+  switch (ntr) {
+    case 1: k_tdiff_vert_b<1, 4><<<gr, b, 0, st>>>(G, tp, dvo, zo); break;
+    case 2: k_tdiff_vert_b<2, 4><<<gr, b, 0, st>>>(G, tp, dvo, zo); break;
+    case 3: k_tdiff_vert_b<3, 4><<<gr, b, 0, st>>>(G, tp, dvo, zo); break;
+    case 4: k_tdiff_vert_b<4, 4><<<gr, b, 0, st>>>(G, tp, dvo, zo); break;
+    default: k_tdiff_vert<<<gr, b, 0, st>>>(G, tp, ntr, dvo, zo); break;
+  }
   count_launch();
 }
 
@@ -646,11 +952,11 @@ void launch_ocvisc(const Geo& G, const double* uoo, const double* voe, const dou
   const dim3 b2(32, 4), bc(32, kVertBlock / 32), b3(32, 4);
   k_visc_speed<<<grid2(IE + 1, JE + 1, b2), b2, 0, st>>>(G, uoo, voe, spu, spv);
   count_launch();
-  k_visc_uv<0><<<grid2(IE + 1, JE + 1, bc), bc, 0, st>>>(G, uoo, uko, avo, spu, ukv);
+  k_visc_uv_b<0, 4><<<grid2(IE + 1, JE + 1, bc), bc, 0, st>>>(G, uoo, uko, avo, spu, ukv);
   count_launch();
-  k_visc_uv<1><<<grid2(IE + 1, JE + 1, bc), bc, 0, st>>>(G, voe, vke, avo, spv, vkv);
+  k_visc_uv_b<1, 4><<<grid2(IE + 1, JE + 1, bc), bc, 0, st>>>(G, voe, vke, avo, spv, vkv);
   count_launch();
-  k_visc_w<<<grid2(IE, JE, bc), bc, 0, st>>>(G, wno, avo, wnv);
+  k_visc_w_b<4><<<grid2(IE, JE, bc), bc, 0, st>>>(G, wno, avo, wnv);
   count_launch();
   dim3 gl = grid2(IE + 1, JE + 1, b3);
   gl.z = KE;

@@ -1131,13 +1131,20 @@ int r_ocadpo(orctm_handle* h, int n) {
 
 // OCADPO for every tracer: one set of sweeps per group of tracers shares the
 // transports and volumes (launch_ocadpo_all); the same results as r_ocadpo
-// tracer by tracer
-int r_ocadpo_all(orctm_handle* h) {
+// tracer by tracer.  uko / vke / wo, when given, are the transports to use
+// (the step's initial ones, held while the momentum path ran first)
+int r_ocadpo_all(orctm_handle* h, const double* uko = nullptr, const double* vke = nullptr,
+                 const double* wo = nullptr) {
   int st;
   const int ntr = h->ntr;
   for (int n = 0; n < ntr; ++n)
     if ((st = wait_uploads(h, {ORCTM_F_THO + n}))) return st;
   if ((st = wait_uploads(h, {ORCTM_F_UKO, ORCTM_F_VKE, ORCTM_F_WO, ORCTM_F_ZO}))) return st;
+  if (!uko) {
+    uko = h->slot[ORCTM_F_UKO];
+    vke = h->slot[ORCTM_F_VKE];
+    wo = h->slot[ORCTM_F_WO];
+  }
   double *out[kMaxTracers] = {}, *mid[kMaxTracers] = {}, *vA = nullptr, *vB = nullptr;
   const double* in[kMaxTracers] = {};
   for (int n = 0; n < ntr; ++n) {
@@ -1146,8 +1153,7 @@ int r_ocadpo_all(orctm_handle* h) {
   }
   if ((st = h->alloc(&vA)) || (st = h->alloc(&vB))) return st;
   PROF(h, ORCTM_PROF_OCADPO,
-       launch_ocadpo_all(h->G, ntr, in, out, mid, h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE],
-                         h->slot[ORCTM_F_WO], h->zo, vA, vB, h->stream));
+       launch_ocadpo_all(h->G, ntr, in, out, mid, uko, vke, wo, h->zo, vA, vB, h->stream));
   ORCTM_CUDA_OK(cudaGetLastError());
   for (int n = 0; n < ntr; ++n) {
     h->bind(ORCTM_F_THO + n, out[n]);
@@ -1188,12 +1194,12 @@ int r_momadv(orctm_handle* h) {
 }
 
 int r_octdiff(orctm_handle* h) {
-  {
-    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
-    if (st0) return st0;
-  }
   int st;
   const int ntr = h->ntr;
+  // what it reads and the slots it rebinds
+  for (int n = 0; n < ntr; ++n)
+    if ((st = wait_uploads(h, {ORCTM_F_THO + n}))) return st;
+  if ((st = wait_uploads(h, {ORCTM_F_DVO, ORCTM_F_ZO}))) return st;
   const double* in[kMaxTracers];
   double* outv[kMaxTracers];
   for (int n = 0; n < ntr; ++n) {
@@ -1220,7 +1226,8 @@ int r_octdiff(orctm_handle* h) {
 
 int r_octimf(orctm_handle* h) {
   {
-    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
+    // the slots it rebinds: their uploads land first
+    const int st0 = wait_uploads(h, {ORCTM_F_UKO, ORCTM_F_VKE, ORCTM_F_UOO, ORCTM_F_VOE});
     if (st0) return st0;
   }
   h->alias(ORCTM_F_UKO, ORCTM_F_UOO);
@@ -1230,7 +1237,9 @@ int r_octimf(orctm_handle* h) {
 
 int r_ocvisc(orctm_handle* h) {
   {
-    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
+    // what it reads and the slots it rebinds
+    const int st0 = wait_uploads(h, {ORCTM_F_UOO, ORCTM_F_VOE, ORCTM_F_WNO, ORCTM_F_UKO,
+                                     ORCTM_F_VKE, ORCTM_F_AVO});
     if (st0) return st0;
   }
   int st;
@@ -1255,7 +1264,10 @@ int r_ocvisc(orctm_handle* h) {
 
 int r_ocvtot_nh(orctm_handle* h, orctm_solve_stats* stats) {
   {
-    const int st0 = wait_all_uploads(h);  // these routines rebind or alias slots
+    // what it reads and the slots it rebinds
+    const int st0 = wait_uploads(h, {ORCTM_F_UOO, ORCTM_F_VOE, ORCTM_F_WNO, ORCTM_F_UOO_1,
+                                     ORCTM_F_VOE_1, ORCTM_F_WNO_1, ORCTM_F_PNH, ORCTM_F_WO,
+                                     ORCTM_F_ZO});
     if (st0) return st0;
   }
   int st;
@@ -2395,20 +2407,43 @@ int orctm_download_baroclinic(orctm_handle* h, int which, double* host, size_t n
   return ORCTM_OK;
 }
 
+// The routines of the step in the driver's order (orctm.f90:1454-1562)
+// depend on one another through the velocities only: OCADPO and OCTDIFF
+// read the transports UKO, VKE, WO the step starts with (and ZO, DVO), and
+// nothing of the momentum path reads the tracers.  So the momentum path
+// (OCUAD, OCVAD, OCWAD, OCTIMF, OCVISC, OCVTOT_NH, OCTIMF) runs first, on
+// the momentum fields alone, and the tracer path after it on the held
+// initial transports: the results are those of the driver's order bit for
+// bit, while the tracers' uploads land during the momentum path and the
+// momentum outputs download during the tracer path.
 int orctm_step_hotpath(orctm_handle* h, orctm_solve_stats* s) {
   ORCTM_ENTER(h);
   int st;
   if ((st = r_momadv<0>(h)) || (st = r_momadv<1>(h)) || (st = r_momadv<2>(h))) return st;
-  if ((st = r_ocadpo_all(h))) return st;  // OCADPO(THO), OCADPO(SAO), passive tracers
-  if ((st = r_octdiff(h))) return st;
-  // tracers are final here: registered tracer outputs start downloading
-  // while OCVISC and the Poisson solve run
-  if ((st = step_outputs(h, true))) return st;
-  if ((st = r_octimf(h)) || (st = r_ocvisc(h))) return st;
+  double* held[3] = {h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], h->slot[ORCTM_F_WO]};
+  for (double* p : held) h->refs[p]++;
+  auto release = [&]() {
+    for (double* p : held) h->unref(p);
+  };
+  if ((st = r_octimf(h)) || (st = r_ocvisc(h))) {
+    release();
+    return st;
+  }
   const int ns = r_ocvtot_nh(h, s);
-  if (ns != ORCTM_OK && ns != ORCTM_E_NOT_CONVERGED) return ns;
+  if (ns != ORCTM_OK && ns != ORCTM_E_NOT_CONVERGED) {
+    release();
+    return ns;
+  }
   r_octimf(h);
-  if ((st = step_outputs(h, false))) return st;
+  // the momentum outputs are final: registered ones start downloading
+  // while the tracers are advected and diffused
+  if ((st = step_outputs(h, false))) {
+    release();
+    return st;
+  }
+  st = r_ocadpo_all(h, held[0], held[1], held[2]);  // OCADPO(THO), OCADPO(SAO), passive tracers
+  release();  // stream-ordered: a later user of these buffers runs after OCADPO
+  if (st || (st = r_octdiff(h)) || (st = step_outputs(h, true))) return st;
   return ns;
 }
 
@@ -2531,9 +2566,10 @@ int orctm_estimate_device_bytes(const orctm_desc* d, int solver, unsigned long l
   const double plane = P * (d->je + 1), n3 = plane * (d->ke + 1);
   // 3D buffers: 12 state fields and the tracers, the routine temporaries of
   // the field pool (at most max(8, 2 ntracers + 2), the advection of all
-  // tracers at once), 9 FP64 solver vectors, the FP64 + FP32 pivots, and 7
+  // tracers at once, plus the step's initial transports held for it), 9
+  // FP64 solver vectors, the FP64 + FP32 pivots, and 7
   // FP32 vectors for the refined solver
-  const double tmp = std::max(8.0, 2.0 * d->ntracers + 2.0);
+  const double tmp = std::max(8.0, 2.0 * d->ntracers + 2.0) + 3.0;  // + the held transports
   const double f3 = 12.0 + d->ntracers + tmp + 9.0 + 1.5 +
                     (solver == ORCTM_SOLVER_FP32_REFINED ? 3.5 : 0.0);
   // 2D tables (compressed columns, metrics, biharmonic and Poisson factors)
