@@ -149,6 +149,7 @@ __global__ void k_octher_column(Geo G, ThermoArgs a, ThermoFields f, double* __r
   double kc = f.kcondep[ij];
   double tprev = t[0], sprev = s[0], pprev = po[0];
   const double zsurf_val = zo[ij] - f.sictho[ij] * a.rhoicwa - f.sicsno[ij] * a.rhosnwa;
+#pragma unroll 2
   for (int K = 2; K <= KE; ++K) {
     const int o = (K - 1) * pl;
     const double tk = t[o], sk = s[o];
@@ -282,70 +283,121 @@ __global__ void k_modmom_init(Geo G, BaroArgs b, ThermoFields f, const double* _
   }
 }
 
+constexpr int kModmomChunk = 8;  // levels a block of k_modmom_iter marches through
+
 // One Coriolis iteration (ocmodmom.f90:76-183) from (ua, va, wa) into
 // (ub, vb, wb); UCOR / VCOR / WCOR are formed on the fly from the old values
 // (WN1O equals WNO at the start of every iteration, so W is one array).
-// Points the iteration does not update are copied.
-__global__ void k_modmom_iter(Geo G, BaroArgs b, ThermoFields f, CorFields c,
-                              const double* __restrict__ uko, const double* __restrict__ vke,
-                              const double* __restrict__ ua, const double* __restrict__ va,
-                              const double* __restrict__ wa, double* __restrict__ ub,
-                              double* __restrict__ vb, double* __restrict__ wb) {
+// Points the iteration does not update are copied.  One thread per (i, j)
+// in [0,IE]x[0,JE] marches down a chunk of kModmomChunk levels (the grid's
+// z index), so the point's 2D factors are loaded once per chunk while the
+// blocks in flight stay on nearby levels.
+__global__ void __launch_bounds__(128) k_modmom_iter(Geo G, BaroArgs b, ThermoFields f, CorFields c,
+                                                     const double* __restrict__ uko,
+                                                     const double* __restrict__ vke,
+                                                     const double* __restrict__ dw,
+                                                     const double* __restrict__ ua,
+                                                     const double* __restrict__ va,
+                                                     const double* __restrict__ wa,
+                                                     double* __restrict__ ub,
+                                                     double* __restrict__ vb,
+                                                     double* __restrict__ wb) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int K = blockIdx.z + 1;  // 1 .. KE+1
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
   const double stabn = b.stabn, stabo = 1. - b.stabn, dt = G.dt, almzer = G.almzer;
-  const int ij = G.L.at2(i, j), o = G.L.at(i, j, K - 1);
+  const int ij = G.L.at2(i, j);
   const int P = G.L.P, pl = G.L.plane;
-  if (K <= KE) {
-    // u-points
-    if (j >= 1) {
-      double u = ua[o];
-      if (j >= 2 && j <= JE - 1 && i >= 1 && i <= IE - 1) {
-        const double vcor_u = 0.25 * ((stabn * va[o] + stabo * vke[o]) + (stabn * va[o + 1] + stabo * vke[o + 1]) +
-                                      (stabn * va[o - P] + stabo * vke[o - P]) +
-                                      (stabn * va[o + 1 - P] + stabo * vke[o + 1 - P]));
-        u = uko[o] + G.dtdxuo[ij] * (f.po[o] - f.po[o + 1]) * thick(G.gu, G.dzw, ij, K) +
-            c.dtfu[ij] * vcor_u * wet(G.gu, ij, K);
-        // the NH part (ocmodmom.f90:122-134) on the same points
-        const double w00 = stabn * wa[o] + stabo * wa[o], w01 = stabn * wa[o + pl] + stabo * wa[o + pl];
-        const double w10 = stabn * wa[o + 1] + stabo * wa[o + 1];
-        const double w11 = stabn * wa[o + 1 + pl] + stabo * wa[o + 1 + pl];
-        const double wcor_u = 0.25 * ((w00 + w01) * G.dlxp[ij] + (w10 + w11) * G.dlxp[ij + 1]) / G.dlxu[ij];
-        u = u - c.cu[ij] * wcor_u * thick(G.gu, G.dzw, ij, K) * c.dlonu[ij] / c.distu[ij];
+  const bool hasu = j >= 1, hasv = i >= 1, hasw = i >= 1 && j >= 1;
+  const bool inu = j >= 2 && j <= JE - 1 && i >= 1 && i <= IE - 1;
+  const bool inv = j >= 1 && j <= JE - 1 && i >= 2 && i <= IE - 1;
+  const bool inw = j >= 2 && j <= JE - 1 && i >= 2 && i <= IE - 1;
+  // the point's 2D factors, once per column
+  double dtdxuo = 0, dtfu = 0, dlxp0 = 0, dlxp1 = 0, dlxu = 1, cu = 0, dlonu = 0, distu = 1;
+  double dpye = 0, dtfv = 0, dlyp0 = 0, dlyp1 = 0, dlyv = 1, cvv = 0, dlonv = 0, distv = 1;
+  if (inu) {
+    dtdxuo = G.dtdxuo[ij]; dtfu = c.dtfu[ij]; dlxp0 = G.dlxp[ij]; dlxp1 = G.dlxp[ij + 1];
+    dlxu = G.dlxu[ij]; cu = c.cu[ij]; dlonu = c.dlonu[ij]; distu = c.distu[ij];
+  }
+  if (inv) {
+    dpye = G.dpye[ij]; dtfv = c.dtfv[ij]; dlyp0 = G.dlyp[ij]; dlyp1 = G.dlyp[ij + P];
+    dlyv = G.dlyv[ij]; cvv = c.cv[ij]; dlonv = c.dlonv[ij]; distv = c.distv[ij];
+  }
+  // this block's chunk of levels
+  const int K0 = 1 + (int)blockIdx.z * kModmomChunk;
+  const int K1 = min(KE + 1, K0 + kModmomChunk - 1);
+  for (int K = K0; K <= K1; ++K) {
+    const int o = ij + (K - 1) * pl;
+    if (K <= KE) {
+      if (hasu) {
+        double u = ua[o];
+        if (inu) {
+          const double vcor_u =
+              0.25 * ((stabn * va[o] + stabo * vke[o]) + (stabn * va[o + 1] + stabo * vke[o + 1]) +
+                      (stabn * va[o - P] + stabo * vke[o - P]) +
+                      (stabn * va[o + 1 - P] + stabo * vke[o + 1 - P]));
+          const double dd = thick(G.gu, G.dzw, ij, K);
+          u = uko[o] + dtdxuo * (f.po[o] - f.po[o + 1]) * dd + dtfu * vcor_u * wet(G.gu, ij, K);
+          const double w00 = stabn * wa[o] + stabo * wa[o], w01 = stabn * wa[o + pl] + stabo * wa[o + pl];
+          const double w10 = stabn * wa[o + 1] + stabo * wa[o + 1];
+          const double w11 = stabn * wa[o + 1 + pl] + stabo * wa[o + 1 + pl];
+          const double wcor_u = 0.25 * ((w00 + w01) * dlxp0 + (w10 + w11) * dlxp1) / dlxu;
+          u = u - cu * wcor_u * dd * dlonu / distu;
+        }
+        ub[o] = u;
       }
-      ub[o] = u;
+      if (hasv) {
+        double v = va[o];
+        if (inv) {
+          const double ucor_v =
+              0.25 * ((stabn * ua[o] + stabo * uko[o]) + (stabn * ua[o - 1] + stabo * uko[o - 1]) +
+                      (stabn * ua[o + P] + stabo * uko[o + P]) +
+                      (stabn * ua[o - 1 + P] + stabo * uko[o - 1 + P]));
+          const double dd = thick(G.gv, G.dzw, ij, K);
+          v = vke[o] + dpye * (f.po[o + P] - f.po[o]) * dd - dtfv * ucor_v * wet(G.gv, ij, K);
+          const double w00 = stabn * wa[o] + stabo * wa[o], w01 = stabn * wa[o + pl] + stabo * wa[o + pl];
+          const double w10 = stabn * wa[o + P] + stabo * wa[o + P];
+          const double w11 = stabn * wa[o + P + pl] + stabo * wa[o + P + pl];
+          const double wcor_v = 0.25 * ((w00 + w01) * dlyp0 + (w10 + w11) * dlyp1) / dlyv;
+          v = v - cvv * wcor_v * dd * dlonv / distv;
+        }
+        vb[o] = v;
+      }
     }
-    // v-points
-    if (i >= 1) {
-      double v = va[o];
-      if (j >= 1 && j <= JE - 1 && i >= 2 && i <= IE - 1) {
-        const double ucor_v = 0.25 * ((stabn * ua[o] + stabo * uko[o]) + (stabn * ua[o - 1] + stabo * uko[o - 1]) +
-                                      (stabn * ua[o + P] + stabo * uko[o + P]) +
-                                      (stabn * ua[o - 1 + P] + stabo * uko[o - 1 + P]));
-        v = vke[o] + G.dpye[ij] * (f.po[o + P] - f.po[o]) * thick(G.gv, G.dzw, ij, K) -
-            c.dtfv[ij] * ucor_v * wet(G.gv, ij, K);
-        const double w00 = stabn * wa[o] + stabo * wa[o], w01 = stabn * wa[o + pl] + stabo * wa[o + pl];
-        const double w10 = stabn * wa[o + P] + stabo * wa[o + P];
-        const double w11 = stabn * wa[o + P + pl] + stabo * wa[o + P + pl];
-        const double wcor_v = 0.25 * ((w00 + w01) * G.dlyp[ij] + (w10 + w11) * G.dlyp[ij + P]) / G.dlyv[ij];
-        v = v - c.cv[ij] * wcor_v * thick(G.gv, G.dzw, ij, K) * c.dlonv[ij] / c.distv[ij];
-      }
-      vb[o] = v;
+    if (hasw) {
+      double w = wa[o];
+      if (inw && K >= 2 && K <= KE) w = w + dw[o];
+      wb[o] = w;
     }
   }
-  // w-points (K in 1 .. KE+1)
-  if (i >= 1 && j >= 1) {
-    double w = wa[o];
-    if (K >= 2 && K <= KE && j >= 2 && j <= JE - 1 && i >= 2 && i <= IE - 1) {
-      const double dk = thick(G.gp, G.dzw, ij, K) + almzer, dkm = thick(G.gp, G.dzw, ij, K - 1) + almzer;
-      const double ucor_w = 0.25 * ((uko[o] + uko[o - 1]) / dk + (uko[o - pl] + uko[o - 1 - pl]) / dkm);
-      const double vcor_w = 0.25 * ((vke[o] + vke[o - P]) / dk + (vke[o - pl] + vke[o - P - pl]) / dkm);
-      w = w + dt * wet(G.gp, ij, K) * (c.aw[ij] * ucor_w - c.bw[ij] * vcor_w);
-    }
-    wb[o] = w;
+}
+
+// The increment of WN1O in every Coriolis iteration, DT WETO (FTWOW1 dlon /
+// dist UCOR_W - FTWOW1 dlat / dist VCOR_W) (ocmodmom.f90:150-166): it reads
+// only UKO and VKE, which the iterations do not change, so it is formed once
+// (the same value each iteration would form) and added in each.  One thread
+// per interior column (i, j) in [2,IE-1]x[2,JE-1], levels 2..KE.
+__global__ void __launch_bounds__(128) k_modmom_dw(Geo G, CorFields c,
+                                                   const double* __restrict__ uko,
+                                                   const double* __restrict__ vke,
+                                                   double* __restrict__ dw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  if (i > IE - 1 || j > JE - 1) return;
+  const double dt = G.dt, almzer = G.almzer;
+  const int ij = G.L.at2(i, j), P = G.L.P, pl = G.L.plane;
+  const double aw = c.aw[ij], bw = c.bw[ij];
+  double dprev = thick(G.gp, G.dzw, ij, 1) + almzer;
+#pragma unroll 4
+  for (int K = 2; K <= KE; ++K) {
+    const int o = ij + (K - 1) * pl;
+    const double dk = thick(G.gp, G.dzw, ij, K) + almzer;
+    const double ucor_w = 0.25 * ((uko[o] + uko[o - 1]) / dk + (uko[o - pl] + uko[o - 1 - pl]) / dprev);
+    const double vcor_w = 0.25 * ((vke[o] + vke[o - P]) / dk + (vke[o - pl] + vke[o - P - pl]) / dprev);
+    dw[o] = dt * wet(G.gp, ij, K) * (aw * ucor_w - bw * vcor_w);
+    dprev = dk;
   }
 }
 
@@ -368,6 +420,7 @@ __global__ void k_modmom_final(Geo G, BaroArgs b, ThermoFields f, BaroFields bf,
   }
   if (j >= 1) {
     double u1 = 0., us = 0.;
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       u1 = u1 + thick(G.gu, G.dzw, ij, K) * uoo[o];
@@ -385,6 +438,7 @@ __global__ void k_modmom_final(Geo G, BaroArgs b, ThermoFields f, BaroFields bf,
   }
   if (i >= 1) {
     double v1 = 0., vs = 0.;
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       v1 = v1 + thick(G.gv, G.dzw, ij, K) * voe[o];
@@ -453,12 +507,14 @@ __global__ void k_occlit_wo(Geo G, ThermoFields f, const double* __restrict__ uk
   if (i > IE || j > JE) return;
   const int ij = G.L.at2(i, j), pl = G.L.plane;
   double below = wo[ij + KE * pl];
+#pragma unroll 4
   for (int K = KE; K >= 1; --K) {
     const int o = ij + (K - 1) * pl;
     below = occlit_div(G, uko, vke, ij, o, K, below);
     wo[o] = below;
   }
   double slow = 0.;
+#pragma unroll 4
   for (int K = 1; K <= KE; ++K) {
     const int o = ij + (K - 1) * pl;
     slow = slow + f.stabio[o] * G.dt * wo[o];
@@ -479,18 +535,21 @@ __global__ void k_occlit_uv(Geo G, BaroArgs b, BaroFields bf, double* __restrict
   const double stabn = b.stabn;
   if (j >= 2 && j <= JE - 1 && i >= 1 && i <= IE - 1) {
     double px = 0.;
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       px = px + thick(G.gu, G.dzw, ij, K) * G.dtdxuo[ij] * (wpo[o + 1] - wpo[o]) * wet(G.gu, ij, K);
     }
     px = px * bf.deutio[ij];
     double ucos = 0.;
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       const double u = uk1o[o] + stabn * (px - G.dtdxuo[ij] * (wpo[o + 1] - wpo[o])) * thick(G.gu, G.dzw, ij, K);
       ucos = ucos + u;
       uko[o] = u * wet(G.gu, ij, K);
     }
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       uko[o] = uko[o] - ucos * bf.deutio[ij] * thick(G.gu, G.dzw, ij, K);
@@ -498,18 +557,21 @@ __global__ void k_occlit_uv(Geo G, BaroArgs b, BaroFields bf, double* __restrict
   }
   if (j >= 1 && j <= JE - 1 && i >= 2 && i <= IE - 1) {
     double py = 0.;
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       py = py + thick(G.gv, G.dzw, ij, K) * G.dpye[ij] * (wpo[o] - wpo[o + P]) * wet(G.gv, ij, K);
     }
     py = py * bf.deutie[ij];
     double vcos = 0.;
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       const double v = vk1e[o] + stabn * (py - G.dpye[ij] * (wpo[o] - wpo[o + P])) * thick(G.gv, G.dzw, ij, K);
       vcos = vcos + v;
       vke[o] = v * wet(G.gv, ij, K);
     }
+#pragma unroll 4
     for (int K = 1; K <= KE; ++K) {
       const int o = ij + (K - 1) * pl;
       vke[o] = vke[o] - vcos * bf.deutie[ij] * thick(G.gv, G.dzw, ij, K);
@@ -530,6 +592,7 @@ __global__ void k_occlit_wpo(Geo G, BaroArgs b, ThermoFields f, const double* __
   const int ij = G.L.at2(i, j), pl = G.L.plane;
   const double Gr = b.grav, conn = b.conn, stabn = b.stabn, dt = G.dt;
   double slow = 0.;
+#pragma unroll 4
   for (int K = KE; K >= 1; --K) {
     const int o = ij + (K - 1) * pl;
     slow = occlit_div(G, uko, vke, ij, o, K, slow);
@@ -539,6 +602,7 @@ __global__ void k_occlit_wpo(Geo G, BaroArgs b, ThermoFields f, const double* __
   const double brems = under * speed * conn * stabn / (1. + speed);
   const double vorw = 1. - brems;
   double tlow = 0., c = 0.;
+#pragma unroll 4
   for (int K = 2; K <= KE; ++K) {
     const int o = ij + (K - 1) * pl;
     const double ove = wpo[o];
@@ -622,15 +686,22 @@ void launch_stabio_rescale(const Geo& G, const ThermoFields& f, cudaStream_t st)
 void launch_ocmodmom(const Geo& G, const BaroArgs& b, const ThermoFields& f, const CorFields& c,
                      const BaroFields& bf, const double* zo, const double* uoo, const double* voe,
                      double* uko, double* vke, double* uk1o, double* vk1e, double* wno,
-                     double* ub, double* vb, double* wb, cudaStream_t st) {
+                     double* ub, double* vb, double* wb, double* dw, cudaStream_t st) {
   const dim3 blk(32, 8);
   k_modmom_init<<<grid3(G.L.ie + 1, G.L.je + 1, G.L.ke, blk), blk, 0, st>>>(G, b, f, zo, uko, vke, uk1o, vk1e);
   count_launch();
+  const dim3 cb0(32, 4);
+  if (G.L.ie > 2 && G.L.je > 2) {
+    k_modmom_dw<<<grid2(G.L.ie - 2, G.L.je - 2, cb0), cb0, 0, st>>>(G, c, uko, vke, dw);
+    count_launch();
+  }
   // 12 iterations (an even count: the state ends in uk1o, vk1e, wno again)
   double *ua = uk1o, *va = vk1e, *wa = wno, *u2 = ub, *v2 = vb, *w2 = wb;
+  const dim3 cb(32, 4);
   for (int it = 0; it < 12; ++it) {
-    k_modmom_iter<<<grid3(G.L.ie + 1, G.L.je + 1, G.L.ke + 1, blk), blk, 0, st>>>(
-        G, b, f, c, uko, vke, ua, va, wa, u2, v2, w2);
+    dim3 gr = grid2(G.L.ie + 1, G.L.je + 1, cb);
+    gr.z = (G.L.ke + 1 + kModmomChunk - 1) / kModmomChunk;
+    k_modmom_iter<<<gr, cb, 0, st>>>(G, b, f, c, uko, vke, dw, ua, va, wa, u2, v2, w2);
     count_launch();
     std::swap(ua, u2);
     std::swap(va, v2);

@@ -2284,15 +2284,17 @@ int r_ocmodmom(orctm_handle* h) {
   if ((st = compute_after_copies(h)) || (st = own_buffer(h, ORCTM_F_UKO)) ||
       (st = own_buffer(h, ORCTM_F_VKE)) || (st = own_buffer(h, ORCTM_F_WNO)))
     return st;
-  double *ub, *vb, *wb;
-  if ((st = h->alloc(&ub)) || (st = h->alloc(&vb)) || (st = h->alloc(&wb))) return st;
+  double *ub, *vb, *wb, *dw;
+  if ((st = h->alloc(&ub)) || (st = h->alloc(&vb)) || (st = h->alloc(&wb)) || (st = h->alloc(&dw)))
+    return st;
   launch_ocmodmom(h->G, h->baro, h->tf, h->cf, h->bf, h->zo, h->slot[ORCTM_F_UOO],
                   h->slot[ORCTM_F_VOE], h->slot[ORCTM_F_UKO], h->slot[ORCTM_F_VKE], h->uk1o,
-                  h->vk1e, h->slot[ORCTM_F_WNO], ub, vb, wb, h->stream);
+                  h->vk1e, h->slot[ORCTM_F_WNO], ub, vb, wb, dw, h->stream);
   const cudaError_t e = cudaGetLastError();
   h->unref(ub);  // stream-ordered: a later user of the buffer runs after these launches
   h->unref(vb);
   h->unref(wb);
+  h->unref(dw);
   ORCTM_CUDA_OK(e);
   return ORCTM_OK;
 }

@@ -112,7 +112,7 @@ void launch_stabio_rescale(const Geo& G, const ThermoFields& f, cudaStream_t st)
 void launch_ocmodmom(const Geo& G, const BaroArgs& b, const ThermoFields& f, const CorFields& c,
                      const BaroFields& bf, const double* zo, const double* uoo, const double* voe,
                      double* uko, double* vke, double* uk1o, double* vk1e, double* wno,
-                     double* ub, double* vb, double* wb, cudaStream_t st);
+                     double* ub, double* vb, double* wb, double* dw, cudaStream_t st);
 // OCCLIT; scratch: wpo, t1o (3D), bruva, contrij (2D); *contra receives the
 // sum of CONTRIJ (device scalar)
 void launch_occlit(const Geo& G, const BaroArgs& b, const ThermoFields& f, const BaroFields& bf,
