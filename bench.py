@@ -373,6 +373,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-whole-step", action="store_true",
                     help="skip the whole-step (orctm_step_full) measurement")
+    ap.add_argument("--tuning", type=lambda s: tuple(int(v) for v in s.split(",")), default=None,
+                    help="COL,SPMV: pin the FP64 Poisson kernel variants instead of autotuning "
+                         "(profiling a given variant)")
+    ap.add_argument("--nvtx", action="store_true",
+                    help="wrap the event-timed FP64 steps (every solver iteration launched "
+                         "on its own) in the NVTX range fp64_steps, for an ncu launch list "
+                         "(--nvtx --nvtx-include fp64_steps/)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-sample", type=lambda s: tuple(int(v) for v in s.split("x")),
                     default=None, help="sub-domain the CPU restatement times (default: the "
@@ -397,6 +404,8 @@ def main():
     gpu = Instance(inst, device=local)
     gpu.upload_state(configs.copy_state(inst))
     gpu.set_solver("fp64", rtol=1e-10, maxit=5000)
+    if args.tuning:
+        gpu.set_tuning(*args.tuning)
     for _ in range(args.warmup):
         gpu.step_hotpath()
 
@@ -404,7 +413,13 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     gpu.set_profiling(True)
+    if args.nvtx:
+        import torch
+
+        torch.cuda.nvtx.range_push("fp64_steps")
     ms, stats, launches = timed_steps(gpu, args.steps, pg)
+    if args.nvtx:
+        torch.cuda.nvtx.range_pop()
     prof = gpu.profile()
     gpu.set_profiling(False)
     ck = clocks.stop()
