@@ -185,8 +185,9 @@ template <typename T>
 bool pcg_col_variant_ok(const Geo& G, int variant);
 int pcg_spmv_variants();
 bool pcg_spmv_variant_ok(int variant);
-void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b,
-                  const double* x, double* r, cudaStream_t st);
+// r = b - A x in double-double, and x := 0 on land rows (their solution)
+void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b, double* x,
+                  double* r, cudaStream_t st);
 void launch_axpy_f64(const Geo& G, const double* d, double* x, cudaStream_t st);
 void launch_scale_to_f32(const Geo& G, const double* r, const SolverState* S, float* r32,
                          cudaStream_t st);

@@ -323,14 +323,18 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
     const int kb = c.kb;
     T yprev = 0, dprev = 0;
     const unsigned base = (unsigned)G.L.at(i, j, 0), plane = (unsigned)G.L.plane;
-    // U: levels whose loads are issued together
+    // U: levels whose loads are issued together.  Levels below the bottom
+    // (K > kb) are land rows: decoupled, right-hand side 0, so every vector
+    // holds exact zeros there (k_resid clears x) and their dot terms are +0;
+    // they are neither loaded nor stored, while the lanes of a warp still
+    // march the levels together (their loads stay coalesced).
     for (int K0 = 1; K0 <= KE; K0 += U) {
       T lb[U], lr[U], lp[U], lq[U], lx[U], ld[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int K = K0 + u;
         lb[u] = lr[u] = lp[u] = lq[u] = lx[u] = ld[u] = T(0);
-        if (K <= KE) {
+        if (K <= kb) {
           const unsigned o = base + plane * (unsigned)(K - 1);
           if (MODE == 1) {
             lb[u] = b[o];
@@ -358,20 +362,21 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
         }
         const unsigned o = base + plane * (unsigned)(K - 1);
         T rk;
+        const bool wetk = K <= kb;
         if (MODE == 1) {
           rk = (T)((double)lb[u] * izp_of(c, P, K));
           bbt = fma(rk, rk, bbt);
         } else {
-          x[o] = fma(alpha, lp[u], lx[u]);
+          if (wetk) x[o] = fma(alpha, lp[u], lx[u]);
           rk = fma(-alpha, lq[u], lr[u]);
         }
-        r[o] = rk;
+        if (wetk) r[o] = rk;
         rrt = fma(rk, rk, rrt);
         // a(K) of B: ZW(K) above a wet level below the surface
         const T up = (K == 1 || K > kb) ? T(0) : (K == kb ? zwa : szw[K - 1]);
         const T yt = fma(-(up * dprev), yprev, rk);
         if (SM) ys[(K - 1) * nt + tid] = yt;
-        else z[o] = yt;  // y kept in z until the backward sweep
+        else if (wetk) z[o] = yt;  // y kept in z until the backward sweep
         yprev = yt;
         dprev = ld[u];
         rzt = fma(yt * yt, dprev, rzt);
@@ -387,7 +392,7 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
       for (int u = 0; u < U; ++u) {
         const int K = K1 - u;
         ly[u] = ld[u] = T(0);
-        if (K >= 1) {
+        if (K >= 1 && K <= kb) {
           const unsigned o = base + plane * (unsigned)(K - 1);
           ly[u] = SM ? ys[(K - 1) * nt + tid] : z[o];
           ld[u] = (T)dinv[o];
@@ -400,7 +405,7 @@ __global__ void __launch_bounds__(128) k_pcg_col(Geo G, PoissonGeo P, SolverStat
         // c(K) of B: ZW(K+1) when level K+1 is wet
         const T dn = (K >= kb || K == KE) ? T(0) : (K + 1 == kb ? zwa : szw[K]);
         const T zt = fma(-dn, znext, ly[u]) * ld[u];
-        z[base + plane * (unsigned)(K - 1)] = zt;
+        if (K <= kb) z[base + plane * (unsigned)(K - 1)] = zt;
         znext = zt;
       }
     }
@@ -456,6 +461,16 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
   const int i = i0 + tx, j = j0 + ty;
   const bool act = i <= IE - 1 && j <= JE - 1;
   const T beta = first ? T(0) : (T)S->beta;
+  // the deepest wet level of the block's columns: below it every cell of the
+  // block is a land row, whose p and q are exact zeros already in memory and
+  // whose dot terms are +0, so the march stops there (loads go one level
+  // further, for the level below the deepest wet row)
+  __shared__ int skmax;
+  if (tid == 0) skmax = 0;
+  __syncthreads();
+  if (act) atomicMax(&skmax, (int)G.gp.kb[G.L.at2(i, j)]);
+  __syncthreads();
+  const int kmax = skmax, klim = min(KE, kmax + 1);
   // halo-tile entries this thread fills: offsets at level 1, validity
   unsigned fo[kF];
   int fs[kF];
@@ -477,7 +492,7 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
     for (int f = 0; f < kF; ++f) {
       qz[slot][f] = T(0);
       qp[slot][f] = T(0);
-      if (fv[f] && K <= KE) {
+      if (fv[f] && K <= klim) {
         const unsigned o = fo[f] + plane * (unsigned)(K - 1);
         qz[slot][f] = z[o];
         if (!first) qp[slot][f] = pold[o];
@@ -564,9 +579,9 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
     cur = nxt;
     nxt = t;
   };
-  for (int K = 1; K <= KE; K += 2) {
+  for (int K = 1; K <= kmax; K += 2) {
     level(K, std::integral_constant<int, 0>{});
-    if (K + 1 <= KE) level(K + 1, std::integral_constant<int, 1>{});
+    if (K + 1 <= kmax) level(K + 1, std::integral_constant<int, 1>{});
   }
   pq += (double)pqt;
   double v[1] = {pq};
@@ -1008,7 +1023,7 @@ __device__ __forceinline__ void dd_sub_prod(DD& s, double c, double x) {
 
 __global__ void __launch_bounds__(128) k_resid(Geo G, PoissonGeo P, SolverState* S,
                                                const double* __restrict__ b,
-                                               const double* __restrict__ x,
+                                               double* __restrict__ x,
                                                double* __restrict__ r) {
   const int KE = G.L.ke, IE = G.L.ie, JE = G.L.je;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -1016,8 +1031,13 @@ __global__ void __launch_bounds__(128) k_resid(Geo G, PoissonGeo P, SolverState*
   double rr = 0.0, bb = 0.0;
   if (i <= IE - 1 && j <= JE - 1) {
     const ColC c = load_col(G, P, i, j);
+    // land rows (K > kb): diagonal only with a zero right-hand side, so the
+    // solution there is 0; x is set to it and r (0) is not stored, which
+    // keeps every solver vector exactly 0 on land for the PCG kernels
+    for (int K = c.kb + 1; K <= KE; ++K)
+      if (AT(x, i, j, K) != 0.0) AT(x, i, j, K) = 0.0;
     double xm = 0.0, x0 = AT(x, i, j, 1), xp = 0.0;
-    for (int K = 1; K <= KE; ++K) {
+    for (int K = 1; K <= c.kb; ++K) {
       xp = K < KE ? AT(x, i, j, K + 1) : 0.0;
       const Coef rw = row<false>(c, P, K, KE);
       const double bk = AT(b, i, j, K);
@@ -1336,8 +1356,8 @@ template cudaError_t launch_pcg_spmv<float>(const Geo&, const PoissonGeo&, Solve
                                             const float*, const float*, float*, float*, int, int,
                                             cudaStream_t);
 
-void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b,
-                  const double* x, double* r, cudaStream_t st) {
+void launch_resid(const Geo& G, const PoissonGeo& P, SolverState* S, const double* b, double* x,
+                  double* r, cudaStream_t st) {
   k_resid<<<grid2(G.L.ie - 2, G.L.je - 2, kColBlock), kColBlock, 0, st>>>(G, P, S, b, x, r);
   count_launch();
 }

@@ -1,4 +1,5 @@
-"""orctm_octdiff_noalloc, the scratch-free entry point, against orctm_octdiff.
+"""orctm_octdiff_noalloc, the scratch-free entry point, against orctm_octdiff
+and against the oracle.
 
 The entry point exists for callers that may not allocate device memory (code
 under CUDA graph capture, hosts whose device memory belongs to another
@@ -6,15 +7,17 @@ runtime); it keeps its scratch in a fixed array inside the library.  This
 test allocates the input and output arrays itself (with torch), calls the
 entry point through the C ABI twice in a row for every tracer -- the second
 call reuses the scratch array the first one left behind -- and compares each
-result with the handle-based orctm_octdiff at the tolerance of the other
-parity tests.  It also checks that a grid beyond the fixed limit is refused.
-This file is collected last on purpose.
+result with the handle-based orctm_octdiff and with the oracle's OCTDIFF at
+the tolerance of the other parity tests, on a c2 box and a c1 slice.  It
+also checks that a grid beyond the fixed limit is refused.  This file is
+collected last on purpose.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
 
+import oracle as O
 from orctm_b200 import _lib
 from orctm_b200 import configs
 from orctm_b200.api import Instance
@@ -38,17 +41,21 @@ class Args(C.Structure):
                 ("dlyv", C.c_void_p), ("zo", C.c_void_p), ("stream", C.c_void_p)]
 
 
-def test_octdiff_noalloc_matches_handle_path():
+@pytest.mark.parametrize("case", ["c2s", "c1s"])
+def test_octdiff_noalloc_matches_handle_path_and_oracle(case):
     import torch
 
     lib = _lib.load()
     lib.orctm_octdiff_noalloc.argtypes = [C.POINTER(Args)]
-    inst = instance("c2s")
+    inst = instance(case)
     st = configs.copy_state(inst)
     with Instance(inst) as gpu:
         gpu.upload_state(st)
         gpu.octdiff()
         want = [gpu.download(f"tracer{n}") for n in range(gpu.ntr)]
+    # the oracle's OCTDIFF_BASE + OCTDIFF_TS on the same inputs
+    ref = [np.array(t, order="F", copy=True) for t in st["tracers"]]
+    O.Oracle(inst).octdiff(ref, np.asfortranarray(st["dvo"]), np.asfortranarray(st["zo"]))
 
     def dev(a):
         return torch.from_numpy(np.ascontiguousarray(np.ravel(a, order="F"))).to("cuda")
@@ -74,6 +81,7 @@ def test_octdiff_noalloc_matches_handle_path():
             torch.cuda.synchronize()
             got = tout.cpu().numpy().reshape(shape, order="F")
             assert_close(got, want[n], TOL, f"call {call}, tracer {n}")
+            assert_close(got, ref[n], TOL, f"call {call}, tracer {n} against the oracle")
 
     big = Args()
     C.pointer(big)[0] = a
