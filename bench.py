@@ -460,11 +460,11 @@ def main():
     hbm, peak_kind = peaks()
     top = max((k for k in prof if prof[k]["launches"] > 0), key=lambda k: prof[k]["ms"])
     per_launch_ms = prof[top]["ms"] / prof[top]["launches"]
-    # the solver kernels skip land rows (K > kb: decoupled, exact zeros), so
-    # their algorithmic bytes count the wet unknowns only
+    # algorithmic bytes per cell x the cells of a launch; the solver kernels
+    # skip the land rows among them (decoupled, exact zeros), which the
+    # measured traffic shows
     wet = int(np.asarray(inst["weto"])[1:-1, 1:-1, :].sum())
-    basis = wet if top in ("pcg_col", "pcg_spmv", "resid") else cells
-    bpl = BYTES_PER_CELL_F64.get(top, 0) * basis
+    bpl = BYTES_PER_CELL_F64.get(top, 0) * cells
     achieved = bpl / (per_launch_ms / 1e3) / 1e9
     traffic = None
     try:
@@ -483,8 +483,8 @@ def main():
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind ==
                 "measured" else "fallback 6.65 TB/s",
                 "bytes_per_launch": bpl, "avg_launch_ms": per_launch_ms,
-                "bytes_basis": ("wet unknowns (%d of %d cells; land rows are skipped)" % (wet, cells))
-                               if basis == wet else "all cells",
+                "bytes_basis": "all cells (%d; of them %d wet: the solver kernels skip the "
+                               "land rows' loads and stores)" % (cells, wet),
                 "breakdown_ms_per_step": {k: round(v["ms"] / args.steps, 3) for k, v in prof.items()},
                 "algorithmic_bytes_per_cell": BYTES_PER_CELL_F64}
 

@@ -471,9 +471,10 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
   if (act) atomicMax(&skmax, (int)G.gp.kb[G.L.at2(i, j)]);
   __syncthreads();
   const int kmax = skmax, klim = min(KE, kmax + 1);
-  // halo-tile entries this thread fills: offsets at level 1, validity
+  // halo-tile entries this thread fills: offsets at level 1, validity, and
+  // the entry's wet levels (below them the values are exact zeros)
   unsigned fo[kF];
-  int fs[kF];
+  int fs[kF], fk[kF];
   bool fv[kF];
 #pragma unroll
   for (int f = 0; f < kF; ++f) {
@@ -483,6 +484,7 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
     fs[f] = e < kH ? e : -1;
     fv[f] = e < kH && ii >= 2 && ii <= IE - 1 && jj >= 2 && jj <= JE - 1;
     fo[f] = fv[f] ? (unsigned)G.L.at(ii, jj, 0) : 0u;
+    fk[f] = fv[f] ? (int)G.gp.kb[G.L.at2(ii, jj)] : 0;
   }
   // the halo values of two levels ahead are held in registers, so the loads of
   // level K+3 are in flight while level K is computed
@@ -492,7 +494,7 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
     for (int f = 0; f < kF; ++f) {
       qz[slot][f] = T(0);
       qp[slot][f] = T(0);
-      if (fv[f] && K <= klim) {
+      if (fv[f] && K <= klim && K <= fk[f]) {
         const unsigned o = fo[f] + plane * (unsigned)(K - 1);
         qz[slot][f] = z[o];
         if (!first) qp[slot][f] = pold[o];
@@ -517,6 +519,7 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
     kreg = c.kreg;
   }
   const unsigned own = act ? (unsigned)G.L.at(i, j, 0) : 0u;
+  const int kown = act ? (int)c.kb : 0;
   const int me = (ty + 1) * kHx + (tx + 1);
   T* prv = ring[0];
   T* cur = ring[1];
@@ -566,8 +569,10 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
         s = fma((T)rw.d, pd, s);
       }
       const unsigned o = own + plane * (unsigned)(K - 1);
-      pnew[o] = p0;
-      q[o] = s;
+      if (K <= kown) {  // land rows keep their zeros
+        pnew[o] = p0;
+        q[o] = s;
+      }
       pqt = fma(p0, s, pqt);
       if ((K & 7) == 0) {
         pq += (double)pqt;
