@@ -539,7 +539,9 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
     store(nxt, SA);
     load(SA, K + 3);
     __syncthreads();
-    if (act) {
+    // land rows of this column (K > kown): p = 0, q = 0 stays in memory and
+    // the dot term is +0, so nothing is formed there
+    if (act && K <= kown) {
       const T p0 = cur[me];
       const T pu = prv[me], pn = cur[me - kHx], pw = cur[me - 1], pe = cur[me + 1];
       const T ps = cur[me + kHx], pd = nxt[me];
@@ -569,10 +571,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_pcg_spmv(Geo G, PoissonGeo P, Sol
         s = fma((T)rw.d, pd, s);
       }
       const unsigned o = own + plane * (unsigned)(K - 1);
-      if (K <= kown) {  // land rows keep their zeros
-        pnew[o] = p0;
-        q[o] = s;
-      }
+      pnew[o] = p0;
+      q[o] = s;
       pqt = fma(p0, s, pqt);
       if ((K & 7) == 0) {
         pq += (double)pqt;
