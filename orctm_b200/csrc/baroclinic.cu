@@ -496,6 +496,23 @@ __device__ __forceinline__ double occlit_div(const Geo& G, const double* uko, co
                       G.dtdyo[ij] * (vke[o] * G.dlxv[ij] - vke[o - P] * G.dlxv[ij - P]) / G.dlxp[ij]);
 }
 
+// the column's metrics of occlit_div, loaded once, and the same expression on
+// loaded velocities: ua = UKO(I-1), ub = UKO(I), va = VKE(J), vb = VKE(J-1)
+struct DivMetrics {
+  double dti, dtdxpo, dlyuw, dlyue, dlyp, dtdyo, dlxvs, dlxvn, dlxp;
+};
+__device__ __forceinline__ DivMetrics div_metrics(const Geo& G, int ij) {
+  const int P = G.L.P;
+  return DivMetrics{G.dti, G.dtdxpo[ij], G.dlyu[ij - 1], G.dlyu[ij], G.dlyp[ij],
+                    G.dtdyo[ij], G.dlxv[ij], G.dlxv[ij - P], G.dlxp[ij]};
+}
+__device__ __forceinline__ double div_term(const DivMetrics& m, double w, double ua, double ub,
+                                           double va, double vb, double below) {
+  return below + m.dti * w *
+                     (m.dtdxpo * (ua * m.dlyuw - ub * m.dlyue) / m.dlyp +
+                      m.dtdyo * (va * m.dlxvs - vb * m.dlxvn) / m.dlxp);
+}
+
 // WO bottom up, then the running sum WPO top down (occlit.f90:104-127); one
 // thread per p-column
 __global__ void k_occlit_wo(Geo G, ThermoFields f, const double* __restrict__ uko,
@@ -524,59 +541,82 @@ __global__ void k_occlit_wo(Geo G, ThermoFields f, const double* __restrict__ uk
 
 // One velocity update of the OCCLIT iteration (occlit.f90:139-228): one
 // thread per (i, j) in [0,IE]x[0,JE] doing the u- and v-columns there
+// One velocity column of the OCCLIT update: PXOIN (or PYEIN) as the
+// vertical sum of the WPO gradient, the new velocity per level and its
+// vertical sum, then the correction.  The WPO difference is wpo[o + oa] -
+// wpo[o + ob] (u: (I+1) - I, v: J - (J+1)); metric is DTDXUO or DPYE, deut
+// DEUTIO or DEUTIE.  The loads of U levels are issued together before they
+// are used; the sums run level by level in the reference's order.
+template <int U>
+__device__ __forceinline__ void occlit_column(const Geo& G, const ColGeo& cg, int ij, int oa, int ob,
+                                              double metric, double deut, double stabn,
+                                              const double* __restrict__ wpo,
+                                              const double* __restrict__ k1, double* __restrict__ k) {
+  const int KE = G.L.ke, pl = G.L.plane;
+  double px = 0.;
+  for (int K0 = 1; K0 <= KE; K0 += U) {
+    double wa[U], wb[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int o = ij + (K0 + u - 1) * pl;
+      wa[u] = K0 + u <= KE ? wpo[o + oa] : 0.0;
+      wb[u] = K0 + u <= KE ? wpo[o + ob] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 + u;
+      if (K > KE) break;
+      px = px + thick(cg, G.dzw, ij, K) * metric * (wa[u] - wb[u]) * wet(cg, ij, K);
+    }
+  }
+  px = px * deut;
+  double cos_ = 0.;
+  for (int K0 = 1; K0 <= KE; K0 += U) {
+    double wa[U], wb[U], l1[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int o = ij + (K0 + u - 1) * pl;
+      const bool ok = K0 + u <= KE;
+      wa[u] = ok ? wpo[o + oa] : 0.0;
+      wb[u] = ok ? wpo[o + ob] : 0.0;
+      l1[u] = ok ? k1[o] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 + u;
+      if (K > KE) break;
+      const double v = l1[u] + stabn * (px - metric * (wa[u] - wb[u])) * thick(cg, G.dzw, ij, K);
+      cos_ = cos_ + v;
+      k[ij + (K - 1) * pl] = v * wet(cg, ij, K);
+    }
+  }
+  for (int K0 = 1; K0 <= KE; K0 += U) {
+    double lk[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) lk[u] = K0 + u <= KE ? k[ij + (K0 + u - 1) * pl] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 + u;
+      if (K > KE) break;
+      k[ij + (K - 1) * pl] = lk[u] - cos_ * deut * thick(cg, G.dzw, ij, K);
+    }
+  }
+}
+
+// One velocity update of the OCCLIT iteration (occlit.f90:139-228): one
+// thread per (i, j) in [0,IE]x[0,JE] doing the u- and v-columns there
 __global__ void k_occlit_uv(Geo G, BaroArgs b, BaroFields bf, double* __restrict__ uko,
                             double* __restrict__ vke, const double* __restrict__ uk1o,
                             const double* __restrict__ vk1e, const double* __restrict__ wpo) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
+  const int IE = G.L.ie, JE = G.L.je;
   if (i > IE || j > JE) return;
-  const int ij = G.L.at2(i, j), pl = G.L.plane, P = G.L.P;
-  const double stabn = b.stabn;
-  if (j >= 2 && j <= JE - 1 && i >= 1 && i <= IE - 1) {
-    double px = 0.;
-#pragma unroll 4
-    for (int K = 1; K <= KE; ++K) {
-      const int o = ij + (K - 1) * pl;
-      px = px + thick(G.gu, G.dzw, ij, K) * G.dtdxuo[ij] * (wpo[o + 1] - wpo[o]) * wet(G.gu, ij, K);
-    }
-    px = px * bf.deutio[ij];
-    double ucos = 0.;
-#pragma unroll 4
-    for (int K = 1; K <= KE; ++K) {
-      const int o = ij + (K - 1) * pl;
-      const double u = uk1o[o] + stabn * (px - G.dtdxuo[ij] * (wpo[o + 1] - wpo[o])) * thick(G.gu, G.dzw, ij, K);
-      ucos = ucos + u;
-      uko[o] = u * wet(G.gu, ij, K);
-    }
-#pragma unroll 4
-    for (int K = 1; K <= KE; ++K) {
-      const int o = ij + (K - 1) * pl;
-      uko[o] = uko[o] - ucos * bf.deutio[ij] * thick(G.gu, G.dzw, ij, K);
-    }
-  }
-  if (j >= 1 && j <= JE - 1 && i >= 2 && i <= IE - 1) {
-    double py = 0.;
-#pragma unroll 4
-    for (int K = 1; K <= KE; ++K) {
-      const int o = ij + (K - 1) * pl;
-      py = py + thick(G.gv, G.dzw, ij, K) * G.dpye[ij] * (wpo[o] - wpo[o + P]) * wet(G.gv, ij, K);
-    }
-    py = py * bf.deutie[ij];
-    double vcos = 0.;
-#pragma unroll 4
-    for (int K = 1; K <= KE; ++K) {
-      const int o = ij + (K - 1) * pl;
-      const double v = vk1e[o] + stabn * (py - G.dpye[ij] * (wpo[o] - wpo[o + P])) * thick(G.gv, G.dzw, ij, K);
-      vcos = vcos + v;
-      vke[o] = v * wet(G.gv, ij, K);
-    }
-#pragma unroll 4
-    for (int K = 1; K <= KE; ++K) {
-      const int o = ij + (K - 1) * pl;
-      vke[o] = vke[o] - vcos * bf.deutie[ij] * thick(G.gv, G.dzw, ij, K);
-    }
-  }
+  const int ij = G.L.at2(i, j), P = G.L.P;
+  if (j >= 2 && j <= JE - 1 && i >= 1 && i <= IE - 1)
+    occlit_column<4>(G, G.gu, ij, 1, 0, G.dtdxuo[ij], bf.deutio[ij], b.stabn, wpo, uk1o, uko);
+  if (j >= 1 && j <= JE - 1 && i >= 2 && i <= IE - 1)
+    occlit_column<4>(G, G.gv, ij, 0, P, G.dpye[ij], bf.deutie[ij], b.stabn, wpo, vk1e, vke);
 }
 
 // The WPO update of the OCCLIT iteration (occlit.f90:238-284): T1O bottom up
@@ -585,32 +625,60 @@ __global__ void k_occlit_wpo(Geo G, BaroArgs b, ThermoFields f, const double* __
                              const double* __restrict__ vke, const double* __restrict__ wo,
                              const double* __restrict__ bruva, double* __restrict__ wpo,
                              double* __restrict__ t1o, double* __restrict__ contrij, double under) {
+  constexpr int U = 4;  // levels whose loads are issued together
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const int ij = G.L.at2(i, j), pl = G.L.plane;
+  const int ij = G.L.at2(i, j), pl = G.L.plane, P = G.L.P;
   const double Gr = b.grav, conn = b.conn, stabn = b.stabn, dt = G.dt;
+  const DivMetrics m = div_metrics(G, ij);
   double slow = 0.;
-#pragma unroll 4
-  for (int K = KE; K >= 1; --K) {
-    const int o = ij + (K - 1) * pl;
-    slow = occlit_div(G, uko, vke, ij, o, K, slow);
-    t1o[o] = slow;
+  for (int K0 = KE; K0 >= 1; K0 -= U) {
+    double ua[U], ub[U], va[U], vb[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int o = ij + (K0 - u - 1) * pl;
+      const bool ok = K0 - u >= 1;
+      ua[u] = ok ? uko[o - 1] : 0.0;
+      ub[u] = ok ? uko[o] : 0.0;
+      va[u] = ok ? vke[o] : 0.0;
+      vb[u] = ok ? vke[o - P] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 - u;
+      if (K < 1) break;
+      slow = div_term(m, wet(G.gp, ij, K), ua[u], ub[u], va[u], vb[u], slow);
+      t1o[ij + (K - 1) * pl] = slow;
+    }
   }
   const double speed = 2. * Gr * bruva[ij] * (G.dtdxuo[ij] * G.dtdxuo[ij] + G.dtdyo[ij] * G.dtdyo[ij]);
   const double brems = under * speed * conn * stabn / (1. + speed);
   const double vorw = 1. - brems;
   double tlow = 0., c = 0.;
-#pragma unroll 4
-  for (int K = 2; K <= KE; ++K) {
-    const int o = ij + (K - 1) * pl;
-    const double ove = wpo[o];
-    tlow = tlow + Gr * f.stabio[o] * dt * (conn * t1o[o] + wo[o]);
-    const double w = vorw * tlow + brems * ove;
-    wpo[o] = w;
-    const double d = ove - w;
-    c = c + d * d;
+  for (int K0 = 2; K0 <= KE; K0 += U) {
+    double ls[U], lt[U], lw[U], lp[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int o = ij + (K0 + u - 1) * pl;
+      const bool ok = K0 + u <= KE;
+      ls[u] = ok ? f.stabio[o] : 0.0;
+      lt[u] = ok ? t1o[o] : 0.0;
+      lw[u] = ok ? wo[o] : 0.0;
+      lp[u] = ok ? wpo[o] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int K = K0 + u;
+      if (K > KE) break;
+      const double ove = lp[u];
+      tlow = tlow + Gr * ls[u] * dt * (conn * lt[u] + lw[u]);
+      const double w = vorw * tlow + brems * ove;
+      wpo[ij + (K - 1) * pl] = w;
+      const double d = ove - w;
+      c = c + d * d;
+    }
   }
   contrij[ij] = c;
 }
