@@ -118,6 +118,43 @@ def read_obc_files(dirname: str, ie: int, je: int, ob: dict, ntide: int, variabl
     return amp, pha
 
 
+def read_model_records(path: str):
+    """The records of a model input file as the reference's experiments write
+    them (grid file arcgri, coordinates anta, initial INITEM / INISAL, daily
+    forcing GI*; BT_forc/mkgrid.f90): Fortran sequential unformatted records,
+    big-endian (-convert big_endian, Makefile:75), in pairs of a header of
+    four 8-byte integers (IDATE, CODE, LEVEL, N) and N 8-byte reals.  Returns
+    [((idate, code, level, n), values)]."""
+    data = open(path, "rb").read()
+    pos = 0
+
+    def record():
+        nonlocal pos
+        if pos + 4 > len(data):
+            raise ValueError(f"{path}: truncated record marker at byte {pos}")
+        n = int(np.frombuffer(data, ">i4", 1, pos)[0])
+        if n < 0 or pos + 8 + n > len(data):
+            raise ValueError(f"{path}: record of {n} bytes at byte {pos} runs past the end")
+        tail = int(np.frombuffer(data, ">i4", 1, pos + 4 + n)[0])
+        if tail != n:
+            raise ValueError(f"{path}: record markers differ at byte {pos}")
+        payload = data[pos + 4:pos + 4 + n]
+        pos += n + 8
+        return payload
+
+    out = []
+    while pos < len(data):
+        hdr = record()
+        if len(hdr) != 32:
+            raise ValueError(f"{path}: header record of {len(hdr)} bytes, expected 32")
+        h = tuple(int(v) for v in np.frombuffer(hdr, ">i8"))
+        vals = record()
+        if len(vals) != 8 * h[3]:
+            raise ValueError(f"{path}: {len(vals)} bytes of values, header says {h[3]} reals")
+        out.append((h, np.frombuffer(vals, ">f8").astype(np.float64)))
+    return out
+
+
 def read_ts_profile(path: str, ke: int) -> np.ndarray:
     """A reference stratification profile (TRef.bin / SRef.bin): KE values,
     one per level from the surface down, each read by its own READ of a
