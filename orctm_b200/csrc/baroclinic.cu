@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(128) k_modmom_iter(Geo G, BaroArgs b, ThermoFi
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
   if (i > IE || j > JE) return;
-  const double stabn = b.stabn, stabo = 1. - b.stabn, dt = G.dt, almzer = G.almzer;
+  const double stabn = b.stabn, stabo = 1. - b.stabn;
   const int ij = G.L.at2(i, j);
   const int P = G.L.P, pl = G.L.plane;
   const bool hasu = j >= 1, hasv = i >= 1, hasw = i >= 1 && j >= 1;

@@ -573,7 +573,12 @@ __global__ void __launch_bounds__(kVertBlock) k_visc_uv_b(Geo G, const double* _
   }
 }
 
-// k_visc_w with the loads of U levels issued together (bit for bit the same)
+// implicit vertical diffusion of w, levels 2..KE (ocvisc.f90:225-270).  One
+// forward sweep forms each level's coefficients, eliminates (the multiplier
+// TRIDSY(K-1,1)/TRIDSY(K-1,2) and the new diagonal, in the reference's
+// operation order) and substitutes; only the eliminated diagonal is kept per
+// level, and the backward sweep recomputes TRIDSY(K,3) by the same expression.
+// The loads of U levels are issued together (the results do not depend on U).
 template <int U>
 __global__ void __launch_bounds__(kVertBlock) k_visc_w_b(Geo G, const double* __restrict__ W,
                                                          const double* __restrict__ avo,
@@ -655,65 +660,6 @@ __global__ void __launch_bounds__(kVertBlock) k_visc_w_b(Geo G, const double* __
       nxt = div_nr((ly[u] - t3 * nxt) * wet(G.gp, ij, K), t2p[K - 1]);
       O[base + (K - 1) * pl] = nxt;
     }
-  }
-}
-
-// implicit vertical diffusion of w, levels 2..KE (ocvisc.f90:225-270).  One
-// forward sweep forms each level's coefficients, eliminates (the multiplier
-// TRIDSY(K-1,1)/TRIDSY(K-1,2) and the new diagonal, in the reference's
-// operation order) and substitutes; only the eliminated diagonal is kept per
-// level, and the backward sweep recomputes TRIDSY(K,3) by the same expression.
-__global__ void __launch_bounds__(kVertBlock) k_visc_w(Geo G, const double* __restrict__ W,
-                                                       const double* __restrict__ avo,
-                                                       double* __restrict__ O) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int IE = G.L.ie, JE = G.L.je, KE = G.L.ke;
-  if (i > IE || j > JE) return;
-  const bool interior = i >= 2 && i <= IE - 1 && j >= 2 && j <= JE - 1 && KE >= 2;
-  if (!interior) {
-    for (int K = 1; K <= KE + 1; ++K) AT(O, i, j, K) = AT(W, i, j, K);
-    return;
-  }
-  const int ij = G.L.at2(i, j);
-  auto den = [&](int K) {
-    return 2.0 * G.almzer + thick(G.gp, G.dzw, ij, K - 1) + thick(G.gp, G.dzw, ij, K);
-  };
-  auto tri1 = [&](int K, double dn) {
-    const double avup = 0.5 * (AT(avo, i, j, K - 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K - 1);
-    return div_nr(-2.0 * G.dt * avup * wet(G.gp, ij, K) * G.di[K - 2], dn);
-  };
-  auto tri3 = [&](int K, double dn) {
-    const double avlo =
-        K < KE ? 0.5 * (AT(avo, i, j, K + 1) + AT(avo, i, j, K)) * wet(G.gp, ij, K) : 0.0;
-    return div_nr(-2.0 * G.dt * avlo * wet(G.gp, ij, K) * G.di[K - 1], dn);
-  };
-  double t2p[kMaxKe];
-  AT(O, i, j, 1) = AT(W, i, j, 1);
-  AT(O, i, j, KE + 1) = AT(W, i, j, KE + 1);
-  double prev = 0.0, t2prev = 1.0, t3prev = 0.0;
-  for (int K = 2; K <= KE; ++K) {
-    const double dn = den(K);
-    const double t1 = tri1(K, dn), t3 = tri3(K, dn);
-    double t2 = 1. - t1 - t3;
-    double y = AT(W, i, j, K);
-    if (K >= 3) {
-      const double m = div_nr(t1, t2prev);
-      t2 = t2 - div_nr(t3prev * t1, t2prev);
-      y = y - m * prev;
-    }
-    t2p[K - 1] = t2;
-    AT(O, i, j, K) = y;
-    prev = y;
-    t2prev = t2;
-    t3prev = K < KE ? t3 : 0.;
-  }
-  double nxt = div_nr(wet(G.gp, ij, KE) * AT(O, i, j, KE), t2p[KE - 1]);
-  AT(O, i, j, KE) = nxt;
-  for (int K = KE - 1; K >= 2; --K) {
-    const double t3 = tri3(K, den(K));
-    nxt = div_nr((AT(O, i, j, K) - t3 * nxt) * wet(G.gp, ij, K), t2p[K - 1]);
-    AT(O, i, j, K) = nxt;
   }
 }
 
