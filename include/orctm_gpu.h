@@ -28,6 +28,9 @@
  *                                            mo_obcs.f90:1881-2032, 2295-2582
  *   orctm_set_obc_ts / orctm_obc_ts  FORC_OBCS_TS + SPONGE_OBCS_TS(THO,SAO)
  *                       octher.f90:114-119, mo_obcs.f90:932-1272
+ *   orctm_set_obc_sponge_exp  OBC_SPONGE_EXP: SPONGE_OBCS_ETA_EXP, _UV_EXP,
+ *                       _TS_EXP instead of the 1/x sponge  orctm.f90:1348-1362,
+ *                       octher.f90:116-120, mo_obcs.f90:507-522, 2588-3222
  *   orctm_set_barotropic  SUBROUTINE ITPREP  itprep.f90:15-40 (with BODEN's
  *                       inverse u/v depths, boden.f90:264-274)
  *   orctm_trotest       SUBROUTINE TROTEST   trotest.f90:1-118
@@ -278,6 +281,19 @@ int orctm_obc_uv(orctm_handle* h, int ldtrun);
  * tracers with a record relax in the bands of orctm_set_obc, in place. */
 int orctm_set_obc_ts(orctm_handle* h, int tracer, const double* const* cli);
 int orctm_obc_ts(orctm_handle* h);
+/* The exponential sponge of a build with OBC_SPONGE_EXP (Makefile:50 has it
+ * off): orctm_obc_eta, orctm_obc_uv, orctm_obc_ts and orctm_step_full then
+ * run SPONGE_OBCS_ETA_EXP, SPONGE_OBCS_UV_EXP and SPONGE_OBCS_TS_EXP
+ * (mo_obcs.f90:2588-3222).  Same bands and corner rule as the 1/x form; the
+ * cell at distance d from the boundary cell changes by
+ *     MASK_b * MASK * DT * EXP(-4 L/Lsp) / TAO * (boundary value - X),
+ * L the summed DLX* (west, east) or DLY* (north, south) of the staggering
+ * from the boundary cell to the cell, Lsp that of the whole band
+ * (mo_obcs.f90:507-522); SAO's south band uses its innermost rate in every
+ * row, as the reference's loop does (mo_obcs.f90:2976).  tao is the namelist
+ * TAO (OCEOBC, orctm.f90:164-166), in s; 0 returns to the 1/x form, as does
+ * orctm_set_obc.  Needs orctm_set_obc first. */
+int orctm_set_obc_sponge_exp(orctm_handle* h, double tao);
 
 /* ---- Barotropic (free-surface) solve and total velocities --------------
  * The part of the reference step that runs just before the hot path

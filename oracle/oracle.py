@@ -53,6 +53,7 @@ class _Obc(C.Structure):
         ("ntide", C.c_int), ("period", _D), ("sponge", C.c_int * 4), ("width", C.c_int * 4),
         ("relax_inner", C.c_double), ("relax_bound", C.c_double),
         ("amp", (_D * 3) * 4), ("pha", (_D * 3) * 4),
+        ("tao", C.c_double), ("salinity", C.c_int),
     ]
 
 
@@ -77,6 +78,7 @@ def obc_struct(obc: dict):
                     dst[b][v] = _p(a)
     o.relax_inner = float(obc["relax_inner"])
     o.relax_bound = float(obc["relax_bound"])
+    o.tao = float(obc.get("tao", 0.0))  # 0: the 1/x sponge
     return o, keep
 
 
@@ -257,10 +259,12 @@ class Oracle:
         o, keep = obc_struct(obc)
         lib().og_obc_uv(C.byref(self.g), C.byref(o), int(step), _p(uoo), _p(voe))
 
-    def obc_ts(self, obc, cli, trf):
+    def obc_ts(self, obc, cli, trf, salinity=False):
         """FORC_OBCS_TS + SPONGE_OBCS_TS on one tracer; cli[b] is side b's
-        climatology record (n, KE) or None."""
+        climatology record (n, KE) or None; salinity: the tracer is SAO
+        (matters in the exponential form only)."""
         o, keep = obc_struct(obc)
+        o.salinity = 1 if salinity else 0
         arrs = [None if c is None else np.asfortranarray(c, dtype=np.float64) for c in cli]
         ptrs = (_D * 4)(*[_D() if a is None else _p(a) for a in arrs])
         lib().og_obc_ts(C.byref(self.g), C.byref(o), ptrs, _p(trf))
@@ -351,7 +355,7 @@ class Oracle:
         if obc is not None and cli is not None:
             for n in (0, 1):
                 if cli[n] is not None:
-                    self.obc_ts(obc, cli[n], st["tracers"][n])
+                    self.obc_ts(obc, cli[n], st["tracers"][n], salinity=n == 1)
         st["po"], st["stabio"], st["rhoo"] = self.octher_column(
             t, tho, sao, st["zo"], st["uko"], st["vke"], st["avo"], st["dvo"], st["kcondep"])
 

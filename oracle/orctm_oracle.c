@@ -1665,7 +1665,8 @@ int og_solve(const og_grid *g, const int *rp, const int *ci, const double *val,
 }
 
 /* ------------------------------------------------------------------------ */
-/* Open-boundary tides and sponge (mo_obcs.f90, OBC_TIDE on, 1/x sponge).   */
+/* Open-boundary tides and sponge (mo_obcs.f90, OBC_TIDE on; the 1/x sponge,  */
+/* or the exponential one of OBC_SPONGE_EXP where og_obc.tao is nonzero).   */
 /* ------------------------------------------------------------------------ */
 /* One boundary value of the tidal sum (mo_obcs.f90:578-584 and the like):
  * sum over td of AM(idx,td) * MASK * COS(2 PI (t - PH(idx,td)) / T(td)). */
@@ -1684,6 +1685,54 @@ static double og_tide(const og_obc *o, const double *am, const double *ph, int n
 static double og_lambda(double s1, double s2, double relb, double reli, int w, double dt) {
   double lambda = (s1 * relb + s2 * reli) / (double)w;
   return lambda != 0.0 ? dt / lambda : 0.0;
+}
+
+/* OBC_SPONGE_EXP (mo_obcs.f90:2588-3222): the rate EXP(-4*L/Lsp)/TAO of the
+ * band cell with normal index x (i west/east, j north/south) in row `row`
+ * (the other index) of side b, staggering `kind` (0 p, 1 u, 2 v).  L is the
+ * SUM of DLX* (west, east) or DLY* (north, south) from the boundary cell to
+ * the cell, Lsp that of the whole band as INI_OBCS forms it
+ * (mo_obcs.f90:508-522): u west from I_START = 0, v north from J_START = 0.
+ * sal: SAO's south band, whose loop reads Lt_s, the L T's loop ended with
+ * (x = JE - w + 1), mo_obcs.f90:2974-2978. */
+static double og_met(const og_grid *g, const double *a, int kind, int i, int j) {
+  DIMS;
+  (void)KE;
+  if (kind == 1) return U2(a, i, j);
+  if (kind == 2) return V2(a, i, j);
+  return P2(a, i, j);
+}
+static double og_sum_x(const og_grid *g, const double *a, int kind, int lo, int hi, int j) {
+  double s = 0.0;
+  for (int i = lo; i <= hi; ++i) s = s + og_met(g, a, kind, i, j);
+  return s;
+}
+static double og_sum_y(const og_grid *g, const double *a, int kind, int i, int lo, int hi) {
+  double s = 0.0;
+  for (int j = lo; j <= hi; ++j) s = s + og_met(g, a, kind, i, j);
+  return s;
+}
+static double og_rate(const og_grid *g, double tao, int kind, int b, int x, int row, int w, int sal) {
+  const int IE = g->ie, JE = g->je;
+  const double *dx = kind == 0 ? g->dlxp : kind == 1 ? g->dlxu : g->dlxv;
+  const double *dy = kind == 0 ? g->dlyp : kind == 1 ? g->dlyu : g->dlyv;
+  double l, lsp;
+  if (b == 0) {
+    const int lo = kind == 1 ? 0 : 1;
+    l = og_sum_x(g, dx, kind, lo, x, row);
+    lsp = og_sum_x(g, dx, kind, lo, lo + w - 1, row);
+  } else if (b == 1) {
+    l = og_sum_x(g, dx, kind, x, IE, row);
+    lsp = og_sum_x(g, dx, kind, IE - w + 1, IE, row);
+  } else if (b == 2) {
+    const int lo = kind == 2 ? 0 : 1;
+    l = og_sum_y(g, dy, kind, row, lo, x);
+    lsp = og_sum_y(g, dy, kind, row, lo, lo + w - 1);
+  } else {
+    l = og_sum_y(g, dy, kind, row, sal ? JE - w + 1 : x, JE);
+    lsp = og_sum_y(g, dy, kind, row, JE - w + 1, JE);
+  }
+  return exp(-(4.0 * l / lsp)) / tao;
 }
 
 void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo) {
@@ -1716,6 +1765,12 @@ void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo) {
       const double s1 = (double)(sw - i + 1), s2 = (double)(i - 1);
       const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
       for (int j = 1; j <= JE; ++j) {
+        if (o->tao != 0.0) {
+          P2(fw, i, j) =
+              P3(g->weto, 1, j, 1) * P3(g->weto, i, j, 1) * dt *
+              og_rate(g, o->tao, 0, 0, i, j, sw, 0) * (zw[j - 1] - P2(zz, i, j));
+          continue;
+        }
         const double zr = (s1 * zw[j - 1] + s2 * P2(zz, i, j)) / (double)sw;
         P2(fw, i, j) = P3(g->weto, 1, j, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
       }
@@ -1725,6 +1780,12 @@ void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo) {
       const double s1 = (double)(i - IE + se), s2 = (double)(IE - i);
       const double lambda = og_lambda(s1, s2, relb, reli, se, dt);
       for (int j = 1; j <= JE; ++j) {
+        if (o->tao != 0.0) {
+          P2(fe, i, j) =
+              P3(g->weto, IE, j, 1) * P3(g->weto, i, j, 1) * dt *
+              og_rate(g, o->tao, 0, 1, i, j, se, 0) * (ze[j - 1] - P2(zz, i, j));
+          continue;
+        }
         const double zr = (s1 * ze[j - 1] + s2 * P2(zz, i, j)) / (double)se;
         P2(fe, i, j) = P3(g->weto, IE, j, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
       }
@@ -1734,6 +1795,12 @@ void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo) {
       const double s1 = (double)(sn - j + 1), s2 = (double)(j - 1);
       const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
       for (int i = 1; i <= IE; ++i) {
+        if (o->tao != 0.0) {
+          P2(fn, i, j) =
+              P3(g->weto, i, 1, 1) * P3(g->weto, i, j, 1) * dt *
+              og_rate(g, o->tao, 0, 2, j, i, sn, 0) * (zn[i - 1] - P2(zz, i, j));
+          continue;
+        }
         const double zr = (s1 * zn[i - 1] + s2 * P2(zz, i, j)) / (double)sn;
         P2(fn, i, j) = P3(g->weto, i, 1, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
       }
@@ -1743,6 +1810,12 @@ void og_obc_eta(const og_grid *g, const og_obc *o, int step, double *zo) {
       const double s1 = (double)(j - JE + ss), s2 = (double)(JE - j);
       const double lambda = og_lambda(s1, s2, relb, reli, ss, dt);
       for (int i = 1; i <= IE; ++i) {
+        if (o->tao != 0.0) {
+          P2(fs, i, j) =
+              P3(g->weto, i, JE, 1) * P3(g->weto, i, j, 1) * dt *
+              og_rate(g, o->tao, 0, 3, j, i, ss, 0) * (zs[i - 1] - P2(zz, i, j));
+          continue;
+        }
         const double zr = (s1 * zs[i - 1] + s2 * P2(zz, i, j)) / (double)ss;
         P2(fs, i, j) = P3(g->weto, i, JE, 1) * P3(g->weto, i, j, 1) * lambda * (zr - P2(zz, i, j));
       }
@@ -1814,6 +1887,12 @@ void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double 
         const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
         for (int j = 1; j <= JE; ++j) {
           const double ob = uzw[j - 1] * U3(g->amsuo, 0, j, k);
+          if (o->tao != 0.0) {
+            U3(uw, i, j, k) =
+                U3(g->amsuo, 0, j, k) * U3(g->amsuo, i, j, k) * dt *
+                og_rate(g, o->tao, 1, 0, i, j, sw, 0) * (ob - U3(uu, i, j, k));
+            continue;
+          }
           const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)sw;
           U3(uw, i, j, k) = U3(g->amsuo, 0, j, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
         }
@@ -1823,6 +1902,12 @@ void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double 
         const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
         for (int j = 0; j <= JE; ++j) {
           const double ob = vzw[j] * V3(g->amsue, 1, j, k);
+          if (o->tao != 0.0) {
+            V3(vw, i, j, k) =
+                V3(g->amsue, 1, j, k) * V3(g->amsue, i, j, k) * dt *
+                og_rate(g, o->tao, 2, 0, i, j, sw, 0) * (ob - V3(vv, i, j, k));
+            continue;
+          }
           const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)sw;
           V3(vw, i, j, k) = V3(g->amsue, 1, j, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
         }
@@ -1834,11 +1919,23 @@ void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double 
         const double lambda = og_lambda(s1, s2, relb, reli, se, dt);
         for (int j = 1; j <= JE; ++j) {
           const double ob = uze[j - 1] * U3(g->amsuo, IE, j, k);
+          if (o->tao != 0.0) {
+            U3(ue, i, j, k) =
+                U3(g->amsuo, IE, j, k) * U3(g->amsuo, i, j, k) * dt *
+                og_rate(g, o->tao, 1, 1, i, j, se, 0) * (ob - U3(uu, i, j, k));
+            continue;
+          }
           const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)se;
           U3(ue, i, j, k) = U3(g->amsuo, IE, j, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
         }
         for (int j = 0; j <= JE; ++j) {
           const double ob = vze[j] * V3(g->amsue, IE, j, k);
+          if (o->tao != 0.0) {
+            V3(ve, i, j, k) =
+                V3(g->amsue, IE, j, k) * V3(g->amsue, i, j, k) * dt *
+                og_rate(g, o->tao, 2, 1, i, j, se, 0) * (ob - V3(vv, i, j, k));
+            continue;
+          }
           const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)se;
           V3(ve, i, j, k) = V3(g->amsue, IE, j, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
         }
@@ -1850,6 +1947,12 @@ void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double 
         const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
         for (int i = 0; i <= IE; ++i) {
           const double ob = uzn[i] * U3(g->amsuo, i, 1, k);
+          if (o->tao != 0.0) {
+            U3(un, i, j, k) =
+                U3(g->amsuo, i, 1, k) * U3(g->amsuo, i, j, k) * dt *
+                og_rate(g, o->tao, 1, 2, j, i, sn, 0) * (ob - U3(uu, i, j, k));
+            continue;
+          }
           const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)sn;
           U3(un, i, j, k) = U3(g->amsuo, i, 1, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
         }
@@ -1859,6 +1962,12 @@ void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double 
         const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
         for (int i = 1; i <= IE; ++i) {
           const double ob = vzn[i - 1] * V3(g->amsue, i, 0, k);
+          if (o->tao != 0.0) {
+            V3(vn, i, j, k) =
+                V3(g->amsue, i, 0, k) * V3(g->amsue, i, j, k) * dt *
+                og_rate(g, o->tao, 2, 2, j, i, sn, 0) * (ob - V3(vv, i, j, k));
+            continue;
+          }
           const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)sn;
           V3(vn, i, j, k) = V3(g->amsue, i, 0, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
         }
@@ -1870,11 +1979,23 @@ void og_obc_uv(const og_grid *g, const og_obc *o, int step, double *uoo, double 
         const double lambda = og_lambda(s1, s2, relb, reli, ss, dt);
         for (int i = 0; i <= IE; ++i) {
           const double ob = uzs[i] * U3(g->amsuo, i, JE, k);
+          if (o->tao != 0.0) {
+            U3(us, i, j, k) =
+                U3(g->amsuo, i, JE, k) * U3(g->amsuo, i, j, k) * dt *
+                og_rate(g, o->tao, 1, 3, j, i, ss, 0) * (ob - U3(uu, i, j, k));
+            continue;
+          }
           const double ur = (s1 * ob + s2 * U3(uu, i, j, k)) / (double)ss;
           U3(us, i, j, k) = U3(g->amsuo, i, JE, k) * U3(g->amsuo, i, j, k) * lambda * (ur - U3(uu, i, j, k));
         }
         for (int i = 1; i <= IE; ++i) {
           const double ob = vzs[i - 1] * V3(g->amsue, i, JE, k);
+          if (o->tao != 0.0) {
+            V3(vs, i, j, k) =
+                V3(g->amsue, i, JE, k) * V3(g->amsue, i, j, k) * dt *
+                og_rate(g, o->tao, 2, 3, j, i, ss, 0) * (ob - V3(vv, i, j, k));
+            continue;
+          }
           const double vr = (s1 * ob + s2 * V3(vv, i, j, k)) / (double)ss;
           V3(vs, i, j, k) = V3(g->amsue, i, JE, k) * V3(g->amsue, i, j, k) * lambda * (vr - V3(vv, i, j, k));
         }
@@ -1958,6 +2079,12 @@ void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], do
         const double s1 = (double)(sw - i + 1), s2 = (double)(i - 1);
         const double lambda = og_lambda(s1, s2, relb, reli, sw, dt);
         for (int j = 1; j <= JE; ++j) {
+          if (o->tao != 0.0) {
+            P3(fw, i, j, k) =
+                P3(g->weto, 1, j, k) * P3(g->weto, i, j, k) * dt *
+                og_rate(g, o->tao, 0, 0, i, j, sw, 0) * (bw[(j - 1) + (size_t)JE * (k - 1)] - P3(tt, i, j, k));
+            continue;
+          }
           const double tr = (s1 * bw[(j - 1) + (size_t)JE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)sw;
           P3(fw, i, j, k) = P3(g->weto, 1, j, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
         }
@@ -1967,6 +2094,12 @@ void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], do
         const double s1 = (double)(i - IE + se), s2 = (double)(IE - i);
         const double lambda = og_lambda(s1, s2, relb, reli, se, dt);
         for (int j = 1; j <= JE; ++j) {
+          if (o->tao != 0.0) {
+            P3(fe, i, j, k) =
+                P3(g->weto, IE, j, k) * P3(g->weto, i, j, k) * dt *
+                og_rate(g, o->tao, 0, 1, i, j, se, 0) * (be[(j - 1) + (size_t)JE * (k - 1)] - P3(tt, i, j, k));
+            continue;
+          }
           const double tr = (s1 * be[(j - 1) + (size_t)JE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)se;
           P3(fe, i, j, k) = P3(g->weto, IE, j, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
         }
@@ -1976,6 +2109,12 @@ void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], do
         const double s1 = (double)(sn - j + 1), s2 = (double)(j - 1);
         const double lambda = og_lambda(s1, s2, relb, reli, sn, dt);
         for (int i = 1; i <= IE; ++i) {
+          if (o->tao != 0.0) {
+            P3(fn, i, j, k) =
+                P3(g->weto, i, 1, k) * P3(g->weto, i, j, k) * dt *
+                og_rate(g, o->tao, 0, 2, j, i, sn, 0) * (bn[(i - 1) + (size_t)IE * (k - 1)] - P3(tt, i, j, k));
+            continue;
+          }
           const double tr = (s1 * bn[(i - 1) + (size_t)IE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)sn;
           P3(fn, i, j, k) = P3(g->weto, i, 1, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
         }
@@ -1985,6 +2124,12 @@ void og_obc_ts(const og_grid *g, const og_obc *o, const double *const cli[4], do
         const double s1 = (double)(j - JE + ss), s2 = (double)(JE - j);
         const double lambda = og_lambda(s1, s2, relb, reli, ss, dt);
         for (int i = 1; i <= IE; ++i) {
+          if (o->tao != 0.0) {
+            P3(fs, i, j, k) =
+                P3(g->weto, i, JE, k) * P3(g->weto, i, j, k) * dt *
+                og_rate(g, o->tao, 0, 3, j, i, ss, o->salinity) * (bs[(i - 1) + (size_t)IE * (k - 1)] - P3(tt, i, j, k));
+            continue;
+          }
           const double tr = (s1 * bs[(i - 1) + (size_t)IE * (k - 1)] + s2 * P3(tt, i, j, k)) / (double)ss;
           P3(fs, i, j, k) = P3(g->weto, i, JE, k) * P3(g->weto, i, j, k) * lambda * (tr - P3(tt, i, j, k));
         }

@@ -108,6 +108,12 @@ typedef struct og_obc {
   int width[4];                     /* spongew, spongee, spongen, sponges */
   double relax_inner, relax_bound;  /* Urelaxinner, Urelaxbound, s */
   const double *amp[4][3], *pha[4][3];
+  /* OBC_SPONGE_EXP: TAO (s) of the exponential sponge (SPONGE_OBCS_ETA_EXP,
+   * _UV_EXP, _TS_EXP, mo_obcs.f90:2588-3222); 0 for the 1/x sponge */
+  double tao;
+  /* og_obc_ts in the exponential form: the tracer is SAO, whose south band
+   * reads the rate T's loop left behind (mo_obcs.f90:2976) */
+  int salinity;
 } og_obc;
 
 /* FORC_OBCS_ETA + SPONGE_OBCS_ETA(ZO) at time step `step` (orctm.f90:1347-1351). */

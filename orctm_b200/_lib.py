@@ -128,7 +128,7 @@ EXPORTS = (
     "orctm_upload_async", "orctm_download_async", "orctm_set_step_outputs", "orctm_wait_copies",
     "orctm_write_extra", "orctm_write_extra_host", "orctm_read_extra", "orctm_read_extra_host",
     "orctm_set_obc", "orctm_obc_eta", "orctm_obc_uv", "orctm_write_gridinfo",
-    "orctm_set_obc_ts", "orctm_obc_ts", "orctm_octdiff_noalloc",
+    "orctm_set_obc_ts", "orctm_obc_ts", "orctm_set_obc_sponge_exp", "orctm_octdiff_noalloc",
     "orctm_set_barotropic", "orctm_troneu", "orctm_ocvtro", "orctm_ocvtot",
     "orctm_download_barotropic", "orctm_ocbarp", "orctm_ocwind", "orctm_trotest",
     "orctm_set_thermo", "orctm_set_coriolis", "orctm_octher", "orctm_ocmodmom", "orctm_occlit",
@@ -186,6 +186,7 @@ def load(build_if_missing: bool = True):
     lib.orctm_obc_uv.argtypes = [C.c_void_p, C.c_int]
     lib.orctm_set_obc_ts.argtypes = [C.c_void_p, C.c_int, C.POINTER(_D)]
     lib.orctm_obc_ts.argtypes = [C.c_void_p]
+    lib.orctm_set_obc_sponge_exp.argtypes = [C.c_void_p, C.c_double]
     lib.orctm_timer_start.argtypes = [C.c_void_p]
     lib.orctm_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.orctm_set_profiling.argtypes = [C.c_void_p, C.c_int]

@@ -396,6 +396,11 @@ class Instance:
         """SPONGE_OBCS_TS(THO, SAO) towards the records of set_obc_ts."""
         _lib.check(self.lib.orctm_obc_ts(self.h), self.h)
 
+    def set_obc_sponge_exp(self, tao: float):
+        """OBC_SPONGE_EXP: the exponential sponge (SPONGE_OBCS_*_EXP) with the
+        namelist TAO in s from now on; 0 returns to the 1/x form."""
+        _lib.check(self.lib.orctm_set_obc_sponge_exp(self.h, C.c_double(tao)), self.h)
+
     def obc_uv(self, ldtrun: int):
         """FORC_OBCS_UV + UPGRADE_OBCS_UV + SPONGE_OBCS_UV(UOO, VOE) at time step ldtrun."""
         _lib.check(self.lib.orctm_obc_uv(self.h, int(ldtrun)), self.h)

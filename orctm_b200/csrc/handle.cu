@@ -188,6 +188,11 @@ struct orctm_handle {
   ObcArgs obc_ts[2] = {};
   double* obc_ts_buf[2] = {nullptr, nullptr};
   size_t obc_ts_cap[2] = {0, 0};
+  // the exponential sponge's rate tables (orctm_set_obc_sponge_exp); SAO's
+  // south band has its own (mo_obcs.f90:2976)
+  double* obc_exp_buf = nullptr;
+  size_t obc_exp_cap = 0;
+  const double* obc_exp_sao_south = nullptr;
   // barotropic solve (orctm_set_barotropic): its constants, its 2D device
   // fields and TRONEU's SOR sweeps captured once as a graph
   bool baro_ready = false;
@@ -1725,14 +1730,26 @@ int orctm_set_obc(orctm_handle* h, const orctm_obc* o) {
       off += 2 * n;
       ORCTM_CUDA_OK(cudaMemcpy(amp, o->amp[b][v], sizeof(double) * n, cudaMemcpyHostToDevice));
       ORCTM_CUDA_OK(cudaMemcpy(pha, o->pha[b][v], sizeof(double) * n, cudaMemcpyHostToDevice));
-      a.side[b] = ObcSide{amp, pha, obc_points(h, b, v)};
+      a.side[b] = ObcSide{amp, pha, obc_points(h, b, v), nullptr};
     }
   }
   h->obc_ready = true;
-  // the T/S records follow the sides and widths set here: set them again
+  // the T/S records follow the sides and widths set here: set them again;
+  // the sponge is the 1/x form until orctm_set_obc_sponge_exp
   h->obc_ts_ready[0] = h->obc_ts_ready[1] = false;
+  h->obc_exp_sao_south = nullptr;
   return ORCTM_OK;
 }
+
+namespace {
+// the exponential sponge's rates of a tracer's side: the p-point table,
+// except SAO's south band, whose loop reads the rate T's loop left behind
+// (Ms_s from Lt_s, mo_obcs.f90:2974-2978); null in the 1/x form
+const double* ts_rates(const orctm_handle* h, int tracer, int b) {
+  if (!h->obc[0].expo) return nullptr;
+  return tracer == 1 && b == 3 ? h->obc_exp_sao_south : h->obc[0].side[b].wexp;
+}
+}  // namespace
 
 int orctm_set_obc_ts(orctm_handle* h, int tracer, const double* const* cli) {
   ORCTM_ENTER(h);
@@ -1763,14 +1780,14 @@ int orctm_set_obc_ts(orctm_handle* h, int tracer, const double* const* cli) {
   ObcArgs a = base;
   size_t off = 0;
   for (int b = 0; b < 4; ++b) {
-    a.side[b] = ObcSide{nullptr, nullptr, 0};
+    a.side[b] = ObcSide{nullptr, nullptr, 0, nullptr};
     if (!base.on[b]) continue;
     const int n = b < 2 ? JE : IE;
     const size_t cnt = (size_t)n * (size_t)KE;
     double* d = h->obc_ts_buf[tracer] + off;
     off += cnt;
     ORCTM_CUDA_OK(cudaMemcpy(d, cli[b], sizeof(double) * cnt, cudaMemcpyHostToDevice));
-    a.side[b] = ObcSide{d, nullptr, n};
+    a.side[b] = ObcSide{d, nullptr, n, ts_rates(h, tracer, b)};
   }
   h->obc_ts[tracer] = a;
   h->obc_ts_ready[tracer] = true;
@@ -1815,6 +1832,114 @@ int orctm_obc_uv(orctm_handle* h, int ldtrun) {
   au.t = av.t = (double)ldtrun * h->G.dt;
   launch_obc_uv(h->G, au, av, h->slot[ORCTM_F_UOO], h->slot[ORCTM_F_VOE], h->stream);
   ORCTM_CUDA_OK(cudaGetLastError());
+  return ORCTM_OK;
+}
+
+// OBC_SPONGE_EXP: the band rates EXP(-4 L/Lsp)/TAO of SPONGE_OBCS_ETA_EXP,
+// _UV_EXP and _TS_EXP (mo_obcs.f90:2588-3222), formed here once from the
+// metrics: L is the length from the boundary cell to the band cell and Lsp
+// the band's (INI_OBCS, mo_obcs.f90:508-522), both SUMs of DLX* (west, east)
+// or DLY* (north, south) of the staggering in ascending index order, as the
+// reference's SUM over its index ranges.
+int orctm_set_obc_sponge_exp(orctm_handle* h, double tao) {
+  ORCTM_ENTER(h);
+  if (!h->obc_ready)
+    return h->fail(ORCTM_E_ARG, "orctm_set_obc_sponge_exp: orctm_set_obc not called");
+  if (!std::isfinite(tao)) return h->fail(ORCTM_E_ARG, "orctm_set_obc_sponge_exp: TAO must be finite");
+  {
+    const int st0 = wait_all_uploads(h);
+    if (st0) return st0;
+  }
+  // the previous tables may still be read by queued launches
+  ORCTM_CUDA_OK(cudaStreamSynchronize(h->stream));
+  const int IE = h->L.ie, JE = h->L.je;
+  auto apply = [&]() {
+    for (int t = 0; t < 2; ++t) {
+      h->obc_ts[t].expo = h->obc[0].expo;
+      for (int b = 0; b < 4; ++b)
+        if (h->obc_ts[t].on[b]) h->obc_ts[t].side[b].wexp = ts_rates(h, t, b);
+    }
+  };
+  if (tao == 0.0) {  // back to the 1/x form
+    for (ObcArgs& a : h->obc) {
+      a.expo = 0;
+      for (ObcSide& sd : a.side) sd.wexp = nullptr;
+    }
+    h->obc_exp_sao_south = nullptr;
+    apply();
+    return ORCTM_OK;
+  }
+  // DLXP, DLYP, DLXU, DLYU, DLXV, DLYV from their device copies (padded plane)
+  const size_t n2 = (size_t)h->L.plane;
+  std::vector<double> met[6];
+  const double* dev[6] = {h->G.dlxp, h->G.dlyp, h->G.dlxu, h->G.dlyu, h->G.dlxv, h->G.dlyv};
+  for (int m = 0; m < 6; ++m) {
+    met[m].resize(n2);
+    ORCTM_CUDA_OK(cudaMemcpy(met[m].data(), dev[m], sizeof(double) * n2, cudaMemcpyDeviceToHost));
+  }
+  const bool south = h->obc[0].on[3] != 0;
+  size_t total = south ? (size_t)IE * (size_t)h->obc[0].width[3] : 0;
+  for (int v = 0; v < 3; ++v)
+    for (int b = 0; b < 4; ++b)
+      if (h->obc[v].on[b]) total += (size_t)obc_points(h, b, v) * (size_t)h->obc[v].width[b];
+  std::vector<double> tab(std::max<size_t>(total, 1));
+  // the band length from the boundary cell to distance d of row q
+  auto length = [&](int v, int b, int q, int d) {
+    const int ilo = v == 1 ? 0 : 1, jlo = v == 2 ? 0 : 1;
+    const std::vector<double>& dl = met[2 * v + (b < 2 ? 0 : 1)];
+    int lo, hi;
+    if (b == 0) lo = ilo, hi = ilo + d - 1;
+    else if (b == 1) lo = IE - d + 1, hi = IE;
+    else if (b == 2) lo = jlo, hi = jlo + d - 1;
+    else lo = JE - d + 1, hi = JE;
+    double L = 0.0;
+    for (int x = lo; x <= hi; ++x)
+      L = L + dl[b < 2 ? h->L.at2(x, q + jlo) : h->L.at2(q + ilo, x)];
+    return L;
+  };
+  size_t off = 0;
+  double* base = nullptr;
+  if (total > h->obc_exp_cap) {
+    int st;
+    double* p;
+    if ((st = h->dev_alloc(&p, total))) return st;
+    h->obc_exp_buf = p;
+    h->obc_exp_cap = total;
+  }
+  base = h->obc_exp_buf;
+  const double* wptr[3][4] = {};
+  for (int v = 0; v < 3; ++v)
+    for (int b = 0; b < 4; ++b) {
+      if (!h->obc[v].on[b]) continue;
+      const int n = obc_points(h, b, v), w = h->obc[v].width[b];
+      for (int q = 0; q < n; ++q) {
+        const double lsp = length(v, b, q, w);
+        if (!(lsp > 0.0)) return h->fail(ORCTM_E_ARG, "orctm_set_obc_sponge_exp: a sponge band's length is not positive");
+        for (int d = 1; d <= w; ++d)
+          tab[off + q + (size_t)n * (d - 1)] = std::exp(-(4.0 * length(v, b, q, d) / lsp)) / tao;
+      }
+      wptr[v][b] = base + off;
+      off += (size_t)n * w;
+    }
+  const double* sao_south = nullptr;
+  if (south) {
+    // every row of SAO's band takes the rate of the band's innermost T cell
+    const int w = h->obc[0].width[3];
+    for (int q = 0; q < IE; ++q) {
+      const double lsp = length(0, 3, q, w);
+      const double r = std::exp(-(4.0 * length(0, 3, q, w) / lsp)) / tao;
+      for (int d = 1; d <= w; ++d) tab[off + q + (size_t)IE * (d - 1)] = r;
+    }
+    sao_south = base + off;
+    off += (size_t)IE * w;
+  }
+  if (total) ORCTM_CUDA_OK(cudaMemcpy(base, tab.data(), sizeof(double) * total, cudaMemcpyHostToDevice));
+  for (int v = 0; v < 3; ++v) {
+    h->obc[v].expo = 1;
+    for (int b = 0; b < 4; ++b) h->obc[v].side[b].wexp = wptr[v][b];
+  }
+  h->obc_exp_sao_south = sao_south;
+  apply();
   return ORCTM_OK;
 }
 

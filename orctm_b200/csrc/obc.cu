@@ -3,6 +3,10 @@
 //   FORC_OBCS_ETA + SPONGE_OBCS_ETA(ZO)              mo_obcs.f90:569-642, 1561-1720
 //   FORC_OBCS_UV + UPGRADE_OBCS_UV + SPONGE_OBCS_UV  mo_obcs.f90:1881-2032, 2295-2582
 //   FORC_OBCS_TS + SPONGE_OBCS_TS                    mo_obcs.f90:932-1272
+// and, with ObcArgs::expo, the exponential sponge of OBC_SPONGE_EXP
+// (SPONGE_OBCS_ETA_EXP, _UV_EXP, _TS_EXP, mo_obcs.f90:2588-3222): the same
+// bands and corner rule, each band term mask * mask * DT * M * (boundary -
+// X) with the rate M = EXP(-4 L/Lsp)/TAO of a table the host forms.
 //
 // The reference forms the boundary values (tidal sums), then per open side a
 // correction array over its sponge band, sums the four arrays and lets the
@@ -86,7 +90,7 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
   for (int b = 0; b < 4; ++b) {
     s1[b] = (double)(a.width[b] - d[b] + 1);
     s2[b] = (double)(d[b] - 1);
-    lam[b] = in[b] ? band_lambda(s1[b], s2[b], a.width[b], a) : 0.0;
+    lam[b] = in[b] && !a.expo ? band_lambda(s1[b], s2[b], a.width[b], a) : 0.0;
   }
   constexpr bool k2d = FK == FK_P && !CLI;  // ZO
   const int nk = k2d ? 1 : G.L.ke;
@@ -112,8 +116,15 @@ __global__ void k_obc_sponge(Geo G, ObcArgs a, double* __restrict__ x) {
         ob = a.side[b].amp[q[b] + a.side[b].n * (K - 1)] * mb[b];
       else
         ob = FK == FK_P ? zb[b] : zb[b] * mb[b];
-      const double xr = (s1[b] * ob + s2[b] * X) / (double)a.width[b];
-      f[b] = mb[b] * mi * lam[b] * (xr - X);
+      if (a.expo) {
+        // OBC_SPONGE_EXP: mask * mask * DT * EXP(-4 L/Lsp)/TAO * (boundary - X)
+        // (mo_obcs.f90:2641, 2906, 3108 and the like)
+        const double m = a.side[b].wexp[q[b] + a.side[b].n * (d[b] - 1)];
+        f[b] = mb[b] * mi * a.dt * m * (ob - X);
+      } else {
+        const double xr = (s1[b] * ob + s2[b] * X) / (double)a.width[b];
+        f[b] = mb[b] * mi * lam[b] * (xr - X);
+      }
     }
     double fo = f[0] + f[1] + f[2] + f[3];
     if (inW && inN) fo = dW < dN ? f[0] : f[2];

@@ -37,6 +37,10 @@ struct ObcSide {
   const double* amp;
   const double* pha;
   int n;  // points along the side
+  // the exponential sponge's rates (OBC_SPONGE_EXP): wexp[q + n * (d - 1)] =
+  // EXP(-4 L/Lsp) / TAO of the band cell at distance d = 1..width from the
+  // boundary in row q (mo_obcs.f90:2640 and the like); null in the 1/x form
+  const double* wexp;
 };
 // Arguments of one open-boundary sponge launch (one staggering), by value.
 struct ObcArgs {
@@ -45,6 +49,7 @@ struct ObcArgs {
   double pi, t, dt, relb, reli;  // PI, i_step * DT, DT, rel_*b, rel_*i
   int on[4];                     // west, east, north, south: open and sponged
   int width[4];                  // spongew, spongee, spongen, sponges
+  int expo;                      // the exponential sponge (side[b].wexp) instead of 1/x
   ObcSide side[4];
 };
 

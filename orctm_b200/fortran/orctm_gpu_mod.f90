@@ -156,6 +156,12 @@ module orctm_gpu_mod
        import :: c_int, c_ptr
        type(c_ptr), value :: h
      end function
+     ! OBC_SPONGE_EXP with the namelist TAO (s); 0 returns to the 1/x sponge
+     integer(c_int) function orctm_set_obc_sponge_exp(h, tao) bind(c, name="orctm_set_obc_sponge_exp")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: tao
+     end function
      integer(c_int) function orctm_set_barotropic(h, b) bind(c, name="orctm_set_barotropic")
        import :: c_int, c_ptr, orctm_barotropic
        type(c_ptr), value :: h

@@ -174,20 +174,68 @@ def matrix(g):
     return sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
 
 
-def obc_sponge_ts(g, obc, cli, x):
+def obc_sponge_ts(g, obc, cli, x, salinity=False):
     """FORC_OBCS_TS + SPONGE_OBCS_TS (mo_obcs.f90:932-1272) on one tracer in
     the same per-cell distance form as obc_sponge, the boundary value of
-    level k being cli[b][q, k] times the boundary cell's WETO at level k."""
-    return obc_sponge(g, obc, 0, x, "t", cli=cli)
+    level k being cli[b][q, k] times the boundary cell's WETO at level k.
+    salinity: the tracer is SAO (SPONGE_OBCS_TS_EXP's south band)."""
+    return obc_sponge(g, obc, 0, x, "t", cli=cli, salinity=salinity)
 
 
-def obc_sponge(g, obc, step, x, kind, cli=None):
+def _exp_rates(g, obc, kind, w, ni, nj, salinity):
+    """OBC_SPONGE_EXP's rate EXP(-4 L/Lsp)/TAO per cell and side, (ni, nj)
+    arrays in the staggering's array indices; L sums the metric from the
+    boundary cell to the cell in ascending index order, one row at a time
+    (sequential, like Fortran's SUM over the index range), Lsp is L of the
+    band's innermost cell; SAO's south band takes Lsp for every cell
+    (mo_obcs.f90:2976)."""
+    st = {"z": "p", "t": "p", "u": "u", "v": "v"}[kind]
+    dx, dy = np.asarray(g["dlx" + st]), np.asarray(g["dly" + st])
+    tao = float(obc["tao"])
+    rates = []
+    for b in range(4):
+        L = np.zeros((ni, nj))
+        if b == 0:
+            acc = np.zeros(nj)
+            for a in range(ni):
+                acc = acc + dx[a, :]
+                L[a, :] = acc
+            lsp = L[min(w[b], ni) - 1, :][None, :]
+        elif b == 1:
+            for a in range(ni):
+                acc = np.zeros(nj)
+                for x in range(a, ni):
+                    acc = acc + dx[x, :]
+                L[a, :] = acc
+            lsp = L[ni - w[b], :][None, :]
+        elif b == 2:
+            acc = np.zeros(ni)
+            for c in range(nj):
+                acc = acc + dy[:, c]
+                L[:, c] = acc
+            lsp = L[:, min(w[b], nj) - 1][:, None]
+        else:
+            for c in range(nj):
+                acc = np.zeros(ni)
+                for y in range(c, nj):
+                    acc = acc + dy[:, y]
+                L[:, c] = acc
+            lsp = L[:, nj - w[b]][:, None]
+            if salinity:
+                L = np.broadcast_to(lsp, (ni, nj))
+        rates.append(np.exp(-(4.0 * L / lsp)) / tao)
+    return rates
+
+
+def obc_sponge(g, obc, step, x, kind, cli=None, salinity=False):
     """Open-boundary tide forcing + 1/x sponge (mo_obcs.f90:569-642 and
     1561-1720 for kind "z" on ZO; 1881-2032 and 2295-2582 for "u" / "v" on
     UOO / VOE), restated per cell from the cell's distance d to each side's
     boundary cell: band weights s1 = w - d + 1, s2 = d - 1, and in the
     corners the band with the smaller d (the later corner loop on equal d).
-    Returns the relaxed copy of x."""
+    With a nonzero obc["tao"], the exponential sponge of OBC_SPONGE_EXP
+    (mo_obcs.f90:2588-3222): the band term is MASK * MASK * DT * M *
+    (boundary - X).  Returns the relaxed copy of x."""
     IE, JE = g["ie"], g["je"]
     ilo = 0 if kind == "u" else 1
     jlo = 0 if kind == "v" else 1
@@ -243,6 +291,9 @@ def obc_sponge(g, obc, step, x, kind, cli=None):
         l = (s1[b] * obc["relax_bound"] + s2[b] * obc["relax_inner"]) / float(w[b])
         with np.errstate(divide="ignore"):
             lam.append(np.where(l != 0.0, g["dt"] / np.where(l != 0.0, l, 1.0), 0.0))
+    expo = float(obc.get("tao", 0.0)) != 0.0
+    if expo:
+        rate = _exp_rates(g, obc, kind, w, ni, nj, salinity)
     anyb = inb[0] | inb[1] | inb[2] | inb[3]
     for k in range(nk):
         X = x3[:, :, k]
@@ -258,6 +309,9 @@ def obc_sponge(g, obc, step, x, kind, cli=None):
                 obk = np.broadcast_to(c[None, :] if b < 2 else c[:, None], (ni, nj)) * mb
             else:
                 obk = zb[b] if kind == "z" else zb[b] * mb
+            if expo:
+                f.append(np.where(inb[b], mb * mi * g["dt"] * rate[b] * (obk - X), 0.0))
+                continue
             xr = (s1[b] * obk + s2[b] * X) / float(w[b])
             f.append(np.where(inb[b], mb * mi * lam[b] * (xr - X), 0.0))
         fo = f[0] + f[1] + f[2] + f[3]

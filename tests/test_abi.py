@@ -98,6 +98,7 @@ def test_open_boundary_and_gridinfo_argument_checks(tmp_path):
     assert lib.orctm_obc_eta(None, 1) == -1
     assert lib.orctm_obc_ts(None) == -1
     assert lib.orctm_set_obc_ts(None, 0, None) == -1
+    assert lib.orctm_set_obc_sponge_exp(None, 3600.0) == -1
     inst = configs.make_instance("c2", builder=grid.build_grid, nx=9, ny=7, nz=4)
     d, keep = api.make_desc(inst)
     g = _lib.GridInfo()                      # every coordinate pointer NULL

@@ -1,7 +1,8 @@
 """Open-boundary tide forcing and sponge on the GPU (orctm_set_obc,
-orctm_obc_eta, orctm_obc_uv) against the oracle's restatement of
-mo_obcs.f90, on the reference's W+S layout and on every-side layouts with
-crossing, uneven, unsponged and zero-relaxation bands.  The kernels and the
+orctm_obc_eta, orctm_obc_uv, orctm_obc_ts, orctm_set_obc_sponge_exp)
+against the oracle's restatement of mo_obcs.f90, on the reference's W+S
+layout and on every-side layouts with crossing, uneven, unsponged and
+zero-relaxation bands, in the 1/x and the exponential form.  The kernels and the
 oracle evaluate the same expressions in the same order; they differ only
 through COS (CUDA's cos against the C library's), hence the 1e-13 bound.
 Also: a buffer shared with UKO after OCTIMF, and pending downloads, keep
@@ -13,7 +14,7 @@ import oracle as O
 from helpers import assert_close
 from orctm_b200 import configs as C
 from orctm_b200.api import Instance
-from test_obc import CASES, _case
+from test_obc import CASES, _case, _exp_case
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-13
@@ -104,6 +105,11 @@ def test_set_obc_rejects_bad_arguments():
     amp[0][1] = None
     with pytest.raises(Exception):
         gpu.set_obc(dict(obc, amp=amp))
+    with pytest.raises(Exception):
+        gpu.set_obc_sponge_exp(3600.0)     # constants not set
+    gpu.set_obc(obc)
+    with pytest.raises(Exception):
+        gpu.set_obc_sponge_exp(float("inf"))
 
 
 @pytest.mark.parametrize("kind", CASES)
@@ -175,3 +181,39 @@ def test_reference_sect35_files_drive_the_sponges():
         cli = [api.read_obc_ts_record(HERE, s, n, JE, KE, 3) for s in (0, 1)] + [None, None]
         orc.obc_ts(obc, cli, st["tracers"][n])
         assert np.array_equal(gpu.download(f"tracer{n}"), st["tracers"][n]), n
+
+
+@pytest.mark.parametrize("kind", CASES)
+def test_obc_exp_sponge_parity(kind):
+    """OBC_SPONGE_EXP (SPONGE_OBCS_UV_EXP, _ETA_EXP, _TS_EXP): UOO, VOE and ZO
+    against the oracle within the COS bound; THO (record set before the
+    switch) and SAO (set after it), whose south band has its own rate, bit
+    for bit, as the rates come from the same host EXP; TAO = 0 returns to
+    the 1/x form.  Stretched metrics, so that the band lengths' summation
+    order matters."""
+    inst, obc = _exp_case(kind)
+    orc, gpu, st = _pair(inst, obc)
+    cli = [C.make_obc_ts(inst, n) for n in (0, 1)]
+    gpu.set_obc_ts(0, cli[0])
+    gpu.set_obc_sponge_exp(obc["tao"])
+    gpu.set_obc_ts(1, cli[1])
+    for step in (1, 4321):
+        gpu.obc_uv(step)
+        orc.obc_uv(obc, step, st["uoo"], st["voe"])
+        gpu.obc_eta(step)
+        orc.obc_eta(obc, step, st["zo"])
+    for k in ("uoo", "voe", "zo"):
+        assert_close(gpu.download(k), st[k], TOL, k)
+    inv = dict(obc, tao=0.0)
+    for form in (obc, inv):
+        gpu.obc_ts()
+        for n in (0, 1):
+            orc.obc_ts(form, cli[n], st["tracers"][n], salinity=n == 1)
+        for n in (0, 1):
+            got = gpu.download(f"tracer{n}")
+            assert np.array_equal(got, st["tracers"][n]), (n, float(np.abs(got - st["tracers"][n]).max()))
+        gpu.set_obc_sponge_exp(0.0)
+    gpu.obc_uv(99)
+    orc.obc_uv(inv, 99, st["uoo"], st["voe"])
+    assert_close(gpu.download("uoo"), st["uoo"], TOL, "UOO after the switch back")
+

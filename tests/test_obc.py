@@ -3,7 +3,9 @@
 an independent numpy restatement in per-cell distance form, on the
 reference's own layout (W+S open) and on cases that open every side with
 bands that cross, differ in width, are switched off or have zero relaxation
-times; the harmonic-constant files round trip.  No GPU."""
+times, in the 1/x form and in the exponential form of OBC_SPONGE_EXP (on
+stretched metrics, so that the band lengths' summation order shows); the
+harmonic-constant files round trip.  No GPU."""
 import numpy as np
 import pytest
 
@@ -40,6 +42,19 @@ def _case(kind):
 
 
 CASES = ("reference", "crossing", "uneven", "one_off", "zero_relax")
+TOL_EXP = 1e-14  # numpy's EXP and the C library's may differ in the last bit too
+
+
+def _exp_case(kind):
+    """_case with the exponential sponge (TAO = 5 DT) and every metric
+    stretched by seeded factors in [0.7, 1.3]."""
+    inst, obc = _case(kind)
+    inst = dict(inst)
+    g = np.random.default_rng(4242)
+    for k in ("dlxp", "dlyp", "dlxu", "dlyu", "dlxv", "dlyv"):
+        a = np.asarray(inst[k], dtype=np.float64)
+        inst[k] = np.asfortranarray(a * g.uniform(0.7, 1.3, a.shape))
+    return inst, dict(obc, tao=5.0 * inst["dt"])
 
 
 @pytest.mark.parametrize("kind", CASES)
@@ -153,3 +168,53 @@ def test_obc_ts_records_round_trip(tmp_path):
     assert np.frombuffer(raw[off:off + 8], dtype=">f8")[0] == recs[1][0, 1]
     with pytest.raises(ValueError):
         api.read_obc_ts_record(str(tmp_path), 0, 0, je, ke, 3)
+
+
+@pytest.mark.parametrize("kind", CASES)
+def test_oracle_exp_sponge_equals_numpy(kind):
+    """SPONGE_OBCS_UV_EXP, _ETA_EXP and _TS_EXP (mo_obcs.f90:2588-3222)."""
+    inst, obc = _exp_case(kind)
+    o = O.Oracle(inst)
+    st = configs.copy_state(inst)
+    u0, v0, z0 = st["uoo"].copy(), st["voe"].copy(), st["zo"].copy()
+    o.obc_uv(obc, 4321, st["uoo"], st["voe"])
+    assert_close(st["uoo"], NR.obc_sponge(inst, obc, 4321, u0, "u"), TOL_EXP, "UOO")
+    assert_close(st["voe"], NR.obc_sponge(inst, obc, 4321, v0, "v"), TOL_EXP, "VOE")
+    assert not np.array_equal(st["uoo"], u0)
+    o.obc_eta(obc, 777, st["zo"])
+    assert_close(st["zo"], NR.obc_sponge(inst, obc, 777, z0, "z"), TOL_EXP, "ZO")
+    for tracer in (0, 1):
+        cli = configs.make_obc_ts(inst, tracer)
+        t = np.array(inst["tracers"][tracer], order="F", copy=True)
+        t0 = t.copy()
+        o.obc_ts(obc, cli, t, salinity=tracer == 1)
+        want = NR.obc_sponge_ts(inst, obc, cli, t0, salinity=tracer == 1)
+        assert_close(t, want, TOL_EXP, f"tracer {tracer}")
+        assert not np.array_equal(t, t0)
+
+
+def test_exp_sponge_differs_from_one_over_x_and_sao_south_band():
+    """The exponential form changes the bands only, and differs from the 1/x
+    form there.  SAO's south-band loop reads the rate T's loop ended with
+    (Ms_s from Lt_s, mo_obcs.f90:2976): given THO's record and field, SAO
+    differs from THO in the south band only, and not in its innermost row,
+    whose rate is that one."""
+    inst, obc = _exp_case("reference")
+    o = O.Oracle(inst)
+    cli = configs.make_obc_ts(inst, 0)
+    t0 = np.array(inst["tracers"][0], order="F", copy=True)
+    res = {}
+    for name, ob, sal in (("exp", obc, False), ("sao", obc, True),
+                          ("inv", dict(obc, tao=0.0), False)):
+        t = np.array(t0, order="F", copy=True)
+        o.obc_ts(ob, cli, t, salinity=sal)
+        res[name] = t
+    JE, w = inst["je"], obc["width"]
+    inner = (slice(w[0], None), slice(0, JE - w[3]))   # outside the west and south bands
+    assert np.array_equal(res["exp"][inner], t0[inner])
+    assert not np.array_equal(res["exp"], t0)
+    assert not np.array_equal(res["exp"], res["inv"])
+    rows = np.nonzero((res["exp"] != res["sao"]).any(axis=(0, 2)))[0]  # j - 1
+    assert rows.size > 0
+    assert rows.min() >= JE - w[3] + 1 and rows.max() <= JE - 1, rows
+
