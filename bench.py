@@ -334,11 +334,22 @@ def run_whole_step(inst, cells, args, ws, rank, pg, local, hot_ms_per_step):
     launches = Instance.kernel_launches() - n0
     barrier(pg)
     ms = max_over_ranks(pg, ms)
+    # the hot path's share in this state (its solve takes more iterations than
+    # in the headline state): per-launcher device time of the hot-path
+    # kernels over a few more, untimed whole steps
+    nprof = min(args.steps, 3)
+    gpu.set_profiling(True)
+    for s in range(nprof):
+        gpu.step_full(args.warmup + args.steps + s + 1, check_contra=False)
+    hot_in_whole = sum(v["ms"] for v in gpu.profile().values()) / nprof
+    gpu.set_profiling(False)
+    hot_in_whole = max_over_ranks(pg, hot_in_whole)
     gpu.close()
     per = ms / args.steps
     return {"value": ws * cells * args.steps / (ms / 1e3), "unit": "cell-steps/s",
-            "ms_per_step": per, "hot_path_ms_per_step": hot_ms_per_step,
-            "before_hot_path_ms_per_step": per - hot_ms_per_step,
+            "ms_per_step": per, "hot_path_ms_per_step": hot_in_whole,
+            "before_hot_path_ms_per_step": per - hot_in_whole,
+            "headline_hot_path_ms_per_step": hot_ms_per_step,
             "poisson_iterations": statistics.mean(s["iterations"] for s in stats),
             "contra_max": max(s["contra"] for s in stats),
             "steps_above_contra_limit": sum(bool(s["unstable"]) for s in stats),

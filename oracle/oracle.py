@@ -2,8 +2,9 @@
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline legs of bench.py, and only as the checker or the timed CPU
-baseline.  PARITY UNPINNED: the reference (Fortran/PETSc) cannot run here and
-ships no golden outputs; see orctm_oracle.c.
+baseline.  PARITY PINNED ONLY IN PART: the reference (Fortran/PETSc) cannot
+run here and ships no golden outputs; its check values and input files pin
+what they cover (see orctm_oracle.h).
 
 Arrays are numpy float64 in Fortran order with the reference's shapes
 (single-rank domain, I_start = J_start = 0):

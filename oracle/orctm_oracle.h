@@ -5,10 +5,15 @@
  * compared against, and the CPU baseline that bench.py times.  Nothing in the
  * product (orctm_b200/, include/) links or calls it.
  *
- * PARITY UNPINNED: the reference (Fortran 90 + PETSc 3.10.2 + MPI) cannot be
- * compiled here and ships no golden outputs or tests, so this restatement is
- * checked only against itself (golden fixtures it generated, an independent
- * numpy restatement of selected routines, and property tests).
+ * PARITY PINNED ONLY IN PART: the reference (Fortran 90 + PETSc 3.10.2 +
+ * MPI) cannot be compiled here and ships no golden outputs or tests.  The
+ * values the reference does hold pin it: the equation of state's check
+ * values (adisitj.f90:48-51 and the UNESCO 1981 values of RHO1J) and the
+ * reference's own input files (the Sect. 3.3 tank's grid, T/S and forcing,
+ * the Sect. 3.5 boundary constants and climatology), which tests run through
+ * this restatement.  Beyond those it is checked against itself (golden
+ * fixtures it generated, an independent numpy restatement of every routine,
+ * and property tests).
  *
  * Arrays use the reference's Fortran layout (column-major, i fastest) with its
  * halos and index origins on a single-rank domain (I_start = J_start = 0):
