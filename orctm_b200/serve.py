@@ -4,7 +4,9 @@ and orctm_batch_run entry points of liborctm_gpu.so).
 ``Server`` admits requests as slots and device memory free up (continuous
 batching at step granularity: every admitted instance advances on its own
 slot thread and stream, and the device runs the slots' kernels
-concurrently); ``run_batch`` submits a whole ensemble at once.  Inputs are
+concurrently); ``run_batch`` submits a whole ensemble at once;
+``NodeServer`` spreads requests over the GPUs of a node, one ``Server`` per
+device behind a least-outstanding-work scheduler.  Inputs are
 instance dicts and state dicts of orctm_b200.configs; outputs come back as
 numpy arrays in the reference's layouts.
 """
@@ -179,6 +181,95 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def pick_device(outstanding) -> int:
+    """The index of the device with the least outstanding work (ties: the
+    lowest index)."""
+    return min(range(len(outstanding)), key=lambda k: (outstanding[k], k))
+
+
+class NodeServer:
+    """An ensemble's requests spread over the GPUs of one node: one Server
+    per device, each with its own slots, admission and memory budget, behind
+    a host scheduler that sends every request to the device with the least
+    outstanding work (the cell-steps of its requests not yet seen done).
+    The instances are independent, so nothing crosses between devices and
+    there is no collective.  ``server`` builds the per-device servers (the
+    tests pass a stand-in)."""
+
+    def __init__(self, devices=None, server=Server, **kw):
+        if devices is None:
+            import torch
+
+            devices = list(range(torch.cuda.device_count()))
+        if not devices:
+            raise ValueError("NodeServer: no device")
+        self.devices = list(devices)
+        self.servers = [server(device=d, **kw) for d in self.devices]
+        self.outstanding = [0] * len(self.devices)
+        self._where = {}      # id(job) -> (server index, work, job)
+        self._seen_done = set()
+
+    def _finished(self, key):
+        k, work, _ = self._where.pop(key)
+        self.outstanding[k] -= work
+
+    def _refresh(self):
+        for key, (k, _, job) in list(self._where.items()):
+            if key not in self._seen_done and self.servers[k].poll(job):
+                self._seen_done.add(key)
+                self._finished(key)
+
+    def submit(self, job: Job) -> Job:
+        self._refresh()
+        k = pick_device(self.outstanding)
+        self.servers[k].submit(job)
+        work = job.cells * job.req.nsteps
+        self.outstanding[k] += work
+        self._where[id(job)] = (k, work, job)
+        job.device = self.devices[k]
+        return job
+
+    def poll(self, job: Job) -> bool:
+        key = id(job)
+        if key in self._seen_done:
+            return True
+        k = self._where[key][0]
+        if self.servers[k].poll(job):
+            self._seen_done.add(key)
+            self._finished(key)
+            return True
+        return False
+
+    def wait(self, job: Job) -> Job:
+        key = id(job)
+        if key not in self._seen_done:
+            self.servers[self._where[key][0]].wait(job)
+            self._seen_done.add(key)
+            self._finished(key)
+        return job
+
+    def drain(self):
+        for srv in self.servers:
+            srv.drain()
+
+    def stats(self) -> dict:
+        per = [srv.stats() for srv in self.servers]
+        total = {k: sum(p[k] for p in per)
+                 for k in ("submitted", "completed", "failed", "steps", "cell_steps")
+                 if all(k in p for p in per)}
+        return {"devices": dict(zip(self.devices, per)), **total}
+
+    def close(self):
+        for srv in self.servers:
+            srv.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def run_batch(jobs: list, **kw) -> dict:

@@ -10,7 +10,7 @@ from orctm_b200 import _lib
 from orctm_b200 import configs as C
 from orctm_b200 import grid
 from orctm_b200.api import Instance
-from orctm_b200.serve import Job, Server, estimate_device_bytes, run_batch
+from orctm_b200.serve import Job, NodeServer, Server, estimate_device_bytes, run_batch
 
 pytestmark = pytest.mark.gpu
 
@@ -67,6 +67,23 @@ def test_served_results_equal_alone(insts, solver):
         _same(j.outputs(), alone[k])
     for k, j in enumerate(second):
         _same(j.outputs(), alone[len(insts) - 1 - k])
+
+
+def test_node_server_equals_alone(insts):
+    """The node scheduler over this box's GPUs (one per call here): every
+    request lands on a device and its result is the one alone."""
+    nsteps = 2
+    with NodeServer(slots=3, solver="fp64", rtol=1e-10, maxit=5000) as node:
+        jobs = [node.submit(Job(i, C.copy_state(i), nsteps)) for i in insts]
+        node.drain()
+        for j in jobs:
+            node.wait(j)
+            assert j.stats["status"] == 0, j.stats
+        st = node.stats()
+    assert st["completed"] == len(insts) and st["failed"] == 0
+    assert all(j.device in node.devices for j in jobs)
+    for j, i in zip(jobs, insts):
+        _same(j.outputs(), _alone(i, nsteps, "fp64"))
 
 
 def test_batch_equals_alone(insts):

@@ -1,5 +1,6 @@
 """Host side of the batch/serve API without a GPU: argument checks, the
-memory estimate, and request marshalling."""
+memory estimate, request marshalling, and the node scheduler that spreads
+requests over devices (NodeServer, with stand-in per-device servers)."""
 import ctypes as C
 
 import numpy as np
@@ -73,3 +74,81 @@ def test_job_marshalling(inst):
 def test_serve_submit_rejects_bad_request():
     lib = S._bind(_lib.load())
     assert lib.orctm_serve_submit(None, None, None) == _lib.ORCTM_E_ARG
+
+
+class _FakeServer:
+    """Stands in for one device's Server: records submissions; a request is
+    done once the test says so."""
+
+    def __init__(self, device, **kw):
+        self.device, self.kw = device, kw
+        self.jobs, self.done, self.waited = [], set(), []
+        self.closed = False
+
+    def submit(self, job):
+        self.jobs.append(job)
+        return job
+
+    def poll(self, job):
+        if id(job) in self.done:
+            self.done.discard(id(job))
+            self.jobs.remove(job)
+            return True
+        return False
+
+    def wait(self, job):
+        self.waited.append(job)
+        self.jobs.remove(job)
+        return job
+
+    def drain(self):
+        pass
+
+    def stats(self):
+        return {"submitted": len(self.jobs), "completed": 0, "failed": 0, "steps": 0,
+                "cell_steps": 0.0}
+
+    def close(self):
+        self.closed = True
+
+
+def _job(cells, nsteps=1):
+    from types import SimpleNamespace
+
+    return SimpleNamespace(cells=cells, req=SimpleNamespace(nsteps=nsteps))
+
+
+def test_pick_device_least_outstanding_lowest_on_ties():
+    assert S.pick_device([0, 0, 0]) == 0
+    assert S.pick_device([5, 2, 2]) == 1
+    assert S.pick_device([3, 7, 1, 1]) == 2
+
+
+def test_node_server_spreads_by_outstanding_work():
+    node = S.NodeServer(devices=[0, 1, 2], server=_FakeServer, slots=4)
+    assert [s.device for s in node.servers] == [0, 1, 2]
+    assert all(s.kw == {"slots": 4} for s in node.servers)
+    big, mid, small = _job(100, 10), _job(50, 10), _job(30, 10)
+    for j in (big, mid, small):
+        node.submit(j)
+    assert (big.device, mid.device, small.device) == (0, 1, 2)
+    assert node.outstanding == [1000, 500, 300]
+    nxt = node.submit(_job(10, 10))              # the least loaded: device 2
+    assert nxt.device == 2 and node.outstanding == [1000, 500, 400]
+    # device 0's request finishes: seen at the next submission, which goes there
+    node.servers[0].done.add(id(big))
+    after = node.submit(_job(20, 10))
+    assert after.device == 0 and node.outstanding == [200, 500, 400]
+    assert node.poll(big) and node.wait(big) is big   # already seen done
+    assert node.servers[0].waited == []
+    node.wait(mid)                               # blocks on device 1's server
+    assert node.servers[1].waited == [mid] and node.outstanding == [200, 0, 400]
+    assert node.stats()["submitted"] == 3
+    node.close()
+    assert all(s.closed for s in node.servers)
+
+
+def test_node_server_needs_a_device():
+    with pytest.raises(ValueError):
+        S.NodeServer(devices=[], server=_FakeServer)
+
