@@ -455,10 +455,10 @@ unsigned long long orctm_kernel_launches(void);
  * estimate, within 1 ulp of IEEE division).  Test support; allocates. */
 int orctm_check_division(int device, const double* a, const double* b, double* q, size_t n);
 
-/* Kernel variants of the Poisson solver: 4 column-kernel variants (forward
- * values in global or shared memory, 4 or 8 levels per load batch) and 6
- * stencil variants (shared-memory ring, L1 form or warp-row form, 32x8 or
- * 32x4 blocks).
+/* Kernel variants of the Poisson solver: 6 column-kernel variants (forward
+ * values in global or shared memory, 4 or 8 levels per load batch, 32x4,
+ * 32x2 or 128x1 blocks) and 9 stencil variants (0-5: shared-memory ring,
+ * L1 form or warp-row form, 32x8 or 32x4 blocks; 6-8: TMA-staged tiles).
  * All variants give bit-identical results.  A variant of -1 (the default)
  * lets the handle time the variants on its own grid before its first solve
  * in each precision and keep the fastest (the choice is cached per grid size
