@@ -4,8 +4,9 @@
  * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
  * cpu_baseline / --impl reference legs of bench.py load this library, and
  * only as the checker or the timed CPU baseline; the CUDA product never calls
- * it.  PARITY UNPINNED: the reference (Fortran 90 + PETSc 3.10.2) cannot be
- * built here and ships no golden outputs (see orctm_oracle.h).
+ * it.  PARITY PINNED ONLY IN PART: the reference (Fortran 90 + PETSc 3.10.2)
+ * cannot be built here and ships no golden outputs; its check values and
+ * input files pin what they cover (see orctm_oracle.h).
  *
  * Every routine follows the reference loop by loop; the file:line cited in
  * front of each block is the reference code it restates
